@@ -1,0 +1,216 @@
+/*
+ * rome_gpu.h - C ABI of the B200 (sm_100a) MAP classification hot path.
+ *
+ * Drop-in replacement for the E-step / M-step functions of ROME 1.1.2's
+ * MAP optimizers.  The reference keeps its optimizer driver, options and
+ * STAR/MRCS I/O; at each call site it hands plain host arrays (FP64, the
+ * reference's FDOUBLE, src/macros.h:29-33) to the entry points below.
+ * Each entry point names the reference function whose work it replaces.
+ *
+ * Conventions
+ *  - Every function returns ROME_OK (0) or a ROME_ERR_* code; the text of
+ *    the last error is available from rome_gpu_last_error().  Nothing
+ *    throws and nothing exits the process (the reference's ERROR_REPORT,
+ *    src/error.h:95-99, becomes an error code).
+ *  - Arrays use the reference layouts: Fourier images in the FFTW half
+ *    plane [size][size/2+1], row-major, rows wrapping to negative
+ *    frequencies (src/reconstruct.cpp:279-291); complex data as separate
+ *    real / imaginary arrays unless stated otherwise.
+ *  - A context is bound to one CUDA device and is not thread-safe; use one
+ *    context per host thread.  Calls block until their outputs are in the
+ *    caller's buffers.
+ *  - Accumulated outputs (wsum_*, backprojectors) are added to (+=), as the
+ *    reference accumulates into mlModel.wsum_* and backprojector[k].
+ */
+#ifndef ROME_GPU_H
+#define ROME_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ROME_GPU_ABI_VERSION 1
+
+enum RomeStatus {
+    ROME_OK = 0,
+    ROME_ERR_ARG = 1,         /* invalid argument or inconsistent sizes */
+    ROME_ERR_OOM = 2,         /* device allocation failed */
+    ROME_ERR_CUDA = 3,        /* CUDA runtime / launch error */
+    ROME_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    ROME_ERR_NUMERIC = 5,     /* NaN/Inf or an empty posterior (exp_sum_weight == 0) */
+    ROME_ERR_STATE = 6,       /* call order violated (e.g. no projectors uploaded) */
+    ROME_ERR_UNSUPPORTED = 7  /* option combination not implemented */
+};
+
+/* Arithmetic of the diff2 cross term Re<X_i, P_j> (the dense contraction).
+ * The min-diff2 subtraction, exp/normalisation of posteriors and all
+ * Fourier-weight sums are FP64 in every mode. */
+enum RomePrecision {
+    ROME_PREC_FP32 = 0,   /* CUDA-core FP32 FMA, FP32 accumulate ("plain FP32") */
+    ROME_PREC_BF16 = 1,   /* tcgen05 BF16 x BF16, FP32 accumulate in TMEM */
+    ROME_PREC_BF16X3 = 2  /* tcgen05 split precision: hi*hi + hi*lo + lo*hi */
+};
+
+typedef struct RomeGpuCtx RomeGpuCtx;
+
+typedef struct {
+    int precision;           /* RomePrecision */
+    int deterministic;       /* nonzero: fixed-order reductions where the ABI allows */
+    size_t workspace_limit;  /* device scratch cap in bytes, 0 = automatic */
+} RomeGpuConfig;
+
+/* Context lifetime.  Replaces nothing in the reference (it owns no device). */
+int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx** out);
+int rome_gpu_destroy(RomeGpuCtx* ctx);
+const char* rome_gpu_last_error(const RomeGpuCtx* ctx);
+int rome_gpu_set_precision(RomeGpuCtx* ctx, int precision);
+int rome_gpu_abi_version(void);
+
+/* Upload the K class projectors and reset the K backprojectors to zero.
+ * Replaces the projector side of MAPModel::setFourierTransformMaps
+ * (src/map_model.cpp:136-160): `data` is MyProjector::data of every class
+ * (src/reconstruct.cpp:44-59, 106-223), interleaved complex
+ * [K][pad_z][pad_size][pad_size/2+1][2], pad_z = pad_size (3D) or 1 (2D).
+ * r_max and padding_factor are ProjectorBase::r_max / padding_factor. */
+int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_classes, int ori_size, int pad_size, int r_max,
+                            int padding_factor, const double* data);
+
+/* Download (and optionally reset) the accumulated backprojector of one
+ * class: MyBackProjector::data (interleaved complex) and ::weight, same
+ * shape as the projector.  Used for the reduction across ranks
+ * (src/map_model.cpp:604-620) and before MAPModel::reconstruction. */
+int rome_gpu_get_backprojector(RomeGpuCtx* ctx, int iclass, double* data, double* weight);
+int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, const double* weight);
+
+/* ---------------------------------------------------------------------
+ * MAP2D E-step for one pool of particles.
+ * Replaces Map2dOptimizer_old::expectationSomeParticles
+ * (src/map2d_optimizer.cpp:802-854): for every pass, the shifted images
+ * (ParticleModel::preShiftedImagesCtfsAndInvSigma2s, src/exp_model.cpp:935-1104),
+ * getReferenceAllOrientations (:856-904), getAllSquaredDifferences
+ * (:907-1074), convertSquaredDifferencesToWeights (:1077-1224) and
+ * findAllSignificantPoints (:1226-1311); then updateOtherParams
+ * (:1417-1663) and backProjection (:1666-1873).  storeWeightedSums
+ * (:1314-1414) stays on the host: it needs only the per-particle outputs.
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int nr_images;             /* exp_nr_images (P) */
+    int ori_size;              /* image size */
+    int current_size;          /* fine size of this iteration */
+    int coarse_size;           /* size of pass 0 when adaptive_oversampling > 0 */
+    int nr_classes;            /* K */
+    int iclass_min, iclass_max;/* exp_iclass_min/max */
+    int nr_groups;
+    int adaptive_oversampling; /* 0: one pass; 1: coarse + fine pass */
+    int nr_psi;                /* coarse in-plane angles (exp_nr_psi) */
+    int nr_trans;              /* coarse translations (exp_nr_trans) */
+    /* SamplingGrid::exp_over_psi [nr_psi][nr_over_rot] for pass 0 and 1
+     * (pass 1 only if adaptive_oversampling > 0); degrees */
+    const double* over_psi[2];
+    /* SamplingGrid::exp_over_trans_x/y [nr_trans][nr_over_trans] per pass */
+    const double* over_trans_x[2];
+    const double* over_trans_y[2];
+    /* HealpixSampler translations_x/y [nr_trans] (the coarse grid the
+     * offset prior uses, src/map2d_optimizer.cpp:1116-1121) */
+    const double* trans_x;
+    const double* trans_y;
+    /* particle images after ParticleModel::setFourierTransforms, at
+     * current_size: Fimages_mask_fine, Fimages_nomask, Fctfs
+     * [P][current_size][current_size/2+1] */
+    const double* Fimg_real;
+    const double* Fimg_imag;
+    const double* Fimg_nomask_real;
+    const double* Fimg_nomask_imag;
+    const double* Fctf;
+    const double* highres_Xi2;  /* exp_highres_Xi2_imgs [P] */
+    const double* old_offsetx;  /* exp_old_offsetx [P] (rounded old offsets) */
+    const double* old_offsety;
+    const int* group;           /* GROUP_NO - 1 [P] */
+    /* model */
+    const double* sigma2_noise;        /* [nr_groups][ori_size/2+1] */
+    const int* Mresol_fine;            /* [current_size][current_size/2+1] */
+    const int* Mresol_coarse;          /* [coarse_size][coarse_size/2+1] */
+    const double* pdf_class;           /* [K] */
+    const double* pdf_direction;       /* [K] (one direction in 2D) */
+    const double* prior_offsetx_class; /* [K] */
+    const double* prior_offsety_class; /* [K] */
+    double sigma2_offset;
+    double sigma2_fudge;
+    double adaptive_fraction;
+    int do_ctf_correction;
+    int refs_are_ctf_corrected;
+    int do_map;
+} RomeMap2dPool;
+
+typedef struct {
+    /* per particle [P] */
+    double* min_diff2;           /* exp_min_diff2 (last pass) */
+    double* sum_weight;          /* exp_sum_weight (last pass) */
+    double* significant_weight;  /* exp_significant_weight (last pass) */
+    double* wsum_norm_correction;/* exp_wsum_norm_correction (updateOtherParams) */
+    double* pmax;                /* exp_metadata PMAX, CLASS (1-based), PSI, XOFF, YOFF, NR_SIGN */
+    int* cls;
+    double* psi;
+    double* xoff;
+    double* yoff;
+    double* nr_sign;
+    /* accumulated model sums (+=) */
+    double* wsum_sigma2_noise;        /* [nr_groups][ori_size/2+1] */
+    double* wsum_pdf_class;           /* [K] */
+    double* wsum_pdf_direction;       /* [K] */
+    double* wsum_prior_offsetx_class; /* [K] */
+    double* wsum_prior_offsety_class; /* [K] */
+    double* wsum_sigma2_offset;       /* [1] */
+    double* wsum_sumw_group;          /* [nr_groups] */
+    /* optional checkpoints in the reference's exp_Mweight layout
+     * [P][K * NrPoints(pass)] (class -> psi -> over_rot -> trans -> over_trans);
+     * entries that were not computed hold INT_MIN (diff2) or 0 (weight).
+     * NULL to skip. */
+    double* diff2[2];
+    double* weight[2];
+    char* Mcoarse_significant;        /* [P][K * nr_psi * nr_trans] (pass 0) */
+} RomeMap2dPoolOut;
+
+int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2dPoolOut* out);
+
+/* Significance selection on given weights (findAllSignificantPoints,
+ * src/map2d_optimizer.cpp:1226-1311 and src/map3d_optimizer.cpp:1812-1931):
+ * for each of n rows of `len` weights, sort the positive weights, walk from
+ * the largest until the running FP64 sum exceeds adaptive_fraction * sum[i],
+ * and return that weight and the number of weights walked.  Exposed for
+ * bit-exact checks of the selection with caller-provided weights. */
+int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, const double* weights, const double* sum_weight,
+                                double adaptive_fraction, double* significant_weight, double* nr_significant);
+
+/* ---------------------------------------------------------------------
+ * M-step reconstruction of one class from its accumulated backprojector.
+ * Replaces MAPModel::reconstruction (src/map_model.cpp:233-241) ->
+ * MyBackProjector::reconstruct (src/reconstruct.cpp:1929-2526) with the
+ * map2d/map3d defaults (trilinear, padding 2, no FSC update, C1).
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int iclass;
+    int gridding_nr_iter;     /* max_iter_preweight (10) */
+    int do_map;
+    int minres_map;
+    double tau2_fudge;
+    double normalise;         /* wsum_pdf_class[iclass] */
+    const double* tau2_in;    /* [ori_size/2+1] */
+} RomeReconIn;
+
+typedef struct {
+    double* vol;              /* [ori_size^ref_dim] real-space reference (Irefs[iclass]) */
+    double* tau2;             /* [ori_size/2+1] (unchanged unless FSC update) */
+    double* sigma2;           /* [ori_size/2+1] */
+    double* data_vs_prior;    /* [ori_size/2+1] */
+} RomeReconOut;
+
+int rome_gpu_reconstruct(RomeGpuCtx* ctx, const RomeReconIn* in, RomeReconOut* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROME_GPU_H */

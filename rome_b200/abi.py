@@ -1,0 +1,132 @@
+"""ctypes view of the C ABI declared in include/rome_gpu.h.
+
+The structures mirror the header field by field; `load_library()` opens the
+in-tree ``librome_b200.so`` built by ``rome_b200/build.py`` and raises if it
+is missing (the product has no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+ROME_OK = 0
+ROME_ERR_ARG = 1
+ROME_ERR_OOM = 2
+ROME_ERR_CUDA = 3
+ROME_ERR_TIMEOUT = 4
+ROME_ERR_NUMERIC = 5
+ROME_ERR_STATE = 6
+ROME_ERR_UNSUPPORTED = 7
+
+ROME_PREC_FP32 = 0
+ROME_PREC_BF16 = 1
+ROME_PREC_BF16X3 = 2
+
+PRECISIONS = {"fp32": ROME_PREC_FP32, "bf16": ROME_PREC_BF16, "bf16x3": ROME_PREC_BF16X3}
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+_CP = C.POINTER(C.c_char)
+
+
+class RomeGpuConfig(C.Structure):
+    _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("workspace_limit", C.c_size_t)]
+
+
+class RomeMap2dPool(C.Structure):
+    _fields_ = [
+        ("nr_images", C.c_int), ("ori_size", C.c_int), ("current_size", C.c_int), ("coarse_size", C.c_int),
+        ("nr_classes", C.c_int), ("iclass_min", C.c_int), ("iclass_max", C.c_int), ("nr_groups", C.c_int),
+        ("adaptive_oversampling", C.c_int), ("nr_psi", C.c_int), ("nr_trans", C.c_int),
+        ("over_psi", _DP * 2), ("over_trans_x", _DP * 2), ("over_trans_y", _DP * 2),
+        ("trans_x", _DP), ("trans_y", _DP),
+        ("Fimg_real", _DP), ("Fimg_imag", _DP), ("Fimg_nomask_real", _DP), ("Fimg_nomask_imag", _DP),
+        ("Fctf", _DP), ("highres_Xi2", _DP), ("old_offsetx", _DP), ("old_offsety", _DP), ("group", _IP),
+        ("sigma2_noise", _DP), ("Mresol_fine", _IP), ("Mresol_coarse", _IP),
+        ("pdf_class", _DP), ("pdf_direction", _DP), ("prior_offsetx_class", _DP), ("prior_offsety_class", _DP),
+        ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
+        ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
+    ]
+
+
+class RomeMap2dPoolOut(C.Structure):
+    _fields_ = [
+        ("min_diff2", _DP), ("sum_weight", _DP), ("significant_weight", _DP), ("wsum_norm_correction", _DP),
+        ("pmax", _DP), ("cls", _IP), ("psi", _DP), ("xoff", _DP), ("yoff", _DP), ("nr_sign", _DP),
+        ("wsum_sigma2_noise", _DP), ("wsum_pdf_class", _DP), ("wsum_pdf_direction", _DP),
+        ("wsum_prior_offsetx_class", _DP), ("wsum_prior_offsety_class", _DP), ("wsum_sigma2_offset", _DP),
+        ("wsum_sumw_group", _DP),
+        ("diff2", _DP * 2), ("weight", _DP * 2), ("Mcoarse_significant", _CP),
+    ]
+
+
+class RomeReconIn(C.Structure):
+    _fields_ = [("iclass", C.c_int), ("gridding_nr_iter", C.c_int), ("do_map", C.c_int), ("minres_map", C.c_int),
+                ("tau2_fudge", C.c_double), ("normalise", C.c_double), ("tau2_in", _DP)]
+
+
+class RomeReconOut(C.Structure):
+    _fields_ = [("vol", _DP), ("tau2", _DP), ("sigma2", _DP), ("data_vs_prior", _DP)]
+
+
+def dptr(a: Optional[np.ndarray]):
+    if a is None:
+        return _DP()
+    assert a.dtype == np.float64 and a.flags.c_contiguous, (a.dtype, a.flags)
+    return a.ctypes.data_as(_DP)
+
+
+def iptr(a: Optional[np.ndarray]):
+    if a is None:
+        return _IP()
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_IP)
+
+
+def cptr(a: Optional[np.ndarray]):
+    if a is None:
+        return _CP()
+    assert a.dtype == np.int8 and a.flags.c_contiguous
+    return a.ctypes.data_as(_CP)
+
+
+#: every symbol include/rome_gpu.h declares (checked by the CPU tests)
+EXPORTED_SYMBOLS = [
+    "rome_gpu_create", "rome_gpu_destroy", "rome_gpu_last_error", "rome_gpu_set_precision",
+    "rome_gpu_abi_version", "rome_gpu_set_projectors", "rome_gpu_get_backprojector",
+    "rome_gpu_set_backprojector", "rome_gpu_map2d_estep_pool", "rome_gpu_select_significant",
+    "rome_gpu_reconstruct",
+]
+
+_LIB = None
+
+
+def library_path() -> str:
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), "librome_b200.so")
+
+
+def load_library():
+    """Open librome_b200.so (in-tree).  Raises if it has not been built."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m rome_b200.build` (no CPU fallback exists)")
+    lib = C.CDLL(path)
+    lib.rome_gpu_create.argtypes = [C.c_int, C.POINTER(RomeGpuConfig), C.POINTER(C.c_void_p)]
+    lib.rome_gpu_destroy.argtypes = [C.c_void_p]
+    lib.rome_gpu_last_error.argtypes = [C.c_void_p]
+    lib.rome_gpu_last_error.restype = C.c_char_p
+    lib.rome_gpu_set_precision.argtypes = [C.c_void_p, C.c_int]
+    lib.rome_gpu_set_projectors.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _DP]
+    lib.rome_gpu_get_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
+    lib.rome_gpu_set_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
+    lib.rome_gpu_map2d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap2dPool), C.POINTER(RomeMap2dPoolOut)]
+    lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
+    lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]
+    _LIB = lib
+    return lib

@@ -1,0 +1,316 @@
+"""Host-side mirror of the MAP2D E-step interface (Map2dOptimizer_old).
+
+`Map2dPool` carries the arrays that ``expectationSomeParticles()``
+(src/map2d_optimizer.cpp:802-854) reads from the optimizer's globals;
+`GpuContext.map2d_estep_pool` sends them through the C ABI
+(``rome_gpu_map2d_estep_pool``) and returns the reference's outputs under the
+reference's names.  `store_weighted_sums` is the host-side remainder
+(src/map2d_optimizer.cpp:1314-1414).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import abi
+
+
+@dataclasses.dataclass
+class Map2dPool:
+    ori_size: int
+    current_size: int
+    coarse_size: int
+    nr_classes: int
+    nr_groups: int
+    adaptive_oversampling: int
+    over_psi: list            # per pass [nr_psi][nr_over_rot]
+    over_trans_x: list        # per pass [nr_trans][nr_over_trans]
+    over_trans_y: list
+    trans_x: np.ndarray       # [nr_trans]
+    trans_y: np.ndarray
+    Fimg_real: np.ndarray     # [P][F(current)]
+    Fimg_imag: np.ndarray
+    Fimg_nomask_real: np.ndarray
+    Fimg_nomask_imag: np.ndarray
+    Fctf: np.ndarray
+    highres_Xi2: np.ndarray
+    old_offsetx: np.ndarray
+    old_offsety: np.ndarray
+    group: np.ndarray         # int32, 0-based
+    sigma2_noise: np.ndarray  # [G][ori/2+1]
+    Mresol_fine: np.ndarray   # int32
+    Mresol_coarse: np.ndarray
+    pdf_class: np.ndarray
+    pdf_direction: np.ndarray
+    prior_offsetx_class: np.ndarray
+    prior_offsety_class: np.ndarray
+    sigma2_offset: float
+    sigma2_fudge: float = 1.0
+    adaptive_fraction: float = 0.999
+    do_ctf_correction: int = 1
+    refs_are_ctf_corrected: int = 1
+    do_map: int = 1
+    iclass_min: int = 0
+    iclass_max: int = -1
+
+    @property
+    def nr_images(self) -> int:
+        return int(self.Fimg_real.shape[0])
+
+    @property
+    def nr_psi(self) -> int:
+        return int(np.asarray(self.over_psi[0]).shape[0])
+
+    @property
+    def nr_trans(self) -> int:
+        return int(np.asarray(self.trans_x).shape[0])
+
+    def npass(self) -> int:
+        return 2 if self.adaptive_oversampling > 0 else 1
+
+    def xsize(self, ipass: int) -> int:
+        nor = np.asarray(self.over_psi[ipass]).shape[1]
+        notr = np.asarray(self.over_trans_x[ipass]).shape[1]
+        return self.nr_classes * self.nr_psi * nor * self.nr_trans * notr
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int32))
+
+
+def pack_pool(p: Map2dPool):
+    """Build the RomeMap2dPool struct; returns (struct, keepalive list)."""
+    keep = []
+
+    def d(a):
+        a = _f64(a)
+        keep.append(a)
+        return abi.dptr(a)
+
+    def i(a):
+        a = _i32(a)
+        keep.append(a)
+        return abi.iptr(a)
+
+    s = abi.RomeMap2dPool()
+    s.nr_images = p.nr_images
+    s.ori_size, s.current_size, s.coarse_size = p.ori_size, p.current_size, p.coarse_size
+    s.nr_classes, s.nr_groups = p.nr_classes, p.nr_groups
+    s.iclass_min = p.iclass_min
+    s.iclass_max = p.iclass_max if p.iclass_max >= 0 else p.nr_classes - 1
+    s.adaptive_oversampling = p.adaptive_oversampling
+    s.nr_psi, s.nr_trans = p.nr_psi, p.nr_trans
+    for ip in range(p.npass()):
+        s.over_psi[ip] = d(p.over_psi[ip])
+        s.over_trans_x[ip] = d(p.over_trans_x[ip])
+        s.over_trans_y[ip] = d(p.over_trans_y[ip])
+    s.trans_x, s.trans_y = d(p.trans_x), d(p.trans_y)
+    s.Fimg_real, s.Fimg_imag = d(p.Fimg_real), d(p.Fimg_imag)
+    s.Fimg_nomask_real, s.Fimg_nomask_imag = d(p.Fimg_nomask_real), d(p.Fimg_nomask_imag)
+    s.Fctf = d(p.Fctf)
+    s.highres_Xi2 = d(p.highres_Xi2)
+    s.old_offsetx, s.old_offsety = d(p.old_offsetx), d(p.old_offsety)
+    s.group = i(p.group)
+    s.sigma2_noise = d(p.sigma2_noise)
+    s.Mresol_fine, s.Mresol_coarse = i(p.Mresol_fine), i(p.Mresol_coarse)
+    s.pdf_class, s.pdf_direction = d(p.pdf_class), d(p.pdf_direction)
+    s.prior_offsetx_class, s.prior_offsety_class = d(p.prior_offsetx_class), d(p.prior_offsety_class)
+    s.sigma2_offset, s.sigma2_fudge, s.adaptive_fraction = p.sigma2_offset, p.sigma2_fudge, p.adaptive_fraction
+    s.do_ctf_correction, s.refs_are_ctf_corrected, s.do_map = p.do_ctf_correction, p.refs_are_ctf_corrected, p.do_map
+    return s, keep
+
+
+def alloc_outputs(p: Map2dPool, checkpoints: bool = False):
+    """Zeroed output arrays + the RomeMap2dPoolOut struct pointing at them."""
+    P, K, G, oF = p.nr_images, p.nr_classes, p.nr_groups, p.ori_size // 2 + 1
+    o: Dict[str, np.ndarray] = {}
+    for name in ["min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "psi", "xoff",
+                 "yoff", "nr_sign"]:
+        o[name] = np.zeros(P, np.float64)
+    o["cls"] = np.zeros(P, np.int32)
+    o["wsum_sigma2_noise"] = np.zeros((G, oF), np.float64)
+    for name in ["wsum_pdf_class", "wsum_pdf_direction", "wsum_prior_offsetx_class", "wsum_prior_offsety_class"]:
+        o[name] = np.zeros(K, np.float64)
+    o["wsum_sigma2_offset"] = np.zeros(1, np.float64)
+    o["wsum_sumw_group"] = np.zeros(G, np.float64)
+    s = abi.RomeMap2dPoolOut()
+    for name, arr in o.items():
+        setattr(s, name, abi.iptr(arr) if arr.dtype == np.int32 else abi.dptr(arr))
+    if checkpoints:
+        for ip in range(p.npass()):
+            o[f"diff2_{ip}"] = np.zeros((P, p.xsize(ip)), np.float64)
+            o[f"weight_{ip}"] = np.zeros((P, p.xsize(ip)), np.float64)
+            s.diff2[ip] = abi.dptr(o[f"diff2_{ip}"])
+            s.weight[ip] = abi.dptr(o[f"weight_{ip}"])
+        o["Mcoarse_significant"] = np.zeros((P, p.nr_classes * p.nr_psi * p.nr_trans), np.int8)
+        s.Mcoarse_significant = abi.cptr(o["Mcoarse_significant"])
+    return s, o
+
+
+class RomeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rome_gpu error {code}: {msg}")
+        self.code = code
+
+
+class GpuContext:
+    """One device context of librome_b200 (``rome_gpu_create``)."""
+
+    def __init__(self, device: int = 0, precision: str = "fp32", deterministic: bool = False):
+        self.lib = abi.load_library()
+        cfg = abi.RomeGpuConfig(abi.PRECISIONS[precision], int(deterministic), 0)
+        h = C.c_void_p()
+        rc = self.lib.rome_gpu_create(device, C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise RomeError(rc, "rome_gpu_create failed")
+        self.h = h
+
+    def _check(self, rc: int):
+        if rc != abi.ROME_OK:
+            msg = self.lib.rome_gpu_last_error(self.h)
+            raise RomeError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if self.h:
+            self.lib.rome_gpu_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_precision(self, precision: str):
+        self._check(self.lib.rome_gpu_set_precision(self.h, abi.PRECISIONS[precision]))
+
+    def set_projectors(self, data: np.ndarray, ori_size: int, r_max: int, padding_factor: int = 2):
+        """data: [K][pad][pad/2+1][2] (2D) or [K][pad][pad][pad/2+1][2] (3D)."""
+        data = _f64(data)
+        ref_dim = 3 if data.ndim == 5 else 2
+        K, pad = data.shape[0], data.shape[-3]
+        self._check(self.lib.rome_gpu_set_projectors(self.h, ref_dim, K, ori_size, pad, r_max, padding_factor,
+                                                     abi.dptr(data)))
+        self.proj_shape = data.shape
+
+    def get_backprojector(self, iclass: int):
+        shp = self.proj_shape[1:]
+        data = np.zeros(shp, np.float64)
+        weight = np.zeros(shp[:-1], np.float64)
+        self._check(self.lib.rome_gpu_get_backprojector(self.h, iclass, abi.dptr(data), abi.dptr(weight)))
+        return data, weight
+
+    def set_backprojector(self, iclass: int, data: np.ndarray, weight: np.ndarray):
+        self._check(self.lib.rome_gpu_set_backprojector(self.h, iclass, abi.dptr(_f64(data)), abi.dptr(_f64(weight))))
+
+    def map2d_estep_pool(self, p: Map2dPool, checkpoints: bool = False) -> Dict[str, np.ndarray]:
+        s, keep = pack_pool(p)
+        so, o = alloc_outputs(p, checkpoints)
+        self._check(self.lib.rome_gpu_map2d_estep_pool(self.h, C.byref(s), C.byref(so)))
+        return o
+
+    def select_significant(self, weights: np.ndarray, sum_weight: np.ndarray, adaptive_fraction: float):
+        w = _f64(weights)
+        n, ln = w.shape
+        sw = np.zeros(n, np.float64)
+        ns = np.zeros(n, np.float64)
+        self._check(self.lib.rome_gpu_select_significant(self.h, n, ln, abi.dptr(w), abi.dptr(_f64(sum_weight)),
+                                                          adaptive_fraction, abi.dptr(sw), abi.dptr(ns)))
+        return sw, ns
+
+    def reconstruct(self, iclass: int, ori_size: int, ref_dim: int, tau2: np.ndarray, tau2_fudge: float,
+                    normalise: float, gridding_nr_iter: int = 10, do_map: bool = True, minres_map: int = 5):
+        oF = ori_size // 2 + 1
+        rin = abi.RomeReconIn(iclass, gridding_nr_iter, int(do_map), minres_map, tau2_fudge, normalise,
+                              abi.dptr(_f64(tau2)))
+        keep_tau = _f64(tau2)
+        rin.tau2_in = abi.dptr(keep_tau)
+        vol = np.zeros((ori_size,) * ref_dim, np.float64)
+        o = {"vol": vol, "tau2": np.zeros(oF), "sigma2": np.zeros(oF), "data_vs_prior": np.zeros(oF)}
+        rout = abi.RomeReconOut(abi.dptr(vol), abi.dptr(o["tau2"]), abi.dptr(o["sigma2"]),
+                                abi.dptr(o["data_vs_prior"]))
+        self._check(self.lib.rome_gpu_reconstruct(self.h, C.byref(rin), C.byref(rout)))
+        return o
+
+
+def store_weighted_sums(p: Map2dPool, est: Dict[str, np.ndarray], power_imgs: np.ndarray, norm_in: np.ndarray,
+                        avg_norm_correction: float, do_norm_correction: bool, Mresol_fine: np.ndarray,
+                        sigma2_noise: np.ndarray, wsum: Dict[str, np.ndarray]):
+    """storeWeightedSums (src/map2d_optimizer.cpp:1314-1414), host side, FP64.
+
+    Returns per-particle (dLL, NORM) and accumulates into ``wsum`` (keys
+    wsum_sigma2_noise, wsum_avg_norm_correction, wsum_LL, wsum_ave_Pmax).
+    """
+    cur_F = p.current_size // 2 + 1
+    ori_F = p.ori_size // 2 + 1
+    P = p.nr_images
+    dll = np.zeros(P)
+    norm = np.array(norm_in, np.float64).copy()
+    wnc = est["wsum_norm_correction"].copy()
+    for i in range(P):
+        g = int(p.group[i])
+        for ires in range(cur_F, ori_F):
+            wsum["wsum_sigma2_noise"][g, ires] += power_imgs[i, ires]
+            wnc[i] += power_imgs[i, ires]
+        if do_norm_correction:
+            old = norm[i] / avg_norm_correction
+            norm[i] = old * np.sqrt(wnc[i] * 2.)
+            wsum["wsum_avg_norm_correction"] += old * np.sqrt(wnc[i] * 2.)
+        ires = Mresol_fine
+        sel = ires > 0
+        logsigma2 = float(np.sum(np.log(2. * np.pi * sigma2_noise[g][ires[sel]])))
+        if est["sum_weight"][i] == 0:
+            raise RomeError(abi.ROME_ERR_NUMERIC, "exp_sum_weight[ipart]==0")
+        dll[i] = np.log(est["sum_weight"][i]) - est["min_diff2"][i] - logsigma2
+        wsum["wsum_LL"] += dll[i]
+        wsum["wsum_ave_Pmax"] += est["pmax"][i]
+    return dll, norm
+
+
+def load_dump(path: str) -> Dict[str, np.ndarray]:
+    """Read a reference-harness dump directory (manifest.txt + *.bin)."""
+    import os
+    out = {}
+    with open(os.path.join(path, "manifest.txt")) as f:
+        for line in f:
+            parts = line.split()
+            if not parts:
+                continue
+            name, dt, shape = parts[0], parts[1], tuple(int(x) for x in parts[2:])
+            arr = np.fromfile(os.path.join(path, name + ".bin"), dtype=np.dtype(dt))
+            out[name] = arr.reshape(shape)
+    return out
+
+
+def pool_from_dump(d: Dict[str, np.ndarray], pool: int = 0) -> Map2dPool:
+    """Map2dPool with the inputs the reference harness recorded for one pool."""
+    pp = f"pool{pool}_"
+    os_ = int(d["adaptive_oversampling"][0])
+    npass = 2 if os_ > 0 else 1
+    return Map2dPool(
+        ori_size=int(d["ori_size"][0]), current_size=int(d["current_size"][0]),
+        coarse_size=int(d["coarse_size"][0]), nr_classes=int(d["nr_classes"][0]),
+        nr_groups=int(d["nr_groups"][0]), adaptive_oversampling=os_,
+        over_psi=[d[f"pass{ip}_over_psi"] for ip in range(npass)],
+        over_trans_x=[d[f"pass{ip}_over_trans_x"] for ip in range(npass)],
+        over_trans_y=[d[f"pass{ip}_over_trans_y"] for ip in range(npass)],
+        trans_x=d["trans_x"], trans_y=d["trans_y"],
+        Fimg_real=d[pp + "Fimg_real"], Fimg_imag=d[pp + "Fimg_imag"],
+        Fimg_nomask_real=d[pp + "Fimg_nomask_real"], Fimg_nomask_imag=d[pp + "Fimg_nomask_imag"],
+        Fctf=d[pp + "Fctf"], highres_Xi2=d[pp + "highres_Xi2"],
+        old_offsetx=d[pp + "old_offsetx"], old_offsety=d[pp + "old_offsety"], group=d[pp + "group"],
+        sigma2_noise=d["sigma2_noise"], Mresol_fine=d["Mresol_fine"], Mresol_coarse=d["Mresol_coarse"],
+        pdf_class=d["pdf_class"], pdf_direction=d["pdf_direction"],
+        prior_offsetx_class=d["prior_offsetx_class"], prior_offsety_class=d["prior_offsety_class"],
+        sigma2_offset=float(d["sigma2_offset"][0]), sigma2_fudge=float(d["sigma2_fudge"][0]),
+        adaptive_fraction=float(d["adaptive_fraction"][0]),
+        do_ctf_correction=int(d["do_ctf_correction"][0]),
+        refs_are_ctf_corrected=int(d["refs_are_ctf_corrected"][0]), do_map=int(d["do_map"][0]),
+    )
