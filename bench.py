@@ -1,0 +1,277 @@
+"""MAP E-step throughput benchmark (particles/s) on B200.
+
+Workload: BASELINE config 2, "MAP2D at scale": 20,000 synthetic particles of
+128 x 128 from K = 50 random-blob class templates, 72 in-plane angles (5 deg)
+x 29 translations (+-6 px, step 2), CTF per particle, white noise at SNR
+0.03, current_size = ori_size = 128 (8,320 Fourier coefficients per image).
+A step is one E-step pass (expectationSomeParticles: diff2, posterior,
+significance, weighted sums, backprojection) over all particles, in pools
+of --pool particles.
+
+Arms:
+  default            this library (librome_b200, CUDA, sm_100a)
+  --impl reference   the reference's CPU implementation on the host cores
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "E-step particles/s: learned-proposal+BF16 vs plain FP32 GPU at >=99% pose agree"
+UNIT = "particles/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="map2d_cfg2")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "bf16x3"])
+    ap.add_argument("--pool", type=int, default=1000)
+    ap.add_argument("--particles", type=int, default=0, help="override the particle count (debug)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                vals = [v.strip() for v in out.stdout.strip().split(",")]
+                if len(vals) == 6:
+                    self.samples.append(vals)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[2 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from rome_b200.map2d import GpuContext
+    from rome_b200.workload import CONFIGS, build_map2d, subset
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    w = CONFIGS[args.config]
+    if args.particles:
+        w = __import__("dataclasses").replace(w, n_particles=args.particles)
+    # every rank processes its own shard of particles (weak scaling, no data-path collective)
+    w = __import__("dataclasses").replace(w, seed=w.seed + 1000 * rank)
+    pool, proj, r_max, truth = build_map2d(w)
+    N = pool.nr_images
+    ctx = GpuContext(local, args.precision, profile=True)
+    ctx.set_projectors(proj, pool.ori_size, r_max)
+    pools = [subset(pool, lo, min(N, lo + args.pool)) for lo in range(0, N, args.pool)]
+
+    def step(dev_inputs):
+        res = []
+        for q in (dev_inputs if dev_inputs is not None else pools):
+            res.append(ctx.map2d_estep_pool(q))
+        return res
+
+    # device-resident inputs for the kernel-only figure
+    dev = [ctx.stage_pool(q) for q in pools]
+    for _ in range(args.warmup):
+        step(dev)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ctx.reset_timings()
+    with ClockSampler(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True)
+        t1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        t0.record()
+        last = None
+        for _ in range(args.steps):
+            last = step(dev)
+        t1.record()
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+    timings = ctx.get_timings()
+    # end to end through the C ABI with host buffers (H2D + D2H inside)
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(max(1, args.steps)):
+        step(None)
+    torch.cuda.synchronize()
+    e_ms = (time.perf_counter() - e0) * 1e3
+    ms_t = torch.tensor([ms, e_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms, e_ms = ms_t.tolist()
+    ms_step = ms / args.steps
+    value = N * world / (ms_step / 1e3)
+    e2e_value = N * world / (e_ms / max(1, args.steps) / 1e3)
+    # pose agreement with the generating truth (all particles of the last step)
+    cls = np.concatenate([r["cls"] for r in last]) - 1
+    pose_ok = float(np.mean(cls == truth["cls"]))
+    hbm, bf16, peak_kind = load_peaks()
+    # dominant kernel: the cross-term contraction, 4 F flops per (particle, hypothesis) on the active pixels
+    gem = timings["cross_gemm"]
+    flops_per_launch = gem["flops"] / max(gem["launches"], 1)
+    achieved = flops_per_launch / (gem["ms"] / max(gem["launches"], 1) / 1e3) / 1e12 if gem["ms"] > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": {"fp32": "f32", "bf16": "bf16", "bf16x3": "bf16x3"}[args.precision],
+        "data": "synthetic (seeded random-blob templates, CTF, white noise)",
+        "config": {"workload": args.config, "particles_per_gpu": N, "image": w.ori_size, "classes": w.n_classes,
+                   "psi": int(round(360 / w.psi_step)), "translations": int(pool.nr_trans), "pool": args.pool,
+                   "precision": args.precision, "inputs": "larger than L2 (no flush)",
+                   "pose_agreement_vs_truth": round(pose_ok, 4)},
+        "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(ctx.h2d_bytes(q) for q in pools)),
+                "d2h_bytes_per_step": int(sum(ctx.d2h_bytes(q) for q in pools))},
+        "gpu_launches": int(timings["total_launches"]),
+        "roofline": {"bound": "tensor", "achieved": round(achieved, 2), "peak": bf16, "unit": "TFLOP/s",
+                     "frac": round(achieved / bf16, 4), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "cross_gemm"},
+        "phases_ms": {k: round(v["ms"], 3) for k, v in timings.items() if isinstance(v, dict)},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, w)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+_W = {}
+
+
+def _oracle_init(proj, r_max):
+    _W["proj"], _W["r_max"] = proj, r_max
+
+
+def _oracle_worker(pool):
+    """One process of the CPU baseline: the oracle E-step on a sub-pool."""
+    from oracle import oracle_py
+    t = time.perf_counter()
+    oracle_py.map2d_estep_pool(pool, _W["proj"], _W["r_max"])
+    return time.perf_counter() - t
+
+
+def oracle_rate(w, target_seconds: float = 15.0, cores: int = 0):
+    """Particles/s of the C oracle (FP64, the reference's operation order and
+    loop structure) on a bounded sample of the same workload: one particle
+    per process, all host cores, sample sized to about `target_seconds`."""
+    import dataclasses
+    import multiprocessing as mp
+    import pickle
+
+    from rome_b200.workload import build_map2d, subset
+    cores = cores or os.cpu_count() or 1
+    probe = dataclasses.replace(w, n_particles=max(cores, 1), seed=w.seed + 7)
+    pool, proj, r_max, _ = build_map2d(probe)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores, initializer=_oracle_init, initargs=(proj, r_max)) as pp:
+        # one particle to size the sample
+        t1 = pp.map(_oracle_worker, [subset(pool, 0, 1)])[0]
+        rounds = max(1, int(target_seconds / max(t1, 1e-3)))
+        n = min(pool.nr_images, cores)
+        jobs = [subset(pool, i, i + 1) for i in range(n)] * rounds
+        t0 = time.perf_counter()
+        pp.map(_oracle_worker, jobs)
+        dt = time.perf_counter() - t0
+    return {"value": round(len(jobs) / dt, 4), "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{len(jobs)} particles of {w.ori_size}x{w.ori_size}, K={w.n_classes}, "
+                      f"{pool.nr_psi} psi x {pool.nr_trans} translations, one particle per process, "
+                      f"{dt:.1f} s wall"}
+
+
+def cpu_baseline(args, w):
+    try:
+        return oracle_rate(w, target_seconds=15.0)
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+
+def run_reference(args):
+    """The reference arm: the CPU implementation on every host core, same
+    workload and metric; rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from rome_b200.workload import CONFIGS
+    w = CONFIGS[args.config]
+    rates = []
+    for _ in range(args.warmup + args.steps) if args.steps <= 1 else range(args.steps):
+        rates.append(oracle_rate(w, target_seconds=20.0))
+    best = rates[-1]
+    line = {"metric": METRIC, "value": best["value"], "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "image": w.ori_size, "classes": w.n_classes},
+            "cpu_baseline": best,
+            "e2e": {"value": best["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

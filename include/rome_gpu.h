@@ -59,7 +59,35 @@ typedef struct {
     int precision;           /* RomePrecision */
     int deterministic;       /* nonzero: fixed-order reductions where the ABI allows */
     size_t workspace_limit;  /* device scratch cap in bytes, 0 = automatic */
+    int profile;             /* nonzero: time each phase with CUDA events (rome_gpu_get_timings) */
 } RomeGpuConfig;
+
+/* Per-phase device time (CUDA events on the context's stream, summed over
+ * calls since the last reset) and launch counts.  The phases follow the
+ * reference's E-step functions. */
+enum RomePhase {
+    ROME_PHASE_PREP = 0,      /* window, CTF, Minvsigma2 */
+    ROME_PHASE_PROJECT,       /* getReferenceAllOrientations */
+    ROME_PHASE_SHIFT,         /* shifted images -> contraction operand */
+    ROME_PHASE_NORM_GEMM,     /* sum_n Minvsigma2 ctf^2 |P|^2 */
+    ROME_PHASE_CROSS_GEMM,    /* Re<X_t, P> over all images x orientations (dominant) */
+    ROME_PHASE_POSTERIOR,     /* weights, sum, argmax, significance */
+    ROME_PHASE_WSUM,          /* updateOtherParams */
+    ROME_PHASE_BACKPROJECT,   /* backProjection */
+    ROME_PHASE_RECONSTRUCT,   /* MyBackProjector::reconstruct */
+    ROME_PHASE_COUNT
+};
+
+typedef struct {
+    double ms[ROME_PHASE_COUNT];        /* device milliseconds per phase */
+    long launches[ROME_PHASE_COUNT];    /* kernel launches per phase */
+    double flops[ROME_PHASE_COUNT];     /* algorithmic flops per phase (contractions) */
+    double bytes[ROME_PHASE_COUNT];     /* algorithmic bytes per phase (HBM-bound kernels) */
+    long total_launches;                /* all kernels of this library since the last reset */
+} RomeGpuTimings;
+
+int rome_gpu_get_timings(RomeGpuCtx* ctx, RomeGpuTimings* out);
+int rome_gpu_reset_timings(RomeGpuCtx* ctx);
 
 /* Context lifetime.  Replaces nothing in the reference (it owns no device). */
 int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx** out);
@@ -142,6 +170,9 @@ typedef struct {
     int do_ctf_correction;
     int refs_are_ctf_corrected;
     int do_map;
+    /* nonzero: Fimg_real/imag, Fimg_nomask_real/imag and Fctf are device
+     * pointers on the context's device (no host-to-device copy) */
+    int inputs_on_device;
 } RomeMap2dPool;
 
 typedef struct {

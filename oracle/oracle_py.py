@@ -22,7 +22,9 @@ def lib():
     if _LIB is None:
         path = os.path.join(_HERE, "_ref", "librome_oracle.so")
         if not os.path.exists(path):
-            raise RuntimeError(f"{path} missing: run `make -C oracle _ref/librome_oracle.so`")
+            # the C restatement needs only gcc (not the reference tree)
+            import subprocess
+            subprocess.check_call(["make", "-C", _HERE, "_ref/librome_oracle.so"], stdout=subprocess.DEVNULL)
         L = C.CDLL(path)
         DP = C.POINTER(C.c_double)
         L.oracle_map2d_estep_pool.argtypes = [C.POINTER(abi.RomeMap2dPool), C.POINTER(abi.RomeMap2dPoolOut), C.c_int,

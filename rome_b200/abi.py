@@ -33,7 +33,17 @@ _CP = C.POINTER(C.c_char)
 
 
 class RomeGpuConfig(C.Structure):
-    _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("workspace_limit", C.c_size_t)]
+    _fields_ = [("precision", C.c_int), ("deterministic", C.c_int), ("workspace_limit", C.c_size_t),
+                ("profile", C.c_int)]
+
+
+PHASES = ["prep", "project", "shift", "norm_gemm", "cross_gemm", "posterior", "wsum", "backproject", "reconstruct"]
+
+
+class RomeGpuTimings(C.Structure):
+    _fields_ = [("ms", C.c_double * len(PHASES)), ("launches", C.c_long * len(PHASES)),
+                ("flops", C.c_double * len(PHASES)), ("bytes", C.c_double * len(PHASES)),
+                ("total_launches", C.c_long)]
 
 
 class RomeMap2dPool(C.Structure):
@@ -49,6 +59,7 @@ class RomeMap2dPool(C.Structure):
         ("pdf_class", _DP), ("pdf_direction", _DP), ("prior_offsetx_class", _DP), ("prior_offsety_class", _DP),
         ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
         ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
+        ("inputs_on_device", C.c_int),
     ]
 
 
@@ -98,7 +109,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_create", "rome_gpu_destroy", "rome_gpu_last_error", "rome_gpu_set_precision",
     "rome_gpu_abi_version", "rome_gpu_set_projectors", "rome_gpu_get_backprojector",
     "rome_gpu_set_backprojector", "rome_gpu_map2d_estep_pool", "rome_gpu_select_significant",
-    "rome_gpu_reconstruct",
+    "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings",
 ]
 
 _LIB = None
@@ -128,5 +139,7 @@ def load_library():
     lib.rome_gpu_map2d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap2dPool), C.POINTER(RomeMap2dPoolOut)]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]
+    lib.rome_gpu_get_timings.argtypes = [C.c_void_p, C.POINTER(RomeGpuTimings)]
+    lib.rome_gpu_reset_timings.argtypes = [C.c_void_p]
     _LIB = lib
     return lib

@@ -1,0 +1,224 @@
+// Shared definitions of librome_b200 (sm_100a): status handling, the device
+// context behind RomeGpuCtx, and small device helpers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/rome_gpu.h"
+
+namespace rome {
+
+// ---------------------------------------------------------------------------
+// errors: every entry point catches RomeFail and turns it into a status code
+struct RomeFail {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] inline void fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    throw RomeFail{code, buf};
+}
+
+#define ROME_CUDA(call)                                                                                  \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            ::rome::fail(e_ == cudaErrorMemoryAllocation ? ROME_ERR_OOM : ROME_ERR_CUDA, "%s:%d %s: %s", \
+                         __FILE__, __LINE__, #call, cudaGetErrorString(e_));                             \
+    } while (0)
+
+#define ROME_CHECK_LAUNCH() ROME_CUDA(cudaGetLastError())
+
+#define ROME_REQUIRE(cond, ...)                             \
+    do {                                                    \
+        if (!(cond)) ::rome::fail(ROME_ERR_ARG, __VA_ARGS__); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers that grow on demand and are reused across calls
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void* get(size_t need) {
+        if (need > bytes) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            bytes = 0;
+            size_t want = need + need / 8 + 256;
+            ROME_CUDA(cudaMalloc(&p, want));
+            bytes = want;
+        }
+        return p;
+    }
+    template <typename T>
+    T* as(size_t count) {
+        return (T*)get(count * sizeof(T) > 0 ? count * sizeof(T) : 16);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+// device workspace slots used by the MAP2D pool driver
+enum Slot {
+    S_FIMG,       // windowed masked image [P][F] double2
+    S_FNOMASK,    // nomask image * ctf * Minvsigma2 [P][F] double2
+    S_CTF,        // local ctf [P][F] double
+    S_MINV,       // Minvsigma2 [P][F] double
+    S_ACT,        // active pixel list [Kact] int
+    S_A,          // cross-term A operand (fp32 or bf16 hi/lo)
+    S_B,          // cross-term B operand
+    S_W2,         // norm GEMM A operand: Minvsigma2 * ctf^2 [P][Kp2] float
+    S_Q,          // norm GEMM B operand: |P|^2 [J][Kp2] float
+    S_NORM,       // norm term [P][J] float
+    S_S,          // sum M |X_t|^2 [P*T] float
+    S_PROJ,       // projections FP64 [J][Kact] double2
+    S_DIFF2,      // diff2 [P][X] float
+    S_ROTM,       // rotation matrices [J][4] double
+    S_JVALID,     // orientation validity [J] int
+    S_SHIFT,      // per-translation (xshift, yshift) [T] double2
+    S_POFF,       // pdf_offset [P][K][ntr] double
+    S_PDIR,       // pdf_direction [K] double
+    S_PART,       // per particle scalars [P][8] double (min, sum, sig, thr, ...)
+    S_PARTI,      // per particle ints [P][8]
+    S_MCOARSE,    // coarse significance [P][K*npsi*ntr] char
+    S_WCHK,       // optional weight checkpoint [P][X] double
+    S_SCRATCH,    // selection scratch
+    S_WSN,        // wsum_sigma2_noise accum [G][oriF] double
+    S_WSUMK,      // class sums [8][K] double + group sums
+    S_MRES,       // Mresol [F] int
+    S_SIG2,       // sigma2_noise [G][oriF] double
+    S_GROUP,      // group [P] int
+    S_OLDOFF,     // old offsets [P] double2
+    S_XI2,        // highres_Xi2 [P] double
+    S_LIST,       // particle list of the selection fallback
+    S_ROTSIG,     // Rot_significant [K*npsi] char
+    S_ACTIDX,     // pixel -> active index [F] int
+    S_TRANS,      // translations of the last pass [T] double2
+    S_TMP0,
+    S_TMP1,
+    S_TMP2,
+    S_COUNT
+};
+
+}  // namespace rome
+
+struct RomeGpuCtx {
+    int device = 0;
+    int precision = ROME_PREC_FP32;
+    int deterministic = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    // class references (projectors) and accumulated backprojectors, FP64
+    int ref_dim = 0, nr_classes = 0, ori_size = 0, pad_size = 0, r_max = 0, padding = 2;
+    long vox = 0;  // voxels per class (pad_z * pad * padF)
+    double2* proj = nullptr;
+    double2* bp_data = nullptr;
+    double* bp_weight = nullptr;
+    rome::DevBuf ws[rome::S_COUNT];
+    // host-side staging
+    std::vector<double> h_tmp;
+    // shift table (cos, sin) from the host's libm, identical to the reference's
+    double2* d_shift_tab = nullptr;
+    double shift_sampling = 0;
+    // per-phase device timings and launch counts (rome_gpu_get_timings)
+    int profile = 0;
+    double phase_ms[ROME_PHASE_COUNT] = {};
+    long phase_launches[ROME_PHASE_COUNT] = {};
+    double phase_flops[ROME_PHASE_COUNT] = {};
+    double phase_bytes[ROME_PHASE_COUNT] = {};
+    long total_launches = 0;
+};
+
+namespace rome {
+
+// run a function, converting RomeFail into a status and recording the message
+template <typename F>
+int guarded(RomeGpuCtx* ctx, F&& f) {
+    try {
+        f();
+        return ROME_OK;
+    } catch (const RomeFail& e) {
+        if (ctx) ctx->last_error = e.msg;
+        return e.code;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->last_error = e.what();
+        return ROME_ERR_ARG;
+    }
+}
+
+// Phase timer: CUDA events on the context's stream around each phase (when
+// profiling is on) and launch / work counters (always).
+class Profiler {
+  public:
+    explicit Profiler(RomeGpuCtx* c) : ctx_(c) {}
+    ~Profiler() {
+        for (auto& r : recs_) {
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+    }
+    void begin(int ph) {
+        if (!ctx_->profile) return;
+        Rec r{ph, nullptr, nullptr};
+        ROME_CUDA(cudaEventCreate(&r.a));
+        ROME_CUDA(cudaEventCreate(&r.b));
+        ROME_CUDA(cudaEventRecord(r.a, ctx_->stream));
+        recs_.push_back(r);
+    }
+    void end(int ph) {
+        if (!ctx_->profile) return;
+        for (auto it = recs_.rbegin(); it != recs_.rend(); ++it)
+            if (it->phase == ph) {
+                ROME_CUDA(cudaEventRecord(it->b, ctx_->stream));
+                return;
+            }
+    }
+    void launched(int ph, int n = 1) {
+        ctx_->phase_launches[ph] += n;
+        ctx_->total_launches += n;
+    }
+    void add_flops(int ph, double f) { ctx_->phase_flops[ph] += f; }
+    void add_bytes(int ph, double b) { ctx_->phase_bytes[ph] += b; }
+    // call after the stream is synchronised
+    void collect() {
+        for (auto& r : recs_) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) ctx_->phase_ms[r.phase] += ms;
+            cudaEventDestroy(r.a);
+            cudaEventDestroy(r.b);
+        }
+        recs_.clear();
+    }
+
+  private:
+    struct Rec {
+        int phase;
+        cudaEvent_t a, b;
+    };
+    RomeGpuCtx* ctx_;
+    std::vector<Rec> recs_;
+};
+
+// round-to-nearest FP64 helpers used where the reference's operation order
+// must be reproduced exactly (no fused multiply-add)
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+constexpr double kPi = 3.14159265358979323846;  // src/macros.h:69
+
+}  // namespace rome

@@ -1,0 +1,174 @@
+// Context lifetime, projector upload and backprojector access (C ABI).
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+
+using namespace rome;
+
+extern "C" int rome_gpu_abi_version(void) { return ROME_GPU_ABI_VERSION; }
+
+extern "C" int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx** out) {
+    if (!out) return ROME_ERR_ARG;
+    *out = nullptr;
+    RomeGpuCtx* ctx = new RomeGpuCtx();
+    int rc = guarded(ctx, [&] {
+        int ndev = 0;
+        ROME_CUDA(cudaGetDeviceCount(&ndev));
+        ROME_REQUIRE(device >= 0 && device < ndev, "device %d out of range (%d devices)", device, ndev);
+        ctx->device = device;
+        ROME_CUDA(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        ROME_CUDA(cudaGetDeviceProperties(&prop, device));
+        if (prop.major < 10)
+            fail(ROME_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major,
+                 prop.minor);
+        if (cfg) {
+            ctx->precision = cfg->precision;
+            ctx->deterministic = cfg->deterministic;
+            ctx->profile = cfg->profile;
+        }
+        ROME_REQUIRE(ctx->precision >= ROME_PREC_FP32 && ctx->precision <= ROME_PREC_BF16X3, "bad precision %d",
+                     ctx->precision);
+        ROME_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+        // The 5000-entry sin/cos table of shiftImageInFourierTransform
+        // (src/image.h:1486-1512), evaluated with the host's libm so the
+        // device reads exactly the reference's table values.
+        const int nr = 5000;
+        std::vector<double2> tab(nr);
+        double sampling = 2 * kPi / (double)nr;
+        for (int i = 0; i < nr; i++) {
+            double xx = (double)i * sampling;
+            tab[i] = make_double2(cos(xx), sin(xx));
+        }
+        ctx->shift_sampling = sampling;
+        ROME_CUDA(cudaMalloc(&ctx->d_shift_tab, sizeof(double2) * nr));
+        ROME_CUDA(cudaMemcpy(ctx->d_shift_tab, tab.data(), sizeof(double2) * nr, cudaMemcpyHostToDevice));
+    });
+    if (rc != ROME_OK) {
+        fprintf(stderr, "rome_gpu_create: %s\n", ctx->last_error.c_str());
+        rome_gpu_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return ROME_OK;
+}
+
+extern "C" int rome_gpu_destroy(RomeGpuCtx* ctx) {
+    if (!ctx) return ROME_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& b : ctx->ws) b.release();
+    if (ctx->proj) cudaFree(ctx->proj);
+    if (ctx->bp_data) cudaFree(ctx->bp_data);
+    if (ctx->bp_weight) cudaFree(ctx->bp_weight);
+    if (ctx->d_shift_tab) cudaFree(ctx->d_shift_tab);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return ROME_OK;
+}
+
+extern "C" const char* rome_gpu_last_error(const RomeGpuCtx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->last_error.c_str();
+}
+
+extern "C" int rome_gpu_set_precision(RomeGpuCtx* ctx, int precision) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(precision >= ROME_PREC_FP32 && precision <= ROME_PREC_BF16X3, "bad precision %d", precision);
+        ctx->precision = precision;
+    });
+}
+
+extern "C" int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_classes, int ori_size, int pad_size,
+                                       int r_max, int padding_factor, const double* data) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(ref_dim == 2 || ref_dim == 3, "ref_dim must be 2 or 3");
+        ROME_REQUIRE(nr_classes > 0 && ori_size > 0 && pad_size > 0 && r_max >= 0 && data, "bad projector args");
+        ROME_REQUIRE(padding_factor == 2, "only padding_factor 2 (the map2d/map3d default) is supported");
+        ROME_REQUIRE(pad_size == 2 * (padding_factor * r_max + 1) + 1,
+                     "pad_size %d inconsistent with r_max %d (ProjectorBase::initialize)", pad_size, r_max);
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        long padF = pad_size / 2 + 1;
+        long vox = (ref_dim == 3 ? (long)pad_size : 1L) * pad_size * padF;
+        if (ctx->proj) cudaFree(ctx->proj);
+        if (ctx->bp_data) cudaFree(ctx->bp_data);
+        if (ctx->bp_weight) cudaFree(ctx->bp_weight);
+        ctx->proj = nullptr;
+        ctx->bp_data = nullptr;
+        ctx->bp_weight = nullptr;
+        ROME_CUDA(cudaMalloc(&ctx->proj, sizeof(double2) * vox * nr_classes));
+        ROME_CUDA(cudaMalloc(&ctx->bp_data, sizeof(double2) * vox * nr_classes));
+        ROME_CUDA(cudaMalloc(&ctx->bp_weight, sizeof(double) * vox * nr_classes));
+        ROME_CUDA(cudaMemcpyAsync(ctx->proj, data, sizeof(double2) * vox * nr_classes, cudaMemcpyHostToDevice,
+                                  ctx->stream));
+        ROME_CUDA(cudaMemsetAsync(ctx->bp_data, 0, sizeof(double2) * vox * nr_classes, ctx->stream));
+        ROME_CUDA(cudaMemsetAsync(ctx->bp_weight, 0, sizeof(double) * vox * nr_classes, ctx->stream));
+        ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->ref_dim = ref_dim;
+        ctx->nr_classes = nr_classes;
+        ctx->ori_size = ori_size;
+        ctx->pad_size = pad_size;
+        ctx->r_max = r_max;
+        ctx->padding = padding_factor;
+        ctx->vox = vox;
+    });
+}
+
+extern "C" int rome_gpu_get_backprojector(RomeGpuCtx* ctx, int iclass, double* data, double* weight) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->bp_data) fail(ROME_ERR_STATE, "no projectors/backprojectors set");
+        ROME_REQUIRE(iclass >= 0 && iclass < ctx->nr_classes, "iclass %d out of range", iclass);
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        if (data)
+            ROME_CUDA(cudaMemcpyAsync(data, ctx->bp_data + (long)iclass * ctx->vox, sizeof(double2) * ctx->vox,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        if (weight)
+            ROME_CUDA(cudaMemcpyAsync(weight, ctx->bp_weight + (long)iclass * ctx->vox, sizeof(double) * ctx->vox,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, const double* weight) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->bp_data) fail(ROME_ERR_STATE, "no projectors/backprojectors set");
+        ROME_REQUIRE(iclass >= 0 && iclass < ctx->nr_classes, "iclass %d out of range", iclass);
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        if (data)
+            ROME_CUDA(cudaMemcpyAsync(ctx->bp_data + (long)iclass * ctx->vox, data, sizeof(double2) * ctx->vox,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        if (weight)
+            ROME_CUDA(cudaMemcpyAsync(ctx->bp_weight + (long)iclass * ctx->vox, weight, sizeof(double) * ctx->vox,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+extern "C" int rome_gpu_get_timings(RomeGpuCtx* ctx, RomeGpuTimings* out) {
+    if (!ctx || !out) return ROME_ERR_ARG;
+    for (int q = 0; q < ROME_PHASE_COUNT; q++) {
+        out->ms[q] = ctx->phase_ms[q];
+        out->launches[q] = ctx->phase_launches[q];
+        out->flops[q] = ctx->phase_flops[q];
+        out->bytes[q] = ctx->phase_bytes[q];
+    }
+    out->total_launches = ctx->total_launches;
+    return ROME_OK;
+}
+
+extern "C" int rome_gpu_reset_timings(RomeGpuCtx* ctx) {
+    if (!ctx) return ROME_ERR_ARG;
+    for (int q = 0; q < ROME_PHASE_COUNT; q++) {
+        ctx->phase_ms[q] = 0;
+        ctx->phase_launches[q] = 0;
+        ctx->phase_flops[q] = 0;
+        ctx->phase_bytes[q] = 0;
+    }
+    ctx->total_launches = 0;
+    return ROME_OK;
+}

@@ -1,0 +1,440 @@
+// MAP2D E-step for one pool of particles on sm_100a.
+//
+// Replaces Map2dOptimizer_old::expectationSomeParticles
+// (src/map2d_optimizer.cpp:802-854) minus storeWeightedSums.  Per pass:
+//   prep      windowed image / CTF / Minvsigma2    (exp_model.cpp:935-1104)
+//   project   rotate2D of every class x psi         (reconstruct.cpp:823-958)
+//   shift     table-based phase shift + A operand   (image.h:1478-1575)
+//   diff2     cross term as a dense contraction, fused epilogue
+//             diff2 = (N_ij - 2 C_(it)j + S_it + highres_Xi2_i) / 2
+//                                                  (map2d_optimizer.cpp:907-1074)
+//   posterior FP64 weights, sum, argmax, significance selection
+//                                                  (map2d_optimizer.cpp:1077-1311)
+// then updateOtherParams (wsum kernel, :1417-1663) and backProjection
+// (slice accumulation + backrotate2D scatter, :1666-1873,
+// reconstruct.cpp:1353-1500).
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "estep_kernels.cuh"
+#include "gemm_simt.cuh"
+#include "gemm_tc.cuh"
+
+using namespace rome;
+
+namespace {
+
+struct PassGeom {
+    int cs, F, csF;          // image size of the pass, half-plane pixels, row length
+    int nor, notr, T, nrot;  // over-rotations, over-translations, T = ntr*notr, nrot = npsi*nor
+    int J;                   // orientations K*nrot
+    long X;                  // hypotheses per particle J*T
+    int Kact, Kp;            // active pixels, padded GEMM depth (2*Kact rounded to 64)
+    int Kq;                  // padded depth of the norm GEMM (Kact rounded to 16)
+    int my_r_max;
+};
+
+template <typename T>
+T* upload(RomeGpuCtx* ctx, Slot s, const T* host, size_t n) {
+    T* d = ctx->ws[s].as<T>(n);
+    if (n) ROME_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
+
+// Euler_angles2matrix(0, 0, psi) (src/math.cpp:86-115); the projector uses
+// the transpose times the padding factor (src/reconstruct.cpp:860-870).
+void rot2d_inv(double psi_deg, int padding, double out[4]) {
+    const double rome_pi = 3.14159265358979323846;
+    double alpha = 0 * rome_pi / 180., beta = 0 * rome_pi / 180., gamma = psi_deg * rome_pi / 180.;
+    double ca = cos(alpha), cb = cos(beta), cg = cos(gamma);
+    double sa = sin(alpha), sb = sin(beta), sg = sin(gamma);
+    double cc = cb * ca, cs = cb * sa;
+    double A00 = cg * cc - sg * sa, A01 = cg * cs + sg * ca;
+    double A10 = -sg * cc - cg * sa, A11 = -sg * cs + cg * ca;
+    out[0] = A00 * (double)padding;  // Ainv[0][0] = A[0][0]
+    out[1] = A10 * (double)padding;  // Ainv[0][1] = A[1][0]
+    out[2] = A01 * (double)padding;  // Ainv[1][0] = A[0][1]
+    out[3] = A11 * (double)padding;  // Ainv[1][1] = A[1][1]
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2dPoolOut* out) {
+    if (!ctx || !in || !out) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->proj || ctx->ref_dim != 2) fail(ROME_ERR_STATE, "2D projectors not set (rome_gpu_set_projectors)");
+        const int P = in->nr_images, K = in->nr_classes, ori = in->ori_size, cur = in->current_size;
+        const int npsi = in->nr_psi, ntr = in->nr_trans, G = in->nr_groups, oriF = ori / 2 + 1;
+        ROME_REQUIRE(P > 0 && K == ctx->nr_classes && ori == ctx->ori_size, "pool/projector mismatch");
+        ROME_REQUIRE(cur > 0 && cur <= ori && cur % 2 == 0, "bad current_size %d", cur);
+        ROME_REQUIRE(in->adaptive_oversampling >= 0 && in->adaptive_oversampling <= 1,
+                     "adaptive_oversampling %d not supported (0 or 1)", in->adaptive_oversampling);
+        ROME_REQUIRE(in->iclass_min >= 0 && in->iclass_max < K && in->iclass_min <= in->iclass_max, "bad class range");
+        ROME_REQUIRE(ctx->r_max == std::min(cur / 2, ori / 2),
+                     "projector r_max %d does not match current_size %d", ctx->r_max, cur);
+        ROME_REQUIRE(in->Fimg_real && in->Fimg_imag && in->Fimg_nomask_real && in->Fimg_nomask_imag && in->Fctf,
+                     "missing particle images");
+        ROME_REQUIRE(npsi > 0 && ntr > 0 && G > 0, "empty sampling");
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const int npass = in->adaptive_oversampling > 0 ? 2 : 1;
+        const int curF2 = cur * (cur / 2 + 1);
+        const long ncoarse = (long)K * npsi * ntr;
+        const bool apply_ctf = in->do_ctf_correction && in->refs_are_ctf_corrected;
+        Profiler prof(ctx);
+
+        // ---- particle data at the fine size ----
+        const double *dFr, *dFi, *dFnr, *dFni, *dCtf;
+        if (in->inputs_on_device) {
+            dFr = in->Fimg_real;
+            dFi = in->Fimg_imag;
+            dFnr = in->Fimg_nomask_real;
+            dFni = in->Fimg_nomask_imag;
+            dCtf = in->Fctf;
+        } else {
+            double* base = ctx->ws[S_TMP0].as<double>((size_t)P * curF2 * 5);
+            const double* src[5] = {in->Fimg_real, in->Fimg_imag, in->Fimg_nomask_real, in->Fimg_nomask_imag,
+                                    in->Fctf};
+            for (int q = 0; q < 5; q++)
+                ROME_CUDA(cudaMemcpyAsync(base + (size_t)q * P * curF2, src[q], sizeof(double) * P * curF2,
+                                          cudaMemcpyHostToDevice, st));
+            dFr = base;
+            dFi = base + (size_t)P * curF2;
+            dFnr = base + (size_t)2 * P * curF2;
+            dFni = base + (size_t)3 * P * curF2;
+            dCtf = base + (size_t)4 * P * curF2;
+        }
+        double* dSig2 = upload(ctx, S_SIG2, in->sigma2_noise, (size_t)G * oriF);
+        int* dGroup = upload(ctx, S_GROUP, in->group, (size_t)P);
+        double* dXi2 = upload(ctx, S_XI2, in->highres_Xi2, (size_t)P);
+        // per-class model values: pdf_direction, prior offsets
+        std::vector<double> hcls((size_t)3 * K);
+        for (int k = 0; k < K; k++) {
+            hcls[k] = in->pdf_direction[k];
+            hcls[K + k] = in->prior_offsetx_class[k];
+            hcls[2 * K + k] = in->prior_offsety_class[k];
+        }
+        double* dCls = upload(ctx, S_PDIR, hcls.data(), hcls.size());
+        double* dPdir = dCls;
+        std::vector<double2> hoff(P);
+        for (int i = 0; i < P; i++) hoff[i] = make_double2(in->old_offsetx[i], in->old_offsety[i]);
+        double2* dOld = upload(ctx, S_OLDOFF, hoff.data(), hoff.size());
+        std::vector<double2> htc(ntr);
+        for (int t = 0; t < ntr; t++) htc[t] = make_double2(in->trans_x[t], in->trans_y[t]);
+        double2* dTrC = upload(ctx, S_TMP1, htc.data(), htc.size());
+        // offset prior per particle, class and coarse translation
+        double* dPoff = ctx->ws[S_POFF].as<double>((size_t)P * K * ntr);
+        prof.begin(ROME_PHASE_PREP);
+        pdf_offset_kernel<<<P, 128, 0, st>>>(P, K, ntr, dOld, dTrC, dCls + K, dCls + 2 * K, in->sigma2_offset, dPoff);
+        prof.launched(ROME_PHASE_PREP);
+        prof.end(ROME_PHASE_PREP);
+        std::vector<int> hclass_ok(K);
+        for (int k = 0; k < K; k++)
+            hclass_ok[k] = (k >= in->iclass_min && k <= in->iclass_max && in->pdf_class[k] > 0. &&
+                            in->pdf_direction[k] > 0.);
+
+        double* dPart = ctx->ws[S_PART].as<double>((size_t)P * 8);  // min, sum, sig, thr, maxw, dcut
+        int* dPartI = ctx->ws[S_PARTI].as<int>((size_t)P * 8);     // best e, nr_sign, overflow, b_low
+        char* dMcoarse = ctx->ws[S_MCOARSE].as<char>((size_t)P * ncoarse);
+        char* dRotSig = ctx->ws[S_ROTSIG].as<char>((size_t)K * npsi);
+
+        std::vector<double> h_min(P), h_sum(P), h_sig(P), h_nsig(P);
+        PassGeom g{};
+        double2* dFimg = nullptr;
+        double* dLctf = nullptr;
+        double* dMinv = nullptr;
+        double2* dProj = nullptr;
+        float* dDiff2 = nullptr;
+        int* dActIdx = nullptr;
+        int* dAct = nullptr;
+        double4* dRot = nullptr;
+        double2* dShift = nullptr;
+        int* dJvalid = nullptr;
+
+        for (int ipass = 0; ipass < npass; ipass++) {
+            const int cs = (ipass == 0 && in->adaptive_oversampling > 0) ? in->coarse_size : cur;
+            const int over = ipass == 0 ? 0 : in->adaptive_oversampling;
+            ROME_REQUIRE(cs > 0 && cs <= cur && cs % 2 == 0, "bad coarse_size %d", cs);
+            g.cs = cs;
+            g.csF = cs / 2 + 1;
+            g.F = cs * g.csF;
+            g.nor = 1 << over;
+            g.notr = 1 << (2 * over);
+            g.T = ntr * g.notr;
+            g.nrot = npsi * g.nor;
+            g.J = K * g.nrot;
+            g.X = (long)g.J * g.T;
+            g.my_r_max = std::min(ctx->r_max, cs / 2);
+            ROME_REQUIRE(in->over_psi[ipass] && in->over_trans_x[ipass] && in->over_trans_y[ipass],
+                         "missing sampling tables for pass %d", ipass);
+            const int* Mresol = ipass == 0 ? in->Mresol_coarse : in->Mresol_fine;
+            ROME_REQUIRE(Mresol, "missing Mresol for pass %d", ipass);
+
+            // active pixels: the support of rotate2D, r^2 <= my_r_max^2 (reconstruct.cpp:866-891)
+            std::vector<int> act, actidx(g.F, -1);
+            for (int row = 0; row < cs; row++) {
+                int y;
+                if (row <= g.my_r_max) y = row;
+                else if (row >= cs - g.my_r_max) y = row - cs;
+                else continue;
+                for (int x = 0; x <= g.my_r_max; x++)
+                    if (x * x + y * y <= g.my_r_max * g.my_r_max) {
+                        actidx[row * g.csF + x] = (int)act.size();
+                        act.push_back(row * g.csF + x);
+                    }
+            }
+            g.Kact = (int)act.size();
+            g.Kp = ((2 * g.Kact + 63) / 64) * 64;
+            g.Kq = ((g.Kact + 15) / 16) * 16;
+            dAct = upload(ctx, S_ACT, act.data(), act.size());
+            dActIdx = upload(ctx, S_ACTIDX, actidx.data(), actidx.size());
+            int* dClassOk = ctx->ws[S_JVALID].as<int>((size_t)K + g.J);
+            ROME_CUDA(cudaMemcpyAsync(dClassOk, hclass_ok.data(), sizeof(int) * K, cudaMemcpyHostToDevice, st));
+            dJvalid = dClassOk + K;
+            int* dMres = upload(ctx, S_MRES, Mresol, (size_t)g.F);
+
+            // rotation matrices and translations of this pass
+            std::vector<double4> hrot(g.J);
+            for (int k = 0; k < K; k++)
+                for (int r = 0; r < g.nrot; r++) {
+                    double m[4];
+                    rot2d_inv(in->over_psi[ipass][r], ctx->padding, m);
+                    hrot[(size_t)k * g.nrot + r] = make_double4(m[0], m[1], m[2], m[3]);
+                }
+            dRot = upload(ctx, S_ROTM, hrot.data(), hrot.size());
+            std::vector<double2> hsh(g.T);
+            for (int t = 0; t < g.T; t++)
+                hsh[t] = make_double2((double)in->over_trans_x[ipass][t] / (-ori),
+                                      (double)in->over_trans_y[ipass][t] / (-ori));
+            dShift = upload(ctx, S_SHIFT, hsh.data(), hsh.size());
+
+            // ---- prep: window to cs, local CTF, Minvsigma2 ----
+            dFimg = ctx->ws[S_FIMG].as<double2>((size_t)P * g.F);
+            dLctf = ctx->ws[S_CTF].as<double>((size_t)P * g.F);
+            dMinv = ctx->ws[S_MINV].as<double>((size_t)P * g.F);
+            prof.begin(ROME_PHASE_PREP);
+            prep_particles_kernel<<<P, 256, 0, st>>>(P, cur, cs, dFr, dFi, dCtf, dMres, dSig2, dGroup, oriF,
+                                                      in->sigma2_fudge, dFimg, dLctf, dMinv);
+            prof.launched(ROME_PHASE_PREP);
+            prof.end(ROME_PHASE_PREP);
+
+            // ---- orientation validity and projections (getReferenceAllOrientations) ----
+            const bool tc = ctx->precision != ROME_PREC_FP32;
+            dProj = ctx->ws[S_PROJ].as<double2>((size_t)g.J * g.Kact);
+            float* dQ = ctx->ws[S_Q].as<float>((size_t)g.J * g.Kq);
+            void* dB = ctx->ws[S_B].get((size_t)g.J * g.Kp * 4);
+            prof.begin(ROME_PHASE_PROJECT);
+            {
+                const int nkp = K * npsi;
+                rot_sig_kernel<<<(nkp + 255) / 256, 256, 0, st>>>(nkp, P, ntr, ncoarse, ipass > 0 ? dMcoarse : nullptr,
+                                                                   dRotSig);
+                prof.launched(ROME_PHASE_PROJECT);
+                jvalid_kernel<<<(g.J + 255) / 256, 256, 0, st>>>(g.J, g.nrot, g.nor, dClassOk, dRotSig, dJvalid);
+                prof.launched(ROME_PHASE_PROJECT);
+            }
+            project2d_kernel<<<g.J, 256, 0, st>>>(g.J, g.Kact, g.Kp, g.Kq, cs, g.csF, g.my_r_max, ctx->pad_size,
+                                                  ctx->pad_size / 2 + 1, g.nrot, ctx->proj, ctx->vox, dRot, dAct,
+                                                  dJvalid, dProj, dQ, dB, ctx->precision);
+            prof.launched(ROME_PHASE_PROJECT);
+            prof.end(ROME_PHASE_PROJECT);
+
+            // ---- shifted images -> A operand, S term ----
+            const long M = (long)P * g.T;
+            void* dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+            float* dS = ctx->ws[S_S].as<float>((size_t)M);
+            float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+            prof.begin(ROME_PHASE_SHIFT);
+            shift_operand_kernel<<<dim3(g.T, P), 256, 0, st>>>(P, g.T, g.F, g.csF, cs, g.Kact, g.Kp, dFimg, dLctf,
+                                                              dMinv, apply_ctf ? 1 : 0, dAct, dShift,
+                                                              ctx->d_shift_tab, ctx->shift_sampling, dA, dS,
+                                                              ctx->precision);
+            prof.launched(ROME_PHASE_SHIFT);
+            w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+            prof.launched(ROME_PHASE_SHIFT);
+            prof.end(ROME_PHASE_SHIFT);
+
+            // ---- norm term N[i][j] = sum_n Minv c^2 |P_j|^2 (FP32 CUDA cores) ----
+            float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * g.J);
+            prof.begin(ROME_PHASE_NORM_GEMM);
+            sgemm_tn(st, P, g.J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, g.J});
+            prof.launched(ROME_PHASE_NORM_GEMM);
+            prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * g.J * g.Kact);
+            prof.end(ROME_PHASE_NORM_GEMM);
+
+            // ---- cross term + fused diff2 epilogue ----
+            dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * g.X);
+            Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJvalid, g.T, g.J, g.X, g.notr, g.nor, ntr, ncoarse,
+                         ipass > 0 ? dMcoarse : nullptr};
+            prof.begin(ROME_PHASE_CROSS_GEMM);
+            if (!tc) {
+                sgemm_tn(st, (int)M, g.J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
+            } else {
+                tc_diff2_gemm(st, (int)M, g.J, g.Kp, dA, dB, ctx->precision, epi);
+            }
+            prof.launched(ROME_PHASE_CROSS_GEMM);
+            // algorithmic work: 4 flops per active complex coefficient per (image, translation, orientation)
+            prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * g.J * g.Kact);
+            prof.end(ROME_PHASE_CROSS_GEMM);
+
+            // ---- posterior: min, FP64 weights, sum, argmax, significance ----
+            double* dW = nullptr;
+            if (out->weight[ipass]) dW = ctx->ws[S_WCHK].as<double>((size_t)P * g.X);
+            prof.begin(ROME_PHASE_POSTERIOR);
+            int nl = post_select(ctx, st, P, g.X, g.T, g.notr, g.nor, npsi, ntr, dDiff2, dPdir, dPoff, K,
+                                 in->adaptive_fraction, dPart, dPartI, dW);
+            prof.launched(ROME_PHASE_POSTERIOR, nl);
+            if (ipass == 0 && (npass > 1 || out->Mcoarse_significant)) {
+                mcoarse_kernel<<<P, 256, 0, st>>>(P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, dDiff2, dPdir, dPoff,
+                                                  dPart, dMcoarse);
+                prof.launched(ROME_PHASE_POSTERIOR);
+            }
+            prof.end(ROME_PHASE_POSTERIOR);
+
+            // ---- checkpoints and per-particle results of this pass ----
+            std::vector<double> hpart((size_t)P * 8);
+            std::vector<int> hparti((size_t)P * 8);
+            ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * P * 8, cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaMemcpyAsync(hparti.data(), dPartI, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
+            if (out->diff2[ipass]) {
+                std::vector<float> hd((size_t)P * g.X);
+                ROME_CUDA(cudaMemcpyAsync(hd.data(), dDiff2, sizeof(float) * hd.size(), cudaMemcpyDeviceToHost, st));
+                ROME_CUDA(cudaStreamSynchronize(st));
+                for (size_t q = 0; q < hd.size(); q++)
+                    out->diff2[ipass][q] = hd[q] < INFINITY ? (double)hd[q] : (double)INT_MIN;
+            }
+            if (out->weight[ipass])
+                ROME_CUDA(cudaMemcpyAsync(out->weight[ipass], dW, sizeof(double) * P * g.X, cudaMemcpyDeviceToHost,
+                                          st));
+            if (ipass == 0 && out->Mcoarse_significant)
+                ROME_CUDA(cudaMemcpyAsync(out->Mcoarse_significant, dMcoarse, (size_t)P * ncoarse,
+                                          cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaStreamSynchronize(st));
+            for (int i = 0; i < P; i++) {
+                double mn = hpart[i * 8 + 0], sw = hpart[i * 8 + 1], sig = hpart[i * 8 + 2], mx = hpart[i * 8 + 4];
+                int best = hparti[i * 8 + 0], nsig = hparti[i * 8 + 1];
+                if (ipass == 0 && nsig == 0)
+                    fail(ROME_ERR_NUMERIC, "my_nr_significant_coarse_samples == 0 for particle %d", i);
+                h_min[i] = mn;
+                h_sum[i] = sw;
+                h_sig[i] = sig;
+                if (ipass == 0) h_nsig[i] = nsig;
+                // convertSquaredDifferencesToWeights metadata (map2d_optimizer.cpp:1199-1216)
+                long e = best;
+                int j = (int)(e / g.T), t = (int)(e % g.T);
+                int r = j % g.nrot, k = j / g.nrot;
+                int itr = t / g.notr, iotr = t % g.notr;
+                if (out->pmax) out->pmax[i] = mx / sw;
+                if (out->cls) out->cls[i] = k + 1;
+                if (out->psi) {
+                    double psi = in->over_psi[ipass][r];
+                    if (psi > 180.) psi -= 360.;
+                    if (psi < -180.) psi += 360.;
+                    out->psi[i] = psi;
+                }
+                if (out->xoff) out->xoff[i] = in->old_offsetx[i] + in->over_trans_x[ipass][itr * g.notr + iotr];
+                if (out->yoff) out->yoff[i] = in->old_offsety[i] + in->over_trans_y[ipass][itr * g.notr + iotr];
+            }
+        }
+
+        // ---- updateOtherParams (last pass, current_size) ----
+        const int lp = npass - 1;
+        std::vector<double2> htr(g.T);
+        for (int t = 0; t < g.T; t++) htr[t] = make_double2(in->over_trans_x[lp][t], in->over_trans_y[lp][t]);
+        double2* dTr = upload(ctx, S_TRANS, htr.data(), htr.size());
+        int* dMresF = upload(ctx, S_MRES, in->Mresol_fine, (size_t)g.F);
+        // accumulators: wsum_sigma2_noise [G][oriF], norm_corr [P];
+        // class sums [0] pdf_class [1] pdf_direction [2] prior x [3] prior y [4] sigma2_offset, then groups
+        double* dWsn = ctx->ws[S_WSN].as<double>((size_t)G * oriF + P);
+        double* dNormCorr = dWsn + (size_t)G * oriF;
+        double* dWk = ctx->ws[S_WSUMK].as<double>((size_t)5 * K + G + 1);
+        ROME_CUDA(cudaMemsetAsync(dWsn, 0, sizeof(double) * ((size_t)G * oriF + P), st));
+        ROME_CUDA(cudaMemsetAsync(dWk, 0, sizeof(double) * ((size_t)5 * K + G + 1), st));
+        {
+            const int NT = 256, PIX = 8;
+            int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
+            prof.begin(ROME_PHASE_WSUM);
+            wsum_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
+                P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, g.F, g.csF, cur, oriF, dDiff2, dPdir, dPoff, dPart, dJvalid,
+                dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx, g.Kact, dShift, ctx->d_shift_tab, ctx->shift_sampling,
+                dMresF, dGroup, dOld, dTr, (const double2*)nullptr, dCls + K, dCls + 2 * K, dWsn, dNormCorr, dWk);
+            prof.launched(ROME_PHASE_WSUM);
+            prof.end(ROME_PHASE_WSUM);
+        }
+
+        // ---- backProjection ----
+        {
+            double2* dFnm = ctx->ws[S_FNOMASK].as<double2>((size_t)P * g.F);
+            double* dMctf2 = dMinv;  // reused in place: becomes ctf^2 * Minvsigma2
+            prof.begin(ROME_PHASE_BACKPROJECT);
+            bp_prep_kernel<<<P, 256, 0, st>>>(P, g.F, dFnr, dFni, dLctf, dMinv, dSig2, dGroup, oriF,
+                                              in->sigma2_fudge, in->do_map, in->do_ctf_correction, dFnm, dMctf2);
+            prof.launched(ROME_PHASE_BACKPROJECT);
+            const int NT = 256, PIX = 8;
+            int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
+            bp_kernel<NT, PIX><<<dim3(nsplit, g.J), NT, 0, st>>>(
+                P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, g.F, g.csF, cur, dDiff2, dPdir, dPoff, dPart, dJvalid, dFnm,
+                dMctf2, dShift, ctx->d_shift_tab, ctx->shift_sampling, dRot, ctx->r_max, ctx->pad_size,
+                ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
+            prof.launched(ROME_PHASE_BACKPROJECT);
+            prof.end(ROME_PHASE_BACKPROJECT);
+        }
+
+        // ---- outputs ----
+        std::vector<double> hwsn((size_t)G * oriF + P), hwk((size_t)5 * K + G + 1);
+        ROME_CUDA(cudaMemcpyAsync(hwsn.data(), dWsn, sizeof(double) * hwsn.size(), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaMemcpyAsync(hwk.data(), dWk, sizeof(double) * hwk.size(), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        prof.collect();
+        for (size_t q = 0; q < (size_t)G * oriF; q++) out->wsum_sigma2_noise[q] += hwsn[q];
+        for (int i = 0; i < P; i++) {
+            if (out->wsum_norm_correction) out->wsum_norm_correction[i] = hwsn[(size_t)G * oriF + i];
+            if (out->min_diff2) out->min_diff2[i] = h_min[i];
+            if (out->sum_weight) out->sum_weight[i] = h_sum[i];
+            if (out->significant_weight) out->significant_weight[i] = h_sig[i];
+            if (out->nr_sign) out->nr_sign[i] = h_nsig[i];
+        }
+        for (int k = 0; k < K; k++) {
+            out->wsum_pdf_class[k] += hwk[0 * K + k];
+            out->wsum_pdf_direction[k] += hwk[1 * K + k];
+            out->wsum_prior_offsetx_class[k] += hwk[2 * K + k];
+            out->wsum_prior_offsety_class[k] += hwk[3 * K + k];
+        }
+        for (int q = 0; q < G; q++) out->wsum_sumw_group[q] += hwk[5 * K + q];
+        for (int k = 0; k < K; k++) out->wsum_sigma2_offset[0] += hwk[4 * K + k];
+        for (int i = 0; i < P; i++)
+            if (h_sum[i] == 0) fail(ROME_ERR_NUMERIC, "exp_sum_weight[%d] == 0", i);
+    });
+}
+
+extern "C" int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, const double* weights,
+                                           const double* sum_weight, double adaptive_fraction,
+                                           double* significant_weight, double* nr_significant) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(n > 0 && len > 0 && weights && sum_weight && significant_weight && nr_significant,
+                     "bad arguments");
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        double* dW = ctx->ws[S_WCHK].as<double>((size_t)n * len);
+        ROME_CUDA(cudaMemcpyAsync(dW, weights, sizeof(double) * n * len, cudaMemcpyHostToDevice, st));
+        double* dPart = ctx->ws[S_PART].as<double>((size_t)n * 8);
+        int* dPartI = ctx->ws[S_PARTI].as<int>((size_t)n * 8);
+        std::vector<double> hp((size_t)n * 8, 0.0);
+        for (int i = 0; i < n; i++) hp[(size_t)i * 8 + 1] = sum_weight[i];
+        ROME_CUDA(cudaMemcpyAsync(dPart, hp.data(), sizeof(double) * n * 8, cudaMemcpyHostToDevice, st));
+        select_given_weights(ctx, st, n, len, dW, adaptive_fraction, dPart, dPartI);
+        std::vector<double> hpart((size_t)n * 8);
+        std::vector<int> hparti((size_t)n * 8);
+        ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * n * 8, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaMemcpyAsync(hparti.data(), dPartI, sizeof(int) * n * 8, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        for (int i = 0; i < n; i++) {
+            significant_weight[i] = hpart[(size_t)i * 8 + 2];
+            nr_significant[i] = hparti[(size_t)i * 8 + 1];
+        }
+    });
+}

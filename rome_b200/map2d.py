@@ -154,6 +154,20 @@ def alloc_outputs(p: Map2dPool, checkpoints: bool = False):
     return s, o
 
 
+DEVICE_FIELDS = ["Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf"]
+
+
+@dataclasses.dataclass
+class StagedPool:
+    """A pool whose particle images were copied to the device (GpuContext.stage_pool)."""
+    pool: Map2dPool
+    dev: dict
+
+    @property
+    def nr_images(self) -> int:
+        return self.pool.nr_images
+
+
 class RomeError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"rome_gpu error {code}: {msg}")
@@ -163,9 +177,10 @@ class RomeError(RuntimeError):
 class GpuContext:
     """One device context of librome_b200 (``rome_gpu_create``)."""
 
-    def __init__(self, device: int = 0, precision: str = "fp32", deterministic: bool = False):
+    def __init__(self, device: int = 0, precision: str = "fp32", deterministic: bool = False, profile: bool = False):
         self.lib = abi.load_library()
-        cfg = abi.RomeGpuConfig(abi.PRECISIONS[precision], int(deterministic), 0)
+        self.device = device
+        cfg = abi.RomeGpuConfig(abi.PRECISIONS[precision], int(deterministic), 0, int(profile))
         h = C.c_void_p()
         rc = self.lib.rome_gpu_create(device, C.byref(cfg), C.byref(h))
         if rc != 0:
@@ -210,11 +225,49 @@ class GpuContext:
     def set_backprojector(self, iclass: int, data: np.ndarray, weight: np.ndarray):
         self._check(self.lib.rome_gpu_set_backprojector(self.h, iclass, abi.dptr(_f64(data)), abi.dptr(_f64(weight))))
 
-    def map2d_estep_pool(self, p: Map2dPool, checkpoints: bool = False) -> Dict[str, np.ndarray]:
-        s, keep = pack_pool(p)
-        so, o = alloc_outputs(p, checkpoints)
+    def map2d_estep_pool(self, p, checkpoints: bool = False) -> Dict[str, np.ndarray]:
+        """E-step of one pool.  `p` is a Map2dPool (host arrays) or a
+        StagedPool whose particle images already live on the device."""
+        if isinstance(p, StagedPool):
+            s, keep = pack_pool(p.pool)
+            for name, t in p.dev.items():
+                setattr(s, name, C.cast(C.c_void_p(t.data_ptr()), abi._DP))
+            s.inputs_on_device = 1
+            so, o = alloc_outputs(p.pool, checkpoints)
+        else:
+            s, keep = pack_pool(p)
+            so, o = alloc_outputs(p, checkpoints)
         self._check(self.lib.rome_gpu_map2d_estep_pool(self.h, C.byref(s), C.byref(so)))
         return o
+
+    def stage_pool(self, p: Map2dPool) -> "StagedPool":
+        """Copy the pool's particle images to the device once (torch owns the memory)."""
+        import torch
+        dev = {}
+        for name in DEVICE_FIELDS:
+            dev[name] = torch.from_numpy(_f64(getattr(p, name))).to(f"cuda:{self.device}")
+        torch.cuda.synchronize(self.device)
+        return StagedPool(p, dev)
+
+    @staticmethod
+    def h2d_bytes(p: Map2dPool) -> int:
+        return sum(int(_f64(getattr(p, n)).nbytes) for n in DEVICE_FIELDS) + p.nr_images * (3 * 8 + 4)
+
+    @staticmethod
+    def d2h_bytes(p: Map2dPool) -> int:
+        P, K, G = p.nr_images, p.nr_classes, p.nr_groups
+        return P * (9 * 8 + 4) + 8 * (G * (p.ori_size // 2 + 1) + 4 * K + G + 1)
+
+    def get_timings(self) -> Dict[str, dict]:
+        t = abi.RomeGpuTimings()
+        self._check(self.lib.rome_gpu_get_timings(self.h, C.byref(t)))
+        out = {name: {"ms": t.ms[q], "launches": t.launches[q], "flops": t.flops[q], "bytes": t.bytes[q]}
+               for q, name in enumerate(abi.PHASES)}
+        out["total_launches"] = t.total_launches
+        return out
+
+    def reset_timings(self):
+        self._check(self.lib.rome_gpu_reset_timings(self.h))
 
     def select_significant(self, weights: np.ndarray, sum_weight: np.ndarray, adaptive_fraction: float):
         w = _f64(weights)

@@ -1,0 +1,244 @@
+"""Synthetic MAP2D pools at the benchmark configurations.
+
+Builds everything ``rome_gpu_map2d_estep_pool`` consumes without touching
+disk: class references (random Gaussian-blob templates), their padded
+Fourier projector maps, particles in Fourier space (a rotated, shifted,
+CTF-modulated projection plus white complex noise at a target SNR), the
+sampling tables and the model state.  The numerics follow the reference's
+definitions (cited per function) so the hypotheses, layouts and posterior
+shapes match a real iteration; values are seeded synthetic data.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+from .map2d import Map2dPool
+from .synthetic import ctf_image
+
+
+@dataclasses.dataclass
+class Map2dWorkload:
+    n_particles: int = 1000
+    ori_size: int = 64
+    current_size: Optional[int] = None  # default: ori_size
+    n_classes: int = 10
+    n_blobs: int = 20
+    blob_sigma: tuple = (2.0, 6.0)
+    psi_step: float = 10.0
+    offset_range: int = 5
+    offset_step: int = 1
+    max_shift: float = 4.0
+    pixel: float = 2.0
+    snr: float = 0.05
+    defocus: tuple = (10000.0, 30000.0)
+    seed: int = 1
+    random_perturbation: float = 0.0  # sampler perturbation in units of the step
+
+
+def grid_templates(rng, ori, K, n_blobs, sig):
+    c = np.arange(ori) - ori // 2
+    yy, xx = np.meshgrid(c, c, indexing="ij")
+    refs = np.zeros((K, ori, ori))
+    for k in range(K):
+        r = 0.3 * ori * np.sqrt(rng.uniform(0, 1, n_blobs))
+        t = rng.uniform(0, 2 * np.pi, n_blobs)
+        s = rng.uniform(sig[0], sig[1], n_blobs)
+        a = rng.uniform(0.5, 1.0, n_blobs)
+        for q in range(n_blobs):
+            refs[k] += a[q] * np.exp(-((xx - r[q] * np.cos(t[q])) ** 2 + (yy - r[q] * np.sin(t[q])) ** 2) / (2 * s[q] ** 2))
+    return refs
+
+
+def projector_map_2d(ref: np.ndarray, current_size: int, padding: int = 2):
+    """MyProjector::computeFourierTransformMap for a 2D reference
+    (src/reconstruct.cpp:106-223): gridding correction, zero padding by 2,
+    centred FFT normalised by the padded size, scaled by padding^2 and
+    windowed to r_max.  Returns (data [pad][pad/2+1][2], r_max, pad_size)."""
+    ori = ref.shape[0]
+    r_max = min(current_size // 2, ori // 2)
+    pad_size = 2 * (padding * r_max + 1) + 1
+    padF = pad_size // 2 + 1
+    # griddingCorrect (reconstruct.cpp:61-103): divide by sinc^2
+    c = np.arange(ori) - ori // 2
+    yy, xx = np.meshgrid(c, c, indexing="ij")
+    r = np.sqrt(xx * xx + yy * yy)
+    rval = r / (ori * padding)
+    sinc = np.where(r > 0, np.sin(np.pi * rval) / np.where(r > 0, np.pi * rval, 1.0), 1.0)
+    vol = ref / (sinc * sinc)
+    P = padding * ori
+    Mpad = np.zeros((P, P))
+    o = P // 2 - ori // 2
+    Mpad[o:o + ori, o:o + ori] = vol
+    F = np.fft.rfft2(np.fft.ifftshift(Mpad)) / (P * P) * (padding * padding)
+    data = np.zeros((pad_size, padF, 2))
+    hP = P // 2 + 1
+    max_r2 = (r_max * padding) ** 2
+    for i in range(P):
+        ip = i if i < hP else i - P
+        jp = np.arange(hP)
+        ok = ip * ip + jp * jp <= max_r2
+        jj = jp[ok]
+        y = ip + pad_size // 2
+        data[y, jj, 0] = F[i, jj].real
+        data[y, jj, 1] = F[i, jj].imag
+    return data, r_max, pad_size
+
+
+def rotate2d_np(data: np.ndarray, r_max: int, psi_deg: np.ndarray, size: int, padding: int = 2) -> np.ndarray:
+    """MyProjector::rotate2D (src/reconstruct.cpp:823-958) for many angles,
+    vectorised; returns complex [n][size][size/2+1]."""
+    pad = data.shape[0]
+    Fs = size // 2 + 1
+    my_r = min(r_max, size // 2)
+    rows = np.arange(size)
+    yv = np.where(rows <= my_r, rows, rows - size)
+    rowok = (rows <= my_r) | (rows >= size - my_r)
+    yy, xx = np.meshgrid(yv, np.arange(Fs), indexing="ij")
+    ok = rowok[:, None] & (xx <= my_r) & (xx * xx + yy * yy <= my_r * my_r)
+    ys, xs = yy[ok].astype(np.float64), xx[ok].astype(np.float64)
+    psi = np.deg2rad(np.atleast_1d(psi_deg))[:, None]
+    cg, sg = np.cos(psi), np.sin(psi)
+    xp = (cg * xs + -sg * ys) * padding
+    yp = (sg * xs + cg * ys) * padding
+    neg = xp < 0
+    xp = np.where(neg, -xp, xp)
+    yp = np.where(neg, -yp, yp)
+    x0 = np.floor(xp).astype(np.int64)
+    fx = xp - x0
+    y0 = np.floor(yp).astype(np.int64)
+    fy = yp - y0
+    y0 = y0 + pad // 2
+    cplx = data[..., 0] + 1j * data[..., 1]
+    d00, d01 = cplx[y0, x0], cplx[y0, x0 + 1]
+    d10, d11 = cplx[y0 + 1, x0], cplx[y0 + 1, x0 + 1]
+    dx0 = d00 + (d01 - d00) * fx
+    dx1 = d10 + (d11 - d10) * fx
+    v = dx0 + (dx1 - dx0) * fy
+    v = np.where(neg, np.conj(v), v)
+    out = np.zeros((psi.shape[0], size, Fs), np.complex128)
+    out[:, ok] = v
+    return out
+
+
+def mresol(size: int) -> np.ndarray:
+    """Mresol_fine / Mresol_coarse (src/map_model.cpp:540-575)."""
+    Fs = size // 2 + 1
+    i = np.arange(size)
+    ip = np.where(i < Fs, i, i - size)
+    jp = np.arange(Fs)
+    ires = np.round(np.sqrt(ip[:, None] ** 2 + jp[None, :] ** 2)).astype(np.int32)
+    bad = (ires >= Fs) | ((jp[None, :] == 0) & (ip[:, None] < 0))
+    return np.where(bad, -1, ires).astype(np.int32).reshape(-1)
+
+
+def translations(offset_range: int, offset_step: int):
+    """HealpixSampler::setTranslations (src/sampling.cpp:121-172)."""
+    maxr = math.ceil(offset_range / offset_step)
+    tx, ty = [], []
+    for ix in range(-maxr, maxr + 1):
+        for iy in range(-maxr, maxr + 1):
+            x, y = ix * offset_step, iy * offset_step
+            if x * x + y * y <= offset_range * offset_range:
+                tx.append(float(x))
+                ty.append(float(y))
+    return np.array(tx), np.array(ty)
+
+
+def psi_angles(psi_step: float):
+    """HealpixSampler::setOrientations, 2D in-plane angles (src/sampling.cpp:174-194)."""
+    n = math.ceil(360.0 / psi_step)
+    step = 360.0 / n
+    return np.arange(n) * step, step
+
+
+def build_map2d(w: Map2dWorkload):
+    """Returns (Map2dPool for all particles, projector data [K][pad][padF][2], r_max, truth dict)."""
+    rng = np.random.default_rng(w.seed)
+    ori = w.ori_size
+    cur = w.current_size or ori
+    K = w.n_classes
+    refs = grid_templates(rng, ori, K, w.n_blobs, w.blob_sigma)
+    proj = []
+    for k in range(K):
+        d, r_max, pad = projector_map_2d(refs[k], cur)
+        proj.append(d)
+    proj = np.stack(proj)
+    N = w.n_particles
+    Fs = cur // 2 + 1
+    cls = rng.integers(0, K, N)
+    psi = rng.uniform(0, 360, N)
+    sx = rng.uniform(-w.max_shift, w.max_shift, N)
+    sy = rng.uniform(-w.max_shift, w.max_shift, N)
+    du = rng.uniform(*w.defocus, N)
+    dv = rng.uniform(*w.defocus, N)
+    da = rng.uniform(0, 180, N)
+    rows = np.arange(cur)
+    ky = np.where(rows < Fs, rows, rows - cur).astype(np.float64)[:, None]
+    kx = np.arange(Fs, dtype=np.float64)[None, :]
+    Fr = np.zeros((N, cur * Fs))
+    Fi = np.zeros((N, cur * Fs))
+    ctf = np.zeros((N, cur * Fs))
+    mres = mresol(cur)
+    sig_all = []
+    chunk = 256
+    for c0 in range(0, N, chunk):
+        c1 = min(N, c0 + chunk)
+        for k in np.unique(cls[c0:c1]):
+            idx = np.nonzero(cls[c0:c1] == k)[0] + c0
+            P = rotate2d_np(proj[k], r_max, psi[idx], cur)
+            for q, i in enumerate(idx):
+                c = ctf_image(cur, ori, w.pixel, du[i], dv[i], da[i], 300.0, 2.7, 0.1)
+                # an image shifted by -s is brought back by the offset s (XOFF/YOFF)
+                ph = np.exp(2j * np.pi * (kx * sx[i] + ky * sy[i]) / ori)
+                s = P[q] * ph * c
+                Fr[i] = s.real.reshape(-1)
+                Fi[i] = s.imag.reshape(-1)
+                ctf[i] = c.reshape(-1)
+                sig_all.append(np.mean(np.abs(s.reshape(-1)[mres > 0]) ** 2))
+    # white noise per component at the requested SNR (signal power / noise power)
+    sig_pow = float(np.mean(sig_all))
+    sigma2 = sig_pow / (2.0 * w.snr)
+    Fr += rng.normal(0, math.sqrt(sigma2), Fr.shape)
+    Fi += rng.normal(0, math.sqrt(sigma2), Fi.shape)
+    Fr[:, 0] = 0.0
+    Fi[:, 0] = 0.0
+    oriF = ori // 2 + 1
+    tx, ty = translations(w.offset_range, w.offset_step)
+    pa, pstep = psi_angles(w.psi_step)
+    pert = w.random_perturbation
+    over_psi = (pa + pert * pstep)[:, None]
+    over_tx = (tx + pert * w.offset_step)[:, None]
+    over_ty = (ty + pert * w.offset_step)[:, None]
+    pool = Map2dPool(
+        ori_size=ori, current_size=cur, coarse_size=cur, nr_classes=K, nr_groups=1, adaptive_oversampling=0,
+        over_psi=[over_psi], over_trans_x=[over_tx], over_trans_y=[over_ty], trans_x=tx, trans_y=ty,
+        Fimg_real=Fr, Fimg_imag=Fi, Fimg_nomask_real=Fr.copy(), Fimg_nomask_imag=Fi.copy(), Fctf=ctf,
+        highres_Xi2=np.zeros(N), old_offsetx=np.zeros(N), old_offsety=np.zeros(N), group=np.zeros(N, np.int32),
+        sigma2_noise=np.full((1, oriF), sigma2), Mresol_fine=mres, Mresol_coarse=mres.copy(),
+        pdf_class=np.full(K, 1.0 / K), pdf_direction=np.full(K, 1.0 / K), prior_offsetx_class=np.zeros(K),
+        prior_offsety_class=np.zeros(K), sigma2_offset=float(w.offset_range) ** 2 / 4.0,
+    )
+    truth = dict(cls=cls, psi=psi, sx=sx, sy=sy)
+    return pool, proj, r_max, truth
+
+
+def subset(p: Map2dPool, lo: int, hi: int) -> Map2dPool:
+    """The particles [lo, hi) of a pool (same model and sampling)."""
+    q = dataclasses.replace(p)
+    for name in ["Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf", "highres_Xi2",
+                 "old_offsetx", "old_offsety", "group"]:
+        setattr(q, name, np.ascontiguousarray(getattr(p, name)[lo:hi]))
+    return q
+
+
+# the benchmark configurations (BASELINE configs 1 and 2)
+CONFIGS = {
+    "map2d_cfg1": Map2dWorkload(n_particles=1000, ori_size=64, n_classes=10, n_blobs=20, psi_step=10.0,
+                                offset_range=5, offset_step=1, max_shift=4.0, pixel=2.0, snr=0.05, seed=1),
+    "map2d_cfg2": Map2dWorkload(n_particles=20000, ori_size=128, n_classes=50, n_blobs=40, psi_step=5.0,
+                                offset_range=6, offset_step=2, max_shift=6.0, pixel=1.5, snr=0.03, seed=2),
+}

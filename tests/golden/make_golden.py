@@ -1,0 +1,91 @@
+"""Generate the golden vectors of the MAP2D hot path from the reference itself.
+
+Runs in a container that has the reference tree: builds oracle/_ref (the
+reference's own sources, compiled by oracle/Makefile), writes seeded
+synthetic datasets with rome_b200.synthetic, runs oracle/_ref/map2d_dump
+(which drives the reference's Map2dOptimizer_old and records every E-step
+stage of the first pool plus the M-step) and packs the arrays the tests
+use into tests/golden/<case>.npz.
+
+    python tests/golden/make_golden.py            # all cases
+    python tests/golden/make_golden.py map2d_a    # one case
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from rome_b200.map2d import load_dump  # noqa: E402
+from rome_b200.synthetic import Map2dSpec, write_dataset_2d  # noqa: E402
+
+# (dataset spec, reference options)
+CASES = {
+    # small single-pass case, CTF on, iteration 2 (CTF-corrected references)
+    "map2d_a": (Map2dSpec(n_particles=40, size=32, n_classes=2, n_blobs=8, blob_sigma=(1.5, 3.0), max_shift=2.0,
+                          snr=0.2, pixel=4.0, seed=3),
+                dict(K=2, iter=2, angpix=4.0, tau2_fudge=2, oversampling=0, pool=10, psi_step=30, offset_range=2,
+                     offset_step=1, ctf=1)),
+    # adaptive oversampling 1 (coarse + fine pass), 48^2, three classes, iteration 3
+    "map2d_b": (Map2dSpec(n_particles=48, size=48, n_classes=3, n_blobs=10, blob_sigma=(1.5, 4.0), max_shift=3.0,
+                          snr=0.1, pixel=3.0, seed=5),
+                dict(K=3, iter=3, angpix=3.0, tau2_fudge=2, oversampling=1, pool=8, psi_step=20, offset_range=3,
+                     offset_step=2, ctf=1)),
+    # configuration-1 shapes at reduced count: 64^2, 10 deg psi, +-5 px step 1, no oversampling
+    "map2d_c": (Map2dSpec(n_particles=36, size=64, n_classes=3, n_blobs=20, blob_sigma=(2.0, 6.0), max_shift=4.0,
+                          snr=0.05, pixel=2.0, seed=1),
+                dict(K=3, iter=2, angpix=2.0, tau2_fudge=2, oversampling=0, pool=6, psi_step=10, offset_range=5,
+                     offset_step=1, ctf=1)),
+}
+
+# arrays copied from the dump into the fixture (the per-translation shifted
+# images and per-orientation projections are large and are checked through
+# the oracle instead)
+SKIP_SUFFIXES = ("Fimg_shifted_real", "Fimg_shifted_imag", "Fref_real", "Fref_imag", "local_Fctf", "Minvsigma2")
+
+
+def build_reference():
+    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "_ref/map2d_dump",
+                           "_ref/librome_oracle.so"], stdout=subprocess.DEVNULL)
+
+
+def make_case(name: str):
+    spec, opt = CASES[name]
+    tmp = tempfile.mkdtemp(prefix="rome_golden_")
+    try:
+        star = write_dataset_2d(os.path.join(tmp, "data"), spec)
+        dump = os.path.join(tmp, "dump")
+        cmd = [os.path.join(ROOT, "oracle", "_ref", "map2d_dump"), "-i", star, "-dump_dir", dump]
+        for k, v in opt.items():
+            cmd += [f"-{k}", str(v)]
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env)
+        d = load_dump(dump)
+        keep = {k: v for k, v in d.items() if not k.endswith(SKIP_SUFFIXES)}
+        # a few shifted images / projections of pass 0 for the kernel-level checks
+        keep["pass0_Fimg_shifted_real_t01"] = d["pass0_Fimg_shifted_real"][:, :2]
+        keep["pass0_Fimg_shifted_imag_t01"] = d["pass0_Fimg_shifted_imag"][:, :2]
+        keep["pool0_pass0_Fref_real_r01"] = d["pool0_pass0_Fref_real"][:, :2]
+        keep["pool0_pass0_Fref_imag_r01"] = d["pool0_pass0_Fref_imag"][:, :2]
+        keep["pass0_Minvsigma2"] = d["pass0_Minvsigma2"]
+        keep["meta_options"] = np.array([str(opt)])
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(out, **keep)
+        print(f"{name}: {len(keep)} arrays, {os.path.getsize(out) / 1e6:.2f} MB")
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    build_reference()
+    names = sys.argv[1:] or list(CASES)
+    for n in names:
+        make_case(n)

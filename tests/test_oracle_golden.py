@@ -1,0 +1,92 @@
+"""Pin the C oracle (oracle/estep_oracle.c) against the reference itself.
+
+The golden vectors in tests/golden/ were recorded by running the
+reference's own Map2dOptimizer_old code (oracle/_ref/map2d_dump, built
+from the reference sources) on seeded synthetic datasets.  The oracle must
+reproduce every E-step stage of the first pool: bit-exact where the
+reference's operation order is followed (diff2, weights, significance,
+poses), to FP64 round-off where only the summation order differs.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle_py
+from tests.util import golden_pool, relerr
+
+CASES = ["map2d_a", "map2d_b", "map2d_c"]
+
+
+@pytest.fixture(scope="module")
+def oracle_runs(golden):
+    out = {}
+    for c in CASES:
+        g = golden[c]
+        p, proj, r_max = golden_pool(g)
+        o, bpd, bpw = oracle_py.map2d_estep_pool(p, proj, r_max, checkpoints=True)
+        out[c] = (g, p, o, bpd, bpw)
+    return out
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_diff2_weights_bit_exact(oracle_runs, case):
+    g, p, o, _, _ = oracle_runs[case]
+    for ip in range(p.npass()):
+        pre = f"pool0_pass{ip}_"
+        assert np.array_equal(o[f"diff2_{ip}"], g[pre + "diff2"]), f"diff2 pass {ip}"
+        assert np.array_equal(o[f"weight_{ip}"], g[pre + "weight"]), f"weight pass {ip}"
+    last = f"pool0_pass{p.npass() - 1}_"
+    assert np.array_equal(o["min_diff2"], g[last + "min_diff2"])
+    assert relerr(o["sum_weight"], g[last + "sum_weight"]) < 1e-14
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_significance_and_poses_bit_exact(oracle_runs, case):
+    g, p, o, _, _ = oracle_runs[case]
+    last = f"pool0_pass{p.npass() - 1}_"
+    assert np.array_equal(o["significant_weight"], g[last + "significant_weight"])
+    assert np.array_equal(o["nr_sign"], g["pool0_pass0_nr_sign"])
+    assert np.array_equal(o["Mcoarse_significant"], g["pool0_pass0_Mcoarse_significant"])
+    for k, gk in [("cls", "class"), ("psi", "psi"), ("xoff", "xoff"), ("yoff", "yoff")]:
+        assert np.array_equal(o[k], g[last + gk]), k
+    assert relerr(o["pmax"], g[last + "pmax"]) < 1e-14
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_wsums_and_backprojection(oracle_runs, case):
+    g, p, o, bpd, bpw = oracle_runs[case]
+    assert relerr(o["wsum_norm_correction"], g["pool0_wsum_norm_correction"]) < 1e-13
+    for k in ["wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_prior_offsetx_class",
+              "wsum_prior_offsety_class", "wsum_sigma2_offset", "wsum_sumw_group"]:
+        assert relerr(o[k], g["pool0_after_update_" + k]) < 1e-13, k
+    assert relerr(bpd, g["pool0_after_bp_bp_data"]) < 1e-13
+    assert relerr(bpw, g["pool0_after_bp_bp_weight"]) < 1e-13
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_shift_table_matches_reference(golden, case):
+    """shiftImageInFourierTransform (image.h:1478-1575) restated bit-exactly."""
+    g = golden[case]
+    p, _, _ = golden_pool(g)
+    cs = int(g["pass0_current_size"][0])
+    assert cs == p.current_size or p.adaptive_oversampling > 0
+    if cs != p.current_size:
+        pytest.skip("pass 0 is windowed to the coarse size")
+    for i in range(p.nr_images):
+        for t in range(2):
+            r, im = oracle_py.shift_image(p.Fimg_real[i], p.Fimg_imag[i], cs, p.over_trans_x[0][t, 0],
+                                          p.over_trans_y[0][t, 0], p.ori_size)
+            assert np.array_equal(r, g["pass0_Fimg_shifted_real_t01"][i, t])
+            assert np.array_equal(im, g["pass0_Fimg_shifted_imag_t01"][i, t])
+
+
+def test_select_edge_cases():
+    """Selection on hand-made rows: ties, one weight, zeros, exact threshold."""
+    sw, ns = oracle_py.select_significant(np.array([0.0, 0.0, 1.0, 0.0]), 1.0, 0.999)
+    assert (sw, ns) == (1.0, 1.0)
+    sw, ns = oracle_py.select_significant(np.array([0.25] * 4), 1.0, 0.999)
+    assert (sw, ns) == (0.25, 4.0)
+    w = np.array([0.5, 0.3, 0.2, 1e-5])
+    sw, ns = oracle_py.select_significant(w, w.sum(), 0.999)
+    assert (sw, ns) == (0.2, 3.0)
+    sw, ns = oracle_py.select_significant(np.zeros(5), 0.0, 0.999)
+    assert ns == 0
