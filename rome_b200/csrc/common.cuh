@@ -133,6 +133,8 @@ struct RomeGpuCtx {
     std::vector<double> h_tmp;
     // shift table (cos, sin) from the host's libm, identical to the reference's
     double2* d_shift_tab = nullptr;
+    // device flag raised by kernels whose bounded waits expire
+    int* d_err = nullptr;
     double shift_sampling = 0;
     // per-phase device timings and launch counts (rome_gpu_get_timings)
     int profile = 0;

@@ -1,9 +1,325 @@
-// tcgen05 BF16 GEMM for the diff2 cross term (work in progress).
+// tcgen05 (5th-generation tensor core) contraction for the diff2 cross term:
+//   C[m][n] = sum_k A[m][k] * B[n][k]      A, B bf16, K-major; C fp32 in TMEM
+// with the diff2 epilogue applied straight out of TMEM.
+//
+// One CTA computes a BM x BN = 128 x BN tile (cta_group::1, UMMA M = 128):
+//   warp 0 / lane 0 : TMA producer (cp.async.bulk.tensor, 128B swizzle,
+//                     STAGES-deep shared-memory ring, mbarrier complete_tx)
+//   warp 1 / lane 0 : MMA issuer (tcgen05.mma kind::f16, 4 x K16 per 64-wide
+//                     K block; tcgen05.commit frees a stage / signals the
+//                     accumulator)
+//   warps 0-3       : epilogue, tcgen05.ld 32x32b (warp w owns TMEM lanes
+//                     32w..32w+31 = rows of the tile)
+// Split precision (ROME_PREC_BF16X3) loads hi and lo planes of both operands
+// and issues hi*hi + hi*lo + lo*hi into the same accumulator.
+//
+// Every mbarrier wait is bounded; on expiry the kernel records a timeout in a
+// device flag, drains the copies it issued (again bounded), frees its TMEM
+// and returns, and the host reports ROME_ERR_TIMEOUT.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "gemm_tc.cuh"
 
 namespace rome {
-void tc_diff2_gemm(cudaStream_t, int, int, int, const void*, const void*, int precision, const Diff2Epi&) {
-    fail(ROME_ERR_UNSUPPORTED, "tensor-core precision %d not available in this build", precision);
+namespace {
+
+constexpr int BM = 128;
+constexpr int BK = 64;  // one 128-byte swizzle atom of bf16
+constexpr long WAIT_LIMIT = 1L << 28;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
 }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// bounded wait on an mbarrier phase (iteration count and 2 s of wall time);
+// returns false on expiry
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t addr = smem_u32(bar);
+    uint64_t t0 = 0;
+    for (long it = 0; it < WAIT_LIMIT; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if ((it & 1023) == 0) {
+            uint64_t t = global_ns();
+            if (it == 0) t0 = t;
+            else if (t - t0 > 2000000000ull) return false;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
+            "r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
+        : "memory");
+}
+
+// UMMA shared-memory descriptor, K-major, 128-byte swizzle: 8-row groups of
+// 1024 bytes (SBO = 64 x 16 B), LBO = 16 B, descriptor version 1 (sm_100)
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)64 << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// instruction descriptor: D f32, A/B bf16, both K-major, M = 128, N = BN
+template <int BN>
+__device__ __forceinline__ uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(a), "l"(b), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
+}
+
+template <int BN, int NPLANE, int STAGES>
+struct TcSmem {
+    static constexpr int A_BYTES = BM * BK * 2;
+    static constexpr int B_BYTES = BN * BK * 2;
+    static constexpr int STAGE_BYTES = NPLANE * (A_BYTES + B_BYTES);
+    static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+};
+
+// NPLANE = 1: bf16; NPLANE = 2: split precision (hi and lo planes)
+template <int BN, int NPLANE, int STAGES, typename Epi>
+__global__ void __launch_bounds__(128, 1)
+    tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA0, const __grid_constant__ CUtensorMap mapA1,
+                   const __grid_constant__ CUtensorMap mapB0, const __grid_constant__ CUtensorMap mapB1, int M, int N,
+                   int Kp, Epi epi, int* err) {
+    using S = TcSmem<BN, NPLANE, STAGES>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint64_t* full = (uint64_t*)(smem + STAGES * S::STAGE_BYTES);
+    uint64_t* empty = full + STAGES;
+    uint64_t* accum = empty + STAGES;
+    uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+    __shared__ int timed_out;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int nk = Kp / BK;
+    constexpr uint32_t TMEM_COLS = BN;  // power of two >= 32
+
+    if (threadIdx.x == 0) {
+        timed_out = 0;
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accum, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_base = *tmem_slot;
+
+    int issued = 0;  // stages the producer armed (for draining after a timeout)
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) + 1) & 1)) {
+                atomicExch(&timed_out, 1);
+                break;
+            }
+            if (timed_out) break;
+            uint8_t* st = smem + s * S::STAGE_BYTES;
+            mbar_expect_tx(&full[s], S::STAGE_BYTES);
+            tma_load_2d(st, &mapA0, &full[s], kb * BK, m0);
+            tma_load_2d(st + S::A_BYTES, &mapB0, &full[s], kb * BK, n0);
+            if (NPLANE == 2) {
+                tma_load_2d(st + S::A_BYTES + S::B_BYTES, &mapA1, &full[s], kb * BK, m0);
+                tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, &mapB1, &full[s], kb * BK, n0);
+            }
+            issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        const uint32_t idesc = idesc_bf16<BN>();
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % STAGES;
+            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
+                atomicExch(&timed_out, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint8_t* st = smem + s * S::STAGE_BYTES;
+            const uint32_t a0 = smem_u32(st), b0 = smem_u32(st + S::A_BYTES);
+            const uint32_t a1 = smem_u32(st + S::A_BYTES + S::B_BYTES), b1 = smem_u32(st + 2 * S::A_BYTES + S::B_BYTES);
+#pragma unroll
+            for (int j = 0; j < BK / 16; j++) {
+                // advance 16 bf16 (32 bytes) along K inside the swizzle atom
+                const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+                umma_bf16(tmem_base, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, acc);
+                if (NPLANE == 2) {
+                    umma_bf16(tmem_base, sw128_desc(a0 + 32 * j), sw128_desc(b1 + 32 * j), idesc, 1u);
+                    umma_bf16(tmem_base, sw128_desc(a1 + 32 * j), sw128_desc(b0 + 32 * j), idesc, 1u);
+                }
+            }
+            umma_commit(&empty[s]);
+        }
+        umma_commit(accum);
+    }
+    __syncwarp();
+    // ---------------- epilogue ----------------
+    bool ok = mbar_wait(accum, 0);
+    if (!ok) atomicExch(&timed_out, 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!timed_out) {
+        const int row = m0 + warp * 32 + lane;
+        const uint32_t lane_base = tmem_base + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            float v[16];
+            tmem_ld16(lane_base + c, v);
+            if (row < M) {
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    int n = n0 + c + q;
+                    if (n < N) epi(row, n, v[q]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (timed_out) {
+        // drain the copies this CTA issued before leaving (bounded)
+        if (warp == 0 && lane == 0) {
+            for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
+                mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
+            atomicExch(err, 1);
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        ROME_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+        if (!p || q != cudaDriverEntryPointSuccess) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+// 2D bf16 tensor map over a [rows][Kp] K-contiguous operand, box BK x box_rows
+CUtensorMap make_map(const void* base, long rows, int Kp, int box_rows) {
+    ROME_REQUIRE(((uintptr_t)base & 15) == 0 && Kp % BK == 0, "operand alignment");
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return m;
+}
+
+template <int BN, int NPLANE, int STAGES, typename Epi>
+void launch(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, const Epi& epi, int* derr) {
+    using S = TcSmem<BN, NPLANE, STAGES>;
+    const __nv_bfloat16* Ah = (const __nv_bfloat16*)A;
+    const __nv_bfloat16* Bh = (const __nv_bfloat16*)B;
+    CUtensorMap a0 = make_map(Ah, M, Kp, BM);
+    CUtensorMap b0 = make_map(Bh, N, Kp, BN);
+    CUtensorMap a1 = NPLANE == 2 ? make_map(Ah + (size_t)M * Kp, M, Kp, BM) : a0;
+    CUtensorMap b1 = NPLANE == 2 ? make_map(Bh + (size_t)N * Kp, N, Kp, BN) : b0;
+    auto kern = tc_gemm_kernel<BN, NPLANE, STAGES, Epi>;
+    ROME_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL));
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    kern<<<grid, 128, S::TOTAL, st>>>(a0, a1, b0, b1, M, N, Kp, epi, derr);
+    ROME_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, int precision,
+                   const Diff2Epi& epi, int* derr) {
+    if (precision == ROME_PREC_BF16)
+        launch<256, 1, 4>(st, M, N, Kp, A, B, epi, derr);
+    else if (precision == ROME_PREC_BF16X3)
+        launch<128, 2, 3>(st, M, N, Kp, A, B, epi, derr);
+    else
+        fail(ROME_ERR_UNSUPPORTED, "precision %d has no tensor-core path", precision);
+}
+
+void tc_check_error(cudaStream_t st, int* derr) {
+    int h = 0;
+    ROME_CUDA(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ROME_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        ROME_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), st));
+        fail(ROME_ERR_TIMEOUT, "tensor-core GEMM: a bounded mbarrier wait expired");
+    }
+}
+
 }  // namespace rome

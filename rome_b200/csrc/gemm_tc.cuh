@@ -1,11 +1,15 @@
-// Tensor-core (tcgen05) cross-term GEMM: declared here, implemented in
-// gemm_tc.cu.  The epilogue type is fixed to the diff2 epilogue.
+// Tensor-core (tcgen05) cross-term contraction, implemented in gemm_tc.cu.
 #pragma once
 #include <cuda_runtime.h>
 
 #include "epilogues.cuh"
 
 namespace rome {
+// diff2 = epilogue(A[M][Kp] . B[N][Kp]^T); A, B bf16 (hi plane, then lo plane
+// for ROME_PREC_BF16X3), K-major, Kp a multiple of 64.
+// derr: the context's device error flag (set when a bounded wait expires)
 void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, int precision,
-                   const Diff2Epi& epi);
-}
+                   const Diff2Epi& epi, int* derr);
+// raises ROME_ERR_TIMEOUT if a tensor-core kernel's bounded wait expired
+void tc_check_error(cudaStream_t st, int* derr);
+}  // namespace rome

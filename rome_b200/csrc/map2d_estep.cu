@@ -273,7 +273,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             if (!tc) {
                 sgemm_tn(st, (int)M, g.J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
             } else {
-                tc_diff2_gemm(st, (int)M, g.J, g.Kp, dA, dB, ctx->precision, epi);
+                tc_diff2_gemm(st, (int)M, g.J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
             }
             prof.launched(ROME_PHASE_CROSS_GEMM);
             // algorithmic work: 4 flops per active complex coefficient per (image, translation, orientation)
@@ -293,6 +293,8 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 prof.launched(ROME_PHASE_POSTERIOR);
             }
             prof.end(ROME_PHASE_POSTERIOR);
+
+            if (tc) tc_check_error(st, ctx->d_err);
 
             // ---- checkpoints and per-particle results of this pass ----
             std::vector<double> hpart((size_t)P * 8);
