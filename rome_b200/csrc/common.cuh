@@ -108,6 +108,13 @@ enum Slot {
     S_ROTSIG,     // Rot_significant [K*npsi] char
     S_ACTIDX,     // pixel -> active index [F] int
     S_TRANS,      // translations of the last pass [T] double2
+    S_LISTCNT,    // list counter + per-orientation counts
+    S_SEG,        // per-particle list segments [P][2]
+    S_SIGLIST,    // significant hypotheses, particle order then orientation order
+    S_OFFJ,       // per-orientation offsets and fill counters
+    S_PHASE,      // phase table of the pass [T][F] double2
+    S_W2B,        // norm operand, bf16 hi/lo planes
+    S_QB,         // |P|^2, bf16 hi/lo planes
     S_TMP0,
     S_TMP1,
     S_TMP2,

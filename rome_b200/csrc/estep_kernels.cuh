@@ -36,6 +36,33 @@ __device__ __forceinline__ double2 table_shift(double x, double y, double2 sh, d
     return make_double2(dsub(ac, bd), dsub(dsub(ab_cd, ac), bd));
 }
 
+// The table index depends only on the translation and the pixel, so a pass
+// tabulates (a, b) = (cos, +-sin) once per (translation, pixel) and every
+// particle reuses it: ph[t][n].  apply_phase is the same three-multiplication
+// product as table_shift; translations below ROME_EQUAL_ACCURACY leave the
+// coefficient untouched exactly as the reference's early return does.
+__device__ __forceinline__ double2 apply_phase(double2 sh, double2 ab, double2 v) {
+    if (fabs(sh.x) < 1e-6 && fabs(sh.y) < 1e-6) return v;
+    double ac = dmul(ab.x, v.x), bd = dmul(ab.y, v.y);
+    double ab_cd = dmul(dadd(ab.x, ab.y), dadd(v.x, v.y));
+    return make_double2(dsub(ac, bd), dsub(dsub(ab_cd, ac), bd));
+}
+
+__global__ void phase_table_kernel(int T, int F, int csF, int cs, const double2* __restrict__ shifts,
+                                   const double2* __restrict__ tab, double sampling, double2* __restrict__ ph) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long)T * F) return;
+    int t = (int)(q / F), n = (int)(q - (long)t * F);
+    int row = n / csF;
+    double x = (double)(n - row * csF), y = (double)(row < csF ? row : row - cs);
+    const double2 sh = shifts[t];
+    const double two_pi = 2 * kPi;
+    double dotp = dmul(two_pi, dadd(dmul(x, sh.x), dmul(y, sh.y)));
+    int idx = ((int)__ddiv_rn(fabs(dotp), sampling)) % 5000;
+    double2 cs2 = tab[idx];
+    ph[q] = make_double2(cs2.x, dotp < 0 ? -cs2.y : cs2.y);
+}
+
 // coordinates of half-plane pixel n of a size x (size/2+1) FFTW image
 __device__ __forceinline__ void pixel_xy(int n, int rowlen, int size, double& x, double& y) {
     int row = n / rowlen;
@@ -201,20 +228,19 @@ __global__ void project2d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
 __global__ void shift_operand_kernel(int P, int T, int F, int csF, int cs, int Kact, int Kp,
                                      const double2* __restrict__ Fimg, const double* __restrict__ lctf,
                                      const double* __restrict__ Minv, int apply_ctf, const int* __restrict__ act,
-                                     const double2* __restrict__ shifts, const double2* __restrict__ tab,
-                                     double sampling, void* __restrict__ Aop, float* __restrict__ S, int precision) {
+                                     const double2* __restrict__ shifts, const double2* __restrict__ ph,
+                                     void* __restrict__ Aop, float* __restrict__ S, int precision) {
     const int t = blockIdx.x, i = blockIdx.y;
     const long r = (long)i * T + t;
     const double2 sh = shifts[t];
     const double2* X = Fimg + (long)i * F;
     const double* M = Minv + (long)i * F;
     const double* C = lctf + (long)i * F;
+    const double2* pht = ph + (long)t * F;
     double s = 0.0;
     // S over every pixel of the pass image
     for (int n = threadIdx.x; n < F; n += blockDim.x) {
-        double x, y;
-        pixel_xy(n, csF, cs, x, y);
-        double2 v = table_shift(x, y, sh, X[n], tab, sampling);
+        double2 v = apply_phase(sh, pht[n], X[n]);
         s += M[n] * (v.x * v.x + v.y * v.y);
     }
     // A operand on the active pixels (zero padded to Kp)
@@ -223,9 +249,7 @@ __global__ void shift_operand_kernel(int P, int T, int F, int csF, int cs, int K
         float fr = 0.f, fi = 0.f;
         if (a < Kact) {
             int n = act[a];
-            double x, y;
-            pixel_xy(n, csF, cs, x, y);
-            double2 v = table_shift(x, y, sh, X[n], tab, sampling);
+            double2 v = apply_phase(sh, pht[n], X[n]);
             double w = apply_ctf ? M[n] * C[n] : M[n];
             fr = (float)(w * v.x);
             fi = (float)(w * v.y);
@@ -860,6 +884,281 @@ __global__ void __launch_bounds__(NT)
         double vr = sr[p], vi = si[p];
         double xp = dadd(dmul(A.x, (double)x), dmul(A.y, (double)y));
         double yp = dadd(dmul(A.z, (double)x), dmul(A.w, (double)y));
+        if (xp < 0) {
+            xp = -xp;
+            yp = -yp;
+            vi = -1 * vi;
+        }
+        int x0 = (int)floor(xp);
+        double fx = dsub(xp, (double)x0);
+        int y0 = (int)floor(yp);
+        double fy = dsub(yp, (double)y0);
+        y0 -= shift;
+        int y1 = y0 + 1;
+        double mfx = dsub(1., fx), mfy = dsub(1., fy);
+        double dd00 = dmul(mfy, mfx), dd01 = dmul(mfy, fx), dd10 = dmul(fy, mfx), dd11 = dmul(fy, fx);
+        double* t00 = (double*)(D + (long)y0 * padF + x0);
+        double* t10 = (double*)(D + (long)y1 * padF + x0);
+        atomicAdd(t00 + 0, dmul(dd00, vr));
+        atomicAdd(t00 + 1, dmul(dd00, vi));
+        atomicAdd(t00 + 2, dmul(dd01, vr));
+        atomicAdd(t00 + 3, dmul(dd01, vi));
+        atomicAdd(t10 + 0, dmul(dd10, vr));
+        atomicAdd(t10 + 1, dmul(dd10, vi));
+        atomicAdd(t10 + 2, dmul(dd11, vr));
+        atomicAdd(t10 + 3, dmul(dd11, vi));
+        double* w00 = W + (long)y0 * padF + x0;
+        double* w10 = W + (long)y1 * padF + x0;
+        atomicAdd(w00 + 0, dmul(dd00, mw));
+        atomicAdd(w00 + 1, dmul(dd01, mw));
+        atomicAdd(w10 + 0, dmul(dd10, mw));
+        atomicAdd(w10 + 1, dmul(dd11, mw));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Significant hypotheses as a compact list.  updateOtherParams and
+// backProjection only touch hypotheses with weight >= significant_weight
+// (src/map2d_optimizer.cpp:1469, :1594, :1800); each particle writes its own
+// contiguous segment of (hypothesis, weight / sum_weight) records.
+struct SigEntry {
+    int i;     // particle
+    int e;     // hypothesis index in the exp_Mweight layout
+    double w;  // weight / exp_sum_weight
+};
+
+__global__ void __launch_bounds__(256)
+    sig_list_kernel(int P, long X, PostLayout L, const float* __restrict__ diff2, const double* __restrict__ pdir,
+                    const double* __restrict__ poff, const double* __restrict__ part, int* __restrict__ counter,
+                    int cap, SigEntry* __restrict__ list, int* __restrict__ seg) {
+    const int i = blockIdx.x;
+    const double mn = part[(long)i * 8 + 0], sumw = part[(long)i * 8 + 1], sig = part[(long)i * 8 + 2];
+    const double dcut = part[(long)i * 8 + 5];
+    const float* d = diff2 + (long)i * X;
+    const double* po = poff + (long)i * L.K * L.ntr;
+    __shared__ int cnt, base;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    // pass 1: count
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        float dv = d[e];
+        if (dv < INFINITY && (double)dv <= dcut) {
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            if (hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]) >= sig) atomicAdd(&cnt, 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        base = atomicAdd(counter, cnt);
+        seg[2 * i] = base;
+        seg[2 * i + 1] = cnt;
+        cnt = 0;
+    }
+    __syncthreads();
+    // pass 2: write (order inside the segment is irrelevant to every consumer's sums up to rounding)
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        float dv = d[e];
+        if (dv < INFINITY && (double)dv <= dcut) {
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            double w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
+            if (w >= sig) {
+                int q = base + atomicAdd(&cnt, 1);
+                if (q < cap) list[q] = SigEntry{i, (int)e, w / sumw};
+            }
+        }
+    }
+}
+
+// counting sort of the list by orientation j = e / T
+__global__ void count_by_j_kernel(int n, int T, const SigEntry* __restrict__ list, int* __restrict__ cnt) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) atomicAdd(&cnt[list[q].e / T], 1);
+}
+
+// exclusive scan of cnt[0..n) into off[0..n], one CTA
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(int n, const int* __restrict__ cnt, int* __restrict__ off) {
+    __shared__ int sh[1024];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b = 0; b < n; b += 1024) {
+        int q = b + threadIdx.x;
+        int v = q < n ? cnt[q] : 0;
+        sh[threadIdx.x] = v;
+        __syncthreads();
+        for (int s = 1; s < 1024; s <<= 1) {
+            int t = threadIdx.x >= s ? sh[threadIdx.x - s] : 0;
+            __syncthreads();
+            sh[threadIdx.x] += t;
+            __syncthreads();
+        }
+        if (q < n) off[q] = carry + sh[threadIdx.x] - v;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += sh[1023];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) off[n] = carry;
+}
+
+__global__ void scatter_by_j_kernel(int n, int T, const SigEntry* __restrict__ list, const int* __restrict__ off,
+                                    int* __restrict__ fill, SigEntry* __restrict__ sorted) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    SigEntry s = list[q];
+    int j = s.e / T;
+    sorted[off[j] + atomicAdd(&fill[j], 1)] = s;
+}
+
+// updateOtherParams over the particle's list segment (see wsum_kernel)
+template <int NT, int PIX>
+__global__ void __launch_bounds__(NT)
+    wsum_list_kernel(int T, int nrot, int K, int F, int csF, int cs, int oriF, const SigEntry* __restrict__ list,
+                     const int* __restrict__ seg, const double2* __restrict__ Fimg, const double* __restrict__ lctf,
+                     int apply_ctf, const double2* __restrict__ proj, const int* __restrict__ actidx, int Kact,
+                     const double2* __restrict__ shifts, const double2* __restrict__ ph,
+                     const int* __restrict__ Mresol, const int* __restrict__ group, const double2* __restrict__ oldoff,
+                     const double2* __restrict__ trans, const double* __restrict__ priorx,
+                     const double* __restrict__ priory, double* __restrict__ wsn, double* __restrict__ normcorr,
+                     double* __restrict__ wk) {
+    const int i = blockIdx.y;
+    const int n0 = blockIdx.x * NT * PIX;
+    const int s0 = seg[2 * i], ns = seg[2 * i + 1];
+    __shared__ double spec[1024];
+    __shared__ double red[32];
+    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) spec[q] = 0.0;
+    __syncthreads();
+    double acc[PIX];
+    int ires_p[PIX];
+    double xs[PIX], ys[PIX], cp[PIX];
+    double2 Xp[PIX];
+    int ap[PIX];
+#pragma unroll
+    for (int p = 0; p < PIX; p++) {
+        acc[p] = 0.0;
+        int n = n0 + threadIdx.x + p * NT;
+        ires_p[p] = n < F ? Mresol[n] : -1;
+        if (ires_p[p] > -1) {
+            pixel_xy(n, csF, cs, xs[p], ys[p]);
+            Xp[p] = Fimg[(long)i * F + n];
+            cp[p] = lctf[(long)i * F + n];
+            ap[p] = actidx[n];
+        }
+    }
+    double sumwd = 0.0;
+    const int g = group[i];
+    const double2 oo = oldoff[i];
+    for (int q = 0; q < ns; q++) {
+        const SigEntry s = list[s0 + q];
+        const int j = s.e / T, t = s.e - j * T;
+        const double w = s.w;
+        const double2 sh = shifts[t];
+        const double2* Pj = proj + (long)j * Kact;
+#pragma unroll
+        for (int p = 0; p < PIX; p++) {
+            if (ires_p[p] > -1) {
+                double2 v = apply_phase(sh, ph[(long)t * F + n0 + threadIdx.x + p * NT], Xp[p]);
+                double2 pv = ap[p] >= 0 ? Pj[ap[p]] : make_double2(0.0, 0.0);
+                double pr = apply_ctf ? dmul(pv.x, cp[p]) : pv.x;
+                double pim = apply_ctf ? dmul(pv.y, cp[p]) : pv.y;
+                double dr = dsub(pr, v.x), di = dsub(pim, v.y);
+                double wd = dmul(w, dadd(dmul(dr, dr), dmul(di, di)));
+                acc[p] += wd;
+                sumwd += wd;
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            int k = j / nrot;
+            double2 tr = trans[t];
+            atomicAdd(&wk[0 * K + k], w);
+            atomicAdd(&wk[1 * K + k], w);
+            atomicAdd(&wk[2 * K + k], w * (oo.x + tr.x));
+            atomicAdd(&wk[3 * K + k], w * (oo.y + tr.y));
+            double ox = priorx[k] - oo.x - tr.x, oy = priory[k] - oo.y - tr.y;
+            atomicAdd(&wk[5 * K + g], w);
+            atomicAdd(&wk[4 * K + k], w * (ox * ox + oy * oy));
+        }
+    }
+#pragma unroll
+    for (int p = 0; p < PIX; p++)
+        if (ires_p[p] > -1 && ires_p[p] < 1024 && acc[p] != 0.0) atomicAdd(&spec[ires_p[p]], acc[p]);
+    sumwd = block_reduce_sum(sumwd, red);
+    __syncthreads();
+    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT)
+        if (spec[q] != 0.0) atomicAdd(&wsn[(long)g * oriF + q], spec[q]);
+    if (threadIdx.x == 0 && sumwd != 0.0) atomicAdd(&normcorr[i], sumwd);
+}
+
+// backProjection over the orientation's list segment (see bp_kernel)
+template <int NT, int PIX>
+__global__ void __launch_bounds__(NT)
+    bp_list_kernel(int T, int nrot, int F, int csF, int cs, const SigEntry* __restrict__ sorted,
+                   const int* __restrict__ off, const double2* __restrict__ Fnm, const double* __restrict__ Mctf2,
+                   const double2* __restrict__ shifts, const double2* __restrict__ ph,
+                   const double4* __restrict__ rot, int r_max, int pad, int padF, double2* __restrict__ bp_data,
+                   double* __restrict__ bp_weight, long vox) {
+    const int j = blockIdx.y;
+    const int s0 = off[j], ns = off[j + 1] - s0;
+    if (ns == 0) return;
+    const int n0 = blockIdx.x * NT * PIX;
+    const int k = j / nrot;
+    double sr[PIX], si[PIX], sw[PIX], xs[PIX], ys[PIX];
+    bool on[PIX];
+    const int max_r2 = r_max * r_max;
+#pragma unroll
+    for (int p = 0; p < PIX; p++) {
+        sr[p] = si[p] = sw[p] = 0.0;
+        int n = n0 + threadIdx.x + p * NT;
+        on[p] = false;
+        if (n < F) {
+            int row = n / csF, x = n - row * csF;
+            int y = row, first_x = 0;
+            bool rowok = true;
+            if (row <= r_max) {
+                y = row;
+                first_x = 0;
+            } else if (row >= cs - r_max) {
+                y = row - cs;
+                first_x = 1;
+            } else
+                rowok = false;
+            on[p] = rowok && x >= first_x && x <= r_max && x * x + y * y <= max_r2;
+            xs[p] = (double)x;
+            ys[p] = (double)(row < csF ? row : row - cs);
+        }
+    }
+    for (int q = 0; q < ns; q++) {
+        const SigEntry s = sorted[s0 + q];
+        const int t = s.e - j * T;
+        const double w = s.w;
+        const double2 sh = shifts[t];
+#pragma unroll
+        for (int p = 0; p < PIX; p++) {
+            if (on[p]) {
+                int n = n0 + threadIdx.x + p * NT;
+                double2 v = apply_phase(sh, ph[(long)t * F + n], Fnm[(long)s.i * F + n]);
+                sr[p] = dadd(sr[p], dmul(v.x, w));
+                si[p] = dadd(si[p], dmul(v.y, w));
+                sw[p] = dadd(sw[p], dmul(Mctf2[(long)s.i * F + n], w));
+            }
+        }
+    }
+    const double4 A = rot[j];
+    const int shift = -(int)((float)pad / 2.0f);
+    double2* D = bp_data + (long)k * vox;
+    double* W = bp_weight + (long)k * vox;
+#pragma unroll
+    for (int p = 0; p < PIX; p++) {
+        if (!on[p]) continue;
+        double mw = sw[p];
+        if (!(mw > 0.)) continue;
+        double x = xs[p], y = ys[p];
+        double vr = sr[p], vi = si[p];
+        double xp = dadd(dmul(A.x, x), dmul(A.y, y));
+        double yp = dadd(dmul(A.z, x), dmul(A.w, y));
         if (xp < 0) {
             xp = -xp;
             yp = -yp;

@@ -312,6 +312,32 @@ void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const v
         fail(ROME_ERR_UNSUPPORTED, "precision %d has no tensor-core path", precision);
 }
 
+void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
+                   int* derr) {
+    launch<128, 2, 3>(st, M, N, Kp, A, B, StoreEpi{out, ld}, derr);
+}
+
+// hi/lo bf16 planes of a [rows][K] fp32 matrix, zero padded to Kpad columns
+__global__ void split_bf16_kernel(const float* __restrict__ in, long rows, int K, int ldin, int Kpad,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= rows * Kpad) return;
+    long r = q / Kpad;
+    int k = (int)(q - r * Kpad);
+    float v = k < K ? in[r * ldin + k] : 0.f;
+    __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[q] = h;
+    lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, int Kpad, void* out) {
+    __nv_bfloat16* hi = (__nv_bfloat16*)out;
+    __nv_bfloat16* lo = hi + rows * Kpad;
+    long n = rows * Kpad;
+    split_bf16_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, rows, K, ldin, Kpad, hi, lo);
+    ROME_CHECK_LAUNCH();
+}
+
 void tc_check_error(cudaStream_t st, int* derr) {
     int h = 0;
     ROME_CUDA(cudaMemcpyAsync(&h, derr, sizeof(int), cudaMemcpyDeviceToHost, st));

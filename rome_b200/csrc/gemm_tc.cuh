@@ -10,6 +10,11 @@ namespace rome {
 // derr: the context's device error flag (set when a bounded wait expires)
 void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, int precision,
                    const Diff2Epi& epi, int* derr);
+// out[m][n] = A . B^T in split precision (hi*hi + hi*lo + lo*hi)
+void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
+                   int* derr);
+// bf16 hi plane then lo plane of a [rows][ldin] fp32 matrix, K columns used, padded to Kpad
+void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, int Kpad, void* out);
 // raises ROME_ERR_TIMEOUT if a tensor-core kernel's bounded wait expired
 void tc_check_error(cudaStream_t st, int* derr);
 }  // namespace rome

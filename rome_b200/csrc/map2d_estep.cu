@@ -153,6 +153,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         int* dAct = nullptr;
         double4* dRot = nullptr;
         double2* dShift = nullptr;
+        double2* dPh = nullptr;
         int* dJvalid = nullptr;
 
         for (int ipass = 0; ipass < npass; ipass++) {
@@ -211,6 +212,12 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 hsh[t] = make_double2((double)in->over_trans_x[ipass][t] / (-ori),
                                       (double)in->over_trans_y[ipass][t] / (-ori));
             dShift = upload(ctx, S_SHIFT, hsh.data(), hsh.size());
+            dPh = ctx->ws[S_PHASE].as<double2>((size_t)g.T * g.F);
+            prof.begin(ROME_PHASE_SHIFT);
+            phase_table_kernel<<<(unsigned)(((long)g.T * g.F + 255) / 256), 256, 0, st>>>(
+                g.T, g.F, g.csF, cs, dShift, ctx->d_shift_tab, ctx->shift_sampling, dPh);
+            prof.launched(ROME_PHASE_SHIFT);
+            prof.end(ROME_PHASE_SHIFT);
 
             // ---- prep: window to cs, local CTF, Minvsigma2 ----
             dFimg = ctx->ws[S_FIMG].as<double2>((size_t)P * g.F);
@@ -249,8 +256,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
             prof.begin(ROME_PHASE_SHIFT);
             shift_operand_kernel<<<dim3(g.T, P), 256, 0, st>>>(P, g.T, g.F, g.csF, cs, g.Kact, g.Kp, dFimg, dLctf,
-                                                              dMinv, apply_ctf ? 1 : 0, dAct, dShift,
-                                                              ctx->d_shift_tab, ctx->shift_sampling, dA, dS,
+                                                              dMinv, apply_ctf ? 1 : 0, dAct, dShift, dPh, dA, dS,
                                                               ctx->precision);
             prof.launched(ROME_PHASE_SHIFT);
             w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
@@ -260,8 +266,20 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             // ---- norm term N[i][j] = sum_n Minv c^2 |P_j|^2 (FP32 CUDA cores) ----
             float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * g.J);
             prof.begin(ROME_PHASE_NORM_GEMM);
-            sgemm_tn(st, P, g.J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, g.J});
-            prof.launched(ROME_PHASE_NORM_GEMM);
+            if (!tc) {
+                sgemm_tn(st, P, g.J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, g.J});
+                prof.launched(ROME_PHASE_NORM_GEMM);
+            } else {
+                // split-BF16 on the tensor cores in every tensor-core mode: the
+                // norm term is all positive, so its hi/lo rounding averages out
+                const int Kq64 = ((g.Kact + 63) / 64) * 64;
+                void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
+                void* dQb = ctx->ws[S_QB].get((size_t)g.J * Kq64 * 4);
+                split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
+                split_bf16(st, dQ, g.J, g.Kact, g.Kq, Kq64, dQb);
+                tc_store_gemm(st, P, g.J, Kq64, dW2b, dQb, dNorm, g.J, ctx->d_err);
+                prof.launched(ROME_PHASE_NORM_GEMM, 3);
+            }
             prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * g.J * g.Kact);
             prof.end(ROME_PHASE_NORM_GEMM);
 
@@ -355,17 +373,33 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         double* dWk = ctx->ws[S_WSUMK].as<double>((size_t)5 * K + G + 1);
         ROME_CUDA(cudaMemsetAsync(dWsn, 0, sizeof(double) * ((size_t)G * oriF + P), st));
         ROME_CUDA(cudaMemsetAsync(dWk, 0, sizeof(double) * ((size_t)5 * K + G + 1), st));
+        // compact list of significant hypotheses (weight >= significant_weight)
+        const PostLayout L{g.T, g.notr, g.nor, npsi, ntr, K};
+        int* dCounter = ctx->ws[S_LISTCNT].as<int>((size_t)2 * g.J + 4);
+        int* dSeg = ctx->ws[S_SEG].as<int>((size_t)2 * P);
+        int cap = std::max(1024, P * 64), nsigtot = 0;
+        SigEntry* dList = nullptr;
+        prof.begin(ROME_PHASE_WSUM);
+        for (int attempt = 0; attempt < 2; attempt++) {
+            dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)cap * 2);
+            ROME_CUDA(cudaMemsetAsync(dCounter, 0, sizeof(int), st));
+            sig_list_kernel<<<P, 256, 0, st>>>(P, g.X, L, dDiff2, dPdir, dPoff, dPart, dCounter, cap, dList, dSeg);
+            prof.launched(ROME_PHASE_WSUM);
+            ROME_CUDA(cudaMemcpyAsync(&nsigtot, dCounter, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaStreamSynchronize(st));
+            if (nsigtot <= cap) break;
+            cap = nsigtot;  // every particle's segment fits on the second pass
+        }
         {
             const int NT = 256, PIX = 8;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
-            prof.begin(ROME_PHASE_WSUM);
-            wsum_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
-                P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, g.F, g.csF, cur, oriF, dDiff2, dPdir, dPoff, dPart, dJvalid,
-                dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx, g.Kact, dShift, ctx->d_shift_tab, ctx->shift_sampling,
-                dMresF, dGroup, dOld, dTr, (const double2*)nullptr, dCls + K, dCls + 2 * K, dWsn, dNormCorr, dWk);
+            wsum_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
+                g.T, g.nrot, K, g.F, g.csF, cur, oriF, dList, dSeg, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
+                g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dCls + K,
+                dCls + 2 * K, dWsn, dNormCorr, dWk);
             prof.launched(ROME_PHASE_WSUM);
-            prof.end(ROME_PHASE_WSUM);
         }
+        prof.end(ROME_PHASE_WSUM);
 
         // ---- backProjection ----
         {
@@ -375,12 +409,28 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             bp_prep_kernel<<<P, 256, 0, st>>>(P, g.F, dFnr, dFni, dLctf, dMinv, dSig2, dGroup, oriF,
                                               in->sigma2_fudge, in->do_map, in->do_ctf_correction, dFnm, dMctf2);
             prof.launched(ROME_PHASE_BACKPROJECT);
+            // group the significant list by orientation (counting sort)
+            int* dCnt = dCounter + 2;
+            int* dOff = ctx->ws[S_OFFJ].as<int>((size_t)2 * g.J + 2);
+            int* dFill = dOff + g.J + 1;
+            SigEntry* dSorted = dList + cap;
+            ROME_CUDA(cudaMemsetAsync(dCnt, 0, sizeof(int) * g.J, st));
+            ROME_CUDA(cudaMemsetAsync(dFill, 0, sizeof(int) * g.J, st));
+            if (nsigtot > 0) {
+                count_by_j_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.T, dList, dCnt);
+                prof.launched(ROME_PHASE_BACKPROJECT);
+            }
+            exclusive_scan_kernel<<<1, 1024, 0, st>>>(g.J, dCnt, dOff);
+            prof.launched(ROME_PHASE_BACKPROJECT);
+            if (nsigtot > 0) {
+                scatter_by_j_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.T, dList, dOff, dFill, dSorted);
+                prof.launched(ROME_PHASE_BACKPROJECT);
+            }
             const int NT = 256, PIX = 8;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
-            bp_kernel<NT, PIX><<<dim3(nsplit, g.J), NT, 0, st>>>(
-                P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, g.F, g.csF, cur, dDiff2, dPdir, dPoff, dPart, dJvalid, dFnm,
-                dMctf2, dShift, ctx->d_shift_tab, ctx->shift_sampling, dRot, ctx->r_max, ctx->pad_size,
-                ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
+            bp_list_kernel<NT, PIX><<<dim3(nsplit, g.J), NT, 0, st>>>(
+                g.T, g.nrot, g.F, g.csF, cur, dSorted, dOff, dFnm, dMctf2, dShift, dPh, dRot, ctx->r_max,
+                ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
             prof.launched(ROME_PHASE_BACKPROJECT);
             prof.end(ROME_PHASE_BACKPROJECT);
         }
