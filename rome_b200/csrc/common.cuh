@@ -115,6 +115,15 @@ enum Slot {
     S_PHASE,      // phase table of the pass [T][F] double2
     S_W2B,        // norm operand, bf16 hi/lo planes
     S_QB,         // |P|^2, bf16 hi/lo planes
+    S_PIDX,       // table index of every (translation, active pixel) [T][Kact] u16
+    S_ROWMIN,     // per-particle min diff2 from the GEMM epilogue [P] u32 keys
+    S_REC_FW,     // reconstruct: Fweight (decentred)
+    S_REC_FNW,    // reconstruct: Fnewweight
+    S_REC_FCONV,  // reconstruct: complex work array
+    S_REC_REAL,   // reconstruct: real-space work array
+    S_REC_SMALL,  // reconstruct: radial sums, tau2, mask sums
+    S_REC_VOL,    // reconstruct: output volume
+    S_REC_TAB,    // reconstruct: blob table
     S_TMP0,
     S_TMP1,
     S_TMP2,

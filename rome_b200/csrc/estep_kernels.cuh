@@ -18,6 +18,9 @@
 
 namespace rome {
 
+template <typename TVal>
+__device__ TVal block_reduce_sum(TVal v, TVal* sh);
+
 // ---------------------------------------------------------------------------
 // shiftImageInFourierTransform for one coefficient (src/image.h:1530-1547):
 // tabulated cos/sin at index (int)(|dotp| / sampling) % 5000 and the
@@ -61,6 +64,98 @@ __global__ void phase_table_kernel(int T, int F, int csF, int cs, const double2*
     int idx = ((int)__ddiv_rn(fabs(dotp), sampling)) % 5000;
     double2 cs2 = tab[idx];
     ph[q] = make_double2(cs2.x, dotp < 0 ? -cs2.y : cs2.y);
+}
+
+// Table index of every (translation, active pixel): the same index the
+// reference's shiftImageInFourierTransform picks, as 16 bits, with the sign
+// of dotp in bit 15 (src/image.h:1530-1537).  Identity translations (below
+// ROME_EQUAL_ACCURACY) are marked with 0xFFFF.
+__global__ void phase_index_kernel(int T, int Kact, int csF, int cs, const int* __restrict__ act,
+                                   const double2* __restrict__ shifts, double sampling,
+                                   unsigned short* __restrict__ pidx) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long)T * Kact) return;
+    int t = (int)(q / Kact), a = (int)(q - (long)t * Kact);
+    const double2 sh = shifts[t];
+    if (fabs(sh.x) < 1e-6 && fabs(sh.y) < 1e-6) {
+        pidx[q] = 0xFFFF;
+        return;
+    }
+    int n = act[a];
+    int row = n / csF;
+    double x = (double)(n - row * csF), y = (double)(row < csF ? row : row - cs);
+    const double two_pi = 2 * kPi;
+    double dotp = dmul(two_pi, dadd(dmul(x, sh.x), dmul(y, sh.y)));
+    int idx = ((int)__ddiv_rn(fabs(dotp), sampling)) % 5000;
+    pidx[q] = (unsigned short)(idx | (dotp < 0 ? 0x8000 : 0));
+}
+
+// Cross-term A operand of one particle for every translation: a = Minvsigma2
+// * ctf * X_t on the active pixels, with the table phase applied in FP32
+// (the operand is stored in FP32 or BF16, so FP32 products keep it exact to
+// its own rounding), and S = sum_n Minvsigma2 |X|^2 over all pixels in FP64
+// (a phase shift leaves |X|^2 unchanged up to rounding, so S is the same
+// for every translation).  One CTA per particle; the 5000-entry table is
+// staged in shared memory as float2.
+template <int NT>
+__global__ void __launch_bounds__(NT)
+    shift_operand2_kernel(int P, int T, int F, int Kact, int Kp, const double2* __restrict__ Fimg,
+                          const double* __restrict__ lctf, const double* __restrict__ Minv, int apply_ctf,
+                          const int* __restrict__ act, const unsigned short* __restrict__ pidx,
+                          const double2* __restrict__ tab, void* __restrict__ Aop, float* __restrict__ S,
+                          int precision) {
+    __shared__ float2 stab[5000];
+    __shared__ double red[32];
+    const int i = blockIdx.x;
+    for (int q = threadIdx.x; q < 5000; q += NT) stab[q] = make_float2((float)tab[q].x, (float)tab[q].y);
+    const double2* X = Fimg + (long)i * F;
+    const double* M = Minv + (long)i * F;
+    const double* C = lctf + (long)i * F;
+    double s = 0.0;
+    for (int n = threadIdx.x; n < F; n += NT) {
+        double2 v = X[n];
+        s += M[n] * (v.x * v.x + v.y * v.y);
+    }
+    s = block_reduce_sum(s, red);  // includes a __syncthreads after the table fill
+    const long M2 = (long)P * T;
+    __nv_bfloat16* Ah = (__nv_bfloat16*)Aop;
+    __nv_bfloat16* Al = Ah + M2 * Kp;
+    for (int a = threadIdx.x; a < Kp / 2; a += NT) {
+        float2 xw = make_float2(0.f, 0.f);
+        if (a < Kact) {
+            int n = act[a];
+            double w = apply_ctf ? M[n] * C[n] : M[n];
+            xw = make_float2((float)(w * X[n].x), (float)(w * X[n].y));
+        }
+        for (int t = 0; t < T; t++) {
+            float fr = 0.f, fi = 0.f;
+            if (a < Kact) {
+                unsigned short pi = pidx[(long)t * Kact + a];
+                if (pi == 0xFFFF) {
+                    fr = xw.x;
+                    fi = xw.y;
+                } else {
+                    float2 cs = stab[pi & 0x7FFF];
+                    float sn = (pi & 0x8000) ? -cs.y : cs.y;
+                    fr = cs.x * xw.x - sn * xw.y;
+                    fi = cs.x * xw.y + sn * xw.x;
+                }
+            }
+            long o = ((long)i * T + t) * Kp + 2 * a;
+            if (precision == ROME_PREC_FP32) {
+                *(float2*)((float*)Aop + o) = make_float2(fr, fi);
+            } else {
+                __nv_bfloat162 h2 = __floats2bfloat162_rn(fr, fi);
+                *(__nv_bfloat162*)(Ah + o) = h2;
+                if (precision == ROME_PREC_BF16X3) {
+                    float2 hf = __bfloat1622float2(h2);
+                    *(__nv_bfloat162*)(Al + o) = __floats2bfloat162_rn(fr - hf.x, fi - hf.y);
+                }
+            }
+        }
+    }
+    if (threadIdx.x == 0)
+        for (int t = 0; t < T; t++) S[(long)i * T + t] = (float)s;
 }
 
 // coordinates of half-plane pixel n of a size x (size/2+1) FFTW image
@@ -296,22 +391,7 @@ __global__ void w2_kernel(int P, int Kact, int Kq, const int* __restrict__ act, 
     }
 }
 
-// ---------------------------------------------------------------------------
-// Posterior and significance (convertSquaredDifferencesToWeights,
-// :1077-1224, findAllSignificantPoints, :1226-1311), one CTA per particle.
-//
-// The selection must reproduce the reference exactly: sort the positive
-// weights, walk from the largest accumulating an FP64 running sum in that
-// order, stop once it exceeds adaptive_fraction * sum.  Only the largest
-// weights can be walked, so the CTA histograms the weights by their FP64
-// exponent (2048 buckets with counts and sums), keeps the top buckets whose
-// total safely exceeds the threshold, sorts those candidates in shared
-// memory (bitonic, descending) and walks them sequentially.  Particles with
-// more than SEL_CAP candidates are finished by select_fallback_kernel.
-constexpr int SEL_THREADS = 512;
-constexpr int SEL_CAP = 8192;
-constexpr int SEL_NB = 2048;
-
+// Layout of the hypothesis index e of one particle (exp_Mweight order).
 struct PostLayout {
     int T, notr, nor, npsi, ntr, K;
 };
@@ -346,432 +426,6 @@ __device__ TVal block_reduce_sum(TVal v, TVal* sh) {
     return r;
 }
 
-// descending bitonic sort of n (power of two) doubles, whole CTA
-__device__ void bitonic_desc(double* a, int n) {
-    for (int k = 2; k <= n; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = threadIdx.x; i < n; i += blockDim.x) {
-                int ixj = i ^ j;
-                if (ixj > i) {
-                    bool desc = (i & k) == 0;
-                    double x = a[i], y = a[ixj];
-                    if (desc ? (x < y) : (x > y)) {
-                        a[i] = y;
-                        a[ixj] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// part[i*8 + ...]: 0 min_diff2, 1 sum_weight, 2 significant_weight, 3 threshold,
-//                  4 max weight, 5 diff2 cut (no weight beyond it can be significant)
-// parti[i*8 + ...]: 0 best hypothesis, 1 nr walked, 2 overflow, 3 lowest candidate bucket
-// Weights are computed from diff2 (mode 0) or read from `wgiven` (mode 1,
-// for rome_gpu_select_significant); mode 0 can also store them to `wout`.
-__global__ void __launch_bounds__(SEL_THREADS)
-    post_select_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2, const double* __restrict__ pdir,
-                       const double* __restrict__ poff, double frac, double* __restrict__ part, int* __restrict__ parti,
-                       const double* __restrict__ wgiven, double* __restrict__ wout) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double* cand = (double*)smem_raw;                 // SEL_CAP
-    double* bsum = cand + SEL_CAP;                    // SEL_NB
-    int* bcnt = (int*)(bsum + SEL_NB);                // SEL_NB
-    __shared__ double red[32];
-    __shared__ float redf[32];
-    __shared__ int ncand, s_blow, s_nsig, s_over;
-    __shared__ double s_sig;
-    const int i = blockIdx.x;
-    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
-    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
-    const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
-
-    for (int b = threadIdx.x; b < SEL_NB; b += blockDim.x) {
-        bsum[b] = 0.0;
-        bcnt[b] = 0;
-    }
-    // ---- min over computed diff2 ----
-    double mn = 0.0;
-    if (mode == 0) {
-        float m = INFINITY;
-        for (long e = threadIdx.x; e < X; e += blockDim.x) m = fminf(m, d[e]);
-        for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
-        if ((threadIdx.x & 31) == 0) redf[threadIdx.x >> 5] = m;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            m = threadIdx.x < (blockDim.x >> 5) ? redf[threadIdx.x] : INFINITY;
-            for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
-            if (threadIdx.x == 0) redf[0] = m;
-        }
-        __syncthreads();
-        mn = (double)redf[0];
-        __syncthreads();
-    }
-    // ---- weights: sum, argmax (first in the reference's loop order), histogram ----
-    double sum = 0.0, maxw = DBL_MIN, maxpd = 0.0;
-    long best_lo = LONG_MAX, best_e = 0;
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        double w;
-        long lo;
-        if (mode == 0) {
-            int k, itr;
-            decode_e(e, L, k, itr, lo);
-            double pd = pdir[k] * po[k * L.ntr + itr];
-            float dv = d[e];
-            if (dv < INFINITY) maxpd = fmax(maxpd, pd);
-            w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
-            if (wout) wout[(long)i * X + e] = w;
-        } else {
-            w = wg[e];
-            lo = e;
-        }
-        sum += w;
-        if (w > maxw || (w == maxw && w > DBL_MIN && lo < best_lo)) {
-            maxw = w;
-            best_lo = lo;
-            best_e = e;
-        }
-        if (w > 0.0) {
-            int b = (int)(__double_as_longlong(w) >> 52);
-            atomicAdd(&bcnt[b], 1);
-            atomicAdd(&bsum[b], w);
-        }
-    }
-    // the reference initialises the running maximum to DBL_MIN with index 0
-    if (!(maxw > DBL_MIN)) {
-        best_lo = LONG_MAX;
-        best_e = 0;
-    }
-    sum = block_reduce_sum(sum, red);
-    if (mode == 1) sum = part[(long)i * 8 + 1];  // the caller's exp_sum_weight
-    // argmax reduction: (max weight, smallest loop-order index)
-    {
-        __shared__ double smax[32];
-        __shared__ long slo[32], se[32];
-        for (int off = 16; off > 0; off >>= 1) {
-            double ow = __shfl_down_sync(0xffffffffu, maxw, off);
-            long olo = __shfl_down_sync(0xffffffffu, best_lo, off);
-            long oe = __shfl_down_sync(0xffffffffu, best_e, off);
-            if (ow > maxw || (ow == maxw && olo < best_lo)) {
-                maxw = ow;
-                best_lo = olo;
-                best_e = oe;
-            }
-        }
-        if ((threadIdx.x & 31) == 0) {
-            smax[threadIdx.x >> 5] = maxw;
-            slo[threadIdx.x >> 5] = best_lo;
-            se[threadIdx.x >> 5] = best_e;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++)
-                if (smax[w] > smax[0] || (smax[w] == smax[0] && slo[w] < slo[0])) {
-                    smax[0] = smax[w];
-                    slo[0] = slo[w];
-                    se[0] = se[w];
-                }
-        }
-        __syncthreads();
-        maxw = smax[0];
-        best_e = se[0];
-        __syncthreads();
-    }
-    if (mode == 0) {
-        for (int off = 16; off > 0; off >>= 1) maxpd = fmax(maxpd, __shfl_down_sync(0xffffffffu, maxpd, off));
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxpd;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++) red[0] = fmax(red[0], red[w]);
-        }
-        __syncthreads();
-        maxpd = red[0];
-        __syncthreads();
-    }
-    const double thr = frac * sum;
-    // ---- candidate buckets: top buckets whose total exceeds thr with margin ----
-    if (threadIdx.x == 0) {
-        double cum = 0.0;
-        int blow = 0, cnt = 0;
-        for (int b = SEL_NB - 1; b >= 0; b--) {
-            cum += bsum[b];
-            cnt += bcnt[b];
-            blow = b;
-            if (cum > thr * (1.0 + 1e-9)) break;
-        }
-        s_blow = blow;
-        ncand = cnt;
-        s_over = cnt > SEL_CAP;
-        s_nsig = 0;
-        s_sig = 0.0;
-    }
-    __syncthreads();
-    const int blow = s_blow;
-    if (!s_over) {
-        const int cnt = ncand;
-        int n2 = 1;
-        while (n2 < cnt) n2 <<= 1;
-        __syncthreads();
-        if (threadIdx.x == 0) ncand = 0;
-        __syncthreads();
-        for (long e = threadIdx.x; e < X; e += blockDim.x) {
-            double w;
-            if (mode == 0) {
-                int k, itr;
-                long lo;
-                decode_e(e, L, k, itr, lo);
-                w = hyp_weight(d[e], mn, pdir[k], po[k * L.ntr + itr]);
-            } else {
-                w = wg[e];
-            }
-            if (w > 0.0 && (int)(__double_as_longlong(w) >> 52) >= blow) {
-                int q = atomicAdd(&ncand, 1);
-                if (q < SEL_CAP) cand[q] = w;
-            }
-        }
-        __syncthreads();
-        for (int q = cnt + threadIdx.x; q < n2; q += blockDim.x) cand[q] = 0.0;
-        __syncthreads();
-        bitonic_desc(cand, n2);
-        if (threadIdx.x == 0) {
-            double fw = 0.0, sig = 0.0;
-            int ns = 0;
-            bool stopped = false;
-            for (int q = 0; q < cnt; q++) {
-                ns++;
-                sig = cand[q];
-                fw += sig;
-                if (fw > thr) {
-                    stopped = true;
-                    break;
-                }
-            }
-            // stopping inside the candidates is guaranteed by the margin unless
-            // every positive weight is a candidate (then the walk is complete)
-            if (!stopped && blow > 0) s_over = 1;
-            s_sig = sig;
-            s_nsig = ns;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        double* pp = part + (long)i * 8;
-        int* pi = parti + (long)i * 8;
-        pp[0] = mn;
-        pp[1] = sum;
-        pp[2] = s_sig;
-        pp[3] = thr;
-        pp[4] = maxw;
-        // a significant weight needs pd * exp(-(d - mn)) >= sig
-        pp[5] = (s_sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / s_sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
-        pi[0] = (int)best_e;
-        pi[1] = s_nsig;
-        pi[2] = s_over;
-        pi[3] = blow;
-    }
-}
-
-// Completes the selection for particles with too many candidates: gathers
-// the candidate weights into a global scratch slot, sorts them there
-// (bitonic, descending) and walks them.  One CTA per listed particle.
-__global__ void __launch_bounds__(SEL_THREADS)
-    select_fallback_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2,
-                           const double* __restrict__ pdir, const double* __restrict__ poff,
-                           const double* __restrict__ wgiven, const int* __restrict__ list, long slot_len,
-                           double* __restrict__ scratch, double* __restrict__ part, int* __restrict__ parti) {
-    const int i = list[blockIdx.x];
-    double* buf = scratch + (long)blockIdx.x * slot_len;
-    __shared__ int ncand;
-    const double mn = part[(long)i * 8 + 0];
-    const double thr = part[(long)i * 8 + 3];
-    const int blow = parti[(long)i * 8 + 3];
-    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
-    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
-    const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
-    if (threadIdx.x == 0) ncand = 0;
-    __syncthreads();
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        double w;
-        if (mode == 0) {
-            int k, itr;
-            long lo;
-            decode_e(e, L, k, itr, lo);
-            w = hyp_weight(d[e], mn, pdir[k], po[k * L.ntr + itr]);
-        } else {
-            w = wg[e];
-        }
-        if (w > 0.0 && (int)(__double_as_longlong(w) >> 52) >= blow) buf[atomicAdd(&ncand, 1)] = w;
-    }
-    __syncthreads();
-    const int cnt = ncand;
-    long n2 = 1;
-    while (n2 < cnt) n2 <<= 1;
-    for (long q = cnt + threadIdx.x; q < n2; q += blockDim.x) buf[q] = 0.0;
-    __syncthreads();
-    for (long k = 2; k <= n2; k <<= 1) {
-        for (long j = k >> 1; j > 0; j >>= 1) {
-            for (long q = threadIdx.x; q < n2; q += blockDim.x) {
-                long ixj = q ^ j;
-                if (ixj > q) {
-                    bool desc = (q & k) == 0;
-                    double x = buf[q], y = buf[ixj];
-                    if (desc ? (x < y) : (x > y)) {
-                        buf[q] = y;
-                        buf[ixj] = x;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    }
-    if (threadIdx.x == 0) {
-        double fw = 0.0, sig = 0.0;
-        int ns = 0;
-        for (int q = 0; q < cnt; q++) {
-            ns++;
-            sig = buf[q];
-            fw += sig;
-            if (fw > thr) break;
-        }
-        part[(long)i * 8 + 2] = sig;
-        parti[(long)i * 8 + 1] = ns;
-        parti[(long)i * 8 + 2] = 0;
-    }
-}
-
-// exp_Mcoarse_significant (findAllSignificantPoints pass 0, :1285-1296)
-__global__ void mcoarse_kernel(int P, long X, int T, int notr, int nor, int npsi, int ntr, int K,
-                               const float* __restrict__ diff2, const double* __restrict__ pdir,
-                               const double* __restrict__ poff, const double* __restrict__ part,
-                               char* __restrict__ mcoarse) {
-    const int i = blockIdx.x;
-    PostLayout L{T, notr, nor, npsi, ntr, K};
-    const double mn = part[(long)i * 8 + 0], sig = part[(long)i * 8 + 2];
-    const float* d = diff2 + (long)i * X;
-    const double* po = poff + (long)i * K * ntr;
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        int k, itr;
-        long lo;
-        decode_e(e, L, k, itr, lo);
-        double w = hyp_weight(d[e], mn, pdir[k], po[k * ntr + itr]);
-        mcoarse[(long)i * X + e] = w >= sig;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// updateOtherParams (src/map2d_optimizer.cpp:1417-1663): for every
-// significant hypothesis, w = weight / sum_weight and
-//   wsum_sigma2_noise[group][ires] += w |ctf P_j - X_t|^2   (ires = Mresol_fine > -1)
-//   exp_wsum_norm_correction[i]    += w |ctf P_j - X_t|^2
-// plus the class / offset / group sums.  Grid (pixel chunks, particles);
-// each thread owns PIX pixels and keeps their sums in registers.
-template <int NT, int PIX>
-__global__ void __launch_bounds__(NT)
-    wsum_kernel(int P, long X, int T, int notr, int nor, int npsi, int ntr, int K, int F, int csF, int cs, int oriF,
-                const float* __restrict__ diff2, const double* __restrict__ pdir, const double* __restrict__ poff,
-                const double* __restrict__ part, const int* __restrict__ jvalid, const double2* __restrict__ Fimg,
-                const double* __restrict__ lctf, int apply_ctf, const double2* __restrict__ proj,
-                const int* __restrict__ actidx, int Kact, const double2* __restrict__ shifts,
-                const double2* __restrict__ tab, double sampling, const int* __restrict__ Mresol,
-                const int* __restrict__ group, const double2* __restrict__ oldoff, const double2* __restrict__ trans,
-                const double2* __restrict__ unused, const double* __restrict__ priorx,
-                const double* __restrict__ priory, double* __restrict__ wsn, double* __restrict__ normcorr,
-                double* __restrict__ wk) {
-    const int i = blockIdx.y;
-    const int n0 = blockIdx.x * NT * PIX;
-    PostLayout L{T, notr, nor, npsi, ntr, K};
-    const double mn = part[(long)i * 8 + 0], sumw = part[(long)i * 8 + 1], sig = part[(long)i * 8 + 2];
-    const double dcut = part[(long)i * 8 + 5];
-    const float* d = diff2 + (long)i * X;
-    const double* po = poff + (long)i * K * ntr;
-    __shared__ long qe[NT];
-    __shared__ double qw[NT];
-    __shared__ int qn;
-    __shared__ double spec[1024];
-    __shared__ double red[32];
-    double acc[PIX];
-#pragma unroll
-    for (int p = 0; p < PIX; p++) acc[p] = 0.0;
-    double sumwd = 0.0;
-    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) spec[q] = 0.0;
-    const int g = group[i];
-    const double2 oo = oldoff[i];
-    for (long c0 = 0; c0 < X; c0 += NT) {
-        if (threadIdx.x == 0) qn = 0;
-        __syncthreads();
-        long e = c0 + threadIdx.x;
-        if (e < X) {
-            float dv = d[e];
-            if (dv < INFINITY && (double)dv <= dcut) {
-                int k, itr;
-                long lo;
-                decode_e(e, L, k, itr, lo);
-                double w = hyp_weight(dv, mn, pdir[k], po[k * ntr + itr]);
-                if (w >= sig) {
-                    int q = atomicAdd(&qn, 1);
-                    qe[q] = e;
-                    qw[q] = w / sumw;
-                }
-            }
-        }
-        __syncthreads();
-        const int nq = qn;
-        for (int q = 0; q < nq; q++) {
-            const long eq = qe[q];
-            const double w = qw[q];
-            const int j = (int)(eq / T), t = (int)(eq - (long)j * T);
-            const double2 sh = shifts[t];
-            const double2* Pj = proj + (long)j * Kact;
-#pragma unroll
-            for (int p = 0; p < PIX; p++) {
-                int n = n0 + threadIdx.x + p * NT;
-                if (n < F && Mresol[n] > -1) {
-                    double x, y;
-                    pixel_xy(n, csF, cs, x, y);
-                    double2 v = table_shift(x, y, sh, Fimg[(long)i * F + n], tab, sampling);
-                    int a = actidx[n];
-                    double2 pv = a >= 0 ? Pj[a] : make_double2(0.0, 0.0);
-                    double c = lctf[(long)i * F + n];
-                    double pr = apply_ctf ? dmul(pv.x, c) : pv.x;
-                    double pim = apply_ctf ? dmul(pv.y, c) : pv.y;
-                    double dr = dsub(pr, v.x), di = dsub(pim, v.y);
-                    double wd = dmul(w, dadd(dmul(dr, dr), dmul(di, di)));
-                    acc[p] += wd;
-                    sumwd += wd;
-                }
-            }
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
-                int k = j / (npsi * nor);
-                double2 tr = trans[t];
-                atomicAdd(&wk[0 * K + k], w);
-                atomicAdd(&wk[1 * K + k], w);
-                atomicAdd(&wk[2 * K + k], w * (oo.x + tr.x));
-                atomicAdd(&wk[3 * K + k], w * (oo.y + tr.y));
-                double ox = priorx[k] - oo.x - tr.x, oy = priory[k] - oo.y - tr.y;
-                atomicAdd(&wk[5 * K + g], w);
-                atomicAdd(&wk[4 * K + k], w * (ox * ox + oy * oy));
-            }
-        }
-        __syncthreads();
-    }
-    // bin the per-pixel sums into resolution shells, then into the group spectrum
-#pragma unroll
-    for (int p = 0; p < PIX; p++) {
-        int n = n0 + threadIdx.x + p * NT;
-        if (n < F) {
-            int ires = Mresol[n];
-            if (ires > -1 && ires < 1024 && acc[p] != 0.0) atomicAdd(&spec[ires], acc[p]);
-        }
-    }
-    sumwd = block_reduce_sum(sumwd, red);
-    __syncthreads();
-    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT)
-        if (spec[q] != 0.0) atomicAdd(&wsn[(long)g * oriF + q], spec[q]);
-    if (threadIdx.x == 0 && sumwd != 0.0) atomicAdd(&normcorr[i], sumwd);
-}
-
 // backProjection preparation (src/map2d_optimizer.cpp:1670-1737): origin of
 // Minvsigma2 restored, Minvsigma2 -> 1 without MAP, CTF -> 1 without CTF
 // correction; nomask image times ctf*Minvsigma2 and Mctf2 = ctf^2*Minvsigma2.
@@ -792,130 +446,6 @@ __global__ void bp_prep_kernel(int P, int F, const double* __restrict__ Fnr, con
     }
 }
 
-// backProjection (src/map2d_optimizer.cpp:1760-1872): for orientation j sum
-// w * X_nomask_t * ctf * Minvsigma2 and w * ctf^2 * Minvsigma2 over every
-// significant (particle, translation), then MyBackProjector::backrotate2D
-// (src/reconstruct.cpp:1353-1500) scatters the slice into the class's
-// 2D backprojector with FP64 atomics.  Grid (pixel chunks, orientations).
-template <int NT, int PIX>
-__global__ void __launch_bounds__(NT)
-    bp_kernel(int P, long X, int T, int notr, int nor, int npsi, int ntr, int K, int F, int csF, int cs,
-              const float* __restrict__ diff2, const double* __restrict__ pdir, const double* __restrict__ poff,
-              const double* __restrict__ part, const int* __restrict__ jvalid, const double2* __restrict__ Fnm,
-              const double* __restrict__ Mctf2, const double2* __restrict__ shifts, const double2* __restrict__ tab,
-              double sampling, const double4* __restrict__ rot, int r_max, int pad, int padF,
-              double2* __restrict__ bp_data, double* __restrict__ bp_weight, long vox) {
-    const int j = blockIdx.y;
-    if (!jvalid[j]) return;
-    const int n0 = blockIdx.x * NT * PIX;
-    const int nrot = npsi * nor;
-    const int k = j / nrot;
-    __shared__ int qi[NT], qt[NT];
-    __shared__ double qw[NT];
-    __shared__ int qn;
-    double sr[PIX], si[PIX], sw[PIX];
-#pragma unroll
-    for (int p = 0; p < PIX; p++) sr[p] = si[p] = sw[p] = 0.0;
-    const long nent = (long)P * T;
-    for (long c0 = 0; c0 < nent; c0 += NT) {
-        if (threadIdx.x == 0) qn = 0;
-        __syncthreads();
-        long q = c0 + threadIdx.x;
-        if (q < nent) {
-            int i = (int)(q / T), t = (int)(q - (long)i * T);
-            long e = (long)j * T + t;
-            float dv = diff2[(long)i * X + e];
-            const double* pp = part + (long)i * 8;
-            if (dv < INFINITY && (double)dv <= pp[5]) {
-                int itr = t / notr;
-                double w = hyp_weight(dv, pp[0], pdir[k], poff[((long)i * K + k) * ntr + itr]);
-                if (w >= pp[2]) {
-                    int s = atomicAdd(&qn, 1);
-                    qi[s] = i;
-                    qt[s] = t;
-                    qw[s] = w / pp[1];
-                }
-            }
-        }
-        __syncthreads();
-        const int nq = qn;
-        for (int s = 0; s < nq; s++) {
-            const int i = qi[s], t = qt[s];
-            const double w = qw[s];
-            const double2 sh = shifts[t];
-#pragma unroll
-            for (int p = 0; p < PIX; p++) {
-                int n = n0 + threadIdx.x + p * NT;
-                if (n < F) {
-                    double x, y;
-                    pixel_xy(n, csF, cs, x, y);
-                    double2 v = table_shift(x, y, sh, Fnm[(long)i * F + n], tab, sampling);
-                    sr[p] = dadd(sr[p], dmul(v.x, w));
-                    si[p] = dadd(si[p], dmul(v.y, w));
-                    sw[p] = dadd(sw[p], dmul(Mctf2[(long)i * F + n], w));
-                }
-            }
-        }
-        __syncthreads();
-    }
-    // backrotate2D scatter
-    const double4 A = rot[j];
-    const int shift = -(int)((float)pad / 2.0f);
-    const int max_r2 = r_max * r_max;
-    double2* D = bp_data + (long)k * vox;
-    double* W = bp_weight + (long)k * vox;
-#pragma unroll
-    for (int p = 0; p < PIX; p++) {
-        int n = n0 + threadIdx.x + p * NT;
-        if (n >= F) continue;
-        int row = n / csF, x = n - row * csF;
-        int y, first_x;
-        if (row <= r_max) {
-            y = row;
-            first_x = 0;
-        } else if (row >= cs - r_max) {
-            y = row - cs;
-            first_x = 1;
-        } else
-            continue;
-        if (x < first_x || x > r_max || x * x + y * y > max_r2) continue;
-        double mw = sw[p];
-        if (!(mw > 0.)) continue;
-        double vr = sr[p], vi = si[p];
-        double xp = dadd(dmul(A.x, (double)x), dmul(A.y, (double)y));
-        double yp = dadd(dmul(A.z, (double)x), dmul(A.w, (double)y));
-        if (xp < 0) {
-            xp = -xp;
-            yp = -yp;
-            vi = -1 * vi;
-        }
-        int x0 = (int)floor(xp);
-        double fx = dsub(xp, (double)x0);
-        int y0 = (int)floor(yp);
-        double fy = dsub(yp, (double)y0);
-        y0 -= shift;
-        int y1 = y0 + 1;
-        double mfx = dsub(1., fx), mfy = dsub(1., fy);
-        double dd00 = dmul(mfy, mfx), dd01 = dmul(mfy, fx), dd10 = dmul(fy, mfx), dd11 = dmul(fy, fx);
-        double* t00 = (double*)(D + (long)y0 * padF + x0);
-        double* t10 = (double*)(D + (long)y1 * padF + x0);
-        atomicAdd(t00 + 0, dmul(dd00, vr));
-        atomicAdd(t00 + 1, dmul(dd00, vi));
-        atomicAdd(t00 + 2, dmul(dd01, vr));
-        atomicAdd(t00 + 3, dmul(dd01, vi));
-        atomicAdd(t10 + 0, dmul(dd10, vr));
-        atomicAdd(t10 + 1, dmul(dd10, vi));
-        atomicAdd(t10 + 2, dmul(dd11, vr));
-        atomicAdd(t10 + 3, dmul(dd11, vi));
-        double* w00 = W + (long)y0 * padF + x0;
-        double* w10 = W + (long)y1 * padF + x0;
-        atomicAdd(w00 + 0, dmul(dd00, mw));
-        atomicAdd(w00 + 1, dmul(dd01, mw));
-        atomicAdd(w10 + 0, dmul(dd10, mw));
-        atomicAdd(w10 + 1, dmul(dd11, mw));
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Significant hypotheses as a compact list.  updateOtherParams and
 // backProjection only touch hypotheses with weight >= significant_weight
@@ -926,52 +456,6 @@ struct SigEntry {
     int e;     // hypothesis index in the exp_Mweight layout
     double w;  // weight / exp_sum_weight
 };
-
-__global__ void __launch_bounds__(256)
-    sig_list_kernel(int P, long X, PostLayout L, const float* __restrict__ diff2, const double* __restrict__ pdir,
-                    const double* __restrict__ poff, const double* __restrict__ part, int* __restrict__ counter,
-                    int cap, SigEntry* __restrict__ list, int* __restrict__ seg) {
-    const int i = blockIdx.x;
-    const double mn = part[(long)i * 8 + 0], sumw = part[(long)i * 8 + 1], sig = part[(long)i * 8 + 2];
-    const double dcut = part[(long)i * 8 + 5];
-    const float* d = diff2 + (long)i * X;
-    const double* po = poff + (long)i * L.K * L.ntr;
-    __shared__ int cnt, base;
-    if (threadIdx.x == 0) cnt = 0;
-    __syncthreads();
-    // pass 1: count
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        float dv = d[e];
-        if (dv < INFINITY && (double)dv <= dcut) {
-            int k, itr;
-            long lo;
-            decode_e(e, L, k, itr, lo);
-            if (hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]) >= sig) atomicAdd(&cnt, 1);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        base = atomicAdd(counter, cnt);
-        seg[2 * i] = base;
-        seg[2 * i + 1] = cnt;
-        cnt = 0;
-    }
-    __syncthreads();
-    // pass 2: write (order inside the segment is irrelevant to every consumer's sums up to rounding)
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        float dv = d[e];
-        if (dv < INFINITY && (double)dv <= dcut) {
-            int k, itr;
-            long lo;
-            decode_e(e, L, k, itr, lo);
-            double w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
-            if (w >= sig) {
-                int q = base + atomicAdd(&cnt, 1);
-                if (q < cap) list[q] = SigEntry{i, (int)e, w / sumw};
-            }
-        }
-    }
-}
 
 // counting sort of the list by orientation j = e / T
 __global__ void count_by_j_kernel(int n, int T, const SigEntry* __restrict__ list, int* __restrict__ cnt) {
@@ -1189,52 +673,6 @@ __global__ void __launch_bounds__(NT)
         atomicAdd(w10 + 0, dmul(dd10, mw));
         atomicAdd(w10 + 1, dmul(dd11, mw));
     }
-}
-
-// ---------------------------------------------------------------------------
-// host wrappers of the selection
-inline int launch_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P, long X, PostLayout L, const float* diff2,
-                          const double* pdir, const double* poff, double frac, double* part, int* parti,
-                          const double* wgiven, double* wout) {
-    size_t smem = sizeof(double) * (SEL_CAP + SEL_NB) + sizeof(int) * SEL_NB;
-    ROME_CUDA(cudaFuncSetAttribute(post_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    post_select_kernel<<<P, SEL_THREADS, smem, st>>>(mode, X, L, diff2, pdir, poff, frac, part, parti, wgiven, wout);
-    ROME_CHECK_LAUNCH();
-    std::vector<int> hpi((size_t)P * 8);
-    ROME_CUDA(cudaMemcpyAsync(hpi.data(), parti, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
-    ROME_CUDA(cudaStreamSynchronize(st));
-    std::vector<int> over;
-    for (int i = 0; i < P; i++)
-        if (hpi[(size_t)i * 8 + 2]) over.push_back(i);
-    if (over.empty()) return 1;
-    int nlaunch = 1;
-    long n2 = 1;
-    while (n2 < X) n2 <<= 1;
-    const int slots = (int)std::min<size_t>(over.size(), 64);
-    double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)slots * n2);
-    int* dli = ctx->ws[S_LIST].as<int>(over.size());
-    ROME_CUDA(cudaMemcpyAsync(dli, over.data(), sizeof(int) * over.size(), cudaMemcpyHostToDevice, st));
-    for (size_t b = 0; b < over.size(); b += slots) {
-        int nb = (int)std::min<size_t>(slots, over.size() - b);
-        select_fallback_kernel<<<nb, SEL_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dli + b, n2,
-                                                          scratch, part, parti);
-        ROME_CHECK_LAUNCH();
-        nlaunch++;
-    }
-    return nlaunch;
-}
-
-inline int post_select(RomeGpuCtx* ctx, cudaStream_t st, int P, long X, int T, int notr, int nor, int npsi, int ntr,
-                        const float* diff2, const double* pdir, const double* poff, int K, double frac, double* part,
-                        int* parti, double* wout) {
-    PostLayout L{T, notr, nor, npsi, ntr, K};
-    return launch_select(ctx, st, 0, P, X, L, diff2, pdir, poff, frac, part, parti, nullptr, wout);
-}
-
-inline void select_given_weights(RomeGpuCtx* ctx, cudaStream_t st, int n, long len, const double* w, double frac,
-                                 double* part, int* parti) {
-    PostLayout L{1, 1, 1, 1, 1, 1};
-    launch_select(ctx, st, 1, n, len, L, nullptr, nullptr, nullptr, frac, part, parti, w, nullptr);
 }
 
 }  // namespace rome

@@ -89,11 +89,13 @@ __global__ void __launch_bounds__(SG_THREADS, 2)
     for (int i = 0; i < 8; i++) {
         int m = m0 + (i < 4 ? ty * 4 + i : 64 + ty * 4 + i - 4);
         if (m >= M) continue;
+        float rmin = INFINITY;
 #pragma unroll
         for (int j = 0; j < 8; j++) {
             int n = n0 + (j < 4 ? tx * 4 + j : 64 + tx * 4 + j - 4);
-            if (n < N) epi(m, n, acc[i][j]);
+            if (n < N) rmin = fminf(rmin, epi(m, n, acc[i][j]));
         }
+        epi.finish_row(m, rmin);
     }
 }
 

@@ -226,6 +226,7 @@ __global__ void __launch_bounds__(128, 1)
     if (!timed_out) {
         const int row = m0 + warp * 32 + lane;
         const uint32_t lane_base = tmem_base + ((uint32_t)(warp * 32) << 16);
+        float rmin = INFINITY;
 #pragma unroll 1
         for (int c = 0; c < BN; c += 16) {
             float v[16];
@@ -234,10 +235,11 @@ __global__ void __launch_bounds__(128, 1)
 #pragma unroll
                 for (int q = 0; q < 16; q++) {
                     int n = n0 + c + q;
-                    if (n < N) epi(row, n, v[q]);
+                    if (n < N) rmin = fminf(rmin, epi(row, n, v[q]));
                 }
             }
         }
+        if (row < M) epi.finish_row(row, rmin);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

@@ -22,6 +22,7 @@
 #include "estep_kernels.cuh"
 #include "gemm_simt.cuh"
 #include "gemm_tc.cuh"
+#include "select_kernels.cuh"
 
 using namespace rome;
 
@@ -155,6 +156,11 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         double2* dShift = nullptr;
         double2* dPh = nullptr;
         int* dJvalid = nullptr;
+        // significant-hypothesis list (filled by the selection of each pass)
+        int* dCounter = ctx->ws[S_LISTCNT].as<int>((size_t)2 * K * npsi * 2 * 4 + 4);
+        int* dSeg = ctx->ws[S_SEG].as<int>((size_t)2 * P);
+        int listcap = std::max(1024, P * 64), nsigtot = 0;
+        SigEntry* dList = nullptr;
 
         for (int ipass = 0; ipass < npass; ipass++) {
             const int cs = (ipass == 0 && in->adaptive_oversampling > 0) ? in->coarse_size : cur;
@@ -255,9 +261,13 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             float* dS = ctx->ws[S_S].as<float>((size_t)M);
             float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
             prof.begin(ROME_PHASE_SHIFT);
-            shift_operand_kernel<<<dim3(g.T, P), 256, 0, st>>>(P, g.T, g.F, g.csF, cs, g.Kact, g.Kp, dFimg, dLctf,
-                                                              dMinv, apply_ctf ? 1 : 0, dAct, dShift, dPh, dA, dS,
-                                                              ctx->precision);
+            unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)g.T * g.Kact);
+            phase_index_kernel<<<(unsigned)(((long)g.T * g.Kact + 255) / 256), 256, 0, st>>>(
+                g.T, g.Kact, g.csF, cs, dAct, dShift, ctx->shift_sampling, dPidx);
+            prof.launched(ROME_PHASE_SHIFT);
+            shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, g.T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                                                           apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
+                                                           ctx->precision);
             prof.launched(ROME_PHASE_SHIFT);
             w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
             prof.launched(ROME_PHASE_SHIFT);
@@ -285,8 +295,10 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
 
             // ---- cross term + fused diff2 epilogue ----
             dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * g.X);
+            unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
+            ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
             Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJvalid, g.T, g.J, g.X, g.notr, g.nor, ntr, ncoarse,
-                         ipass > 0 ? dMcoarse : nullptr};
+                         ipass > 0 ? dMcoarse : nullptr, dRowMin};
             prof.begin(ROME_PHASE_CROSS_GEMM);
             if (!tc) {
                 sgemm_tn(st, (int)M, g.J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
@@ -301,14 +313,23 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             // ---- posterior: min, FP64 weights, sum, argmax, significance ----
             double* dW = nullptr;
             if (out->weight[ipass]) dW = ctx->ws[S_WCHK].as<double>((size_t)P * g.X);
+            const PostLayout Lp{g.T, g.notr, g.nor, npsi, ntr, K};
             prof.begin(ROME_PHASE_POSTERIOR);
-            int nl = post_select(ctx, st, P, g.X, g.T, g.notr, g.nor, npsi, ntr, dDiff2, dPdir, dPoff, K,
-                                 in->adaptive_fraction, dPart, dPartI, dW);
-            prof.launched(ROME_PHASE_POSTERIOR, nl);
+            for (;;) {
+                dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
+                SelectResult sr = run_select(ctx, st, 0, P, g.X, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
+                                             dPart, dPartI, nullptr, dW, dList, dCounter, listcap, dSeg, dRowMin);
+                prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
+                nsigtot = sr.nlist;
+                if (sr.nlist <= listcap) break;
+                listcap = sr.nlist;  // every segment fits on the second run
+            }
             if (ipass == 0 && (npass > 1 || out->Mcoarse_significant)) {
-                mcoarse_kernel<<<P, 256, 0, st>>>(P, g.X, g.T, g.notr, g.nor, npsi, ntr, K, dDiff2, dPdir, dPoff,
-                                                  dPart, dMcoarse);
-                prof.launched(ROME_PHASE_POSTERIOR);
+                ROME_CUDA(cudaMemsetAsync(dMcoarse, 0, (size_t)P * ncoarse, st));
+                if (nsigtot > 0) {
+                    mcoarse_from_list_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.X, dList, dMcoarse);
+                    prof.launched(ROME_PHASE_POSTERIOR);
+                }
             }
             prof.end(ROME_PHASE_POSTERIOR);
 
@@ -373,23 +394,9 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         double* dWk = ctx->ws[S_WSUMK].as<double>((size_t)5 * K + G + 1);
         ROME_CUDA(cudaMemsetAsync(dWsn, 0, sizeof(double) * ((size_t)G * oriF + P), st));
         ROME_CUDA(cudaMemsetAsync(dWk, 0, sizeof(double) * ((size_t)5 * K + G + 1), st));
-        // compact list of significant hypotheses (weight >= significant_weight)
-        const PostLayout L{g.T, g.notr, g.nor, npsi, ntr, K};
-        int* dCounter = ctx->ws[S_LISTCNT].as<int>((size_t)2 * g.J + 4);
-        int* dSeg = ctx->ws[S_SEG].as<int>((size_t)2 * P);
-        int cap = std::max(1024, P * 64), nsigtot = 0;
-        SigEntry* dList = nullptr;
+        // significant hypotheses of the last pass are in dList (particle segments)
+        const int cap = listcap;
         prof.begin(ROME_PHASE_WSUM);
-        for (int attempt = 0; attempt < 2; attempt++) {
-            dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)cap * 2);
-            ROME_CUDA(cudaMemsetAsync(dCounter, 0, sizeof(int), st));
-            sig_list_kernel<<<P, 256, 0, st>>>(P, g.X, L, dDiff2, dPdir, dPoff, dPart, dCounter, cap, dList, dSeg);
-            prof.launched(ROME_PHASE_WSUM);
-            ROME_CUDA(cudaMemcpyAsync(&nsigtot, dCounter, sizeof(int), cudaMemcpyDeviceToHost, st));
-            ROME_CUDA(cudaStreamSynchronize(st));
-            if (nsigtot <= cap) break;
-            cap = nsigtot;  // every particle's segment fits on the second pass
-        }
         {
             const int NT = 256, PIX = 8;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
@@ -478,7 +485,8 @@ extern "C" int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, con
         std::vector<double> hp((size_t)n * 8, 0.0);
         for (int i = 0; i < n; i++) hp[(size_t)i * 8 + 1] = sum_weight[i];
         ROME_CUDA(cudaMemcpyAsync(dPart, hp.data(), sizeof(double) * n * 8, cudaMemcpyHostToDevice, st));
-        select_given_weights(ctx, st, n, len, dW, adaptive_fraction, dPart, dPartI);
+        run_select(ctx, st, 1, n, len, PostLayout{1, 1, 1, 1, 1, 1}, nullptr, nullptr, nullptr, adaptive_fraction,
+                   dPart, dPartI, dW, nullptr, nullptr, nullptr, 0, nullptr);
         std::vector<double> hpart((size_t)n * 8);
         std::vector<int> hparti((size_t)n * 8);
         ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * n * 8, cudaMemcpyDeviceToHost, st));

@@ -1,0 +1,453 @@
+// Posterior and significance selection, one CTA per particle
+// (convertSquaredDifferencesToWeights, src/map2d_optimizer.cpp:1077-1224;
+// findAllSignificantPoints, :1226-1311; the 3D versions are
+// src/map3d_optimizer.cpp:1610-1931).
+//
+// The reference sorts all positive weights and walks from the largest,
+// summing in FP64 until the running sum exceeds f * sum (f =
+// adaptive_fraction).  Only weights w >= t0 = (1 - f) * sum / X can ever be
+// walked: the X hypotheses below t0 hold less than (1 - f) * sum, so the
+// weights at or above t0 already exceed f * sum.  The CTA therefore keeps
+// just those candidates (with their hypothesis index), sorts them in shared
+// memory and walks them sequentially, reproducing the reference's FP64
+// accumulation order exactly.  t0 carries a relative margin of 1e-6 of
+// (1 - f) * sum, far above the rounding of the running sum; if the walk ever
+// ran out of candidates, or there are more than SEL2_CAP of them, the
+// particle is finished by select_fallback2_kernel in global memory.
+//
+// The same kernel emits the significant hypotheses (w >= significant
+// weight) as the particle's contiguous segment of the SigEntry list used by
+// updateOtherParams and backProjection.
+#pragma once
+
+#include "estep_kernels.cuh"
+
+namespace rome {
+
+constexpr int SEL2_THREADS = 512;
+constexpr int SEL2_CAP = 8192;
+
+// part[i*8]:  0 min_diff2, 1 sum_weight, 2 significant_weight, 3 threshold f*sum,
+//             4 max weight, 5 diff2 cut for weights >= significant_weight, 6 t0, 7 diff2 cut for t0
+// parti[i*8]: 0 best hypothesis, 1 nr walked, 2 overflow, 3 list count, 4 list base
+__device__ __forceinline__ void bitonic_desc_kv(double* key, int* val, int n) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += blockDim.x) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    bool desc = (i & k) == 0;
+                    double x = key[i], y = key[ixj];
+                    if (desc ? (x < y) : (x > y)) {
+                        key[i] = y;
+                        key[ixj] = x;
+                        int t = val[i];
+                        val[i] = val[ixj];
+                        val[ixj] = t;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+__global__ void __launch_bounds__(SEL2_THREADS)
+    post_select2_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2,
+                        const double* __restrict__ pdir, const double* __restrict__ poff, double frac,
+                        double* __restrict__ part, int* __restrict__ parti, const double* __restrict__ wgiven,
+                        double* __restrict__ wout, SigEntry* __restrict__ list, int* __restrict__ counter, int cap,
+                        int* __restrict__ seg, const unsigned* __restrict__ rowmin) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* key = (double*)smem_raw;           // SEL2_CAP
+    int* idx = (int*)(key + SEL2_CAP);         // SEL2_CAP
+    __shared__ double red[32];
+    __shared__ float redf[32];
+    __shared__ double smax[32];
+    __shared__ long slo[32], se[32];
+    __shared__ int ncand, s_nsig, s_over, s_m, s_base;
+    __shared__ double s_sig;
+    const int i = blockIdx.x;
+    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
+    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
+    const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
+
+    // ---- min over computed diff2 ----
+    double mn = 0.0;
+    if (mode == 0 && rowmin) {
+        // folded into the GEMM epilogue
+        unsigned k = rowmin[i];
+        mn = k == 0xFFFFFFFFu ? (double)INFINITY : (double)key_float(k);
+    } else if (mode == 0) {
+        float m = INFINITY;
+        for (long e = threadIdx.x; e < X; e += blockDim.x) m = fminf(m, d[e]);
+        for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
+        if ((threadIdx.x & 31) == 0) redf[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            m = threadIdx.x < (blockDim.x >> 5) ? redf[threadIdx.x] : INFINITY;
+            for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
+            if (threadIdx.x == 0) redf[0] = m;
+        }
+        __syncthreads();
+        mn = (double)redf[0];
+        __syncthreads();
+    }
+    // ---- weights: sum, argmax (first in the reference's loop order), max prior ----
+    double sum = 0.0, maxw = DBL_MIN, maxpd = 0.0;
+    long best_lo = LONG_MAX, best_e = 0;
+    if (mode == 0) {
+        // orientation-major sweep: one division per orientation, the loop-order
+        // index only on ties (argmax of the reference's loop, :1140-1146)
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
+        const int J = (int)(X / L.T), nrot = L.npsi * L.nor;
+        const int tsh = L.notr == 1 ? 0 : (L.notr == 4 ? 2 : 31);
+        for (int j = warp; j < J; j += nwarp) {
+            const int k = j / nrot;
+            const double pdk = pdir[k];
+            const double* pok = po + k * L.ntr;
+            for (int t = lane; t < L.T; t += 32) {
+                const long e = (long)j * L.T + t;
+                const int itr = tsh < 31 ? (t >> tsh) : t / L.notr;
+                float dv = d[e];
+                if (dv < INFINITY) maxpd = fmax(maxpd, pdk * pok[itr]);
+                double w = hyp_weight(dv, mn, pdk, pok[itr]);
+                if (wout) wout[(long)i * X + e] = w;
+                sum += w;
+                if (w >= maxw && w > DBL_MIN) {
+                    int kk, it2;
+                    long lo;
+                    decode_e(e, L, kk, it2, lo);
+                    if (w > maxw || lo < best_lo) {
+                        maxw = w;
+                        best_lo = lo;
+                        best_e = e;
+                    }
+                }
+            }
+        }
+    } else {
+        for (long e = threadIdx.x; e < X; e += blockDim.x) {
+            double w = wg[e];
+            sum += w;
+            if (w > maxw || (w == maxw && w > DBL_MIN && e < best_lo)) {
+                maxw = w;
+                best_lo = e;
+                best_e = e;
+            }
+        }
+    }
+    if (!(maxw > DBL_MIN)) {
+        best_lo = LONG_MAX;
+        best_e = 0;
+    }
+    sum = block_reduce_sum(sum, red);
+    if (mode == 1) sum = part[(long)i * 8 + 1];  // the caller's exp_sum_weight
+    for (int off = 16; off > 0; off >>= 1) {
+        double ow = __shfl_down_sync(0xffffffffu, maxw, off);
+        long olo = __shfl_down_sync(0xffffffffu, best_lo, off);
+        long oe = __shfl_down_sync(0xffffffffu, best_e, off);
+        if (ow > maxw || (ow == maxw && olo < best_lo)) {
+            maxw = ow;
+            best_lo = olo;
+            best_e = oe;
+        }
+        maxpd = fmax(maxpd, __shfl_down_sync(0xffffffffu, maxpd, off));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smax[threadIdx.x >> 5] = maxw;
+        slo[threadIdx.x >> 5] = best_lo;
+        se[threadIdx.x >> 5] = best_e;
+        red[threadIdx.x >> 5] = maxpd;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            if (smax[w] > smax[0] || (smax[w] == smax[0] && slo[w] < slo[0])) {
+                smax[0] = smax[w];
+                slo[0] = slo[w];
+                se[0] = se[w];
+            }
+            red[0] = fmax(red[0], red[w]);
+        }
+        ncand = 0;
+        s_over = 0;
+    }
+    __syncthreads();
+    maxw = smax[0];
+    best_e = se[0];
+    maxpd = red[0];
+    const double thr = frac * sum;
+    const double t0 = frac < 1.0 ? (1.0 - frac) * sum / (double)X * (1.0 - 1e-6) : 0.0;
+    const double dlim0 = (mode == 0 && t0 > 0.0 && maxpd > 0.0) ? mn + log(maxpd / t0) + 1e-6 * (1.0 + fabs(mn))
+                                                                : INFINITY;
+    __syncthreads();
+    // ---- candidates w >= t0 ----
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        double w;
+        if (mode == 0) {
+            float dv = d[e];
+            if (!(dv < INFINITY) || (double)dv > dlim0) continue;
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
+        } else {
+            w = wg[e];
+        }
+        if (w > 0.0 && w >= t0) {
+            int q = atomicAdd(&ncand, 1);
+            if (q < SEL2_CAP) {
+                key[q] = w;
+                idx[q] = (int)e;
+            }
+        }
+    }
+    __syncthreads();
+    const int cnt = ncand;
+    if (cnt > SEL2_CAP) {
+        if (threadIdx.x == 0) s_over = 1;
+    } else {
+        int n2 = 1;
+        while (n2 < cnt) n2 <<= 1;
+        for (int q = cnt + threadIdx.x; q < n2; q += blockDim.x) {
+            key[q] = -1.0;
+            idx[q] = -1;
+        }
+        __syncthreads();
+        bitonic_desc_kv(key, idx, n2);
+        if (threadIdx.x == 0) {
+            double fw = 0.0, sig = 0.0;
+            int ns = 0;
+            bool stopped = false;
+            for (int q = 0; q < cnt; q++) {
+                ns++;
+                sig = key[q];
+                fw += sig;
+                if (fw > thr) {
+                    stopped = true;
+                    break;
+                }
+            }
+            if (!stopped && t0 > 0.0) s_over = 1;  // cannot happen with the margin; finish in global memory
+            s_sig = sig;
+            s_nsig = ns;
+            int m = ns;
+            while (m < cnt && key[m] >= sig) m++;  // ties of the significant weight are significant too
+            s_m = (ns > 0) ? m : 0;
+        }
+    }
+    __syncthreads();
+    // ---- significant list segment ----
+    if (!s_over && list) {
+        if (threadIdx.x == 0) {
+            s_base = atomicAdd(counter, s_m);
+            seg[2 * i] = s_base;
+            seg[2 * i + 1] = s_m;
+        }
+        __syncthreads();
+        const double inv = 1.0 / sum;
+        (void)inv;
+        for (int q = threadIdx.x; q < s_m; q += blockDim.x)
+            if (s_base + q < cap) list[s_base + q] = SigEntry{i, idx[q], key[q] / sum};
+    }
+    if (threadIdx.x == 0) {
+        double* pp = part + (long)i * 8;
+        int* pi = parti + (long)i * 8;
+        pp[0] = mn;
+        pp[1] = sum;
+        pp[2] = s_over ? 0.0 : s_sig;
+        pp[3] = thr;
+        pp[4] = maxw;
+        pp[5] = (!s_over && s_sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / s_sig) + 1e-6 * (1.0 + fabs(mn))
+                                                        : INFINITY;
+        pp[6] = t0;
+        pp[7] = dlim0;
+        pi[0] = (int)best_e;
+        pi[1] = s_over ? 0 : s_nsig;
+        pi[2] = s_over;
+        pi[3] = s_over ? 0 : s_m;
+        pi[4] = s_over ? 0 : s_base;
+    }
+}
+
+// Completes the selection of listed particles in global memory: gathers the
+// candidates (w >= t0, or every positive weight when the shared-memory walk
+// ran out), sorts them (bitonic, descending) and walks them.  One CTA per
+// listed particle, each with its own scratch slot.
+__global__ void __launch_bounds__(SEL2_THREADS)
+    select_fallback2_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2,
+                            const double* __restrict__ pdir, const double* __restrict__ poff,
+                            const double* __restrict__ wgiven, const int* __restrict__ plist, long slot_len,
+                            double* __restrict__ scratch, double* __restrict__ part, int* __restrict__ parti) {
+    const int i = plist[blockIdx.x];
+    double* buf = scratch + (long)blockIdx.x * slot_len;
+    __shared__ int ncand;
+    double* pp = part + (long)i * 8;
+    const double mn = pp[0], thr = pp[3];
+    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
+    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
+    const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
+    if (threadIdx.x == 0) ncand = 0;
+    __syncthreads();
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        double w;
+        if (mode == 0) {
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            w = hyp_weight(d[e], mn, pdir[k], po[k * L.ntr + itr]);
+        } else {
+            w = wg[e];
+        }
+        if (w > 0.0) buf[atomicAdd(&ncand, 1)] = w;
+    }
+    __syncthreads();
+    const int cnt = ncand;
+    long n2 = 1;
+    while (n2 < cnt) n2 <<= 1;
+    for (long q = cnt + threadIdx.x; q < n2; q += blockDim.x) buf[q] = -1.0;
+    __syncthreads();
+    for (long k = 2; k <= n2; k <<= 1) {
+        for (long j = k >> 1; j > 0; j >>= 1) {
+            for (long q = threadIdx.x; q < n2; q += blockDim.x) {
+                long ixj = q ^ j;
+                if (ixj > q) {
+                    bool desc = (q & k) == 0;
+                    double x = buf[q], y = buf[ixj];
+                    if (desc ? (x < y) : (x > y)) {
+                        buf[q] = y;
+                        buf[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        double fw = 0.0, sig = 0.0;
+        int ns = 0;
+        for (int q = 0; q < cnt; q++) {
+            ns++;
+            sig = buf[q];
+            fw += sig;
+            if (fw > thr) break;
+        }
+        pp[2] = sig;
+        parti[(long)i * 8 + 1] = ns;
+        double maxpd = 0.0;
+        if (mode == 0)
+            for (int k = 0; k < L.K; k++)
+                for (int t = 0; t < L.ntr; t++) maxpd = fmax(maxpd, pdir[k] * po[k * L.ntr + t]);
+        pp[5] = (sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
+    }
+}
+
+// list segments of listed particles (the ones the fallback finished)
+__global__ void __launch_bounds__(256)
+    sig_list_some_kernel(const int* __restrict__ plist, long X, PostLayout L, const float* __restrict__ diff2,
+                         const double* __restrict__ pdir, const double* __restrict__ poff,
+                         const double* __restrict__ part, int* __restrict__ counter, int cap,
+                         SigEntry* __restrict__ list, int* __restrict__ seg) {
+    const int i = plist[blockIdx.x];
+    const double mn = part[(long)i * 8 + 0], sumw = part[(long)i * 8 + 1], sig = part[(long)i * 8 + 2];
+    const double dcut = part[(long)i * 8 + 5];
+    const float* d = diff2 + (long)i * X;
+    const double* po = poff + (long)i * L.K * L.ntr;
+    __shared__ int cnt, base;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        float dv = d[e];
+        if (dv < INFINITY && (double)dv <= dcut) {
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            if (hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]) >= sig) atomicAdd(&cnt, 1);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        base = atomicAdd(counter, cnt);
+        seg[2 * i] = base;
+        seg[2 * i + 1] = cnt;
+        cnt = 0;
+    }
+    __syncthreads();
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        float dv = d[e];
+        if (dv < INFINITY && (double)dv <= dcut) {
+            int k, itr;
+            long lo;
+            decode_e(e, L, k, itr, lo);
+            double w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
+            if (w >= sig) {
+                int q = base + atomicAdd(&cnt, 1);
+                if (q < cap) list[q] = SigEntry{i, (int)e, w / sumw};
+            }
+        }
+    }
+}
+
+// exp_Mcoarse_significant from the list (pass 0: the hypothesis index is the coarse index)
+__global__ void mcoarse_from_list_kernel(int n, long X, const SigEntry* __restrict__ list, char* __restrict__ mcoarse) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) mcoarse[(long)list[q].i * X + list[q].e] = 1;
+}
+
+struct SelectResult {
+    int nlist;     // total significant entries
+    int launches;  // kernels launched
+};
+
+// Posterior + selection + list for P particles.  list/seg/counter may be null
+// (selection only).  Returns the list size; the caller re-runs with a larger
+// capacity when it exceeds `cap` (entries past cap are not written).
+inline SelectResult run_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P, long X, PostLayout L,
+                               const float* diff2, const double* pdir, const double* poff, double frac, double* part,
+                               int* parti, const double* wgiven, double* wout, SigEntry* list, int* counter, int cap,
+                               int* seg, const unsigned* rowmin = nullptr) {
+    SelectResult res{0, 0};
+    size_t smem = (sizeof(double) + sizeof(int)) * SEL2_CAP;
+    ROME_CUDA(cudaFuncSetAttribute(post_select2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (counter) ROME_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+    post_select2_kernel<<<P, SEL2_THREADS, smem, st>>>(mode, X, L, diff2, pdir, poff, frac, part, parti, wgiven, wout,
+                                                       list, counter, cap, seg, rowmin);
+    ROME_CHECK_LAUNCH();
+    res.launches++;
+    std::vector<int> hpi((size_t)P * 8);
+    ROME_CUDA(cudaMemcpyAsync(hpi.data(), parti, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
+    int hcount = 0;
+    if (counter) ROME_CUDA(cudaMemcpyAsync(&hcount, counter, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ROME_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> over;
+    for (int i = 0; i < P; i++)
+        if (hpi[(size_t)i * 8 + 2]) over.push_back(i);
+    if (!over.empty()) {
+        long n2 = 1;
+        while (n2 < X) n2 <<= 1;
+        const int slots = (int)std::min<size_t>(over.size(), 64);
+        double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)slots * n2);
+        int* dli = ctx->ws[S_LIST].as<int>(over.size());
+        ROME_CUDA(cudaMemcpyAsync(dli, over.data(), sizeof(int) * over.size(), cudaMemcpyHostToDevice, st));
+        for (size_t b = 0; b < over.size(); b += slots) {
+            int nb = (int)std::min<size_t>(slots, over.size() - b);
+            select_fallback2_kernel<<<nb, SEL2_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dli + b, n2,
+                                                                scratch, part, parti);
+            ROME_CHECK_LAUNCH();
+            res.launches++;
+        }
+        if (counter && mode == 0) {
+            sig_list_some_kernel<<<(int)over.size(), 256, 0, st>>>(dli, X, L, diff2, pdir, poff, part, counter, cap,
+                                                                  list, seg);
+            ROME_CHECK_LAUNCH();
+            res.launches++;
+            ROME_CUDA(cudaMemcpyAsync(&hcount, counter, sizeof(int), cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaStreamSynchronize(st));
+        }
+    }
+    res.nlist = hcount;
+    return res;
+}
+
+}  // namespace rome
