@@ -215,6 +215,24 @@ int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2
 int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, const double* weights, const double* sum_weight,
                                 double adaptive_fraction, double* significant_weight, double* nr_significant);
 
+/* Same selection and results as rome_gpu_select_significant, without any
+ * device allocation: every device buffer lives in one fixed array compiled
+ * into the library (about 16.5 MiB per device).  No counterpart in the
+ * reference; it is for callers that must not allocate device memory during
+ * the call (all HBM handed to their own pool, a hard memory budget, or no
+ * implicit synchronisation from cudaMalloc/cudaFree allowed).
+ * Limits: n <= ROME_SELECT_STATIC_MAX_IMAGES, n * len <=
+ * ROME_SELECT_STATIC_MAX_WEIGHTS; beyond them it returns ROME_ERR_ARG.
+ * The first call on a device looks the array up (cudaGetSymbolAddress) and
+ * should come before any stream capture on that device.  Calls on one
+ * device share the array, so overlapping calls would race: the function
+ * takes a process-wide lock and returns after its stream work is done. */
+#define ROME_SELECT_STATIC_MAX_IMAGES 4096
+#define ROME_SELECT_STATIC_MAX_WEIGHTS (1 << 20)
+int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const double* weights,
+                                       const double* sum_weight, double adaptive_fraction,
+                                       double* significant_weight, double* nr_significant);
+
 /* ---------------------------------------------------------------------
  * M-step reconstruction of one class from its accumulated backprojector.
  * Replaces MAPModel::reconstruction (src/map_model.cpp:233-241) ->

@@ -109,6 +109,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_create", "rome_gpu_destroy", "rome_gpu_last_error", "rome_gpu_set_precision",
     "rome_gpu_abi_version", "rome_gpu_set_projectors", "rome_gpu_get_backprojector",
     "rome_gpu_set_backprojector", "rome_gpu_map2d_estep_pool", "rome_gpu_select_significant",
+    "rome_gpu_select_significant_static",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings",
 ]
 
@@ -138,6 +139,8 @@ def load_library():
     lib.rome_gpu_set_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
     lib.rome_gpu_map2d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap2dPool), C.POINTER(RomeMap2dPoolOut)]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
+    lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
+                                                       _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]
     lib.rome_gpu_get_timings.argtypes = [C.c_void_p, C.POINTER(RomeGpuTimings)]
     lib.rome_gpu_reset_timings.argtypes = [C.c_void_p]

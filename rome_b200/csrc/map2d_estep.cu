@@ -17,6 +17,8 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "estep_kernels.cuh"
@@ -496,5 +498,153 @@ extern "C" int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, con
             significant_weight[i] = hpart[(size_t)i * 8 + 2];
             nr_significant[i] = hparti[(size_t)i * 8 + 1];
         }
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Significance selection without device allocation.
+//
+// rome_gpu_select_significant_static runs the same kernels as
+// rome_gpu_select_significant, but every device buffer it touches is carved
+// from one fixed array compiled into this library (g_select_static below)
+// instead of the context's grow-on-demand workspace.  It is meant for callers
+// that must not allocate device memory during the call: a host that has
+// handed all free HBM to its own pool allocator, a caller running inside a
+// memory budget it cannot exceed, or code that must not trigger the implicit
+// device synchronisation a cudaMalloc/cudaFree can cause.
+//
+// Limits: n <= ROME_SELECT_STATIC_MAX_IMAGES and n * len <=
+// ROME_SELECT_STATIC_MAX_WEIGHTS; larger requests return ROME_ERR_ARG and
+// touch nothing.  The array is 8 MiB of weights + 8 MiB of sort scratch for
+// rows whose candidate set does not fit in shared memory + per-row scalars.
+//
+// The first call on each device looks the array's device address up
+// (cudaGetSymbolAddress, which may load the module on that device); make
+// that first call before any stream capture on the device.  All calls on one
+// device share the array, so two calls overlapping in time would race on it:
+// the entry point holds a process-wide lock and returns only after its
+// stream work has finished, which serialises calls from different host
+// threads.
+namespace {
+
+constexpr size_t kStaticAlign = 256;
+constexpr size_t align_up(size_t v) { return (v + kStaticAlign - 1) / kStaticAlign * kStaticAlign; }
+
+constexpr size_t kOffW = 0;  // caller weights [n][len] double
+constexpr size_t kOffFB = kOffW + align_up(sizeof(double) * ROME_SELECT_STATIC_MAX_WEIGHTS);  // fallback sort slots
+constexpr size_t kOffPart = kOffFB + align_up(sizeof(double) * ROME_SELECT_STATIC_MAX_WEIGHTS);
+constexpr size_t kOffPartI = kOffPart + align_up(sizeof(double) * 8 * ROME_SELECT_STATIC_MAX_IMAGES);
+constexpr size_t kOffList = kOffPartI + align_up(sizeof(int) * 8 * ROME_SELECT_STATIC_MAX_IMAGES);
+constexpr size_t kOffCount = kOffList + align_up(sizeof(int) * ROME_SELECT_STATIC_MAX_IMAGES);
+constexpr size_t kOffIO = kOffCount + kStaticAlign;  // sum_weight in, [sig | nsig] out
+constexpr size_t kStaticBytes = kOffIO + align_up(sizeof(double) * 2 * ROME_SELECT_STATIC_MAX_IMAGES);
+
+static __device__ __align__(256) unsigned char g_select_static[kStaticBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_lock;
+unsigned char* g_static_base[kMaxDevices] = {};
+
+// per-row scalars start from zero, except the caller's sum of weights
+__global__ void static_prep_kernel(int n, const double* __restrict__ sumw, double* __restrict__ part,
+                                   int* __restrict__ parti) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int k = 0; k < 8; k++) {
+        part[(long)i * 8 + k] = k == 1 ? sumw[i] : 0.0;
+        parti[(long)i * 8 + k] = 0;
+    }
+}
+
+// rows whose candidates overflowed shared memory, compacted in one block
+__global__ void static_overflow_kernel(int n, const int* __restrict__ parti, int* __restrict__ list,
+                                       int* __restrict__ count) {
+    __shared__ int cnt;
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        if (parti[(long)i * 8 + 2]) list[atomicAdd(&cnt, 1)] = i;
+    __syncthreads();
+    if (threadIdx.x == 0) *count = cnt;
+}
+
+__global__ void static_finish_kernel(int n, const double* __restrict__ part, const int* __restrict__ parti,
+                                     double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = part[(long)i * 8 + 2];
+    out[n + i] = (double)parti[(long)i * 8 + 1];
+}
+
+}  // namespace
+
+extern "C" int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const double* weights,
+                                                  const double* sum_weight, double adaptive_fraction,
+                                                  double* significant_weight, double* nr_significant) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(n > 0 && len > 0 && weights && sum_weight && significant_weight && nr_significant,
+                     "bad arguments");
+        ROME_REQUIRE(n <= ROME_SELECT_STATIC_MAX_IMAGES,
+                     "select_significant_static: %d images exceed the static limit of %d", n,
+                     ROME_SELECT_STATIC_MAX_IMAGES);
+        ROME_REQUIRE(len <= (long)ROME_SELECT_STATIC_MAX_WEIGHTS / n,
+                     "select_significant_static: %d x %ld weights exceed the static limit of %d", n, len,
+                     ROME_SELECT_STATIC_MAX_WEIGHTS);
+        ROME_REQUIRE(ctx->device >= 0 && ctx->device < kMaxDevices, "device %d out of range", ctx->device);
+        std::lock_guard<std::mutex> lock(g_static_lock);
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        if (!g_static_base[ctx->device]) {
+            void* p = nullptr;
+            ROME_CUDA(cudaGetSymbolAddress(&p, g_select_static));
+            g_static_base[ctx->device] = (unsigned char*)p;
+        }
+        unsigned char* base = g_static_base[ctx->device];
+        double* dW = (double*)(base + kOffW);
+        double* dFB = (double*)(base + kOffFB);
+        double* dPart = (double*)(base + kOffPart);
+        int* dPartI = (int*)(base + kOffPartI);
+        int* dList = (int*)(base + kOffList);
+        int* dCount = (int*)(base + kOffCount);
+        double* dIO = (double*)(base + kOffIO);
+        cudaStream_t st = ctx->stream;
+
+        ROME_CUDA(cudaMemcpyAsync(dW, weights, sizeof(double) * n * len, cudaMemcpyHostToDevice, st));
+        ROME_CUDA(cudaMemcpyAsync(dIO, sum_weight, sizeof(double) * n, cudaMemcpyHostToDevice, st));
+        static_prep_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, dIO, dPart, dPartI);
+        ROME_CHECK_LAUNCH();
+        const size_t smem = (sizeof(double) + sizeof(int)) * SEL2_CAP;
+        ROME_CUDA(cudaFuncSetAttribute(post_select2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const PostLayout L{1, 1, 1, 1, 1, 1};
+        post_select2_kernel<<<n, SEL2_THREADS, smem, st>>>(1, len, L, nullptr, nullptr, nullptr, adaptive_fraction,
+                                                           dPart, dPartI, dW, nullptr, nullptr, nullptr, 0, nullptr,
+                                                           nullptr);
+        ROME_CHECK_LAUNCH();
+        static_overflow_kernel<<<1, 256, 0, st>>>(n, dPartI, dList, dCount);
+        ROME_CHECK_LAUNCH();
+        int nover = 0;
+        ROME_CUDA(cudaMemcpyAsync(&nover, dCount, sizeof(int), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        int launches = 3;
+        if (nover > 0) {
+            long n2 = 1;
+            while (n2 < len) n2 <<= 1;  // len <= the weight limit, so one slot always fits
+            const int slots = (int)std::min<long>(nover, (long)ROME_SELECT_STATIC_MAX_WEIGHTS / n2);
+            for (int b = 0; b < nover; b += slots) {
+                const int nb = std::min(slots, nover - b);
+                select_fallback2_kernel<<<nb, SEL2_THREADS, 0, st>>>(1, len, L, nullptr, nullptr, nullptr, dW,
+                                                                    dList + b, n2, dFB, dPart, dPartI);
+                ROME_CHECK_LAUNCH();
+                launches++;
+            }
+        }
+        static_finish_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, dPart, dPartI, dIO);
+        ROME_CHECK_LAUNCH();
+        launches++;
+        ROME_CUDA(cudaMemcpyAsync(significant_weight, dIO, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaMemcpyAsync(nr_significant, dIO + n, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        ctx->phase_launches[ROME_PHASE_POSTERIOR] += launches;
+        ctx->total_launches += launches;
     });
 }
