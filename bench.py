@@ -39,8 +39,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="map2d_cfg2")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "bf16", "bf16x3"])
-    ap.add_argument("--pool", type=int, default=1000)
+    ap.add_argument("--precision", default="bf16", choices=["fp32", "bf16", "bf16x3"])
+    ap.add_argument("--pool", type=int, default=2000)
     ap.add_argument("--particles", type=int, default=0, help="override the particle count (debug)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -120,7 +120,7 @@ def run_ours(args):
     N = pool.nr_images
     ctx = GpuContext(local, args.precision, profile=True)
     ctx.set_projectors(proj, pool.ori_size, r_max)
-    pools = [subset(pool, lo, min(N, lo + args.pool)) for lo in range(0, N, args.pool)]
+    pools = [pin_pool(subset(pool, lo, min(N, lo + args.pool))) for lo in range(0, N, args.pool)]
 
     def step(dev_inputs):
         res = []
@@ -148,13 +148,20 @@ def run_ours(args):
         torch.cuda.synchronize()
         ms = t0.elapsed_time(t1)
     timings = ctx.get_timings()
-    # end to end through the C ABI with host buffers (H2D + D2H inside)
+    # end to end through the C ABI with pinned host buffers (H2D + D2H inside)
     torch.cuda.synchronize()
-    e0 = time.perf_counter()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
     for _ in range(max(1, args.steps)):
         step(None)
+    e1.record()
     torch.cuda.synchronize()
-    e_ms = (time.perf_counter() - e0) * 1e3
+    e_ms = e0.elapsed_time(e1)
+    # the plain FP32 GPU E-step on the first pool: the metric's comparison arm
+    fp32 = plain_fp32(args, ctx, pools[0], last[0], proj, r_max) if rank == 0 else None
     ms_t = torch.tensor([ms, e_ms], device="cuda")
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -177,18 +184,20 @@ def run_ours(args):
         "data": "synthetic (seeded random-blob templates, CTF, white noise)",
         "config": {"workload": args.config, "particles_per_gpu": N, "image": w.ori_size, "classes": w.n_classes,
                    "psi": int(round(360 / w.psi_step)), "translations": int(pool.nr_trans), "pool": args.pool,
-                   "precision": args.precision, "inputs": "larger than L2 (no flush)",
-                   "pose_agreement_vs_truth": round(pose_ok, 4)},
+                   "precision": args.precision, "proposal": "none (exhaustive search)",
+                   "inputs": "larger than L2 (no flush)", "pose_agreement_vs_truth": round(pose_ok, 4)},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
                 "h2d_bytes_per_step": int(sum(ctx.h2d_bytes(q) for q in pools)),
                 "d2h_bytes_per_step": int(sum(ctx.d2h_bytes(q) for q in pools))},
         "gpu_launches": int(timings["total_launches"]),
         "roofline": {"bound": "tensor", "achieved": round(achieved, 2), "peak": bf16, "unit": "TFLOP/s",
-                     "frac": round(achieved / bf16, 4), "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "cross_gemm"},
+                     "frac": round(achieved / bf16, 4), "traffic": cross_gemm_traffic(args, pools[0].nr_images),
+                     "peak_kind": peak_kind, "kernel": "cross_gemm (tc_gemm_kernel, diff2 epilogue)"},
         "phases_ms": {k: round(v["ms"], 3) for k, v in timings.items() if isinstance(v, dict)},
         "clocks": clk.summary(),
     }
+    if fp32 is not None:
+        line["plain_fp32"] = fp32
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w)
     ctx.close()
@@ -196,6 +205,60 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def pin_pool(p):
+    """The pool's image arrays copied into page-locked host memory (the
+    end-to-end figure copies them to the device inside the timed region)."""
+    import dataclasses
+
+    import torch
+    from rome_b200.map2d import DEVICE_FIELDS
+    rep = {}
+    for name in DEVICE_FIELDS:
+        a = np.ascontiguousarray(getattr(p, name), np.float64)
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        rep[name] = t.numpy()
+    return dataclasses.replace(p, **rep)
+
+
+def plain_fp32(args, ctx, pool, res_main, proj, r_max):
+    """Particles/s of the plain FP32 E-step (CUDA-core contraction) on one
+    pool, and the pose agreement of the benchmarked mode with it."""
+    import torch
+    from rome_b200.map2d import GpuContext
+    if args.precision == "fp32":
+        return None
+    with GpuContext(ctx.device, "fp32") as c32:
+        c32.set_projectors(proj, pool.ori_size, r_max)
+        dev = c32.stage_pool(pool)
+        c32.map2d_estep_pool(dev)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        r32 = c32.map2d_estep_pool(dev)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+    same = ((r32["cls"] == res_main["cls"]) & (r32["psi"] == res_main["psi"]) & (r32["xoff"] == res_main["xoff"])
+            & (r32["yoff"] == res_main["yoff"]))
+    return {"value": round(pool.nr_images / (ms / 1e3), 2), "unit": UNIT, "particles": pool.nr_images,
+            "pose_agreement": round(float(same.mean()), 5)}
+
+
+def cross_gemm_traffic(args, pool_particles):
+    """DRAM bytes per launch of the cross-term GEMM from the committed ncu
+    capture (profiles/cross_gemm_traffic.json), scaled to this pool size by
+    the number of rows (particles x translations) the launch processes."""
+    path = os.path.join(ROOT, "profiles", "cross_gemm_traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    if d.get("workload") != args.config or d.get("precision") != args.precision:
+        return None
+    return int(d["dram_bytes_per_launch"] * pool_particles / d["pool"])
 
 
 _W = {}
@@ -241,29 +304,83 @@ def oracle_rate(w, target_seconds: float = 15.0, cores: int = 0):
                       f"{dt:.1f} s wall"}
 
 
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "map2d_bench")
+
+
+def reference_rate(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str):
+    """Particles/s of the reference's own MAP2D E-step (oracle/_ref/map2d_bench:
+    the reference sources compiled unchanged, every OpenMP thread of the host)
+    on a dataset of the same workload: iteration 1 through the reference's
+    driver, then iteration 2's expectationSomeParticles() timed per pool at
+    full image size with all classes searched.  The first `warm_pools` pools
+    are not counted."""
+    from rome_b200.synthetic import Map2dSpec, write_dataset_2d
+    npools = warm_pools + timed_pools
+    spec = Map2dSpec(n_particles=pool * npools, size=w.ori_size, n_classes=w.n_classes, n_blobs=w.n_blobs,
+                     blob_sigma=w.blob_sigma, max_shift=w.max_shift, defocus=w.defocus, pixel=w.pixel, snr=w.snr,
+                     seed=w.seed + 101)
+    star = write_dataset_2d(os.path.join(tmpdir, "data"), spec)
+    cmd = [REF_BENCH, "-i", star, "-K", str(w.n_classes), "-angpix", str(w.pixel), "-psi_step",
+           str(int(round(w.psi_step))), "-offset_range", str(w.offset_range), "-offset_step", str(w.offset_step),
+           "-oversampling", "0", "-ctf", "1", "-pool", str(pool), "-time_pools", str(npools)]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, cwd=tmpdir)
+    if out.returncode != 0:
+        raise RuntimeError(f"map2d_bench exited {out.returncode}: {out.stderr[-300:]}")
+    pools, threads, cur = [], 0, 0
+    for ln in out.stdout.splitlines():
+        kv = dict(x.split("=") for x in ln.split()[1:] if "=" in x)
+        if ln.startswith("map2d_bench_pool"):
+            pools.append((int(kv["particles"]), float(kv["estep_s"])))
+        elif ln.startswith("map2d_bench "):
+            threads, cur = int(kv["threads"]), int(kv["current_size"])
+    timed = pools[warm_pools:]
+    n = sum(p for p, _ in timed)
+    t = sum(x for _, x in timed)
+    return {"value": round(n / t, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n} particles ({len(timed)} pools of {pool}) of {w.ori_size}x{w.ori_size}, K={w.n_classes}, "
+                      f"{int(round(360 / w.psi_step))} psi x translations +-{w.offset_range} step {w.offset_step}, "
+                      f"current_size {cur}, reference expectationSomeParticles() timed with dtime(), "
+                      f"{t:.1f} s; {warm_pools} warm-up pools not counted"}, t / max(len(timed), 1)
+
+
 def cpu_baseline(args, w):
+    """The reported CPU baseline: the reference itself when oracle/_ref was
+    built, else the oracle port."""
+    import tempfile
     try:
+        if os.path.exists(REF_BENCH):
+            with tempfile.TemporaryDirectory(prefix="rome_refbench_") as tmp:
+                return reference_rate(w, pool=16, warm_pools=1, timed_pools=4, tmpdir=tmp)[0]
         return oracle_rate(w, target_seconds=15.0)
     except Exception as e:  # the baseline is reported, never required
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
 
 def run_reference(args):
-    """The reference arm: the CPU implementation on every host core, same
-    workload and metric; rank 0 only."""
+    """The reference arm: the reference's own CPU E-step (oracle/_ref, or the
+    oracle port where the reference could not be built) on every host core,
+    same workload and metric; rank 0 only, the other ranks exit at once."""
+    import tempfile
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from rome_b200.workload import CONFIGS
     w = CONFIGS[args.config]
-    rates = []
-    for _ in range(args.warmup + args.steps) if args.steps <= 1 else range(args.steps):
-        rates.append(oracle_rate(w, target_seconds=20.0))
-    best = rates[-1]
+    if os.path.exists(REF_BENCH):
+        # one pool of 16 particles per step; warm-up pools are run and dropped
+        steps = max(1, min(args.steps, 16))
+        warm = max(0, min(args.warmup, 4))
+        with tempfile.TemporaryDirectory(prefix="rome_refbench_") as tmp:
+            best, s_per_step = reference_rate(w, pool=16, warm_pools=warm, timed_pools=steps, tmpdir=tmp)
+    else:
+        best = oracle_rate(w, target_seconds=20.0)
+        s_per_step = None
     line = {"metric": METRIC, "value": best["value"], "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": args.config, "image": w.ori_size, "classes": w.n_classes},
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(s_per_step * 1e3, 3) if s_per_step else None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": args.config, "image": w.ori_size, "classes": w.n_classes,
+                       "step": "one pool of 16 particles"},
             "cpu_baseline": best,
             "e2e": {"value": best["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

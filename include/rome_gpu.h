@@ -206,6 +206,103 @@ typedef struct {
 
 int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2dPoolOut* out);
 
+/* ---------------------------------------------------------------------
+ * MAP3D E-step for one pool of particles: both sampling passes,
+ * updateOtherParams and backProjection.  Replaces
+ * Map3dOptimizer_old::expectationSomeParticles minus storeWeightedSums
+ * (src/map3d_optimizer.cpp:883-953): preShiftedImagesCtfsAndInvSigma2s,
+ * getReferenceAllOrientations (:956-985), getAllSquaredDifferences
+ * (coarse :1195-1259, fine :1261-1372), convertSquaredDifferencesToWeights
+ * (:1610-1810), findAllSignificantPoints (:1812-1931), updateOtherParams
+ * (:2059-2236, CoarseAndFineSearch::updateModel :1484-1602) and
+ * backProjection (:2242-2506, MyBackProjector::backproject
+ * src/reconstruct.cpp:977-1164).  Maximum-likelihood mode with
+ * adaptive_oversampling 1 (the reference's 3D path always has the fine
+ * pass); cross-correlation mode and scale correction return
+ * ROME_ERR_UNSUPPORTED.  Projectors must be set with ref_dim 3.
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int nr_images;
+    int ori_size, current_size, coarse_size;
+    int nr_classes, iclass_min, iclass_max;
+    int nr_groups;
+    int adaptive_oversampling;       /* 1 */
+    int nr_dir, nr_psi, nr_trans;    /* coarse grid: HEALPix directions, psi, translations */
+    /* samplingGrid.setOrientation of every (dir, psi), per pass:
+     * [nr_dir][nr_psi][nr_over_rot][3] = (rot, tilt, psi) in degrees;
+     * nr_over_rot = 1 in pass 0, 8 in pass 1 */
+    const double* angles[2];
+    /* samplingGrid.exp_over_trans_x/y per pass: [nr_trans][nr_over_trans] (1 / 4) */
+    const double* over_trans_x[2];
+    const double* over_trans_y[2];
+    const double* trans_x;           /* sampler3d.getTranslation: [nr_trans] */
+    const double* trans_y;
+    /* particle data at current_size (Fourier half-planes), as in RomeMap2dPool */
+    const double* Fimg_real;
+    const double* Fimg_imag;
+    const double* Fimg_nomask_real;
+    const double* Fimg_nomask_imag;
+    const double* Fctf;
+    const double* highres_Xi2;
+    const double* old_offsetx;
+    const double* old_offsety;
+    const int* group;
+    const double* sigma2_noise;      /* [G][ori/2+1] */
+    const int* Mresol_fine;
+    const int* Mresol_coarse;
+    const double* pdf_class;         /* [K] */
+    const double* pdf_direction;     /* [K][nr_dir] */
+    const double* prior_offsetx_class;
+    const double* prior_offsety_class;
+    double sigma2_offset;
+    double sigma2_fudge;
+    double adaptive_fraction;
+    int do_ctf_correction;
+    int refs_are_ctf_corrected;
+    int do_map;
+    int do_scale_correction;         /* must be 0 */
+    int do_cross_correlation;        /* must be 0 */
+    int inputs_on_device;
+} RomeMap3dPool;
+
+typedef struct {
+    /* per particle, final pass (NULL to skip) */
+    double* min_diff2;
+    double* sum_weight;
+    double* significant_weight;
+    double* wsum_norm_correction;
+    double* pmax;
+    int* cls;                        /* 1-based */
+    double* rot;
+    double* tilt;
+    double* psi;
+    double* xoff;
+    double* yoff;
+    double* nr_sign;                 /* coarse-pass NR_SIGN */
+    /* model sums, accumulated */
+    double* wsum_sigma2_noise;       /* [G][ori/2+1] */
+    double* wsum_pdf_class;          /* [K] */
+    double* wsum_pdf_direction;      /* [K][nr_dir] */
+    double* wsum_sigma2_offset;      /* [1] */
+    double* wsum_sumw_group;         /* [G] */
+    /* optional checkpoints (NULL to skip) */
+    double* pass_min_diff2[2];       /* [P] */
+    double* pass_sum_weight[2];      /* [P] */
+    double* pass_significant_weight[2]; /* [P] */
+    double* coarse_diff2;            /* [P][K][nr_dir][nr_psi][nr_trans], INT_MIN where not computed */
+    char* Mcoarse_significant;       /* [P][K * nr_dir * nr_psi * nr_trans] */
+    /* fine-pass hypotheses in the reference's list order: per particle
+     * fine_count[i] records of (coarse index (k,dir,psi,trans) * 32 +
+     * over_rot * 4 + over_trans, diff2, weight); capacity fine_capacity */
+    long fine_capacity;
+    int* fine_count;                 /* [P] */
+    long* fine_index;
+    double* fine_diff2;
+    double* fine_weight;
+} RomeMap3dPoolOut;
+
+int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* in, RomeMap3dPoolOut* out);
+
 /* Significance selection on given weights (findAllSignificantPoints,
  * src/map2d_optimizer.cpp:1226-1311 and src/map3d_optimizer.cpp:1812-1931):
  * for each of n rows of `len` weights, sort the positive weights, walk from

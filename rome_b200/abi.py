@@ -74,6 +74,37 @@ class RomeMap2dPoolOut(C.Structure):
     ]
 
 
+class RomeMap3dPool(C.Structure):
+    _fields_ = [
+        ("nr_images", C.c_int), ("ori_size", C.c_int), ("current_size", C.c_int), ("coarse_size", C.c_int),
+        ("nr_classes", C.c_int), ("iclass_min", C.c_int), ("iclass_max", C.c_int), ("nr_groups", C.c_int),
+        ("adaptive_oversampling", C.c_int), ("nr_dir", C.c_int), ("nr_psi", C.c_int), ("nr_trans", C.c_int),
+        ("angles", _DP * 2), ("over_trans_x", _DP * 2), ("over_trans_y", _DP * 2),
+        ("trans_x", _DP), ("trans_y", _DP),
+        ("Fimg_real", _DP), ("Fimg_imag", _DP), ("Fimg_nomask_real", _DP), ("Fimg_nomask_imag", _DP),
+        ("Fctf", _DP), ("highres_Xi2", _DP), ("old_offsetx", _DP), ("old_offsety", _DP), ("group", _IP),
+        ("sigma2_noise", _DP), ("Mresol_fine", _IP), ("Mresol_coarse", _IP),
+        ("pdf_class", _DP), ("pdf_direction", _DP), ("prior_offsetx_class", _DP), ("prior_offsety_class", _DP),
+        ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
+        ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
+        ("do_scale_correction", C.c_int), ("do_cross_correlation", C.c_int), ("inputs_on_device", C.c_int),
+    ]
+
+
+class RomeMap3dPoolOut(C.Structure):
+    _fields_ = [
+        ("min_diff2", _DP), ("sum_weight", _DP), ("significant_weight", _DP), ("wsum_norm_correction", _DP),
+        ("pmax", _DP), ("cls", _IP), ("rot", _DP), ("tilt", _DP), ("psi", _DP), ("xoff", _DP), ("yoff", _DP),
+        ("nr_sign", _DP),
+        ("wsum_sigma2_noise", _DP), ("wsum_pdf_class", _DP), ("wsum_pdf_direction", _DP), ("wsum_sigma2_offset", _DP),
+        ("wsum_sumw_group", _DP),
+        ("pass_min_diff2", _DP * 2), ("pass_sum_weight", _DP * 2), ("pass_significant_weight", _DP * 2),
+        ("coarse_diff2", _DP), ("Mcoarse_significant", _CP),
+        ("fine_capacity", C.c_long), ("fine_count", _IP), ("fine_index", C.POINTER(C.c_long)),
+        ("fine_diff2", _DP), ("fine_weight", _DP),
+    ]
+
+
 class RomeReconIn(C.Structure):
     _fields_ = [("iclass", C.c_int), ("gridding_nr_iter", C.c_int), ("do_map", C.c_int), ("minres_map", C.c_int),
                 ("tau2_fudge", C.c_double), ("normalise", C.c_double), ("tau2_in", _DP)]
@@ -109,7 +140,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_create", "rome_gpu_destroy", "rome_gpu_last_error", "rome_gpu_set_precision",
     "rome_gpu_abi_version", "rome_gpu_set_projectors", "rome_gpu_get_backprojector",
     "rome_gpu_set_backprojector", "rome_gpu_map2d_estep_pool", "rome_gpu_select_significant",
-    "rome_gpu_select_significant_static",
+    "rome_gpu_select_significant_static", "rome_gpu_map3d_estep_pool",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings",
 ]
 
@@ -138,6 +169,7 @@ def load_library():
     lib.rome_gpu_get_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
     lib.rome_gpu_set_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
     lib.rome_gpu_map2d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap2dPool), C.POINTER(RomeMap2dPoolOut)]
+    lib.rome_gpu_map3d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap3dPool), C.POINTER(RomeMap3dPoolOut)]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]

@@ -124,6 +124,8 @@ enum Slot {
     S_REC_SMALL,  // reconstruct: radial sums, tau2, mask sums
     S_REC_VOL,    // reconstruct: output volume
     S_REC_TAB,    // reconstruct: blob table
+    S_FE,         // 3D fine pass: coarse-significant points (i, r, u, itr) [E] int4
+    S_FENT,       // 3D fine pass: row-layout prior index [P][stride] int2
     S_TMP0,
     S_TMP1,
     S_TMP2,

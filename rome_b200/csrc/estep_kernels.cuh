@@ -17,6 +17,8 @@
 #include "epilogues.cuh"
 
 namespace rome {
+// internal linkage: every translation unit that launches these kernels gets its own copy
+namespace {
 
 template <typename TVal>
 __device__ TVal block_reduce_sum(TVal v, TVal* sh);
@@ -392,8 +394,20 @@ __global__ void w2_kernel(int P, int Kact, int Kq, const int* __restrict__ act, 
 }
 
 // Layout of the hypothesis index e of one particle (exp_Mweight order).
+// Hypothesis layout of one particle's row.  Dense rows (every pass of 2D,
+// the coarse pass of 3D) hold e = j * T + t with j = (k, psi, over_rot) and
+// t = (trans, over_trans); k indexes pdf_direction and k / ndir the class of
+// the offset prior (3D folds the direction into k: k = class * ndir + dir).
+// Ragged rows (the 3D fine pass) hold epr hypotheses per coarse-significant
+// entry r; ent[i * ent_stride + r] = (k, coarse translation), x < 0 marks
+// padding, and the row order is already the reference's loop order.
 struct PostLayout {
     int T, notr, nor, npsi, ntr, K;
+    int ndir = 1;
+    const int2* ent = nullptr;
+    int ent_stride = 0;
+    int epr = 0;
+    int list_zeros = 0;  // 3D: computed zero weights take part in the sorted walk
 };
 
 __device__ __forceinline__ void decode_e(long e, const PostLayout& L, int& k, int& itr, long& loop_order) {
@@ -406,6 +420,25 @@ __device__ __forceinline__ void decode_e(long e, const PostLayout& L, int& k, in
     int iotr = t - itr * L.notr;
     // order of the reference's weight loop: class, psi, trans, over_rot, over_trans
     loop_order = ((((long)k * L.npsi + ipsi) * L.ntr + itr) * L.nor + ior) * L.notr + iotr;
+}
+
+// prior pdf_orientation and pdf_offset of hypothesis e in particle i's row
+// (po points at the particle's [class][ntr] offset priors); false for padding
+__device__ __forceinline__ bool hyp_prior(long e, int i, const PostLayout& L, const double* __restrict__ pdir,
+                                          const double* __restrict__ po, double& pd, double& pof, long& lo) {
+    int k, itr;
+    if (L.ent) {
+        const int2 en = L.ent[(long)i * L.ent_stride + e / L.epr];
+        if (en.x < 0) return false;
+        k = en.x;
+        itr = en.y;
+        lo = e;
+    } else {
+        decode_e(e, L, k, itr, lo);
+    }
+    pd = pdir[k];
+    pof = po[(k / L.ndir) * L.ntr + itr];
+    return true;
 }
 
 template <typename TVal>
@@ -675,4 +708,5 @@ __global__ void __launch_bounds__(NT)
     }
 }
 
+}  // namespace
 }  // namespace rome

@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 
 namespace rome {
+// internal linkage: every translation unit that launches these kernels gets its own copy
+namespace {
 
 constexpr int SG_BM = 128, SG_BN = 128, SG_BK = 16, SG_THREADS = 256;
 
@@ -106,4 +108,5 @@ inline void sgemm_tn(cudaStream_t st, int M, int N, int K, const float* A, long 
     sgemm_tn_kernel<Epi><<<grid, SG_THREADS, 0, st>>>(M, N, K, A, lda, B, ldb, epi);
 }
 
+}  // namespace
 }  // namespace rome

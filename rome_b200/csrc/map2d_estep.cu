@@ -28,6 +28,7 @@
 
 using namespace rome;
 
+namespace rome {
 namespace {
 
 struct PassGeom {
@@ -64,6 +65,7 @@ void rot2d_inv(double psi_deg, int padding, double out[4]) {
 }
 
 }  // namespace
+}  // namespace rome
 
 // ---------------------------------------------------------------------------
 extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2dPoolOut* out) {
@@ -525,6 +527,7 @@ extern "C" int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, con
 // the entry point holds a process-wide lock and returns only after its
 // stream work has finished, which serialises calls from different host
 // threads.
+namespace rome {
 namespace {
 
 constexpr size_t kStaticAlign = 256;
@@ -577,6 +580,7 @@ __global__ void static_finish_kernel(int n, const double* __restrict__ part, con
 }
 
 }  // namespace
+}  // namespace rome
 
 extern "C" int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const double* weights,
                                                   const double* sum_weight, double adaptive_fraction,

@@ -1,0 +1,627 @@
+// MAP3D E-step for one pool of particles on sm_100a.
+//
+// Replaces Map3dOptimizer_old::expectationSomeParticles
+// (src/map3d_optimizer.cpp:883-953) minus storeWeightedSums.
+//
+// Coarse pass (coarse_size, nr_over_rot = nr_over_trans = 1): every
+// hypothesis (class, dir, psi, trans) whose class and direction have a
+// positive prior, laid out densely like the 2D pass with the direction
+// folded into the class index (k = class * ndir + dir): 3D Fourier-slice
+// projections (project3d_kernel), the cross term on the tensor cores (or
+// FP32 CUDA cores) with the fused diff2 epilogue, then the FP64 posterior
+// and significance walk.
+//
+// Fine pass (current_size, 8 over-rotations x 4 over-translations): only
+// the coarse-significant (orientation, translation) points of each
+// particle, compacted in the reference's list order; the squared
+// differences of their 32 sub-hypotheses (fine_diff2_kernel), the posterior
+// over the ragged rows, then updateOtherParams and backProjection over the
+// significant fine hypotheses.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "common.cuh"
+#include "estep3d_kernels.cuh"
+#include "estep_kernels.cuh"
+#include "gemm_simt.cuh"
+#include "gemm_tc.cuh"
+#include "select_kernels.cuh"
+
+using namespace rome;
+
+namespace rome {
+namespace {
+
+template <typename T>
+T* upload3(RomeGpuCtx* ctx, Slot s, const T* host, size_t n) {
+    T* d = ctx->ws[s].as<T>(n);
+    if (n) ROME_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return d;
+}
+
+// Euler_angles2matrix (src/math.cpp:86-115); the projector and the
+// back-projector use Ainv[i][j] = A[j][i] * padding (src/reconstruct.cpp:265-276).
+Rot3 rot3_inv(double rot, double tilt, double psi, int padding) {
+    const double d2r = 3.14159265358979323846 / 180.;
+    const double alpha = rot * d2r, beta = tilt * d2r, gamma = psi * d2r;
+    const double ca = cos(alpha), cb = cos(beta), cg = cos(gamma);
+    const double sa = sin(alpha), sb = sin(beta), sg = sin(gamma);
+    const double cc = cb * ca, cs = cb * sa, sc = sb * ca, ss = sb * sa;
+    const double A00 = cg * cc - sg * sa, A01 = cg * cs + sg * ca, A02 = -cg * sb;
+    const double A10 = -sg * cc - cg * sa, A11 = -sg * cs + cg * ca, A12 = sg * sb;
+    (void)sc;
+    (void)ss;
+    const double p = (double)padding;
+    return Rot3{A00 * p, A10 * p, A01 * p, A11 * p, A02 * p, A12 * p};
+}
+
+__global__ void fill_float_kernel(long n, float v, float* __restrict__ out) {
+    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[q] = v;
+}
+
+struct Pass {
+    int cs, csF, F, Kact, Kp, Kq, my_r_max;
+};
+
+// active pixels of a pass: the support of the projection, r^2 <= my_r_max^2
+// (src/reconstruct.cpp:278-299)
+Pass active_pixels(int cs, int r_max, std::vector<int>& act, std::vector<int>& actidx) {
+    Pass g{};
+    g.cs = cs;
+    g.csF = cs / 2 + 1;
+    g.F = cs * g.csF;
+    g.my_r_max = std::min(r_max, cs / 2);
+    act.clear();
+    actidx.assign(g.F, -1);
+    for (int row = 0; row < cs; row++) {
+        int y;
+        if (row <= g.my_r_max) y = row;
+        else if (row >= cs - g.my_r_max) y = row - cs;
+        else continue;
+        for (int x = 0; x <= g.my_r_max; x++)
+            if (x * x + y * y <= g.my_r_max * g.my_r_max) {
+                actidx[row * g.csF + x] = (int)act.size();
+                act.push_back(row * g.csF + x);
+            }
+    }
+    g.Kact = (int)act.size();
+    g.Kp = ((2 * g.Kact + 63) / 64) * 64;
+    g.Kq = ((g.Kact + 15) / 16) * 16;
+    return g;
+}
+
+}  // namespace
+}  // namespace rome
+
+extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* in, RomeMap3dPoolOut* out) {
+    if (!ctx || !in || !out) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->proj || ctx->ref_dim != 3) fail(ROME_ERR_STATE, "3D projectors not set (rome_gpu_set_projectors)");
+        const int P = in->nr_images, K = in->nr_classes, ori = in->ori_size, cur = in->current_size;
+        const int ndir = in->nr_dir, npsi = in->nr_psi, ntr = in->nr_trans, G = in->nr_groups, oriF = ori / 2 + 1;
+        ROME_REQUIRE(P > 0 && K == ctx->nr_classes && ori == ctx->ori_size, "pool/projector mismatch");
+        ROME_REQUIRE(cur > 0 && cur <= ori && cur % 2 == 0, "bad current_size %d", cur);
+        ROME_REQUIRE(in->coarse_size > 0 && in->coarse_size <= cur && in->coarse_size % 2 == 0, "bad coarse_size %d",
+                     in->coarse_size);
+        if (in->adaptive_oversampling != 1)
+            fail(ROME_ERR_UNSUPPORTED, "3D E-step needs adaptive_oversampling 1 (got %d)", in->adaptive_oversampling);
+        if (in->do_scale_correction) fail(ROME_ERR_UNSUPPORTED, "scale correction is not supported");
+        if (in->do_cross_correlation) fail(ROME_ERR_UNSUPPORTED, "cross-correlation mode is not supported");
+        ROME_REQUIRE(in->iclass_min >= 0 && in->iclass_max < K && in->iclass_min <= in->iclass_max, "bad class range");
+        ROME_REQUIRE(ctx->r_max == std::min(cur / 2, ori / 2), "projector r_max %d does not match current_size %d",
+                     ctx->r_max, cur);
+        ROME_REQUIRE(in->Fimg_real && in->Fimg_imag && in->Fimg_nomask_real && in->Fimg_nomask_imag && in->Fctf,
+                     "missing particle images");
+        ROME_REQUIRE(ndir > 0 && npsi > 0 && ntr > 0 && G > 0, "empty sampling");
+        for (int p = 0; p < 2; p++)
+            ROME_REQUIRE(in->angles[p] && in->over_trans_x[p] && in->over_trans_y[p], "missing sampling tables (pass %d)",
+                         p);
+        ROME_REQUIRE(in->Mresol_coarse && in->Mresol_fine && in->pdf_direction && in->pdf_class, "missing model arrays");
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        cudaStream_t st = ctx->stream;
+        const int curF2 = cur * (cur / 2 + 1);
+        const int KD = K * ndir;
+        const int Jc = KD * npsi;                  // coarse orientations (class, dir, psi)
+        const long ncoarse = (long)Jc * ntr;       // coarse hypotheses per particle
+        const int NOR = 8, NOTR = 4, NH = NOR * NOTR;
+        const bool apply_ctf = in->do_ctf_correction && in->refs_are_ctf_corrected;
+        const bool tc = ctx->precision != ROME_PREC_FP32;
+        Profiler prof(ctx);
+
+        // ---- particle data at current_size ----
+        const double *dFr, *dFi, *dFnr, *dFni, *dCtf;
+        if (in->inputs_on_device) {
+            dFr = in->Fimg_real;
+            dFi = in->Fimg_imag;
+            dFnr = in->Fimg_nomask_real;
+            dFni = in->Fimg_nomask_imag;
+            dCtf = in->Fctf;
+        } else {
+            double* base = ctx->ws[S_TMP0].as<double>((size_t)P * curF2 * 5);
+            const double* src[5] = {in->Fimg_real, in->Fimg_imag, in->Fimg_nomask_real, in->Fimg_nomask_imag,
+                                    in->Fctf};
+            for (int q = 0; q < 5; q++)
+                ROME_CUDA(cudaMemcpyAsync(base + (size_t)q * P * curF2, src[q], sizeof(double) * P * curF2,
+                                          cudaMemcpyHostToDevice, st));
+            dFr = base;
+            dFi = base + (size_t)P * curF2;
+            dFnr = base + (size_t)2 * P * curF2;
+            dFni = base + (size_t)3 * P * curF2;
+            dCtf = base + (size_t)4 * P * curF2;
+        }
+        double* dSig2 = upload3(ctx, S_SIG2, in->sigma2_noise, (size_t)G * oriF);
+        int* dGroup = upload3(ctx, S_GROUP, in->group, (size_t)P);
+        double* dXi2 = upload3(ctx, S_XI2, in->highres_Xi2, (size_t)P);
+        // model values: pdf_direction [K*ndir], prior offsets [K] x 2
+        std::vector<double> hcls((size_t)KD + 2 * K);
+        for (int q = 0; q < KD; q++) hcls[q] = in->pdf_direction[q];
+        for (int k = 0; k < K; k++) {
+            hcls[KD + k] = in->prior_offsetx_class[k];
+            hcls[KD + K + k] = in->prior_offsety_class[k];
+        }
+        double* dCls = upload3(ctx, S_PDIR, hcls.data(), hcls.size());
+        const double* dPdir = dCls;
+        const double* dPriorX = dCls + KD;
+        const double* dPriorY = dCls + KD + K;
+        std::vector<double2> hoff(P);
+        for (int i = 0; i < P; i++) hoff[i] = make_double2(in->old_offsetx[i], in->old_offsety[i]);
+        double2* dOld = upload3(ctx, S_OLDOFF, hoff.data(), hoff.size());
+        std::vector<double2> htc(ntr);
+        for (int t = 0; t < ntr; t++) htc[t] = make_double2(in->trans_x[t], in->trans_y[t]);
+        double2* dTrC = upload3(ctx, S_TMP1, htc.data(), htc.size());
+        double* dPoff = ctx->ws[S_POFF].as<double>((size_t)P * K * ntr);
+        prof.begin(ROME_PHASE_PREP);
+        pdf_offset_kernel<<<P, 128, 0, st>>>(P, K, ntr, dOld, dTrC, dPriorX, dPriorY, in->sigma2_offset, dPoff);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_PREP);
+        prof.end(ROME_PHASE_PREP);
+        // (class, dir) pairs the reference visits (map3d_optimizer.cpp:1205-1206, :1279-1280)
+        std::vector<int> hcd_ok(KD);
+        for (int q = 0; q < KD; q++) {
+            const int k = q / ndir;
+            hcd_ok[q] = k >= in->iclass_min && k <= in->iclass_max && in->pdf_class[k] > 0. && in->pdf_direction[q] > 0.;
+        }
+
+        double* dPart = ctx->ws[S_PART].as<double>((size_t)P * 8);
+        int* dPartI = ctx->ws[S_PARTI].as<int>((size_t)P * 8);
+        char* dMcoarse = ctx->ws[S_MCOARSE].as<char>((size_t)P * ncoarse);
+        int* dSeg = ctx->ws[S_SEG].as<int>((size_t)2 * P);
+        std::vector<double> h_min(P), h_sum(P), h_sig(P), h_nsig(P);
+        std::vector<double> hpart((size_t)P * 8);
+        std::vector<int> hparti((size_t)P * 8);
+
+        // ================= pass 0: coarse, dense =================
+        {
+            std::vector<int> act, actidx;
+            const Pass g = active_pixels(in->coarse_size, ctx->r_max, act, actidx);
+            const int cs = g.cs, T = ntr, J = Jc;
+            const long X = (long)J * T;
+            int* dAct = upload3(ctx, S_ACT, act.data(), act.size());
+            int* dMres = upload3(ctx, S_MRES, in->Mresol_coarse, (size_t)g.F);
+            std::vector<int> hj((size_t)2 * J);  // jvalid, jclass
+            std::vector<Rot3> hrot(J);
+            for (int j = 0; j < J; j++) {
+                const int cd = j / npsi, dp = j % (ndir * npsi);
+                hj[j] = hcd_ok[cd];
+                hj[J + j] = cd / ndir;
+                const double* a = in->angles[0] + (size_t)dp * 3;
+                hrot[j] = rot3_inv(a[0], a[1], a[2], ctx->padding);
+            }
+            int* dJ = upload3(ctx, S_JVALID, hj.data(), hj.size());
+            Rot3* dRot = upload3(ctx, S_ROTM, hrot.data(), hrot.size());
+            std::vector<double2> hsh(T);
+            for (int t = 0; t < T; t++)
+                hsh[t] = make_double2(in->over_trans_x[0][t] / (-ori), in->over_trans_y[0][t] / (-ori));
+            double2* dShift = upload3(ctx, S_SHIFT, hsh.data(), hsh.size());
+
+            double2* dFimg = ctx->ws[S_FIMG].as<double2>((size_t)P * g.F);
+            double* dLctf = ctx->ws[S_CTF].as<double>((size_t)P * g.F);
+            double* dMinv = ctx->ws[S_MINV].as<double>((size_t)P * g.F);
+            prof.begin(ROME_PHASE_PREP);
+            prep_particles_kernel<<<P, 256, 0, st>>>(P, cur, cs, dFr, dFi, dCtf, dMres, dSig2, dGroup, oriF,
+                                                      in->sigma2_fudge, dFimg, dLctf, dMinv);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_PREP);
+            prof.end(ROME_PHASE_PREP);
+
+            float* dQ = ctx->ws[S_Q].as<float>((size_t)J * g.Kq);
+            void* dB = ctx->ws[S_B].get((size_t)J * g.Kp * 4);
+            prof.begin(ROME_PHASE_PROJECT);
+            project3d_kernel<<<J, 128, 0, st>>>(J, g.Kact, g.Kp, g.Kq, cs, g.csF, g.my_r_max, ctx->pad_size,
+                                                 ctx->pad_size / 2 + 1, dJ + J, ctx->proj, ctx->vox, dRot, dAct, dJ,
+                                                 nullptr, dQ, dB, ctx->precision);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_PROJECT);
+            prof.end(ROME_PHASE_PROJECT);
+
+            const long M = (long)P * T;
+            void* dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+            float* dS = ctx->ws[S_S].as<float>((size_t)M);
+            float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+            unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)T * g.Kact);
+            prof.begin(ROME_PHASE_SHIFT);
+            phase_index_kernel<<<(unsigned)(((long)T * g.Kact + 255) / 256), 256, 0, st>>>(
+                T, g.Kact, g.csF, cs, dAct, dShift, ctx->shift_sampling, dPidx);
+            ROME_CHECK_LAUNCH();
+            shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                                                           apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
+                                                           ctx->precision);
+            ROME_CHECK_LAUNCH();
+            w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_SHIFT, 3);
+            prof.end(ROME_PHASE_SHIFT);
+
+            float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * J);
+            prof.begin(ROME_PHASE_NORM_GEMM);
+            if (!tc) {
+                sgemm_tn(st, P, J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, J});
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_NORM_GEMM);
+            } else {
+                const int Kq64 = ((g.Kact + 63) / 64) * 64;
+                void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
+                void* dQb = ctx->ws[S_QB].get((size_t)J * Kq64 * 4);
+                split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
+                split_bf16(st, dQ, J, g.Kact, g.Kq, Kq64, dQb);
+                tc_store_gemm(st, P, J, Kq64, dW2b, dQb, dNorm, J, ctx->d_err);
+                prof.launched(ROME_PHASE_NORM_GEMM, 3);
+            }
+            prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * J * g.Kact);
+            prof.end(ROME_PHASE_NORM_GEMM);
+
+            float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * X);
+            unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
+            ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
+            Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJ, T, J, X, 1, 1, ntr, ncoarse, nullptr, dRowMin};
+            prof.begin(ROME_PHASE_CROSS_GEMM);
+            if (!tc) sgemm_tn(st, (int)M, J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
+            else tc_diff2_gemm(st, (int)M, J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_CROSS_GEMM);
+            prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * J * g.Kact);
+            prof.end(ROME_PHASE_CROSS_GEMM);
+
+            // posterior, walk, coarse-significant points
+            PostLayout Lp{T, 1, 1, npsi, ntr, K};
+            Lp.ndir = ndir;
+            Lp.list_zeros = 1;
+            int* dCounter = ctx->ws[S_LISTCNT].as<int>(4);
+            int listcap = std::max(1024, P * 64), nsig = 0;
+            SigEntry* dList = nullptr;
+            prof.begin(ROME_PHASE_POSTERIOR);
+            for (;;) {
+                dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap);
+                SelectResult sr = run_select(ctx, st, 0, P, X, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,
+                                             dPartI, nullptr, nullptr, dList, dCounter, listcap, dSeg, dRowMin);
+                prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
+                nsig = sr.nlist;
+                if (sr.nlist <= listcap) break;
+                listcap = sr.nlist;
+            }
+            ROME_CUDA(cudaMemsetAsync(dMcoarse, 0, (size_t)P * ncoarse, st));
+            if (nsig > 0) {
+                mcoarse_from_list_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, X, dList, dMcoarse);
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_POSTERIOR);
+            }
+            prof.end(ROME_PHASE_POSTERIOR);
+            if (tc) tc_check_error(st, ctx->d_err);
+
+            ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * P * 8, cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaMemcpyAsync(hparti.data(), dPartI, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
+            if (out->coarse_diff2) {
+                std::vector<float> hd((size_t)P * X);
+                ROME_CUDA(cudaMemcpyAsync(hd.data(), dDiff2, sizeof(float) * hd.size(), cudaMemcpyDeviceToHost, st));
+                ROME_CUDA(cudaStreamSynchronize(st));
+                for (size_t q = 0; q < hd.size(); q++)
+                    out->coarse_diff2[q] = hd[q] < INFINITY ? (double)hd[q] : (double)INT_MIN;
+            }
+            if (out->Mcoarse_significant)
+                ROME_CUDA(cudaMemcpyAsync(out->Mcoarse_significant, dMcoarse, (size_t)P * ncoarse,
+                                          cudaMemcpyDeviceToHost, st));
+            ROME_CUDA(cudaStreamSynchronize(st));
+            for (int i = 0; i < P; i++) {
+                h_min[i] = hpart[i * 8 + 0];
+                h_sum[i] = hpart[i * 8 + 1];
+                h_sig[i] = hpart[i * 8 + 2];
+                h_nsig[i] = hparti[i * 8 + 1];
+                if (h_nsig[i] == 0) fail(ROME_ERR_NUMERIC, "my_nr_significant_coarse_samples == 0 for particle %d", i);
+                if (out->pass_min_diff2[0]) out->pass_min_diff2[0][i] = h_min[i];
+                if (out->pass_sum_weight[0]) out->pass_sum_weight[0][i] = h_sum[i];
+                if (out->pass_significant_weight[0]) out->pass_significant_weight[0][i] = h_sig[i];
+            }
+        }
+
+        // ================= pass 1: fine, over the coarse-significant points =================
+        std::vector<int> act, actidx;
+        const Pass g = active_pixels(cur, ctx->r_max, act, actidx);
+        const int Tf = ntr * NOTR;
+        int* dAct = upload3(ctx, S_ACT, act.data(), act.size());
+        int* dActIdx = upload3(ctx, S_ACTIDX, actidx.data(), actidx.size());
+        int* dMresF = upload3(ctx, S_MRES, in->Mresol_fine, (size_t)g.F);
+
+        // orientations some particle needs (getReferenceAllOrientations, :956-985)
+        char* dRotSig = ctx->ws[S_ROTSIG].as<char>((size_t)Jc);
+        rot_sig_kernel<<<(Jc + 255) / 256, 256, 0, st>>>(Jc, P, ntr, ncoarse, dMcoarse, dRotSig);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_PROJECT);
+        std::vector<char> hrs(Jc);
+        ROME_CUDA(cudaMemcpyAsync(hrs.data(), dRotSig, Jc, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        std::vector<int> uj, ucompact(Jc, -1);
+        for (int jc = 0; jc < Jc; jc++)
+            if (hrs[jc] && hcd_ok[jc / npsi]) {
+                ucompact[jc] = (int)uj.size();
+                uj.push_back(jc);
+            }
+        const int nU = (int)uj.size(), Jf = nU * NOR;
+        ROME_REQUIRE(nU > 0, "no significant coarse orientation");
+        int* dUcomp = upload3(ctx, S_TMP2, ucompact.data(), ucompact.size());
+        std::vector<int> hjf((size_t)2 * Jf);  // jclass, jcd
+        std::vector<Rot3> hrotf(Jf);
+        for (int u = 0; u < nU; u++) {
+            const int jc = uj[u], cd = jc / npsi, dp = jc % (ndir * npsi);
+            for (int o = 0; o < NOR; o++) {
+                const int jf = u * NOR + o;
+                hjf[jf] = cd / ndir;
+                hjf[Jf + jf] = cd;
+                const double* a = in->angles[1] + ((size_t)dp * NOR + o) * 3;
+                hrotf[jf] = rot3_inv(a[0], a[1], a[2], ctx->padding);
+            }
+        }
+        int* dJf = upload3(ctx, S_JVALID, hjf.data(), hjf.size());
+        Rot3* dRotF = upload3(ctx, S_ROTM, hrotf.data(), hrotf.size());
+        std::vector<double2> hsh(Tf), htr(Tf);
+        for (int t = 0; t < Tf; t++) {
+            hsh[t] = make_double2(in->over_trans_x[1][t] / (-ori), in->over_trans_y[1][t] / (-ori));
+            htr[t] = make_double2(in->over_trans_x[1][t], in->over_trans_y[1][t]);
+        }
+        double2* dShift = upload3(ctx, S_SHIFT, hsh.data(), hsh.size());
+        double2* dTr = upload3(ctx, S_TRANS, htr.data(), htr.size());
+        double2* dPh = ctx->ws[S_PHASE].as<double2>((size_t)Tf * g.F);
+        prof.begin(ROME_PHASE_SHIFT);
+        phase_table_kernel<<<(unsigned)(((long)Tf * g.F + 255) / 256), 256, 0, st>>>(
+            Tf, g.F, g.csF, cur, dShift, ctx->d_shift_tab, ctx->shift_sampling, dPh);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_SHIFT);
+        prof.end(ROME_PHASE_SHIFT);
+
+        double2* dFimg = ctx->ws[S_FIMG].as<double2>((size_t)P * g.F);
+        double* dLctf = ctx->ws[S_CTF].as<double>((size_t)P * g.F);
+        double* dMinv = ctx->ws[S_MINV].as<double>((size_t)P * g.F);
+        prof.begin(ROME_PHASE_PREP);
+        prep_particles_kernel<<<P, 256, 0, st>>>(P, cur, cur, dFr, dFi, dCtf, dMresF, dSig2, dGroup, oriF,
+                                                  in->sigma2_fudge, dFimg, dLctf, dMinv);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_PREP);
+        prof.end(ROME_PHASE_PREP);
+
+        // fine projections: FP64 for wsum/backprojection, FP32 operands for diff2
+        double2* dProj = ctx->ws[S_PROJ].as<double2>((size_t)Jf * g.Kact);
+        float* dQ = ctx->ws[S_Q].as<float>((size_t)Jf * g.Kq);
+        float* dB = ctx->ws[S_B].as<float>((size_t)Jf * g.Kp);
+        prof.begin(ROME_PHASE_PROJECT);
+        project3d_kernel<<<Jf, 128, 0, st>>>(Jf, g.Kact, g.Kp, g.Kq, cur, g.csF, g.my_r_max, ctx->pad_size,
+                                              ctx->pad_size / 2 + 1, dJf, ctx->proj, ctx->vox, dRotF, dAct, nullptr,
+                                              dProj, dQ, dB, ROME_PREC_FP32);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_PROJECT);
+        prof.end(ROME_PHASE_PROJECT);
+
+        const long Mf = (long)P * Tf;
+        float* dA = ctx->ws[S_A].as<float>((size_t)Mf * g.Kp);
+        float* dS = ctx->ws[S_S].as<float>((size_t)Mf);
+        float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+        unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)Tf * g.Kact);
+        prof.begin(ROME_PHASE_SHIFT);
+        phase_index_kernel<<<(unsigned)(((long)Tf * g.Kact + 255) / 256), 256, 0, st>>>(
+            Tf, g.Kact, g.csF, cur, dAct, dShift, ctx->shift_sampling, dPidx);
+        ROME_CHECK_LAUNCH();
+        shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, Tf, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                                                       apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
+                                                       ROME_PREC_FP32);
+        ROME_CHECK_LAUNCH();
+        w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_SHIFT, 3);
+        prof.end(ROME_PHASE_SHIFT);
+
+        // compaction of the coarse-significant points
+        int* dCnt = ctx->ws[S_OFFJ].as<int>((size_t)2 * P + 2);
+        int* dOffP = dCnt + P;
+        mcoarse_count_kernel<<<P, 256, 0, st>>>(ncoarse, dMcoarse, dCnt);
+        ROME_CHECK_LAUNCH();
+        std::vector<int> hcnt(P), hoffp(P + 1);
+        ROME_CUDA(cudaMemcpyAsync(hcnt.data(), dCnt, sizeof(int) * P, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        int stride = 1;
+        hoffp[0] = 0;
+        for (int i = 0; i < P; i++) {
+            hoffp[i + 1] = hoffp[i] + hcnt[i];
+            stride = std::max(stride, hcnt[i]);
+        }
+        const int E = hoffp[P];
+        ROME_CUDA(cudaMemcpyAsync(dOffP, hoffp.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, st));
+        int4* dFe = ctx->ws[S_FE].as<int4>((size_t)std::max(E, 1));
+        int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)P * stride);
+        ROME_CUDA(cudaMemsetAsync(dEnt, 0xFF, sizeof(int2) * (size_t)P * stride, st));
+        fine_entries_kernel<<<P, 1024, 0, st>>>(ncoarse, ntr, npsi, dMcoarse, dOffP, dUcomp, stride, dFe, dEnt);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_PROJECT, 2);
+
+        // fine squared differences, ragged rows [P][stride * 32] padded with +inf
+        const long Xf = (long)stride * NH;
+        float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xf);
+        unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
+        prof.begin(ROME_PHASE_CROSS_GEMM);
+        fill_float_kernel<<<(unsigned)((P * Xf + 255) / 256), 256, 0, st>>>(P * Xf, INFINITY, dDiff2);
+        ROME_CHECK_LAUNCH();
+        ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
+        if (E > 0) {
+            fine_diff2_kernel<128, 8, 4><<<E, 128, 0, st>>>(Tf, g.Kp, g.Kq, dFe, dA, dB, dW2, dQ, dS, dXi2, Xf, dDiff2,
+                                                          dRowMin);
+            ROME_CHECK_LAUNCH();
+        }
+        prof.launched(ROME_PHASE_CROSS_GEMM, 2);
+        prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)E * NH * g.Kact);
+        prof.end(ROME_PHASE_CROSS_GEMM);
+
+        // posterior over the ragged rows
+        PostLayout Lf{Tf, NOTR, NOR, npsi, ntr, K};
+        Lf.ndir = ndir;
+        Lf.ent = dEnt;
+        Lf.ent_stride = stride;
+        Lf.epr = NH;
+        Lf.list_zeros = 1;
+        double* dW = nullptr;
+        if (out->fine_weight) dW = ctx->ws[S_WCHK].as<double>((size_t)P * Xf);
+        int* dCounter = ctx->ws[S_LISTCNT].as<int>((size_t)Jf + 4);
+        int listcap = std::max(1024, P * 64), nsig = 0;
+        SigEntry* dList = nullptr;
+        prof.begin(ROME_PHASE_POSTERIOR);
+        for (;;) {
+            dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
+            SelectResult sr = run_select(ctx, st, 0, P, Xf, Lf, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,
+                                         dPartI, nullptr, dW, dList, dCounter, listcap, dSeg, dRowMin);
+            prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
+            nsig = sr.nlist;
+            if (sr.nlist <= listcap) break;
+            listcap = sr.nlist;
+        }
+        if (nsig > 0) {
+            fine_list_dense_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, NOR, NOTR, Tf, stride, dFe, dOffP, dList);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_POSTERIOR);
+        }
+        prof.end(ROME_PHASE_POSTERIOR);
+
+        ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * P * 8, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaMemcpyAsync(hparti.data(), dPartI, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
+        std::vector<int4> hfe(std::max(E, 1));
+        if (E > 0) ROME_CUDA(cudaMemcpyAsync(hfe.data(), dFe, sizeof(int4) * E, cudaMemcpyDeviceToHost, st));
+        std::vector<float> hd;
+        std::vector<double> hw;
+        if (out->fine_count || out->fine_index || out->fine_diff2 || out->fine_weight) {
+            hd.resize((size_t)P * Xf);
+            ROME_CUDA(cudaMemcpyAsync(hd.data(), dDiff2, sizeof(float) * hd.size(), cudaMemcpyDeviceToHost, st));
+            if (dW) {
+                hw.resize((size_t)P * Xf);
+                ROME_CUDA(cudaMemcpyAsync(hw.data(), dW, sizeof(double) * hw.size(), cudaMemcpyDeviceToHost, st));
+            }
+        }
+        ROME_CUDA(cudaStreamSynchronize(st));
+        if (!hd.empty()) {
+            long q = 0;
+            for (int i = 0; i < P; i++) {
+                const int n = hcnt[i] * NH;
+                if (out->fine_count) out->fine_count[i] = n;
+                for (int e = 0; e < n; e++, q++) {
+                    if (q >= out->fine_capacity) fail(ROME_ERR_ARG, "fine_capacity %ld too small", out->fine_capacity);
+                    const int4 en = hfe[hoffp[i] + e / NH];
+                    const long jc = uj[en.z];
+                    if (out->fine_index) out->fine_index[q] = ((jc * ntr + en.w) * NH) + e % NH;
+                    if (out->fine_diff2) out->fine_diff2[q] = (double)hd[(size_t)i * Xf + e];
+                    if (out->fine_weight) out->fine_weight[q] = hw.empty() ? 0.0 : hw[(size_t)i * Xf + e];
+                }
+            }
+        }
+        for (int i = 0; i < P; i++) {
+            const double mn = hpart[i * 8 + 0], sw = hpart[i * 8 + 1], sig = hpart[i * 8 + 2], mx = hpart[i * 8 + 4];
+            const int best = hparti[i * 8 + 0];
+            h_min[i] = mn;
+            h_sum[i] = sw;
+            h_sig[i] = sig;
+            if (out->pass_min_diff2[1]) out->pass_min_diff2[1][i] = mn;
+            if (out->pass_sum_weight[1]) out->pass_sum_weight[1][i] = sw;
+            if (out->pass_significant_weight[1]) out->pass_significant_weight[1][i] = sig;
+            // convertSquaredDifferencesToWeights metadata (map3d_optimizer.cpp:1787-1804)
+            const int r = best / NH, h = best % NH, o = h / NOTR, t = h % NOTR;
+            if (hcnt[i] == 0 || r >= hcnt[i]) continue;
+            const int4 en = hfe[hoffp[i] + r];
+            const int jc = uj[en.z], cd = jc / npsi, dp = jc % (ndir * npsi);
+            const double* a = in->angles[1] + ((size_t)dp * NOR + o) * 3;
+            if (out->pmax) out->pmax[i] = mx / sw;
+            if (out->cls) out->cls[i] = cd / ndir + 1;
+            if (out->rot) out->rot[i] = a[0];
+            if (out->tilt) out->tilt[i] = a[1];
+            if (out->psi) out->psi[i] = a[2];
+            if (out->xoff) out->xoff[i] = in->old_offsetx[i] + in->over_trans_x[1][en.w * NOTR + t];
+            if (out->yoff) out->yoff[i] = in->old_offsety[i] + in->over_trans_y[1][en.w * NOTR + t];
+        }
+
+        // ---- updateOtherParams ----
+        double* dWsn = ctx->ws[S_WSN].as<double>((size_t)G * oriF + P);
+        double* dNormCorr = dWsn + (size_t)G * oriF;
+        const int nwk = K + KD + 1 + G;
+        double* dWk = ctx->ws[S_WSUMK].as<double>((size_t)nwk);
+        ROME_CUDA(cudaMemsetAsync(dWsn, 0, sizeof(double) * ((size_t)G * oriF + P), st));
+        ROME_CUDA(cudaMemsetAsync(dWk, 0, sizeof(double) * nwk, st));
+        const int NT = 256, PIX = 8;
+        const int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
+        prof.begin(ROME_PHASE_WSUM);
+        wsum3d_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
+            Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
+            g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_WSUM);
+        prof.end(ROME_PHASE_WSUM);
+
+        // ---- backProjection ----
+        {
+            double2* dFnm = ctx->ws[S_FNOMASK].as<double2>((size_t)P * g.F);
+            double* dMctf2 = dMinv;  // becomes ctf^2 * Minvsigma2 in place
+            prof.begin(ROME_PHASE_BACKPROJECT);
+            bp_prep_kernel<<<P, 256, 0, st>>>(P, g.F, dFnr, dFni, dLctf, dMinv, dSig2, dGroup, oriF, in->sigma2_fudge,
+                                              in->do_map, in->do_ctf_correction, dFnm, dMctf2);
+            ROME_CHECK_LAUNCH();
+            int* dJcnt = dCounter + 2;
+            int* dJoff = ctx->ws[S_REC_SMALL].as<int>((size_t)2 * Jf + 2);
+            int* dFill = dJoff + Jf + 1;
+            SigEntry* dSorted = dList + listcap;
+            ROME_CUDA(cudaMemsetAsync(dJcnt, 0, sizeof(int) * Jf, st));
+            ROME_CUDA(cudaMemsetAsync(dFill, 0, sizeof(int) * Jf, st));
+            if (nsig > 0) {
+                count_by_j_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, Tf, dList, dJcnt);
+                ROME_CHECK_LAUNCH();
+            }
+            exclusive_scan_kernel<<<1, 1024, 0, st>>>(Jf, dJcnt, dJoff);
+            ROME_CHECK_LAUNCH();
+            if (nsig > 0) {
+                scatter_by_j_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, Tf, dList, dJoff, dFill, dSorted);
+                ROME_CHECK_LAUNCH();
+            }
+            bp3d_list_kernel<NT, PIX><<<dim3(nsplit, Jf), NT, 0, st>>>(
+                Tf, g.F, g.csF, cur, dSorted, dJoff, dJf, dFnm, dMctf2, dShift, dPh, dRotF, ctx->r_max, ctx->pad_size,
+                ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_BACKPROJECT, 5);
+            prof.end(ROME_PHASE_BACKPROJECT);
+        }
+
+        // ---- outputs ----
+        std::vector<double> hwsn((size_t)G * oriF + P), hwk(nwk);
+        ROME_CUDA(cudaMemcpyAsync(hwsn.data(), dWsn, sizeof(double) * hwsn.size(), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaMemcpyAsync(hwk.data(), dWk, sizeof(double) * hwk.size(), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        prof.collect();
+        for (size_t q = 0; q < (size_t)G * oriF; q++) out->wsum_sigma2_noise[q] += hwsn[q];
+        for (int i = 0; i < P; i++) {
+            if (out->wsum_norm_correction) out->wsum_norm_correction[i] = hwsn[(size_t)G * oriF + i];
+            if (out->min_diff2) out->min_diff2[i] = h_min[i];
+            if (out->sum_weight) out->sum_weight[i] = h_sum[i];
+            if (out->significant_weight) out->significant_weight[i] = h_sig[i];
+            if (out->nr_sign) out->nr_sign[i] = h_nsig[i];
+        }
+        for (int k = 0; k < K; k++) out->wsum_pdf_class[k] += hwk[k];
+        for (int q = 0; q < KD; q++) out->wsum_pdf_direction[q] += hwk[K + q];
+        out->wsum_sigma2_offset[0] += hwk[K + KD];
+        for (int q = 0; q < G; q++) out->wsum_sumw_group[q] += hwk[K + KD + 1 + q];
+        for (int i = 0; i < P; i++)
+            if (h_sum[i] == 0) fail(ROME_ERR_NUMERIC, "exp_sum_weight[%d] == 0", i);
+    });
+}

@@ -23,6 +23,8 @@
 #include "estep_kernels.cuh"
 
 namespace rome {
+// internal linkage: every translation unit that launches these kernels gets its own copy
+namespace {
 
 constexpr int SEL2_THREADS = 512;
 constexpr int SEL2_CAP = 8192;
@@ -96,7 +98,24 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     // ---- weights: sum, argmax (first in the reference's loop order), max prior ----
     double sum = 0.0, maxw = DBL_MIN, maxpd = 0.0;
     long best_lo = LONG_MAX, best_e = 0;
-    if (mode == 0) {
+    if (mode == 0 && L.ent) {
+        // ragged rows: the row order is the loop order
+        for (long e = threadIdx.x; e < X; e += blockDim.x) {
+            double pd, pof;
+            long lo;
+            if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) continue;
+            float dv = d[e];
+            if (dv < INFINITY) maxpd = fmax(maxpd, pd * pof);
+            double w = hyp_weight(dv, mn, pd, pof);
+            if (wout) wout[(long)i * X + e] = w;
+            sum += w;
+            if (w > maxw || (w == maxw && w > DBL_MIN && lo < best_lo)) {
+                maxw = w;
+                best_lo = lo;
+                best_e = e;
+            }
+        }
+    } else if (mode == 0) {
         // orientation-major sweep: one division per orientation, the loop-order
         // index only on ties (argmax of the reference's loop, :1140-1146)
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
@@ -105,7 +124,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
         for (int j = warp; j < J; j += nwarp) {
             const int k = j / nrot;
             const double pdk = pdir[k];
-            const double* pok = po + k * L.ntr;
+            const double* pok = po + (k / L.ndir) * L.ntr;
             for (int t = lane; t < L.T; t += 32) {
                 const long e = (long)j * L.T + t;
                 const int itr = tsh < 31 ? (t >> tsh) : t / L.notr;
@@ -188,10 +207,10 @@ __global__ void __launch_bounds__(SEL2_THREADS)
         if (mode == 0) {
             float dv = d[e];
             if (!(dv < INFINITY) || (double)dv > dlim0) continue;
-            int k, itr;
+            double pd, pof;
             long lo;
-            decode_e(e, L, k, itr, lo);
-            w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
+            if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) continue;
+            w = hyp_weight(dv, mn, pd, pof);
         } else {
             w = wg[e];
         }
@@ -229,7 +248,9 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                     break;
                 }
             }
-            if (!stopped && t0 > 0.0) s_over = 1;  // cannot happen with the margin; finish in global memory
+            // cannot happen with the margin; finish in global memory (also the
+            // 3D walk into computed zero weights)
+            if (!stopped && (t0 > 0.0 || L.list_zeros)) s_over = 1;
             s_sig = sig;
             s_nsig = ns;
             int m = ns;
@@ -282,26 +303,34 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                             double* __restrict__ scratch, double* __restrict__ part, int* __restrict__ parti) {
     const int i = plist[blockIdx.x];
     double* buf = scratch + (long)blockIdx.x * slot_len;
-    __shared__ int ncand;
+    __shared__ int ncand, nzero;
+    __shared__ double red[32];
     double* pp = part + (long)i * 8;
     const double mn = pp[0], thr = pp[3];
     const float* d = diff2 ? diff2 + (long)i * X : nullptr;
     const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
     const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
-    if (threadIdx.x == 0) ncand = 0;
+    if (threadIdx.x == 0) ncand = nzero = 0;
     __syncthreads();
+    double maxpd = 0.0;
     for (long e = threadIdx.x; e < X; e += blockDim.x) {
         double w;
         if (mode == 0) {
-            int k, itr;
+            double pd, pof;
             long lo;
-            decode_e(e, L, k, itr, lo);
-            w = hyp_weight(d[e], mn, pdir[k], po[k * L.ntr + itr]);
+            if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) continue;
+            const float dv = d[e];
+            if (!(dv < INFINITY)) continue;
+            maxpd = fmax(maxpd, pd * pof);
+            w = hyp_weight(dv, mn, pd, pof);
+            if (w == 0.0 && L.list_zeros) atomicAdd(&nzero, 1);
         } else {
             w = wg[e];
         }
         if (w > 0.0) buf[atomicAdd(&ncand, 1)] = w;
     }
+    for (int off = 16; off > 0; off >>= 1) maxpd = fmax(maxpd, __shfl_down_sync(0xffffffffu, maxpd, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = maxpd;
     __syncthreads();
     const int cnt = ncand;
     long n2 = 1;
@@ -327,19 +356,27 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     if (threadIdx.x == 0) {
         double fw = 0.0, sig = 0.0;
         int ns = 0;
+        bool stopped = false;
         for (int q = 0; q < cnt; q++) {
             ns++;
             sig = buf[q];
             fw += sig;
-            if (fw > thr) break;
+            if (fw > thr) {
+                stopped = true;
+                break;
+            }
+        }
+        // 3D sorts every computed weight, zeros included (map3d_optimizer.cpp:1840-1864):
+        // a walk that passes all positive weights continues through the zeros
+        if (!stopped && nzero > 0) {
+            ns += nzero;
+            sig = 0.0;
         }
         pp[2] = sig;
         parti[(long)i * 8 + 1] = ns;
-        double maxpd = 0.0;
-        if (mode == 0)
-            for (int k = 0; k < L.K; k++)
-                for (int t = 0; t < L.ntr; t++) maxpd = fmax(maxpd, pdir[k] * po[k * L.ntr + t]);
-        pp[5] = (sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
+        double mp = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) mp = fmax(mp, red[w]);
+        pp[5] = (sig > 0.0 && mp > 0.0) ? mn + log(mp / sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
     }
 }
 
@@ -359,11 +396,10 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     for (long e = threadIdx.x; e < X; e += blockDim.x) {
         float dv = d[e];
-        if (dv < INFINITY && (double)dv <= dcut) {
-            int k, itr;
-            long lo;
-            decode_e(e, L, k, itr, lo);
-            if (hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]) >= sig) atomicAdd(&cnt, 1);
+        double pd, pof;
+        long lo;
+        if (dv < INFINITY && (double)dv <= dcut && hyp_prior(e, i, L, pdir, po, pd, pof, lo)) {
+            if (hyp_weight(dv, mn, pd, pof) >= sig) atomicAdd(&cnt, 1);
         }
     }
     __syncthreads();
@@ -376,11 +412,10 @@ __global__ void __launch_bounds__(256)
     __syncthreads();
     for (long e = threadIdx.x; e < X; e += blockDim.x) {
         float dv = d[e];
-        if (dv < INFINITY && (double)dv <= dcut) {
-            int k, itr;
-            long lo;
-            decode_e(e, L, k, itr, lo);
-            double w = hyp_weight(dv, mn, pdir[k], po[k * L.ntr + itr]);
+        double pd, pof;
+        long lo;
+        if (dv < INFINITY && (double)dv <= dcut && hyp_prior(e, i, L, pdir, po, pd, pof, lo)) {
+            double w = hyp_weight(dv, mn, pd, pof);
             if (w >= sig) {
                 int q = base + atomicAdd(&cnt, 1);
                 if (q < cap) list[q] = SigEntry{i, (int)e, w / sumw};
@@ -450,4 +485,5 @@ inline SelectResult run_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P
     return res;
 }
 
+}  // namespace
 }  // namespace rome

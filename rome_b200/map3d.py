@@ -1,0 +1,222 @@
+"""Host side of the MAP3D E-step: the pool description that mirrors
+``Map3dOptimizer_old``'s expectation state (src/map3d_optimizer.cpp:615-727)
+and the call into ``rome_gpu_map3d_estep_pool``.
+
+The sampling tables are the caller's: ``angles[p][dir][psi][over_rot]`` is
+what ``SamplingGrid::setOrientation`` returns for pass p
+(src/sampling.cpp), ``over_trans_x/y[p]`` are ``exp_over_trans_x/y``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import abi
+from .map2d import GpuContext, _f64, _i32
+
+__all__ = ["Map3dPool", "map3d_estep_pool", "pool3d_from_dump", "fine_lists_from_dump"]
+
+
+@dataclasses.dataclass
+class Map3dPool:
+    ori_size: int
+    current_size: int
+    coarse_size: int
+    nr_classes: int
+    nr_groups: int
+    nr_dir: int
+    angles: list            # [2] arrays [ndir][npsi][nor][3]
+    over_trans_x: list      # [2] arrays [ntr][notr]
+    over_trans_y: list
+    trans_x: np.ndarray
+    trans_y: np.ndarray
+    Fimg_real: np.ndarray   # [P][F(current_size)]
+    Fimg_imag: np.ndarray
+    Fimg_nomask_real: np.ndarray
+    Fimg_nomask_imag: np.ndarray
+    Fctf: np.ndarray
+    highres_Xi2: np.ndarray
+    old_offsetx: np.ndarray
+    old_offsety: np.ndarray
+    group: np.ndarray
+    sigma2_noise: np.ndarray      # [G][ori/2+1]
+    Mresol_fine: np.ndarray
+    Mresol_coarse: np.ndarray
+    pdf_class: np.ndarray         # [K]
+    pdf_direction: np.ndarray     # [K][ndir]
+    prior_offsetx_class: np.ndarray
+    prior_offsety_class: np.ndarray
+    sigma2_offset: float
+    sigma2_fudge: float = 1.0
+    adaptive_fraction: float = 0.999
+    do_ctf_correction: bool = True
+    refs_are_ctf_corrected: bool = True
+    do_map: bool = True
+    iclass_min: int = 0
+    iclass_max: int = -1
+    adaptive_oversampling: int = 1
+
+    @property
+    def nr_images(self) -> int:
+        return int(self.Fimg_real.shape[0])
+
+    @property
+    def nr_psi(self) -> int:
+        return int(self.angles[0].shape[1])
+
+    @property
+    def nr_trans(self) -> int:
+        return int(self.over_trans_x[0].shape[0])
+
+    @property
+    def ncoarse(self) -> int:
+        return self.nr_classes * self.nr_dir * self.nr_psi * self.nr_trans
+
+
+def _pack(p: Map3dPool):
+    keep = []
+
+    def d(a):
+        a = _f64(a)
+        keep.append(a)
+        return abi.dptr(a)
+
+    def i(a):
+        a = _i32(a)
+        keep.append(a)
+        return abi.iptr(a)
+
+    s = abi.RomeMap3dPool()
+    s.nr_images, s.ori_size, s.current_size, s.coarse_size = p.nr_images, p.ori_size, p.current_size, p.coarse_size
+    s.nr_classes, s.nr_groups = p.nr_classes, p.nr_groups
+    s.iclass_min = p.iclass_min
+    s.iclass_max = p.iclass_max if p.iclass_max >= 0 else p.nr_classes - 1
+    s.adaptive_oversampling = p.adaptive_oversampling
+    s.nr_dir, s.nr_psi, s.nr_trans = p.nr_dir, p.nr_psi, p.nr_trans
+    for q in range(2):
+        s.angles[q] = d(p.angles[q])
+        s.over_trans_x[q] = d(p.over_trans_x[q])
+        s.over_trans_y[q] = d(p.over_trans_y[q])
+    s.trans_x, s.trans_y = d(p.trans_x), d(p.trans_y)
+    s.Fimg_real, s.Fimg_imag = d(p.Fimg_real), d(p.Fimg_imag)
+    s.Fimg_nomask_real, s.Fimg_nomask_imag = d(p.Fimg_nomask_real), d(p.Fimg_nomask_imag)
+    s.Fctf, s.highres_Xi2 = d(p.Fctf), d(p.highres_Xi2)
+    s.old_offsetx, s.old_offsety, s.group = d(p.old_offsetx), d(p.old_offsety), i(p.group)
+    s.sigma2_noise, s.Mresol_fine, s.Mresol_coarse = d(p.sigma2_noise), i(p.Mresol_fine), i(p.Mresol_coarse)
+    s.pdf_class, s.pdf_direction = d(p.pdf_class), d(p.pdf_direction)
+    s.prior_offsetx_class, s.prior_offsety_class = d(p.prior_offsetx_class), d(p.prior_offsety_class)
+    s.sigma2_offset, s.sigma2_fudge, s.adaptive_fraction = p.sigma2_offset, p.sigma2_fudge, p.adaptive_fraction
+    s.do_ctf_correction, s.refs_are_ctf_corrected = int(p.do_ctf_correction), int(p.refs_are_ctf_corrected)
+    s.do_map = int(p.do_map)
+    s.do_scale_correction = 0
+    s.do_cross_correlation = 0
+    s.inputs_on_device = 0
+    return s, keep
+
+
+def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
+                     fine_capacity: Optional[int] = None) -> Dict[str, np.ndarray]:
+    """One pool through ``rome_gpu_map3d_estep_pool``; returns the per-particle
+    results, the model sums of this pool, and (with ``checkpoints``) the coarse
+    diff2 array, Mcoarse_significant and the fine-pass lists."""
+    P, K, G, oF = p.nr_images, p.nr_classes, p.nr_groups, p.ori_size // 2 + 1
+    s, keep = _pack(p)
+    o: Dict[str, np.ndarray] = {}
+    so = abi.RomeMap3dPoolOut()
+    for name in ("min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "rot", "tilt",
+                 "psi", "xoff", "yoff", "nr_sign"):
+        o[name] = np.zeros(P)
+        setattr(so, name, abi.dptr(o[name]))
+    o["cls"] = np.zeros(P, np.int32)
+    so.cls = abi.iptr(o["cls"])
+    o["wsum_sigma2_noise"] = np.zeros((G, oF))
+    o["wsum_pdf_class"] = np.zeros(K)
+    o["wsum_pdf_direction"] = np.zeros((K, p.nr_dir))
+    o["wsum_sigma2_offset"] = np.zeros(1)
+    o["wsum_sumw_group"] = np.zeros(G)
+    for name in ("wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_sigma2_offset",
+                 "wsum_sumw_group"):
+        setattr(so, name, abi.dptr(o[name]))
+    if checkpoints:
+        for q in range(2):
+            for name in ("pass_min_diff2", "pass_sum_weight", "pass_significant_weight"):
+                o[f"{name}{q}"] = np.zeros(P)
+                getattr(so, name)[q] = abi.dptr(o[f"{name}{q}"])
+        o["coarse_diff2"] = np.zeros((P, p.ncoarse))
+        so.coarse_diff2 = abi.dptr(o["coarse_diff2"])
+        o["Mcoarse_significant"] = np.zeros((P, p.ncoarse), np.int8)
+        so.Mcoarse_significant = abi.cptr(o["Mcoarse_significant"])
+        cap = fine_capacity if fine_capacity is not None else P * p.ncoarse * 32
+        o["fine_count"] = np.zeros(P, np.int32)
+        o["fine_index"] = np.zeros(cap, np.int64)
+        o["fine_diff2"] = np.zeros(cap)
+        o["fine_weight"] = np.zeros(cap)
+        so.fine_capacity = cap
+        so.fine_count = abi.iptr(o["fine_count"])
+        so.fine_index = o["fine_index"].ctypes.data_as(C.POINTER(C.c_long))
+        so.fine_diff2 = abi.dptr(o["fine_diff2"])
+        so.fine_weight = abi.dptr(o["fine_weight"])
+    ctx._check(ctx.lib.rome_gpu_map3d_estep_pool(ctx.h, C.byref(s), C.byref(so)))
+    if checkpoints:
+        n = int(o["fine_count"].sum())
+        for name in ("fine_index", "fine_diff2", "fine_weight"):
+            o[name] = o[name][:n]
+    return o
+
+
+def pool3d_from_dump(d: Dict[str, np.ndarray], pool: int = 0) -> Map3dPool:
+    """The E-step inputs of one pool recorded by oracle/ref_harness/map3d_dump."""
+    pp = f"pool{pool}_"
+    g = lambda k: d[k]  # noqa: E731
+    sc = lambda k: float(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    return Map3dPool(
+        ori_size=ic("ori_size"), current_size=ic("current_size"), coarse_size=ic("coarse_size"),
+        nr_classes=ic("nr_classes"), nr_groups=ic("nr_groups"), nr_dir=ic("nr_dir"),
+        angles=[g(f"{pp}pass0_angles"), g(f"{pp}pass1_angles")],
+        over_trans_x=[g(f"{pp}pass0_over_trans_x"), g(f"{pp}pass1_over_trans_x")],
+        over_trans_y=[g(f"{pp}pass0_over_trans_y"), g(f"{pp}pass1_over_trans_y")],
+        trans_x=g("trans_x"), trans_y=g("trans_y"),
+        Fimg_real=g(pp + "Fimg_real"), Fimg_imag=g(pp + "Fimg_imag"),
+        Fimg_nomask_real=g(pp + "Fimg_nomask_real"), Fimg_nomask_imag=g(pp + "Fimg_nomask_imag"),
+        Fctf=g(pp + "Fctf"), highres_Xi2=g(pp + "highres_Xi2"),
+        old_offsetx=g(pp + "old_offsetx"), old_offsety=g(pp + "old_offsety"), group=g(pp + "group"),
+        sigma2_noise=g("sigma2_noise"), Mresol_fine=g("Mresol_fine"), Mresol_coarse=g("Mresol_coarse"),
+        pdf_class=g("pdf_class"), pdf_direction=g("pdf_direction"),
+        prior_offsetx_class=g("prior_offsetx_class"), prior_offsety_class=g("prior_offsety_class"),
+        sigma2_offset=sc("sigma2_offset"), sigma2_fudge=sc("sigma2_fudge"),
+        adaptive_fraction=sc("adaptive_fraction"), do_ctf_correction=bool(ic("do_ctf_correction")),
+        refs_are_ctf_corrected=bool(ic("refs_are_ctf_corrected")), do_map=bool(ic("do_map")),
+        adaptive_oversampling=ic("adaptive_oversampling"))
+
+
+def fine_lists_from_dump(d: Dict[str, np.ndarray], prefix: str, nr_trans: int, nh: int = 32):
+    """Exp_Mweight_old lists of a dump (count[P][K][ndir][npsi], ihidden, value)
+    re-indexed like the library's fine_index: coarse index (k, dir, psi, trans)
+    * nh + over_rot * nr_over_trans + over_trans, with nh = nr_over_rot *
+    nr_over_trans (32 in the fine pass, 1 in the coarse pass, where the index
+    is the coarse index itself).  Returns per-particle (index, value)."""
+    cnt = d[prefix + "count"]
+    ih = d[prefix + "ihidden"].astype(np.int64)
+    val = d[prefix + "value"]
+    P = cnt.shape[0]
+    flat = cnt.reshape(P, -1)
+    out = []
+    q = 0
+    for i in range(P):
+        idx, v = [], []
+        for kdp, n in enumerate(flat[i]):
+            if n == 0:
+                continue
+            h = ih[q:q + n]
+            itr = h // nh
+            rest = h - itr * nh  # over_rot * nr_over_trans + over_trans
+            idx.append((kdp * nr_trans + itr) * nh + rest)
+            v.append(val[q:q + n])
+            q += n
+        out.append((np.concatenate(idx) if idx else np.zeros(0, np.int64),
+                     np.concatenate(v) if v else np.zeros(0)))
+    return out

@@ -29,6 +29,12 @@ __all__ = [
     "write_mrcs",
     "write_star",
     "write_dataset_2d",
+    "Map3dSpec",
+    "euler_matrix",
+    "make_volumes_3d",
+    "render_volume",
+    "make_particles_3d",
+    "write_dataset_3d",
 ]
 
 
@@ -189,3 +195,134 @@ def write_dataset_2d(out_dir: str, spec: Map2dSpec, name: str = "particles") -> 
     write_star(star, mrcs, meta, spec.voltage, spec.cs, spec.q0)
     np.savez(os.path.join(out_dir, name + "_truth.npz"), **meta)
     return star
+
+
+# ---------------------------------------------------------------------------
+# 3D: blob volumes, projections at uniform random orientations
+
+
+@dataclasses.dataclass
+class Map3dSpec:
+    n_particles: int = 1000
+    size: int = 64
+    n_classes: int = 4
+    n_blobs: int = 60
+    blob_sigma: Sequence[float] = (2.0, 8.0)
+    max_shift: float = 4.0
+    defocus: Sequence[float] = (10000.0, 30000.0)
+    voltage: float = 300.0
+    cs: float = 2.7
+    q0: float = 0.1
+    pixel: float = 2.0
+    snr: float = 0.05
+    seed: int = 1
+
+
+def euler_matrix(rot: float, tilt: float, psi: float) -> np.ndarray:
+    """ZYZ Euler matrix in degrees, the convention of ``Euler_angles2matrix``
+    (src/math.cpp:86-115)."""
+    a, b, g = np.deg2rad([rot, tilt, psi])
+    ca, cb, cg, sa, sb, sg = np.cos(a), np.cos(b), np.cos(g), np.sin(a), np.sin(b), np.sin(g)
+    cc, cs, sc, ss = cb * ca, cb * sa, sb * ca, sb * sa
+    return np.array([[cg * cc - sg * sa, cg * cs + sg * ca, -cg * sb],
+                     [-sg * cc - cg * sa, -sg * cs + cg * ca, sg * sb],
+                     [sc, ss, cb]])
+
+
+def make_volumes_3d(rng: np.random.Generator, spec: Map3dSpec) -> List[dict]:
+    """K volumes, each a sum of ``n_blobs`` isotropic Gaussian blobs inside the particle sphere."""
+    out = []
+    radius = 0.3 * spec.size
+    for _ in range(spec.n_classes):
+        v = rng.normal(size=(spec.n_blobs, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        r = radius * rng.uniform(0, 1, spec.n_blobs) ** (1.0 / 3.0)
+        out.append(dict(centers=v * r[:, None],
+                        sigmas=rng.uniform(spec.blob_sigma[0], spec.blob_sigma[1], spec.n_blobs),
+                        amps=rng.uniform(0.5, 1.0, spec.n_blobs)))
+    return out
+
+
+def render_volume(size: int, vol: dict) -> np.ndarray:
+    """Real-space volume [z][y][x], origin at size//2 (the reference's centre convention)."""
+    c = np.arange(size) - size // 2
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    out = np.zeros((size,) * 3, np.float64)
+    for (cx, cy, cz), s, a in zip(vol["centers"], vol["sigmas"], vol["amps"]):
+        out += a * np.exp(-((xx - cx) ** 2 + (yy - cy) ** 2 + (zz - cz) ** 2) / (2 * s * s))
+    return out
+
+
+def _uniform_rotations(rng: np.random.Generator, n: int):
+    """Orientations uniform on SO(3): rot, psi uniform, cos(tilt) uniform."""
+    rot = rng.uniform(0.0, 360.0, n)
+    tilt = np.rad2deg(np.arccos(rng.uniform(-1.0, 1.0, n)))
+    psi = rng.uniform(0.0, 360.0, n)
+    return rot, tilt, psi
+
+
+def make_particles_3d(spec: Map3dSpec, volumes: Optional[List[dict]] = None):
+    """Project class volumes at uniform random orientations, shift, CTF, noise.
+
+    A Gaussian blob of width s projects to a 2D Gaussian of the same width
+    with amplitude a*s*sqrt(2 pi) centred at (A c)_xy, which is the real-space
+    counterpart of the Fourier slice the reference extracts with A^T
+    (src/reconstruct.cpp:226-410), so projections are exact.
+    """
+    rng = np.random.default_rng(spec.seed)
+    if volumes is None:
+        volumes = make_volumes_3d(rng, spec)
+    n, s = spec.n_particles, spec.size
+    cls = rng.integers(0, spec.n_classes, n)
+    rot, tilt, psi = _uniform_rotations(rng, n)
+    shx = rng.uniform(-spec.max_shift, spec.max_shift, n)
+    shy = rng.uniform(-spec.max_shift, spec.max_shift, n)
+    du = rng.uniform(spec.defocus[0], spec.defocus[1], n)
+    dv = rng.uniform(spec.defocus[0], spec.defocus[1], n)
+    dang = rng.uniform(0.0, 180.0, n)
+    imgs = np.empty((n, s, s), np.float32)
+    c = np.arange(s) - s // 2
+    yy, xx = np.meshgrid(c, c, indexing="ij")
+    disc = (xx * xx + yy * yy) <= (0.45 * s) ** 2
+    for p in range(n):
+        v = volumes[cls[p]]
+        A = euler_matrix(rot[p], tilt[p], psi[p])
+        cen = (v["centers"] @ A.T)[:, :2] + np.array([shx[p], shy[p]])
+        img = _render_blobs_2d(s, cen, v["sigmas"], v["amps"] * v["sigmas"] * np.sqrt(2 * np.pi))
+        F = np.fft.rfft2(np.fft.ifftshift(img))
+        F *= ctf_image(s, s, spec.pixel, du[p], dv[p], dang[p], spec.voltage, spec.cs, spec.q0)
+        sig = np.fft.fftshift(np.fft.irfft2(F, s=(s, s)))
+        var = float(np.var(sig[disc]))
+        sigma = np.sqrt(var / spec.snr) if var > 0 else 1.0
+        noisy = sig + rng.normal(0.0, sigma, (s, s))
+        noisy = (noisy - noisy[~disc].mean()) / max(noisy[~disc].std(), 1e-12)
+        imgs[p] = noisy.astype(np.float32)
+    meta = dict(cls=cls, rot=rot, tilt=tilt, psi=psi, shx=shx, shy=shy, du=du, dv=dv, dang=dang)
+    return imgs, meta, volumes
+
+
+def write_dataset_3d(out_dir: str, spec: Map3dSpec, name: str = "particles", ref_lowpass_sigma: float = 2.0):
+    """Generate a 3D dataset and a starting reference volume.
+
+    Returns (STAR path, reference MRC path).  The reference is the average of
+    the class volumes blurred by a Gaussian of ``ref_lowpass_sigma`` pixels
+    (every class starts from it, as ``MAPModel::initializeRef`` does,
+    src/map_model.cpp:56-84).
+    """
+    os.makedirs(out_dir, exist_ok=True)
+    imgs, meta, volumes = make_particles_3d(spec)
+    mrcs = os.path.abspath(os.path.join(out_dir, name + ".mrcs"))
+    star = os.path.join(out_dir, name + ".star")
+    write_mrcs(mrcs, imgs, spec.pixel)
+    write_star(star, mrcs, meta, spec.voltage, spec.cs, spec.q0)
+    blurred = []
+    for v in volumes:
+        b = dict(v)
+        b["sigmas"] = np.sqrt(v["sigmas"] ** 2 + ref_lowpass_sigma ** 2)
+        b["amps"] = v["amps"] * (v["sigmas"] / b["sigmas"]) ** 3
+        blurred.append(render_volume(spec.size, b))
+    ref = np.mean(blurred, axis=0)
+    ref_path = os.path.abspath(os.path.join(out_dir, name + "_ref.mrc"))
+    write_mrcs(ref_path, ref.astype(np.float32), spec.pixel)
+    np.savez(os.path.join(out_dir, name + "_truth.npz"), **meta)
+    return star, ref_path

@@ -25,7 +25,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from rome_b200.map2d import load_dump  # noqa: E402
-from rome_b200.synthetic import Map2dSpec, write_dataset_2d  # noqa: E402
+from rome_b200.synthetic import Map2dSpec, Map3dSpec, write_dataset_2d, write_dataset_3d  # noqa: E402
 
 # (dataset spec, reference options)
 CASES = {
@@ -46,6 +46,16 @@ CASES = {
                      offset_step=1, ctf=1)),
 }
 
+# 3D cases: (dataset spec, reference options) for oracle/_ref/map3d_dump
+CASES3D = {
+    # HEALPix order 1 (48 directions, 12 psi), oversampling 1, +-2 px step 1, iteration 2
+    "map3d_a": (Map3dSpec(n_particles=96, size=24, n_classes=2, n_blobs=10, blob_sigma=(1.2, 2.5), max_shift=2.0,
+                          snr=2.0, pixel=4.0, seed=7),
+                dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1, pool=4,
+                     offset_range=2, offset_step=1, ctf=1, uniform_directions=1)),
+}
+SKIP3D = ("Fimg_shifted_real", "Fimg_shifted_imag", "local_Fctf", "Minvsigma2", "local_sqrtXi2")
+
 # arrays copied from the dump into the fixture (the per-translation shifted
 # images and per-orientation projections are large and are checked through
 # the oracle instead)
@@ -53,8 +63,29 @@ SKIP_SUFFIXES = ("Fimg_shifted_real", "Fimg_shifted_imag", "Fref_real", "Fref_im
 
 
 def build_reference():
-    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "_ref/map2d_dump",
+    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "_ref/map2d_dump", "_ref/map3d_dump",
                            "_ref/librome_oracle.so"], stdout=subprocess.DEVNULL)
+
+
+def make_case3d(name: str):
+    spec, opt = CASES3D[name]
+    tmp = tempfile.mkdtemp(prefix="rome_golden_")
+    try:
+        star, ref = write_dataset_3d(os.path.join(tmp, "data"), spec)
+        dump = os.path.join(tmp, "dump")
+        cmd = [os.path.join(ROOT, "oracle", "_ref", "map3d_dump"), "-i", star, "-ref", ref, "-dump_dir", dump]
+        for k, v in opt.items():
+            cmd += [f"-{k}", str(v)]
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=tmp)
+        d = load_dump(dump)
+        keep = {k: v for k, v in d.items() if not k.endswith(SKIP3D)}
+        keep["meta_options"] = np.array([str(opt)])
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(out, **keep)
+        print(f"{name}: {len(keep)} arrays, {os.path.getsize(out) / 1e6:.2f} MB")
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
 
 
 def make_case(name: str):
@@ -67,7 +98,7 @@ def make_case(name: str):
         for k, v in opt.items():
             cmd += [f"-{k}", str(v)]
         env = dict(os.environ, OMP_NUM_THREADS="1")
-        subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env)
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=tmp)
         d = load_dump(dump)
         keep = {k: v for k, v in d.items() if not k.endswith(SKIP_SUFFIXES)}
         # a few shifted images / projections of pass 0 for the kernel-level checks
@@ -86,6 +117,9 @@ def make_case(name: str):
 
 if __name__ == "__main__":
     build_reference()
-    names = sys.argv[1:] or list(CASES)
+    names = sys.argv[1:] or list(CASES) + list(CASES3D)
     for n in names:
-        make_case(n)
+        if n in CASES3D:
+            make_case3d(n)
+        else:
+            make_case(n)
