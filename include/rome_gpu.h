@@ -355,6 +355,44 @@ typedef struct {
 
 int rome_gpu_reconstruct(RomeGpuCtx* ctx, const RomeReconIn* in, RomeReconOut* out);
 
+/* ---------------------------------------------------------------------
+ * Learned pose proposals (no counterpart in the reference).  A small CNN
+ * over a particle's low-pass Fourier magnitude predicts a distribution over
+ * (class, psi mod 180); it is trained on the GPU on (image, posterior)
+ * pairs produced by the exhaustive E-step, and its top-k outputs restrict
+ * the E-step's search (rome_gpu_map2d_estep_pool_proposed).
+ * Input: x[n][2][size][size] (rome_gpu_proposal_features); output index
+ * o = class * (nr_psi / 2) + (psi index mod nr_psi / 2).
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int size;          /* input grid side, multiple of 8, <= 64 */
+    int channels[4];   /* conv layers (3x3; strides 1, 2, 2, 2) */
+    int n_out;         /* outputs */
+} RomeProposalSpec;
+
+typedef struct RomeProposalNet RomeProposalNet;
+
+int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec* spec, unsigned long long seed,
+                             RomeProposalNet** net);
+void rome_gpu_proposal_destroy(RomeProposalNet* net);
+long rome_gpu_proposal_num_params(const RomeProposalNet* net);
+/* flat parameters w0 b0 .. w3 b3 wf bf, each block at a multiple of 4 floats */
+int rome_gpu_proposal_get_params(RomeProposalNet* net, float* params);
+int rome_gpu_proposal_set_params(RomeProposalNet* net, const float* params);
+/* network input of P particles from their masked Fourier images and CTFs
+ * at size cur (FFTW half-planes, FP64, host) */
+int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, const double* Fimg_real,
+                               const double* Fimg_imag, const double* ctf, float* x);
+/* mean soft-target cross-entropy of n samples, its gradient (flat, as the
+ * parameters) and the logits [n][n_out]; each output may be NULL */
+int rome_gpu_proposal_loss_grad(RomeProposalNet* net, int n, const float* x, const float* targets, double* loss,
+                                float* grad, float* logits);
+/* Adam (beta 0.9 / 0.999) over shuffled mini-batches; epoch_loss[epochs] */
+int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float* x, const float* targets, int epochs,
+                            int batch, float lr, unsigned long long seed, double* epoch_loss);
+/* top-k outputs per sample (descending) and their softmax probabilities */
+int rome_gpu_proposal_predict(RomeProposalNet* net, int n, const float* x, int k, int* idx, float* prob);
+
 #ifdef __cplusplus
 }
 #endif
