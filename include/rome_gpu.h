@@ -356,18 +356,21 @@ typedef struct {
 int rome_gpu_reconstruct(RomeGpuCtx* ctx, const RomeReconIn* in, RomeReconOut* out);
 
 /* ---------------------------------------------------------------------
- * Learned pose proposals (no counterpart in the reference).  A small CNN
- * over a particle's low-pass Fourier magnitude predicts a distribution over
- * (class, psi mod 180); it is trained on the GPU on (image, posterior)
- * pairs produced by the exhaustive E-step, and its top-k outputs restrict
- * the E-step's search (rome_gpu_map2d_estep_pool_proposed).
- * Input: x[n][2][size][size] (rome_gpu_proposal_features); output index
- * o = class * (nr_psi / 2) + (psi index mod nr_psi / 2).
+ * Learned pose proposals (no counterpart in the reference).  A small
+ * network over a particle's Fourier magnitude in polar coordinates
+ * (rotation = circular shift along the angle, every layer equivariant to
+ * it) predicts a distribution over (class, psi mod 180); it is trained on
+ * the GPU on (image, posterior) pairs produced by the exhaustive E-step, and
+ * its top-k outputs restrict the E-step's search (RomeMap2dPool.proposals).
+ * Input: x[n][2][n_r][n_theta] (rome_gpu_proposal_features); output index
+ * o = class * n_theta + psi index mod n_theta, n_theta = nr_psi / 2.
  * ------------------------------------------------------------------- */
 typedef struct {
-    int size;          /* input grid side, multiple of 8, <= 64 */
-    int channels[4];   /* conv layers (3x3; strides 1, 2, 2, 2) */
-    int n_out;         /* outputs */
+    int n_r;            /* radial samples */
+    int n_theta;        /* angular samples over [0, 180) deg: nr_psi / 2 */
+    int channels[2];    /* the two 3x3 convolution layers */
+    int n_classes;      /* K */
+    double r_lo, r_hi;  /* radius range in Fourier pixels of the feature image */
 } RomeProposalSpec;
 
 typedef struct RomeProposalNet RomeProposalNet;
@@ -376,7 +379,7 @@ int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec* spec, unsi
                              RomeProposalNet** net);
 void rome_gpu_proposal_destroy(RomeProposalNet* net);
 long rome_gpu_proposal_num_params(const RomeProposalNet* net);
-/* flat parameters w0 b0 .. w3 b3 wf bf, each block at a multiple of 4 floats */
+/* flat parameters w0 b0 w1 b1 wf bf, each block at a multiple of 4 floats */
 int rome_gpu_proposal_get_params(RomeProposalNet* net, float* params);
 int rome_gpu_proposal_set_params(RomeProposalNet* net, const float* params);
 /* network input of P particles from their masked Fourier images and CTFs
@@ -384,7 +387,7 @@ int rome_gpu_proposal_set_params(RomeProposalNet* net, const float* params);
 int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, const double* Fimg_real,
                                const double* Fimg_imag, const double* ctf, float* x);
 /* mean soft-target cross-entropy of n samples, its gradient (flat, as the
- * parameters) and the logits [n][n_out]; each output may be NULL */
+ * parameters) and the logits [n][n_classes * n_theta]; outputs may be NULL */
 int rome_gpu_proposal_loss_grad(RomeProposalNet* net, int n, const float* x, const float* targets, double* loss,
                                 float* grad, float* logits);
 /* Adam (beta 0.9 / 0.999) over shuffled mini-batches; epoch_loss[epochs] */
@@ -392,6 +395,14 @@ int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float* x, const f
                             int batch, float lr, unsigned long long seed, double* epoch_loss);
 /* top-k outputs per sample (descending) and their softmax probabilities */
 int rome_gpu_proposal_predict(RomeProposalNet* net, int n, const float* x, int k, int* idx, float* prob);
+/* features + top-k of P particles (Fourier images and CTFs at size cur,
+ * host arrays, or device arrays on the context's device when
+ * inputs_on_device), expanded to the restricted E-step's input: proposals
+ * [P][2k] ascending orientation indices class * 2 n_theta + psi (host), and
+ * the probability mass of the k outputs per particle (host, may be NULL);
+ * k <= 64 */
+int rome_gpu_proposal_propose(RomeProposalNet* net, int P, int cur, const double* Fimg_real, const double* Fimg_imag,
+                              const double* ctf, int inputs_on_device, int k, int* proposals, float* mass);
 
 #ifdef __cplusplus
 }

@@ -3,19 +3,22 @@ checker for the CUDA training and inference kernels in
 rome_b200/csrc/proposal.cu, never called by the product).
 
 The network has no counterpart in the reference; it is the learned prior of
-the E-step (a small CNN over the low-pass Fourier magnitude of a particle that
-predicts a distribution over (class, psi mod 180)).  Layers, all FP64 here:
+the E-step.  It sees a particle's Fourier magnitude in polar coordinates,
+where an in-plane rotation by psi is a circular shift along the angle axis,
+and is equivariant to that shift by construction, so one set of weights
+serves every psi:
 
-    x [N][2][S][S]
-    conv3x3 s1 (2 -> c0) + ReLU
-    conv3x3 s2 (c0 -> c1) + ReLU
-    conv3x3 s2 (c1 -> c2) + ReLU
-    conv3x3 s2 (c2 -> c3) + ReLU          -> [N][c3][S/8][S/8]
-    flatten, linear (c3*(S/8)^2 -> O)     -> logits
-    loss = mean_n sum_o -t[n][o] * log softmax(z[n])[o]
+    x [N][2][R][A]     log(1 + |X|) and |CTF| at radii r_lo..r_hi (R bins)
+                       and angles theta_a = a * 180 / A (A = nr_psi / 2)
+    conv3x3 (2 -> c0) + ReLU, conv3x3 (c0 -> c1) + ReLU
+                       (zero padding along r, circular along theta)
+    head: z[n][k][p] = bf[k] + sum_{c,r,d} wf[k][c][r][d] h[n][c][r][(d - p) mod A]
+    loss = mean_n sum_{k,p} -t[n][k][p] log softmax(z[n])[k][p]
 
-Convolutions use zero padding 1; a stride-2 output pixel (ho, wo) reads the
-input at (2 ho + kh - 1, 2 wo + kw - 1).
+With P_psi(k) = F_T(R(psi) k) for the reference's rotate2D (Euler(0, 0, psi)
+transposed), the magnitude seen at angle theta is the template's at theta +
+psi, so the correlation above peaks at p = psi / (180 / A): output p is the
+psi index modulo 180 degrees.  All arithmetic here is FP64.
 """
 from __future__ import annotations
 
@@ -23,62 +26,70 @@ from typing import Dict, List, Tuple
 
 import numpy as np
 
-STRIDES = (1, 2, 2, 2)
+
+def param_shapes(n_r: int, n_theta: int, channels: Tuple[int, int], n_classes: int) -> List[Tuple[str, tuple]]:
+    c0, c1 = channels
+    return [("w0", (c0, 2, 3, 3)), ("b0", (c0,)), ("w1", (c1, c0, 3, 3)), ("b1", (c1,)),
+            ("wf", (n_classes, c1, n_r, n_theta)), ("bf", (n_classes,))]
 
 
-def param_shapes(in_ch: int, size: int, channels: Tuple[int, int, int, int], n_out: int) -> List[Tuple[str, tuple]]:
-    shapes = []
-    c_prev = in_ch
-    for li, c in enumerate(channels):
-        shapes.append((f"w{li}", (c, c_prev, 3, 3)))
-        shapes.append((f"b{li}", (c,)))
-        c_prev = c
-    flat = channels[-1] * (size // 8) ** 2
-    shapes.append(("wf", (n_out, flat)))
-    shapes.append(("bf", (n_out,)))
-    return shapes
+def _pad(x: np.ndarray) -> np.ndarray:
+    """zero padding 1 along r (axis 2), circular padding 1 along theta (axis 3)"""
+    x = np.concatenate([x[..., -1:], x, x[..., :1]], axis=3)
+    z = np.zeros(x.shape[:2] + (1, x.shape[3]), x.dtype)
+    return np.concatenate([z, x, z], axis=2)
 
 
-def conv3x3(x: np.ndarray, w: np.ndarray, b: np.ndarray, stride: int) -> np.ndarray:
-    N, C, H, W = x.shape
-    Co = w.shape[0]
-    Ho, Wo = (H - 1) // stride + 1, (W - 1) // stride + 1
-    xp = np.zeros((N, C, H + 2, W + 2), x.dtype)
-    xp[:, :, 1:H + 1, 1:W + 1] = x
-    out = np.zeros((N, Co, Ho, Wo), x.dtype)
+def conv(x: np.ndarray, w: np.ndarray, b: np.ndarray) -> np.ndarray:
+    N, C, R, A = x.shape
+    xp = _pad(x)
+    out = np.zeros((N, w.shape[0], R, A))
     for kh in range(3):
         for kw in range(3):
-            patch = xp[:, :, kh:kh + stride * (Ho - 1) + 1:stride, kw:kw + stride * (Wo - 1) + 1:stride]
-            out += np.einsum("nchw,oc->nohw", patch, w[:, :, kh, kw])
+            out += np.einsum("nchw,oc->nohw", xp[:, :, kh:kh + R, kw:kw + A], w[:, :, kh, kw])
     return out + b[None, :, None, None]
 
 
-def conv3x3_backward(x, w, dy, stride):
-    N, C, H, W = x.shape
-    _, _, Ho, Wo = dy.shape
-    xp = np.zeros((N, C, H + 2, W + 2), x.dtype)
-    xp[:, :, 1:H + 1, 1:W + 1] = x
+def conv_backward(x, w, dy):
+    N, C, R, A = x.shape
+    xp = _pad(x)
     dxp = np.zeros_like(xp)
     dw = np.zeros_like(w)
     for kh in range(3):
         for kw in range(3):
-            sl = (slice(None), slice(None), slice(kh, kh + stride * (Ho - 1) + 1, stride),
-                  slice(kw, kw + stride * (Wo - 1) + 1, stride))
-            dw[:, :, kh, kw] = np.einsum("nohw,nchw->oc", dy, xp[sl])
-            dxp[sl] += np.einsum("nohw,oc->nchw", dy, w[:, :, kh, kw])
-    db = dy.sum(axis=(0, 2, 3))
-    return dxp[:, :, 1:H + 1, 1:W + 1], dw, db
+            dw[:, :, kh, kw] = np.einsum("nohw,nchw->oc", dy, xp[:, :, kh:kh + R, kw:kw + A])
+            dxp[:, :, kh:kh + R, kw:kw + A] += np.einsum("nohw,oc->nchw", dy, w[:, :, kh, kw])
+    dx = dxp[:, :, 1:R + 1, 1:A + 1].copy()
+    dx[:, :, :, 0] += dxp[:, :, 1:R + 1, A + 1]   # circular wrap of the theta padding
+    dx[:, :, :, A - 1] += dxp[:, :, 1:R + 1, 0]
+    return dx, dw, dy.sum(axis=(0, 2, 3))
+
+
+def head(h: np.ndarray, wf: np.ndarray, bf: np.ndarray) -> np.ndarray:
+    N, C, R, A = h.shape
+    z = np.zeros((N, wf.shape[0], A))
+    for p in range(A):
+        hs = np.roll(h, p, axis=3)  # hs[..., d] = h[..., (d - p) mod A]
+        z[:, :, p] = np.einsum("ncrd,kcrd->nk", hs, wf)
+    return z + bf[None, :, None]
+
+
+def head_backward(h, wf, dz):
+    N, C, R, A = h.shape
+    dwf = np.zeros_like(wf)
+    dh = np.zeros_like(h)
+    for p in range(A):
+        hs = np.roll(h, p, axis=3)
+        dwf += np.einsum("nk,ncrd->kcrd", dz[:, :, p], hs)
+        dh += np.roll(np.einsum("nk,kcrd->ncrd", dz[:, :, p], wf), -p, axis=3)
+    return dh, dwf, dz.sum(axis=(0, 2))
 
 
 def forward(params: Dict[str, np.ndarray], x: np.ndarray):
-    acts = [x]
-    h = x
-    for li, s in enumerate(STRIDES):
-        h = np.maximum(conv3x3(h, params[f"w{li}"], params[f"b{li}"], s), 0.0)
-        acts.append(h)
-    flat = h.reshape(h.shape[0], -1)
-    z = flat @ params["wf"].T + params["bf"]
-    return z, acts
+    h0 = np.maximum(conv(x, params["w0"], params["b0"]), 0.0)
+    h1 = np.maximum(conv(h0, params["w1"], params["b1"]), 0.0)
+    z = head(h1, params["wf"], params["bf"]).reshape(x.shape[0], -1)
+    return z, (x, h0, h1)
 
 
 def softmax(z: np.ndarray) -> np.ndarray:
@@ -87,44 +98,53 @@ def softmax(z: np.ndarray) -> np.ndarray:
 
 
 def loss_and_grads(params: Dict[str, np.ndarray], x: np.ndarray, t: np.ndarray):
-    """Mean soft-target cross-entropy over the batch and its gradients."""
+    """Mean soft-target cross-entropy over the batch, its gradients, logits."""
     N = x.shape[0]
-    z, acts = forward(params, x)
+    z, (x0, h0, h1) = forward(params, x)
     p = softmax(z)
     loss = float(-np.sum(t * np.log(np.maximum(p, 1e-300))) / N)
-    dz = (p - t) / N
+    dz = ((p - t) / N).reshape(N, params["wf"].shape[0], -1)
     g = {}
-    flat = acts[-1].reshape(N, -1)
-    g["wf"] = dz.T @ flat
-    g["bf"] = dz.sum(axis=0)
-    dh = (dz @ params["wf"]).reshape(acts[-1].shape)
-    for li in reversed(range(len(STRIDES))):
-        dh = dh * (acts[li + 1] > 0)
-        dx, g[f"w{li}"], g[f"b{li}"] = conv3x3_backward(acts[li], params[f"w{li}"], dh, STRIDES[li])
-        dh = dx
+    dh1, g["wf"], g["bf"] = head_backward(h1, params["wf"], dz)
+    dh1 = dh1 * (h1 > 0)
+    dh0, g["w1"], g["b1"] = conv_backward(h0, params["w1"], dh1)
+    dh0 = dh0 * (h0 > 0)
+    _, g["w0"], g["b0"] = conv_backward(x0, params["w0"], dh0)
     return loss, g, z
 
 
-def features(Fimg_real: np.ndarray, Fimg_imag: np.ndarray, ctf: np.ndarray, cur: int, size: int) -> np.ndarray:
-    """Network input from the particle's masked Fourier image (FFTW half-plane,
-    [cur][cur/2+1]): channel 0 log(1 + |X|), channel 1 |CTF|, on the centred
-    size x size grid of frequencies (kx, ky) in [-size/2, size/2), the
-    negative-kx half filled by Friedel symmetry |X(-k)| = |X(k)|; each channel
+def features(Fimg_real: np.ndarray, Fimg_imag: np.ndarray, ctf: np.ndarray, cur: int, n_r: int, n_theta: int,
+             r_lo: float, r_hi: float) -> np.ndarray:
+    """Network input from a particle's masked Fourier image (FFTW half-plane
+    [cur][cur/2+1]): bilinear samples of log(1 + |X|) and |CTF| at radius
+    r_i = r_lo + i (r_hi - r_lo) / (n_r - 1) and angle theta_a = a pi / n_theta
+    (kx = r cos, ky = r sin; negative kx by Friedel symmetry), each channel
     of each particle normalised to zero mean and unit variance."""
     P = Fimg_real.shape[0]
     cf = cur // 2 + 1
-    mag = np.sqrt(Fimg_real ** 2 + Fimg_imag ** 2).reshape(P, cur, cf)
+    mag = np.log1p(np.sqrt(Fimg_real ** 2 + Fimg_imag ** 2)).reshape(P, cur, cf)
     c = np.abs(ctf).reshape(P, cur, cf)
-    h = size // 2
-    out = np.zeros((P, 2, size, size))
-    for iy in range(size):
-        ky = iy - h
-        for ix in range(size):
-            kx = ix - h
-            sx, sy = (kx, ky) if kx >= 0 else (-kx, -ky)
-            row = sy if sy >= 0 else sy + cur
-            out[:, 0, iy, ix] = np.log1p(mag[:, row, sx])
-            out[:, 1, iy, ix] = c[:, row, sx]
+    out = np.zeros((P, 2, n_r, n_theta))
+
+    def sample(img, kx, ky):
+        # value at integer frequency (x, y) with Friedel symmetry for x < 0
+        def at(x, y):
+            if x < 0:
+                x, y = -x, -y
+            row = y if y >= 0 else y + cur
+            return img[:, row, x]
+        x0, y0 = int(np.floor(kx)), int(np.floor(ky))
+        fx, fy = kx - x0, ky - y0
+        return ((1 - fy) * ((1 - fx) * at(x0, y0) + fx * at(x0 + 1, y0))
+                + fy * ((1 - fx) * at(x0, y0 + 1) + fx * at(x0 + 1, y0 + 1)))
+
+    for i in range(n_r):
+        r = r_lo + i * (r_hi - r_lo) / (n_r - 1)
+        for a in range(n_theta):
+            th = a * np.pi / n_theta
+            kx, ky = r * np.cos(th), r * np.sin(th)
+            out[:, 0, i, a] = sample(mag, kx, ky)
+            out[:, 1, i, a] = sample(c, kx, ky)
     m = out.mean(axis=(2, 3), keepdims=True)
     s = out.std(axis=(2, 3), keepdims=True)
     return (out - m) / np.maximum(s, 1e-12)

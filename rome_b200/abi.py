@@ -105,6 +105,11 @@ class RomeMap3dPoolOut(C.Structure):
     ]
 
 
+class RomeProposalSpec(C.Structure):
+    _fields_ = [("n_r", C.c_int), ("n_theta", C.c_int), ("channels", C.c_int * 2), ("n_classes", C.c_int),
+                ("r_lo", C.c_double), ("r_hi", C.c_double)]
+
+
 class RomeReconIn(C.Structure):
     _fields_ = [("iclass", C.c_int), ("gridding_nr_iter", C.c_int), ("do_map", C.c_int), ("minres_map", C.c_int),
                 ("tau2_fudge", C.c_double), ("normalise", C.c_double), ("tau2_in", _DP)]
@@ -141,6 +146,10 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_abi_version", "rome_gpu_set_projectors", "rome_gpu_get_backprojector",
     "rome_gpu_set_backprojector", "rome_gpu_map2d_estep_pool", "rome_gpu_select_significant",
     "rome_gpu_select_significant_static", "rome_gpu_map3d_estep_pool",
+    "rome_gpu_proposal_create", "rome_gpu_proposal_destroy", "rome_gpu_proposal_num_params",
+    "rome_gpu_proposal_get_params", "rome_gpu_proposal_set_params", "rome_gpu_proposal_features",
+    "rome_gpu_proposal_loss_grad", "rome_gpu_proposal_train", "rome_gpu_proposal_predict",
+    "rome_gpu_proposal_propose",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings",
 ]
 
@@ -170,6 +179,22 @@ def load_library():
     lib.rome_gpu_set_backprojector.argtypes = [C.c_void_p, C.c_int, _DP, _DP]
     lib.rome_gpu_map2d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap2dPool), C.POINTER(RomeMap2dPoolOut)]
     lib.rome_gpu_map3d_estep_pool.argtypes = [C.c_void_p, C.POINTER(RomeMap3dPool), C.POINTER(RomeMap3dPoolOut)]
+    _FP = C.POINTER(C.c_float)
+    lib.rome_gpu_proposal_create.argtypes = [C.c_void_p, C.POINTER(RomeProposalSpec), C.c_ulonglong,
+                                             C.POINTER(C.c_void_p)]
+    lib.rome_gpu_proposal_destroy.argtypes = [C.c_void_p]
+    lib.rome_gpu_proposal_destroy.restype = None
+    lib.rome_gpu_proposal_num_params.argtypes = [C.c_void_p]
+    lib.rome_gpu_proposal_num_params.restype = C.c_long
+    lib.rome_gpu_proposal_get_params.argtypes = [C.c_void_p, _FP]
+    lib.rome_gpu_proposal_set_params.argtypes = [C.c_void_p, _FP]
+    lib.rome_gpu_proposal_features.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP, _DP, _FP]
+    lib.rome_gpu_proposal_loss_grad.argtypes = [C.c_void_p, C.c_int, _FP, _FP, _DP, _FP, _FP]
+    lib.rome_gpu_proposal_train.argtypes = [C.c_void_p, C.c_int, _FP, _FP, C.c_int, C.c_int, C.c_float,
+                                            C.c_ulonglong, _DP]
+    lib.rome_gpu_proposal_predict.argtypes = [C.c_void_p, C.c_int, _FP, C.c_int, _IP, _FP]
+    lib.rome_gpu_proposal_propose.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_int, C.c_int, _IP, _FP]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]

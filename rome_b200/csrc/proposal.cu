@@ -1,18 +1,23 @@
-// Learned pose proposals for the MAP E-step: a small CNN over the low-pass
-// Fourier magnitude of each particle that predicts a distribution over
-// (class, psi mod 180 deg), trained on the GPU on (image, posterior) pairs
-// produced by the exhaustive E-step itself, with hand-written FP32 forward,
-// backward and Adam kernels.  Its top-k (class, psi) pairs (each psi taken
-// with psi + 180, which the magnitude cannot tell apart) restrict the
-// E-step's search; the exhaustive E-step stays the fallback and the judge.
+// Learned pose proposals for the MAP E-step (no counterpart in the
+// reference): a small network over a particle's Fourier magnitude in polar
+// coordinates predicts a distribution over (class, psi mod 180 deg); it is
+// trained on the GPU on (image, posterior) pairs produced by the exhaustive
+// E-step itself, with hand-written FP32 forward, backward and Adam kernels.
+// Its top-k (class, psi) pairs (each psi with psi + 180, which the magnitude
+// cannot tell apart) restrict the E-step's search; the exhaustive E-step
+// stays the fallback and the judge.
 //
-// Network (N samples, S x S input, channels c0..c3, O outputs):
-//   x[N][2][S][S] -> conv3x3 s1 + ReLU -> conv3x3 s2 + ReLU
-//                 -> conv3x3 s2 + ReLU -> conv3x3 s2 + ReLU -> [N][c3][S/8][S/8]
-//                 -> linear -> z[N][O];  loss = mean_n sum_o -t log softmax(z)
-// Parameters are one flat FP32 array in the order w0 b0 w1 b1 w2 b2 w3 b3 wf bf
-// (w[l]: [c_l][c_{l-1}][3][3], wf: [O][c3 (S/8)^2]), each block starting at a
-// multiple of 4 floats (zero padding between blocks).
+// In polar coordinates an in-plane rotation is a circular shift along the
+// angle axis, and every layer is equivariant to that shift, so one set of
+// weights serves all psi (a first design, a plain CNN with a dense head,
+// generalised poorly: it had to learn every rotation of every class
+// separately):
+//   x[N][2][R][A]  log(1+|X|), |CTF| at R radii x A = nr_psi/2 angles in [0, 180)
+//   conv3x3 (2 -> c0) + ReLU, conv3x3 (c0 -> c1) + ReLU   (r: zero pad, theta: circular)
+//   z[n][k][p] = bf[k] + sum_{c,r,d} wf[k][c][r][d] h[n][c][r][(d - p) mod A]
+//   loss = mean_n sum -t log softmax(z[n])  (soft targets: the E-step posterior)
+// Parameters: one flat FP32 array w0 b0 w1 b1 wf bf, each block at a multiple
+// of 4 floats.  The CPU restatement is oracle/proposal_oracle.py.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -21,33 +26,29 @@
 #include <vector>
 
 #include "common.cuh"
-#include "epilogues.cuh"
-#include "gemm_simt.cuh"
 
 using namespace rome;
 
 struct RomeProposalNet {
     RomeGpuCtx* ctx = nullptr;
     RomeProposalSpec spec{};
-    int ch[5] = {0};     // ch[0] = input channels
-    int hw[5] = {0};     // spatial size after each layer
-    long off_w[5] = {0}, off_b[5] = {0};  // index 4 = the linear layer
+    int R = 0, A = 0, K = 0, c0 = 0, c1 = 0;
+    long off[6] = {0};  // w0 b0 w1 b1 wf bf
     long nparam = 0;
-    int flat = 0;        // c3 * (S/8)^2
     float* params = nullptr;
     float* grads = nullptr;
     float* adam_m = nullptr;
     float* adam_v = nullptr;
     long adam_t = 0;
-    // batch buffers (capacity cap_n)
-    int cap_n = 0;
-    float* act[5] = {nullptr};   // act[0] input, act[l+1] post-ReLU of layer l
-    float* dact[5] = {nullptr};
-    float* z = nullptr;          // [N][O]
+    int cap_n = 0;        // batch capacity
+    float* x = nullptr;   // [N][2][R][A]
+    float* h0 = nullptr;  // [N][c0][R][A]
+    float* h1 = nullptr;  // [N][c1][R][A]
+    float* dh0 = nullptr;
+    float* dh1 = nullptr;
+    float* z = nullptr;   // [N][K*A]
     float* dz = nullptr;
-    float* tgt = nullptr;        // [N][O]
-    float* tmpA = nullptr;       // transposes for the linear layer
-    float* tmpB = nullptr;
+    float* tgt = nullptr;
     double* loss_acc = nullptr;
     int* idx = nullptr;
 };
@@ -57,35 +58,35 @@ namespace {
 
 constexpr int PT = 256;
 
-// ---- convolution 3x3, zero padding 1, stride s, fused bias + ReLU ----
-__global__ void __launch_bounds__(PT) conv_fwd_kernel(int Ci, int H, int W, int Co, int Ho, int Wo, int s,
-                                                       const float* __restrict__ x, const float* __restrict__ w,
-                                                       const float* __restrict__ b, float* __restrict__ y) {
+// ---- 3x3 convolution on the polar grid: zero padding along r, circular along theta ----
+__global__ void __launch_bounds__(PT) pconv_fwd_kernel(int Ci, int R, int A, int Co, const float* __restrict__ x,
+                                                        const float* __restrict__ w, const float* __restrict__ b,
+                                                        float* __restrict__ y) {
     extern __shared__ float sw[];  // Ci * 9 weights of this output channel
     const int co = blockIdx.y, n = blockIdx.z;
     for (int q = threadIdx.x; q < Ci * 9; q += PT) sw[q] = w[(long)co * Ci * 9 + q];
     __syncthreads();
     const int p = blockIdx.x * PT + threadIdx.x;
-    if (p >= Ho * Wo) return;
-    const int ho = p / Wo, wo = p - ho * Wo;
-    const float* xn = x + (long)n * Ci * H * W;
+    if (p >= R * A) return;
+    const int r = p / A, a = p - r * A;
+    const float* xn = x + (long)n * Ci * R * A;
     float acc = b[co];
     for (int ci = 0; ci < Ci; ci++) {
-        const float* xc = xn + (long)ci * H * W;
+        const float* xc = xn + (long)ci * R * A;
         const float* wc = sw + ci * 9;
 #pragma unroll
         for (int kh = 0; kh < 3; kh++) {
-            const int h = ho * s + kh - 1;
-            if (h < 0 || h >= H) continue;
+            const int rr = r + kh - 1;
+            if (rr < 0 || rr >= R) continue;
 #pragma unroll
             for (int kw = 0; kw < 3; kw++) {
-                const int ww = wo * s + kw - 1;
-                if (ww < 0 || ww >= W) continue;
-                acc = fmaf(wc[kh * 3 + kw], xc[h * W + ww], acc);
+                int aa = a + kw - 1;
+                aa = aa < 0 ? aa + A : (aa >= A ? aa - A : aa);
+                acc = fmaf(wc[kh * 3 + kw], xc[rr * A + aa], acc);
             }
         }
     }
-    y[(((long)n * Co + co) * Ho + ho) * Wo + wo] = fmaxf(acc, 0.f);
+    y[(((long)n * Co + co) * R + r) * A + a] = fmaxf(acc, 0.f);
 }
 
 // dy <- dy * (y > 0): the ReLU's gradient, in place
@@ -94,31 +95,26 @@ __global__ void relu_mask_kernel(long n, const float* __restrict__ y, float* __r
     if (q < n && !(y[q] > 0.f)) dy[q] = 0.f;
 }
 
-// dx[n][ci][h][w] = sum_co sum_taps w[co][ci][kh][kw] dy[n][co][ho][wo], h = s ho + kh - 1
-__global__ void __launch_bounds__(PT) conv_bwd_data_kernel(int Ci, int H, int W, int Co, int Ho, int Wo, int s,
-                                                            const float* __restrict__ dy, const float* __restrict__ w,
-                                                            float* __restrict__ dx) {
+// dx[n][ci][r][a] = sum_co sum_taps w[co][ci][kh][kw] dy[n][co][r + 1 - kh][(a + 1 - kw) mod A]
+__global__ void __launch_bounds__(PT) pconv_bwd_data_kernel(int Ci, int R, int A, int Co, const float* __restrict__ dy,
+                                                             const float* __restrict__ w, float* __restrict__ dx) {
     const int ci = blockIdx.y, n = blockIdx.z;
     const int p = blockIdx.x * PT + threadIdx.x;
-    if (p >= H * W) return;
-    const int h = p / W, ww = p - h * W;
+    if (p >= R * A) return;
+    const int r = p / A, a = p - r * A;
     float acc = 0.f;
     for (int kh = 0; kh < 3; kh++) {
-        const int th = h + 1 - kh;
-        if (th < 0 || th % s) continue;
-        const int ho = th / s;
-        if (ho >= Ho) continue;
+        const int ro = r + 1 - kh;
+        if (ro < 0 || ro >= R) continue;
         for (int kw = 0; kw < 3; kw++) {
-            const int tw = ww + 1 - kw;
-            if (tw < 0 || tw % s) continue;
-            const int wo = tw / s;
-            if (wo >= Wo) continue;
-            const float* dyp = dy + (long)n * Co * Ho * Wo + (long)ho * Wo + wo;
+            int ao = a + 1 - kw;
+            ao = ao < 0 ? ao + A : (ao >= A ? ao - A : ao);
+            const float* dyp = dy + (long)n * Co * R * A + (long)ro * A + ao;
             const float* wp = w + (long)ci * 9 + kh * 3 + kw;
-            for (int co = 0; co < Co; co++) acc = fmaf(wp[(long)co * Ci * 9], dyp[(long)co * Ho * Wo], acc);
+            for (int co = 0; co < Co; co++) acc = fmaf(wp[(long)co * Ci * 9], dyp[(long)co * R * A], acc);
         }
     }
-    dx[(((long)n * Ci + ci) * H + h) * W + ww] = acc;
+    dx[(((long)n * Ci + ci) * R + r) * A + a] = acc;
 }
 
 template <typename T>
@@ -135,32 +131,32 @@ __device__ T block_sum(T v, T* sh) {
     return r;  // valid in thread 0
 }
 
-// dw[co][ci][kh][kw] = sum_{n,ho,wo} dy[n][co][ho][wo] x[n][ci][s ho + kh - 1][s wo + kw - 1]
-__global__ void __launch_bounds__(PT) conv_bwd_weight_kernel(int N, int Ci, int H, int W, int Co, int Ho, int Wo,
-                                                              int s, const float* __restrict__ x,
-                                                              const float* __restrict__ dy, float* __restrict__ dw) {
+// dw[co][ci][kh][kw] = sum_{n,r,a} dy[n][co][r][a] x[n][ci][r + kh - 1][(a + kw - 1) mod A]
+__global__ void __launch_bounds__(PT) pconv_bwd_weight_kernel(int N, int Ci, int R, int A, int Co,
+                                                               const float* __restrict__ x, const float* __restrict__ dy,
+                                                               float* __restrict__ dw) {
     __shared__ float sh[32];
     const int co = blockIdx.x, ci = blockIdx.y;
     float acc[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) acc[k] = 0.f;
-    const long tot = (long)N * Ho * Wo;
+    const long tot = (long)N * R * A;
     for (long q = threadIdx.x; q < tot; q += PT) {
-        const int n = (int)(q / (Ho * Wo));
-        const int p = (int)(q - (long)n * Ho * Wo);
-        const int ho = p / Wo, wo = p - ho * Wo;
-        const float g = dy[((long)n * Co + co) * Ho * Wo + p];
+        const int n = (int)(q / (R * A));
+        const int p = (int)(q - (long)n * R * A);
+        const int r = p / A, a = p - r * A;
+        const float g = dy[((long)n * Co + co) * R * A + p];
         if (g == 0.f) continue;
-        const float* xc = x + ((long)n * Ci + ci) * H * W;
+        const float* xc = x + ((long)n * Ci + ci) * R * A;
 #pragma unroll
         for (int kh = 0; kh < 3; kh++) {
-            const int h = ho * s + kh - 1;
-            if (h < 0 || h >= H) continue;
+            const int rr = r + kh - 1;
+            if (rr < 0 || rr >= R) continue;
 #pragma unroll
             for (int kw = 0; kw < 3; kw++) {
-                const int ww = wo * s + kw - 1;
-                if (ww < 0 || ww >= W) continue;
-                acc[kh * 3 + kw] = fmaf(g, xc[h * W + ww], acc[kh * 3 + kw]);
+                int aa = a + kw - 1;
+                aa = aa < 0 ? aa + A : (aa >= A ? aa - A : aa);
+                acc[kh * 3 + kw] = fmaf(g, xc[rr * A + aa], acc[kh * 3 + kw]);
             }
         }
     }
@@ -185,29 +181,94 @@ __global__ void __launch_bounds__(PT) bias_grad_kernel(int N, int C, int HW, con
     if (threadIdx.x == 0) db[c] = v;
 }
 
-// out[c][r] = in[r][c] for r < rows, c < cols; zero for r in [rows, rows_pad)
-__global__ void transpose_pad_kernel(int rows, int cols, int rows_pad, const float* __restrict__ in, long ldin,
-                                     float* __restrict__ out) {
-    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (long)rows_pad * cols) return;
-    const int c = (int)(q / rows_pad), r = (int)(q - (long)c * rows_pad);
-    out[q] = r < rows ? in[(long)r * ldin + c] : 0.f;
+// ---- equivariant head: circular correlation along theta, full over (c, r) ----
+// z[n][k][p] = bf[k] + sum_{c,r,d} wf[k][c][r][d] h[n][c][r][(d - p) mod A]
+// One CTA per sample with h[n] in shared memory; warp w takes classes w, w+8, ...
+// and its lanes the output angles p.
+__global__ void __launch_bounds__(PT) head_fwd_kernel(int CR, int A, int K, const float* __restrict__ h,
+                                                       const float* __restrict__ wf, const float* __restrict__ bf,
+                                                       float* __restrict__ z) {
+    extern __shared__ float sh_h[];  // CR * A
+    const int n = blockIdx.x;
+    const float* hn = h + (long)n * CR * A;
+    for (int q = threadIdx.x; q < CR * A; q += PT) sh_h[q] = hn[q];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = warp; k < K; k += PT / 32) {
+        const float* wk = wf + (long)k * CR * A;
+        for (int p0 = 0; p0 < A; p0 += 32) {
+            const int p = p0 + lane;
+            float acc = 0.f;
+            if (p < A) {
+                for (int cr = 0; cr < CR; cr++) {
+                    const float* hr = sh_h + cr * A;
+                    const float* wr = wk + cr * A;
+                    int idx = A - p;  // (d - p) mod A at d = 0
+                    if (idx == A) idx = 0;
+                    for (int d = 0; d < A; d++) {
+                        acc = fmaf(__ldg(wr + d), hr[idx], acc);
+                        if (++idx == A) idx = 0;
+                    }
+                }
+                z[((long)n * K + k) * A + p] = acc + bf[k];
+            }
+        }
+    }
 }
 
-// out[r][c] = in[r][c] for c < cols, zero for c in [cols, cols_pad)
-__global__ void pad_cols_kernel(int rows, int cols, int cols_pad, const float* __restrict__ in,
-                                float* __restrict__ out) {
-    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (long)rows * cols_pad) return;
-    const int r = (int)(q / cols_pad), c = (int)(q - (long)r * cols_pad);
-    out[q] = c < cols ? in[(long)r * cols + c] : 0.f;
+// dh[n][c][r][t] = sum_{k,p} dz[n][k][p] wf[k][c][r][(t + p) mod A]; one CTA per sample
+__global__ void __launch_bounds__(PT) head_bwd_data_kernel(int CR, int A, int K, const float* __restrict__ dz,
+                                                            const float* __restrict__ wf, float* __restrict__ dh) {
+    extern __shared__ float sdz[];  // K * A
+    const int n = blockIdx.x;
+    for (int q = threadIdx.x; q < K * A; q += PT) sdz[q] = dz[(long)n * K * A + q];
+    __syncthreads();
+    for (int e = threadIdx.x; e < CR * A; e += PT) {
+        const int cr = e / A, t = e - cr * A;
+        float acc = 0.f;
+        for (int k = 0; k < K; k++) {
+            const float* wr = wf + ((long)k * CR + cr) * A;
+            const float* dk = sdz + k * A;
+            int idx = t;  // (t + p) mod A at p = 0
+            for (int p = 0; p < A; p++) {
+                acc = fmaf(dk[p], __ldg(wr + idx), acc);
+                if (++idx == A) idx = 0;
+            }
+        }
+        dh[(long)n * CR * A + e] = acc;
+    }
 }
 
-__global__ void add_bias_kernel(int N, int O, long ld, const float* __restrict__ b, float* __restrict__ z) {
-    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= (long)N * O) return;
-    const int n = (int)(q / O), o = (int)(q - (long)n * O);
-    z[(long)n * ld + o] += b[o];
+// dwf[k][c][r][d] = sum_{n,p} dz[n][k][p] h[n][c][r][(d - p) mod A]; one CTA per class
+__global__ void __launch_bounds__(PT) head_bwd_weight_kernel(int N, int CR, int A, int K, const float* __restrict__ dz,
+                                                              const float* __restrict__ h, float* __restrict__ dwf,
+                                                              float* __restrict__ dbf) {
+    __shared__ float sdz[256];
+    __shared__ float red[32];
+    const int k = blockIdx.x;
+    float bsum = 0.f;
+    for (int e0 = 0; e0 < CR * A; e0 += PT) {
+        const int e = e0 + threadIdx.x;
+        const int cr = e / A, d = e - cr * A;
+        float acc = 0.f;
+        for (int n = 0; n < N; n++) {
+            __syncthreads();
+            for (int q = threadIdx.x; q < A; q += PT) sdz[q] = dz[((long)n * K + k) * A + q];
+            __syncthreads();
+            if (e < CR * A) {
+                const float* hr = h + ((long)n * CR + cr) * A;
+                int idx = d;  // (d - p) mod A at p = 0
+                for (int p = 0; p < A; p++) {
+                    acc = fmaf(sdz[p], __ldg(hr + idx), acc);
+                    if (--idx < 0) idx = A - 1;
+                }
+            }
+            if (e0 == 0 && threadIdx.x < A) bsum += sdz[threadIdx.x];
+        }
+        if (e < CR * A) dwf[(long)k * CR * A + e] = acc;
+    }
+    bsum = block_sum(bsum, red);
+    if (threadIdx.x == 0) dbf[k] = bsum;
 }
 
 // per sample: p = softmax(z), loss += -sum t log p, dz = (p - t) / N
@@ -268,29 +329,49 @@ __global__ void gather_rows_kernel(int n, long row, const int* __restrict__ idx,
     dst[q] = src[(long)idx[r] * row + (q - (long)r * row)];
 }
 
-// Network input of one particle (see oracle/proposal_oracle.py features()):
-// log(1 + |X|) and |CTF| on the centred size x size frequency grid, the
-// negative-kx half by Friedel symmetry, each channel normalised.
-__global__ void __launch_bounds__(PT) features_kernel(int cur, int size, const double* __restrict__ Fr,
-                                                       const double* __restrict__ Fi, const double* __restrict__ ctf,
-                                                       float* __restrict__ x) {
-    extern __shared__ float sx[];  // 2 * size * size
+// Network input of one particle (oracle/proposal_oracle.py features()):
+// bilinear samples of log(1 + |X|) and |CTF| on the polar grid r_i = r_lo +
+// i (r_hi - r_lo) / (R - 1), theta_a = a pi / A (negative kx by Friedel
+// symmetry), each channel normalised to zero mean and unit variance.
+__device__ __forceinline__ double half_plane_at(const double* v, int cur, int cf, int x, int y, bool logmag,
+                                                const double* vi) {
+    if (x < 0) {
+        x = -x;
+        y = -y;
+    }
+    const int row = y >= 0 ? y : y + cur;
+    const long e = (long)row * cf + x;
+    if (logmag) return log1p(sqrt(v[e] * v[e] + vi[e] * vi[e]));
+    return fabs(v[e]);
+}
+
+__global__ void __launch_bounds__(PT) polar_features_kernel(int cur, int R, int A, double r_lo, double r_hi,
+                                                             const double* __restrict__ Fr,
+                                                             const double* __restrict__ Fi,
+                                                             const double* __restrict__ ctf, float* __restrict__ x) {
+    extern __shared__ float sx[];  // 2 * R * A
     __shared__ double shd[32];
     __shared__ double s_mean[2], s_std[2];
-    const int i = blockIdx.x, cf = cur / 2 + 1, h = size / 2, n2 = size * size;
+    const int i = blockIdx.x, cf = cur / 2 + 1, n2 = R * A;
     const long base = (long)i * cur * cf;
+    const double kPiD = 3.14159265358979323846;
     for (int q = threadIdx.x; q < n2; q += PT) {
-        const int iy = q / size, ix = q - iy * size;
-        int kx = ix - h, ky = iy - h;
-        if (kx < 0) {
-            kx = -kx;
-            ky = -ky;
+        const int ri = q / A, a = q - ri * A;
+        const double r = r_lo + ri * (r_hi - r_lo) / (R - 1);
+        const double th = a * kPiD / A;
+        const double kx = r * cos(th), ky = r * sin(th);
+        const int x0 = (int)floor(kx), y0 = (int)floor(ky);
+        const double fx = kx - x0, fy = ky - y0;
+        for (int c = 0; c < 2; c++) {
+            const double* v = c == 0 ? Fr + base : ctf + base;
+            const double* vi = Fi + base;
+            const bool lm = c == 0;
+            const double v00 = half_plane_at(v, cur, cf, x0, y0, lm, vi);
+            const double v01 = half_plane_at(v, cur, cf, x0 + 1, y0, lm, vi);
+            const double v10 = half_plane_at(v, cur, cf, x0, y0 + 1, lm, vi);
+            const double v11 = half_plane_at(v, cur, cf, x0 + 1, y0 + 1, lm, vi);
+            sx[c * n2 + q] = (float)((1 - fy) * ((1 - fx) * v00 + fx * v01) + fy * ((1 - fx) * v10 + fx * v11));
         }
-        const int row = ky >= 0 ? ky : ky + cur;
-        const long e = base + (long)row * cf + kx;
-        const double re = Fr[e], im = Fi[e];
-        sx[q] = (float)log1p(sqrt(re * re + im * im));
-        sx[n2 + q] = (float)fabs(ctf[e]);
     }
     __syncthreads();
     for (int c = 0; c < 2; c++) {
@@ -372,97 +453,94 @@ __global__ void __launch_bounds__(PT) topk_kernel(int O, int k, const float* __r
     }
 }
 
+// network outputs o = class * A + p (top-k per particle) -> the 2k
+// orientations class * 2A + p and class * 2A + p + A, sorted ascending
+// (the restricted E-step wants ascending, distinct lists); one thread per
+// particle, insertion sort of at most 2 * 64 entries
+__global__ void expand_proposals_kernel(int P, int k, int A, const int* __restrict__ idx,
+                                        const float* __restrict__ prob, int* __restrict__ prop,
+                                        float* __restrict__ mass) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P) return;
+    int* out = prop + (long)i * 2 * k;
+    float m = 0.f;
+    int n = 0;
+    for (int q = 0; q < k; q++) {
+        const int o = idx[(long)i * k + q];
+        m += prob[(long)i * k + q];
+        const int c = o / A, p = o - c * A;
+        for (int h = 0; h < 2; h++) {
+            const int j = c * 2 * A + p + h * A;
+            int pos = n++;
+            while (pos > 0 && out[pos - 1] > j) {
+                out[pos] = out[pos - 1];
+                pos--;
+            }
+            out[pos] = j;
+        }
+    }
+    if (mass) mass[i] = m;
+}
+
 void net_alloc_batch(RomeProposalNet* net, int n) {
     if (n <= net->cap_n) return;
-    auto& sp = net->spec;
-    for (int l = 0; l < 5; l++) {
-        if (net->act[l]) cudaFree(net->act[l]);
-        if (net->dact[l]) cudaFree(net->dact[l]);
-        const size_t e = (size_t)n * net->ch[l] * net->hw[l] * net->hw[l];
-        ROME_CUDA(cudaMalloc(&net->act[l], sizeof(float) * e));
-        ROME_CUDA(cudaMalloc(&net->dact[l], sizeof(float) * e));
-    }
-    for (float** p : {&net->z, &net->dz, &net->tgt}) {
+    const size_t ra = (size_t)net->R * net->A, O = (size_t)net->K * net->A;
+    for (float** p : {&net->x, &net->h0, &net->h1, &net->dh0, &net->dh1, &net->z, &net->dz, &net->tgt})
         if (*p) cudaFree(*p);
-        ROME_CUDA(cudaMalloc(p, sizeof(float) * (size_t)n * sp.n_out));
-    }
-    const int npad = (n + 15) / 16 * 16, opad = (sp.n_out + 15) / 16 * 16;
-    const size_t tsz = std::max({(size_t)npad * sp.n_out, (size_t)npad * net->flat, (size_t)opad * net->flat,
-                                 (size_t)n * opad});
-    for (float** p : {&net->tmpA, &net->tmpB}) {
-        if (*p) cudaFree(*p);
-        ROME_CUDA(cudaMalloc(p, sizeof(float) * tsz));
-    }
+    ROME_CUDA(cudaMalloc(&net->x, sizeof(float) * n * 2 * ra));
+    ROME_CUDA(cudaMalloc(&net->h0, sizeof(float) * n * net->c0 * ra));
+    ROME_CUDA(cudaMalloc(&net->dh0, sizeof(float) * n * net->c0 * ra));
+    ROME_CUDA(cudaMalloc(&net->h1, sizeof(float) * n * net->c1 * ra));
+    ROME_CUDA(cudaMalloc(&net->dh1, sizeof(float) * n * net->c1 * ra));
+    for (float** p : {&net->z, &net->dz, &net->tgt}) ROME_CUDA(cudaMalloc(p, sizeof(float) * n * O));
     if (net->idx) cudaFree(net->idx);
     ROME_CUDA(cudaMalloc(&net->idx, sizeof(int) * n));
     net->cap_n = n;
 }
 
 void net_forward(RomeProposalNet* net, int n, cudaStream_t st) {
-    auto& sp = net->spec;
-    static const int strides[4] = {1, 2, 2, 2};
-    for (int l = 0; l < 4; l++) {
-        const int Ci = net->ch[l], H = net->hw[l], Co = net->ch[l + 1], Ho = net->hw[l + 1];
-        dim3 grid((Ho * Ho + PT - 1) / PT, Co, n);
-        conv_fwd_kernel<<<grid, PT, sizeof(float) * Ci * 9, st>>>(Ci, H, H, Co, Ho, Ho, strides[l], net->act[l],
-                                                                 net->params + net->off_w[l],
-                                                                 net->params + net->off_b[l], net->act[l + 1]);
-        ROME_CHECK_LAUNCH();
-    }
-    // linear: z[n][o] = act4[n][:] . wf[o][:] + bf[o]
-    sgemm_tn(st, n, sp.n_out, net->flat, net->act[4], net->flat, net->params + net->off_w[4], net->flat,
-             StoreEpi{net->z, sp.n_out});
-    ROME_CHECK_LAUNCH();
-    add_bias_kernel<<<(unsigned)(((long)n * sp.n_out + PT - 1) / PT), PT, 0, st>>>(n, sp.n_out, sp.n_out,
-                                                                                   net->params + net->off_b[4], net->z);
+    const int R = net->R, A = net->A;
+    dim3 g0((R * A + PT - 1) / PT, net->c0, n), g1((R * A + PT - 1) / PT, net->c1, n);
+    pconv_fwd_kernel<<<g0, PT, sizeof(float) * 2 * 9, st>>>(2, R, A, net->c0, net->x, net->params + net->off[0],
+                                                          net->params + net->off[1], net->h0);
+    pconv_fwd_kernel<<<g1, PT, sizeof(float) * net->c0 * 9, st>>>(net->c0, R, A, net->c1, net->h0,
+                                                                 net->params + net->off[2], net->params + net->off[3],
+                                                                 net->h1);
+    const int hsmem = (int)(sizeof(float) * net->c1 * R * A);
+    ROME_CUDA(cudaFuncSetAttribute(head_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, hsmem));
+    head_fwd_kernel<<<n, PT, hsmem, st>>>(net->c1 * R, A, net->K, net->h1, net->params + net->off[4],
+                                          net->params + net->off[5], net->z);
     ROME_CHECK_LAUNCH();
 }
 
-// gradients of the mean loss into net->grads (dz must hold dL/dz)
+// gradients of the mean loss into net->grads (dz holds dL/dz)
 void net_backward(RomeProposalNet* net, int n, cudaStream_t st) {
-    auto& sp = net->spec;
-    const int O = sp.n_out, F = net->flat;
-    const int npad = (n + 15) / 16 * 16, opad = (O + 15) / 16 * 16;
-    // gwf[o][f] = sum_n dz[n][o] act4[n][f]: A = dz^T [O][npad], B = act4^T [F][npad]
-    transpose_pad_kernel<<<(unsigned)(((long)npad * O + PT - 1) / PT), PT, 0, st>>>(n, O, npad, net->dz, O, net->tmpA);
-    transpose_pad_kernel<<<(unsigned)(((long)npad * F + PT - 1) / PT), PT, 0, st>>>(n, F, npad, net->act[4], F,
-                                                                                    net->tmpB);
+    const int R = net->R, A = net->A, CR = net->c1 * R;
+    head_bwd_weight_kernel<<<net->K, PT, 0, st>>>(n, CR, A, net->K, net->dz, net->h1, net->grads + net->off[4],
+                                                   net->grads + net->off[5]);
+    head_bwd_data_kernel<<<n, PT, sizeof(float) * net->K * A, st>>>(CR, A, net->K, net->dz,
+                                                                    net->params + net->off[4], net->dh1);
     ROME_CHECK_LAUNCH();
-    sgemm_tn(st, O, F, npad, net->tmpA, npad, net->tmpB, npad, StoreEpi{net->grads + net->off_w[4], F});
-    bias_grad_kernel<<<O, PT, 0, st>>>(n, O, 1, net->dz, net->grads + net->off_b[4]);
+    const long n1 = (long)n * net->c1 * R * A, n0 = (long)n * net->c0 * R * A;
+    relu_mask_kernel<<<(unsigned)((n1 + PT - 1) / PT), PT, 0, st>>>(n1, net->h1, net->dh1);
+    pconv_bwd_weight_kernel<<<dim3(net->c1, net->c0), PT, 0, st>>>(n, net->c0, R, A, net->c1, net->h0, net->dh1,
+                                                                   net->grads + net->off[2]);
+    bias_grad_kernel<<<net->c1, PT, 0, st>>>(n, net->c1, R * A, net->dh1, net->grads + net->off[3]);
+    dim3 g0((R * A + PT - 1) / PT, net->c0, n);
+    pconv_bwd_data_kernel<<<g0, PT, 0, st>>>(net->c0, R, A, net->c1, net->dh1, net->params + net->off[2], net->dh0);
+    relu_mask_kernel<<<(unsigned)((n0 + PT - 1) / PT), PT, 0, st>>>(n0, net->h0, net->dh0);
+    pconv_bwd_weight_kernel<<<dim3(net->c0, 2), PT, 0, st>>>(n, 2, R, A, net->c0, net->x, net->dh0,
+                                                             net->grads + net->off[0]);
+    bias_grad_kernel<<<net->c0, PT, 0, st>>>(n, net->c0, R * A, net->dh0, net->grads + net->off[1]);
     ROME_CHECK_LAUNCH();
-    // dact4[n][f] = sum_o dz[n][o] wf[o][f]: A = dz with columns padded to opad, B = wf^T [F][opad]
-    pad_cols_kernel<<<(unsigned)(((long)n * opad + PT - 1) / PT), PT, 0, st>>>(n, O, opad, net->dz, net->tmpB);
-    transpose_pad_kernel<<<(unsigned)(((long)opad * F + PT - 1) / PT), PT, 0, st>>>(O, F, opad,
-                                                                                    net->params + net->off_w[4], F,
-                                                                                    net->tmpA);
-    ROME_CHECK_LAUNCH();
-    sgemm_tn(st, n, F, opad, net->tmpB, opad, net->tmpA, opad, StoreEpi{net->dact[4], F});
-    ROME_CHECK_LAUNCH();
-    static const int strides[4] = {1, 2, 2, 2};
-    for (int l = 3; l >= 0; l--) {
-        const int Ci = net->ch[l], H = net->hw[l], Co = net->ch[l + 1], Ho = net->hw[l + 1];
-        const long ny = (long)n * Co * Ho * Ho;
-        relu_mask_kernel<<<(unsigned)((ny + PT - 1) / PT), PT, 0, st>>>(ny, net->act[l + 1], net->dact[l + 1]);
-        conv_bwd_weight_kernel<<<dim3(Co, Ci), PT, 0, st>>>(n, Ci, H, H, Co, Ho, Ho, strides[l], net->act[l],
-                                                            net->dact[l + 1], net->grads + net->off_w[l]);
-        bias_grad_kernel<<<Co, PT, 0, st>>>(n, Co, Ho * Ho, net->dact[l + 1], net->grads + net->off_b[l]);
-        if (l > 0) {
-            dim3 grid((H * H + PT - 1) / PT, Ci, n);
-            conv_bwd_data_kernel<<<grid, PT, 0, st>>>(Ci, H, H, Co, Ho, Ho, strides[l], net->dact[l + 1],
-                                                      net->params + net->off_w[l], net->dact[l]);
-        }
-        ROME_CHECK_LAUNCH();
-    }
 }
 
-double net_loss_grad(RomeProposalNet* net, int n, cudaStream_t st) {
+void net_loss_grad(RomeProposalNet* net, int n, cudaStream_t st) {
     ROME_CUDA(cudaMemsetAsync(net->loss_acc, 0, sizeof(double), st));
     net_forward(net, n, st);
-    softmax_xent_kernel<<<n, PT, 0, st>>>(n, net->spec.n_out, net->z, net->tgt, net->dz, net->loss_acc);
+    softmax_xent_kernel<<<n, PT, 0, st>>>(n, net->K * net->A, net->z, net->tgt, net->dz, net->loss_acc);
     ROME_CHECK_LAUNCH();
     net_backward(net, n, st);
-    return 0.0;
 }
 
 }  // namespace
@@ -473,51 +551,45 @@ extern "C" int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec*
     if (!ctx || !spec || !out) return ROME_ERR_ARG;
     *out = nullptr;
     return guarded(ctx, [&] {
-        ROME_REQUIRE(spec->size >= 8 && spec->size % 8 == 0 && spec->size <= 64, "input size %d (multiple of 8, <= 64)",
-                     spec->size);
-        ROME_REQUIRE(spec->n_out > 0 && spec->n_out <= 8192, "n_out %d", spec->n_out);
-        for (int l = 0; l < 4; l++) ROME_REQUIRE(spec->channels[l] > 0 && spec->channels[l] <= 128, "channels");
+        ROME_REQUIRE(spec->n_r >= 2 && spec->n_r <= 64, "n_r %d (2..64)", spec->n_r);
+        ROME_REQUIRE(spec->n_theta >= 4 && spec->n_theta <= 256, "n_theta %d (4..256)", spec->n_theta);
+        ROME_REQUIRE(spec->n_classes > 0 && spec->n_classes * spec->n_theta <= 8192, "n_classes %d", spec->n_classes);
+        ROME_REQUIRE(spec->channels[0] > 0 && spec->channels[0] <= 64 && spec->channels[1] > 0 &&
+                         spec->channels[1] <= 64,
+                     "channels");
+        ROME_REQUIRE(spec->r_lo >= 0 && spec->r_hi > spec->r_lo, "radius range");
+        ROME_REQUIRE((size_t)spec->channels[1] * spec->n_r * spec->n_theta * sizeof(float) <= 200 * 1024,
+                     "head input too large for shared memory");
         ROME_CUDA(cudaSetDevice(ctx->device));
         auto* net = new RomeProposalNet();
         net->ctx = ctx;
         net->spec = *spec;
-        net->ch[0] = 2;
-        net->hw[0] = spec->size;
-        for (int l = 0; l < 4; l++) {
-            net->ch[l + 1] = spec->channels[l];
-            net->hw[l + 1] = l == 0 ? spec->size : (net->hw[l] - 1) / 2 + 1;
-        }
-        net->flat = net->ch[4] * net->hw[4] * net->hw[4];
-        if (net->flat % 16) {
-            delete net;
-            fail(ROME_ERR_ARG, "flattened size %d must be a multiple of 16", net->hw[4]);
-        }
-        // every block starts on a 16-byte boundary (vector loads of the linear layer)
+        net->R = spec->n_r;
+        net->A = spec->n_theta;
+        net->K = spec->n_classes;
+        net->c0 = spec->channels[0];
+        net->c1 = spec->channels[1];
         auto a4 = [](long v) { return (v + 3) / 4 * 4; };
+        const long sizes[6] = {(long)net->c0 * 2 * 9, net->c0, (long)net->c1 * net->c0 * 9, net->c1,
+                               (long)net->K * net->c1 * net->R * net->A, net->K};
         long o = 0;
-        for (int l = 0; l < 4; l++) {
-            net->off_w[l] = o;
-            o = a4(o + (long)net->ch[l + 1] * net->ch[l] * 9);
-            net->off_b[l] = o;
-            o = a4(o + net->ch[l + 1]);
+        for (int b = 0; b < 6; b++) {
+            net->off[b] = o;
+            o = a4(o + sizes[b]);
         }
-        net->off_w[4] = o;
-        o = a4(o + (long)spec->n_out * net->flat);
-        net->off_b[4] = o;
-        o = a4(o + spec->n_out);
         net->nparam = o;
         // He-normal weights, zero biases (host RNG, seeded)
         std::vector<float> h(o, 0.f);
         std::mt19937_64 rng(seed);
-        for (int l = 0; l < 5; l++) {
-            const long nw = (l < 4 ? (long)net->ch[l + 1] * net->ch[l] * 9 : (long)spec->n_out * net->flat);
-            const double fan_in = l < 4 ? net->ch[l] * 9.0 : (double)net->flat;
-            std::normal_distribution<double> nd(0.0, std::sqrt(2.0 / fan_in) * (l < 4 ? 1.0 : 0.5));
-            for (long q = 0; q < nw; q++) h[net->off_w[l] + q] = (float)nd(rng);
+        const double fan[3] = {2 * 9.0, net->c0 * 9.0, (double)net->c1 * net->R * net->A};
+        for (int l = 0; l < 3; l++) {
+            std::normal_distribution<double> nd(0.0, std::sqrt(2.0 / fan[l]) * (l < 2 ? 1.0 : 0.5));
+            for (long q = 0; q < sizes[2 * l]; q++) h[net->off[2 * l] + q] = (float)nd(rng);
         }
         for (float** p : {&net->params, &net->grads, &net->adam_m, &net->adam_v})
             ROME_CUDA(cudaMalloc(p, sizeof(float) * o));
         ROME_CUDA(cudaMemcpy(net->params, h.data(), sizeof(float) * o, cudaMemcpyHostToDevice));
+        ROME_CUDA(cudaMemset(net->grads, 0, sizeof(float) * o));
         ROME_CUDA(cudaMemset(net->adam_m, 0, sizeof(float) * o));
         ROME_CUDA(cudaMemset(net->adam_v, 0, sizeof(float) * o));
         ROME_CUDA(cudaMalloc(&net->loss_acc, sizeof(double)));
@@ -528,13 +600,9 @@ extern "C" int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec*
 extern "C" void rome_gpu_proposal_destroy(RomeProposalNet* net) {
     if (!net) return;
     cudaSetDevice(net->ctx->device);
-    for (float* p : {net->params, net->grads, net->adam_m, net->adam_v, net->z, net->dz, net->tgt, net->tmpA,
-                     net->tmpB})
+    for (float* p : {net->params, net->grads, net->adam_m, net->adam_v, net->x, net->h0, net->h1, net->dh0, net->dh1,
+                     net->z, net->dz, net->tgt})
         if (p) cudaFree(p);
-    for (int l = 0; l < 5; l++) {
-        if (net->act[l]) cudaFree(net->act[l]);
-        if (net->dact[l]) cudaFree(net->dact[l]);
-    }
     if (net->loss_acc) cudaFree(net->loss_acc);
     if (net->idx) cudaFree(net->idx);
     delete net;
@@ -568,16 +636,13 @@ extern "C" int rome_gpu_proposal_loss_grad(RomeProposalNet* net, int n, const fl
         ROME_CUDA(cudaSetDevice(net->ctx->device));
         cudaStream_t st = net->ctx->stream;
         net_alloc_batch(net, n);
-        const long in = (long)n * 2 * net->spec.size * net->spec.size;
-        ROME_CUDA(cudaMemcpyAsync(net->act[0], x, sizeof(float) * in, cudaMemcpyHostToDevice, st));
-        ROME_CUDA(cudaMemcpyAsync(net->tgt, t, sizeof(float) * (size_t)n * net->spec.n_out, cudaMemcpyHostToDevice,
-                                  st));
+        const long row_x = 2L * net->R * net->A, O = (long)net->K * net->A;
+        ROME_CUDA(cudaMemcpyAsync(net->x, x, sizeof(float) * row_x * n, cudaMemcpyHostToDevice, st));
+        ROME_CUDA(cudaMemcpyAsync(net->tgt, t, sizeof(float) * O * n, cudaMemcpyHostToDevice, st));
         net_loss_grad(net, n, st);
         if (loss) ROME_CUDA(cudaMemcpyAsync(loss, net->loss_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
         if (grad) ROME_CUDA(cudaMemcpyAsync(grad, net->grads, sizeof(float) * net->nparam, cudaMemcpyDeviceToHost, st));
-        if (logits)
-            ROME_CUDA(cudaMemcpyAsync(logits, net->z, sizeof(float) * (size_t)n * net->spec.n_out,
-                                      cudaMemcpyDeviceToHost, st));
+        if (logits) ROME_CUDA(cudaMemcpyAsync(logits, net->z, sizeof(float) * O * n, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
     });
 }
@@ -590,10 +655,12 @@ extern "C" int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float*
         cudaStream_t st = net->ctx->stream;
         const int B = std::min(batch, n);
         net_alloc_batch(net, B);
-        const long row_x = 2L * net->spec.size * net->spec.size, row_t = net->spec.n_out;
+        const long row_x = 2L * net->R * net->A, row_t = (long)net->K * net->A;
         float *dx = nullptr, *dt = nullptr;
+        int* dperm = nullptr;
         ROME_CUDA(cudaMalloc(&dx, sizeof(float) * row_x * n));
         ROME_CUDA(cudaMalloc(&dt, sizeof(float) * row_t * n));
+        ROME_CUDA(cudaMalloc(&dperm, sizeof(int) * n));
         ROME_CUDA(cudaMemcpyAsync(dx, x, sizeof(float) * row_x * n, cudaMemcpyHostToDevice, st));
         ROME_CUDA(cudaMemcpyAsync(dt, t, sizeof(float) * row_t * n, cudaMemcpyHostToDevice, st));
         std::vector<int> perm(n);
@@ -602,17 +669,17 @@ extern "C" int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float*
         const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
         for (int ep = 0; ep < epochs; ep++) {
             std::shuffle(perm.begin(), perm.end(), rng);
+            ROME_CUDA(cudaMemcpyAsync(dperm, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st));
             ROME_CUDA(cudaMemsetAsync(net->loss_acc, 0, sizeof(double), st));
             int nb = 0;
             for (int b0 = 0; b0 + B <= n; b0 += B, nb++) {
-                ROME_CUDA(cudaMemcpyAsync(net->idx, perm.data() + b0, sizeof(int) * B, cudaMemcpyHostToDevice, st));
-                gather_rows_kernel<<<(unsigned)((B * row_x + PT - 1) / PT), PT, 0, st>>>(B, row_x, net->idx, dx,
-                                                                                        net->act[0]);
-                gather_rows_kernel<<<(unsigned)((B * row_t + PT - 1) / PT), PT, 0, st>>>(B, row_t, net->idx, dt,
+                gather_rows_kernel<<<(unsigned)((B * row_x + PT - 1) / PT), PT, 0, st>>>(B, row_x, dperm + b0, dx,
+                                                                                        net->x);
+                gather_rows_kernel<<<(unsigned)((B * row_t + PT - 1) / PT), PT, 0, st>>>(B, row_t, dperm + b0, dt,
                                                                                         net->tgt);
                 ROME_CHECK_LAUNCH();
                 net_forward(net, B, st);
-                softmax_xent_kernel<<<B, PT, 0, st>>>(B, net->spec.n_out, net->z, net->tgt, net->dz, net->loss_acc);
+                softmax_xent_kernel<<<B, PT, 0, st>>>(B, (int)row_t, net->z, net->tgt, net->dz, net->loss_acc);
                 ROME_CHECK_LAUNCH();
                 net_backward(net, B, st);
                 net->adam_t++;
@@ -620,36 +687,35 @@ extern "C" int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float*
                 adam_kernel<<<(unsigned)((net->nparam + PT - 1) / PT), PT, 0, st>>>(
                     net->nparam, lr, b1, b2, eps, c1, c2, net->grads, net->params, net->adam_m, net->adam_v);
                 ROME_CHECK_LAUNCH();
-                // the staging copy of the index list must finish before the host refills it
-                ROME_CUDA(cudaStreamSynchronize(st));
             }
             double l = 0;
             ROME_CUDA(cudaMemcpyAsync(&l, net->loss_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
+            // the host reshuffles `perm` next epoch: its copy must be done
             ROME_CUDA(cudaStreamSynchronize(st));
             if (epoch_loss) epoch_loss[ep] = nb ? l / nb : 0.0;
         }
         cudaFree(dx);
         cudaFree(dt);
+        cudaFree(dperm);
     });
 }
 
 namespace rome {
-// logits of n feature rows already on the device, then top-k per row
+// top-k outputs of n feature rows already on the device
 void proposal_predict_device(RomeProposalNet* net, int n, const float* dfeat, int k, int* didx, float* dprob,
                              cudaStream_t st) {
-    int done = 0;
-    const long row_x = 2L * net->spec.size * net->spec.size;
+    const long row_x = 2L * net->R * net->A;
+    const int O = net->K * net->A;
     const int chunk = 4096;
     net_alloc_batch(net, std::min(n, chunk));
-    while (done < n) {
+    const int n2 = 1 << (32 - __builtin_clz((unsigned)(O - 1)));
+    const size_t smem = (sizeof(float) + sizeof(int)) * n2;
+    ROME_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (int done = 0; done < n;) {
         const int m = std::min(chunk, n - done);
-        ROME_CUDA(cudaMemcpyAsync(net->act[0], dfeat + (long)done * row_x, sizeof(float) * row_x * m,
+        ROME_CUDA(cudaMemcpyAsync(net->x, dfeat + (long)done * row_x, sizeof(float) * row_x * m,
                                   cudaMemcpyDeviceToDevice, st));
         net_forward(net, m, st);
-        const int O = net->spec.n_out;
-        const int n2 = 1 << (32 - __builtin_clz((unsigned)(O - 1)));
-        const size_t smem = (sizeof(float) + sizeof(int)) * n2;
-        ROME_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         topk_kernel<<<m, PT, smem, st>>>(O, k, net->z, didx + (long)done * k, dprob ? dprob + (long)done * k : nullptr);
         ROME_CHECK_LAUNCH();
         done += m;
@@ -658,9 +724,9 @@ void proposal_predict_device(RomeProposalNet* net, int n, const float* dfeat, in
 
 void proposal_features_device(RomeProposalNet* net, int P, int cur, const double* Fr, const double* Fi,
                               const double* ctf, float* dfeat, cudaStream_t st) {
-    const int S = net->spec.size;
-    ROME_REQUIRE(S <= cur, "proposal input size %d exceeds the image size %d", S, cur);
-    features_kernel<<<P, PT, sizeof(float) * 2 * S * S, st>>>(cur, S, Fr, Fi, ctf, dfeat);
+    ROME_REQUIRE(net->spec.r_hi + 1 < cur / 2, "radius %.1f too large for image size %d", net->spec.r_hi, cur);
+    polar_features_kernel<<<P, PT, sizeof(float) * 2 * net->R * net->A, st>>>(cur, net->R, net->A, net->spec.r_lo,
+                                                                            net->spec.r_hi, Fr, Fi, ctf, dfeat);
     ROME_CHECK_LAUNCH();
 }
 }  // namespace rome
@@ -672,7 +738,7 @@ extern "C" int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, 
         ROME_CUDA(cudaSetDevice(net->ctx->device));
         cudaStream_t st = net->ctx->stream;
         const long F = (long)cur * (cur / 2 + 1);
-        const long row_x = 2L * net->spec.size * net->spec.size;
+        const long row_x = 2L * net->R * net->A;
         double* d = net->ctx->ws[S_TMP2].as<double>((size_t)3 * P * F);
         float* dx = (float*)net->ctx->ws[S_TMP1].get(sizeof(float) * row_x * P);
         ROME_CUDA(cudaMemcpyAsync(d, Fr, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
@@ -685,11 +751,11 @@ extern "C" int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, 
 }
 
 extern "C" int rome_gpu_proposal_predict(RomeProposalNet* net, int n, const float* x, int k, int* idx, float* prob) {
-    if (!net || n <= 0 || !x || k <= 0 || k > net->spec.n_out || !idx) return ROME_ERR_ARG;
+    if (!net || n <= 0 || !x || k <= 0 || k > net->K * net->A || !idx) return ROME_ERR_ARG;
     return guarded(net->ctx, [&] {
         ROME_CUDA(cudaSetDevice(net->ctx->device));
         cudaStream_t st = net->ctx->stream;
-        const long row_x = 2L * net->spec.size * net->spec.size;
+        const long row_x = 2L * net->R * net->A;
         float* dx = (float*)net->ctx->ws[S_TMP1].get(sizeof(float) * row_x * n);
         int* di = (int*)net->ctx->ws[S_TMP0].get((sizeof(int) + sizeof(float)) * (size_t)n * k);
         float* dp = (float*)(di + (size_t)n * k);
@@ -697,6 +763,45 @@ extern "C" int rome_gpu_proposal_predict(RomeProposalNet* net, int n, const floa
         proposal_predict_device(net, n, dx, k, di, dp, st);
         ROME_CUDA(cudaMemcpyAsync(idx, di, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
         if (prob) ROME_CUDA(cudaMemcpyAsync(prob, dp, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
+extern "C" int rome_gpu_proposal_propose(RomeProposalNet* net, int P, int cur, const double* Fr, const double* Fi,
+                                         const double* ctf, int inputs_on_device, int k, int* proposals,
+                                         float* mass) {
+    if (!net || P <= 0 || !Fr || !Fi || !ctf || k <= 0 || k > 64 || k > net->K * net->A || !proposals)
+        return ROME_ERR_ARG;
+    return guarded(net->ctx, [&] {
+        ROME_CUDA(cudaSetDevice(net->ctx->device));
+        cudaStream_t st = net->ctx->stream;
+        const long F = (long)cur * (cur / 2 + 1);
+        const long row_x = 2L * net->R * net->A;
+        const double *dFr = Fr, *dFi = Fi, *dC = ctf;
+        if (!inputs_on_device) {
+            double* d = net->ctx->ws[S_TMP2].as<double>((size_t)3 * P * F);
+            ROME_CUDA(cudaMemcpyAsync(d, Fr, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(d + P * F, Fi, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(d + 2 * P * F, ctf, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            dFr = d;
+            dFi = d + P * F;
+            dC = d + 2 * P * F;
+        }
+        float* dx = (float*)net->ctx->ws[S_TMP1].get(sizeof(float) * row_x * P);
+        char* buf = (char*)net->ctx->ws[S_TMP0].get((sizeof(int) + sizeof(float)) * (size_t)P * k +
+                                                    (sizeof(int) * 2 * k + sizeof(float)) * (size_t)P);
+        int* di = (int*)buf;
+        float* dp = (float*)(di + (size_t)P * k);
+        int* dprop = (int*)(dp + (size_t)P * k);
+        float* dmass = (float*)(dprop + (size_t)P * 2 * k);
+        proposal_features_device(net, P, cur, dFr, dFi, dC, dx, st);
+        proposal_predict_device(net, P, dx, k, di, dp, st);
+        expand_proposals_kernel<<<(P + 127) / 128, 128, 0, st>>>(P, k, net->A, di, dp, dprop, dmass);
+        ROME_CHECK_LAUNCH();
+        // features, then per chunk of 4096: two convolutions, the head and top-k; then the expansion
+        net->ctx->total_launches += 2 + 4L * ((P + 4095) / 4096);
+        ROME_CUDA(cudaMemcpyAsync(proposals, dprop, sizeof(int) * (size_t)P * 2 * k, cudaMemcpyDeviceToHost, st));
+        if (mass) ROME_CUDA(cudaMemcpyAsync(mass, dmass, sizeof(float) * P, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
     });
 }

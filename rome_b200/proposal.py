@@ -1,0 +1,174 @@
+"""Learned pose proposals: the Python side of rome_gpu_proposal_* (a small
+rotation-equivariant network trained on the GPU on (image, posterior) pairs
+of the exhaustive E-step) and the proposal-restricted E-step built on it.
+
+Output index of the network: o = class * (nr_psi / 2) + (psi mod nr_psi / 2);
+the Fourier magnitude the network sees cannot tell psi from psi + 180, so a
+proposed output expands to the two orientations class * nr_psi + psi and
+class * nr_psi + psi + nr_psi / 2.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Tuple
+
+import numpy as np
+
+from . import abi
+from .map2d import GpuContext, Map2dPool, _f64
+
+__all__ = ["ProposalNet", "param_offsets", "flat_to_dict", "dict_to_flat", "posterior_targets",
+           "expand_proposals", "DEFAULT_CHANNELS"]
+
+DEFAULT_CHANNELS = (16, 16)
+_FP = C.POINTER(C.c_float)
+
+
+def _fptr(a: np.ndarray):
+    assert a.dtype == np.float32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_FP)
+
+
+def param_offsets(n_r: int, n_theta: int, channels, n_classes: int) -> List[Tuple[str, tuple, int]]:
+    """(name, shape, offset) of every parameter block in the flat array; each
+    block starts at a multiple of 4 floats, as the library lays them out."""
+    a4 = lambda v: (v + 3) // 4 * 4  # noqa: E731
+    c0, c1 = channels
+    shapes = [("w0", (c0, 2, 3, 3)), ("b0", (c0,)), ("w1", (c1, c0, 3, 3)), ("b1", (c1,)),
+              ("wf", (n_classes, c1, n_r, n_theta)), ("bf", (n_classes,))]
+    out, o = [], 0
+    for name, shape in shapes:
+        out.append((name, shape, o))
+        o = a4(o + int(np.prod(shape)))
+    return out + [("_total", (), o)]
+
+
+def flat_to_dict(flat: np.ndarray, n_r: int, n_theta: int, channels, n_classes: int) -> Dict[str, np.ndarray]:
+    d = {}
+    for name, shape, off in param_offsets(n_r, n_theta, channels, n_classes)[:-1]:
+        n = int(np.prod(shape))
+        d[name] = np.asarray(flat[off:off + n], np.float64).reshape(shape)
+    return d
+
+
+def dict_to_flat(d: Dict[str, np.ndarray], n_r: int, n_theta: int, channels, n_classes: int) -> np.ndarray:
+    offs = param_offsets(n_r, n_theta, channels, n_classes)
+    flat = np.zeros(offs[-1][2], np.float32)
+    for name, shape, off in offs[:-1]:
+        flat[off:off + int(np.prod(shape))] = np.asarray(d[name], np.float32).ravel()
+    return flat
+
+
+def posterior_targets(marg: np.ndarray, nr_classes: int, nr_psi: int) -> np.ndarray:
+    """Training targets from the E-step's (class, psi) posterior marginals:
+    psi folded modulo 180 degrees, each row normalised to 1."""
+    h = nr_psi // 2
+    m = marg.reshape(-1, nr_classes, 2, h).sum(axis=2).reshape(-1, nr_classes * h)
+    s = m.sum(axis=1, keepdims=True)
+    return (m / np.where(s > 0, s, 1.0)).astype(np.float32)
+
+
+def expand_proposals(idx: np.ndarray, nr_psi: int) -> np.ndarray:
+    """Network outputs [n][k] -> ascending orientation lists [n][2k]."""
+    h = nr_psi // 2
+    cls, pm = idx // h, idx % h
+    j = np.concatenate([cls * nr_psi + pm, cls * nr_psi + pm + h], axis=1)
+    return np.sort(j, axis=1).astype(np.int32)
+
+
+class ProposalNet:
+    """rome_gpu_proposal_* on one GpuContext: n_classes x n_theta outputs
+    (n_theta = nr_psi / 2), polar input of n_r radii in [r_lo, r_hi]."""
+
+    def __init__(self, ctx: GpuContext, n_classes: int, n_theta: int, n_r: int = 16, channels=DEFAULT_CHANNELS,
+                 r_lo: float = 2.0, r_hi: float = 24.0, seed: int = 0):
+        self.ctx, self.lib = ctx, ctx.lib
+        self.n_classes, self.n_theta, self.n_r, self.channels = n_classes, n_theta, n_r, tuple(channels)
+        self.r_lo, self.r_hi = r_lo, r_hi
+        self.n_out = n_classes * n_theta
+        spec = abi.RomeProposalSpec(n_r, n_theta, (C.c_int * 2)(*channels), n_classes, r_lo, r_hi)
+        h = C.c_void_p()
+        ctx._check(self.lib.rome_gpu_proposal_create(ctx.h, C.byref(spec), seed, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.rome_gpu_proposal_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def nparam(self) -> int:
+        return int(self.lib.rome_gpu_proposal_num_params(self.h))
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.nparam, np.float32)
+        self.ctx._check(self.lib.rome_gpu_proposal_get_params(self.h, _fptr(out)))
+        return out
+
+    def set_params(self, flat: np.ndarray):
+        flat = np.ascontiguousarray(flat, np.float32)
+        assert flat.size == self.nparam
+        self.ctx._check(self.lib.rome_gpu_proposal_set_params(self.h, _fptr(flat)))
+
+    def features(self, p: Map2dPool) -> np.ndarray:
+        x = np.zeros((p.nr_images, 2, self.n_r, self.n_theta), np.float32)
+        fr, fi, ct = _f64(p.Fimg_real), _f64(p.Fimg_imag), _f64(p.Fctf)
+        self.ctx._check(self.lib.rome_gpu_proposal_features(self.h, p.nr_images, p.current_size, abi.dptr(fr),
+                                                            abi.dptr(fi), abi.dptr(ct), _fptr(x)))
+        return x
+
+    def loss_grad(self, x: np.ndarray, t: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        n = x.shape[0]
+        loss = np.zeros(1)
+        grad = np.zeros(self.nparam, np.float32)
+        logits = np.zeros((n, self.n_out), np.float32)
+        self.ctx._check(self.lib.rome_gpu_proposal_loss_grad(self.h, n, _fptr(x), _fptr(t), abi.dptr(loss),
+                                                             _fptr(grad), _fptr(logits)))
+        return float(loss[0]), grad, logits
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int = 10, batch: int = 256, lr: float = 1e-3,
+              seed: int = 1) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        losses = np.zeros(epochs)
+        self.ctx._check(self.lib.rome_gpu_proposal_train(self.h, x.shape[0], _fptr(x), _fptr(t), epochs, batch,
+                                                         lr, seed, abi.dptr(losses)))
+        return losses
+
+    def predict(self, x: np.ndarray, k: int):
+        x = np.ascontiguousarray(x, np.float32)
+        n = x.shape[0]
+        idx = np.zeros((n, k), np.int32)
+        prob = np.zeros((n, k), np.float32)
+        self.ctx._check(self.lib.rome_gpu_proposal_predict(self.h, n, _fptr(x), k, abi.iptr(idx), _fptr(prob)))
+        return idx, prob
+
+    def propose(self, p, k: int):
+        """Top-k network outputs of every particle of a pool (a Map2dPool, or
+        a StagedPool whose images live on the device), expanded to ascending
+        orientation lists [P][2k], and the probability mass they cover."""
+        from .map2d import StagedPool
+        base = p.pool if isinstance(p, StagedPool) else p
+        P = base.nr_images
+        prop = np.zeros((P, 2 * k), np.int32)
+        mass = np.zeros(P, np.float32)
+        keep = None
+        if isinstance(p, StagedPool):
+            ptrs = [C.c_void_p(p.dev[n].data_ptr()) for n in ("Fimg_real", "Fimg_imag", "Fctf")]
+            on_dev = 1
+        else:
+            keep = [_f64(base.Fimg_real), _f64(base.Fimg_imag), _f64(base.Fctf)]
+            ptrs = [C.c_void_p(a.ctypes.data) for a in keep]
+            on_dev = 0
+        self.ctx._check(self.lib.rome_gpu_proposal_propose(self.h, P, base.current_size, ptrs[0], ptrs[1], ptrs[2],
+                                                           on_dev, k, abi.iptr(prop), _fptr(mass)))
+        del keep
+        return prop, mass
