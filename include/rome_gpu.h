@@ -173,6 +173,14 @@ typedef struct {
     /* nonzero: Fimg_real/imag, Fimg_nomask_real/imag and Fctf are device
      * pointers on the context's device (no host-to-device copy) */
     int inputs_on_device;
+    /* optional search restriction (adaptive_oversampling 0 only; no
+     * reference counterpart): per particle nr_proposals orientation indices
+     * j = class * nr_psi + psi, ascending and distinct (host array
+     * [P][nr_proposals]); only those orientations, with every translation,
+     * are evaluated, and the posterior is normalised over them.  NULL: the
+     * exhaustive search of the reference. */
+    const int* proposals;
+    int nr_proposals;
 } RomeMap2dPool;
 
 typedef struct {
@@ -202,6 +210,10 @@ typedef struct {
     double* diff2[2];
     double* weight[2];
     char* Mcoarse_significant;        /* [P][K * nr_psi * nr_trans] (pass 0) */
+    /* optional [P][K * nr_psi]: the significant normalised weights of the
+     * last pass summed per (class, psi) (the posterior the proposal network
+     * is trained on); NULL to skip */
+    double* post_class_psi;
 } RomeMap2dPoolOut;
 
 int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2dPoolOut* out);

@@ -59,7 +59,7 @@ class RomeMap2dPool(C.Structure):
         ("pdf_class", _DP), ("pdf_direction", _DP), ("prior_offsetx_class", _DP), ("prior_offsety_class", _DP),
         ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
         ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
-        ("inputs_on_device", C.c_int),
+        ("inputs_on_device", C.c_int), ("proposals", _IP), ("nr_proposals", C.c_int),
     ]
 
 
@@ -70,7 +70,7 @@ class RomeMap2dPoolOut(C.Structure):
         ("wsum_sigma2_noise", _DP), ("wsum_pdf_class", _DP), ("wsum_pdf_direction", _DP),
         ("wsum_prior_offsetx_class", _DP), ("wsum_prior_offsety_class", _DP), ("wsum_sigma2_offset", _DP),
         ("wsum_sumw_group", _DP),
-        ("diff2", _DP * 2), ("weight", _DP * 2), ("Mcoarse_significant", _CP),
+        ("diff2", _DP * 2), ("weight", _DP * 2), ("Mcoarse_significant", _CP), ("post_class_psi", _DP),
     ]
 
 

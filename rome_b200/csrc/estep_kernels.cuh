@@ -398,8 +398,9 @@ __global__ void w2_kernel(int P, int Kact, int Kq, const int* __restrict__ act, 
 // the coarse pass of 3D) hold e = j * T + t with j = (k, psi, over_rot) and
 // t = (trans, over_trans); k indexes pdf_direction and k / ndir the class of
 // the offset prior (3D folds the direction into k: k = class * ndir + dir).
-// Ragged rows (the 3D fine pass) hold epr hypotheses per coarse-significant
-// entry r; ent[i * ent_stride + r] = (k, coarse translation), x < 0 marks
+// Ragged rows (the 3D fine pass, the restricted 2D search) hold epr
+// hypotheses per entry r; ent[i * ent_stride + r] = (k, coarse translation),
+// or (k, -1) when the entry's hypotheses are its translations; x < 0 marks
 // padding, and the row order is already the reference's loop order.
 struct PostLayout {
     int T, notr, nor, npsi, ntr, K;
@@ -431,7 +432,8 @@ __device__ __forceinline__ bool hyp_prior(long e, int i, const PostLayout& L, co
         const int2 en = L.ent[(long)i * L.ent_stride + e / L.epr];
         if (en.x < 0) return false;
         k = en.x;
-        itr = en.y;
+        // y < 0: the entry's hypotheses are its translations (restricted 2D search)
+        itr = en.y >= 0 ? en.y : (int)(e % L.epr) / L.notr;
         lo = e;
     } else {
         decode_e(e, L, k, itr, lo);

@@ -24,6 +24,7 @@
 #include "estep_kernels.cuh"
 #include "gemm_simt.cuh"
 #include "gemm_tc.cuh"
+#include "restricted_kernels.cuh"
 #include "select_kernels.cuh"
 
 using namespace rome;
@@ -166,6 +167,23 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         int listcap = std::max(1024, P * 64), nsigtot = 0;
         SigEntry* dList = nullptr;
 
+        // optional restricted search (learned proposals): validated on the host
+        const bool restricted = in->proposals != nullptr;
+        const int nprop = restricted ? in->nr_proposals : 0;
+        int* dProp = nullptr;
+        if (restricted) {
+            ROME_REQUIRE(npass == 1, "proposals need adaptive_oversampling 0");
+            ROME_REQUIRE(nprop > 0 && nprop <= K * npsi, "nr_proposals %d out of range (1..%d)", nprop, K * npsi);
+            for (int i = 0; i < P; i++)
+                for (int q = 0; q < nprop; q++) {
+                    const int j = in->proposals[(size_t)i * nprop + q];
+                    ROME_REQUIRE(j >= 0 && j < K * npsi, "proposal %d of particle %d out of range", j, i);
+                    ROME_REQUIRE(q == 0 || j > in->proposals[(size_t)i * nprop + q - 1],
+                                 "proposals of particle %d not ascending and distinct", i);
+                }
+            dProp = upload(ctx, S_FE, in->proposals, (size_t)P * nprop);
+        }
+
         for (int ipass = 0; ipass < npass; ipass++) {
             const int cs = (ipass == 0 && in->adaptive_oversampling > 0) ? in->coarse_size : cur;
             const int over = ipass == 0 ? 0 : in->adaptive_oversampling;
@@ -277,56 +295,103 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             prof.launched(ROME_PHASE_SHIFT);
             prof.end(ROME_PHASE_SHIFT);
 
-            // ---- norm term N[i][j] = sum_n Minv c^2 |P_j|^2 (FP32 CUDA cores) ----
-            float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * g.J);
-            prof.begin(ROME_PHASE_NORM_GEMM);
-            if (!tc) {
-                sgemm_tn(st, P, g.J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, g.J});
-                prof.launched(ROME_PHASE_NORM_GEMM);
-            } else {
-                // split-BF16 on the tensor cores in every tensor-core mode: the
-                // norm term is all positive, so its hi/lo rounding averages out
-                const int Kq64 = ((g.Kact + 63) / 64) * 64;
-                void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
-                void* dQb = ctx->ws[S_QB].get((size_t)g.J * Kq64 * 4);
-                split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
-                split_bf16(st, dQ, g.J, g.Kact, g.Kq, Kq64, dQb);
-                tc_store_gemm(st, P, g.J, Kq64, dW2b, dQb, dNorm, g.J, ctx->d_err);
-                prof.launched(ROME_PHASE_NORM_GEMM, 3);
-            }
-            prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * g.J * g.Kact);
-            prof.end(ROME_PHASE_NORM_GEMM);
-
-            // ---- cross term + fused diff2 epilogue ----
-            dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * g.X);
             unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
             ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
-            Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJvalid, g.T, g.J, g.X, g.notr, g.nor, ntr, ncoarse,
-                         ipass > 0 ? dMcoarse : nullptr, dRowMin};
-            prof.begin(ROME_PHASE_CROSS_GEMM);
-            if (!tc) {
-                sgemm_tn(st, (int)M, g.J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
+            long Xrow = g.X;  // hypotheses per particle row
+            if (!restricted) {
+                // ---- norm term N[i][j] = sum_n Minv c^2 |P_j|^2 (FP32 CUDA cores) ----
+                float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * g.J);
+                prof.begin(ROME_PHASE_NORM_GEMM);
+                if (!tc) {
+                    sgemm_tn(st, P, g.J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, g.J});
+                    prof.launched(ROME_PHASE_NORM_GEMM);
+                } else {
+                    // split-BF16 on the tensor cores in every tensor-core mode: the
+                    // norm term is all positive, so its hi/lo rounding averages out
+                    const int Kq64 = ((g.Kact + 63) / 64) * 64;
+                    void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
+                    void* dQb = ctx->ws[S_QB].get((size_t)g.J * Kq64 * 4);
+                    split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
+                    split_bf16(st, dQ, g.J, g.Kact, g.Kq, Kq64, dQb);
+                    tc_store_gemm(st, P, g.J, Kq64, dW2b, dQb, dNorm, g.J, ctx->d_err);
+                    prof.launched(ROME_PHASE_NORM_GEMM, 3);
+                }
+                prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * g.J * g.Kact);
+                prof.end(ROME_PHASE_NORM_GEMM);
+
+                // ---- cross term + fused diff2 epilogue ----
+                dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * g.X);
+                Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJvalid, g.T, g.J, g.X, g.notr, g.nor, ntr, ncoarse,
+                             ipass > 0 ? dMcoarse : nullptr, dRowMin};
+                prof.begin(ROME_PHASE_CROSS_GEMM);
+                if (!tc) {
+                    sgemm_tn(st, (int)M, g.J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
+                } else {
+                    tc_diff2_gemm(st, (int)M, g.J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
+                }
+                prof.launched(ROME_PHASE_CROSS_GEMM);
+                // algorithmic work: 4 flops per active complex coefficient per (image, translation, orientation)
+                prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * g.J * g.Kact);
+                prof.end(ROME_PHASE_CROSS_GEMM);
             } else {
-                tc_diff2_gemm(st, (int)M, g.J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
+                // ---- restricted search: only the proposed orientations ----
+                Xrow = (long)nprop * g.T;
+                dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xrow);
+                dim3 grid((nprop + RS_QQ - 1) / RS_QQ, (g.T + RS_TQ - 1) / RS_TQ, P);
+                prof.begin(ROME_PHASE_CROSS_GEMM);
+                if (ctx->precision == ROME_PREC_FP32)
+                    restricted_diff2_kernel<ROME_PREC_FP32><<<grid, RS_THREADS, 0, st>>>(
+                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                else if (ctx->precision == ROME_PREC_BF16)
+                    restricted_diff2_kernel<ROME_PREC_BF16><<<grid, RS_THREADS, 0, st>>>(
+                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                else
+                    restricted_diff2_kernel<ROME_PREC_BF16X3><<<grid, RS_THREADS, 0, st>>>(
+                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_CROSS_GEMM);
+                prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)P * Xrow * g.Kact);
+                prof.end(ROME_PHASE_CROSS_GEMM);
             }
-            prof.launched(ROME_PHASE_CROSS_GEMM);
-            // algorithmic work: 4 flops per active complex coefficient per (image, translation, orientation)
-            prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * g.J * g.Kact);
-            prof.end(ROME_PHASE_CROSS_GEMM);
 
             // ---- posterior: min, FP64 weights, sum, argmax, significance ----
             double* dW = nullptr;
-            if (out->weight[ipass]) dW = ctx->ws[S_WCHK].as<double>((size_t)P * g.X);
-            const PostLayout Lp{g.T, g.notr, g.nor, npsi, ntr, K};
+            if (out->weight[ipass] && !restricted) dW = ctx->ws[S_WCHK].as<double>((size_t)P * g.X);
+            PostLayout Lp{g.T, g.notr, g.nor, npsi, ntr, K};
+            if (restricted) {
+                int2* dEntR = ctx->ws[S_FENT].as<int2>((size_t)P * nprop);
+                restricted_entries_kernel<<<(unsigned)(((long)P * nprop + 255) / 256), 256, 0, st>>>(
+                    (long)P * nprop, g.nrot, dProp, dEntR);
+                ROME_CHECK_LAUNCH();
+                Lp.ent = dEntR;
+                Lp.ent_stride = nprop;
+                Lp.epr = g.T;
+            }
             prof.begin(ROME_PHASE_POSTERIOR);
             for (;;) {
                 dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
-                SelectResult sr = run_select(ctx, st, 0, P, g.X, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
+                SelectResult sr = run_select(ctx, st, 0, P, Xrow, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
                                              dPart, dPartI, nullptr, dW, dList, dCounter, listcap, dSeg, dRowMin);
                 prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
                 nsigtot = sr.nlist;
                 if (sr.nlist <= listcap) break;
                 listcap = sr.nlist;  // every segment fits on the second run
+            }
+            if (restricted && nsigtot > 0) {
+                restricted_list_dense_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.T, nprop, dProp, dList);
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_POSTERIOR);
+            }
+            if (ipass == npass - 1 && out->post_class_psi) {
+                double* dMarg = ctx->ws[S_TMP2].as<double>((size_t)P * K * npsi);
+                ROME_CUDA(cudaMemsetAsync(dMarg, 0, sizeof(double) * P * K * npsi, st));
+                if (nsigtot > 0) {
+                    post_marginal_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.T, g.nor, K * npsi, dList,
+                                                                               dMarg);
+                    ROME_CHECK_LAUNCH();
+                }
+                ROME_CUDA(cudaMemcpyAsync(out->post_class_psi, dMarg, sizeof(double) * P * K * npsi,
+                                          cudaMemcpyDeviceToHost, st));
             }
             if (ipass == 0 && (npass > 1 || out->Mcoarse_significant)) {
                 ROME_CUDA(cudaMemsetAsync(dMcoarse, 0, (size_t)P * ncoarse, st));
@@ -344,14 +409,14 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             std::vector<int> hparti((size_t)P * 8);
             ROME_CUDA(cudaMemcpyAsync(hpart.data(), dPart, sizeof(double) * P * 8, cudaMemcpyDeviceToHost, st));
             ROME_CUDA(cudaMemcpyAsync(hparti.data(), dPartI, sizeof(int) * P * 8, cudaMemcpyDeviceToHost, st));
-            if (out->diff2[ipass]) {
+            if (out->diff2[ipass] && !restricted) {
                 std::vector<float> hd((size_t)P * g.X);
                 ROME_CUDA(cudaMemcpyAsync(hd.data(), dDiff2, sizeof(float) * hd.size(), cudaMemcpyDeviceToHost, st));
                 ROME_CUDA(cudaStreamSynchronize(st));
                 for (size_t q = 0; q < hd.size(); q++)
                     out->diff2[ipass][q] = hd[q] < INFINITY ? (double)hd[q] : (double)INT_MIN;
             }
-            if (out->weight[ipass])
+            if (out->weight[ipass] && dW)
                 ROME_CUDA(cudaMemcpyAsync(out->weight[ipass], dW, sizeof(double) * P * g.X, cudaMemcpyDeviceToHost,
                                           st));
             if (ipass == 0 && out->Mcoarse_significant)
@@ -370,6 +435,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 // convertSquaredDifferencesToWeights metadata (map2d_optimizer.cpp:1199-1216)
                 long e = best;
                 int j = (int)(e / g.T), t = (int)(e % g.T);
+                if (restricted) j = in->proposals[(size_t)i * nprop + j];  // row position -> orientation
                 int r = j % g.nrot, k = j / g.nrot;
                 int itr = t / g.notr, iotr = t % g.notr;
                 if (out->pmax) out->pmax[i] = mx / sw;

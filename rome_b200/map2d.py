@@ -55,6 +55,8 @@ class Map2dPool:
     do_map: int = 1
     iclass_min: int = 0
     iclass_max: int = -1
+    # optional restricted search: [P][nr_proposals] orientations (class * nr_psi + psi), ascending
+    proposals: Optional[np.ndarray] = None
 
     @property
     def nr_images(self) -> int:
@@ -124,10 +126,15 @@ def pack_pool(p: Map2dPool):
     s.prior_offsetx_class, s.prior_offsety_class = d(p.prior_offsetx_class), d(p.prior_offsety_class)
     s.sigma2_offset, s.sigma2_fudge, s.adaptive_fraction = p.sigma2_offset, p.sigma2_fudge, p.adaptive_fraction
     s.do_ctf_correction, s.refs_are_ctf_corrected, s.do_map = p.do_ctf_correction, p.refs_are_ctf_corrected, p.do_map
+    if p.proposals is not None:
+        pr = _i32(p.proposals)
+        keep.append(pr)
+        s.proposals = abi.iptr(pr)
+        s.nr_proposals = int(pr.shape[1])
     return s, keep
 
 
-def alloc_outputs(p: Map2dPool, checkpoints: bool = False):
+def alloc_outputs(p: Map2dPool, checkpoints: bool = False, marginals: bool = False):
     """Zeroed output arrays + the RomeMap2dPoolOut struct pointing at them."""
     P, K, G, oF = p.nr_images, p.nr_classes, p.nr_groups, p.ori_size // 2 + 1
     o: Dict[str, np.ndarray] = {}
@@ -151,6 +158,9 @@ def alloc_outputs(p: Map2dPool, checkpoints: bool = False):
             s.weight[ip] = abi.dptr(o[f"weight_{ip}"])
         o["Mcoarse_significant"] = np.zeros((P, p.nr_classes * p.nr_psi * p.nr_trans), np.int8)
         s.Mcoarse_significant = abi.cptr(o["Mcoarse_significant"])
+    if marginals:
+        o["post_class_psi"] = np.zeros((P, p.nr_classes * p.nr_psi), np.float64)
+        s.post_class_psi = abi.dptr(o["post_class_psi"])
     return s, o
 
 
@@ -225,18 +235,21 @@ class GpuContext:
     def set_backprojector(self, iclass: int, data: np.ndarray, weight: np.ndarray):
         self._check(self.lib.rome_gpu_set_backprojector(self.h, iclass, abi.dptr(_f64(data)), abi.dptr(_f64(weight))))
 
-    def map2d_estep_pool(self, p, checkpoints: bool = False) -> Dict[str, np.ndarray]:
+    def map2d_estep_pool(self, p, checkpoints: bool = False, marginals: bool = False,
+                         proposals: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
         """E-step of one pool.  `p` is a Map2dPool (host arrays) or a
-        StagedPool whose particle images already live on the device."""
+        StagedPool whose particle images already live on the device.
+        `proposals` ([P][k] orientation indices, ascending) restricts the
+        search; `marginals` returns the posterior summed per (class, psi)."""
+        base = p.pool if isinstance(p, StagedPool) else p
+        if proposals is not None:
+            base = dataclasses.replace(base, proposals=proposals)
+        s, keep = pack_pool(base)
         if isinstance(p, StagedPool):
-            s, keep = pack_pool(p.pool)
             for name, t in p.dev.items():
                 setattr(s, name, C.cast(C.c_void_p(t.data_ptr()), abi._DP))
             s.inputs_on_device = 1
-            so, o = alloc_outputs(p.pool, checkpoints)
-        else:
-            s, keep = pack_pool(p)
-            so, o = alloc_outputs(p, checkpoints)
+        so, o = alloc_outputs(base, checkpoints, marginals)
         self._check(self.lib.rome_gpu_map2d_estep_pool(self.h, C.byref(s), C.byref(so)))
         return o
 

@@ -37,6 +37,7 @@ class Map2dWorkload:
     defocus: tuple = (10000.0, 30000.0)
     seed: int = 1
     random_perturbation: float = 0.0  # sampler perturbation in units of the step
+    particle_seed: Optional[int] = None  # particles from another seed, same class templates
 
 
 def grid_templates(rng, ori, K, n_blobs, sig):
@@ -167,6 +168,8 @@ def build_map2d(w: Map2dWorkload):
         d, r_max, pad = projector_map_2d(refs[k], cur)
         proj.append(d)
     proj = np.stack(proj)
+    if w.particle_seed is not None:
+        rng = np.random.default_rng(w.particle_seed)
     N = w.n_particles
     Fs = cur // 2 + 1
     cls = rng.integers(0, K, N)
@@ -232,6 +235,8 @@ def subset(p: Map2dPool, lo: int, hi: int) -> Map2dPool:
     for name in ["Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf", "highres_Xi2",
                  "old_offsetx", "old_offsety", "group"]:
         setattr(q, name, np.ascontiguousarray(getattr(p, name)[lo:hi]))
+    if p.proposals is not None:
+        q.proposals = np.ascontiguousarray(p.proposals[lo:hi])
     return q
 
 
