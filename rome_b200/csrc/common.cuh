@@ -149,6 +149,11 @@ struct RomeGpuCtx {
     rome::DevBuf ws[rome::S_COUNT];
     // host-side staging
     std::vector<double> h_tmp;
+    // page-locked arena for the small per-call uploads (tables, per-particle
+    // scalars): copies from it are asynchronous and do not wait behind the
+    // caller's own large transfers on other streams; reset at every entry point
+    char* h_arena = nullptr;
+    size_t h_arena_cap = 0, h_arena_used = 0;
     // shift table (cos, sin) from the host's libm, identical to the reference's
     double2* d_shift_tab = nullptr;
     // device flag raised by kernels whose bounded waits expire
@@ -164,6 +169,30 @@ struct RomeGpuCtx {
 };
 
 namespace rome {
+
+// start of an entry point: the stream is idle (every entry point ends with a
+// synchronize; this one also covers an earlier call that failed part-way), so
+// the upload arena can be reused from its start
+inline void arena_reset(RomeGpuCtx* ctx) {
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->h_arena_used = 0;
+}
+
+// host -> device copy of n elements on the context's stream, staged through
+// the page-locked arena when it has room
+template <typename T>
+void stage_copy(RomeGpuCtx* ctx, T* dst, const T* host, size_t n) {
+    const size_t bytes = sizeof(T) * n, at = (ctx->h_arena_used + 255) & ~(size_t)255;
+    if (ctx->h_arena && at + bytes <= ctx->h_arena_cap) {
+        memcpy(ctx->h_arena + at, host, bytes);
+        ctx->h_arena_used = at + bytes;
+        host = (const T*)(ctx->h_arena + at);
+    }
+    if (n) {
+        cudaError_t e = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) fail(ROME_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    }
+}
 
 // run a function, converting RomeFail into a status and recording the message
 template <typename F>

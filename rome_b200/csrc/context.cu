@@ -46,6 +46,8 @@ extern "C" int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx*
         ROME_CUDA(cudaMemcpy(ctx->d_shift_tab, tab.data(), sizeof(double2) * nr, cudaMemcpyHostToDevice));
         ROME_CUDA(cudaMalloc(&ctx->d_err, sizeof(int)));
         ROME_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
+        ctx->h_arena_cap = (size_t)16 << 20;
+        ROME_CUDA(cudaHostAlloc((void**)&ctx->h_arena, ctx->h_arena_cap, cudaHostAllocDefault));
     });
     if (rc != ROME_OK) {
         fprintf(stderr, "rome_gpu_create: %s\n", ctx->last_error.c_str());
@@ -66,6 +68,7 @@ extern "C" int rome_gpu_destroy(RomeGpuCtx* ctx) {
     if (ctx->bp_weight) cudaFree(ctx->bp_weight);
     if (ctx->d_shift_tab) cudaFree(ctx->d_shift_tab);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->h_arena) cudaFreeHost(ctx->h_arena);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ROME_OK;

@@ -27,6 +27,20 @@ struct StoreEpi {
     __device__ __forceinline__ void finish_row(int, float) const {}
 };
 
+// out[m][n] = v + bias[n / group] (a per-class bias over `group` columns)
+struct BiasStoreEpi {
+    float* out;
+    int ld;
+    const float* bias;
+    int group;
+    __device__ __forceinline__ float operator()(int m, int n, float v) const {
+        v += bias[n / group];
+        out[(long)m * ld + n] = v;
+        return v;
+    }
+    __device__ __forceinline__ void finish_row(int, float) const {}
+};
+
 // diff2 epilogue of the cross-term GEMM (rows m = particle*T + translation,
 // columns j = orientation), written in the reference's exp_Mweight layout
 // [particle][((class*npsi+psi)*nor+over_rot)*T + trans*notr + over_trans].

@@ -22,107 +22,10 @@
 
 #include "common.cuh"
 #include "gemm_tc.cuh"
+#include "tc_ptx.cuh"
 
 namespace rome {
 namespace {
-
-constexpr int BM = 128;
-constexpr int BK = 64;  // one 128-byte swizzle atom of bf16
-constexpr long WAIT_LIMIT = 1L << 28;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// bounded wait on an mbarrier phase (iteration count and 2 s of wall time);
-// returns false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t addr = smem_u32(bar);
-    uint64_t t0 = 0;
-    for (long it = 0; it < WAIT_LIMIT; it++) {
-        uint32_t ok;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(ok)
-            : "r"(addr), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if ((it & 1023) == 0) {
-            uint64_t t = global_ns();
-            if (it == 0) t0 = t;
-            else if (t - t0 > 2000000000ull) return false;
-        }
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::
-            "r"(smem_u32(dst)),
-        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-        : "memory");
-}
-
-// UMMA shared-memory descriptor, K-major, 128-byte swizzle: 8-row groups of
-// 1024 bytes (SBO = 64 x 16 B), LBO = 16 B, descriptor version 1 (sm_100)
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr & 0x3FFFF) >> 4);
-    d |= (uint64_t)1 << 16;
-    d |= (uint64_t)64 << 32;
-    d |= (uint64_t)1 << 46;
-    d |= (uint64_t)2 << 61;
-    return d;
-}
-
-// instruction descriptor: D f32, A/B bf16, both K-major, M = 128, N = BN
-template <int BN>
-__device__ __forceinline__ uint32_t idesc_bf16() {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc));
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int q = 0; q < 16; q++) v[q] = __uint_as_float(r[q]);
-}
 
 template <int BN, int NPLANE, int STAGES>
 struct TcSmem {
@@ -258,34 +161,6 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
-// ---------------------------------------------------------------------------
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        ROME_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
-        if (!p || q != cudaDriverEntryPointSuccess) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    }
-    return fn;
-}
-
-// 2D bf16 tensor map over a [rows][Kp] K-contiguous operand, box BK x box_rows
-CUtensorMap make_map(const void* base, long rows, int Kp, int box_rows) {
-    ROME_REQUIRE(((uintptr_t)base & 15) == 0 && Kp % BK == 0, "operand alignment");
-    CUtensorMap m;
-    cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
-    cuuint32_t box[2] = {(cuuint32_t)BK, (cuuint32_t)box_rows};
-    cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
-                             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r != CUDA_SUCCESS) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-    return m;
-}
-
 template <int BN, int NPLANE, int STAGES, typename Epi>
 void launch(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, const Epi& epi, int* derr) {
     using S = TcSmem<BN, NPLANE, STAGES>;
@@ -319,6 +194,11 @@ void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const v
     launch<128, 2, 3>(st, M, N, Kp, A, B, StoreEpi{out, ld}, derr);
 }
 
+void tc_bias_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
+                  const float* bias, int group, int* derr) {
+    launch<128, 2, 3>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
+}
+
 // hi/lo bf16 planes of a [rows][K] fp32 matrix, zero padded to Kpad columns
 __global__ void split_bf16_kernel(const float* __restrict__ in, long rows, int K, int ldin, int Kpad,
                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
@@ -337,6 +217,36 @@ void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, in
     __nv_bfloat16* lo = hi + rows * Kpad;
     long n = rows * Kpad;
     split_bf16_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, rows, K, ldin, Kpad, hi, lo);
+    ROME_CHECK_LAUNCH();
+}
+
+// transposed split: out[c][r] = in[r][c] (hi plane [cols][rows_pad], then lo),
+// rows beyond `rows` zero; 32 x 32 tiles through shared memory
+__global__ void split_bf16_t_kernel(const float* __restrict__ in, int rows, int cols, int ldin, int rows_pad,
+                                    __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    __shared__ float tile[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int r = r0 + y, c = c0 + threadIdx.x;
+        tile[y][threadIdx.x] = (r < rows && c < cols) ? in[(long)r * ldin + c] : 0.f;
+    }
+    __syncthreads();
+    for (int y = threadIdx.y; y < 32; y += blockDim.y) {
+        const int c = c0 + y, r = r0 + threadIdx.x;
+        if (c < cols && r < rows_pad) {
+            const float v = tile[threadIdx.x][y];
+            const __nv_bfloat16 h = __float2bfloat16_rn(v);
+            hi[(long)c * rows_pad + r] = h;
+            lo[(long)c * rows_pad + r] = __float2bfloat16_rn(v - __bfloat162float(h));
+        }
+    }
+}
+
+void split_bf16_t(cudaStream_t st, const float* in, int rows, int cols, int ldin, int rows_pad, void* out) {
+    __nv_bfloat16* hi = (__nv_bfloat16*)out;
+    __nv_bfloat16* lo = hi + (size_t)cols * rows_pad;
+    dim3 grid((cols + 31) / 32, (rows_pad + 31) / 32);
+    split_bf16_t_kernel<<<grid, dim3(32, 8), 0, st>>>(in, rows, cols, ldin, rows_pad, hi, lo);
     ROME_CHECK_LAUNCH();
 }
 

@@ -13,8 +13,13 @@ void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const v
 // out[m][n] = A . B^T in split precision (hi*hi + hi*lo + lo*hi)
 void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
                    int* derr);
+// out[m][n] = A . B^T + bias[n / group], split precision
+void tc_bias_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
+                  const float* bias, int group, int* derr);
 // bf16 hi plane then lo plane of a [rows][ldin] fp32 matrix, K columns used, padded to Kpad
 void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, int Kpad, void* out);
+// the same planes of the transpose: [cols][rows_pad] from a [rows][ldin] matrix (rows beyond `rows` zero)
+void split_bf16_t(cudaStream_t st, const float* in, int rows, int cols, int ldin, int rows_pad, void* out);
 // raises ROME_ERR_TIMEOUT if a tensor-core kernel's bounded wait expired
 void tc_check_error(cudaStream_t st, int* derr);
 }  // namespace rome

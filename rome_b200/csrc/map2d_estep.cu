@@ -25,6 +25,7 @@
 #include "gemm_simt.cuh"
 #include "gemm_tc.cuh"
 #include "restricted_kernels.cuh"
+#include "restricted_tc.cuh"
 #include "select_kernels.cuh"
 
 using namespace rome;
@@ -45,7 +46,7 @@ struct PassGeom {
 template <typename T>
 T* upload(RomeGpuCtx* ctx, Slot s, const T* host, size_t n) {
     T* d = ctx->ws[s].as<T>(n);
-    if (n) ROME_CUDA(cudaMemcpyAsync(d, host, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    stage_copy(ctx, d, host, n);
     return d;
 }
 
@@ -73,6 +74,8 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
     if (!ctx || !in || !out) return ROME_ERR_ARG;
     return guarded(ctx, [&] {
         if (!ctx->proj || ctx->ref_dim != 2) fail(ROME_ERR_STATE, "2D projectors not set (rome_gpu_set_projectors)");
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        arena_reset(ctx);
         const int P = in->nr_images, K = in->nr_classes, ori = in->ori_size, cur = in->current_size;
         const int npsi = in->nr_psi, ntr = in->nr_trans, G = in->nr_groups, oriF = ori / 2 + 1;
         ROME_REQUIRE(P > 0 && K == ctx->nr_classes && ori == ctx->ori_size, "pool/projector mismatch");
@@ -279,20 +282,40 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
 
             // ---- shifted images -> A operand, S term ----
             const long M = (long)P * g.T;
-            void* dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+            // restricted search on the tensor cores: no shifted images, the
+            // translations enter through a [32][Kp] phase operand instead
+            const bool rtc = restricted && tc && g.T <= 256;
+            const int Kh = g.Kp / 2;
+            void* dA = nullptr;
+            float2* dXw = nullptr;
+            float* dW2h = nullptr;
+            void* dSh = nullptr;
             float* dS = ctx->ws[S_S].as<float>((size_t)M);
-            float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+            float* dW2 = nullptr;
             prof.begin(ROME_PHASE_SHIFT);
             unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)g.T * g.Kact);
             phase_index_kernel<<<(unsigned)(((long)g.T * g.Kact + 255) / 256), 256, 0, st>>>(
                 g.T, g.Kact, g.csF, cs, dAct, dShift, ctx->shift_sampling, dPidx);
             prof.launched(ROME_PHASE_SHIFT);
-            shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, g.T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
-                                                           apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
-                                                           ctx->precision);
-            prof.launched(ROME_PHASE_SHIFT);
-            w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
-            prof.launched(ROME_PHASE_SHIFT);
+            if (rtc) {
+                char* buf = (char*)ctx->ws[S_A].get((size_t)P * Kh * (sizeof(float2) + sizeof(float)));
+                dXw = (float2*)buf;
+                dW2h = (float*)(buf + (size_t)P * Kh * sizeof(float2));
+                dSh = ctx->ws[S_NORM].get((size_t)2 * restricted_tile_tn(g.T) * g.Kp * 2);
+                restricted_prep(st, P, g.F, g.Kact, Kh, dFimg, dLctf, dMinv, apply_ctf ? 1 : 0, dAct, dXw, dW2h, dS);
+                prof.launched(ROME_PHASE_SHIFT);
+                restricted_shift_operand(st, g.T, g.Kact, g.Kp, dPidx, ctx->d_shift_tab, ctx->precision, dSh);
+                prof.launched(ROME_PHASE_SHIFT);
+            } else {
+                dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+                dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+                shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, g.T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                                                               apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA,
+                                                               dS, ctx->precision);
+                prof.launched(ROME_PHASE_SHIFT);
+                w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+                prof.launched(ROME_PHASE_SHIFT);
+            }
             prof.end(ROME_PHASE_SHIFT);
 
             unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
@@ -339,16 +362,25 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xrow);
                 dim3 grid((nprop + RS_QQ - 1) / RS_QQ, (g.T + RS_TQ - 1) / RS_TQ, P);
                 prof.begin(ROME_PHASE_CROSS_GEMM);
-                if (ctx->precision == ROME_PREC_FP32)
-                    restricted_diff2_kernel<ROME_PREC_FP32><<<grid, RS_THREADS, 0, st>>>(
-                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
-                else if (ctx->precision == ROME_PREC_BF16)
-                    restricted_diff2_kernel<ROME_PREC_BF16><<<grid, RS_THREADS, 0, st>>>(
-                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
-                else
-                    restricted_diff2_kernel<ROME_PREC_BF16X3><<<grid, RS_THREADS, 0, st>>>(
-                        g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
-                ROME_CHECK_LAUNCH();
+                if (rtc) {
+                    restricted_tc_diff2(st, ctx->precision, P, nprop, g.T, g.Kp, dProp, dJvalid, dXw, dW2h, dB, g.J,
+                                        dSh, dS, dXi2, Xrow, dDiff2, dRowMin, ctx->d_err);
+                } else {
+                    // CUDA cores over the shifted images (FP32 mode, or more than 256 translations)
+                    if (ctx->precision == ROME_PREC_FP32)
+                        restricted_diff2_kernel<ROME_PREC_FP32><<<grid, RS_THREADS, 0, st>>>(
+                            g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2,
+                            dRowMin);
+                    else if (ctx->precision == ROME_PREC_BF16)
+                        restricted_diff2_kernel<ROME_PREC_BF16><<<grid, RS_THREADS, 0, st>>>(
+                            g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2,
+                            dRowMin);
+                    else
+                        restricted_diff2_kernel<ROME_PREC_BF16X3><<<grid, RS_THREADS, 0, st>>>(
+                            g.T, g.Kp, g.Kq, nprop, M, g.J, dProp, dJvalid, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2,
+                            dRowMin);
+                    ROME_CHECK_LAUNCH();
+                }
                 prof.launched(ROME_PHASE_CROSS_GEMM);
                 prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)P * Xrow * g.Kact);
                 prof.end(ROME_PHASE_CROSS_GEMM);

@@ -19,13 +19,17 @@
 // Parameters: one flat FP32 array w0 b0 w1 b1 wf bf, each block at a multiple
 // of 4 floats.  The CPU restatement is oracle/proposal_oracle.py.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 #include <random>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
+#include "gemm_tc.cuh"
 
 using namespace rome;
 
@@ -51,6 +55,17 @@ struct RomeProposalNet {
     float* tgt = nullptr;
     double* loss_acc = nullptr;
     int* idx = nullptr;
+    // the head as tensor-core GEMMs (split-bf16 operands):
+    //   z = h . WT^T,  WT[(k,p)][(c,r,d)] = wf[k][c][r][(d + p) mod A]
+    int CRA = 0, CRAp = 0, KA = 0, KAp = 0;  // C*R*A and K*A, padded to multiples of 64
+    void* wt = nullptr;                      // WT  [KA][CRAp] hi, lo
+    void* wtt = nullptr;                     // WT^T [CRA][KAp] hi, lo
+    float* dwt = nullptr;                    // dL/dWT [KA][CRA]
+    bool wt_dirty = true;                    // parameters changed since WT was expanded
+    void* hs = nullptr;                      // h1 [n][CRAp] hi, lo
+    void* dzs = nullptr;                     // dz [n][KAp] hi, lo
+    void* dzt = nullptr;                     // dz^T [KA][npad] hi, lo
+    void* ht = nullptr;                      // h1^T [CRA][npad] hi, lo
 };
 
 namespace rome {
@@ -87,6 +102,63 @@ __global__ void __launch_bounds__(PT) pconv_fwd_kernel(int Ci, int R, int A, int
         }
     }
     y[(((long)n * Co + co) * R + r) * A + a] = fmaxf(acc, 0.f);
+}
+
+// The same convolution with one CTA per sample: the sample's input planes
+// and the layer's weights ([ci][tap][co], 16-byte groups of 4 output
+// channels) in shared memory; each thread item is 4 output channels at one
+// (r, theta) position, consecutive threads at consecutive positions.  The
+// taps are accumulated in the order of pconv_fwd_kernel (bias, then ci, kh,
+// kw), so both give identical results.  Used when Co % 4 == 0 and the
+// sample fits in shared memory (pconv_smem_bytes).
+size_t pconv_smem_bytes(int Ci, int R, int A, int Co) {
+    const size_t xin = ((size_t)Ci * R * A + 3) / 4 * 4;
+    return sizeof(float) * (xin + (size_t)Ci * 9 * Co);
+}
+
+__global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A, int Co,
+                                                             const float* __restrict__ x,
+                                                             const float* __restrict__ w,
+                                                             const float* __restrict__ b, float* __restrict__ y) {
+    extern __shared__ float4 sm4[];
+    float* xs = (float*)sm4;
+    const int RA = R * A, G = Co / 4;
+    float* ws = xs + ((long)Ci * RA + 3) / 4 * 4;
+    const int n = blockIdx.x;
+    const float* xn = x + (long)n * Ci * RA;
+    for (int q = threadIdx.x; q < Ci * RA; q += PT) xs[q] = xn[q];
+    for (int q = threadIdx.x; q < Co * Ci * 9; q += PT) {
+        const int co = q / (Ci * 9), rest = q - co * (Ci * 9);
+        ws[rest * Co + co] = w[q];
+    }
+    __syncthreads();
+    for (int item = threadIdx.x; item < G * RA; item += PT) {
+        const int g = item / RA, pos = item - g * RA;
+        const int r = pos / A, a = pos - r * A;
+        const int am = a == 0 ? A - 1 : a - 1, ap = a == A - 1 ? 0 : a + 1;
+        float acc[4] = {b[4 * g], b[4 * g + 1], b[4 * g + 2], b[4 * g + 3]};
+        for (int ci = 0; ci < Ci; ci++) {
+            const float* xc = xs + ci * RA;
+            const float4* wc = (const float4*)(ws + (long)ci * 9 * Co) + g;
+#pragma unroll
+            for (int kh = 0; kh < 3; kh++) {
+                const int rr = r + kh - 1;
+                if (rr < 0 || rr >= R) continue;
+                const float* row = xc + rr * A;
+                const float v[3] = {row[am], row[a], row[ap]};
+#pragma unroll
+                for (int kw = 0; kw < 3; kw++) {
+                    const float4 wv = wc[(kh * 3 + kw) * G];
+                    acc[0] = fmaf(wv.x, v[kw], acc[0]);
+                    acc[1] = fmaf(wv.y, v[kw], acc[1]);
+                    acc[2] = fmaf(wv.z, v[kw], acc[2]);
+                    acc[3] = fmaf(wv.w, v[kw], acc[3]);
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++) y[(((long)n * Co + 4 * g + c) * R + r) * A + a] = fmaxf(acc[c], 0.f);
+    }
 }
 
 // dy <- dy * (y > 0): the ReLU's gradient, in place
@@ -183,92 +255,44 @@ __global__ void __launch_bounds__(PT) bias_grad_kernel(int N, int C, int HW, con
 
 // ---- equivariant head: circular correlation along theta, full over (c, r) ----
 // z[n][k][p] = bf[k] + sum_{c,r,d} wf[k][c][r][d] h[n][c][r][(d - p) mod A]
-// One CTA per sample with h[n] in shared memory; warp w takes classes w, w+8, ...
-// and its lanes the output angles p.
-__global__ void __launch_bounds__(PT) head_fwd_kernel(int CR, int A, int K, const float* __restrict__ h,
-                                                       const float* __restrict__ wf, const float* __restrict__ bf,
-                                                       float* __restrict__ z) {
-    extern __shared__ float sh_h[];  // CR * A
-    const int n = blockIdx.x;
-    const float* hn = h + (long)n * CR * A;
-    for (int q = threadIdx.x; q < CR * A; q += PT) sh_h[q] = hn[q];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = warp; k < K; k += PT / 32) {
-        const float* wk = wf + (long)k * CR * A;
-        for (int p0 = 0; p0 < A; p0 += 32) {
-            const int p = p0 + lane;
-            float acc = 0.f;
-            if (p < A) {
-                for (int cr = 0; cr < CR; cr++) {
-                    const float* hr = sh_h + cr * A;
-                    const float* wr = wk + cr * A;
-                    int idx = A - p;  // (d - p) mod A at d = 0
-                    if (idx == A) idx = 0;
-                    for (int d = 0; d < A; d++) {
-                        acc = fmaf(__ldg(wr + d), hr[idx], acc);
-                        if (++idx == A) idx = 0;
-                    }
-                }
-                z[((long)n * K + k) * A + p] = acc + bf[k];
-            }
-        }
+//            = bf[k] + sum_{c,r,d'} h[n][c][r][d'] wf[k][c][r][(d' + p) mod A]
+// i.e. z = h . WT^T with the rolled weight matrix WT[(k,p)][(c,r,d')]; the
+// three products of forward and backward run as split-bf16 tcgen05 GEMMs.
+
+// WT (transposed = 0: [KA][CRAp]) or WT^T (transposed = 1: [CRA][KAp]), split
+// into bf16 hi and lo planes, zero padded
+__global__ void head_expand_kernel(int K, int CR, int A, int ld, int rows, int transposed, const float* __restrict__ wf,
+                                   __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long)rows * ld) return;
+    const int row = (int)(q / ld), col = (int)(q - (long)row * ld);
+    const int kp = transposed ? col : row, crd = transposed ? row : col;
+    float v = 0.f;
+    if (kp < K * A && crd < CR * A) {
+        const int k = kp / A, p = kp - k * A, cr = crd / A, d = crd - cr * A;
+        int dd = d + p;
+        if (dd >= A) dd -= A;
+        v = wf[((long)k * CR + cr) * A + dd];
     }
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[q] = h;
+    lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
 }
 
-// dh[n][c][r][t] = sum_{k,p} dz[n][k][p] wf[k][c][r][(t + p) mod A]; one CTA per sample
-__global__ void __launch_bounds__(PT) head_bwd_data_kernel(int CR, int A, int K, const float* __restrict__ dz,
-                                                            const float* __restrict__ wf, float* __restrict__ dh) {
-    extern __shared__ float sdz[];  // K * A
-    const int n = blockIdx.x;
-    for (int q = threadIdx.x; q < K * A; q += PT) sdz[q] = dz[(long)n * K * A + q];
-    __syncthreads();
-    for (int e = threadIdx.x; e < CR * A; e += PT) {
-        const int cr = e / A, t = e - cr * A;
-        float acc = 0.f;
-        for (int k = 0; k < K; k++) {
-            const float* wr = wf + ((long)k * CR + cr) * A;
-            const float* dk = sdz + k * A;
-            int idx = t;  // (t + p) mod A at p = 0
-            for (int p = 0; p < A; p++) {
-                acc = fmaf(dk[p], __ldg(wr + idx), acc);
-                if (++idx == A) idx = 0;
-            }
-        }
-        dh[(long)n * CR * A + e] = acc;
+// dwf[k][c][r][d] = sum_p dWT[(k,p)][(c,r,(d - p) mod A)]
+__global__ void head_fold_kernel(int K, int CR, int A, const float* __restrict__ dwt, float* __restrict__ dwf) {
+    const long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long)K * CR * A) return;
+    const int k = (int)(q / ((long)CR * A));
+    const int crd = (int)(q - (long)k * CR * A), cr = crd / A, d = crd - cr * A;
+    const long CRA = (long)CR * A;
+    float acc = 0.f;
+    int idx = d;  // (d - p) mod A at p = 0
+    for (int p = 0; p < A; p++) {
+        acc += dwt[((long)k * A + p) * CRA + (long)cr * A + idx];
+        if (--idx < 0) idx = A - 1;
     }
-}
-
-// dwf[k][c][r][d] = sum_{n,p} dz[n][k][p] h[n][c][r][(d - p) mod A]; one CTA per class
-__global__ void __launch_bounds__(PT) head_bwd_weight_kernel(int N, int CR, int A, int K, const float* __restrict__ dz,
-                                                              const float* __restrict__ h, float* __restrict__ dwf,
-                                                              float* __restrict__ dbf) {
-    __shared__ float sdz[256];
-    __shared__ float red[32];
-    const int k = blockIdx.x;
-    float bsum = 0.f;
-    for (int e0 = 0; e0 < CR * A; e0 += PT) {
-        const int e = e0 + threadIdx.x;
-        const int cr = e / A, d = e - cr * A;
-        float acc = 0.f;
-        for (int n = 0; n < N; n++) {
-            __syncthreads();
-            for (int q = threadIdx.x; q < A; q += PT) sdz[q] = dz[((long)n * K + k) * A + q];
-            __syncthreads();
-            if (e < CR * A) {
-                const float* hr = h + ((long)n * CR + cr) * A;
-                int idx = d;  // (d - p) mod A at p = 0
-                for (int p = 0; p < A; p++) {
-                    acc = fmaf(sdz[p], __ldg(hr + idx), acc);
-                    if (--idx < 0) idx = A - 1;
-                }
-            }
-            if (e0 == 0 && threadIdx.x < A) bsum += sdz[threadIdx.x];
-        }
-        if (e < CR * A) dwf[(long)k * CR * A + e] = acc;
-    }
-    bsum = block_sum(bsum, red);
-    if (threadIdx.x == 0) dbf[k] = bsum;
+    dwf[q] = acc;
 }
 
 // per sample: p = softmax(z), loss += -sum t log p, dz = (p - t) / N
@@ -395,61 +419,52 @@ __global__ void __launch_bounds__(PT) polar_features_kernel(int cur, int R, int 
 }
 
 // top-k of each row of logits (descending; ties by lower index), with the
-// softmax probability of each
-__global__ void __launch_bounds__(PT) topk_kernel(int O, int k, const float* __restrict__ z, int* __restrict__ idx,
-                                                   float* __restrict__ prob) {
-    extern __shared__ unsigned char smraw[];
-    const int n2 = 1 << (32 - __clz(O - 1));
-    float* key = (float*)smraw;
-    int* val = (int*)(key + n2);
-    __shared__ float shf[32];
-    __shared__ float s_max, s_sum;
-    const int r = blockIdx.x;
-    const float* zr = z + (long)r * O;
-    for (int q = threadIdx.x; q < n2; q += PT) {
-        key[q] = q < O ? zr[q] : -INFINITY;
-        val[q] = q < O ? q : 0x7fffffff;
-    }
-    float m = -INFINITY;
-    for (int o = threadIdx.x; o < O; o += PT) m = fmaxf(m, zr[o]);
-    for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, off));
-    if ((threadIdx.x & 31) == 0) shf[threadIdx.x >> 5] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        float mm = shf[0];
-        for (int q = 1; q < PT / 32; q++) mm = fmaxf(mm, shf[q]);
-        s_max = mm;
-    }
-    __syncthreads();
-    float se = 0.f;
-    for (int o = threadIdx.x; o < O; o += PT) se += __expf(zr[o] - s_max);
-    se = block_sum(se, shf);
-    if (threadIdx.x == 0) s_sum = se;
-    __syncthreads();
-    // bitonic sort, descending by key, ascending index on ties
-    for (int kk = 2; kk <= n2; kk <<= 1) {
-        for (int j = kk >> 1; j > 0; j >>= 1) {
-            for (int q = threadIdx.x; q < n2; q += PT) {
-                const int p = q ^ j;
-                if (p > q) {
-                    const bool desc = (q & kk) == 0;
-                    const float a = key[q], b = key[p];
-                    const int ia = val[q], ib = val[p];
-                    const bool a_first = a > b || (a == b && ia < ib);
-                    if (desc ? !a_first : a_first) {
-                        key[q] = b;
-                        key[p] = a;
-                        val[q] = ib;
-                        val[p] = ia;
-                    }
-                }
+// softmax probability of each.  One warp per row and no sort: k rounds of a warp
+// argmax over the row, each round restricted to the elements after the
+// previous pick in the order (value descending, index ascending), which
+// excludes every earlier pick.  The row is read from L1/L2 each round.
+__global__ void __launch_bounds__(PT) topk_warp_kernel(int n, int O, int k, const float* __restrict__ z,
+                                                        int* __restrict__ idx, float* __restrict__ prob) {
+    const int row = (int)(((long)blockIdx.x * PT + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;  // whole warps leave together
+    const float* zr = z + (long)row * O;
+    float pv = INFINITY, mx = 0.f, sum = 0.f;
+    int pi = -1;
+    for (int q = 0; q < k; q++) {
+        float bv = -INFINITY;
+        int bi = INT_MAX;
+        for (int o = lane; o < O; o += 32) {
+            const float v = __ldg(zr + o);
+            const bool below = v < pv || (v == pv && o > pi);
+            const bool better = v > bv || (v == bv && o < bi);
+            if (below && better) {
+                bv = v;
+                bi = o;
             }
-            __syncthreads();
         }
-    }
-    for (int q = threadIdx.x; q < k; q += PT) {
-        idx[(long)r * k + q] = val[q];
-        if (prob) prob[(long)r * k + q] = __expf(key[q] - s_max) / s_sum;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const float ov = __shfl_xor_sync(0xffffffffu, bv, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ov > bv || (ov == bv && oi < bi)) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if (q == 0) {
+            mx = bv;
+            float se = 0.f;
+            for (int o = lane; o < O; o += 32) se += __expf(__ldg(zr + o) - mx);
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) se += __shfl_xor_sync(0xffffffffu, se, off);
+            sum = se;
+        }
+        if (lane == 0) {
+            idx[(long)row * k + q] = bi;
+            if (prob) prob[(long)row * k + q] = __expf(bv - mx) / sum;
+        }
+        pv = bv;
+        pi = bi;
     }
 }
 
@@ -487,40 +502,82 @@ void net_alloc_batch(RomeProposalNet* net, int n) {
     const size_t ra = (size_t)net->R * net->A, O = (size_t)net->K * net->A;
     for (float** p : {&net->x, &net->h0, &net->h1, &net->dh0, &net->dh1, &net->z, &net->dz, &net->tgt})
         if (*p) cudaFree(*p);
+    for (void** p : {&net->hs, &net->dzs, &net->dzt, &net->ht})
+        if (*p) cudaFree(*p);
     ROME_CUDA(cudaMalloc(&net->x, sizeof(float) * n * 2 * ra));
     ROME_CUDA(cudaMalloc(&net->h0, sizeof(float) * n * net->c0 * ra));
     ROME_CUDA(cudaMalloc(&net->dh0, sizeof(float) * n * net->c0 * ra));
     ROME_CUDA(cudaMalloc(&net->h1, sizeof(float) * n * net->c1 * ra));
     ROME_CUDA(cudaMalloc(&net->dh1, sizeof(float) * n * net->c1 * ra));
     for (float** p : {&net->z, &net->dz, &net->tgt}) ROME_CUDA(cudaMalloc(p, sizeof(float) * n * O));
+    const size_t npad = (size_t)(n + 63) / 64 * 64;
+    ROME_CUDA(cudaMalloc(&net->hs, 4 * (size_t)n * net->CRAp));
+    ROME_CUDA(cudaMalloc(&net->dzs, 4 * (size_t)n * net->KAp));
+    ROME_CUDA(cudaMalloc(&net->dzt, 4 * (size_t)net->KA * npad));
+    ROME_CUDA(cudaMalloc(&net->ht, 4 * (size_t)net->CRA * npad));
     if (net->idx) cudaFree(net->idx);
     ROME_CUDA(cudaMalloc(&net->idx, sizeof(int) * n));
     net->cap_n = n;
 }
 
+// WT and WT^T from the current head weights (after every parameter change)
+void net_expand_head(RomeProposalNet* net, cudaStream_t st) {
+    if (!net->wt_dirty) return;
+    const int CR = net->c1 * net->R;
+    const float* wf = net->params + net->off[4];
+    const long n1 = (long)net->KA * net->CRAp, n2 = (long)net->CRA * net->KAp;
+    __nv_bfloat16* w1 = (__nv_bfloat16*)net->wt;
+    __nv_bfloat16* w2 = (__nv_bfloat16*)net->wtt;
+    head_expand_kernel<<<(unsigned)((n1 + PT - 1) / PT), PT, 0, st>>>(net->K, CR, net->A, net->CRAp, net->KA, 0, wf,
+                                                                     w1, w1 + n1);
+    head_expand_kernel<<<(unsigned)((n2 + PT - 1) / PT), PT, 0, st>>>(net->K, CR, net->A, net->KAp, net->CRA, 1, wf,
+                                                                     w2, w2 + n2);
+    ROME_CHECK_LAUNCH();
+    net->ctx->total_launches += 2;
+    net->wt_dirty = false;
+}
+
+// one 3x3 polar convolution + ReLU over n samples
+void conv_forward(int Ci, int R, int A, int Co, int n, const float* x, const float* w, const float* b, float* y,
+                  cudaStream_t st) {
+    const size_t sm = pconv_smem_bytes(Ci, R, A, Co);
+    if (Co % 4 == 0 && sm <= 96 * 1024) {
+        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        pconv_fwd_smem_kernel<<<n, PT, sm, st>>>(Ci, R, A, Co, x, w, b, y);
+    } else {
+        dim3 g((R * A + PT - 1) / PT, Co, n);
+        pconv_fwd_kernel<<<g, PT, sizeof(float) * Ci * 9, st>>>(Ci, R, A, Co, x, w, b, y);
+    }
+    ROME_CHECK_LAUNCH();
+}
+
 void net_forward(RomeProposalNet* net, int n, cudaStream_t st) {
     const int R = net->R, A = net->A;
-    dim3 g0((R * A + PT - 1) / PT, net->c0, n), g1((R * A + PT - 1) / PT, net->c1, n);
-    pconv_fwd_kernel<<<g0, PT, sizeof(float) * 2 * 9, st>>>(2, R, A, net->c0, net->x, net->params + net->off[0],
-                                                          net->params + net->off[1], net->h0);
-    pconv_fwd_kernel<<<g1, PT, sizeof(float) * net->c0 * 9, st>>>(net->c0, R, A, net->c1, net->h0,
-                                                                 net->params + net->off[2], net->params + net->off[3],
-                                                                 net->h1);
-    const int hsmem = (int)(sizeof(float) * net->c1 * R * A);
-    ROME_CUDA(cudaFuncSetAttribute(head_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, hsmem));
-    head_fwd_kernel<<<n, PT, hsmem, st>>>(net->c1 * R, A, net->K, net->h1, net->params + net->off[4],
-                                          net->params + net->off[5], net->z);
-    ROME_CHECK_LAUNCH();
+    const float* P = net->params;
+    conv_forward(2, R, A, net->c0, n, net->x, P + net->off[0], P + net->off[1], net->h0, st);
+    conv_forward(net->c0, R, A, net->c1, n, net->h0, P + net->off[2], P + net->off[3], net->h1, st);
+    net_expand_head(net, st);
+    split_bf16(st, net->h1, n, net->CRA, net->CRA, net->CRAp, net->hs);
+    tc_bias_gemm(st, n, net->KA, net->CRAp, net->hs, net->wt, net->z, net->KA, net->params + net->off[5], A,
+                 net->ctx->d_err);
+    net->ctx->total_launches += 4;
 }
 
 // gradients of the mean loss into net->grads (dz holds dL/dz)
 void net_backward(RomeProposalNet* net, int n, cudaStream_t st) {
     const int R = net->R, A = net->A, CR = net->c1 * R;
-    head_bwd_weight_kernel<<<net->K, PT, 0, st>>>(n, CR, A, net->K, net->dz, net->h1, net->grads + net->off[4],
-                                                   net->grads + net->off[5]);
-    head_bwd_data_kernel<<<n, PT, sizeof(float) * net->K * A, st>>>(CR, A, net->K, net->dz,
-                                                                    net->params + net->off[4], net->dh1);
+    const int npad = (n + 63) / 64 * 64;
+    // head: dWT = dz^T . h (folded into dwf), dbf = sum dz, dh = dz . WT
+    split_bf16_t(st, net->dz, n, net->KA, net->KA, npad, net->dzt);
+    split_bf16_t(st, net->h1, n, net->CRA, net->CRA, npad, net->ht);
+    tc_store_gemm(st, net->KA, net->CRA, npad, net->dzt, net->ht, net->dwt, net->CRA, net->ctx->d_err);
+    const long nw = (long)net->K * CR * A;
+    head_fold_kernel<<<(unsigned)((nw + PT - 1) / PT), PT, 0, st>>>(net->K, CR, A, net->dwt, net->grads + net->off[4]);
+    bias_grad_kernel<<<net->K, PT, 0, st>>>(n, net->K, A, net->dz, net->grads + net->off[5]);
     ROME_CHECK_LAUNCH();
+    split_bf16(st, net->dz, n, net->KA, net->KA, net->KAp, net->dzs);
+    tc_store_gemm(st, n, net->CRA, net->KAp, net->dzs, net->wtt, net->dh1, net->CRA, net->ctx->d_err);
+    net->ctx->total_launches += 7;
     const long n1 = (long)n * net->c1 * R * A, n0 = (long)n * net->c0 * R * A;
     relu_mask_kernel<<<(unsigned)((n1 + PT - 1) / PT), PT, 0, st>>>(n1, net->h1, net->dh1);
     pconv_bwd_weight_kernel<<<dim3(net->c1, net->c0), PT, 0, st>>>(n, net->c0, R, A, net->c1, net->h0, net->dh1,
@@ -558,8 +615,6 @@ extern "C" int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec*
                          spec->channels[1] <= 64,
                      "channels");
         ROME_REQUIRE(spec->r_lo >= 0 && spec->r_hi > spec->r_lo, "radius range");
-        ROME_REQUIRE((size_t)spec->channels[1] * spec->n_r * spec->n_theta * sizeof(float) <= 200 * 1024,
-                     "head input too large for shared memory");
         ROME_CUDA(cudaSetDevice(ctx->device));
         auto* net = new RomeProposalNet();
         net->ctx = ctx;
@@ -593,6 +648,13 @@ extern "C" int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec*
         ROME_CUDA(cudaMemset(net->adam_m, 0, sizeof(float) * o));
         ROME_CUDA(cudaMemset(net->adam_v, 0, sizeof(float) * o));
         ROME_CUDA(cudaMalloc(&net->loss_acc, sizeof(double)));
+        net->CRA = net->c1 * net->R * net->A;
+        net->CRAp = (net->CRA + 63) / 64 * 64;
+        net->KA = net->K * net->A;
+        net->KAp = (net->KA + 63) / 64 * 64;
+        ROME_CUDA(cudaMalloc(&net->wt, 4 * (size_t)net->KA * net->CRAp));
+        ROME_CUDA(cudaMalloc(&net->wtt, 4 * (size_t)net->CRA * net->KAp));
+        ROME_CUDA(cudaMalloc(&net->dwt, sizeof(float) * (size_t)net->KA * net->CRA));
         *out = net;
     });
 }
@@ -605,6 +667,8 @@ extern "C" void rome_gpu_proposal_destroy(RomeProposalNet* net) {
         if (p) cudaFree(p);
     if (net->loss_acc) cudaFree(net->loss_acc);
     if (net->idx) cudaFree(net->idx);
+    for (void* p : {net->wt, net->wtt, (void*)net->dwt, net->hs, net->dzs, net->dzt, net->ht})
+        if (p) cudaFree(p);
     delete net;
 }
 
@@ -623,6 +687,7 @@ extern "C" int rome_gpu_proposal_set_params(RomeProposalNet* net, const float* h
     return guarded(net->ctx, [&] {
         ROME_CUDA(cudaSetDevice(net->ctx->device));
         ROME_CUDA(cudaMemcpy(net->params, host, sizeof(float) * net->nparam, cudaMemcpyHostToDevice));
+        net->wt_dirty = true;
         net->adam_t = 0;
         ROME_CUDA(cudaMemset(net->adam_m, 0, sizeof(float) * net->nparam));
         ROME_CUDA(cudaMemset(net->adam_v, 0, sizeof(float) * net->nparam));
@@ -644,6 +709,7 @@ extern "C" int rome_gpu_proposal_loss_grad(RomeProposalNet* net, int n, const fl
         if (grad) ROME_CUDA(cudaMemcpyAsync(grad, net->grads, sizeof(float) * net->nparam, cudaMemcpyDeviceToHost, st));
         if (logits) ROME_CUDA(cudaMemcpyAsync(logits, net->z, sizeof(float) * O * n, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
+        tc_check_error(st, net->ctx->d_err);
     });
 }
 
@@ -687,11 +753,13 @@ extern "C" int rome_gpu_proposal_train(RomeProposalNet* net, int n, const float*
                 adam_kernel<<<(unsigned)((net->nparam + PT - 1) / PT), PT, 0, st>>>(
                     net->nparam, lr, b1, b2, eps, c1, c2, net->grads, net->params, net->adam_m, net->adam_v);
                 ROME_CHECK_LAUNCH();
+                net->wt_dirty = true;
             }
             double l = 0;
             ROME_CUDA(cudaMemcpyAsync(&l, net->loss_acc, sizeof(double), cudaMemcpyDeviceToHost, st));
             // the host reshuffles `perm` next epoch: its copy must be done
             ROME_CUDA(cudaStreamSynchronize(st));
+            tc_check_error(st, net->ctx->d_err);
             if (epoch_loss) epoch_loss[ep] = nb ? l / nb : 0.0;
         }
         cudaFree(dx);
@@ -708,15 +776,13 @@ void proposal_predict_device(RomeProposalNet* net, int n, const float* dfeat, in
     const int O = net->K * net->A;
     const int chunk = 4096;
     net_alloc_batch(net, std::min(n, chunk));
-    const int n2 = 1 << (32 - __builtin_clz((unsigned)(O - 1)));
-    const size_t smem = (sizeof(float) + sizeof(int)) * n2;
-    ROME_CUDA(cudaFuncSetAttribute(topk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     for (int done = 0; done < n;) {
         const int m = std::min(chunk, n - done);
         ROME_CUDA(cudaMemcpyAsync(net->x, dfeat + (long)done * row_x, sizeof(float) * row_x * m,
                                   cudaMemcpyDeviceToDevice, st));
         net_forward(net, m, st);
-        topk_kernel<<<m, PT, smem, st>>>(O, k, net->z, didx + (long)done * k, dprob ? dprob + (long)done * k : nullptr);
+        topk_warp_kernel<<<(m + PT / 32 - 1) / (PT / 32), PT, 0, st>>>(m, O, k, net->z, didx + (long)done * k,
+                                                                       dprob ? dprob + (long)done * k : nullptr);
         ROME_CHECK_LAUNCH();
         done += m;
     }
@@ -747,6 +813,7 @@ extern "C" int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, 
         proposal_features_device(net, P, cur, d, d + P * F, d + 2 * P * F, dx, st);
         ROME_CUDA(cudaMemcpyAsync(x_out, dx, sizeof(float) * row_x * P, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
+        tc_check_error(st, net->ctx->d_err);
     });
 }
 
@@ -764,6 +831,7 @@ extern "C" int rome_gpu_proposal_predict(RomeProposalNet* net, int n, const floa
         ROME_CUDA(cudaMemcpyAsync(idx, di, sizeof(int) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
         if (prob) ROME_CUDA(cudaMemcpyAsync(prob, dp, sizeof(float) * (size_t)n * k, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
+        tc_check_error(st, net->ctx->d_err);
     });
 }
 
@@ -798,10 +866,12 @@ extern "C" int rome_gpu_proposal_propose(RomeProposalNet* net, int P, int cur, c
         proposal_predict_device(net, P, dx, k, di, dp, st);
         expand_proposals_kernel<<<(P + 127) / 128, 128, 0, st>>>(P, k, net->A, di, dp, dprop, dmass);
         ROME_CHECK_LAUNCH();
-        // features, then per chunk of 4096: two convolutions, the head and top-k; then the expansion
-        net->ctx->total_launches += 2 + 4L * ((P + 4095) / 4096);
+        // features and the expansion, and top-k per chunk of 4096 (the network's own launches are counted where
+        // they are made)
+        net->ctx->total_launches += 2 + 1L * ((P + 4095) / 4096);
         ROME_CUDA(cudaMemcpyAsync(proposals, dprop, sizeof(int) * (size_t)P * 2 * k, cudaMemcpyDeviceToHost, st));
         if (mass) ROME_CUDA(cudaMemcpyAsync(mass, dmass, sizeof(float) * P, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
+        tc_check_error(st, net->ctx->d_err);
     });
 }

@@ -165,6 +165,65 @@ def alloc_outputs(p: Map2dPool, checkpoints: bool = False, marginals: bool = Fal
 
 
 DEVICE_FIELDS = ["Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf"]
+# fields with one entry (row) per particle
+PARTICLE_FIELDS = DEVICE_FIELDS + ["highres_Xi2", "old_offsetx", "old_offsety", "group"]
+# outputs with one entry per particle (the rest are sums over the pool)
+PARTICLE_OUTPUTS = ["min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "psi", "xoff",
+                    "yoff", "nr_sign", "cls", "post_class_psi"]
+
+
+def take_pool(p, idx: np.ndarray):
+    """The particles `idx` of a pool, in that order: a Map2dPool, or a
+    StagedPool whose images are gathered on the device (its host image
+    fields become zero-width placeholders: only the device copies are read)."""
+    idx = np.asarray(idx, np.int64)
+    if isinstance(p, StagedPool):
+        import torch
+        base = dataclasses.replace(p.pool)
+        for name in PARTICLE_FIELDS:
+            a = getattr(p.pool, name)
+            setattr(base, name, np.empty((len(idx), 0)) if name in DEVICE_FIELDS else np.ascontiguousarray(a[idx]))
+        if p.pool.proposals is not None:
+            base.proposals = np.ascontiguousarray(p.pool.proposals[idx])
+        ti = torch.from_numpy(idx).to(next(iter(p.dev.values())).device)
+        return StagedPool(base, {name: t.index_select(0, ti) for name, t in p.dev.items()})
+    q = dataclasses.replace(p)
+    for name in PARTICLE_FIELDS:
+        setattr(q, name, np.ascontiguousarray(getattr(p, name)[idx]))
+    if p.proposals is not None:
+        q.proposals = np.ascontiguousarray(p.proposals[idx])
+    return q
+
+
+def concat_pools(pools):
+    """One pool holding the particles of several pools of the same model and
+    sampling, in order (StagedPools: device images concatenated on the device)."""
+    if isinstance(pools[0], StagedPool):
+        import torch
+        base = concat_pools([q.pool for q in pools])
+        return StagedPool(base, {name: torch.cat([q.dev[name] for q in pools]) for name in pools[0].dev})
+    q = dataclasses.replace(pools[0])
+    for name in PARTICLE_FIELDS:
+        setattr(q, name, np.concatenate([getattr(x, name) for x in pools]))
+    if pools[0].proposals is not None:
+        q.proposals = np.concatenate([x.proposals for x in pools])
+    return q
+
+
+def merge_results(parts, n: int) -> Dict[str, np.ndarray]:
+    """Outputs of E-steps over disjoint particle subsets [(idx, result)] of one
+    pool of n particles: per-particle outputs scattered back to pool order,
+    pool sums added."""
+    out: Dict[str, np.ndarray] = {}
+    for idx, r in parts:
+        for name, a in r.items():
+            if name in PARTICLE_OUTPUTS:
+                if name not in out:
+                    out[name] = np.zeros((n,) + a.shape[1:], a.dtype)
+                out[name][idx] = a
+            else:
+                out[name] = out[name] + a if name in out else a.copy()
+    return out
 
 
 @dataclasses.dataclass
@@ -261,6 +320,47 @@ class GpuContext:
             dev[name] = torch.from_numpy(_f64(getattr(p, name))).to(f"cuda:{self.device}")
         torch.cuda.synchronize(self.device)
         return StagedPool(p, dev)
+
+    def stage_pool_async(self, p: Map2dPool, stream):
+        """Start copying the pool's images to the device on a side stream (a
+        torch.cuda.Stream); returns the StagedPool and a torch event to wait
+        on before it is used.  With page-locked host arrays the copy runs
+        while the context computes an earlier pool."""
+        import torch
+        dev = {}
+        with torch.cuda.stream(stream):
+            for name in DEVICE_FIELDS:
+                h = torch.from_numpy(_f64(getattr(p, name)))
+                d = torch.empty(h.shape, dtype=h.dtype, device=f"cuda:{self.device}")
+                # pieces of about 8 MB, so that the context's own small uploads are not held
+                # up behind one long transfer
+                step = max(1, (8 << 20) // max(1, h[0].numel() * h.element_size()))
+                for r0 in range(0, h.shape[0], step):
+                    d[r0:r0 + step].copy_(h[r0:r0 + step], non_blocking=True)
+                dev[name] = d
+            ev = torch.cuda.Event()
+            ev.record(stream)
+        return StagedPool(p, dev), ev
+
+    def staged(self, pools):
+        """Yield the host pools as StagedPools, copying pool k + 1 to the
+        device while the caller works on pool k."""
+        import torch
+        side = torch.cuda.Stream(device=self.device)
+        nxt = self.stage_pool_async(pools[0], side) if len(pools) else None
+        for k in range(len(pools)):
+            cur, ev = nxt
+            if k + 1 < len(pools):
+                nxt = self.stage_pool_async(pools[k + 1], side)
+            ev.synchronize()
+            yield cur
+
+    def map2d_estep_pools(self, pools, run=None):
+        """E-steps of a sequence of host pools with the copy of pool k + 1
+        overlapping the E-step of pool k.  `run(staged_pool)` performs one
+        E-step (default: map2d_estep_pool); returns the list of its results."""
+        run = run or self.map2d_estep_pool
+        return [run(q) for q in self.staged(pools)]
 
     @staticmethod
     def h2d_bytes(p: Map2dPool) -> int:

@@ -15,10 +15,10 @@ from typing import Dict, List, Tuple
 import numpy as np
 
 from . import abi
-from .map2d import GpuContext, Map2dPool, _f64
+from .map2d import PARTICLE_OUTPUTS, GpuContext, Map2dPool, _f64, concat_pools, merge_results, take_pool
 
 __all__ = ["ProposalNet", "param_offsets", "flat_to_dict", "dict_to_flat", "posterior_targets",
-           "expand_proposals", "DEFAULT_CHANNELS"]
+           "expand_proposals", "learned_estep", "learned_estep_pools", "DEFAULT_CHANNELS"]
 
 DEFAULT_CHANNELS = (16, 16)
 _FP = C.POINTER(C.c_float)
@@ -172,3 +172,66 @@ class ProposalNet:
                                                            on_dev, k, abi.iptr(prop), _fptr(mass)))
         del keep
         return prop, mass
+
+
+def learned_estep(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: float = 0.0, marginals: bool = False):
+    """E-step of one pool (Map2dPool or StagedPool) with learned proposals:
+    every particle is searched over the 2k orientations of its top-k network
+    outputs, except those whose top-k outputs hold less than `min_mass` of the
+    network's probability, which are searched exhaustively.  Returns (the
+    E-step outputs in pool order, proposals [P][2k], mass [P], the indices of
+    the exhaustively searched particles)."""
+    props, mass = net.propose(pool, k)
+    n = pool.nr_images
+    low = np.flatnonzero(mass < min_mass)
+    if low.size == 0:
+        return ctx.map2d_estep_pool(pool, marginals=marginals, proposals=props), props, mass, low
+    high = np.flatnonzero(mass >= min_mass)
+    parts = []
+    if high.size:
+        parts.append((high, ctx.map2d_estep_pool(take_pool(pool, high), marginals=marginals, proposals=props[high])))
+    parts.append((low, ctx.map2d_estep_pool(take_pool(pool, low), marginals=marginals)))
+    return merge_results(parts, n), props, mass, low
+
+
+def learned_estep_pools(ctx: GpuContext, net: ProposalNet, pools, k: int, min_mass: float = 0.0,
+                        marginals: bool = False):
+    """learned_estep over several pools of one iteration (any iterable, e.g.
+    GpuContext.staged(host_pools)), with the particles that fall back to the
+    exhaustive search gathered from every pool into a single exhaustive
+    E-step (one call instead of one per pool).  Returns one
+    (outputs, proposals, mass, fallback indices) per pool; the fallback call's
+    pool sums (wsum_*) are added to the first pool's, so the sums over all
+    pools are those of the whole set."""
+    staged, fallback = [], []
+    for pool in pools:
+        props, mass = net.propose(pool, k)
+        low = np.flatnonzero(mass < min_mass)
+        high = np.flatnonzero(mass >= min_mass)
+        parts = []
+        if high.size:
+            sub = pool if low.size == 0 else take_pool(pool, high)
+            parts.append((high, ctx.map2d_estep_pool(sub, marginals=marginals, proposals=props[high])))
+        if low.size:
+            fallback.append(take_pool(pool, low))
+        # the pool itself is not kept: only its fallback particles are
+        staged.append((pool.nr_images, parts, props, mass, low))
+    sums = {}
+    if fallback:
+        r = ctx.map2d_estep_pool(concat_pools(fallback), marginals=marginals)
+        off = 0
+        for _, parts, _, _, low in staged:
+            if low.size:
+                parts.append((low, {name: a[off:off + low.size] for name, a in r.items() if name in PARTICLE_OUTPUTS}))
+                off += low.size
+        sums = {name: a for name, a in r.items() if name not in PARTICLE_OUTPUTS}
+    out = []
+    for q, (n, parts, props, mass, low) in enumerate(staged):
+        res = merge_results(parts, n)
+        for name, a in sums.items():
+            if q == 0:
+                res[name] = res[name] + a if name in res else a.copy()
+            elif name not in res:
+                res[name] = np.zeros_like(a)
+        out.append((res, props, mass, low))
+    return out

@@ -114,3 +114,79 @@ def test_training_gain_and_restricted_search(ctx):
     frac = props.shape[1] / (K * npsi)
     print(f"restricted search over {frac:.3f} of the orientations: pose agreement {agree:.4f}")
     assert agree >= 0.85
+
+
+@pytest.mark.parametrize("offset_range", [2, 4])  # 13 and 49 translations: 32- and 64-wide tiles
+def test_restricted_tensor_core_modes_match_fp32(offset_range):
+    """The tensor-core restricted contraction (w = xw * conj(P) formed in
+    shared memory, contracted with the translation-phase operand) against
+    the FP32 CUDA-core restricted path on the same proposal lists: split
+    BF16 to 2e-5 in min_diff2 and identical poses; plain BF16 to 1e-3 and
+    >= 97% identical poses (BF16 rounding of w and of the phases)."""
+    w = Map2dWorkload(n_particles=300, ori_size=64, n_classes=4, n_blobs=16, psi_step=10, offset_range=offset_range,
+                      offset_step=1, max_shift=3, pixel=2.0, snr=0.05, seed=23)
+    p, proj, r_max, _ = build_map2d(w)
+    J = p.nr_classes * p.nr_psi
+    rng = np.random.default_rng(5)
+    nprop = 40  # not a divisor of the 128-row tile: rows of one particle straddle tiles
+    props = np.sort(np.stack([rng.choice(J, nprop, replace=False) for _ in range(p.nr_images)]), axis=1)
+    props = props.astype(np.int32)
+    out = {}
+    for prec in ("fp32", "bf16x3", "bf16"):
+        with GpuContext(0, prec) as c:
+            c.set_projectors(proj, p.ori_size, r_max)
+            out[prec] = c.map2d_estep_pool(p, proposals=props, marginals=True)
+    ref = out["fp32"]
+    for prec, tol, agree_min in (("bf16x3", 2e-5, 1.0), ("bf16", 1e-3, 0.97)):
+        o = out[prec]
+        assert relerr(o["min_diff2"], ref["min_diff2"]) <= tol, (prec, relerr(o["min_diff2"], ref["min_diff2"]))
+        same = (o["cls"] == ref["cls"]) & (o["psi"] == ref["psi"]) & (o["xoff"] == ref["xoff"]) & (
+            o["yoff"] == ref["yoff"])
+        assert same.mean() >= agree_min, (prec, same.mean())
+        # every reported orientation is one of the particle's proposals
+        # reported psi: the table angle folded into (-180, 180]
+        tab = np.asarray(p.over_psi[-1])[:, 0]
+        ipsi = {(float(v) - 360.0 if v > 180 else float(v)): k for k, v in enumerate(tab)}
+        jbest = (o["cls"] - 1) * p.nr_psi + np.array([ipsi[float(v)] for v in o["psi"]])
+        assert all(jbest[i] in props[i] for i in range(p.nr_images))
+
+
+def test_learned_pools_with_fallback_match_per_pool_calls(ctx):
+    """learned_estep_pools (fallback particles of all pools in one exhaustive
+    call) gives every particle the outputs of learned_estep on its own pool,
+    and the same pool sums in total; with min_mass = 1 every particle is
+    searched exhaustively and the outputs are the exhaustive E-step's."""
+    from rome_b200.map2d import GpuContext as G
+    from rome_b200.proposal import learned_estep, learned_estep_pools
+    w = Map2dWorkload(n_particles=600, ori_size=64, n_classes=4, n_blobs=16, psi_step=10, offset_range=2,
+                      offset_step=1, max_shift=2, pixel=2.0, snr=0.1, seed=31)
+    p, proj, r_max, _ = build_map2d(w)
+    pools = [subset(p, lo, lo + 200) for lo in (0, 200, 400)]
+    with G(0, "bf16") as c:
+        c.set_projectors(proj, p.ori_size, r_max)
+        with ProposalNet(c, p.nr_classes, p.nr_psi // 2, 12, (8, 8), 2.0, 12.0, seed=1) as net:
+            staged = [c.stage_pool(q) for q in pools]
+            masses = np.concatenate([net.propose(q, 6)[1] for q in staged])
+            mixed = float(np.median(masses))  # about half of the particles fall back
+            for mm in (mixed, 1.0):
+                got = learned_estep_pools(c, net, staged, 6, mm)
+                want = [learned_estep(c, net, q, 6, mm) for q in staged]
+                nlow = sum(len(g[3]) for g in got)
+                assert nlow == sum(len(x[3]) for x in want)
+                assert 0 < nlow and (mm == 1.0 or nlow < p.nr_images)
+                for g, x in zip(got, want):
+                    for key in ("cls", "psi", "xoff", "yoff"):
+                        assert np.array_equal(g[0][key], x[0][key]), key
+                    assert relerr(g[0]["sum_weight"], x[0]["sum_weight"]) <= 1e-9
+                tot_g = sum(g[0]["wsum_pdf_class"] for g in got)
+                tot_w = sum(x[0]["wsum_pdf_class"] for x in want)
+                assert relerr(tot_g, tot_w) <= 1e-9
+                if mm == 1.0:
+                    assert nlow == p.nr_images
+                    for g, q in zip(got, staged):
+                        e = c.map2d_estep_pool(q)
+                        assert np.array_equal(g[0]["cls"], e["cls"]) and np.array_equal(g[0]["psi"], e["psi"])
+            # the prefetching iterator yields the same pools
+            hs = [q for q in c.staged(pools)]
+            assert all(np.array_equal(a.dev["Fctf"].cpu().numpy(), b.dev["Fctf"].cpu().numpy())
+                       for a, b in zip(hs, staged))
