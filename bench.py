@@ -161,7 +161,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
-    from rome_b200.map2d import GpuContext
+    from rome_b200.map2d import GpuContext, pin_pool
     from rome_b200.proposal import learned_estep_pools
     from rome_b200.workload import CONFIGS, build_map2d, subset
 
@@ -309,22 +309,6 @@ def run_ours(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
-
-
-def pin_pool(p):
-    """The pool's image arrays copied into page-locked host memory (the
-    end-to-end figure copies them to the device inside the timed region)."""
-    import dataclasses
-
-    import torch
-    from rome_b200.map2d import DEVICE_FIELDS
-    rep = {}
-    for name in DEVICE_FIELDS:
-        a = np.ascontiguousarray(getattr(p, name), np.float64)
-        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = a
-        rep[name] = t.numpy()
-    return dataclasses.replace(p, **rep)
 
 
 def cross_gemm_traffic(args, pool_particles):

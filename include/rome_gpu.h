@@ -343,6 +343,18 @@ int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const d
                                        double* significant_weight, double* nr_significant);
 
 /* ---------------------------------------------------------------------
+ * Host -> device copy of page-locked host memory by a kernel on the given
+ * CUDA stream (0: the context's stream), reading the host buffer through
+ * the unified address space instead of using a copy engine.  No reference
+ * counterpart: callers staging the next pool's images while the current
+ * pool computes use it so that the E-step's own small uploads do not queue
+ * behind the large transfer.  host: page-locked (cudaHostAlloc /
+ * cudaHostRegister), dst: device memory; both 16-byte aligned.  Returns
+ * ROME_ERR_ARG for pageable or unaligned buffers.  Asynchronous.
+ * ------------------------------------------------------------------- */
+int rome_gpu_copy_from_host(RomeGpuCtx* ctx, void* dst, const void* host, size_t bytes, void* stream);
+
+/* ---------------------------------------------------------------------
  * M-step reconstruction of one class from its accumulated backprojector.
  * Replaces MAPModel::reconstruction (src/map_model.cpp:233-241) ->
  * MyBackProjector::reconstruct (src/reconstruct.cpp:1929-2526) with the

@@ -150,7 +150,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_proposal_get_params", "rome_gpu_proposal_set_params", "rome_gpu_proposal_features",
     "rome_gpu_proposal_loss_grad", "rome_gpu_proposal_train", "rome_gpu_proposal_predict",
     "rome_gpu_proposal_propose",
-    "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings",
+    "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
 ]
 
 _LIB = None
@@ -196,6 +196,7 @@ def load_library():
     lib.rome_gpu_proposal_propose.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_int, C.c_int, _IP, _FP]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
+    lib.rome_gpu_copy_from_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]

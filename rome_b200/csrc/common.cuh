@@ -3,6 +3,8 @@
 #pragma once
 
 #include <cuda_runtime.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include <cstdarg>
@@ -153,6 +155,7 @@ struct RomeGpuCtx {
     // scalars): copies from it are asynchronous and do not wait behind the
     // caller's own large transfers on other streams; reset at every entry point
     char* h_arena = nullptr;
+    char* d_arena = nullptr;  // the arena's device (mapped) address
     size_t h_arena_cap = 0, h_arena_used = 0;
     // shift table (cos, sin) from the host's libm, identical to the reference's
     double2* d_shift_tab = nullptr;
@@ -178,20 +181,36 @@ inline void arena_reset(RomeGpuCtx* ctx) {
     ctx->h_arena_used = 0;
 }
 
-// host -> device copy of n elements on the context's stream, staged through
-// the page-locked arena when it has room
+// device-side copy out of the mapped host arena (16-byte body when both ends are aligned, then bytes);
+// static: each translation unit has its own copy
+static __global__ void arena_copy_kernel(const unsigned char* __restrict__ src, unsigned char* __restrict__ dst, size_t n) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x, t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t n16 = (((uintptr_t)src | (uintptr_t)dst) & 15) ? 0 : n / 16;
+    for (size_t q = t0; q < n16; q += stride) ((uint4*)dst)[q] = ((const uint4*)src)[q];
+    for (size_t q = n16 * 16 + t0; q < n; q += stride) dst[q] = src[q];
+}
+
+// host -> device copy of n elements on the context's stream.  Through the
+// page-locked, mapped arena when it has room: the host copies into the arena
+// and a kernel copies it onward, so these small per-call uploads never wait
+// behind large transfers that a caller runs on the copy engines meanwhile
+// (e.g. the next pool's images); otherwise a plain cudaMemcpyAsync.
 template <typename T>
 void stage_copy(RomeGpuCtx* ctx, T* dst, const T* host, size_t n) {
     const size_t bytes = sizeof(T) * n, at = (ctx->h_arena_used + 255) & ~(size_t)255;
-    if (ctx->h_arena && at + bytes <= ctx->h_arena_cap) {
+    if (!n) return;
+    if (ctx->h_arena && ctx->d_arena && at + bytes <= ctx->h_arena_cap) {
         memcpy(ctx->h_arena + at, host, bytes);
         ctx->h_arena_used = at + bytes;
-        host = (const T*)(ctx->h_arena + at);
-    }
-    if (n) {
-        cudaError_t e = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+        const unsigned grid = (unsigned)std::min<size_t>((bytes / 16 + 255) / 256 + 1, 64);
+        arena_copy_kernel<<<grid, 256, 0, ctx->stream>>>((const unsigned char*)(ctx->d_arena + at),
+                                                         (unsigned char*)dst, bytes);
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) fail(ROME_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+        return;
     }
+    cudaError_t e = cudaMemcpyAsync(dst, host, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) fail(ROME_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
 }
 
 // run a function, converting RomeFail into a status and recording the message

@@ -1,4 +1,5 @@
 // Context lifetime, projector upload and backprojector access (C ABI).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -47,7 +48,8 @@ extern "C" int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx*
         ROME_CUDA(cudaMalloc(&ctx->d_err, sizeof(int)));
         ROME_CUDA(cudaMemset(ctx->d_err, 0, sizeof(int)));
         ctx->h_arena_cap = (size_t)16 << 20;
-        ROME_CUDA(cudaHostAlloc((void**)&ctx->h_arena, ctx->h_arena_cap, cudaHostAllocDefault));
+        ROME_CUDA(cudaHostAlloc((void**)&ctx->h_arena, ctx->h_arena_cap, cudaHostAllocMapped));
+        ROME_CUDA(cudaHostGetDevicePointer((void**)&ctx->d_arena, ctx->h_arena, 0));
     });
     if (rc != ROME_OK) {
         fprintf(stderr, "rome_gpu_create: %s\n", ctx->last_error.c_str());
@@ -177,4 +179,44 @@ extern "C" int rome_gpu_reset_timings(RomeGpuCtx* ctx) {
     }
     ctx->total_launches = 0;
     return ROME_OK;
+}
+
+namespace rome {
+namespace {
+// grid-stride 16-byte copy; each thread keeps four loads in flight (host reads over PCIe are latency-bound)
+__global__ void __launch_bounds__(512) copy_from_host_kernel(const uint4* __restrict__ src, uint4* __restrict__ dst,
+                                                             size_t n16) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (; q + 3 * stride < n16; q += 4 * stride) {
+        const uint4 a = src[q], b = src[q + stride], c = src[q + 2 * stride], d = src[q + 3 * stride];
+        dst[q] = a;
+        dst[q + stride] = b;
+        dst[q + 2 * stride] = c;
+        dst[q + 3 * stride] = d;
+    }
+    for (; q < n16; q += stride) dst[q] = src[q];
+}
+}  // namespace
+}  // namespace rome
+
+extern "C" int rome_gpu_copy_from_host(RomeGpuCtx* ctx, void* dst, const void* host, size_t bytes, void* stream) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(dst && host && ((uintptr_t)dst & 15) == 0 && ((uintptr_t)host & 15) == 0 && bytes % 16 == 0,
+                     "copy_from_host: buffers must be 16-byte aligned and the size a multiple of 16");
+        cudaPointerAttributes a{};
+        ROME_CUDA(cudaPointerGetAttributes(&a, host));
+        ROME_REQUIRE(a.type == cudaMemoryTypeHost && a.devicePointer != nullptr,
+                     "copy_from_host: the host buffer is not page-locked and mapped");
+        cudaPointerAttributes b{};
+        ROME_CUDA(cudaPointerGetAttributes(&b, dst));
+        ROME_REQUIRE(b.type == cudaMemoryTypeDevice, "copy_from_host: dst is not device memory");
+        if (bytes == 0) return;
+        cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+        const size_t n16 = bytes / 16;
+        const unsigned grid = (unsigned)std::min<size_t>((n16 + 511) / 512, 128);
+        copy_from_host_kernel<<<grid, 512, 0, st>>>((const uint4*)a.devicePointer, (uint4*)dst, n16);
+        ROME_CHECK_LAUNCH();
+    });
 }

@@ -225,7 +225,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             dAct = upload(ctx, S_ACT, act.data(), act.size());
             dActIdx = upload(ctx, S_ACTIDX, actidx.data(), actidx.size());
             int* dClassOk = ctx->ws[S_JVALID].as<int>((size_t)K + g.J);
-            ROME_CUDA(cudaMemcpyAsync(dClassOk, hclass_ok.data(), sizeof(int) * K, cudaMemcpyHostToDevice, st));
+            stage_copy(ctx, dClassOk, hclass_ok.data(), (size_t)K);
             dJvalid = dClassOk + K;
             int* dMres = upload(ctx, S_MRES, Mresol, (size_t)g.F);
 

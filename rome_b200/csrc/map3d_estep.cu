@@ -448,7 +448,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             stride = std::max(stride, hcnt[i]);
         }
         const int E = hoffp[P];
-        ROME_CUDA(cudaMemcpyAsync(dOffP, hoffp.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, st));
+        stage_copy(ctx, dOffP, hoffp.data(), (size_t)P + 1);
         int4* dFe = ctx->ws[S_FE].as<int4>((size_t)std::max(E, 1));
         int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)P * stride);
         ROME_CUDA(cudaMemsetAsync(dEnt, 0xFF, sizeof(int2) * (size_t)P * stride, st));

@@ -464,7 +464,7 @@ inline SelectResult run_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P
         const int slots = (int)std::min<size_t>(over.size(), 64);
         double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)slots * n2);
         int* dli = ctx->ws[S_LIST].as<int>(over.size());
-        ROME_CUDA(cudaMemcpyAsync(dli, over.data(), sizeof(int) * over.size(), cudaMemcpyHostToDevice, st));
+        stage_copy(ctx, dli, over.data(), over.size());
         for (size_t b = 0; b < over.size(); b += slots) {
             int nb = (int)std::min<size_t>(slots, over.size() - b);
             select_fallback2_kernel<<<nb, SEL2_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dli + b, n2,

@@ -1,0 +1,93 @@
+"""Multi-GPU plumbing for the MAP E-step: one process per GPU, particles
+sharded across ranks with no collective on the data path, and the one real
+exchange step of an EM iteration -- the sum of every rank's weighted sums and
+back-projected class volumes -- as NCCL (or gloo) all-reduces.
+
+Reference counterparts:
+* particle ranges: ``divide_equally`` / ``divide_equally_pool``
+  (src/mpi.cpp:34-61), used by ``setImagesDistribution``
+  (src/map_optimizer_base.h:373-409);
+* per-iteration reduction of the model sums: ``MLModel::reduceData``
+  (src/ml_model.cpp:587-637) and of the back-projectors
+  ``MAPModel::reduceData`` (src/map_model.cpp:604-620).
+"""
+from __future__ import annotations
+
+import math
+from typing import Dict, Tuple
+
+import numpy as np
+
+__all__ = ["divide_equally", "divide_equally_pool", "allreduce_model_sums", "allreduce_backprojectors",
+           "max_over_ranks"]
+
+# the pool sums of one E-step call (rome_b200.map2d.alloc_outputs), added over ranks
+MODEL_SUM_KEYS = ("wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_prior_offsetx_class",
+                  "wsum_prior_offsety_class", "wsum_sigma2_offset", "wsum_sumw_group")
+
+
+def divide_equally(n: int, size: int, rank: int) -> Tuple[int, int]:
+    """Inclusive range [first, last] of rank `rank` when n jobs are split over
+    `size` ranks: the first n % size ranks take one job more
+    (src/mpi.cpp:34-49)."""
+    per, rest = divmod(n, size)
+    if rank < rest:
+        first = rank * (per + 1)
+        return first, first + per
+    first = rank * per + rest
+    return first, first + per - 1
+
+
+def divide_equally_pool(n: int, nr_pool: int, size: int, rank: int) -> Tuple[int, int]:
+    """The same over whole pools of nr_pool particles: inclusive particle
+    range [first, last] of `rank` (src/mpi.cpp:52-61)."""
+    blocks = math.ceil(n / nr_pool)
+    b0, b1 = divide_equally(blocks, size, rank)
+    return b0 * nr_pool, min((b1 + 1) * nr_pool - 1, n - 1)
+
+
+def _allreduce_np(arrays: Dict[str, np.ndarray], device) -> Dict[str, np.ndarray]:
+    """Sum FP64 host arrays over all ranks in one flattened all-reduce."""
+    import torch
+    import torch.distributed as dist
+    keys = sorted(arrays)
+    flat = np.concatenate([np.ascontiguousarray(arrays[k], np.float64).ravel() for k in keys]) if keys else np.zeros(0)
+    t = torch.from_numpy(flat).to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    out, off = {}, 0
+    flat = t.cpu().numpy()
+    for k in keys:
+        a = arrays[k]
+        out[k] = flat[off:off + a.size].reshape(a.shape).copy()
+        off += a.size
+    return out
+
+
+def allreduce_model_sums(sums: Dict[str, np.ndarray], device="cpu") -> Dict[str, np.ndarray]:
+    """The iteration's weighted sums (wsum_*) of this rank, summed over all
+    ranks (every rank gets the total).  Keys other than MODEL_SUM_KEYS pass
+    through unchanged: per-particle outputs stay with their rank."""
+    picked = {k: v for k, v in sums.items() if k in MODEL_SUM_KEYS}
+    out = dict(sums)
+    out.update(_allreduce_np(picked, device))
+    return out
+
+
+def allreduce_backprojectors(ctx, nr_classes: int, device=None):
+    """Sum every class's back-projector (data and weight, FP64) over all
+    ranks in place in each rank's context: get_backprojector -> all-reduce
+    on the rank's GPU (NCCL) -> set_backprojector."""
+    dev = device if device is not None else f"cuda:{ctx.device}"
+    for k in range(nr_classes):
+        data, weight = ctx.get_backprojector(k)
+        red = _allreduce_np({"data": data, "weight": weight}, dev)
+        ctx.set_backprojector(k, red["data"], red["weight"])
+
+
+def max_over_ranks(value: float, device="cpu") -> float:
+    """The maximum of a per-rank scalar (e.g. device time of a step)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())

@@ -172,6 +172,50 @@ PARTICLE_OUTPUTS = ["min_diff2", "sum_weight", "significant_weight", "wsum_norm_
                     "yoff", "nr_sign", "cls", "post_class_psi"]
 
 
+def pin_pool(p: Map2dPool) -> Map2dPool:
+    """The pool with its image arrays copied into page-locked host memory
+    (what GpuContext.staged / stage_pool_async read from)."""
+    import torch
+    rep = {}
+    for name in DEVICE_FIELDS:
+        a = _f64(getattr(p, name))
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        rep[name] = t.numpy()  # keeps the pinned tensor alive
+    return dataclasses.replace(p, **rep)
+
+
+def _device_index(idx: np.ndarray, device):
+    """An int64 index array on the device, copied by a kernel from page-locked
+    memory (rome_gpu_copy_from_host) rather than by a copy engine that may be
+    busy with a large transfer of the next pool."""
+    import torch
+    n = len(idx)
+    npad = n + (n & 1)  # 16-byte multiple
+    h = torch.zeros(npad, dtype=torch.int64, pin_memory=True)
+    h.numpy()[:n] = idx
+    d = torch.empty(npad, dtype=torch.int64, device=device)
+    lib = abi.load_library()
+    ctx = _index_ctx(device)
+    rc = lib.rome_gpu_copy_from_host(ctx.h, C.c_void_p(d.data_ptr()), C.c_void_p(h.data_ptr()), 8 * npad,
+                                     C.c_void_p(torch.cuda.current_stream(device).cuda_stream))
+    if rc != abi.ROME_OK:
+        raise RomeError(rc, lib.rome_gpu_last_error(ctx.h).decode())
+    torch.cuda.current_stream(device).synchronize()  # h is released on return
+    return d[:n]
+
+
+_INDEX_CTX = {}
+
+
+def _index_ctx(device):
+    """A context per device for the small index copies (error reporting only)."""
+    dev = device.index if hasattr(device, "index") and device.index is not None else 0
+    if dev not in _INDEX_CTX:
+        _INDEX_CTX[dev] = GpuContext(dev)
+    return _INDEX_CTX[dev]
+
+
 def take_pool(p, idx: np.ndarray):
     """The particles `idx` of a pool, in that order: a Map2dPool, or a
     StagedPool whose images are gathered on the device (its host image
@@ -185,7 +229,7 @@ def take_pool(p, idx: np.ndarray):
             setattr(base, name, np.empty((len(idx), 0)) if name in DEVICE_FIELDS else np.ascontiguousarray(a[idx]))
         if p.pool.proposals is not None:
             base.proposals = np.ascontiguousarray(p.pool.proposals[idx])
-        ti = torch.from_numpy(idx).to(next(iter(p.dev.values())).device)
+        ti = _device_index(idx, next(iter(p.dev.values())).device)
         return StagedPool(base, {name: t.index_select(0, ti) for name, t in p.dev.items()})
     q = dataclasses.replace(p)
     for name in PARTICLE_FIELDS:
@@ -322,22 +366,15 @@ class GpuContext:
         return StagedPool(p, dev)
 
     def stage_pool_async(self, p: Map2dPool, stream):
-        """Start copying the pool's images to the device on a side stream (a
-        torch.cuda.Stream); returns the StagedPool and a torch event to wait
-        on before it is used.  With page-locked host arrays the copy runs
-        while the context computes an earlier pool."""
+        """Start copying the pool's images (page-locked host arrays) to the
+        device on a side stream (a torch.cuda.Stream); returns the StagedPool
+        and a torch event to wait on before it is used.  The copy runs while
+        the context computes an earlier pool."""
         import torch
         dev = {}
         with torch.cuda.stream(stream):
             for name in DEVICE_FIELDS:
-                h = torch.from_numpy(_f64(getattr(p, name)))
-                d = torch.empty(h.shape, dtype=h.dtype, device=f"cuda:{self.device}")
-                # pieces of about 8 MB, so that the context's own small uploads are not held
-                # up behind one long transfer
-                step = max(1, (8 << 20) // max(1, h[0].numel() * h.element_size()))
-                for r0 in range(0, h.shape[0], step):
-                    d[r0:r0 + step].copy_(h[r0:r0 + step], non_blocking=True)
-                dev[name] = d
+                dev[name] = torch.from_numpy(_f64(getattr(p, name))).to(f"cuda:{self.device}", non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(stream)
         return StagedPool(p, dev), ev
@@ -346,7 +383,11 @@ class GpuContext:
         """Yield the host pools as StagedPools, copying pool k + 1 to the
         device while the caller works on pool k."""
         import torch
-        side = torch.cuda.Stream(device=self.device)
+        # one side stream per context: device blocks the caching allocator
+        # hands out on it are reused by the next call's copies
+        side = getattr(self, "_side", None)
+        if side is None:
+            side = self._side = torch.cuda.Stream(device=self.device)
         nxt = self.stage_pool_async(pools[0], side) if len(pools) else None
         for k in range(len(pools)):
             cur, ev = nxt

@@ -1,0 +1,90 @@
+"""Particle sharding and the per-iteration reduction on world size 2 (gloo,
+CPU): the ranges reproduce the reference's divide_equally /
+divide_equally_pool (src/mpi.cpp:34-61) -- disjoint, covering, sizes within
+one -- and the all-reduce of the model sums gives every rank the total."""
+import multiprocessing as mp
+import os
+
+import numpy as np
+import pytest
+
+from rome_b200.distributed import (MODEL_SUM_KEYS, allreduce_model_sums, divide_equally, divide_equally_pool,
+                                   max_over_ranks)
+
+
+def _ref_divide_equally(n, size, rank):
+    # the reference's integer arithmetic, written out independently
+    jobs = n // size
+    rest = n % size
+    if rank < rest:
+        first = rank * (jobs + 1)
+        last = first + jobs
+    else:
+        first = rank * jobs + rest
+        last = first + jobs - 1
+    return first, last
+
+
+@pytest.mark.parametrize("n", [0, 1, 7, 50, 1000, 20001])
+@pytest.mark.parametrize("size", [1, 2, 3, 8])
+def test_divide_equally_covers_and_balances(n, size):
+    ranges = [divide_equally(n, size, r) for r in range(size)]
+    assert ranges == [_ref_divide_equally(n, size, r) for r in range(size)]
+    got = [x for f, l in ranges for x in range(f, l + 1)]
+    assert got == list(range(n))
+    sizes = [l - f + 1 for f, l in ranges]
+    assert max(sizes) - min(sizes) <= 1
+
+
+@pytest.mark.parametrize("n,pool", [(20000, 2000), (1000, 50), (1001, 50), (7, 3)])
+@pytest.mark.parametrize("size", [1, 2, 4])
+def test_divide_equally_pool_whole_pools(n, pool, size):
+    ranges = [divide_equally_pool(n, pool, size, r) for r in range(size)]
+    got = [x for f, l in ranges for x in range(f, l + 1)]
+    assert got == list(range(n))
+    for f, l in ranges:
+        if l >= f:
+            assert f % pool == 0
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        rng = np.random.default_rng(rank)
+        sums = {k: rng.normal(size=(3, 4) if k == "wsum_sigma2_noise" else (5,)) for k in MODEL_SUM_KEYS}
+        sums["min_diff2"] = np.full(4, float(rank))  # per particle: not reduced
+        out = allreduce_model_sums(sums)
+        m = max_over_ranks(10.0 + rank)
+        q.put((rank, {k: v.tolist() for k, v in out.items()}, m))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_allreduce_model_sums_world2():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 2000
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = dict()
+    for _ in range(2):
+        rank, out, m = q.get(timeout=120)
+        res[rank] = (out, m)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    want = {}
+    for rank in range(2):
+        rng = np.random.default_rng(rank)
+        for k in MODEL_SUM_KEYS:
+            v = rng.normal(size=(3, 4) if k == "wsum_sigma2_noise" else (5,))
+            want[k] = want.get(k, 0) + v
+    for rank in range(2):
+        out, m = res[rank]
+        assert m == 11.0
+        for k in MODEL_SUM_KEYS:
+            np.testing.assert_allclose(np.array(out[k]), want[k], rtol=1e-15, atol=1e-15)
+        assert out["min_diff2"] == [float(rank)] * 4
