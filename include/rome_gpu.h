@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define ROME_GPU_ABI_VERSION 1
+#define ROME_GPU_ABI_VERSION 2
 
 enum RomeStatus {
     ROME_OK = 0,
@@ -75,6 +75,8 @@ enum RomePhase {
     ROME_PHASE_WSUM,          /* updateOtherParams */
     ROME_PHASE_BACKPROJECT,   /* backProjection */
     ROME_PHASE_RECONSTRUCT,   /* MyBackProjector::reconstruct */
+    ROME_PHASE_RESTRICTED,    /* diff2 over each particle's proposed orientations only */
+    ROME_PHASE_PROPOSE,       /* proposal network: features, forward, top-k, expansion */
     ROME_PHASE_COUNT
 };
 
@@ -181,6 +183,12 @@ typedef struct {
      * exhaustive search of the reference. */
     const int* proposals;
     int nr_proposals;
+    /* optional, with inputs_on_device only (no reference counterpart): host
+     * array [P]; particle i's images are row particle_rows[i] of the device
+     * image arrays (a subset of a staged pool without copying it).  The
+     * per-particle host arrays (highres_Xi2, offsets, group, proposals) are
+     * given in the processed order.  NULL: row i. */
+    const int* particle_rows;
 } RomeMap2dPool;
 
 typedef struct {

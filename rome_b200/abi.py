@@ -37,7 +37,10 @@ class RomeGpuConfig(C.Structure):
                 ("profile", C.c_int)]
 
 
-PHASES = ["prep", "project", "shift", "norm_gemm", "cross_gemm", "posterior", "wsum", "backproject", "reconstruct"]
+ABI_VERSION = 2  # ROME_GPU_ABI_VERSION of include/rome_gpu.h
+
+PHASES = ["prep", "project", "shift", "norm_gemm", "cross_gemm", "posterior", "wsum", "backproject", "reconstruct",
+          "restricted", "propose"]
 
 
 class RomeGpuTimings(C.Structure):
@@ -59,7 +62,7 @@ class RomeMap2dPool(C.Structure):
         ("pdf_class", _DP), ("pdf_direction", _DP), ("prior_offsetx_class", _DP), ("prior_offsety_class", _DP),
         ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
         ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
-        ("inputs_on_device", C.c_int), ("proposals", _IP), ("nr_proposals", C.c_int),
+        ("inputs_on_device", C.c_int), ("proposals", _IP), ("nr_proposals", C.c_int), ("particle_rows", _IP),
     ]
 
 
@@ -169,6 +172,10 @@ def load_library():
     if not os.path.exists(path):
         raise RuntimeError(f"{path} is missing: build it with `python -m rome_b200.build` (no CPU fallback exists)")
     lib = C.CDLL(path)
+    lib.rome_gpu_abi_version.restype = C.c_int
+    if lib.rome_gpu_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{path} has ABI version {lib.rome_gpu_abi_version()}, this binding expects {ABI_VERSION}: "
+                           "rebuild it with `python -m rome_b200.build`")
     lib.rome_gpu_create.argtypes = [C.c_int, C.POINTER(RomeGpuConfig), C.POINTER(C.c_void_p)]
     lib.rome_gpu_destroy.argtypes = [C.c_void_p]
     lib.rome_gpu_last_error.argtypes = [C.c_void_p]

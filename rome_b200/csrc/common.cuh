@@ -131,6 +131,7 @@ enum Slot {
     S_TMP0,
     S_TMP1,
     S_TMP2,
+    S_ROWS,       // particle_rows of a subset pool [P] int
     S_COUNT
 };
 
@@ -154,6 +155,10 @@ struct RomeGpuCtx {
     // page-locked arena for the small per-call uploads (tables, per-particle
     // scalars): copies from it are asynchronous and do not wait behind the
     // caller's own large transfers on other streams; reset at every entry point
+    // projections of the last 2D pass-0 call and what they were made from
+    // (reused by the next pool of the same iteration); bumped by set_projectors
+    long proj_version = 0;
+    std::string proj_key;
     char* h_arena = nullptr;
     char* d_arena = nullptr;  // the arena's device (mapped) address
     size_t h_arena_cap = 0, h_arena_used = 0;

@@ -99,6 +99,8 @@ extern "C" int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_clas
         ROME_REQUIRE(pad_size == 2 * (padding_factor * r_max + 1) + 1,
                      "pad_size %d inconsistent with r_max %d (ProjectorBase::initialize)", pad_size, r_max);
         ROME_CUDA(cudaSetDevice(ctx->device));
+        ctx->proj_version++;
+        ctx->proj_key.clear();
         long padF = pad_size / 2 + 1;
         long vox = (ref_dim == 3 ? (long)pad_size : 1L) * pad_size * padF;
         if (ctx->proj) cudaFree(ctx->proj);

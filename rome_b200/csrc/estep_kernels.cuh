@@ -183,19 +183,22 @@ __device__ __forceinline__ double hyp_weight(float d, double mn, double pdir, do
 // (src/exp_model.cpp:1015-1103): window the fine-size image and CTF to the
 // pass size (windowFourierTransform / windowTransform, src/image.h:419-568)
 // and build Minvsigma2 = 1/(sigma2_fudge * sigma2_noise[ires]), 0 at ires <= 0.
+// rows: optional input row of each particle (a subset of a staged pool).
 __global__ void prep_particles_kernel(int P, int cur, int cs, const double* __restrict__ Fr,
                                       const double* __restrict__ Fi, const double* __restrict__ ctf_fine,
                                       const int* __restrict__ Mresol, const double* __restrict__ sigma2,
                                       const int* __restrict__ group, int oriF, double fudge, double2* __restrict__ Fimg,
-                                      double* __restrict__ lctf, double* __restrict__ Minv) {
+                                      double* __restrict__ lctf, double* __restrict__ Minv,
+                                      const int* __restrict__ rows = nullptr) {
     const int i = blockIdx.x;
+    const long ri = rows ? rows[i] : i;
     const int curF = cur / 2 + 1, curF2 = cur * curF, csF = cs / 2 + 1, F = cs * csF;
     const double* s2 = sigma2 + (long)group[i] * oriF;
     for (int n = threadIdx.x; n < F; n += blockDim.x) {
         int oi = n / csF, j = n - oi * csF;
         int ip = oi < csF ? oi : oi - cs;
         int in_i = ip < 0 ? ip + cur : ip;
-        long src = (long)i * curF2 + (long)in_i * curF + j;
+        long src = ri * curF2 + (long)in_i * curF + j;
         long dst = (long)i * F + n;
         Fimg[dst] = make_double2(Fr[src], Fi[src]);
         lctf[dst] = ctf_fine[src];
@@ -467,16 +470,18 @@ __device__ TVal block_reduce_sum(TVal v, TVal* sh) {
 __global__ void bp_prep_kernel(int P, int F, const double* __restrict__ Fnr, const double* __restrict__ Fni,
                                const double* __restrict__ lctf, double* __restrict__ Minv,
                                const double* __restrict__ sigma2, const int* __restrict__ group, int oriF, double fudge,
-                               int do_map, int do_ctf, double2* __restrict__ Fnm, double* __restrict__ Mctf2) {
+                               int do_map, int do_ctf, double2* __restrict__ Fnm, double* __restrict__ Mctf2,
+                               const int* __restrict__ rows = nullptr) {
     const int i = blockIdx.x;
+    const long ri = rows ? rows[i] : i;
     for (int n = threadIdx.x; n < F; n += blockDim.x) {
-        long q = (long)i * F + n;
+        long q = (long)i * F + n, qi = ri * F + n;
         double m = Minv[q];
         if (n == 0) m = 1. / (fudge * sigma2[(long)group[i] * oriF + 0]);
         if (!do_map) m = 1.0;
         double c = do_ctf ? lctf[q] : 1.0;
         double mc = dmul(c, m);
-        Fnm[q] = make_double2(dmul(Fnr[q], mc), dmul(Fni[q], mc));
+        Fnm[q] = make_double2(dmul(Fnr[qi], mc), dmul(Fni[qi], mc));
         Mctf2[q] = dmul(c, mc);
     }
 }

@@ -19,6 +19,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <string>
 
 #include "common.cuh"
 #include "estep_kernels.cuh"
@@ -97,6 +98,12 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         Profiler prof(ctx);
 
         // ---- particle data at the fine size ----
+        const int* dRows = nullptr;  // input row of each particle (subset of a staged pool)
+        if (in->particle_rows) {
+            ROME_REQUIRE(in->inputs_on_device, "particle_rows needs inputs_on_device");
+            for (int i = 0; i < P; i++) ROME_REQUIRE(in->particle_rows[i] >= 0, "negative particle row");
+            dRows = upload(ctx, S_ROWS, in->particle_rows, (size_t)P);
+        }
         const double *dFr, *dFi, *dFnr, *dFni, *dCtf;
         if (in->inputs_on_device) {
             dFr = in->Fimg_real;
@@ -256,7 +263,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             dMinv = ctx->ws[S_MINV].as<double>((size_t)P * g.F);
             prof.begin(ROME_PHASE_PREP);
             prep_particles_kernel<<<P, 256, 0, st>>>(P, cur, cs, dFr, dFi, dCtf, dMres, dSig2, dGroup, oriF,
-                                                      in->sigma2_fudge, dFimg, dLctf, dMinv);
+                                                      in->sigma2_fudge, dFimg, dLctf, dMinv, dRows);
             prof.launched(ROME_PHASE_PREP);
             prof.end(ROME_PHASE_PREP);
 
@@ -274,10 +281,24 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 jvalid_kernel<<<(g.J + 255) / 256, 256, 0, st>>>(g.J, g.nrot, g.nor, dClassOk, dRotSig, dJvalid);
                 prof.launched(ROME_PHASE_PROJECT);
             }
-            project2d_kernel<<<g.J, 256, 0, st>>>(g.J, g.Kact, g.Kp, g.Kq, cs, g.csF, g.my_r_max, ctx->pad_size,
-                                                  ctx->pad_size / 2 + 1, g.nrot, ctx->proj, ctx->vox, dRot, dAct,
-                                                  dJvalid, dProj, dQ, dB, ctx->precision);
-            prof.launched(ROME_PHASE_PROJECT);
+            // the projections depend only on the model and the pass's sampling, not on the
+            // particles: a pass-0 call with the same inputs as the previous one reuses them
+            std::string key;
+            if (ipass == 0) {
+                auto put = [&key](const void* p, size_t n) { key.append((const char*)p, n); };
+                const long hdr[12] = {ctx->proj_version, ctx->ref_dim, cs, g.my_r_max, K, npsi, g.nor, g.J, g.Kact,
+                                      g.Kp, ctx->precision, ctx->padding};
+                put(hdr, sizeof(hdr));
+                put(hclass_ok.data(), sizeof(int) * hclass_ok.size());
+                put(in->over_psi[0], sizeof(double) * (size_t)npsi * g.nor);
+            }
+            if (key.empty() || key != ctx->proj_key) {
+                project2d_kernel<<<g.J, 256, 0, st>>>(g.J, g.Kact, g.Kp, g.Kq, cs, g.csF, g.my_r_max,
+                                                      ctx->pad_size, ctx->pad_size / 2 + 1, g.nrot, ctx->proj,
+                                                      ctx->vox, dRot, dAct, dJvalid, dProj, dQ, dB, ctx->precision);
+                prof.launched(ROME_PHASE_PROJECT);
+                ctx->proj_key = key;  // empty after a later pass: its projections replace pass 0's
+            }
             prof.end(ROME_PHASE_PROJECT);
 
             // ---- shifted images -> A operand, S term ----
@@ -361,7 +382,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 Xrow = (long)nprop * g.T;
                 dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xrow);
                 dim3 grid((nprop + RS_QQ - 1) / RS_QQ, (g.T + RS_TQ - 1) / RS_TQ, P);
-                prof.begin(ROME_PHASE_CROSS_GEMM);
+                prof.begin(ROME_PHASE_RESTRICTED);
                 if (rtc) {
                     restricted_tc_diff2(st, ctx->precision, P, nprop, g.T, g.Kp, dProp, dJvalid, dXw, dW2h, dB, g.J,
                                         dSh, dS, dXi2, Xrow, dDiff2, dRowMin, ctx->d_err);
@@ -381,9 +402,9 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                             dRowMin);
                     ROME_CHECK_LAUNCH();
                 }
-                prof.launched(ROME_PHASE_CROSS_GEMM);
-                prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)P * Xrow * g.Kact);
-                prof.end(ROME_PHASE_CROSS_GEMM);
+                prof.launched(ROME_PHASE_RESTRICTED);
+                prof.add_flops(ROME_PHASE_RESTRICTED, 4.0 * (double)P * Xrow * g.Kact);
+                prof.end(ROME_PHASE_RESTRICTED);
             }
 
             // ---- posterior: min, FP64 weights, sum, argmax, significance ----
@@ -516,7 +537,8 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             double* dMctf2 = dMinv;  // reused in place: becomes ctf^2 * Minvsigma2
             prof.begin(ROME_PHASE_BACKPROJECT);
             bp_prep_kernel<<<P, 256, 0, st>>>(P, g.F, dFnr, dFni, dLctf, dMinv, dSig2, dGroup, oriF,
-                                              in->sigma2_fudge, in->do_map, in->do_ctf_correction, dFnm, dMctf2);
+                                              in->sigma2_fudge, in->do_map, in->do_ctf_correction, dFnm, dMctf2,
+                                              dRows);
             prof.launched(ROME_PHASE_BACKPROJECT);
             // group the significant list by orientation (counting sort)
             int* dCnt = dCounter + 2;

@@ -103,6 +103,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         if (!ctx->proj || ctx->ref_dim != 3) fail(ROME_ERR_STATE, "3D projectors not set (rome_gpu_set_projectors)");
         ROME_CUDA(cudaSetDevice(ctx->device));
         arena_reset(ctx);
+        ctx->proj_key.clear();  // this call reuses the 2D projection slots
         const int P = in->nr_images, K = in->nr_classes, ori = in->ori_size, cur = in->current_size;
         const int ndir = in->nr_dir, npsi = in->nr_psi, ntr = in->nr_trans, G = in->nr_groups, oriF = ori / 2 + 1;
         ROME_REQUIRE(P > 0 && K == ctx->nr_classes && ori == ctx->ori_size, "pool/projector mismatch");

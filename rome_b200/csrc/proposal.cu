@@ -855,6 +855,8 @@ extern "C" int rome_gpu_proposal_propose(RomeProposalNet* net, int P, int cur, c
             dFi = d + P * F;
             dC = d + 2 * P * F;
         }
+        Profiler prof(net->ctx);
+        prof.begin(ROME_PHASE_PROPOSE);
         float* dx = (float*)net->ctx->ws[S_TMP1].get(sizeof(float) * row_x * P);
         char* buf = (char*)net->ctx->ws[S_TMP0].get((sizeof(int) + sizeof(float)) * (size_t)P * k +
                                                     (sizeof(int) * 2 * k + sizeof(float)) * (size_t)P);
@@ -869,9 +871,12 @@ extern "C" int rome_gpu_proposal_propose(RomeProposalNet* net, int P, int cur, c
         // features and the expansion, and top-k per chunk of 4096 (the network's own launches are counted where
         // they are made)
         net->ctx->total_launches += 2 + 1L * ((P + 4095) / 4096);
+        net->ctx->phase_launches[ROME_PHASE_PROPOSE] += 2 + 1L * ((P + 4095) / 4096);
+        prof.end(ROME_PHASE_PROPOSE);
         ROME_CUDA(cudaMemcpyAsync(proposals, dprop, sizeof(int) * (size_t)P * 2 * k, cudaMemcpyDeviceToHost, st));
         if (mass) ROME_CUDA(cudaMemcpyAsync(mass, dmass, sizeof(float) * P, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
+        prof.collect();
         tc_check_error(st, net->ctx->d_err);
     });
 }

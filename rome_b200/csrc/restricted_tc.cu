@@ -38,7 +38,7 @@ namespace {
 
 constexpr int RT_ROWS = 128;                   // (particle, proposal) rows per tile: UMMA M
 constexpr int RT_TMAX = 256;                   // translation columns: UMMA N = TN in {32, 64, 128, 256}
-constexpr int RT_PRODUCERS = 256;              // row = tid % 128, half of the 64-column block = tid / 128
+constexpr int RT_PRODUCERS = 256;              // 8 producer warps: 16-byte chunk = tid % 8, rows tid / 8 + 32 u
 constexpr int RT_THREADS = RT_PRODUCERS + 64;  // + one TMA warp + one MMA warp
 
 template <int NPLANE, int TN>
@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
     uint64_t* bfull = full + L::STAGES;                                // TMA bytes of the translation tile
     uint64_t* empty = bfull + L::STAGES;                               // MMAs done reading the stage
     uint64_t* done = empty + L::STAGES;                                // accumulator complete
-    __shared__ float norm_hi[RT_ROWS];
+    __shared__ float norm_row[RT_ROWS];
     __shared__ uint32_t tmem_slot;
     __shared__ int timed_out;
     volatile int* vto = &timed_out;
@@ -107,20 +107,32 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
     int issued = 0;  // translation tiles the TMA thread requested (for draining after a timeout)
     if (warp < RT_PRODUCERS / 32) {
         // ---------------- producers: w = xw * conj(P) into the swizzled A tile ----------------
-        const int rl = tid & (RT_ROWS - 1), half = tid / RT_ROWS;
-        const long r = m0 + rl;
-        const bool valid = r < rows;
-        int i = 0, j = 0;
-        if (valid) {
-            i = (int)(r / nprop);
-            j = prop[r];
-        }
+        // thread -> (16-byte chunk cc of the 128-byte K-block row, rows rsub + 32 u): the eight
+        // threads of a row read its 128 contiguous bytes of P, a warp four whole rows per step
+        const int cc = tid & 7, rsub = tid >> 3;
         const int Kh = Kp / 2;
-        const uint4* b0 = (const uint4*)(B + (long)j * Kp);
-        const uint4* b1 = (const uint4*)(B + (Jrows + j) * (long)Kp);
-        const float4* xr = (const float4*)(xw + (long)i * Kh);
-        const float4* wr = (const float4*)(w2 + (long)i * Kh);
-        float nacc = 0.f;
+        constexpr int NU = RT_ROWS / (RT_PRODUCERS / 8);  // rows per thread (4)
+        const uint4* b0[NU];
+        const uint4* b1[NU];
+        const float4* xr[NU];
+        const float4* wr[NU];
+        bool vrow[NU];
+        float nacc[NU];
+#pragma unroll
+        for (int u = 0; u < NU; u++) {
+            const long r = m0 + rsub + 32 * u;
+            vrow[u] = r < rows;
+            int i = 0, j = 0;
+            if (vrow[u]) {
+                i = (int)(r / nprop);
+                j = prop[r];
+            }
+            b0[u] = (const uint4*)(B + (long)j * Kp);
+            b1[u] = (const uint4*)(B + (Jrows + j) * (long)Kp);
+            xr[u] = (const float4*)(xw + (long)i * Kh);
+            wr[u] = (const float4*)(w2 + (long)i * Kh);
+            nacc[u] = 0.f;
+        }
         for (int kb = 0; kb < nk; kb++) {
             const int s = kb % L::STAGES;
             if (kb >= L::STAGES && !mbar_wait(&empty[s], ((kb / L::STAGES) + 1) & 1)) {
@@ -129,26 +141,26 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
             }
             if (*vto) break;
             uint8_t* st = smem + s * L::STAGE_BYTES;
+            const int px = kb * 32 + cc * 4;  // first of the chunk's 4 complex pixels
 #pragma unroll
-            for (int cc = 0; cc < 4; cc++) {
-                const int c = half * 4 + cc;    // 16-byte chunk of the 128-byte row = 4 complex pixels
-                const int px = kb * 32 + c * 4;  // first pixel of the chunk
+            for (int u = 0; u < NU; u++) {
+                const int rl = rsub + 32 * u;
                 uint4 hv = make_uint4(0u, 0u, 0u, 0u), lv = make_uint4(0u, 0u, 0u, 0u);
                 float4 xa = make_float4(0.f, 0.f, 0.f, 0.f), xb = xa, wv = xa;
-                if (valid) {
-                    hv = __ldg(b0 + px / 4);
-                    if (NPLANE == 2) lv = __ldg(b1 + px / 4);
-                    xa = __ldg(xr + px / 2);
-                    xb = __ldg(xr + px / 2 + 1);
-                    wv = __ldg(wr + px / 4);
+                if (vrow[u]) {
+                    hv = __ldg(b0[u] + px / 4);
+                    if (NPLANE == 2) lv = __ldg(b1[u] + px / 4);
+                    xa = __ldg(xr[u] + px / 2);
+                    xb = __ldg(xr[u] + px / 2 + 1);
+                    wv = __ldg(wr[u] + px / 4);
                 }
                 float2 p[4] = {bf2_to_f2(hv.x), bf2_to_f2(hv.y), bf2_to_f2(hv.z), bf2_to_f2(hv.w)};
                 if (NPLANE == 2) {
                     const float2 l[4] = {bf2_to_f2(lv.x), bf2_to_f2(lv.y), bf2_to_f2(lv.z), bf2_to_f2(lv.w)};
 #pragma unroll
-                    for (int u = 0; u < 4; u++) {
-                        p[u].x += l[u].x;
-                        p[u].y += l[u].y;
+                    for (int e = 0; e < 4; e++) {
+                        p[e].x += l[e].x;
+                        p[e].y += l[e].y;
                     }
                 }
                 const float2 x[4] = {make_float2(xa.x, xa.y), make_float2(xa.z, xa.w), make_float2(xb.x, xb.y),
@@ -156,34 +168,49 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
                 const float wq[4] = {wv.x, wv.y, wv.z, wv.w};
                 uint32_t hi[4], lo[4];
 #pragma unroll
-                for (int u = 0; u < 4; u++) {
-                    const float re = fmaf(x[u].x, p[u].x, x[u].y * p[u].y);
-                    const float im = fmaf(x[u].y, p[u].x, -(x[u].x * p[u].y));
-                    nacc = fmaf(wq[u], fmaf(p[u].x, p[u].x, p[u].y * p[u].y), nacc);
-                    hi[u] = f2_to_bf2(re, im);
+                for (int e = 0; e < 4; e++) {
+                    const float re = fmaf(x[e].x, p[e].x, x[e].y * p[e].y);
+                    const float im = fmaf(x[e].y, p[e].x, -(x[e].x * p[e].y));
+                    nacc[u] = fmaf(wq[e], fmaf(p[e].x, p[e].x, p[e].y * p[e].y), nacc[u]);
+                    hi[e] = f2_to_bf2(re, im);
                     if (NPLANE == 2) {
-                        const float2 hf = bf2_to_f2(hi[u]);
-                        lo[u] = f2_to_bf2(re - hf.x, im - hf.y);
+                        const float2 hf = bf2_to_f2(hi[e]);
+                        lo[e] = f2_to_bf2(re - hf.x, im - hf.y);
                     }
                 }
-                // row rl of the tile at rl * 128 bytes; 16-byte chunk c stored at c ^ (rl % 8)
-                const uint32_t off = (uint32_t)rl * 128u + ((uint32_t)(c ^ (rl & 7)) << 4);
+                // row rl of the tile at rl * 128 bytes; 16-byte chunk cc stored at cc ^ (rl % 8)
+                const uint32_t off = (uint32_t)rl * 128u + ((uint32_t)(cc ^ (rl & 7)) << 4);
                 *(uint4*)(st + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 if (NPLANE == 2) *(uint4*)(st + L::A_BYTES + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
             }
             fence_async_smem();
             mbar_arrive(&full[s]);
         }
-        // the two halves of each row's norm term
-        if (half == 1) norm_hi[rl] = nacc;
+        // each row's norm term: the sum over its eight chunk threads (consecutive lanes)
+#pragma unroll
+        for (int u = 0; u < NU; u++) {
+            float v = nacc[u];
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+            v += __shfl_xor_sync(0xffffffffu, v, 2);
+            v += __shfl_xor_sync(0xffffffffu, v, 4);
+            if (cc == 0) norm_row[rsub + 32 * u] = v;
+        }
         asm volatile("bar.sync 1, %0;" ::"n"(RT_PRODUCERS) : "memory");
 
-        // ---------------- epilogue (warps 0-3: TMEM lanes 32 w .. 32 w + 31) ----------------
+        // ---------------- epilogue (warps 0-3: TMEM lanes 32 w .. 32 w + 31 = rows) ----------------
         if (!mbar_wait(done, 0)) *vto = 1;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const int bad = __shfl_sync(0xffffffffu, *vto, 0);
-        if (half == 0 && !bad) {
-            nacc += norm_hi[rl];
+        if (warp < 4 && !bad) {
+            const int rl = tid;  // 0..127
+            const long r = m0 + rl;
+            const bool valid = r < rows;
+            int i = 0, j = 0;
+            if (valid) {
+                i = (int)(r / nprop);
+                j = prop[r];
+            }
+            const float nrm = norm_row[rl];
             const uint32_t tb = tmem + ((uint32_t)(warp * 32) << 16);
             float m = INFINITY;
             int q = 0;
@@ -206,7 +233,7 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
                     for (int u = 0; u < 32; u++) {
                         if (t0 + u < T) {
                             const float d =
-                                jv ? (float)(0.5 * ((double)nacc - 2.0 * (double)v[u] + sx)) : INFINITY;
+                                jv ? (float)(0.5 * ((double)nrm - 2.0 * (double)v[u] + sx)) : INFINITY;
                             out[t0 + u] = d;
                             m = fminf(m, d);
                         }

@@ -57,6 +57,8 @@ class Map2dPool:
     iclass_max: int = -1
     # optional restricted search: [P][nr_proposals] orientations (class * nr_psi + psi), ascending
     proposals: Optional[np.ndarray] = None
+    # optional, staged pools only: device image row of each particle (a subset without a copy)
+    particle_rows: Optional[np.ndarray] = None
 
     @property
     def nr_images(self) -> int:
@@ -131,6 +133,8 @@ def pack_pool(p: Map2dPool):
         keep.append(pr)
         s.proposals = abi.iptr(pr)
         s.nr_proposals = int(pr.shape[1])
+    if p.particle_rows is not None:
+        s.particle_rows = i(p.particle_rows)
     return s, keep
 
 
@@ -222,15 +226,16 @@ def take_pool(p, idx: np.ndarray):
     fields become zero-width placeholders: only the device copies are read)."""
     idx = np.asarray(idx, np.int64)
     if isinstance(p, StagedPool):
-        import torch
+        # no copy: the subset reads its rows of the staged images (particle_rows)
         base = dataclasses.replace(p.pool)
         for name in PARTICLE_FIELDS:
             a = getattr(p.pool, name)
             setattr(base, name, np.empty((len(idx), 0)) if name in DEVICE_FIELDS else np.ascontiguousarray(a[idx]))
         if p.pool.proposals is not None:
             base.proposals = np.ascontiguousarray(p.pool.proposals[idx])
-        ti = _device_index(idx, next(iter(p.dev.values())).device)
-        return StagedPool(base, {name: t.index_select(0, ti) for name, t in p.dev.items()})
+        rows = idx if p.pool.particle_rows is None else np.asarray(p.pool.particle_rows)[idx]
+        base.particle_rows = np.ascontiguousarray(rows, np.int32)
+        return StagedPool(base, p.dev)
     q = dataclasses.replace(p)
     for name in PARTICLE_FIELDS:
         setattr(q, name, np.ascontiguousarray(getattr(p, name)[idx]))
@@ -244,8 +249,17 @@ def concat_pools(pools):
     sampling, in order (StagedPools: device images concatenated on the device)."""
     if isinstance(pools[0], StagedPool):
         import torch
-        base = concat_pools([q.pool for q in pools])
-        return StagedPool(base, {name: torch.cat([q.dev[name] for q in pools]) for name in pools[0].dev})
+
+        def rows(q, name):
+            t = q.dev[name]
+            if q.pool.particle_rows is None:
+                return t
+            return t.index_select(0, _device_index(np.asarray(q.pool.particle_rows, np.int64), t.device))
+
+        base = concat_pools([dataclasses.replace(q.pool, particle_rows=None) for q in pools])
+        out = StagedPool(base, {name: torch.cat([rows(q, name) for q in pools]) for name in pools[0].dev})
+        torch.cuda.current_stream(next(iter(out.dev.values())).device).synchronize()
+        return out
     q = dataclasses.replace(pools[0])
     for name in PARTICLE_FIELDS:
         setattr(q, name, np.concatenate([getattr(x, name) for x in pools]))
@@ -349,6 +363,9 @@ class GpuContext:
             base = dataclasses.replace(base, proposals=proposals)
         s, keep = pack_pool(base)
         if isinstance(p, StagedPool):
+            import torch
+            # the library's stream does not wait for torch's: tensors made on it must be complete
+            torch.cuda.current_stream(self.device).synchronize()
             for name, t in p.dev.items():
                 setattr(s, name, C.cast(C.c_void_p(t.data_ptr()), abi._DP))
             s.inputs_on_device = 1

@@ -162,6 +162,10 @@ class ProposalNet:
         mass = np.zeros(P, np.float32)
         keep = None
         if isinstance(p, StagedPool):
+            import torch
+            torch.cuda.current_stream(self.ctx.device).synchronize()
+            if base.particle_rows is not None:
+                raise ValueError("propose takes a whole staged pool, not a particle_rows subset")
             ptrs = [C.c_void_p(p.dev[n].data_ptr()) for n in ("Fimg_real", "Fimg_imag", "Fctf")]
             on_dev = 1
         else:
