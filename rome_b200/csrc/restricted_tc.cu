@@ -38,7 +38,7 @@ namespace {
 
 constexpr int RT_ROWS = 128;                   // (particle, proposal) rows per tile: UMMA M
 constexpr int RT_TMAX = 256;                   // translation columns: UMMA N = TN in {32, 64, 128, 256}
-constexpr int RT_PRODUCERS = 256;              // 8 producer warps: 16-byte chunk = tid % 8, rows tid / 8 + 32 u
+constexpr int RT_PRODUCERS = 256;              // 8 producer warps: 16-byte chunk = tid % 8, rows 4 (tid / 8) + u
 constexpr int RT_THREADS = RT_PRODUCERS + 64;  // + one TMA warp + one MMA warp
 
 template <int NPLANE, int TN>
@@ -107,26 +107,31 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
     int issued = 0;  // translation tiles the TMA thread requested (for draining after a timeout)
     if (warp < RT_PRODUCERS / 32) {
         // ---------------- producers: w = xw * conj(P) into the swizzled A tile ----------------
-        // thread -> (16-byte chunk cc of the 128-byte K-block row, rows rsub + 32 u): the eight
-        // threads of a row read its 128 contiguous bytes of P, a warp four whole rows per step
+        // thread -> (16-byte chunk cc of the 128-byte K-block row, rows 4 rsub + u): the eight
+        // threads of a row read its 128 contiguous bytes of P, a warp four whole rows per
+        // step; a thread's four rows are consecutive, so they usually share the particle
+        // (its image and weights are then loaded once for all four)
         const int cc = tid & 7, rsub = tid >> 3;
         const int Kh = Kp / 2;
         constexpr int NU = RT_ROWS / (RT_PRODUCERS / 8);  // rows per thread (4)
         const uint4* b0[NU];
         const uint4* b1[NU];
+        bool vrow[NU], newi[NU];
+        float nacc[NU];
         const float4* xr[NU];
         const float4* wr[NU];
-        bool vrow[NU];
-        float nacc[NU];
+        int iprev = -1;
 #pragma unroll
         for (int u = 0; u < NU; u++) {
-            const long r = m0 + rsub + 32 * u;
+            const long r = m0 + NU * rsub + u;
             vrow[u] = r < rows;
             int i = 0, j = 0;
             if (vrow[u]) {
                 i = (int)(r / nprop);
                 j = prop[r];
             }
+            newi[u] = u == 0 || i != iprev;
+            iprev = i;
             b0[u] = (const uint4*)(B + (long)j * Kp);
             b1[u] = (const uint4*)(B + (Jrows + j) * (long)Kp);
             xr[u] = (const float4*)(xw + (long)i * Kh);
@@ -142,21 +147,29 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
             if (*vto) break;
             uint8_t* st = smem + s * L::STAGE_BYTES;
             const int px = kb * 32 + cc * 4;  // first of the chunk's 4 complex pixels
+            // all loads of the step first (rows' P chunks, then the particles' image and weights)
+            uint4 hv[NU], lv[NU];
 #pragma unroll
             for (int u = 0; u < NU; u++) {
-                const int rl = rsub + 32 * u;
-                uint4 hv = make_uint4(0u, 0u, 0u, 0u), lv = make_uint4(0u, 0u, 0u, 0u);
-                float4 xa = make_float4(0.f, 0.f, 0.f, 0.f), xb = xa, wv = xa;
-                if (vrow[u]) {
-                    hv = __ldg(b0[u] + px / 4);
-                    if (NPLANE == 2) lv = __ldg(b1[u] + px / 4);
-                    xa = __ldg(xr[u] + px / 2);
-                    xb = __ldg(xr[u] + px / 2 + 1);
-                    wv = __ldg(wr[u] + px / 4);
+                hv[u] = vrow[u] ? __ldg(b0[u] + px / 4) : make_uint4(0u, 0u, 0u, 0u);
+                if (NPLANE == 2) lv[u] = vrow[u] ? __ldg(b1[u] + px / 4) : make_uint4(0u, 0u, 0u, 0u);
+            }
+            float4 xa = make_float4(0.f, 0.f, 0.f, 0.f), xb = xa, wv = xa;
+#pragma unroll
+            for (int u = 0; u < NU; u++) {
+                if (newi[u]) {
+                    if (vrow[u]) {
+                        xa = __ldg(xr[u] + px / 2);
+                        xb = __ldg(xr[u] + px / 2 + 1);
+                        wv = __ldg(wr[u] + px / 4);
+                    } else {
+                        xa = xb = wv = make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
                 }
-                float2 p[4] = {bf2_to_f2(hv.x), bf2_to_f2(hv.y), bf2_to_f2(hv.z), bf2_to_f2(hv.w)};
+                float2 p[4] = {bf2_to_f2(hv[u].x), bf2_to_f2(hv[u].y), bf2_to_f2(hv[u].z), bf2_to_f2(hv[u].w)};
                 if (NPLANE == 2) {
-                    const float2 l[4] = {bf2_to_f2(lv.x), bf2_to_f2(lv.y), bf2_to_f2(lv.z), bf2_to_f2(lv.w)};
+                    const float2 l[4] = {bf2_to_f2(lv[u].x), bf2_to_f2(lv[u].y), bf2_to_f2(lv[u].z),
+                                         bf2_to_f2(lv[u].w)};
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         p[e].x += l[e].x;
@@ -179,6 +192,7 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
                     }
                 }
                 // row rl of the tile at rl * 128 bytes; 16-byte chunk cc stored at cc ^ (rl % 8)
+                const int rl = NU * rsub + u;
                 const uint32_t off = (uint32_t)rl * 128u + ((uint32_t)(cc ^ (rl & 7)) << 4);
                 *(uint4*)(st + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 if (NPLANE == 2) *(uint4*)(st + L::A_BYTES + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
@@ -193,7 +207,7 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
             v += __shfl_xor_sync(0xffffffffu, v, 1);
             v += __shfl_xor_sync(0xffffffffu, v, 2);
             v += __shfl_xor_sync(0xffffffffu, v, 4);
-            if (cc == 0) norm_row[rsub + 32 * u] = v;
+            if (cc == 0) norm_row[NU * rsub + u] = v;
         }
         asm volatile("bar.sync 1, %0;" ::"n"(RT_PRODUCERS) : "memory");
 

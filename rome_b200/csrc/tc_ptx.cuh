@@ -70,6 +70,17 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
         : "memory");
 }
 
+// four rows (r0..r3) of a 2D tensor at column c0 into four consecutive box rows of
+// shared memory (the map's box is one row high); swizzled like a tile load
+__device__ __forceinline__ void tma_gather4(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int r0, int r1,
+                                            int r2, int r3) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, "
+        "%5, %6, %7}], [%2];" ::"r"(smem_u32(dst)),
+        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(c0), "r"(r0), "r"(r1), "r"(r2), "r"(r3)
+        : "memory");
+}
+
 // UMMA shared-memory descriptor, K-major, 128-byte swizzle: 8-row groups of
 // 1024 bytes (SBO = 64 x 16 B), LBO = 16 B, descriptor version 1 (sm_100)
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
