@@ -113,6 +113,13 @@ int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_classes, int or
  * (src/map_model.cpp:604-620) and before MAPModel::reconstruction. */
 int rome_gpu_get_backprojector(RomeGpuCtx* ctx, int iclass, double* data, double* weight);
 int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, const double* weight);
+/* dst's back-projectors (all classes, data and weight) += src's, on the
+ * device; both contexts on the same device with the same projector shape.
+ * clear_src: zero src's afterwards.  For pools of one iteration spread over
+ * several contexts (e.g. one per host thread); the reference's counterpart is
+ * the per-thread replica reduction MAPModel::reduceThreadMap
+ * (src/map_model.cpp:209-231). */
+int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int clear_src);
 
 /* ---------------------------------------------------------------------
  * MAP2D E-step for one pool of particles.

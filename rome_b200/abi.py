@@ -154,6 +154,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_proposal_loss_grad", "rome_gpu_proposal_train", "rome_gpu_proposal_predict",
     "rome_gpu_proposal_propose",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
+    "rome_gpu_add_backprojectors",
 ]
 
 _LIB = None
@@ -204,6 +205,7 @@ def load_library():
                                               C.c_int, C.c_int, _IP, _FP]
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
     lib.rome_gpu_copy_from_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
+    lib.rome_gpu_add_backprojectors.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]

@@ -159,6 +159,37 @@ extern "C" int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const dou
     });
 }
 
+namespace rome {
+namespace {
+__global__ void add_volume_kernel(long n, double* __restrict__ dst, const double* __restrict__ src) {
+    for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+        dst[q] += src[q];
+}
+}  // namespace
+}  // namespace rome
+
+extern "C" int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int clear_src) {
+    if (!dst || !src || dst == src) return ROME_ERR_ARG;
+    return guarded(dst, [&] {
+        if (!dst->bp_data || !src->bp_data) fail(ROME_ERR_STATE, "no projectors/backprojectors set");
+        ROME_REQUIRE(dst->device == src->device, "contexts on different devices (%d, %d)", dst->device, src->device);
+        ROME_REQUIRE(dst->ref_dim == src->ref_dim && dst->nr_classes == src->nr_classes && dst->vox == src->vox,
+                     "back-projector shapes differ");
+        ROME_CUDA(cudaSetDevice(dst->device));
+        ROME_CUDA(cudaStreamSynchronize(src->stream));
+        const long n2 = 2L * dst->vox * dst->nr_classes, n1 = dst->vox * dst->nr_classes;
+        add_volume_kernel<<<1184, 256, 0, dst->stream>>>(n2, (double*)dst->bp_data, (const double*)src->bp_data);
+        add_volume_kernel<<<1184, 256, 0, dst->stream>>>(n1, dst->bp_weight, src->bp_weight);
+        ROME_CHECK_LAUNCH();
+        ROME_CUDA(cudaStreamSynchronize(dst->stream));
+        if (clear_src) {
+            ROME_CUDA(cudaMemsetAsync(src->bp_data, 0, sizeof(double2) * n1, src->stream));
+            ROME_CUDA(cudaMemsetAsync(src->bp_weight, 0, sizeof(double) * n1, src->stream));
+            ROME_CUDA(cudaStreamSynchronize(src->stream));
+        }
+    });
+}
+
 extern "C" int rome_gpu_get_timings(RomeGpuCtx* ctx, RomeGpuTimings* out) {
     if (!ctx || !out) return ROME_ERR_ARG;
     for (int q = 0; q < ROME_PHASE_COUNT; q++) {

@@ -131,15 +131,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 lookup_encode_fn() {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    ROME_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
+    if (!p || q != cudaDriverEntryPointSuccess) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    return (PFN_cuTensorMapEncodeTiled_v12000)p;
+}
+
+// looked up once (a function-local static: initialised once even with several host threads)
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void* p = nullptr;
-        ROME_CUDA(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
-        if (!p || q != cudaDriverEntryPointSuccess) fail(ROME_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-        fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    }
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = lookup_encode_fn();
     return fn;
 }
 

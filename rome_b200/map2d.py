@@ -349,6 +349,10 @@ class GpuContext:
         self._check(self.lib.rome_gpu_get_backprojector(self.h, iclass, abi.dptr(data), abi.dptr(weight)))
         return data, weight
 
+    def add_backprojectors(self, src: "GpuContext", clear: bool = True):
+        """This context's back-projectors += src's (same device), src zeroed when clear."""
+        self._check(self.lib.rome_gpu_add_backprojectors(self.h, src.h, int(clear)))
+
     def set_backprojector(self, iclass: int, data: np.ndarray, weight: np.ndarray):
         self._check(self.lib.rome_gpu_set_backprojector(self.h, iclass, abi.dptr(_f64(data)), abi.dptr(_f64(weight))))
 

@@ -199,38 +199,71 @@ def learned_estep(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: flo
 
 
 def learned_estep_pools(ctx: GpuContext, net: ProposalNet, pools, k: int, min_mass: float = 0.0,
-                        marginals: bool = False):
-    """learned_estep over several pools of one iteration (any iterable, e.g.
-    GpuContext.staged(host_pools)), with the particles that fall back to the
-    exhaustive search gathered from every pool into a single exhaustive
-    E-step (one call instead of one per pool).  Returns one
-    (outputs, proposals, mass, fallback indices) per pool; the fallback call's
-    pool sums (wsum_*) are added to the first pool's, so the sums over all
-    pools are those of the whole set."""
-    staged, fallback = [], []
-    for pool in pools:
-        props, mass = net.propose(pool, k)
-        low = np.flatnonzero(mass < min_mass)
-        high = np.flatnonzero(mass >= min_mass)
-        parts = []
-        if high.size:
-            sub = pool if low.size == 0 else take_pool(pool, high)
-            parts.append((high, ctx.map2d_estep_pool(sub, marginals=marginals, proposals=props[high])))
-        if low.size:
-            fallback.append(take_pool(pool, low))
-        # the pool itself is not kept: only its fallback particles are
-        staged.append((pool.nr_images, parts, props, mass, low))
+                        marginals: bool = False, workers=None):
+    """learned_estep over several pools of one iteration (a list, or any
+    iterable such as GpuContext.staged(host_pools) whose pools are worked on
+    as they arrive), with the particles that fall back to the exhaustive
+    search gathered from every pool into a single exhaustive E-step (one call
+    instead of one per pool, after the pools).
+
+    workers: optional further (GpuContext, ProposalNet) pairs on the same
+    device with the same model; pools are dealt round-robin to one host
+    thread per pair, so that one context's host-side work overlaps another's
+    kernels, and their back-projectors are added into `ctx`'s at the end.
+
+    Returns one (outputs, proposals, mass, fallback indices) per pool; the
+    fallback call's pool sums (wsum_*) are added to the first pool's, so the
+    sums over all pools are those of the whole set."""
+    lanes = [(ctx, net)] + list(workers or [])
+    if len(lanes) == 1:
+        return _learned_stream(lanes, None, pools, k, min_mass, marginals)
+    from concurrent.futures import ThreadPoolExecutor
+    execs = [ThreadPoolExecutor(max_workers=1) for _ in lanes]
+    try:
+        return _learned_stream(lanes, execs, pools, k, min_mass, marginals)
+    finally:
+        for e in execs:
+            e.shutdown(wait=True)
+        for c, _ in lanes[1:]:
+            ctx.add_backprojectors(c, clear=True)
+
+
+def _pool_part(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: float, marginals: bool):
+    """propose + restricted E-step of one pool's confident particles; the rest
+    are returned as a view for the exhaustive fallback."""
+    props, mass = net.propose(pool, k)
+    low = np.flatnonzero(mass < min_mass)
+    high = np.flatnonzero(mass >= min_mass)
+    parts = []
+    if high.size:
+        sub = pool if low.size == 0 else take_pool(pool, high)
+        parts.append((high, ctx.map2d_estep_pool(sub, marginals=marginals, proposals=props[high])))
+    return pool.nr_images, parts, props, mass, low, (take_pool(pool, low) if low.size else None)
+
+
+def _learned_stream(lanes, execs, pools, k, min_mass, marginals):
+    """learned_estep_pools over an iterator of pools (e.g. pools still being
+    copied in): each pool is worked on as it arrives, the exhaustive call for
+    all fallback particles comes last."""
+    ctx = lanes[0][0]
+    if execs is None:
+        staged = [_pool_part(*lanes[0], pool, k, min_mass, marginals) for pool in pools]
+    else:
+        futs = [execs[q % len(lanes)].submit(_pool_part, *lanes[q % len(lanes)], pool, k, min_mass, marginals)
+                for q, pool in enumerate(pools)]
+        staged = [f.result() for f in futs]
+    fallback = [f for *_, f in staged if f is not None]
     sums = {}
     if fallback:
         r = ctx.map2d_estep_pool(concat_pools(fallback), marginals=marginals)
         off = 0
-        for _, parts, _, _, low in staged:
+        for _, parts, _, _, low, _ in staged:
             if low.size:
                 parts.append((low, {name: a[off:off + low.size] for name, a in r.items() if name in PARTICLE_OUTPUTS}))
                 off += low.size
         sums = {name: a for name, a in r.items() if name not in PARTICLE_OUTPUTS}
     out = []
-    for q, (n, parts, props, mass, low) in enumerate(staged):
+    for q, (n, parts, props, mass, low, _) in enumerate(staged):
         res = merge_results(parts, n)
         for name, a in sums.items():
             if q == 0:

@@ -190,3 +190,38 @@ def test_learned_pools_with_fallback_match_per_pool_calls(ctx):
             hs = [q for q in c.staged(pools)]
             assert all(np.array_equal(a.dev["Fctf"].cpu().numpy(), b.dev["Fctf"].cpu().numpy())
                        for a, b in zip(hs, staged))
+
+
+def test_learned_pools_with_two_worker_threads_match_one():
+    """Pools dealt to two host threads (two contexts, two copies of the
+    network) give every particle the same outputs as one thread, and the
+    back-projectors merged into the first context equal one context's."""
+    from rome_b200.map2d import GpuContext as G
+    from rome_b200.proposal import learned_estep_pools
+    w = Map2dWorkload(n_particles=600, ori_size=64, n_classes=4, n_blobs=16, psi_step=10, offset_range=2,
+                      offset_step=1, max_shift=2, pixel=2.0, snr=0.1, seed=37)
+    p, proj, r_max, _ = build_map2d(w)
+    pools = [subset(p, lo, lo + 100) for lo in range(0, 600, 100)]
+    with G(0, "bf16") as c0, G(0, "bf16") as c1, G(0, "bf16") as ref:
+        nets = []
+        for c in (c0, c1, ref):
+            c.set_projectors(proj, p.ori_size, r_max)
+            nets.append(ProposalNet(c, p.nr_classes, p.nr_psi // 2, 12, (8, 8), 2.0, 12.0, seed=2))
+        for n in nets[1:]:
+            n.set_params(nets[0].get_params())
+        mm = float(np.median(nets[2].propose(pools[0], 6)[1]))  # some particles fall back
+        two = learned_estep_pools(c0, nets[0], [c0.stage_pool(q) for q in pools], 6, mm, workers=[(c1, nets[1])])
+        one = learned_estep_pools(ref, nets[2], [ref.stage_pool(q) for q in pools], 6, mm)
+        for a, b in zip(two, one):
+            assert np.array_equal(a[1], b[1]) and np.array_equal(a[3], b[3])
+            for k in ("cls", "psi", "xoff", "yoff"):
+                assert np.array_equal(a[0][k], b[0][k]), k
+            assert relerr(a[0]["sum_weight"], b[0]["sum_weight"]) == 0.0
+        assert relerr(sum(a[0]["wsum_pdf_class"] for a in two), sum(b[0]["wsum_pdf_class"] for b in one)) <= 1e-12
+        for k in range(p.nr_classes):
+            d2, w2 = c0.get_backprojector(k)
+            d1, w1 = ref.get_backprojector(k)
+            assert relerr(d2, d1) <= 1e-12 and relerr(w2, w1) <= 1e-12
+            assert not c1.get_backprojector(k)[1].any()  # cleared after the merge
+        for n in nets:
+            n.close()
