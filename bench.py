@@ -121,19 +121,24 @@ def train_proposals(args, ctx, w, rank):
     K, npsi, cur = tp.nr_classes, tp.nr_psi, tp.current_size
     net = ProposalNet(ctx, K, npsi // 2, 16, (16, 16), 2.0, min(24.0, cur / 2 - 2), seed=3)
     t0 = time.perf_counter()
+    staged = [ctx.stage_pool(subset(tp, lo, min(tp.nr_images, lo + args.pool)))
+              for lo in range(0, tp.nr_images, args.pool)]  # one (pageable) copy to the device
+    t_stage = time.perf_counter() - t0
+    t0 = time.perf_counter()
     xs, ts = [], []
-    for lo in range(0, tp.nr_images, args.pool):
-        q = subset(tp, lo, min(tp.nr_images, lo + args.pool))
+    for q in staged:
         r = ctx.map2d_estep_pool(q, marginals=True)
         ts.append(posterior_targets(r["post_class_psi"], K, npsi))
         xs.append(net.features(q))
     torch.cuda.synchronize()
     t_label = time.perf_counter() - t0
+    del staged
     t0 = time.perf_counter()
     losses = net.train(np.concatenate(xs), np.concatenate(ts), epochs=args.train_epochs, batch=256, lr=3e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
-    info = {"train_particles": int(tp.nr_images), "epochs": args.train_epochs, "label_s": round(t_label, 2),
+    info = {"train_particles": int(tp.nr_images), "epochs": args.train_epochs, "stage_s": round(t_stage, 2),
+            "label_s": round(t_label, 2),
             "train_s": round(t_train, 2), "loss_first": round(float(losses[0]), 4),
             "loss_last": round(float(losses[-1]), 4), "params": int(net.nparam),
             "net": "polar |F| and |CTF| input 16 radii x %d angles, 2 circular 3x3 convs (16, 16), "

@@ -422,9 +422,10 @@ long rome_gpu_proposal_num_params(const RomeProposalNet* net);
 int rome_gpu_proposal_get_params(RomeProposalNet* net, float* params);
 int rome_gpu_proposal_set_params(RomeProposalNet* net, const float* params);
 /* network input of P particles from their masked Fourier images and CTFs
- * at size cur (FFTW half-planes, FP64, host) */
+ * at size cur (FFTW half-planes, FP64; host arrays, or device arrays with
+ * inputs_on_device), written to host memory */
 int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, const double* Fimg_real,
-                               const double* Fimg_imag, const double* ctf, float* x);
+                               const double* Fimg_imag, const double* ctf, int inputs_on_device, float* x);
 /* mean soft-target cross-entropy of n samples, its gradient (flat, as the
  * parameters) and the logits [n][n_classes * n_theta]; outputs may be NULL */
 int rome_gpu_proposal_loss_grad(RomeProposalNet* net, int n, const float* x, const float* targets, double* loss,

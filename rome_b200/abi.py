@@ -196,7 +196,8 @@ def load_library():
     lib.rome_gpu_proposal_num_params.restype = C.c_long
     lib.rome_gpu_proposal_get_params.argtypes = [C.c_void_p, _FP]
     lib.rome_gpu_proposal_set_params.argtypes = [C.c_void_p, _FP]
-    lib.rome_gpu_proposal_features.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP, _DP, _FP]
+    lib.rome_gpu_proposal_features.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                               C.c_int, _FP]
     lib.rome_gpu_proposal_loss_grad.argtypes = [C.c_void_p, C.c_int, _FP, _FP, _DP, _FP, _FP]
     lib.rome_gpu_proposal_train.argtypes = [C.c_void_p, C.c_int, _FP, _FP, C.c_int, C.c_int, C.c_float,
                                             C.c_ulonglong, _DP]

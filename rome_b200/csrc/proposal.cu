@@ -66,6 +66,8 @@ struct RomeProposalNet {
     void* dzs = nullptr;                     // dz [n][KAp] hi, lo
     void* dzt = nullptr;                     // dz^T [KA][npad] hi, lo
     void* ht = nullptr;                      // h1^T [CRA][npad] hi, lo
+    float* wflip = nullptr;                  // conv 2 weights flipped for its input gradient
+    float* wpart = nullptr;                  // per-sample conv weight/bias gradients [n][Co*Ci*9 + Co]
 };
 
 namespace rome {
@@ -116,6 +118,7 @@ size_t pconv_smem_bytes(int Ci, int R, int A, int Co) {
     return sizeof(float) * (xin + (size_t)Ci * 9 * Co);
 }
 
+template <bool RELU>
 __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A, int Co,
                                                              const float* __restrict__ x,
                                                              const float* __restrict__ w,
@@ -136,7 +139,13 @@ __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A
         const int g = item / RA, pos = item - g * RA;
         const int r = pos / A, a = pos - r * A;
         const int am = a == 0 ? A - 1 : a - 1, ap = a == A - 1 ? 0 : a + 1;
-        float acc[4] = {b[4 * g], b[4 * g + 1], b[4 * g + 2], b[4 * g + 3]};
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        if (b) {
+            acc[0] = b[4 * g];
+            acc[1] = b[4 * g + 1];
+            acc[2] = b[4 * g + 2];
+            acc[3] = b[4 * g + 3];
+        }
         for (int ci = 0; ci < Ci; ci++) {
             const float* xc = xs + ci * RA;
             const float4* wc = (const float4*)(ws + (long)ci * 9 * Co) + g;
@@ -157,8 +166,86 @@ __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A
             }
         }
 #pragma unroll
-        for (int c = 0; c < 4; c++) y[(((long)n * Co + 4 * g + c) * R + r) * A + a] = fmaxf(acc[c], 0.f);
+        for (int c = 0; c < 4; c++) y[(((long)n * Co + 4 * g + c) * R + r) * A + a] = RELU ? fmaxf(acc[c], 0.f) : acc[c];
     }
+}
+
+// w'[ci][co][t] = w[co][ci][8 - t]: the input gradient of a 3x3 polar convolution
+// is the same convolution of dy with these weights (channels swapped, taps flipped)
+__global__ void flip_weights_kernel(int Co, int Ci, const float* __restrict__ w, float* __restrict__ wt) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= Co * Ci * 9) return;
+    const int co = q / (Ci * 9), rest = q - co * (Ci * 9), ci = rest / 9, t = rest - ci * 9;
+    wt[((long)ci * Co + co) * 9 + (8 - t)] = w[q];
+}
+
+// Weight and bias gradients of a 3x3 polar convolution, one CTA per sample:
+// the sample's input planes (row stride R*A + 1 against bank conflicts) and
+// output gradients in shared memory; thread -> (co, ci) pair, its 9 taps in
+// registers.  part[n][(co*Ci + ci)*9 + t] and part[n][Co*Ci*9 + co] are the
+// sample's contributions, summed over samples by conv_grad_reduce_kernel in a
+// fixed order (deterministic).
+size_t wgrad_smem_bytes(int Ci, int R, int A, int Co) {
+    return sizeof(float) * ((size_t)Ci * (R * A + 1) + (size_t)Co * R * A);
+}
+
+__global__ void __launch_bounds__(PT) conv_wgrad_sample_kernel(int Ci, int R, int A, int Co,
+                                                                const float* __restrict__ x,
+                                                                const float* __restrict__ dy,
+                                                                float* __restrict__ part) {
+    extern __shared__ float smw[];
+    const int RA = R * A, XS = RA + 1;
+    float* xs = smw;
+    float* gs = smw + (long)Ci * XS;
+    const int n = blockIdx.x;
+    for (int q = threadIdx.x; q < Ci * RA; q += PT) {
+        const int c = q / RA;
+        xs[c * XS + (q - c * RA)] = x[(long)n * Ci * RA + q];
+    }
+    for (int q = threadIdx.x; q < Co * RA; q += PT) gs[q] = dy[(long)n * Co * RA + q];
+    __syncthreads();
+    const long stride = (long)Co * Ci * 9 + Co;
+    for (int pr = threadIdx.x; pr < Co * Ci; pr += PT) {
+        const int co = pr / Ci, ci = pr - co * Ci;
+        const float* xc = xs + ci * XS;
+        const float* gc = gs + co * RA;
+        float acc[9];
+#pragma unroll
+        for (int t = 0; t < 9; t++) acc[t] = 0.f;
+        for (int r = 0; r < R; r++) {
+            for (int a = 0; a < A; a++) {
+                const float g = gc[r * A + a];
+                const int am = a == 0 ? A - 1 : a - 1, ap = a == A - 1 ? 0 : a + 1;
+#pragma unroll
+                for (int kh = 0; kh < 3; kh++) {
+                    const int rr = r + kh - 1;
+                    if (rr < 0 || rr >= R) continue;
+                    const float* row = xc + rr * A;
+                    acc[kh * 3 + 0] = fmaf(g, row[am], acc[kh * 3 + 0]);
+                    acc[kh * 3 + 1] = fmaf(g, row[a], acc[kh * 3 + 1]);
+                    acc[kh * 3 + 2] = fmaf(g, row[ap], acc[kh * 3 + 2]);
+                }
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 9; t++) part[n * stride + (long)pr * 9 + t] = acc[t];
+    }
+    for (int co = threadIdx.x; co < Co; co += PT) {
+        float sacc = 0.f;
+        for (int q = 0; q < RA; q++) sacc += gs[co * RA + q];
+        part[n * stride + (long)Co * Ci * 9 + co] = sacc;
+    }
+}
+
+// out[j] = sum_n part[n][j] (n ascending), j < Co*Ci*9 -> dw, then Co biases -> db
+__global__ void conv_grad_reduce_kernel(int N, int nw, int nb, const float* __restrict__ part, float* __restrict__ dw,
+                                        float* __restrict__ db) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nw + nb) return;
+    float s = 0.f;
+    for (int n = 0; n < N; n++) s += part[(long)n * (nw + nb) + j];
+    if (j < nw) dw[j] = s;
+    else db[j - nw] = s;
 }
 
 // dy <- dy * (y > 0): the ReLU's gradient, in place
@@ -517,6 +604,9 @@ void net_alloc_batch(RomeProposalNet* net, int n) {
     ROME_CUDA(cudaMalloc(&net->ht, 4 * (size_t)net->CRA * npad));
     if (net->idx) cudaFree(net->idx);
     ROME_CUDA(cudaMalloc(&net->idx, sizeof(int) * n));
+    if (net->wpart) cudaFree(net->wpart);
+    const size_t per = std::max((size_t)net->c1 * net->c0 * 9 + net->c1, (size_t)net->c0 * 2 * 9 + net->c0);
+    ROME_CUDA(cudaMalloc(&net->wpart, sizeof(float) * per * n));
     net->cap_n = n;
 }
 
@@ -542,8 +632,9 @@ void conv_forward(int Ci, int R, int A, int Co, int n, const float* x, const flo
                   cudaStream_t st) {
     const size_t sm = pconv_smem_bytes(Ci, R, A, Co);
     if (Co % 4 == 0 && sm <= 96 * 1024) {
-        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        pconv_fwd_smem_kernel<<<n, PT, sm, st>>>(Ci, R, A, Co, x, w, b, y);
+        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sm));
+        pconv_fwd_smem_kernel<true><<<n, PT, sm, st>>>(Ci, R, A, Co, x, w, b, y);
     } else {
         dim3 g((R * A + PT - 1) / PT, Co, n);
         pconv_fwd_kernel<<<g, PT, sizeof(float) * Ci * 9, st>>>(Ci, R, A, Co, x, w, b, y);
@@ -563,6 +654,23 @@ void net_forward(RomeProposalNet* net, int n, cudaStream_t st) {
     net->ctx->total_launches += 4;
 }
 
+// weight and bias gradients of one convolution (Ci -> Co) over n samples
+void conv_weight_grads(RomeProposalNet* net, int n, int Ci, int Co, const float* x, const float* dy, float* dw,
+                       float* db, cudaStream_t st) {
+    const int R = net->R, A = net->A;
+    const size_t sm = wgrad_smem_bytes(Ci, R, A, Co);
+    if (sm <= 200 * 1024) {
+        const int nw = Co * Ci * 9, nb = Co;
+        ROME_CUDA(cudaFuncSetAttribute(conv_wgrad_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        conv_wgrad_sample_kernel<<<n, PT, sm, st>>>(Ci, R, A, Co, x, dy, net->wpart);
+        conv_grad_reduce_kernel<<<(nw + nb + PT - 1) / PT, PT, 0, st>>>(n, nw, nb, net->wpart, dw, db);
+    } else {
+        pconv_bwd_weight_kernel<<<dim3(Co, Ci), PT, 0, st>>>(n, Ci, R, A, Co, x, dy, dw);
+        bias_grad_kernel<<<Co, PT, 0, st>>>(n, Co, R * A, dy, db);
+    }
+    ROME_CHECK_LAUNCH();
+}
+
 // gradients of the mean loss into net->grads (dz holds dL/dz)
 void net_backward(RomeProposalNet* net, int n, cudaStream_t st) {
     const int R = net->R, A = net->A, CR = net->c1 * R;
@@ -580,15 +688,24 @@ void net_backward(RomeProposalNet* net, int n, cudaStream_t st) {
     net->ctx->total_launches += 7;
     const long n1 = (long)n * net->c1 * R * A, n0 = (long)n * net->c0 * R * A;
     relu_mask_kernel<<<(unsigned)((n1 + PT - 1) / PT), PT, 0, st>>>(n1, net->h1, net->dh1);
-    pconv_bwd_weight_kernel<<<dim3(net->c1, net->c0), PT, 0, st>>>(n, net->c0, R, A, net->c1, net->h0, net->dh1,
-                                                                   net->grads + net->off[2]);
-    bias_grad_kernel<<<net->c1, PT, 0, st>>>(n, net->c1, R * A, net->dh1, net->grads + net->off[3]);
-    dim3 g0((R * A + PT - 1) / PT, net->c0, n);
-    pconv_bwd_data_kernel<<<g0, PT, 0, st>>>(net->c0, R, A, net->c1, net->dh1, net->params + net->off[2], net->dh0);
+    conv_weight_grads(net, n, net->c0, net->c1, net->h0, net->dh1, net->grads + net->off[2], net->grads + net->off[3],
+                      st);
+    // input gradient of conv 2 = conv of dh1 with the flipped, transposed weights
+    const size_t smd = pconv_smem_bytes(net->c1, R, A, net->c0);
+    if (net->c0 % 4 == 0 && smd <= 96 * 1024) {
+        flip_weights_kernel<<<(net->c1 * net->c0 * 9 + PT - 1) / PT, PT, 0, st>>>(net->c1, net->c0,
+                                                                              net->params + net->off[2], net->wflip);
+        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smd));
+        pconv_fwd_smem_kernel<false><<<n, PT, smd, st>>>(net->c1, R, A, net->c0, net->dh1, net->wflip, nullptr,
+                                                         net->dh0);
+    } else {
+        dim3 g0((R * A + PT - 1) / PT, net->c0, n);
+        pconv_bwd_data_kernel<<<g0, PT, 0, st>>>(net->c0, R, A, net->c1, net->dh1, net->params + net->off[2],
+                                                 net->dh0);
+    }
     relu_mask_kernel<<<(unsigned)((n0 + PT - 1) / PT), PT, 0, st>>>(n0, net->h0, net->dh0);
-    pconv_bwd_weight_kernel<<<dim3(net->c0, 2), PT, 0, st>>>(n, 2, R, A, net->c0, net->x, net->dh0,
-                                                             net->grads + net->off[0]);
-    bias_grad_kernel<<<net->c0, PT, 0, st>>>(n, net->c0, R * A, net->dh0, net->grads + net->off[1]);
+    conv_weight_grads(net, n, 2, net->c0, net->x, net->dh0, net->grads + net->off[0], net->grads + net->off[1], st);
     ROME_CHECK_LAUNCH();
 }
 
@@ -655,6 +772,7 @@ extern "C" int rome_gpu_proposal_create(RomeGpuCtx* ctx, const RomeProposalSpec*
         ROME_CUDA(cudaMalloc(&net->wt, 4 * (size_t)net->KA * net->CRAp));
         ROME_CUDA(cudaMalloc(&net->wtt, 4 * (size_t)net->CRA * net->KAp));
         ROME_CUDA(cudaMalloc(&net->dwt, sizeof(float) * (size_t)net->KA * net->CRA));
+        ROME_CUDA(cudaMalloc(&net->wflip, sizeof(float) * (size_t)net->c1 * net->c0 * 9));
         *out = net;
     });
 }
@@ -667,7 +785,8 @@ extern "C" void rome_gpu_proposal_destroy(RomeProposalNet* net) {
         if (p) cudaFree(p);
     if (net->loss_acc) cudaFree(net->loss_acc);
     if (net->idx) cudaFree(net->idx);
-    for (void* p : {net->wt, net->wtt, (void*)net->dwt, net->hs, net->dzs, net->dzt, net->ht})
+    for (void* p : {net->wt, net->wtt, (void*)net->dwt, net->hs, net->dzs, net->dzt, net->ht, (void*)net->wflip,
+                    (void*)net->wpart})
         if (p) cudaFree(p);
     delete net;
 }
@@ -798,19 +917,25 @@ void proposal_features_device(RomeProposalNet* net, int P, int cur, const double
 }  // namespace rome
 
 extern "C" int rome_gpu_proposal_features(RomeProposalNet* net, int P, int cur, const double* Fr, const double* Fi,
-                                          const double* ctf, float* x_out) {
+                                          const double* ctf, int inputs_on_device, float* x_out) {
     if (!net || P <= 0 || !Fr || !Fi || !ctf || !x_out) return ROME_ERR_ARG;
     return guarded(net->ctx, [&] {
         ROME_CUDA(cudaSetDevice(net->ctx->device));
         cudaStream_t st = net->ctx->stream;
         const long F = (long)cur * (cur / 2 + 1);
         const long row_x = 2L * net->R * net->A;
-        double* d = net->ctx->ws[S_TMP2].as<double>((size_t)3 * P * F);
         float* dx = (float*)net->ctx->ws[S_TMP1].get(sizeof(float) * row_x * P);
-        ROME_CUDA(cudaMemcpyAsync(d, Fr, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
-        ROME_CUDA(cudaMemcpyAsync(d + P * F, Fi, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
-        ROME_CUDA(cudaMemcpyAsync(d + 2 * P * F, ctf, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
-        proposal_features_device(net, P, cur, d, d + P * F, d + 2 * P * F, dx, st);
+        const double *dFr = Fr, *dFi = Fi, *dC = ctf;
+        if (!inputs_on_device) {
+            double* d = net->ctx->ws[S_TMP2].as<double>((size_t)3 * P * F);
+            ROME_CUDA(cudaMemcpyAsync(d, Fr, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(d + P * F, Fi, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(d + 2 * P * F, ctf, sizeof(double) * P * F, cudaMemcpyHostToDevice, st));
+            dFr = d;
+            dFi = d + P * F;
+            dC = d + 2 * P * F;
+        }
+        proposal_features_device(net, P, cur, dFr, dFi, dC, dx, st);
         ROME_CUDA(cudaMemcpyAsync(x_out, dx, sizeof(float) * row_x * P, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
         tc_check_error(st, net->ctx->d_err);

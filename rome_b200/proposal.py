@@ -116,11 +116,26 @@ class ProposalNet:
         assert flat.size == self.nparam
         self.ctx._check(self.lib.rome_gpu_proposal_set_params(self.h, _fptr(flat)))
 
-    def features(self, p: Map2dPool) -> np.ndarray:
-        x = np.zeros((p.nr_images, 2, self.n_r, self.n_theta), np.float32)
-        fr, fi, ct = _f64(p.Fimg_real), _f64(p.Fimg_imag), _f64(p.Fctf)
-        self.ctx._check(self.lib.rome_gpu_proposal_features(self.h, p.nr_images, p.current_size, abi.dptr(fr),
-                                                            abi.dptr(fi), abi.dptr(ct), _fptr(x)))
+    def features(self, p) -> np.ndarray:
+        """Network input [P][2][n_r][n_theta] of a pool (Map2dPool, or a whole
+        StagedPool whose images live on the device)."""
+        from .map2d import StagedPool
+        base = p.pool if isinstance(p, StagedPool) else p
+        x = np.zeros((base.nr_images, 2, self.n_r, self.n_theta), np.float32)
+        if isinstance(p, StagedPool):
+            import torch
+            torch.cuda.current_stream(self.ctx.device).synchronize()
+            if base.particle_rows is not None:
+                raise ValueError("features takes a whole staged pool, not a particle_rows subset")
+            ptrs = [C.c_void_p(p.dev[n].data_ptr()) for n in ("Fimg_real", "Fimg_imag", "Fctf")]
+            keep, on_dev = None, 1
+        else:
+            keep = [_f64(base.Fimg_real), _f64(base.Fimg_imag), _f64(base.Fctf)]
+            ptrs = [C.c_void_p(a.ctypes.data) for a in keep]
+            on_dev = 0
+        self.ctx._check(self.lib.rome_gpu_proposal_features(self.h, base.nr_images, base.current_size, ptrs[0],
+                                                            ptrs[1], ptrs[2], on_dev, _fptr(x)))
+        del keep
         return x
 
     def loss_grad(self, x: np.ndarray, t: np.ndarray):

@@ -57,6 +57,7 @@ def test_features_match_oracle(ctx):
     p, _, _, _ = build_map2d(w)
     with ProposalNet(ctx, 3, 9, 16, r_lo=2.0, r_hi=24.0) as net:
         x = net.features(p)
+        assert np.array_equal(net.features(ctx.stage_pool(p)), x)  # device inputs: the same kernel
     r = po.features(p.Fimg_real, p.Fimg_imag, p.Fctf, p.current_size, 16, 9, 2.0, 24.0)
     assert np.max(np.abs(x - r)) <= 1e-4
 
