@@ -290,6 +290,14 @@ typedef struct {
     int do_scale_correction;         /* must be 0 */
     int do_cross_correlation;        /* must be 0 */
     int inputs_on_device;
+    /* optional coarse-pass search restriction (no reference counterpart): per
+     * particle nr_proposals coarse orientations j = (class * nr_dir + dir) *
+     * nr_psi + psi, ascending and distinct (host array [P][nr_proposals]);
+     * the coarse pass evaluates only those, with every translation, and the
+     * fine pass refines the coarse-significant points among them as usual.
+     * NULL: the exhaustive coarse pass of the reference. */
+    const int* proposals;
+    int nr_proposals;
 } RomeMap3dPool;
 
 typedef struct {
@@ -326,6 +334,10 @@ typedef struct {
     long* fine_index;
     double* fine_diff2;
     double* fine_weight;
+    /* optional (no reference counterpart): the coarse pass's significant
+     * normalised weights summed per coarse orientation, [P][K * nr_dir * nr_psi]
+     * (training targets of the proposal network) */
+    double* post_coarse;
 } RomeMap3dPoolOut;
 
 int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* in, RomeMap3dPoolOut* out);

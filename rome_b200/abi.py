@@ -91,6 +91,7 @@ class RomeMap3dPool(C.Structure):
         ("sigma2_offset", C.c_double), ("sigma2_fudge", C.c_double), ("adaptive_fraction", C.c_double),
         ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
         ("do_scale_correction", C.c_int), ("do_cross_correlation", C.c_int), ("inputs_on_device", C.c_int),
+        ("proposals", _IP), ("nr_proposals", C.c_int),
     ]
 
 
@@ -104,7 +105,7 @@ class RomeMap3dPoolOut(C.Structure):
         ("pass_min_diff2", _DP * 2), ("pass_sum_weight", _DP * 2), ("pass_significant_weight", _DP * 2),
         ("coarse_diff2", _DP), ("Mcoarse_significant", _CP),
         ("fine_capacity", C.c_long), ("fine_count", _IP), ("fine_index", C.POINTER(C.c_long)),
-        ("fine_diff2", _DP), ("fine_weight", _DP),
+        ("fine_diff2", _DP), ("fine_weight", _DP), ("post_coarse", _DP),
     ]
 
 

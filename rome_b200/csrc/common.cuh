@@ -132,6 +132,7 @@ enum Slot {
     S_TMP1,
     S_TMP2,
     S_ROWS,       // particle_rows of a subset pool [P] int
+    S_PROP,       // proposals of a restricted search [P][nprop] int
     S_COUNT
 };
 

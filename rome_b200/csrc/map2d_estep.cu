@@ -191,7 +191,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                     ROME_REQUIRE(q == 0 || j > in->proposals[(size_t)i * nprop + q - 1],
                                  "proposals of particle %d not ascending and distinct", i);
                 }
-            dProp = upload(ctx, S_FE, in->proposals, (size_t)P * nprop);
+            dProp = upload(ctx, S_PROP, in->proposals, (size_t)P * nprop);
         }
 
         for (int ipass = 0; ipass < npass; ipass++) {

@@ -25,6 +25,8 @@
 
 #include "common.cuh"
 #include "estep3d_kernels.cuh"
+#include "restricted_kernels.cuh"
+#include "restricted_tc.cuh"
 #include "estep_kernels.cuh"
 #include "gemm_simt.cuh"
 #include "gemm_tc.cuh"
@@ -134,6 +136,22 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         const bool apply_ctf = in->do_ctf_correction && in->refs_are_ctf_corrected;
         const bool tc = ctx->precision != ROME_PREC_FP32;
         Profiler prof(ctx);
+        // optional coarse-pass restriction (learned proposals): validated on the host
+        const bool restricted = in->proposals != nullptr;
+        const int nprop = restricted ? in->nr_proposals : 0;
+        int* dProp = nullptr;
+        if (restricted) {
+            ROME_REQUIRE(nprop > 0 && nprop <= Jc, "nr_proposals %d (1..%d)", nprop, Jc);
+            ROME_REQUIRE(!out->coarse_diff2, "coarse_diff2 checkpoints are not available with proposals");
+            for (int i = 0; i < P; i++) {
+                const int* pr = in->proposals + (size_t)i * nprop;
+                for (int q = 0; q < nprop; q++) {
+                    ROME_REQUIRE(pr[q] >= 0 && pr[q] < Jc, "proposal %d of particle %d out of range", pr[q], i);
+                    ROME_REQUIRE(q == 0 || pr[q] > pr[q - 1], "proposals of particle %d not ascending", i);
+                }
+            }
+            dProp = upload3(ctx, S_PROP, in->proposals, (size_t)P * nprop);
+        }
 
         // ---- particle data at current_size ----
         const double *dFr, *dFi, *dFnr, *dFni, *dCtf;
@@ -242,69 +260,136 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             prof.end(ROME_PHASE_PROJECT);
 
             const long M = (long)P * T;
-            void* dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+            // restricted search on the tensor cores: no shifted images (a [TN][Kp] phase operand instead)
+            const bool rtc = restricted && tc && T <= 256;
+            const int Kh = g.Kp / 2;
+            void* dA = nullptr;
             float* dS = ctx->ws[S_S].as<float>((size_t)M);
-            float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+            float* dW2 = nullptr;
+            float2* dXw = nullptr;
+            float* dW2h = nullptr;
+            void* dSh = nullptr;
             unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)T * g.Kact);
             prof.begin(ROME_PHASE_SHIFT);
             phase_index_kernel<<<(unsigned)(((long)T * g.Kact + 255) / 256), 256, 0, st>>>(
                 T, g.Kact, g.csF, cs, dAct, dShift, ctx->shift_sampling, dPidx);
             ROME_CHECK_LAUNCH();
-            shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
-                                                           apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
-                                                           ctx->precision);
-            ROME_CHECK_LAUNCH();
-            w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
-            ROME_CHECK_LAUNCH();
+            if (rtc) {
+                char* buf = (char*)ctx->ws[S_A].get((size_t)P * Kh * (sizeof(float2) + sizeof(float)));
+                dXw = (float2*)buf;
+                dW2h = (float*)(buf + (size_t)P * Kh * sizeof(float2));
+                dSh = ctx->ws[S_NORM].get((size_t)2 * restricted_tile_tn(T) * g.Kp * 2);
+                restricted_prep(st, P, g.F, g.Kact, Kh, dFimg, dLctf, dMinv, apply_ctf ? 1 : 0, dAct, dXw, dW2h, dS);
+                restricted_shift_operand(st, T, g.Kact, g.Kp, dPidx, ctx->d_shift_tab, ctx->precision, dSh);
+            } else {
+                dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
+                dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
+                shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                                                               apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA,
+                                                               dS, ctx->precision);
+                ROME_CHECK_LAUNCH();
+                w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+                ROME_CHECK_LAUNCH();
+            }
             prof.launched(ROME_PHASE_SHIFT, 3);
             prof.end(ROME_PHASE_SHIFT);
 
-            float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * J);
-            prof.begin(ROME_PHASE_NORM_GEMM);
-            if (!tc) {
-                sgemm_tn(st, P, J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, J});
-                ROME_CHECK_LAUNCH();
-                prof.launched(ROME_PHASE_NORM_GEMM);
-            } else {
-                const int Kq64 = ((g.Kact + 63) / 64) * 64;
-                void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
-                void* dQb = ctx->ws[S_QB].get((size_t)J * Kq64 * 4);
-                split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
-                split_bf16(st, dQ, J, g.Kact, g.Kq, Kq64, dQb);
-                tc_store_gemm(st, P, J, Kq64, dW2b, dQb, dNorm, J, ctx->d_err);
-                prof.launched(ROME_PHASE_NORM_GEMM, 3);
-            }
-            prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * J * g.Kact);
-            prof.end(ROME_PHASE_NORM_GEMM);
-
-            float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * X);
             unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
             ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
-            Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJ, T, J, X, 1, 1, ntr, ncoarse, nullptr, dRowMin};
-            prof.begin(ROME_PHASE_CROSS_GEMM);
-            if (!tc) sgemm_tn(st, (int)M, J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
-            else tc_diff2_gemm(st, (int)M, J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
-            ROME_CHECK_LAUNCH();
-            prof.launched(ROME_PHASE_CROSS_GEMM);
-            prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * J * g.Kact);
-            prof.end(ROME_PHASE_CROSS_GEMM);
+            const long Xrow = restricted ? (long)nprop * T : X;  // hypotheses per particle row
+            float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xrow);
+            if (!restricted) {
+                float* dNorm = ctx->ws[S_NORM].as<float>((size_t)P * J);
+                prof.begin(ROME_PHASE_NORM_GEMM);
+                if (!tc) {
+                    sgemm_tn(st, P, J, g.Kq, dW2, g.Kq, dQ, g.Kq, StoreEpi{dNorm, J});
+                    ROME_CHECK_LAUNCH();
+                    prof.launched(ROME_PHASE_NORM_GEMM);
+                } else {
+                    const int Kq64 = ((g.Kact + 63) / 64) * 64;
+                    void* dW2b = ctx->ws[S_W2B].get((size_t)P * Kq64 * 4);
+                    void* dQb = ctx->ws[S_QB].get((size_t)J * Kq64 * 4);
+                    split_bf16(st, dW2, P, g.Kact, g.Kq, Kq64, dW2b);
+                    split_bf16(st, dQ, J, g.Kact, g.Kq, Kq64, dQb);
+                    tc_store_gemm(st, P, J, Kq64, dW2b, dQb, dNorm, J, ctx->d_err);
+                    prof.launched(ROME_PHASE_NORM_GEMM, 3);
+                }
+                prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * J * g.Kact);
+                prof.end(ROME_PHASE_NORM_GEMM);
+
+                Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJ, T, J, X, 1, 1, ntr, ncoarse, nullptr, dRowMin};
+                prof.begin(ROME_PHASE_CROSS_GEMM);
+                if (!tc) sgemm_tn(st, (int)M, J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
+                else tc_diff2_gemm(st, (int)M, J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_CROSS_GEMM);
+                prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * J * g.Kact);
+                prof.end(ROME_PHASE_CROSS_GEMM);
+            } else {
+                // ---- restricted coarse search: only the proposed orientations ----
+                prof.begin(ROME_PHASE_RESTRICTED);
+                if (rtc) {
+                    restricted_tc_diff2(st, ctx->precision, P, nprop, T, g.Kp, dProp, dJ, dXw, dW2h, dB, J, dSh, dS,
+                                        dXi2, Xrow, dDiff2, dRowMin, ctx->d_err);
+                } else {
+                    dim3 grid((nprop + RS_QQ - 1) / RS_QQ, (T + RS_TQ - 1) / RS_TQ, P);
+                    if (ctx->precision == ROME_PREC_FP32)
+                        restricted_diff2_kernel<ROME_PREC_FP32><<<grid, RS_THREADS, 0, st>>>(
+                            T, g.Kp, g.Kq, nprop, M, J, dProp, dJ, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                    else if (ctx->precision == ROME_PREC_BF16)
+                        restricted_diff2_kernel<ROME_PREC_BF16><<<grid, RS_THREADS, 0, st>>>(
+                            T, g.Kp, g.Kq, nprop, M, J, dProp, dJ, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                    else
+                        restricted_diff2_kernel<ROME_PREC_BF16X3><<<grid, RS_THREADS, 0, st>>>(
+                            T, g.Kp, g.Kq, nprop, M, J, dProp, dJ, dA, dB, dW2, dQ, dS, dXi2, Xrow, dDiff2, dRowMin);
+                    ROME_CHECK_LAUNCH();
+                }
+                prof.launched(ROME_PHASE_RESTRICTED);
+                prof.add_flops(ROME_PHASE_RESTRICTED, 4.0 * (double)P * Xrow * g.Kact);
+                prof.end(ROME_PHASE_RESTRICTED);
+            }
 
             // posterior, walk, coarse-significant points
             PostLayout Lp{T, 1, 1, npsi, ntr, K};
             Lp.ndir = ndir;
             Lp.list_zeros = 1;
+            if (restricted) {
+                // ragged rows: the prior of row position q * T + t comes from proposal q
+                int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)P * nprop);
+                restricted_entries_kernel<<<(unsigned)(((long)P * nprop + 255) / 256), 256, 0, st>>>(
+                    (long)P * nprop, npsi, dProp, dEnt);
+                ROME_CHECK_LAUNCH();
+                Lp.ent = dEnt;
+                Lp.ent_stride = nprop;
+                Lp.epr = T;
+            }
             int* dCounter = ctx->ws[S_LISTCNT].as<int>(4);
             int listcap = std::max(1024, P * 64), nsig = 0;
             SigEntry* dList = nullptr;
             prof.begin(ROME_PHASE_POSTERIOR);
             for (;;) {
                 dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap);
-                SelectResult sr = run_select(ctx, st, 0, P, X, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,
-                                             dPartI, nullptr, nullptr, dList, dCounter, listcap, dSeg, dRowMin);
+                SelectResult sr = run_select(ctx, st, 0, P, Xrow, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
+                                             dPart, dPartI, nullptr, nullptr, dList, dCounter, listcap, dSeg, dRowMin);
                 prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
                 nsig = sr.nlist;
                 if (sr.nlist <= listcap) break;
                 listcap = sr.nlist;
+            }
+            if (restricted && nsig > 0) {
+                // row position q * T + t -> dense coarse hypothesis j * T + t
+                restricted_list_dense_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, T, nprop, dProp, dList);
+                ROME_CHECK_LAUNCH();
+            }
+            if (out->post_coarse) {
+                double* dMarg = ctx->ws[S_TMP2].as<double>((size_t)P * J);
+                ROME_CUDA(cudaMemsetAsync(dMarg, 0, sizeof(double) * P * J, st));
+                if (nsig > 0) {
+                    post_marginal_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, T, 1, J, dList, dMarg);
+                    ROME_CHECK_LAUNCH();
+                }
+                ROME_CUDA(cudaMemcpyAsync(out->post_coarse, dMarg, sizeof(double) * P * J, cudaMemcpyDeviceToHost,
+                                          st));
             }
             ROME_CUDA(cudaMemsetAsync(dMcoarse, 0, (size_t)P * ncoarse, st));
             if (nsig > 0) {

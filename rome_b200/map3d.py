@@ -58,6 +58,8 @@ class Map3dPool:
     iclass_min: int = 0
     iclass_max: int = -1
     adaptive_oversampling: int = 1
+    # optional restricted coarse search: [P][nr_proposals] coarse orientations (class * nr_dir + dir) * nr_psi + psi
+    proposals: Optional[np.ndarray] = None
 
     @property
     def nr_images(self) -> int:
@@ -114,14 +116,25 @@ def _pack(p: Map3dPool):
     s.do_scale_correction = 0
     s.do_cross_correlation = 0
     s.inputs_on_device = 0
+    if p.proposals is not None:
+        pr = _i32(p.proposals)
+        keep.append(pr)
+        s.proposals = abi.iptr(pr)
+        s.nr_proposals = int(pr.shape[1])
     return s, keep
 
 
 def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
-                     fine_capacity: Optional[int] = None) -> Dict[str, np.ndarray]:
+                     fine_capacity: Optional[int] = None, marginals: bool = False,
+                     proposals: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
     """One pool through ``rome_gpu_map3d_estep_pool``; returns the per-particle
     results, the model sums of this pool, and (with ``checkpoints``) the coarse
-    diff2 array, Mcoarse_significant and the fine-pass lists."""
+    diff2 array, Mcoarse_significant and the fine-pass lists.  ``proposals``
+    ([P][k] coarse orientations, ascending) restricts the coarse pass;
+    ``marginals`` returns the coarse posterior per coarse orientation
+    (``post_coarse`` [P][K * nr_dir * nr_psi])."""
+    if proposals is not None:
+        p = dataclasses.replace(p, proposals=proposals)
     P, K, G, oF = p.nr_images, p.nr_classes, p.nr_groups, p.ori_size // 2 + 1
     s, keep = _pack(p)
     o: Dict[str, np.ndarray] = {}
@@ -159,6 +172,9 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
         so.fine_index = o["fine_index"].ctypes.data_as(C.POINTER(C.c_long))
         so.fine_diff2 = abi.dptr(o["fine_diff2"])
         so.fine_weight = abi.dptr(o["fine_weight"])
+    if marginals:
+        o["post_coarse"] = np.zeros((P, K * p.nr_dir * p.nr_psi))
+        so.post_coarse = abi.dptr(o["post_coarse"])
     ctx._check(ctx.lib.rome_gpu_map3d_estep_pool(ctx.h, C.byref(s), C.byref(so)))
     if checkpoints:
         n = int(o["fine_count"].sum())
@@ -220,3 +236,18 @@ def fine_lists_from_dump(d: Dict[str, np.ndarray], prefix: str, nr_trans: int, n
         out.append((np.concatenate(idx) if idx else np.zeros(0, np.int64),
                      np.concatenate(v) if v else np.zeros(0)))
     return out
+
+
+def direction_templates(net, projector_data: np.ndarray, r_max: int, p: Map3dPool) -> np.ndarray:
+    """Network-input features of every coarse (class, direction) projection at
+    psi = 0 without CTF ([K * nr_dir][2][n_r][n_theta]), the templates of
+    ProposalNet.init_matched_filter for 3D proposals."""
+    from .workload import project3d_np
+    K, cur = p.nr_classes, p.current_size
+    dirs = np.asarray(p.angles[0])[:, 0, 0, :2]  # (rot, tilt) of each coarse direction
+    ang = np.concatenate([dirs, np.zeros((len(dirs), 1))], axis=1)
+    slices = np.concatenate([project3d_np(projector_data[k], r_max, ang, cur) for k in range(K)])
+    fake = dataclasses.replace(p, Fimg_real=slices.real.reshape(len(slices), -1),
+                               Fimg_imag=slices.imag.reshape(len(slices), -1),
+                               Fctf=np.ones((len(slices), cur * (cur // 2 + 1))))
+    return net.features(fake)

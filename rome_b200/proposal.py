@@ -166,6 +166,31 @@ class ProposalNet:
         self.ctx._check(self.lib.rome_gpu_proposal_predict(self.h, n, _fptr(x), k, abi.iptr(idx), _fptr(prob)))
         return idx, prob
 
+    def init_matched_filter(self, templates: np.ndarray, scale: float = 1.0, seed: int = 0):
+        """Start from a matched filter instead of random weights: the two
+        convolutions pass the log-magnitude channel through (centre tap 1 on
+        channel 0, every other weight small), and the head correlates it,
+        over all rotations, with each output class's template features
+        (templates [n_classes][2][n_r][n_theta], e.g. the features of each
+        class/direction's projection; zero mean, unit norm per class).
+        Training then refines it.  The physics supplies what few training
+        particles per class cannot (e.g. one class per 3D direction)."""
+        rng = np.random.default_rng(seed)
+        d = flat_to_dict(self.get_params(), self.n_r, self.n_theta, self.channels, self.n_classes)
+        for name in d:
+            d[name] = d[name] * 0.01
+        d["w0"][0, 0, 1, 1] = 1.0
+        d["w1"][0, 0, 1, 1] = 1.0
+        d["b0"][:] = 0.0
+        d["b1"][:] = 0.0
+        t = np.asarray(templates, np.float64)[:, 0]  # the log-magnitude channel
+        t = t - t.mean(axis=(1, 2), keepdims=True)
+        t = t / np.maximum(np.linalg.norm(t.reshape(len(t), -1), axis=1), 1e-30)[:, None, None]
+        d["wf"][:, 0] = scale * t
+        d["bf"][:] = 0.0
+        self.set_params(dict_to_flat(d, self.n_r, self.n_theta, self.channels, self.n_classes))
+        del rng
+
     def propose(self, p, k: int):
         """Top-k network outputs of every particle of a pool (a Map2dPool, or
         a StagedPool whose images live on the device), expanded to ascending

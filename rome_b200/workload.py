@@ -229,6 +229,206 @@ def build_map2d(w: Map2dWorkload):
     return pool, proj, r_max, truth
 
 
+# ---------------------------------------------------------------------------
+# 3D: random-blob volumes, Fourier-slice particles, HEALPix sampling
+
+
+@dataclasses.dataclass
+class Map3dWorkload:
+    n_particles: int = 1000
+    ori_size: int = 32
+    current_size: Optional[int] = None  # default: ori_size
+    coarse_size: Optional[int] = None   # default: current_size / 2 (even, >= 12)
+    n_classes: int = 2
+    n_blobs: int = 30
+    blob_sigma: tuple = (1.5, 4.0)
+    healpix_order: int = 1
+    offset_range: int = 2
+    offset_step: int = 1
+    max_shift: float = 2.0
+    pixel: float = 2.0
+    snr: float = 0.1
+    defocus: tuple = (10000.0, 30000.0)
+    seed: int = 1
+    random_perturbation: float = 0.0
+    particle_seed: Optional[int] = None
+
+
+def blob_volumes(rng, ori, K, n_blobs, sig):
+    """K volumes ori^3, each a sum of n_blobs Gaussian blobs inside 0.3 ori of the centre."""
+    c = np.arange(ori) - ori // 2
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    vols = np.zeros((K, ori, ori, ori))
+    for k in range(K):
+        u = rng.normal(size=(n_blobs, 3))
+        u /= np.linalg.norm(u, axis=1, keepdims=True)
+        r = 0.3 * ori * np.cbrt(rng.uniform(0, 1, n_blobs))
+        ctr = u * r[:, None]
+        s = rng.uniform(sig[0], sig[1], n_blobs)
+        a = rng.uniform(0.5, 1.0, n_blobs)
+        for q in range(n_blobs):
+            d2 = (xx - ctr[q, 0]) ** 2 + (yy - ctr[q, 1]) ** 2 + (zz - ctr[q, 2]) ** 2
+            vols[k] += a[q] * np.exp(-d2 / (2 * s[q] ** 2))
+    return vols
+
+
+def projector_map_3d(vol: np.ndarray, current_size: int, padding: int = 2):
+    """MyProjector::computeFourierTransformMap for a 3D reference
+    (src/reconstruct.cpp:106-223), as projector_map_2d: gridding correction,
+    zero padding by 2, centred FFT, windowed to r_max.  Returns
+    (data [pad][pad][pad/2+1][2], r_max, pad_size)."""
+    ori = vol.shape[0]
+    r_max = min(current_size // 2, ori // 2)
+    pad_size = 2 * (padding * r_max + 1) + 1
+    padF = pad_size // 2 + 1
+    c = np.arange(ori) - ori // 2
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    r = np.sqrt(xx * xx + yy * yy + zz * zz)
+    rval = r / (ori * padding)
+    sinc = np.where(r > 0, np.sin(np.pi * rval) / np.where(r > 0, np.pi * rval, 1.0), 1.0)
+    P = padding * ori
+    Mpad = np.zeros((P, P, P))
+    o = P // 2 - ori // 2
+    Mpad[o:o + ori, o:o + ori, o:o + ori] = vol / (sinc * sinc)
+    F = np.fft.rfftn(np.fft.ifftshift(Mpad)) / (P * P * P) * padding ** 3
+    hP = P // 2 + 1
+    ip = np.where(np.arange(P) < hP, np.arange(P), np.arange(P) - P)
+    kz, ky, kx = np.meshgrid(ip, ip, np.arange(hP), indexing="ij")
+    ok = (kz * kz + ky * ky + kx * kx <= (r_max * padding) ** 2) & (np.abs(kz) <= pad_size // 2) & (
+        np.abs(ky) <= pad_size // 2) & (kx < padF)
+    data = np.zeros((pad_size, pad_size, padF, 2))
+    zi, yi, xi = kz[ok] + pad_size // 2, ky[ok] + pad_size // 2, kx[ok]
+    data[zi, yi, xi, 0] = F[ok].real
+    data[zi, yi, xi, 1] = F[ok].imag
+    return data, r_max, pad_size
+
+
+def project3d_np(data: np.ndarray, r_max: int, angles: np.ndarray, size: int, padding: int = 2) -> np.ndarray:
+    """MyProjector::project, trilinear (src/reconstruct.cpp:226-410), for many
+    (rot, tilt, psi) at once; returns complex [n][size][size/2+1]."""
+    from .sampling import euler_matrix
+    pad = data.shape[0]
+    Fs = size // 2 + 1
+    my_r = min(r_max, size // 2)
+    rows = np.arange(size)
+    yv = np.where(rows <= my_r, rows, rows - size)
+    rowok = (rows <= my_r) | (rows >= size - my_r)
+    yy, xx = np.meshgrid(yv, np.arange(Fs), indexing="ij")
+    ok = rowok[:, None] & (xx <= my_r) & (xx * xx + yy * yy <= my_r * my_r)
+    ys, xs = yy[ok].astype(np.float64), xx[ok].astype(np.float64)
+    A = np.stack([euler_matrix(*a) for a in np.atleast_2d(angles)]) * padding  # [n][3][3]
+    xp = A[:, 0, 0, None] * xs + A[:, 1, 0, None] * ys
+    yp = A[:, 0, 1, None] * xs + A[:, 1, 1, None] * ys
+    zp = A[:, 0, 2, None] * xs + A[:, 1, 2, None] * ys
+    neg = xp < 0
+    xp, yp, zp = np.where(neg, -xp, xp), np.where(neg, -yp, yp), np.where(neg, -zp, zp)
+    x0 = np.floor(xp).astype(np.int64)
+    y0 = np.floor(yp).astype(np.int64)
+    z0 = np.floor(zp).astype(np.int64)
+    fx, fy, fz = xp - x0, yp - y0, zp - z0
+    y0 += pad // 2
+    z0 += pad // 2
+    cplx = data[..., 0] + 1j * data[..., 1]
+    lerp = lambda a, lo, hi: lo + (hi - lo) * a  # noqa: E731
+    c00 = lerp(fx, cplx[z0, y0, x0], cplx[z0, y0, x0 + 1])
+    c01 = lerp(fx, cplx[z0 + 1, y0, x0], cplx[z0 + 1, y0, x0 + 1])
+    c10 = lerp(fx, cplx[z0, y0 + 1, x0], cplx[z0, y0 + 1, x0 + 1])
+    c11 = lerp(fx, cplx[z0 + 1, y0 + 1, x0], cplx[z0 + 1, y0 + 1, x0 + 1])
+    v = lerp(fz, lerp(fy, c00, c10), lerp(fy, c01, c11))
+    v = np.where(neg, np.conj(v), v)
+    out = np.zeros((A.shape[0], size, Fs), np.complex128)
+    out[:, ok] = v
+    return out
+
+
+def build_map3d(w: Map3dWorkload):
+    """Returns (Map3dPool for all particles, projector data [K][pad][pad][padF][2],
+    r_max, truth dict).  Sampling: HEALPix order w.healpix_order with
+    adaptive oversampling 1 (rome_b200.sampling, the reference's sampler)."""
+    from .map3d import Map3dPool
+    from .sampling import oversampled_orientations_3d, oversampled_translations
+    rng = np.random.default_rng(w.seed)
+    ori = w.ori_size
+    cur = w.current_size or ori
+    cs = w.coarse_size or max(12, (cur // 2) // 2 * 2)
+    K = w.n_classes
+    vols = blob_volumes(rng, ori, K, w.n_blobs, w.blob_sigma)
+    proj = []
+    for k in range(K):
+        d, r_max, pad = projector_map_3d(vols[k], cur)
+        proj.append(d)
+    proj = np.stack(proj)
+    if w.particle_seed is not None:
+        rng = np.random.default_rng(w.particle_seed)
+    N = w.n_particles
+    Fs = cur // 2 + 1
+    cls = rng.integers(0, K, N)
+    rot = rng.uniform(0.0, 360.0, N)
+    tilt = np.rad2deg(np.arccos(rng.uniform(-1.0, 1.0, N)))
+    psi = rng.uniform(0.0, 360.0, N)
+    sx = rng.uniform(-w.max_shift, w.max_shift, N)
+    sy = rng.uniform(-w.max_shift, w.max_shift, N)
+    du = rng.uniform(*w.defocus, N)
+    dv = rng.uniform(*w.defocus, N)
+    da = rng.uniform(0, 180, N)
+    rows = np.arange(cur)
+    ky = np.where(rows < Fs, rows, rows - cur).astype(np.float64)[:, None]
+    kx = np.arange(Fs, dtype=np.float64)[None, :]
+    Fr = np.zeros((N, cur * Fs))
+    Fi = np.zeros((N, cur * Fs))
+    ctf = np.zeros((N, cur * Fs))
+    mres = mresol(cur)
+    sig_all = []
+    chunk = 64
+    for c0 in range(0, N, chunk):
+        c1 = min(N, c0 + chunk)
+        for k in np.unique(cls[c0:c1]):
+            idx = np.nonzero(cls[c0:c1] == k)[0] + c0
+            Pk = project3d_np(proj[k], r_max, np.stack([rot[idx], tilt[idx], psi[idx]], axis=1), cur)
+            for q, i in enumerate(idx):
+                c = ctf_image(cur, ori, w.pixel, du[i], dv[i], da[i], 300.0, 2.7, 0.1)
+                ph = np.exp(2j * np.pi * (kx * sx[i] + ky * sy[i]) / ori)
+                s = Pk[q] * ph * c
+                Fr[i] = s.real.reshape(-1)
+                Fi[i] = s.imag.reshape(-1)
+                ctf[i] = c.reshape(-1)
+                sig_all.append(np.mean(np.abs(s.reshape(-1)[mres > 0]) ** 2))
+    sig_pow = float(np.mean(sig_all))
+    sigma2 = sig_pow / (2.0 * w.snr)
+    Fr += rng.normal(0, math.sqrt(sigma2), Fr.shape)
+    Fi += rng.normal(0, math.sqrt(sigma2), Fi.shape)
+    Fr[:, 0] = 0.0
+    Fi[:, 0] = 0.0
+    oriF = ori // 2 + 1
+    tx, ty = translations(w.offset_range, w.offset_step)
+    rp = w.random_perturbation
+    angles = [oversampled_orientations_3d(w.healpix_order, o, rp) for o in (0, 1)]
+    otr = [oversampled_translations(tx, ty, float(w.offset_step), o, rp) for o in (0, 1)]
+    ndir = angles[0].shape[0]
+    pool = Map3dPool(
+        ori_size=ori, current_size=cur, coarse_size=cs, nr_classes=K, nr_groups=1, nr_dir=ndir, angles=angles,
+        over_trans_x=[otr[0][0], otr[1][0]], over_trans_y=[otr[0][1], otr[1][1]], trans_x=tx, trans_y=ty,
+        Fimg_real=Fr, Fimg_imag=Fi, Fimg_nomask_real=Fr.copy(), Fimg_nomask_imag=Fi.copy(), Fctf=ctf,
+        highres_Xi2=np.zeros(N), old_offsetx=np.zeros(N), old_offsety=np.zeros(N), group=np.zeros(N, np.int32),
+        sigma2_noise=np.full((1, oriF), sigma2), Mresol_fine=mres, Mresol_coarse=mresol(cs),
+        pdf_class=np.full(K, 1.0 / K), pdf_direction=np.full((K, ndir), 1.0 / ndir),
+        prior_offsetx_class=np.zeros(K), prior_offsety_class=np.zeros(K),
+        sigma2_offset=float(w.offset_range) ** 2 / 4.0, adaptive_oversampling=1)
+    truth = dict(cls=cls, rot=rot, tilt=tilt, psi=psi, sx=sx, sy=sy)
+    return pool, proj, r_max, truth
+
+
+def subset3d(p, lo: int, hi: int):
+    """The particles [lo, hi) of a 3D pool."""
+    q = dataclasses.replace(p)
+    for name in ["Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf", "highres_Xi2",
+                 "old_offsetx", "old_offsety", "group"]:
+        setattr(q, name, np.ascontiguousarray(getattr(p, name)[lo:hi]))
+    if getattr(p, "proposals", None) is not None:
+        q.proposals = np.ascontiguousarray(p.proposals[lo:hi])
+    return q
+
+
 def subset(p: Map2dPool, lo: int, hi: int) -> Map2dPool:
     """The particles [lo, hi) of a pool (same model and sampling)."""
     q = dataclasses.replace(p)
