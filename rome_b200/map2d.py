@@ -250,14 +250,16 @@ def concat_pools(pools):
     if isinstance(pools[0], StagedPool):
         import torch
 
-        def rows(q, name):
-            t = q.dev[name]
-            if q.pool.particle_rows is None:
-                return t
-            return t.index_select(0, _device_index(np.asarray(q.pool.particle_rows, np.int64), t.device))
+        dev0 = next(iter(pools[0].dev.values())).device
+        idx = [None if q.pool.particle_rows is None
+               else _device_index(np.asarray(q.pool.particle_rows, np.int64), dev0) for q in pools]
+
+        def rows(q, ix, name):
+            return q.dev[name] if ix is None else q.dev[name].index_select(0, ix)
 
         base = concat_pools([dataclasses.replace(q.pool, particle_rows=None) for q in pools])
-        out = StagedPool(base, {name: torch.cat([rows(q, name) for q in pools]) for name in pools[0].dev})
+        out = StagedPool(base, {name: torch.cat([rows(q, ix, name) for q, ix in zip(pools, idx)])
+                                for name in pools[0].dev})
         torch.cuda.current_stream(next(iter(out.dev.values())).device).synchronize()
         return out
     q = dataclasses.replace(pools[0])
