@@ -126,7 +126,7 @@ def _pack(p: Map3dPool):
 
 def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
                      fine_capacity: Optional[int] = None, marginals: bool = False,
-                     proposals: Optional[np.ndarray] = None) -> Dict[str, np.ndarray]:
+                     proposals: Optional[np.ndarray] = None, dev: Optional[dict] = None) -> Dict[str, np.ndarray]:
     """One pool through ``rome_gpu_map3d_estep_pool``; returns the per-particle
     results, the model sums of this pool, and (with ``checkpoints``) the coarse
     diff2 array, Mcoarse_significant and the fine-pass lists.  ``proposals``
@@ -137,6 +137,13 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
         p = dataclasses.replace(p, proposals=proposals)
     P, K, G, oF = p.nr_images, p.nr_classes, p.nr_groups, p.ori_size // 2 + 1
     s, keep = _pack(p)
+    if dev is not None:
+        # images already on the device (torch tensors named like the pool fields)
+        import torch
+        torch.cuda.current_stream(ctx.device).synchronize()
+        for name, t in dev.items():
+            setattr(s, name, C.cast(C.c_void_p(t.data_ptr()), abi._DP))
+        s.inputs_on_device = 1
     o: Dict[str, np.ndarray] = {}
     so = abi.RomeMap3dPoolOut()
     for name in ("min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "rot", "tilt",
@@ -176,6 +183,7 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
         o["post_coarse"] = np.zeros((P, K * p.nr_dir * p.nr_psi))
         so.post_coarse = abi.dptr(o["post_coarse"])
     ctx._check(ctx.lib.rome_gpu_map3d_estep_pool(ctx.h, C.byref(s), C.byref(so)))
+    del keep
     if checkpoints:
         n = int(o["fine_count"].sum())
         for name in ("fine_index", "fine_diff2", "fine_weight"):

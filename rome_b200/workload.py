@@ -446,4 +446,10 @@ CONFIGS = {
                                 offset_range=5, offset_step=1, max_shift=4.0, pixel=2.0, snr=0.05, seed=1),
     "map2d_cfg2": Map2dWorkload(n_particles=20000, ori_size=128, n_classes=50, n_blobs=40, psi_step=5.0,
                                 offset_range=6, offset_step=2, max_shift=6.0, pixel=1.5, snr=0.03, seed=2),
+    # MAP3D: 10,000 particles of 128^2 from K=4 blob volumes (60 blobs, sigma 2-8 voxels), HEALPix order 2
+    # (192 directions x 24 coarse psi), +-4 px step 2 (13 translations), adaptive oversampling 1; coarse
+    # size 20 as the reference's formula gives for these images (map_model.cpp:505-520)
+    "map3d_cfg3": Map3dWorkload(n_particles=10000, ori_size=128, coarse_size=20, n_classes=4, n_blobs=60,
+                                blob_sigma=(2.0, 8.0), healpix_order=2, offset_range=4, offset_step=2, max_shift=4.0,
+                                pixel=1.5, snr=0.05, seed=3),
 }
