@@ -299,6 +299,38 @@ int main(int argc, char* argv[]) {
             }
             d.i32(pp + "group", grp.data(), {P});
             d.f64(pp + "norm_in", norm.data(), {P});
+            // inputs of the image preparation (ParticleModel::setFourierTransforms,
+            // src/exp_model.h:397-640): the pool's images as read, the metadata it uses
+            {
+                const int o2 = ori_size * ori_size;
+                std::vector<double> raw((size_t)P * o2);
+                for (int i = 0; i < P; i++) {
+                    auto src = images[(first - first_local_image) + i].wptrAll();
+                    for (int j = 0; j < o2; j++) raw[(size_t)i * o2 + j] = src[j];
+                }
+                d.f64(pp + "raw_images", raw.data(), {P, ori_size, ori_size});
+                std::vector<double> meta((size_t)P * 10);
+                for (int i = 0; i < P; i++) {
+                    const auto& m = exp_metadata[i];
+                    const double v[10] = {m.NORM,          m.XOFF,          m.YOFF,   m.CTF_DEFOCUS_U, m.CTF_DEFOCUS_V,
+                                          m.CTF_DEFOCUS_ANGLE, m.CTF_VOLTAGE, m.CTF_CS, m.CTF_Q0,        m.CTF_BFAC};
+                    for (int q = 0; q < 10; q++) meta[(size_t)i * 10 + q] = v[q];
+                }
+                d.f64(pp + "prep_metadata", meta.data(), {P, 10});
+                if (pool_index == 0) {
+                    d.scalar("prep_avg_norm_correction", mlModel.avg_norm_correction);
+                    d.scalar("prep_pixel_size", particleModel.pixel_size);
+                    d.scalar("prep_particle_diameter", particleModel.particle_diameter);
+                    d.iscalar("prep_width_mask_edge", particleModel.width_mask_edge);
+                    d.scalar("prep_sigma2_fudge", particleModel.sigma2_fudge);
+                    d.iscalar("prep_random_seed", particleModel.random_seed);
+                    d.iscalar("prep_do_norm_correction", particleModel.do_norm_correction);
+                    d.iscalar("prep_do_zero_mask", particleModel.do_zero_mask);
+                    d.iscalar("prep_only_flip_phases", particleModel.only_flip_phases);
+                    d.iscalar("prep_ctf_phase_flipped", particleModel.ctf_phase_flipped);
+                    d.iscalar("prep_intact_ctf_first_peak", particleModel.intact_ctf_first_peak);
+                }
+            }
 
             // the stages of expectationSomeParticles()
             int npass = adaptive_oversampling > 0 ? 2 : 1;
