@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define ROME_GPU_ABI_VERSION 2
+#define ROME_GPU_ABI_VERSION 3
 
 enum RomeStatus {
     ROME_OK = 0,
@@ -58,7 +58,8 @@ typedef struct RomeGpuCtx RomeGpuCtx;
 typedef struct {
     int precision;           /* RomePrecision */
     int deterministic;       /* nonzero: fixed-order reductions where the ABI allows */
-    size_t workspace_limit;  /* device scratch cap in bytes, 0 = automatic */
+    size_t workspace_limit;  /* device scratch cap in bytes, 0 = automatic (1.5 GiB); bounds the
+                                work buffers of rome_gpu_prepare_particles, which then runs in chunks */
     int profile;             /* nonzero: time each phase with CUDA events (rome_gpu_get_timings) */
 } RomeGpuConfig;
 
@@ -77,6 +78,7 @@ enum RomePhase {
     ROME_PHASE_RECONSTRUCT,   /* MyBackProjector::reconstruct */
     ROME_PHASE_RESTRICTED,    /* diff2 over each particle's proposed orientations only */
     ROME_PHASE_PROPOSE,       /* proposal network: features, forward, top-k, expansion */
+    ROME_PHASE_IMAGES,        /* setFourierTransforms: translate, noise, soft mask, FFTs, CTF */
     ROME_PHASE_COUNT
 };
 
@@ -120,6 +122,76 @@ int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, 
  * the per-thread replica reduction MAPModel::reduceThreadMap
  * (src/map_model.cpp:209-231). */
 int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int clear_src);
+
+/* ---------------------------------------------------------------------
+ * Particle image preparation for one pool.  Replaces
+ * ParticleModel::setFourierTransforms (src/exp_model.h:397-640), called by
+ * the optimizers' expectation() before expectationSomeParticles: norm
+ * correction, translation by the rounded old offsets (no wrap), the
+ * centred, normalised Fourier transform windowed to current_size
+ * (Fimages_nomask); a noise image drawn from sigma2_noise with the
+ * reference's seeded generator (seed random_seed + first_image + i, glibc
+ * srand/rand through Random_generator::rnd_gaus) blended outside the
+ * particle diameter with a raised-cosine edge (softMaskOutsideMap), or the
+ * background average when do_zero_mask; its windowed transform
+ * (Fimages_mask_fine), power spectrum and highres_Xi2 (when current_size <
+ * ori_size), and the CTF image (CTF::getFftwImage).  The outputs are the
+ * image inputs of rome_gpu_map2d_estep_pool; with outputs_on_device they
+ * can be handed to it without leaving the device (inputs_on_device).
+ * Even ori_size only; current_size <= ori_size.
+ * ------------------------------------------------------------------- */
+typedef struct {
+    int nr_images;          /* exp_nr_images (P) */
+    int ori_size;
+    int current_size;       /* fine_size */
+    int nr_groups;
+    int first_image;        /* exp_first_image: part of the noise seed */
+    const void* images;     /* exp_images as read [P][ori_size][ori_size] */
+    int image_type;         /* 0: double (FDOUBLE), 1: float (MRC mode 2 as stored) */
+    int images_on_device;   /* nonzero: `images` is a device pointer on the context's device */
+    /* exp_metadata fields [P] (host) */
+    const double* norm;     /* NORM */
+    const double* xoff;     /* XOFF, YOFF (the old offsets before rounding) */
+    const double* yoff;
+    const double* ctf_defocus_u;
+    const double* ctf_defocus_v;
+    const double* ctf_defocus_angle;
+    const double* ctf_voltage;
+    const double* ctf_cs;
+    const double* ctf_q0;
+    const double* ctf_bfac;
+    const int* group;                /* GROUP_NO - 1 [P] */
+    const double* sigma2_noise;      /* mlModel.sigma2_noise [nr_groups][ori_size/2+1] */
+    double avg_norm_correction;      /* mlModel.avg_norm_correction */
+    double pixel_size;
+    double particle_diameter;        /* Angstrom */
+    double sigma2_fudge;
+    int width_mask_edge;             /* pixels */
+    int random_seed;
+    int do_norm_correction;
+    int do_zero_mask;
+    int do_ctf_correction;
+    int ctf_phase_flipped;           /* CTF image as |ctf| */
+    int only_flip_phases;            /* CTF image as sign(ctf) */
+    int intact_ctf_first_peak;
+} RomePrepIn;
+
+typedef struct {
+    /* [P][current_size][current_size/2+1]: Fimages_mask_fine, Fimages_nomask, Fctfs */
+    double* Fimg_real;
+    double* Fimg_imag;
+    double* Fimg_nomask_real;
+    double* Fimg_nomask_imag;
+    double* Fctf;
+    int outputs_on_device;  /* nonzero: the five arrays above are device pointers on the context's device */
+    /* host [P] */
+    double* highres_Xi2;    /* exp_highres_Xi2_imgs */
+    double* old_offsetx;    /* exp_old_offsetx / y: round(XOFF), round(YOFF) */
+    double* old_offsety;
+    double* power_imgs;     /* host [P][ori_size/2+1] exp_power_imgs (zero when current_size == ori_size); NULL to skip */
+} RomePrepOut;
+
+int rome_gpu_prepare_particles(RomeGpuCtx* ctx, const RomePrepIn* in, RomePrepOut* out);
 
 /* ---------------------------------------------------------------------
  * MAP2D E-step for one pool of particles.

@@ -37,10 +37,10 @@ class RomeGpuConfig(C.Structure):
                 ("profile", C.c_int)]
 
 
-ABI_VERSION = 2  # ROME_GPU_ABI_VERSION of include/rome_gpu.h
+ABI_VERSION = 3  # ROME_GPU_ABI_VERSION of include/rome_gpu.h
 
 PHASES = ["prep", "project", "shift", "norm_gemm", "cross_gemm", "posterior", "wsum", "backproject", "reconstruct",
-          "restricted", "propose"]
+          "restricted", "propose", "images"]
 
 
 class RomeGpuTimings(C.Structure):
@@ -123,6 +123,24 @@ class RomeReconOut(C.Structure):
     _fields_ = [("vol", _DP), ("tau2", _DP), ("sigma2", _DP), ("data_vs_prior", _DP)]
 
 
+class RomePrepIn(C.Structure):
+    _fields_ = [("nr_images", C.c_int), ("ori_size", C.c_int), ("current_size", C.c_int), ("nr_groups", C.c_int),
+                ("first_image", C.c_int), ("images", C.c_void_p), ("image_type", C.c_int),
+                ("images_on_device", C.c_int), ("norm", _DP), ("xoff", _DP), ("yoff", _DP),
+                ("ctf_defocus_u", _DP), ("ctf_defocus_v", _DP), ("ctf_defocus_angle", _DP), ("ctf_voltage", _DP),
+                ("ctf_cs", _DP), ("ctf_q0", _DP), ("ctf_bfac", _DP), ("group", _IP), ("sigma2_noise", _DP),
+                ("avg_norm_correction", C.c_double), ("pixel_size", C.c_double), ("particle_diameter", C.c_double),
+                ("sigma2_fudge", C.c_double), ("width_mask_edge", C.c_int), ("random_seed", C.c_int),
+                ("do_norm_correction", C.c_int), ("do_zero_mask", C.c_int), ("do_ctf_correction", C.c_int),
+                ("ctf_phase_flipped", C.c_int), ("only_flip_phases", C.c_int), ("intact_ctf_first_peak", C.c_int)]
+
+
+class RomePrepOut(C.Structure):
+    _fields_ = [("Fimg_real", _DP), ("Fimg_imag", _DP), ("Fimg_nomask_real", _DP), ("Fimg_nomask_imag", _DP),
+                ("Fctf", _DP), ("outputs_on_device", C.c_int), ("highres_Xi2", _DP), ("old_offsetx", _DP),
+                ("old_offsety", _DP), ("power_imgs", _DP)]
+
+
 def dptr(a: Optional[np.ndarray]):
     if a is None:
         return _DP()
@@ -155,7 +173,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_proposal_loss_grad", "rome_gpu_proposal_train", "rome_gpu_proposal_predict",
     "rome_gpu_proposal_propose",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
-    "rome_gpu_add_backprojectors",
+    "rome_gpu_add_backprojectors", "rome_gpu_prepare_particles",
 ]
 
 _LIB = None
@@ -211,6 +229,7 @@ def load_library():
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]
+    lib.rome_gpu_prepare_particles.argtypes = [C.c_void_p, C.POINTER(RomePrepIn), C.POINTER(RomePrepOut)]
     lib.rome_gpu_get_timings.argtypes = [C.c_void_p, C.POINTER(RomeGpuTimings)]
     lib.rome_gpu_reset_timings.argtypes = [C.c_void_p]
     _LIB = lib

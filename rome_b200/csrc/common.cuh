@@ -133,6 +133,14 @@ enum Slot {
     S_TMP2,
     S_ROWS,       // particle_rows of a subset pool [P] int
     S_PROP,       // proposals of a restricted search [P][nprop] int
+    S_PREP_RAW,   // image preparation: raw images of a chunk (host input)
+    S_PREP_R,     // image preparation: real-space work images [chunk][n][n] double
+    S_PREP_C,     // image preparation: half-plane transforms [chunk][n][n/2+1] double2
+    S_PREP_NC,    // image preparation: noise spectra of a chunk, row-major over (row, image) [n][chunk][n/2+1] double2
+    S_PREP_NR,    // image preparation: noise images [n][chunk][n] double
+    S_PREP_PART,  // image preparation: per-particle parameters [P][12] double
+    S_PREP_OUT,   // image preparation: outputs when they go to the host
+    S_PREP_TAB,   // image preparation: shell tables, noise sigmas, per-image sums
     S_COUNT
 };
 
@@ -142,6 +150,7 @@ struct RomeGpuCtx {
     int device = 0;
     int precision = ROME_PREC_FP32;
     int deterministic = 0;
+    size_t workspace_limit = 0;  // RomeGpuConfig::workspace_limit (0: automatic)
     cudaStream_t stream = nullptr;
     std::string last_error;
     // class references (projectors) and accumulated backprojectors, FP64
@@ -175,6 +184,8 @@ struct RomeGpuCtx {
     double phase_flops[ROME_PHASE_COUNT] = {};
     double phase_bytes[ROME_PHASE_COUNT] = {};
     long total_launches = 0;
+    // cached cuFFT plans of the image preparation (prep.cu)
+    void* prep_plans = nullptr;
 };
 
 namespace rome {
@@ -182,6 +193,9 @@ namespace rome {
 // start of an entry point: the stream is idle (every entry point ends with a
 // synchronize; this one also covers an earlier call that failed part-way), so
 // the upload arena can be reused from its start
+// releases the image preparation's cuFFT plans (prep.cu)
+void prep_release(RomeGpuCtx* ctx);
+
 inline void arena_reset(RomeGpuCtx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     ctx->h_arena_used = 0;

@@ -28,6 +28,7 @@ extern "C" int rome_gpu_create(int device, const RomeGpuConfig* cfg, RomeGpuCtx*
             ctx->precision = cfg->precision;
             ctx->deterministic = cfg->deterministic;
             ctx->profile = cfg->profile;
+            ctx->workspace_limit = cfg->workspace_limit;
         }
         ROME_REQUIRE(ctx->precision >= ROME_PREC_FP32 && ctx->precision <= ROME_PREC_BF16X3, "bad precision %d",
                      ctx->precision);
@@ -64,6 +65,7 @@ extern "C" int rome_gpu_destroy(RomeGpuCtx* ctx) {
     if (!ctx) return ROME_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    rome::prep_release(ctx);
     for (auto& b : ctx->ws) b.release();
     if (ctx->proj) cudaFree(ctx->proj);
     if (ctx->bp_data) cudaFree(ctx->bp_data);

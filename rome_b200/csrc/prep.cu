@@ -1,0 +1,808 @@
+// Particle image preparation on the device: ParticleModel::setFourierTransforms
+// (src/exp_model.h:397-640) for one pool, entry point rome_gpu_prepare_particles.
+//
+// Per chunk of images (FP64 throughout, like the reference):
+//   translate_center   norm correction, integer translation by the rounded old
+//                      offsets without wrap (translate -> applyGeometry,
+//                      src/image.h:53-257), CenterFFT (src/image.h:344-380)
+//   cuFFT D2Z          the unnormalised transform; the window kernel divides by
+//                      n^2 (normalizeComplex, src/fft_base.cpp:103-109) and cuts
+//                      to current_size (windowFourierTransform, src/image.h:496-566)
+//   noise              the reference's noise spectra (src/exp_model.h:489-532),
+//                      one warp per image, with the seeded generator restated
+//                      below, written in the column transform's layout; inverse
+//                      transform as column DFTs then row C2R (the decomposition
+//                      of FFTW's multi-dimensional C2R, which reads only the real
+//                      part of the x = 0 and x = n/2 columns)
+//   mask               softMaskOutsideMap (src/image.h:571-634) with the noise
+//                      image, or the raised-cosine weighted background average
+//   cuFFT D2Z          masked transform -> window, power spectrum, highres_Xi2
+//   ctf                CTF::getFftwImage (src/ctf.cpp:173-191, src/ctf.h:151-204)
+#include <cufft.h>
+
+#include <cmath>
+#include <map>
+#include <tuple>
+
+#include "common.cuh"
+
+namespace rome {
+namespace {
+
+#define ROME_CUFFT(call)                                                                        \
+    do {                                                                                        \
+        cufftResult r_ = (call);                                                                \
+        if (r_ != CUFFT_SUCCESS) ::rome::fail(ROME_ERR_CUDA, "%s:%d %s: cufft error %d", __FILE__, \
+                                              __LINE__, #call, (int)r_);                        \
+    } while (0)
+
+// per-particle parameter record [P][PP_COUNT] (doubles)
+enum {
+    PP_NORM = 0,  // NORM
+    PP_DX,        // round(XOFF)
+    PP_DY,        // round(YOFF)
+    PP_DU,        // CTF defocus U, V, angle, voltage, Cs, Q0, B-factor
+    PP_DV,
+    PP_DANG,
+    PP_KV,
+    PP_CS,
+    PP_Q0,
+    PP_BFAC,
+    PP_GROUP,
+    PP_COUNT = 12
+};
+
+// per-particle CTF constants [P][CK_COUNT] (CTF::initialise)
+enum { CK_K1 = 0, CK_K2, CK_K3, CK_K4, CK_AVG, CK_DEV, CK_C2, CK_S2, CK_Q0, CK_COUNT };
+
+// cuFFT plans of one (image size, chunk) pair
+struct PrepPlan {
+    cufftHandle fwd = 0;  // D2Z 2D n x n, batch chunk
+    cufftHandle col = 0;  // Z2Z 1D along rows of the (row, image) layout, batch chunk * (n/2+1)
+    cufftHandle row = 0;  // Z2D 1D, batch n * chunk
+};
+
+struct PrepPlans {
+    std::map<std::pair<int, int>, PrepPlan> plans;
+    long tick = 0;
+    std::map<std::pair<int, int>, long> used;
+};
+
+void destroy_plan(PrepPlan& p) {
+    if (p.fwd) cufftDestroy(p.fwd);
+    if (p.col) cufftDestroy(p.col);
+    if (p.row) cufftDestroy(p.row);
+    p = PrepPlan{};
+}
+
+PrepPlan& get_plan(RomeGpuCtx* ctx, int n, int chunk) {
+    if (!ctx->prep_plans) ctx->prep_plans = new PrepPlans();
+    auto* pp = (PrepPlans*)ctx->prep_plans;
+    const auto key = std::make_pair(n, chunk);
+    pp->used[key] = ++pp->tick;
+    auto it = pp->plans.find(key);
+    if (it != pp->plans.end()) return it->second;
+    // keep a few plan sets (a full chunk and the remainders of recent pools)
+    while (pp->plans.size() >= 4) {
+        auto old = pp->plans.begin();
+        for (auto jt = pp->plans.begin(); jt != pp->plans.end(); ++jt)
+            if (pp->used[jt->first] < pp->used[old->first]) old = jt;
+        destroy_plan(old->second);
+        pp->used.erase(old->first);
+        pp->plans.erase(old);
+    }
+    PrepPlan p;
+    const int oF = n / 2 + 1;
+    try {
+        int dims[2] = {n, n};
+        ROME_CUFFT(cufftPlanMany(&p.fwd, 2, dims, nullptr, 1, 0, nullptr, 1, 0, CUFFT_D2Z, chunk));
+        int n1[1] = {n};
+        int emb_c[1] = {n};
+        ROME_CUFFT(cufftPlanMany(&p.col, 1, n1, emb_c, chunk * oF, 1, emb_c, chunk * oF, 1, CUFFT_Z2Z, chunk * oF));
+        int emb_in[1] = {oF}, emb_out[1] = {n};
+        ROME_CUFFT(cufftPlanMany(&p.row, 1, n1, emb_in, 1, oF, emb_out, 1, n, CUFFT_Z2D, n * chunk));
+        ROME_CUFFT(cufftSetStream(p.fwd, ctx->stream));
+        ROME_CUFFT(cufftSetStream(p.col, ctx->stream));
+        ROME_CUFFT(cufftSetStream(p.row, ctx->stream));
+    } catch (...) {
+        destroy_plan(p);
+        throw;
+    }
+    return pp->plans.emplace(key, p).first->second;
+}
+
+// ---------------------------------------------------------------------------
+// The reference's seeded noise generator.  Random_generator with
+// MAP3D_OLD_BASELINE (src/math.h:35, src/math.cpp:361-388) is std::srand /
+// std::rand, i.e. glibc's TYPE_3 additive feedback generator: a table of 31
+// words r[0] = seed, r[i] = 16807 r[i-1] mod (2^31 - 1); then the words
+// y_s = y_{s-31} + y_{s-3} (mod 2^32) with y_{-31+i} = r[(i + 3) mod 31], the
+// s-th output being y_s >> 1, and the first 310 outputs discarded.
+// Uniforms are (float)rand() / (float)RAND_MAX (RAND_MAX rounds to 2^31), and
+// rnd_gaus (src/math.cpp:443-480) is the polar Box-Muller method on them with
+// W = pow(U1, 2) + pow(U2, 2) in double rounded to float and the multiplier
+// sqrt(-2 log W / W) in double rounded to float.
+//
+// One warp per image.  Lane j (< 31) holds word j of the window of the last
+// 31 words; the next 31 words follow in one step, as
+//   y_{k+j} = y_{k+j-31} + y_{k+j-3} = sum_{m >= 0} W[j - 3m] + W[28 + j mod 3],
+// a prefix sum of stride 3 over the lanes.  Two steps give 62 outputs, i.e.
+// 31 Box-Muller attempts in sequence order, one per lane; a ballot ranks the
+// accepted ones, and the m-th accepted attempt of the image fills the m-th
+// drawing pixel (its real part from X1, its imaginary part from the cached X2,
+// as rnd_gaus returns them on two consecutive calls).
+constexpr unsigned kFull = 0xffffffffu;
+constexpr long kM31 = 2147483647L;
+
+__device__ __forceinline__ uint32_t glibc_step(uint32_t& W, int lane) {
+    uint32_t T = W;
+#pragma unroll
+    for (int d = 3; d < 31; d *= 2) {  // 3, 6, 12, 24
+        const uint32_t v = __shfl_up_sync(kFull, T, d);
+        if (lane >= d) T += v;
+    }
+    const uint32_t y = T + __shfl_sync(kFull, W, 28 + lane % 3);
+    W = y;
+    return y >> 1;
+}
+
+__device__ __forceinline__ float rand_uniform01(uint32_t v) {
+    return __fdiv_rn(__uint2float_rn(v), 2147483648.0f);
+}
+
+// one Box-Muller attempt: U1, U2 and whether W is inside the unit circle
+__device__ __forceinline__ bool polar_attempt(uint32_t v1, uint32_t v2, float& U1, float& U2) {
+    U1 = __fadd_rn(-1.0f, __fmul_rn(rand_uniform01(v1), 2.0f));
+    U2 = __fadd_rn(-1.0f, __fmul_rn(rand_uniform01(v2), 2.0f));
+    const double d1 = (double)U1, d2 = (double)U2;
+    const float W = __double2float_rn(__dadd_rn(__dmul_rn(d1, d1), __dmul_rn(d2, d2)));
+    return !(W >= 1.0f || W == 0.0f);
+}
+
+__device__ __forceinline__ float polar_multiplier(float U1, float U2) {
+    const double d1 = (double)U1, d2 = (double)U2;
+    const double W = (double)__double2float_rn(__dadd_rn(__dmul_rn(d1, d1), __dmul_rn(d2, d2)));
+    return __double2float_rn(__dsqrt_rn(__ddiv_rn(-2.0 * log(W), W)));
+}
+
+// Noise spectra of the images of a chunk, written as double2 in the (row,
+// image) layout of the column transform, NC[(i * chunk + c) * oF + j], drawn in
+// the reference's fill order (src/exp_model.h:509-534): row i, column j, real
+// then imaginary part; a pixel draws when its shell ires = round(|(i', j)|)
+// is < n/2+1 and its sigma sqrt(sigma2_fudge * sigma2_noise[group][ires]),
+// rounded to float, is not zero (rnd_gaus returns mu without a draw for a
+// zero sigma); the other pixels are zero.  Groups with the same zero shells
+// share a pattern: pat_of_group [G]; per pattern, the drawing pixels in fill
+// order (draw_pix from draw_start, draw_count of them) and the others
+// (zero_pix from zero_start, zero_count).  sigf: [G][n/2+1].
+constexpr int kNoiseWarps = 8;
+
+__global__ void __launch_bounds__(kNoiseWarps * 32) noise_spectra_kernel(
+    int P, int npix, int oF, uint32_t seed0, const double* __restrict__ part, const int* __restrict__ pat_of_group,
+    const int* __restrict__ draw_start, const int* __restrict__ draw_count, const int* __restrict__ draw_pix,
+    const int* __restrict__ zero_start, const int* __restrict__ zero_count, const int* __restrict__ zero_pix,
+    const unsigned short* __restrict__ ires_tab, const float* __restrict__ sigf, double2* __restrict__ out) {
+    const int img = blockIdx.x * kNoiseWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (img >= P) return;  // whole warps leave together
+    const int g = (int)part[(size_t)img * PP_COUNT + PP_GROUP], pat = pat_of_group[g];
+    const float* sig = sigf + (size_t)g * oF;
+    // seeding (srandom_r): lane i holds r[i] = 16807^i r[0] mod (2^31 - 1), i >= 1
+    uint32_t seed = seed0 + (uint32_t)img;
+    if (seed == 0) seed = 1;
+    const int32_t r0 = (int32_t)seed;
+    uint32_t init = (uint32_t)r0;
+    if (lane >= 1 && lane < 31) {
+        long w = (long)r0 % kM31;
+        if (w < 0) w += kM31;
+        long a = 1;
+        for (int i = 0; i < lane; ++i) a = (a * 16807L) % kM31;
+        init = (uint32_t)((a * w) % kM31);
+    }
+    uint32_t W = __shfl_sync(kFull, init, lane < 31 ? (lane + 3) % 31 : 0);
+    if (lane == 31) W = 0;
+    for (int k = 0; k < 10; ++k) glibc_step(W, lane);  // 310 outputs discarded
+    const int need = draw_count[pat];
+    const int* dp = draw_pix + draw_start[pat];
+    int base = 0;
+    while (base < need) {
+        const uint32_t A = glibc_step(W, lane), B = glibc_step(W, lane);
+        // attempt `lane` uses outputs 2 lane and 2 lane + 1 of the 62
+        const int v1 = 2 * lane, v2 = 2 * lane + 1;
+        const uint32_t a1 = __shfl_sync(kFull, A, v1 < 31 ? v1 : 0), b1 = __shfl_sync(kFull, B, v1 >= 31 ? v1 - 31 : 0);
+        const uint32_t a2 = __shfl_sync(kFull, A, v2 < 31 ? v2 : 0), b2 = __shfl_sync(kFull, B, v2 >= 31 ? v2 - 31 : 0);
+        float U1 = 0.f, U2 = 0.f;
+        const bool ok = lane < 31 && polar_attempt(v1 < 31 ? a1 : b1, v2 < 31 ? a2 : b2, U1, U2);
+        const unsigned mask = __ballot_sync(kFull, ok);
+        const int m = base + __popc(mask & ((1u << lane) - 1u));
+        if (ok && m < need) {
+            const int q = dp[m];
+            const float s = sig[ires_tab[q]];
+            const float mult = polar_multiplier(U1, U2);
+            const float X1 = __fmul_rn(U1, mult), X2 = __fmul_rn(U2, mult);
+            const int i = q / oF;
+            out[((size_t)i * P + img) * oF + (q - i * oF)] =
+                make_double2((double)__fadd_rn(0.0f, __fmul_rn(s, X1)), (double)__fadd_rn(0.0f, __fmul_rn(s, X2)));
+        }
+        base += __popc(mask);
+    }
+    const int* zp = zero_pix + zero_start[pat];
+    for (int k = lane; k < zero_count[pat]; k += 32) {
+        const int q = zp[k], i = q / oF;
+        out[((size_t)i * P + img) * oF + (q - i * oF)] = make_double2(0.0, 0.0);
+    }
+}
+
+// value of the norm-corrected, translated image at (a, b): exp_image after
+// `translate(tempImage, exp_image, ori, round(XOFF), round(YOFF), DONT_WRAP)`;
+// an integer shift makes applyGeometry's bilinear weights 0 / 1, so it is a
+// copy from (a - dy, b - dx) with zeros where that leaves the image
+template <typename T>
+__device__ __forceinline__ double translated_at(const T* __restrict__ img, int n, int a, int b, int dx, int dy,
+                                                int do_norm, double avg, double norm) {
+    const int sa = a - dy, sb = b - dx;
+    if (sa < 0 || sa >= n || sb < 0 || sb >= n) return 0.0;
+    double v = (double)img[(size_t)sa * n + sb];
+    if (do_norm) v = __ddiv_rn(__dmul_rn(v, avg), norm);
+    return v;
+}
+
+// The per-pixel kernels below run a 2D grid: x over the pixels of one image,
+// y over the images of the chunk (looping when there are more than 65535).
+
+// CenterFFT(forward) of the translated image: out[i][j] = t[(i - n/2) mod n][(j - n/2) mod n].
+// Each thread handles 4 pixels 256 apart (4 loads in flight); blocks of 256.
+template <typename T>
+__global__ void translate_center_kernel(int chunk, int n, const T* __restrict__ raw, const double* __restrict__ part,
+                                        int do_norm, double avg, double* __restrict__ out) {
+    const int nn = n * n, h = n / 2;
+    for (int p = blockIdx.y; p < chunk; p += gridDim.y) {
+        const double* pp = part + (size_t)p * PP_COUNT;
+        const int dx = (int)pp[PP_DX], dy = (int)pp[PP_DY];
+        const double norm = pp[PP_NORM];
+        const T* img = raw + (size_t)p * nn;
+        for (int q0 = blockIdx.x * 1024 + threadIdx.x; q0 < nn; q0 += gridDim.x * 1024) {
+            double v[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + 256 * k;
+                v[k] = 0.0;
+                if (q < nn) {
+                    const int i = q / n, j = q - (q / n) * n;
+                    const int a = i - h < 0 ? i - h + n : i - h, b = j - h < 0 ? j - h + n : j - h;
+                    v[k] = translated_at(img, n, a, b, dx, dy, do_norm, avg, norm);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (q0 + 256 * k < nn) out[(size_t)p * nn + q0 + 256 * k] = v[k];
+        }
+    }
+}
+
+// windowFourierTransform of the normalised transform: F [chunk][n][n/2+1]
+// (unnormalised) -> out [chunk][fine][fine/2+1], component / n^2
+__global__ void window_kernel(int chunk, int n, int fine, const double2* __restrict__ F, double* __restrict__ out_re,
+                              double* __restrict__ out_im) {
+    const int oF = n / 2 + 1, fF = fine / 2 + 1, per = fine * fF;
+    const double nn = (double)n * (double)n;
+    for (int p = blockIdx.y; p < chunk; p += gridDim.y) {
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < per; q += gridDim.x * blockDim.x) {
+            const int i = q / fF, j = q - (q / fF) * fF;
+            const int ip = i < fF ? i : i - fine;
+            const int si = ip < 0 ? ip + n : ip;
+            const double2 v = F[((size_t)p * n + si) * oF + j];
+            out_re[(size_t)p * per + q] = __ddiv_rn(v.x, nn);
+            out_im[(size_t)p * per + q] = __ddiv_rn(v.y, nn);
+        }
+    }
+}
+
+// after the column DFTs: each row's C2R reads only the real part of its x = 0
+// and x = n/2 entries (what FFTW's half-complex backward transform does)
+__global__ void real_edges_kernel(long rows, int oF, int n, double2* __restrict__ nc) {
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += (long)gridDim.x * blockDim.x) {
+        nc[r * oF].y = 0.0;
+        if ((n & 1) == 0) nc[r * oF + n / 2].y = 0.0;
+    }
+}
+
+// softMaskOutsideMap's background average (no noise image): sum of w * value
+// over the pixels at r >= radius divided by sum of w.  mw: the mask weight of
+// every uncentred pixel (< 0 inside the radius, the raised cosine in the edge
+// band, > 1 beyond radius + width, where w = 1).  One block of 256 per image.
+template <typename T>
+__global__ void background_kernel(int n, const T* __restrict__ raw, const double* __restrict__ part, int do_norm,
+                                  double avg, const double* __restrict__ mw, double* __restrict__ bg) {
+    const int p = blockIdx.x;
+    const double* pp = part + (size_t)p * PP_COUNT;
+    const T* img = raw + (size_t)p * n * n;
+    const int dx = (int)pp[PP_DX], dy = (int)pp[PP_DY];
+    double s = 0.0, sw = 0.0;
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+        const double w0 = mw[q];
+        if (w0 < 0.0) continue;
+        const double w = w0 > 1.0 ? 1.0 : w0;
+        const int a = q / n, b = q - (q / n) * n;
+        s += w * translated_at(img, n, a, b, dx, dy, do_norm, avg, pp[PP_NORM]);
+        sw += w;
+    }
+    __shared__ double red[2][256];
+    red[0][threadIdx.x] = s;
+    red[1][threadIdx.x] = sw;
+    __syncthreads();
+    for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            red[0][threadIdx.x] += red[0][threadIdx.x + k];
+            red[1][threadIdx.x] += red[1][threadIdx.x + k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) bg[p] = red[0][0] / red[1][0];
+}
+
+// softMaskOutsideMap of the translated image, written centred (CenterFFT):
+// inside the radius the pixel stays, in the edge band it becomes
+// (1 - w) * value + w * add, beyond it `add` -- the noise image at the same
+// uncentred pixel, or the background average
+template <typename T>
+__global__ void mask_center_kernel(int chunk, int n, const T* __restrict__ raw, const double* __restrict__ part,
+                                   int do_norm, double avg, const double* __restrict__ mw,
+                                   const double* __restrict__ noise_img, const double* __restrict__ bg,
+                                   double* __restrict__ out) {
+    const int nn = n * n, h = n / 2;
+    for (int p = blockIdx.y; p < chunk; p += gridDim.y) {
+        const double* pp = part + (size_t)p * PP_COUNT;
+        const int dx = (int)pp[PP_DX], dy = (int)pp[PP_DY];
+        const double norm = pp[PP_NORM];
+        const T* img = raw + (size_t)p * nn;
+        for (int q0 = blockIdx.x * 1024 + threadIdx.x; q0 < nn; q0 += gridDim.x * 1024) {
+            double v[4], w[4], add[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int q = q0 + 256 * k;
+                v[k] = 0.0;
+                w[k] = -1.0;
+                add[k] = 0.0;
+                if (q < nn) {
+                    const int i = q / n, j = q - (q / n) * n;
+                    const int a = i - h < 0 ? i - h + n : i - h, b = j - h < 0 ? j - h + n : j - h;
+                    v[k] = translated_at(img, n, a, b, dx, dy, do_norm, avg, norm);
+                    w[k] = mw[a * n + b];
+                    add[k] = noise_img ? noise_img[((size_t)a * chunk + p) * n + b] : bg[p];
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                double x = v[k];
+                if (w[k] >= 0.0) x = w[k] > 1.0 ? add[k] : (1 - w[k]) * v[k] + w[k] * add[k];
+                if (q0 + 256 * k < nn) out[(size_t)p * nn + q0 + 256 * k] = x;
+            }
+        }
+    }
+}
+
+// power spectrum of the masked, normalised transform over shells 1..n/2
+// (the x = 0 column's negative rows skipped) and highres_Xi2, the sum over
+// shells >= current_size/2+1.  One block per image; thread s sums shell s
+// over its pixels in row-major order (the reference's order within a shell).
+// shell_start [oF+1], shell_pix: pixel indices i * oF + j by shell.
+__global__ void power_kernel(int n, int fine, const double2* __restrict__ F, const int* __restrict__ shell_start,
+                             const int* __restrict__ shell_pix, double* __restrict__ power, double* __restrict__ xi2) {
+    const int p = blockIdx.x, oF = n / 2 + 1, fF = fine / 2 + 1;
+    const double nn = (double)n * (double)n;
+    const double2* f = F + (size_t)p * n * oF;
+    extern __shared__ double spec[];
+    for (int s = threadIdx.x; s < oF; s += blockDim.x) {
+        double acc = 0.0;
+        for (int k = shell_start[s]; k < shell_start[s + 1]; ++k) {
+            const double2 v = f[shell_pix[k]];
+            const double re = __ddiv_rn(v.x, nn), im = __ddiv_rn(v.y, nn);
+            acc += re * re + im * im;
+        }
+        spec[s] = acc;
+        power[(size_t)p * oF + s] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double x = 0.0;
+        for (int s = fF; s < oF; ++s) x += spec[s];
+        xi2[p] = x;
+    }
+}
+
+// CTF::initialise (src/ctf.cpp:136-171) per particle: [P][CK_COUNT]
+__global__ void ctf_constants_kernel(int P, const double* __restrict__ part, double* __restrict__ ck) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const double* pp = part + (size_t)p * PP_COUNT;
+    double* k = ck + (size_t)p * CK_COUNT;
+    const double local_cs = pp[PP_CS] * 1e7, local_kv = pp[PP_KV] * 1e3;
+    const double rad_az = pp[PP_DANG] * kPi / 180.0;
+    const double lambda = 12.2643247 / sqrt(local_kv * (1. + local_kv * 0.978466e-6));
+    k[CK_K1] = kPi / 2 * 2 * lambda;
+    k[CK_K2] = kPi / 2 * local_cs * lambda * lambda * lambda;
+    k[CK_K3] = sqrt(1 - pp[PP_Q0] * pp[PP_Q0]);
+    k[CK_K4] = -pp[PP_BFAC] / 4.;
+    k[CK_AVG] = -(pp[PP_DU] + pp[PP_DV]) * 0.5;
+    k[CK_DEV] = -(pp[PP_DU] - pp[PP_DV]) * 0.5;
+    k[CK_C2] = cos(2 * rad_az);
+    k[CK_S2] = sin(2 * rad_az);
+    k[CK_Q0] = pp[PP_Q0];
+}
+
+// CTF::getFftwImage(fine, ori, ori, angpix, do_abs, only_flip, intact_first_peak,
+// damping on) (src/ctf.cpp:173-191, getCTF / getDeltaF src/ctf.h:151-204);
+// cos(2 (atan2(Y, X) - azimuth)) as ((X^2 - Y^2) cos 2az + 2XY sin 2az) / |u|^2
+__global__ void ctf_kernel(int P, int fine, int ori, double angpix, const double* __restrict__ ck, int do_abs,
+                           int only_flip, int intact, double* __restrict__ out) {
+    const int fF = fine / 2 + 1, per = fine * fF;
+    const double xs = (double)ori * angpix;
+    for (int p = blockIdx.y; p < P; p += gridDim.y) {
+        const double* k = ck + (size_t)p * CK_COUNT;
+        const double K1 = k[CK_K1], K2 = k[CK_K2], K3 = k[CK_K3], K4 = k[CK_K4], avg = k[CK_AVG], dev = k[CK_DEV],
+                     c2 = k[CK_C2], s2 = k[CK_S2], q0 = k[CK_Q0];
+        for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < per; q += gridDim.x * blockDim.x) {
+            const int i = q / fF, j = q - (q / fF) * fF;
+            const int ip = i < fF ? i : i - fine;
+            const double X = (double)j / xs, Y = (double)ip / xs;
+            const double u2 = X * X + Y * Y, u4 = u2 * u2;
+            const double deltaf =
+                (fabs(X) < 1e-6 && fabs(Y) < 1e-6) ? 0.0 : avg + dev * (((X * X - Y * Y) * c2 + 2 * X * Y * s2) / u2);
+            const double arg = K1 * deltaf * u2 + K2 * u4;
+            double v;
+            if (intact && fabs(arg) < kPi / 2.) {
+                v = 1.;
+            } else {
+                double sn, cs;
+                sincos(arg, &sn, &cs);
+                v = -(K3 * sn - q0 * cs);
+            }
+            if (K4 != 0.0) v *= exp(K4 * u2);
+            if (do_abs) v = fabs(v);
+            else if (only_flip) v = v < 0. ? -1. : 1.;
+            out[(size_t)p * per + q] = v;
+        }
+    }
+}
+
+}  // namespace
+
+namespace {
+
+__global__ void fill_kernel(double* __restrict__ x, size_t n, double v) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) x[i] = v;
+}
+
+unsigned grid_for(size_t total, int threads = 256) {
+    return (unsigned)std::max<size_t>(1, std::min<size_t>((total + threads - 1) / threads, 148 * 16));
+}
+
+size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// 2D grid of the per-pixel kernels: x covers `per_image` elements with 256
+// threads, y the images (at most 65535; the kernels loop over the rest)
+dim3 grid2(size_t per_image, int images) {
+    return dim3((unsigned)std::max<size_t>(1, (per_image + 255) / 256), (unsigned)std::max(1, std::min(images, 65535)));
+}
+
+// C round(): halfway cases away from zero
+double c_round(double x) { return std::round(x); }
+
+template <typename T>
+void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
+    const int P = in.nr_images, n = in.ori_size, fine = in.current_size, G = in.nr_groups;
+    const int oF = n / 2 + 1, fF = fine / 2 + 1;
+    const size_t npix = (size_t)n * oF, Ff = (size_t)fine * fF, nn = (size_t)n * n;
+    const bool noise = !in.do_zero_mask;
+    cudaStream_t st = ctx->stream;
+    Profiler prof(ctx);
+
+    // ---- host side: per-particle parameters, old offsets, tables ----
+    std::vector<double> part((size_t)P * PP_COUNT, 0.0);
+    for (int p = 0; p < P; ++p) {
+        const int g = in.group[p];
+        ROME_REQUIRE(g >= 0 && g < G, "particle %d: group %d outside [0, %d)", p, g, G);
+        if (in.do_norm_correction) ROME_REQUIRE(in.norm[p] != 0.0, "particle %d: NORM is zero", p);
+        if (in.do_ctf_correction) {
+            // CTF::initialise's checks (src/ctf.cpp:163-168)
+            if (in.ctf_q0[p] < 0. || in.ctf_q0[p] > 1.)
+                fail(ROME_ERR_ARG, "particle %d: amplitude contrast Q0 = %g outside [0, 1]", p, in.ctf_q0[p]);
+            if (std::fabs(in.ctf_defocus_u[p]) < 1e-6 && std::fabs(in.ctf_defocus_v[p]) < 1e-6 &&
+                std::fabs(in.ctf_q0[p]) < 1e-6 && std::fabs(in.ctf_cs[p]) < 1e-6)
+                fail(ROME_ERR_ARG, "particle %d: CTF parameters are all zero", p);
+        }
+        double* r = &part[(size_t)p * PP_COUNT];
+        r[PP_NORM] = in.norm[p];
+        const double ox = c_round(in.xoff[p]), oy = c_round(in.yoff[p]);
+        ROME_REQUIRE(std::fabs(ox) < 1e9 && std::fabs(oy) < 1e9, "particle %d: offset out of range", p);
+        out.old_offsetx[p] = ox;
+        out.old_offsety[p] = oy;
+        r[PP_DX] = ox;
+        r[PP_DY] = oy;
+        if (in.do_ctf_correction) {
+            r[PP_DU] = in.ctf_defocus_u[p];
+            r[PP_DV] = in.ctf_defocus_v[p];
+            r[PP_DANG] = in.ctf_defocus_angle[p];
+            r[PP_KV] = in.ctf_voltage[p];
+            r[PP_CS] = in.ctf_cs[p];
+            r[PP_Q0] = in.ctf_q0[p];
+            r[PP_BFAC] = in.ctf_bfac[p];
+        }
+        r[PP_GROUP] = g;
+    }
+    // shell of every half-plane pixel, round(sqrt(i'^2 + j^2)) (src/exp_model.h:514-516)
+    std::vector<unsigned short> ires(npix);
+    for (int i = 0; i < n; ++i) {
+        const int ip = i < oF ? i : i - n;
+        for (int j = 0; j < oF; ++j) ires[(size_t)i * oF + j] = (unsigned short)std::round(std::sqrt((double)(ip * ip + j * j)));
+    }
+    std::vector<float> sigf((size_t)G * oF, 0.f);
+    // groups with the same zero-sigma shells share one list of drawing pixels
+    std::vector<int> pat_of_group(G, 0), draw_start, draw_count, draw_pix, zero_start, zero_count, zero_pix;
+    if (noise) {
+        std::map<std::vector<int>, int> patterns;
+        for (int g = 0; g < G; ++g) {
+            std::vector<int> zero_shells;
+            for (int s = 0; s < oF; ++s) {
+                const double pw = in.sigma2_fudge * in.sigma2_noise[(size_t)g * oF + s];
+                ROME_REQUIRE(pw >= 0.0, "sigma2_noise[%d][%d] is negative", g, s);
+                sigf[(size_t)g * oF + s] = (float)std::sqrt(pw);
+                if (sigf[(size_t)g * oF + s] == 0.f) zero_shells.push_back(s);
+            }
+            auto it = patterns.find(zero_shells);
+            if (it == patterns.end()) {
+                const int id = (int)patterns.size();
+                it = patterns.emplace(zero_shells, id).first;
+                std::vector<char> zs(oF, 0);
+                for (int s : zero_shells) zs[s] = 1;
+                draw_start.push_back((int)draw_pix.size());
+                zero_start.push_back((int)zero_pix.size());
+                for (size_t q = 0; q < npix; ++q) {
+                    if (ires[q] < oF && !zs[ires[q]]) draw_pix.push_back((int)q);
+                    else zero_pix.push_back((int)q);
+                }
+                draw_count.push_back((int)draw_pix.size() - draw_start.back());
+                zero_count.push_back((int)zero_pix.size() - zero_start.back());
+            }
+            pat_of_group[g] = it->second;
+        }
+    }
+    // shells 1..oF-1 of the power spectrum, pixels in row-major order, the
+    // negative rows of the x = 0 column skipped (src/exp_model.h:576-595)
+    std::vector<int> shell_start(oF + 1, 0), shell_pix;
+    {
+        std::vector<std::vector<int>> by(oF);
+        for (int i = 0; i < n; ++i) {
+            const int ip = i < oF ? i : i - n;
+            for (int j = 0; j < oF; ++j) {
+                const int s = ires[(size_t)i * oF + j];
+                if (s > 0 && s < oF && !(j == 0 && ip < 0)) by[s].push_back(i * oF + j);
+            }
+        }
+        for (int s = 0; s < oF; ++s) {
+            shell_start[s + 1] = shell_start[s] + (int)by[s].size();
+            shell_pix.insert(shell_pix.end(), by[s].begin(), by[s].end());
+        }
+    }
+
+    // ---- device buffers ----
+    double* d_part = ctx->ws[S_PREP_PART].as<double>(part.size());
+    stage_copy(ctx, d_part, part.data(), part.size());
+    // one table buffer: shells, noise patterns and sigmas, power shells, per-image sums
+    size_t tab_bytes = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t at = tab_bytes;
+        tab_bytes += align256(std::max<size_t>(bytes, 1));
+        return at;
+    };
+    const size_t o_ires = carve(npix * 2), o_sig = carve(sigf.size() * 4), o_pog = carve((size_t)G * 4),
+                 o_dst = carve(draw_start.size() * 4), o_dcn = carve(draw_count.size() * 4),
+                 o_dpx = carve(draw_pix.size() * 4), o_zst = carve(zero_start.size() * 4),
+                 o_zcn = carve(zero_count.size() * 4), o_zpx = carve(zero_pix.size() * 4),
+                 o_ss = carve(shell_start.size() * 4), o_sp = carve(shell_pix.size() * 4), o_bg = carve((size_t)P * 8),
+                 o_xi2 = carve((size_t)P * 8), o_pow = carve((size_t)P * oF * 8), o_mw = carve(nn * 8),
+                 o_ctfk = carve((size_t)P * CK_COUNT * 8);
+    char* tab = (char*)ctx->ws[S_PREP_TAB].get(tab_bytes);
+    auto at = [&](size_t off) { return (void*)(tab + off); };
+    auto* d_ires = (unsigned short*)at(o_ires);
+    auto* d_sig = (float*)at(o_sig);
+    auto* d_ss = (int*)at(o_ss);
+    auto* d_sp = (int*)at(o_sp);
+    auto* d_bg = (double*)at(o_bg);
+    auto* d_xi2 = (double*)at(o_xi2);
+    auto* d_pow = (double*)at(o_pow);
+    auto* d_mw = (double*)at(o_mw);
+    auto* d_ctfk = (double*)at(o_ctfk);
+    stage_copy(ctx, d_ires, ires.data(), ires.size());
+    if (noise) {
+        stage_copy(ctx, d_sig, sigf.data(), sigf.size());
+        stage_copy(ctx, (int*)at(o_pog), pat_of_group.data(), pat_of_group.size());
+        stage_copy(ctx, (int*)at(o_dst), draw_start.data(), draw_start.size());
+        stage_copy(ctx, (int*)at(o_dcn), draw_count.data(), draw_count.size());
+        stage_copy(ctx, (int*)at(o_dpx), draw_pix.data(), draw_pix.size());
+        stage_copy(ctx, (int*)at(o_zst), zero_start.data(), zero_start.size());
+        stage_copy(ctx, (int*)at(o_zcn), zero_count.data(), zero_count.size());
+        stage_copy(ctx, (int*)at(o_zpx), zero_pix.data(), zero_pix.size());
+    }
+    stage_copy(ctx, d_ss, shell_start.data(), shell_start.size());
+    stage_copy(ctx, d_sp, shell_pix.data(), shell_pix.size());
+    // softMaskOutsideMap's weight of every (uncentred) pixel: < 0 inside the
+    // radius, the raised cosine in the edge band, > 1 beyond it
+    {
+        const double radius = in.particle_diameter / (2. * in.pixel_size), width = (double)in.width_mask_edge;
+        const double radius_p = radius + width;
+        const int origin = -(n / 2);
+        std::vector<double> mw(nn);
+        for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b) {
+                const double r = std::sqrt((double)((a + origin) * (a + origin) + (b + origin) * (b + origin)));
+                mw[(size_t)a * n + b] = r < radius ? -1.0 : r <= radius_p ? 0.5 + 0.5 * std::cos(kPi * (radius_p - r) / width) : 2.0;
+            }
+        stage_copy(ctx, d_mw, mw.data(), mw.size());
+    }
+
+    double *o_re, *o_im, *o_nre, *o_nim, *o_ctf;
+    if (out.outputs_on_device) {
+        o_re = out.Fimg_real;
+        o_im = out.Fimg_imag;
+        o_nre = out.Fimg_nomask_real;
+        o_nim = out.Fimg_nomask_imag;
+        o_ctf = out.Fctf;
+    } else {
+        double* b = ctx->ws[S_PREP_OUT].as<double>(5 * (size_t)P * Ff);
+        o_re = b;
+        o_im = b + (size_t)P * Ff;
+        o_nre = b + 2 * (size_t)P * Ff;
+        o_nim = b + 3 * (size_t)P * Ff;
+        o_ctf = b + 4 * (size_t)P * Ff;
+    }
+
+    prof.begin(ROME_PHASE_IMAGES);
+    // chunks of equal size bounded by the work buffers' footprint
+    const size_t per_img = nn * 8 + npix * 16 + (noise ? npix * 16 + nn * 8 : 0) + (in.images_on_device ? 0 : nn * sizeof(T));
+    const size_t budget = ctx->workspace_limit ? ctx->workspace_limit : (size_t)1536 << 20;
+    // (cuFFT's 32-bit plans: a chunk holds fewer than 2^31 elements)
+    const int cmax = (int)std::max<size_t>(1, std::min<size_t>({(size_t)P, budget / per_img, (size_t)2147483647 / nn}));
+    const int nchunk = (P + cmax - 1) / cmax, chunk = (P + nchunk - 1) / nchunk;
+    double* d_R = ctx->ws[S_PREP_R].as<double>((size_t)chunk * nn);
+    double2* d_C = ctx->ws[S_PREP_C].as<double2>((size_t)chunk * npix);
+    double2* d_NC = noise ? ctx->ws[S_PREP_NC].as<double2>((size_t)chunk * npix) : nullptr;
+    double* d_NR = noise ? ctx->ws[S_PREP_NR].as<double>((size_t)chunk * nn) : nullptr;
+    const T* d_raw_all = in.images_on_device ? (const T*)in.images : nullptr;
+    T* d_raw_chunk = in.images_on_device ? nullptr : ctx->ws[S_PREP_RAW].as<T>((size_t)chunk * nn);
+    const int norm_on = in.do_norm_correction ? 1 : 0;
+    const uint32_t seed0 = (uint32_t)(in.random_seed + in.first_image);
+    const double avg = in.avg_norm_correction;
+
+    for (int c0 = 0; c0 < P; c0 += chunk) {
+        const int pc = std::min(chunk, P - c0);
+        const T* raw;
+        if (in.images_on_device) {
+            raw = d_raw_all + (size_t)c0 * nn;
+        } else {
+            ROME_CUDA(cudaMemcpyAsync(d_raw_chunk, (const T*)in.images + (size_t)c0 * nn, (size_t)pc * nn * sizeof(T),
+                                      cudaMemcpyHostToDevice, st));
+            raw = d_raw_chunk;
+        }
+        const double* pp = d_part + (size_t)c0 * PP_COUNT;
+        PrepPlan& plan = get_plan(ctx, n, pc);
+        // unmasked image
+        translate_center_kernel<T><<<grid2((nn + 3) / 4, pc), 256, 0, st>>>(pc, n, raw, pp, norm_on, avg, d_R);
+        ROME_CHECK_LAUNCH();
+        ROME_CUFFT(cufftExecD2Z(plan.fwd, d_R, (cufftDoubleComplex*)d_C));
+        window_kernel<<<grid2(Ff, pc), 256, 0, st>>>(pc, n, fine, d_C, o_nre + (size_t)c0 * Ff, o_nim + (size_t)c0 * Ff);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_IMAGES, 2);
+        // noise image or background average
+        if (noise) {
+            noise_spectra_kernel<<<(pc + kNoiseWarps - 1) / kNoiseWarps, kNoiseWarps * 32, 0, st>>>(
+                pc, (int)npix, oF, seed0 + (uint32_t)c0, pp, (const int*)at(o_pog), (const int*)at(o_dst),
+                (const int*)at(o_dcn), (const int*)at(o_dpx), (const int*)at(o_zst), (const int*)at(o_zcn),
+                (const int*)at(o_zpx), d_ires, d_sig, d_NC);
+            ROME_CHECK_LAUNCH();
+            ROME_CUFFT(cufftExecZ2Z(plan.col, (cufftDoubleComplex*)d_NC, (cufftDoubleComplex*)d_NC, CUFFT_INVERSE));
+            real_edges_kernel<<<grid_for((size_t)n * pc), 256, 0, st>>>((long)n * pc, oF, n, d_NC);
+            ROME_CHECK_LAUNCH();
+            ROME_CUFFT(cufftExecZ2D(plan.row, (cufftDoubleComplex*)d_NC, d_NR));
+            prof.launched(ROME_PHASE_IMAGES, 2);
+        } else {
+            background_kernel<T><<<pc, 256, 0, st>>>(n, raw, pp, norm_on, avg, d_mw, d_bg + c0);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_IMAGES);
+        }
+        mask_center_kernel<T><<<grid2((nn + 3) / 4, pc), 256, 0, st>>>(pc, n, raw, pp, norm_on, avg, d_mw, d_NR,
+                                                                       d_bg + c0, d_R);
+        ROME_CHECK_LAUNCH();
+        ROME_CUFFT(cufftExecD2Z(plan.fwd, d_R, (cufftDoubleComplex*)d_C));
+        window_kernel<<<grid2(Ff, pc), 256, 0, st>>>(pc, n, fine, d_C, o_re + (size_t)c0 * Ff, o_im + (size_t)c0 * Ff);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_IMAGES, 2);
+        if (fine < n) {
+            power_kernel<<<pc, 128, oF * sizeof(double), st>>>(n, fine, d_C, d_ss, d_sp, d_pow + (size_t)c0 * oF,
+                                                                d_xi2 + c0);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_IMAGES);
+        }
+    }
+    if (fine >= n) {
+        ROME_CUDA(cudaMemsetAsync(d_xi2, 0, (size_t)P * 8, st));
+        ROME_CUDA(cudaMemsetAsync(d_pow, 0, (size_t)P * oF * 8, st));
+    }
+    if (in.do_ctf_correction) {
+        ctf_constants_kernel<<<(P + 127) / 128, 128, 0, st>>>(P, d_part, d_ctfk);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_IMAGES);
+        ctf_kernel<<<grid2(Ff, P), 256, 0, st>>>(P, fine, n, in.pixel_size, d_ctfk, in.ctf_phase_flipped ? 1 : 0,
+                                                 in.only_flip_phases ? 1 : 0, in.intact_ctf_first_peak ? 1 : 0, o_ctf);
+    } else {
+        fill_kernel<<<grid_for((size_t)P * Ff), 256, 0, st>>>(o_ctf, (size_t)P * Ff, 1.0);
+    }
+    ROME_CHECK_LAUNCH();
+    prof.launched(ROME_PHASE_IMAGES);
+    prof.end(ROME_PHASE_IMAGES);
+    // algorithmic traffic: images in, the five output arrays and the power spectra out
+    prof.add_bytes(ROME_PHASE_IMAGES, (double)P * ((double)nn * sizeof(T) + 5.0 * Ff * 8 + oF * 8.0));
+
+    ROME_CUDA(cudaMemcpyAsync(out.highres_Xi2, d_xi2, (size_t)P * 8, cudaMemcpyDeviceToHost, st));
+    if (out.power_imgs)
+        ROME_CUDA(cudaMemcpyAsync(out.power_imgs, d_pow, (size_t)P * oF * 8, cudaMemcpyDeviceToHost, st));
+    if (!out.outputs_on_device) {
+        double* dsts[5] = {out.Fimg_real, out.Fimg_imag, out.Fimg_nomask_real, out.Fimg_nomask_imag, out.Fctf};
+        double* srcs[5] = {o_re, o_im, o_nre, o_nim, o_ctf};
+        for (int k = 0; k < 5; ++k)
+            ROME_CUDA(cudaMemcpyAsync(dsts[k], srcs[k], (size_t)P * Ff * 8, cudaMemcpyDeviceToHost, st));
+    }
+    ROME_CUDA(cudaStreamSynchronize(st));
+    prof.collect();
+}
+
+}  // namespace
+
+void prep_release(RomeGpuCtx* ctx) {
+    if (!ctx || !ctx->prep_plans) return;
+    auto* pp = (PrepPlans*)ctx->prep_plans;
+    for (auto& kv : pp->plans) destroy_plan(kv.second);
+    delete pp;
+    ctx->prep_plans = nullptr;
+}
+
+}  // namespace rome
+
+using namespace rome;
+
+extern "C" int rome_gpu_prepare_particles(RomeGpuCtx* ctx, const RomePrepIn* in, RomePrepOut* out) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        ROME_REQUIRE(in && out, "null argument");
+        const RomePrepIn& a = *in;
+        ROME_REQUIRE(a.nr_images >= 0, "nr_images %d", a.nr_images);
+        if (a.nr_images == 0) return;
+        ROME_REQUIRE(a.ori_size >= 2 && a.ori_size % 2 == 0 && a.ori_size <= 4096, "ori_size %d: even sizes 2..4096",
+                     a.ori_size);
+        ROME_REQUIRE(a.current_size >= 1 && a.current_size <= a.ori_size, "current_size %d outside [1, ori_size]",
+                     a.current_size);
+        ROME_REQUIRE(a.nr_groups >= 1, "nr_groups %d", a.nr_groups);
+        ROME_REQUIRE(a.image_type == 0 || a.image_type == 1, "image_type %d", a.image_type);
+        ROME_REQUIRE(a.images && a.norm && a.xoff && a.yoff && a.group && a.sigma2_noise, "missing input array");
+        ROME_REQUIRE(!a.do_ctf_correction || (a.ctf_defocus_u && a.ctf_defocus_v && a.ctf_defocus_angle &&
+                                              a.ctf_voltage && a.ctf_cs && a.ctf_q0 && a.ctf_bfac),
+                     "missing CTF parameters");
+        ROME_REQUIRE(out->Fimg_real && out->Fimg_imag && out->Fimg_nomask_real && out->Fimg_nomask_imag && out->Fctf &&
+                         out->highres_Xi2 && out->old_offsetx && out->old_offsety,
+                     "missing output array");
+        ROME_REQUIRE(a.pixel_size > 0 && a.width_mask_edge >= 0, "pixel_size %g, width_mask_edge %d", a.pixel_size,
+                     a.width_mask_edge);
+        if (!a.do_zero_mask) {
+            // Random_generator::init(seed) seeds from the clock for seed < 0:
+            // not reproducible, so not supported
+            const long s0 = (long)a.random_seed + a.first_image, s1 = s0 + a.nr_images - 1;
+            ROME_REQUIRE(s0 >= 0 && s1 <= 2147483647L, "noise seeds %ld..%ld outside [0, 2^31)", s0, s1);
+        }
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        arena_reset(ctx);
+        if (a.image_type == 0)
+            run_prepare<double>(ctx, a, *out);
+        else
+            run_prepare<float>(ctx, a, *out);
+    });
+}

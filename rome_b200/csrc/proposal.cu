@@ -22,6 +22,8 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <numeric>
 #include <random>
 #include <vector>
@@ -627,13 +629,27 @@ void net_expand_head(RomeProposalNet* net, cudaStream_t st) {
     net->wt_dirty = false;
 }
 
+// Raise a kernel's dynamic shared memory limit to its cap, once.  The limit
+// is a property of the function shared by every host thread; setting it to
+// each launch's own size would let one thread lower it between another
+// thread's set and launch, so it is only ever raised, to the cap the launch
+// sites check against.
+void raise_smem_limit(const void* fn, int bytes) {
+    static std::mutex mu;
+    static std::map<const void*, int> limit;
+    std::lock_guard<std::mutex> g(mu);
+    int& cur = limit[fn];
+    if (cur >= bytes) return;
+    ROME_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    cur = bytes;
+}
+
 // one 3x3 polar convolution + ReLU over n samples
 void conv_forward(int Ci, int R, int A, int Co, int n, const float* x, const float* w, const float* b, float* y,
                   cudaStream_t st) {
     const size_t sm = pconv_smem_bytes(Ci, R, A, Co);
     if (Co % 4 == 0 && sm <= 96 * 1024) {
-        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sm));
+        raise_smem_limit((const void*)pconv_fwd_smem_kernel<true>, 96 * 1024);
         pconv_fwd_smem_kernel<true><<<n, PT, sm, st>>>(Ci, R, A, Co, x, w, b, y);
     } else {
         dim3 g((R * A + PT - 1) / PT, Co, n);
@@ -661,7 +677,7 @@ void conv_weight_grads(RomeProposalNet* net, int n, int Ci, int Co, const float*
     const size_t sm = wgrad_smem_bytes(Ci, R, A, Co);
     if (sm <= 200 * 1024) {
         const int nw = Co * Ci * 9, nb = Co;
-        ROME_CUDA(cudaFuncSetAttribute(conv_wgrad_sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        raise_smem_limit((const void*)conv_wgrad_sample_kernel, 200 * 1024);
         conv_wgrad_sample_kernel<<<n, PT, sm, st>>>(Ci, R, A, Co, x, dy, net->wpart);
         conv_grad_reduce_kernel<<<(nw + nb + PT - 1) / PT, PT, 0, st>>>(n, nw, nb, net->wpart, dw, db);
     } else {
@@ -695,8 +711,7 @@ void net_backward(RomeProposalNet* net, int n, cudaStream_t st) {
     if (net->c0 % 4 == 0 && smd <= 96 * 1024) {
         flip_weights_kernel<<<(net->c1 * net->c0 * 9 + PT - 1) / PT, PT, 0, st>>>(net->c1, net->c0,
                                                                               net->params + net->off[2], net->wflip);
-        ROME_CUDA(cudaFuncSetAttribute(pconv_fwd_smem_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smd));
+        raise_smem_limit((const void*)pconv_fwd_smem_kernel<false>, 96 * 1024);
         pconv_fwd_smem_kernel<false><<<n, PT, smd, st>>>(net->c1, R, A, net->c0, net->dh1, net->wflip, nullptr,
                                                          net->dh0);
     } else {

@@ -306,10 +306,11 @@ class RomeError(RuntimeError):
 class GpuContext:
     """One device context of librome_b200 (``rome_gpu_create``)."""
 
-    def __init__(self, device: int = 0, precision: str = "fp32", deterministic: bool = False, profile: bool = False):
+    def __init__(self, device: int = 0, precision: str = "fp32", deterministic: bool = False, profile: bool = False,
+                 workspace_limit: int = 0):
         self.lib = abi.load_library()
         self.device = device
-        cfg = abi.RomeGpuConfig(abi.PRECISIONS[precision], int(deterministic), 0, int(profile))
+        cfg = abi.RomeGpuConfig(abi.PRECISIONS[precision], int(deterministic), int(workspace_limit), int(profile))
         h = C.c_void_p()
         rc = self.lib.rome_gpu_create(device, C.byref(cfg), C.byref(h))
         if rc != 0:

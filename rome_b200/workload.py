@@ -225,8 +225,47 @@ def build_map2d(w: Map2dWorkload):
         pdf_class=np.full(K, 1.0 / K), pdf_direction=np.full(K, 1.0 / K), prior_offsetx_class=np.zeros(K),
         prior_offsety_class=np.zeros(K), sigma2_offset=float(w.offset_range) ** 2 / 4.0,
     )
-    truth = dict(cls=cls, psi=psi, sx=sx, sy=sy)
+    truth = dict(cls=cls, psi=psi, sx=sx, sy=sy, defocus_u=du, defocus_v=dv, defocus_angle=da)
     return pool, proj, r_max, truth
+
+
+def raw_particles(p: Map2dPool, truth: dict, first_image: int = 0, dtype=np.float32):
+    """The pool's particles as read from an MRC stack: real-space images
+    (float32) whose centred transform is the pool's unmasked spectra, with
+    the metadata the image preparation reads (NORM 1, old offsets 0, the
+    CTF parameters the spectra were made with)."""
+    from .particles import ParticleImages, images_from_spectra
+    N = p.nr_images
+    imgs = images_from_spectra(p.Fimg_nomask_real, p.Fimg_nomask_imag, p.current_size, p.ori_size, dtype)
+    ctf = np.zeros((N, 7))
+    ctf[:, 0], ctf[:, 1], ctf[:, 2] = truth["defocus_u"], truth["defocus_v"], truth["defocus_angle"]
+    ctf[:, 3:7] = [300.0, 2.7, 0.1, 0.0]
+    return ParticleImages(images=imgs, norm=np.ones(N), xoff=np.zeros(N), yoff=np.zeros(N), ctf=ctf,
+                          group=np.asarray(p.group, np.int32), first_image=first_image)
+
+
+def prep_options(w: Map2dWorkload):
+    """Preparation settings of a synthetic workload: a particle diameter of
+    0.84 of the box (the templates' blobs lie within 0.3 of it, plus their
+    width and the shifts), the reference's 5-pixel soft edge, noise outside."""
+    from .particles import PrepOptions
+    return PrepOptions(pixel_size=w.pixel, particle_diameter=0.84 * w.ori_size * w.pixel, width_mask_edge=5,
+                       random_seed=int(w.seed))
+
+
+def image_template(p: Map2dPool) -> Map2dPool:
+    """The pool without its image arrays (zero-width placeholders): the model,
+    sampling and per-particle scalars that prepared pools are made from."""
+    from .map2d import DEVICE_FIELDS
+    return dataclasses.replace(p, **{f: np.empty((p.nr_images, 0)) for f in DEVICE_FIELDS})
+
+
+def slice_particles(imgs, lo: int, hi: int):
+    """Particles [lo, hi) of a ParticleImages (first_image moves with lo)."""
+    import dataclasses as dc
+    return dc.replace(imgs, images=imgs.images[lo:hi], norm=imgs.norm[lo:hi], xoff=imgs.xoff[lo:hi],
+                      yoff=imgs.yoff[lo:hi], ctf=imgs.ctf[lo:hi], group=imgs.group[lo:hi],
+                      first_image=imgs.first_image + lo)
 
 
 # ---------------------------------------------------------------------------
