@@ -43,7 +43,8 @@ def parse():
     ap.add_argument("--pool", type=int, default=2000)
     ap.add_argument("--particles", type=int, default=0, help="override the particle count (debug)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive"])
+    ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive", "prep"],
+                    help="prep: the image preparation (setFourierTransforms) alone, from float32 images")
     ap.add_argument("--topk", type=int, default=16, help="network outputs proposed per particle (x2 orientations)")
     ap.add_argument("--train-particles", type=int, default=20000)
     ap.add_argument("--train-epochs", type=int, default=15)
@@ -605,8 +606,80 @@ def run_ours_3d(args):
     print(json.dumps(line), flush=True)
 
 
+def run_prep(args):
+    """Secondary mode: the image preparation (ParticleModel::setFourierTransforms)
+    of the configuration's particles from float32 images, pool by pool.  value:
+    images resident in HBM; e2e: page-locked host images copied in (next pool
+    while this one is prepared), prepared arrays left on the device for the
+    E-step, per-particle outputs read back.  One JSON line."""
+    import dataclasses
+
+    import torch
+
+    from rome_b200.map2d import GpuContext
+    from rome_b200.particles import h2d_bytes, pin_particles, prepare_particles, prepared_stream
+    from rome_b200.workload import CONFIGS, build_map2d, image_template, prep_options, raw_particles, slice_particles, subset
+    w = CONFIGS[args.config]
+    if args.particles:
+        w = dataclasses.replace(w, n_particles=args.particles)
+    pool, _, _, truth = build_map2d(w)
+    raw = raw_particles(pool, truth)
+    tmpl = image_template(pool)
+    del pool
+    opts = prep_options(w)
+    N = tmpl.nr_images
+    bounds = [(lo, min(N, lo + args.pool)) for lo in range(0, N, args.pool)]
+    ctx = GpuContext(0, "fp32", profile=True)
+    d_raw = torch.from_numpy(raw.images).to("cuda:0")
+    dr = dataclasses.replace(raw, images=d_raw)
+
+    def step():
+        return [prepare_particles(ctx, slice_particles(dr, lo, hi), opts, tmpl.sigma2_noise, tmpl.current_size,
+                                  on_device=True, power=False) for lo, hi in bounds]
+
+    for _ in range(args.warmup):
+        step()
+    ctx.reset_timings()
+    with ClockSampler(0) as clk:
+        ms, _ = _timed(torch, step, args.steps)
+    t = ctx.get_timings()
+    host = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
+    items = [(subset(tmpl, lo, hi), h) for (lo, hi), h in zip(bounds, host)]
+    e_step = lambda: [q.pool.highres_Xi2 for q in prepared_stream(ctx, items, opts)]  # noqa: E731
+    e_step()
+    e_ms, _ = _timed(torch, e_step, args.steps)
+    hbm, _, peak_kind = load_peaks()
+    ph = t["images"]
+    # algorithmic bytes: the float32 image in, the five FP64 half-plane arrays out
+    F = tmpl.current_size * (tmpl.current_size // 2 + 1)
+    per = raw.images[0].nbytes + 5 * F * 8
+    achieved = per * N * args.steps / (ph["ms"] / 1e3) / 1e9
+    line = {
+        "metric": "image preparation particles/s (setFourierTransforms)", "value": round(N / (ms / args.steps / 1e3), 2),
+        "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (the configuration's particles as float32 real-space images)",
+        "config": {"workload": args.config + " image preparation", "particles": N, "image": w.ori_size,
+                   "pool": args.pool, "options": dataclasses.asdict(opts), "inputs": "larger than L2 (no flush)"},
+        "e2e": {"value": round(N / (e_ms / args.steps / 1e3), 2), "unit": UNIT,
+                "h2d_bytes_per_step": int(sum(h2d_bytes(h) for h in host)),
+                "d2h_bytes_per_step": int(N * 3 * 8)},
+        "gpu_launches": int(t["total_launches"]),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "the preparation phase as a whole (own kernels and cuFFT), algorithmic bytes "
+                               f"{per} per image", "launches": int(ph["launches"])},
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
+    if a.mode == "prep" and a.impl != "reference":
+        run_prep(a)
+        sys.exit(0)
     if a.config.startswith("map3d") and a.impl != "reference":
         run_ours_3d(a)
         sys.exit(0)
