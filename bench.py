@@ -634,8 +634,10 @@ def run_prep(args):
     dr = dataclasses.replace(raw, images=d_raw)
 
     def step():
-        return [prepare_particles(ctx, slice_particles(dr, lo, hi), opts, tmpl.sigma2_noise, tmpl.current_size,
-                                  on_device=True, power=False) for lo, hi in bounds]
+        # each pool's outputs are released before the next pool (an E-step would consume them)
+        for lo, hi in bounds:
+            prepare_particles(ctx, slice_particles(dr, lo, hi), opts, tmpl.sigma2_noise, tmpl.current_size,
+                              on_device=True, power=False)
 
     for _ in range(args.warmup):
         step()

@@ -184,7 +184,7 @@ struct RomeGpuCtx {
     double phase_flops[ROME_PHASE_COUNT] = {};
     double phase_bytes[ROME_PHASE_COUNT] = {};
     long total_launches = 0;
-    // cached cuFFT plans of the image preparation (prep.cu)
+    // the image preparation's cuFFT plans and host-built tables (prep.cu)
     void* prep_plans = nullptr;
 };
 

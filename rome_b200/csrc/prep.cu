@@ -75,9 +75,7 @@ void destroy_plan(PrepPlan& p) {
     p = PrepPlan{};
 }
 
-PrepPlan& get_plan(RomeGpuCtx* ctx, int n, int chunk) {
-    if (!ctx->prep_plans) ctx->prep_plans = new PrepPlans();
-    auto* pp = (PrepPlans*)ctx->prep_plans;
+PrepPlan& get_plan(RomeGpuCtx* ctx, PrepPlans* pp, int n, int chunk) {
     const auto key = std::make_pair(n, chunk);
     pp->used[key] = ++pp->tick;
     auto it = pp->plans.find(key);
@@ -488,6 +486,147 @@ dim3 grid2(size_t per_image, int images) {
 // C round(): halfway cases away from zero
 double c_round(double x) { return std::round(x); }
 
+// the host-built tables of the preparation and where they sit in S_PREP_TAB
+struct PrepTables {
+    bool valid = false;
+    std::vector<double> key;  // sizes, mask radius and width, sigma2_fudge, sigma2_noise
+    size_t o_ires = 0, o_sig = 0, o_pog = 0, o_dst = 0, o_dcn = 0, o_dpx = 0, o_zst = 0, o_zcn = 0, o_zpx = 0, o_ss = 0,
+           o_sp = 0, o_mw = 0;
+};
+
+struct PrepState {
+    PrepPlans plans;
+    PrepTables tables;
+    // a second stream for the work that does not need the images (noise
+    // spectra, CTF images), overlapping the unmasked path on the context's
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_noise = nullptr, ev_nc_free = nullptr, ev_ctf = nullptr;
+};
+
+PrepState* prep_state(RomeGpuCtx* ctx) {
+    if (!ctx->prep_plans) ctx->prep_plans = new PrepState();
+    auto* ps = (PrepState*)ctx->prep_plans;
+    if (!ps->side) {
+        ROME_CUDA(cudaStreamCreateWithFlags(&ps->side, cudaStreamNonBlocking));
+        for (cudaEvent_t* e : {&ps->ev_ready, &ps->ev_noise, &ps->ev_nc_free, &ps->ev_ctf})
+            ROME_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    return ps;
+}
+
+void build_tables(RomeGpuCtx* ctx, PrepTables& tb, int n, int fine, int G, bool noise, double radius, double width,
+                  double sigma2_fudge, const double* sigma2_noise) {
+    const int oF = n / 2 + 1;
+    const size_t npix = (size_t)n * oF, nn = (size_t)n * n;
+    (void)fine;
+    // shell of every half-plane pixel, round(sqrt(i'^2 + j^2)) (src/exp_model.h:514-516)
+    std::vector<unsigned short> ires(npix);
+    for (int i = 0; i < n; ++i) {
+        const int ip = i < oF ? i : i - n;
+        for (int j = 0; j < oF; ++j) ires[(size_t)i * oF + j] = (unsigned short)std::round(std::sqrt((double)(ip * ip + j * j)));
+    }
+    std::vector<float> sigf((size_t)G * oF, 0.f);
+    // groups with the same zero-sigma shells share one list of drawing pixels
+    std::vector<int> pat_of_group(G, 0), draw_start, draw_count, draw_pix, zero_start, zero_count, zero_pix;
+    if (noise) {
+        std::map<std::vector<int>, int> patterns;
+        for (int g = 0; g < G; ++g) {
+            std::vector<int> zero_shells;
+            for (int s = 0; s < oF; ++s) {
+                const double pw = sigma2_fudge * sigma2_noise[(size_t)g * oF + s];
+                ROME_REQUIRE(pw >= 0.0, "sigma2_noise[%d][%d] is negative", g, s);
+                sigf[(size_t)g * oF + s] = (float)std::sqrt(pw);
+                if (sigf[(size_t)g * oF + s] == 0.f) zero_shells.push_back(s);
+            }
+            auto it = patterns.find(zero_shells);
+            if (it == patterns.end()) {
+                const int id = (int)patterns.size();
+                it = patterns.emplace(zero_shells, id).first;
+                std::vector<char> zs(oF, 0);
+                for (int s : zero_shells) zs[s] = 1;
+                draw_start.push_back((int)draw_pix.size());
+                zero_start.push_back((int)zero_pix.size());
+                for (size_t q = 0; q < npix; ++q) {
+                    if (ires[q] < oF && !zs[ires[q]]) draw_pix.push_back((int)q);
+                    else zero_pix.push_back((int)q);
+                }
+                draw_count.push_back((int)draw_pix.size() - draw_start.back());
+                zero_count.push_back((int)zero_pix.size() - zero_start.back());
+            }
+            pat_of_group[g] = it->second;
+        }
+    }
+    // shells 1..oF-1 of the power spectrum, pixels in row-major order, the
+    // negative rows of the x = 0 column skipped (src/exp_model.h:576-595)
+    std::vector<int> shell_start(oF + 1, 0), shell_pix;
+    {
+        std::vector<std::vector<int>> by(oF);
+        for (int i = 0; i < n; ++i) {
+            const int ip = i < oF ? i : i - n;
+            for (int j = 0; j < oF; ++j) {
+                const int s = ires[(size_t)i * oF + j];
+                if (s > 0 && s < oF && !(j == 0 && ip < 0)) by[s].push_back(i * oF + j);
+            }
+        }
+        for (int s = 0; s < oF; ++s) {
+            shell_start[s + 1] = shell_start[s] + (int)by[s].size();
+            shell_pix.insert(shell_pix.end(), by[s].begin(), by[s].end());
+        }
+    }
+    // softMaskOutsideMap's weight of every (uncentred) pixel: < 0 inside the
+    // radius, the raised cosine in the edge band, > 1 beyond it
+    std::vector<double> mw(nn);
+    {
+        const double radius_p = radius + width;
+        const int origin = -(n / 2);
+        for (int a = 0; a < n; ++a)
+            for (int b = 0; b < n; ++b) {
+                const double r = std::sqrt((double)((a + origin) * (a + origin) + (b + origin) * (b + origin)));
+                mw[(size_t)a * n + b] =
+                    r < radius ? -1.0 : r <= radius_p ? 0.5 + 0.5 * std::cos(kPi * (radius_p - r) / width) : 2.0;
+            }
+    }
+    size_t bytes = 0;
+    auto carve = [&](size_t b) {
+        const size_t o = bytes;
+        bytes += align256(std::max<size_t>(b, 1));
+        return o;
+    };
+    tb.o_ires = carve(npix * 2);
+    tb.o_sig = carve(sigf.size() * 4);
+    tb.o_pog = carve((size_t)G * 4);
+    tb.o_dst = carve(draw_start.size() * 4);
+    tb.o_dcn = carve(draw_count.size() * 4);
+    tb.o_dpx = carve(draw_pix.size() * 4);
+    tb.o_zst = carve(zero_start.size() * 4);
+    tb.o_zcn = carve(zero_count.size() * 4);
+    tb.o_zpx = carve(zero_pix.size() * 4);
+    tb.o_ss = carve(shell_start.size() * 4);
+    tb.o_sp = carve(shell_pix.size() * 4);
+    tb.o_mw = carve(nn * 8);
+    char* tab = (char*)ctx->ws[S_PREP_TAB].get(bytes);
+    auto up = [&](size_t off, const auto& v) {
+        if (!v.empty()) {
+            ROME_CUDA(cudaMemcpyAsync(tab + off, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice, ctx->stream));
+        }
+    };
+    up(tb.o_ires, ires);
+    up(tb.o_sig, sigf);
+    up(tb.o_pog, pat_of_group);
+    up(tb.o_dst, draw_start);
+    up(tb.o_dcn, draw_count);
+    up(tb.o_dpx, draw_pix);
+    up(tb.o_zst, zero_start);
+    up(tb.o_zcn, zero_count);
+    up(tb.o_zpx, zero_pix);
+    up(tb.o_ss, shell_start);
+    up(tb.o_sp, shell_pix);
+    up(tb.o_mw, mw);
+    // the host vectors are pageable: the copies are complete when they return, but wait anyway
+    // so that nothing of this call's tables is in flight when the vectors go
+    ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
 template <typename T>
 void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
     const int P = in.nr_images, n = in.ori_size, fine = in.current_size, G = in.nr_groups;
@@ -530,116 +669,43 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
         }
         r[PP_GROUP] = g;
     }
-    // shell of every half-plane pixel, round(sqrt(i'^2 + j^2)) (src/exp_model.h:514-516)
-    std::vector<unsigned short> ires(npix);
-    for (int i = 0; i < n; ++i) {
-        const int ip = i < oF ? i : i - n;
-        for (int j = 0; j < oF; ++j) ires[(size_t)i * oF + j] = (unsigned short)std::round(std::sqrt((double)(ip * ip + j * j)));
+    // ---- tables that depend only on the sizes, the mask and sigma2_noise:
+    // built on the host and uploaded when those change (once per iteration) ----
+    auto* state = prep_state(ctx);
+    PrepTables& tb = state->tables;
+    const double radius = in.particle_diameter / (2. * in.pixel_size), width = (double)in.width_mask_edge;
+    std::vector<double> key = {(double)n, (double)fine, (double)G, noise ? 1.0 : 0.0, radius, width, in.sigma2_fudge};
+    if (noise) key.insert(key.end(), in.sigma2_noise, in.sigma2_noise + (size_t)G * oF);
+    if (!tb.valid || key != tb.key) {
+        tb.valid = false;
+        build_tables(ctx, tb, n, fine, G, noise, radius, width, in.sigma2_fudge, in.sigma2_noise);
+        tb.key = std::move(key);
+        tb.valid = true;
     }
-    std::vector<float> sigf((size_t)G * oF, 0.f);
-    // groups with the same zero-sigma shells share one list of drawing pixels
-    std::vector<int> pat_of_group(G, 0), draw_start, draw_count, draw_pix, zero_start, zero_count, zero_pix;
-    if (noise) {
-        std::map<std::vector<int>, int> patterns;
-        for (int g = 0; g < G; ++g) {
-            std::vector<int> zero_shells;
-            for (int s = 0; s < oF; ++s) {
-                const double pw = in.sigma2_fudge * in.sigma2_noise[(size_t)g * oF + s];
-                ROME_REQUIRE(pw >= 0.0, "sigma2_noise[%d][%d] is negative", g, s);
-                sigf[(size_t)g * oF + s] = (float)std::sqrt(pw);
-                if (sigf[(size_t)g * oF + s] == 0.f) zero_shells.push_back(s);
-            }
-            auto it = patterns.find(zero_shells);
-            if (it == patterns.end()) {
-                const int id = (int)patterns.size();
-                it = patterns.emplace(zero_shells, id).first;
-                std::vector<char> zs(oF, 0);
-                for (int s : zero_shells) zs[s] = 1;
-                draw_start.push_back((int)draw_pix.size());
-                zero_start.push_back((int)zero_pix.size());
-                for (size_t q = 0; q < npix; ++q) {
-                    if (ires[q] < oF && !zs[ires[q]]) draw_pix.push_back((int)q);
-                    else zero_pix.push_back((int)q);
-                }
-                draw_count.push_back((int)draw_pix.size() - draw_start.back());
-                zero_count.push_back((int)zero_pix.size() - zero_start.back());
-            }
-            pat_of_group[g] = it->second;
-        }
-    }
-    // shells 1..oF-1 of the power spectrum, pixels in row-major order, the
-    // negative rows of the x = 0 column skipped (src/exp_model.h:576-595)
-    std::vector<int> shell_start(oF + 1, 0), shell_pix;
-    {
-        std::vector<std::vector<int>> by(oF);
-        for (int i = 0; i < n; ++i) {
-            const int ip = i < oF ? i : i - n;
-            for (int j = 0; j < oF; ++j) {
-                const int s = ires[(size_t)i * oF + j];
-                if (s > 0 && s < oF && !(j == 0 && ip < 0)) by[s].push_back(i * oF + j);
-            }
-        }
-        for (int s = 0; s < oF; ++s) {
-            shell_start[s + 1] = shell_start[s] + (int)by[s].size();
-            shell_pix.insert(shell_pix.end(), by[s].begin(), by[s].end());
-        }
-    }
-
-    // ---- device buffers ----
-    double* d_part = ctx->ws[S_PREP_PART].as<double>(part.size());
-    stage_copy(ctx, d_part, part.data(), part.size());
-    // one table buffer: shells, noise patterns and sigmas, power shells, per-image sums
-    size_t tab_bytes = 0;
-    auto carve = [&](size_t bytes) {
-        const size_t at = tab_bytes;
-        tab_bytes += align256(std::max<size_t>(bytes, 1));
-        return at;
-    };
-    const size_t o_ires = carve(npix * 2), o_sig = carve(sigf.size() * 4), o_pog = carve((size_t)G * 4),
-                 o_dst = carve(draw_start.size() * 4), o_dcn = carve(draw_count.size() * 4),
-                 o_dpx = carve(draw_pix.size() * 4), o_zst = carve(zero_start.size() * 4),
-                 o_zcn = carve(zero_count.size() * 4), o_zpx = carve(zero_pix.size() * 4),
-                 o_ss = carve(shell_start.size() * 4), o_sp = carve(shell_pix.size() * 4), o_bg = carve((size_t)P * 8),
-                 o_xi2 = carve((size_t)P * 8), o_pow = carve((size_t)P * oF * 8), o_mw = carve(nn * 8),
-                 o_ctfk = carve((size_t)P * CK_COUNT * 8);
-    char* tab = (char*)ctx->ws[S_PREP_TAB].get(tab_bytes);
+    char* tab = (char*)ctx->ws[S_PREP_TAB].p;
     auto at = [&](size_t off) { return (void*)(tab + off); };
-    auto* d_ires = (unsigned short*)at(o_ires);
-    auto* d_sig = (float*)at(o_sig);
-    auto* d_ss = (int*)at(o_ss);
-    auto* d_sp = (int*)at(o_sp);
-    auto* d_bg = (double*)at(o_bg);
-    auto* d_xi2 = (double*)at(o_xi2);
-    auto* d_pow = (double*)at(o_pow);
-    auto* d_mw = (double*)at(o_mw);
-    auto* d_ctfk = (double*)at(o_ctfk);
-    stage_copy(ctx, d_ires, ires.data(), ires.size());
-    if (noise) {
-        stage_copy(ctx, d_sig, sigf.data(), sigf.size());
-        stage_copy(ctx, (int*)at(o_pog), pat_of_group.data(), pat_of_group.size());
-        stage_copy(ctx, (int*)at(o_dst), draw_start.data(), draw_start.size());
-        stage_copy(ctx, (int*)at(o_dcn), draw_count.data(), draw_count.size());
-        stage_copy(ctx, (int*)at(o_dpx), draw_pix.data(), draw_pix.size());
-        stage_copy(ctx, (int*)at(o_zst), zero_start.data(), zero_start.size());
-        stage_copy(ctx, (int*)at(o_zcn), zero_count.data(), zero_count.size());
-        stage_copy(ctx, (int*)at(o_zpx), zero_pix.data(), zero_pix.size());
-    }
-    stage_copy(ctx, d_ss, shell_start.data(), shell_start.size());
-    stage_copy(ctx, d_sp, shell_pix.data(), shell_pix.size());
-    // softMaskOutsideMap's weight of every (uncentred) pixel: < 0 inside the
-    // radius, the raised cosine in the edge band, > 1 beyond it
-    {
-        const double radius = in.particle_diameter / (2. * in.pixel_size), width = (double)in.width_mask_edge;
-        const double radius_p = radius + width;
-        const int origin = -(n / 2);
-        std::vector<double> mw(nn);
-        for (int a = 0; a < n; ++a)
-            for (int b = 0; b < n; ++b) {
-                const double r = std::sqrt((double)((a + origin) * (a + origin) + (b + origin) * (b + origin)));
-                mw[(size_t)a * n + b] = r < radius ? -1.0 : r <= radius_p ? 0.5 + 0.5 * std::cos(kPi * (radius_p - r) / width) : 2.0;
-            }
-        stage_copy(ctx, d_mw, mw.data(), mw.size());
-    }
+    auto* d_ires = (unsigned short*)at(tb.o_ires);
+    auto* d_sig = (float*)at(tb.o_sig);
+    auto* d_ss = (int*)at(tb.o_ss);
+    auto* d_sp = (int*)at(tb.o_sp);
+    auto* d_mw = (double*)at(tb.o_mw);
+
+    // ---- per-call buffers: particle records, CTF constants, per-image sums ----
+    size_t call_bytes = 0;
+    auto carve = [&](size_t bytes) {
+        const size_t o = call_bytes;
+        call_bytes += align256(std::max<size_t>(bytes, 1));
+        return o;
+    };
+    const size_t o_part = carve(part.size() * 8), o_ctfk = carve((size_t)P * CK_COUNT * 8), o_bg = carve((size_t)P * 8),
+                 o_xi2 = carve((size_t)P * 8), o_pow = carve((size_t)P * oF * 8);
+    char* cb = (char*)ctx->ws[S_PREP_PART].get(call_bytes);
+    auto* d_part = (double*)(cb + o_part);
+    auto* d_ctfk = (double*)(cb + o_ctfk);
+    auto* d_bg = (double*)(cb + o_bg);
+    auto* d_xi2 = (double*)(cb + o_xi2);
+    auto* d_pow = (double*)(cb + o_pow);
+    stage_copy(ctx, d_part, part.data(), part.size());
 
     double *o_re, *o_im, *o_nre, *o_nim, *o_ctf;
     if (out.outputs_on_device) {
@@ -674,8 +740,39 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
     const uint32_t seed0 = (uint32_t)(in.random_seed + in.first_image);
     const double avg = in.avg_norm_correction;
 
+    // CTF images on the side stream once the particle records are on the device
+    cudaStream_t side = state->side;
+    ROME_CUDA(cudaEventRecord(state->ev_ready, st));
+    ROME_CUDA(cudaStreamWaitEvent(side, state->ev_ready, 0));
+    if (in.do_ctf_correction) {
+        ctf_constants_kernel<<<(P + 127) / 128, 128, 0, side>>>(P, d_part, d_ctfk);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_IMAGES);
+        ctf_kernel<<<grid2(Ff, P), 256, 0, side>>>(P, fine, n, in.pixel_size, d_ctfk, in.ctf_phase_flipped ? 1 : 0,
+                                                   in.only_flip_phases ? 1 : 0, in.intact_ctf_first_peak ? 1 : 0,
+                                                   o_ctf);
+    } else {
+        fill_kernel<<<grid_for((size_t)P * Ff), 256, 0, side>>>(o_ctf, (size_t)P * Ff, 1.0);
+    }
+    ROME_CHECK_LAUNCH();
+    prof.launched(ROME_PHASE_IMAGES);
+    ROME_CUDA(cudaEventRecord(state->ev_ctf, side));
+    ROME_CUDA(cudaEventRecord(state->ev_nc_free, st));
+
     for (int c0 = 0; c0 < P; c0 += chunk) {
         const int pc = std::min(chunk, P - c0);
+        const double* pp = d_part + (size_t)c0 * PP_COUNT;
+        // this chunk's noise spectra on the side stream, once the previous chunk's are consumed
+        if (noise) {
+            ROME_CUDA(cudaStreamWaitEvent(side, state->ev_nc_free, 0));
+            noise_spectra_kernel<<<(pc + kNoiseWarps - 1) / kNoiseWarps, kNoiseWarps * 32, 0, side>>>(
+                pc, (int)npix, oF, seed0 + (uint32_t)c0, pp, (const int*)at(tb.o_pog), (const int*)at(tb.o_dst),
+                (const int*)at(tb.o_dcn), (const int*)at(tb.o_dpx), (const int*)at(tb.o_zst), (const int*)at(tb.o_zcn),
+                (const int*)at(tb.o_zpx), d_ires, d_sig, d_NC);
+            ROME_CHECK_LAUNCH();
+            ROME_CUDA(cudaEventRecord(state->ev_noise, side));
+            prof.launched(ROME_PHASE_IMAGES);
+        }
         const T* raw;
         if (in.images_on_device) {
             raw = d_raw_all + (size_t)c0 * nn;
@@ -684,8 +781,7 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
                                       cudaMemcpyHostToDevice, st));
             raw = d_raw_chunk;
         }
-        const double* pp = d_part + (size_t)c0 * PP_COUNT;
-        PrepPlan& plan = get_plan(ctx, n, pc);
+        PrepPlan& plan = get_plan(ctx, &state->plans, n, pc);
         // unmasked image
         translate_center_kernel<T><<<grid2((nn + 3) / 4, pc), 256, 0, st>>>(pc, n, raw, pp, norm_on, avg, d_R);
         ROME_CHECK_LAUNCH();
@@ -695,16 +791,13 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
         prof.launched(ROME_PHASE_IMAGES, 2);
         // noise image or background average
         if (noise) {
-            noise_spectra_kernel<<<(pc + kNoiseWarps - 1) / kNoiseWarps, kNoiseWarps * 32, 0, st>>>(
-                pc, (int)npix, oF, seed0 + (uint32_t)c0, pp, (const int*)at(o_pog), (const int*)at(o_dst),
-                (const int*)at(o_dcn), (const int*)at(o_dpx), (const int*)at(o_zst), (const int*)at(o_zcn),
-                (const int*)at(o_zpx), d_ires, d_sig, d_NC);
-            ROME_CHECK_LAUNCH();
+            ROME_CUDA(cudaStreamWaitEvent(st, state->ev_noise, 0));
             ROME_CUFFT(cufftExecZ2Z(plan.col, (cufftDoubleComplex*)d_NC, (cufftDoubleComplex*)d_NC, CUFFT_INVERSE));
             real_edges_kernel<<<grid_for((size_t)n * pc), 256, 0, st>>>((long)n * pc, oF, n, d_NC);
             ROME_CHECK_LAUNCH();
             ROME_CUFFT(cufftExecZ2D(plan.row, (cufftDoubleComplex*)d_NC, d_NR));
-            prof.launched(ROME_PHASE_IMAGES, 2);
+            ROME_CUDA(cudaEventRecord(state->ev_nc_free, st));
+            prof.launched(ROME_PHASE_IMAGES);
         } else {
             background_kernel<T><<<pc, 256, 0, st>>>(n, raw, pp, norm_on, avg, d_mw, d_bg + c0);
             ROME_CHECK_LAUNCH();
@@ -728,17 +821,7 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
         ROME_CUDA(cudaMemsetAsync(d_xi2, 0, (size_t)P * 8, st));
         ROME_CUDA(cudaMemsetAsync(d_pow, 0, (size_t)P * oF * 8, st));
     }
-    if (in.do_ctf_correction) {
-        ctf_constants_kernel<<<(P + 127) / 128, 128, 0, st>>>(P, d_part, d_ctfk);
-        ROME_CHECK_LAUNCH();
-        prof.launched(ROME_PHASE_IMAGES);
-        ctf_kernel<<<grid2(Ff, P), 256, 0, st>>>(P, fine, n, in.pixel_size, d_ctfk, in.ctf_phase_flipped ? 1 : 0,
-                                                 in.only_flip_phases ? 1 : 0, in.intact_ctf_first_peak ? 1 : 0, o_ctf);
-    } else {
-        fill_kernel<<<grid_for((size_t)P * Ff), 256, 0, st>>>(o_ctf, (size_t)P * Ff, 1.0);
-    }
-    ROME_CHECK_LAUNCH();
-    prof.launched(ROME_PHASE_IMAGES);
+    ROME_CUDA(cudaStreamWaitEvent(st, state->ev_ctf, 0));
     prof.end(ROME_PHASE_IMAGES);
     // algorithmic traffic: images in, the five output arrays and the power spectra out
     prof.add_bytes(ROME_PHASE_IMAGES, (double)P * ((double)nn * sizeof(T) + 5.0 * Ff * 8 + oF * 8.0));
@@ -760,9 +843,15 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
 
 void prep_release(RomeGpuCtx* ctx) {
     if (!ctx || !ctx->prep_plans) return;
-    auto* pp = (PrepPlans*)ctx->prep_plans;
-    for (auto& kv : pp->plans) destroy_plan(kv.second);
-    delete pp;
+    auto* ps = (PrepState*)ctx->prep_plans;
+    for (auto& kv : ps->plans.plans) destroy_plan(kv.second);
+    if (ps->side) {
+        cudaStreamSynchronize(ps->side);
+        cudaStreamDestroy(ps->side);
+        for (cudaEvent_t e : {ps->ev_ready, ps->ev_noise, ps->ev_nc_free, ps->ev_ctf})
+            if (e) cudaEventDestroy(e);
+    }
+    delete ps;
     ctx->prep_plans = nullptr;
 }
 
