@@ -323,6 +323,9 @@ def run_ours(args):
         covered = (props == jbest[:, None]).any(axis=1)
         judge["proposal_coverage_of_fp32_mode"] = round(float(np.mean(covered)), 5)
         judge["mean_proposal_mass"] = round(float(mass.mean()), 4)
+        nsig = np.concatenate([r[0]["nr_sign"] for r in last])
+        judge["significant_hypotheses_per_particle"] = {"mean": round(float(nsig.mean()), 2),
+                                                        "p90": float(np.percentile(nsig, 90))}
         judge["orientations_searched"] = f"{props.shape[1]} of {pool.nr_classes * pool.nr_psi}"
         judge["exhaustive_fallback_fraction"] = round(nlow / N, 5)
         # what other fallback thresholds would give: (fraction searched exhaustively, pose agreement)
