@@ -163,8 +163,10 @@ __device__ __forceinline__ float polar_multiplier(float U1, float U2) {
     return __double2float_rn(__dsqrt_rn(__ddiv_rn(-2.0 * log(W), W)));
 }
 
-// Noise spectra of the images of a chunk, written as double2 in the (row,
-// image) layout of the column transform, NC[(i * chunk + c) * oF + j], drawn in
+// Noise spectra of the images of a chunk, written as double2 at
+// out[i * si + c * sp + j] (image c, row i, column j): the (row, image) layout
+// of the cuFFT column transform (si = chunk * oF, sp = oF) or one spectrum per
+// image (si = oF, sp = n * oF) for the fused kernels; drawn in
 // the reference's fill order (src/exp_model.h:509-534): row i, column j, real
 // then imaginary part; a pixel draws when its shell ires = round(|(i', j)|)
 // is < n/2+1 and its sigma sqrt(sigma2_fudge * sigma2_noise[group][ires]),
@@ -179,7 +181,8 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) noise_spectra_kernel(
     int P, int npix, int oF, uint32_t seed0, const double* __restrict__ part, const int* __restrict__ pat_of_group,
     const int* __restrict__ draw_start, const int* __restrict__ draw_count, const int* __restrict__ draw_pix,
     const int* __restrict__ zero_start, const int* __restrict__ zero_count, const int* __restrict__ zero_pix,
-    const unsigned short* __restrict__ ires_tab, const float* __restrict__ sigf, double2* __restrict__ out) {
+    const unsigned short* __restrict__ ires_tab, const float* __restrict__ sigf, long si, long sp,
+    double2* __restrict__ out) {
     const int img = blockIdx.x * kNoiseWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (img >= P) return;  // whole warps leave together
     const int g = (int)part[(size_t)img * PP_COUNT + PP_GROUP], pat = pat_of_group[g];
@@ -218,7 +221,7 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) noise_spectra_kernel(
             const float mult = polar_multiplier(U1, U2);
             const float X1 = __fmul_rn(U1, mult), X2 = __fmul_rn(U2, mult);
             const int i = q / oF;
-            out[((size_t)i * P + img) * oF + (q - i * oF)] =
+            out[i * si + img * sp + (q - i * oF)] =
                 make_double2((double)__fadd_rn(0.0f, __fmul_rn(s, X1)), (double)__fadd_rn(0.0f, __fmul_rn(s, X2)));
         }
         base += __popc(mask);
@@ -226,7 +229,7 @@ __global__ void __launch_bounds__(kNoiseWarps * 32) noise_spectra_kernel(
     const int* zp = zero_pix + zero_start[pat];
     for (int k = lane; k < zero_count[pat]; k += 32) {
         const int q = zp[k], i = q / oF;
-        out[((size_t)i * P + img) * oF + (q - i * oF)] = make_double2(0.0, 0.0);
+        out[i * si + img * sp + (q - i * oF)] = make_double2(0.0, 0.0);
     }
 }
 
@@ -463,6 +466,387 @@ __global__ void ctf_kernel(int P, int fine, int ori, double angpix, const double
     }
 }
 
+// ---------------------------------------------------------------------------
+// Fused preparation for power-of-two sizes n = 32 E (E = 1, 2, 4): one CTA
+// holds one image's half-plane spectrum in shared memory, and every 1D
+// transform is one warp's: lane l holds elements l + 32 m (m < E); an E-point
+// DFT over m, the twiddles W_n^(l k1), then a 32-point radix-2
+// decimation-in-frequency DFT across the lanes by shuffles leave element
+// k1 + E * bitrev5(l) in lane l.  Two real rows go through one complex
+// transform (a + i b), split into their half spectra after it; the inverse
+// real transforms take two half rows the same way.  The 2D order is the one
+// of FFTW's multi-dimensional real transforms: rows then columns forward,
+// columns then rows backward, the backward row transforms reading only the
+// real part of the x = 0 and x = n/2 entries.  CenterFFT is the factor
+// (-1)^(i + j) on the spectrum (an n/2 shift of an even-sized image).
+
+constexpr int kFusedWarps = 32;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 shfl_xor2(double2 v, int m) {
+    return make_double2(__shfl_xor_sync(0xffffffffu, v.x, m), __shfl_xor_sync(0xffffffffu, v.y, m));
+}
+
+// the warp's length-32E transform; tw[q] = exp(-2 pi i q / (32 E)), conjugated for the inverse (unnormalised).
+// In: lane l holds element l + 32 m in v[m].  Out: lane l holds element k1 + E bitrev5(l) in v[k1].
+template <int E, bool INV>
+__device__ __forceinline__ void warp_fft(double2 (&v)[E], int lane, const double2* __restrict__ tw) {
+    constexpr int N = 32 * E;
+    auto W = [&](int q) {
+        const double2 t = tw[q];
+        return INV ? make_double2(t.x, -t.y) : t;
+    };
+    if constexpr (E == 2) {
+        const double2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    } else if constexpr (E == 4) {
+        const double2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+        const double2 b0 = cadd(v[1], v[3]), b1 = csub(v[1], v[3]);
+        // b1 times -i (forward) or +i (inverse)
+        const double2 r = INV ? make_double2(-b1.y, b1.x) : make_double2(b1.y, -b1.x);
+        v[0] = cadd(a0, b0);
+        v[1] = cadd(a1, r);
+        v[2] = csub(a0, b0);
+        v[3] = csub(a1, r);
+    }
+#pragma unroll
+    for (int k1 = 1; k1 < E; ++k1) v[k1] = cmul(v[k1], W((lane * k1) & (N - 1)));
+#pragma unroll
+    for (int s = 16; s >= 1; s >>= 1) {
+        const bool upper = lane & s;
+        const double2 w = W((lane & (s - 1)) * (N / (2 * s)));
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) {
+            const double2 o = shfl_xor2(v[k1], s);
+            v[k1] = upper ? cmul(csub(o, v[k1]), w) : cadd(v[k1], o);
+        }
+    }
+}
+
+__device__ __forceinline__ int bitrev5(int l) { return (int)(__brev((unsigned)l) >> 27); }
+
+// Shared-memory positions.  The transforms leave element k1 + E bitrev5(l)
+// in lane l: rows (or scratch entries) 4 apart for consecutive lanes, which
+// with 16-byte elements would put 16 lanes on the same banks.  Element
+// (row, c) of the spectrum sits at column c ^ ((row >> 2) & 7) of its row (c
+// below n/2; the n/2 column stays), scratch entry k at k ^ ((k >> 3) & 7) in
+// its group of 8: row-wise, column-wise and bit-reversed accesses then all
+// take the minimum of 4 wavefronts per warp.
+template <int N>
+__device__ __forceinline__ int zidx(int row, int c) {
+    constexpr int LD = N / 2 + 1;
+    return row * LD + (c < N / 2 ? c ^ ((row >> 2) & 7) : c);
+}
+__device__ __forceinline__ int sidx(int k) { return (k & ~7) | ((k ^ (k >> 3)) & 7); }
+
+// shared memory of the fused kernels: the spectrum Z [n][n/2+1] (a row also
+// holds the n doubles of a real row), per-warp scratch [16][n], twiddles [n],
+// the power shells [n/2+1], a reduction area
+template <int E>
+struct FusedSmem {
+    static constexpr int N = 32 * E, LD = N / 2 + 1;
+    static constexpr size_t Z = (size_t)N * LD * 16, SCR = (size_t)kFusedWarps * N * 16, TW = (size_t)N * 16,
+                            SPEC = ((size_t)LD * 8 + 15) / 16 * 16, RED = 2 * kFusedWarps * 32 * 8;
+    static constexpr size_t TOTAL = Z + SCR + TW + SPEC + RED;
+};
+
+// forward transform of the n real rows held in Z (row i's doubles at the
+// start of its slot), or produced by load_row(i, x), into the half-plane
+// spectrum in Z: rows in pairs, then the columns
+template <int E, typename LoadRow>
+__device__ __forceinline__ void fused_forward(double2* Z, double2* scr, const double2* tw, LoadRow load_row) {
+    constexpr int N = 32 * E;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double2* my = scr + warp * N;
+    for (int r = warp; r < N / 2; r += kFusedWarps) {
+        double2 v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = make_double2(load_row(2 * r, lane + 32 * m), load_row(2 * r + 1, lane + 32 * m));
+        warp_fft<E, false>(v, lane, tw);
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) my[sidx(k1 + E * bitrev5(lane))] = v[k1];
+        __syncwarp();
+        for (int k = lane; k <= N / 2; k += 32) {
+            const double2 a = my[sidx(k)], b = my[sidx((N - k) & (N - 1))];
+            Z[zidx<N>(2 * r, k)] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+            Z[zidx<N>(2 * r + 1, k)] = make_double2(0.5 * (a.y + b.y), 0.5 * (b.x - a.x));
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    // columns 1 .. n/2-1, and columns 0 and n/2 (real after the row pass) as one complex column
+    for (int c = warp; c < N / 2; c += kFusedWarps) {
+        double2 v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int row = lane + 32 * m;
+            v[m] = c ? Z[zidx<N>(row, c)] : make_double2(Z[zidx<N>(row, 0)].x, Z[zidx<N>(row, N / 2)].x);
+        }
+        warp_fft<E, false>(v, lane, tw);
+        __syncwarp();
+        if (c) {
+#pragma unroll
+            for (int k1 = 0; k1 < E; ++k1) Z[zidx<N>(k1 + E * bitrev5(lane), c)] = v[k1];
+        } else {
+#pragma unroll
+            for (int k1 = 0; k1 < E; ++k1) my[sidx(k1 + E * bitrev5(lane))] = v[k1];
+            __syncwarp();
+            for (int k = lane; k < N; k += 32) {
+                const double2 a = my[sidx(k)], b = my[sidx((N - k) & (N - 1))];
+                Z[zidx<N>(k, 0)] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+                Z[zidx<N>(k, N / 2)] = make_double2(0.5 * (a.y + b.y), 0.5 * (b.x - a.x));
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+}
+
+// backward transform of the half-plane spectrum in Z into n real rows (in
+// place, each row's doubles at the start of its slot), unnormalised
+template <int E>
+__device__ __forceinline__ void fused_backward(double2* Z, const double2* tw) {
+    constexpr int N = 32 * E, LD = N / 2 + 1;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // columns 1 .. n/2-1; columns 0 and n/2 enter the row transforms by their
+    // real parts only, so they go together as one complex column of their
+    // Hermitian parts h[k] = (s[k] + conj(s[-k])) / 2 (real inverse transforms)
+    for (int c = warp; c < N / 2; c += kFusedWarps) {
+        double2 v[E];
+        if (c) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) v[m] = Z[zidx<N>(lane + 32 * m, c)];
+        } else {
+            double2 s0[E], s1[E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                s0[m] = Z[zidx<N>(lane + 32 * m, 0)];
+                s1[m] = Z[zidx<N>(lane + 32 * m, N / 2)];
+            }
+            // element n - k of element k = l + 32 m sits in lane (32 - l) & 31, slot E-1-m (slot (E-m) mod E in lane 0)
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                double2 t0 = s0[E - 1 - m], t1 = s1[E - 1 - m];
+                if (lane == 0) {
+                    t0 = s0[(E - m) % E];
+                    t1 = s1[(E - m) % E];
+                }
+                const int from = (32 - lane) & 31;
+                const double2 r0 = make_double2(__shfl_sync(0xffffffffu, t0.x, from), __shfl_sync(0xffffffffu, t0.y, from));
+                const double2 r1 = make_double2(__shfl_sync(0xffffffffu, t1.x, from), __shfl_sync(0xffffffffu, t1.y, from));
+                const double2 h0 = make_double2(0.5 * (s0[m].x + r0.x), 0.5 * (s0[m].y - r0.y));
+                const double2 h1 = make_double2(0.5 * (s1[m].x + r1.x), 0.5 * (s1[m].y - r1.y));
+                v[m] = make_double2(h0.x - h1.y, h0.y + h1.x);  // h0 + i h1
+            }
+        }
+        warp_fft<E, true>(v, lane, tw);
+        __syncwarp();
+        if (c) {
+#pragma unroll
+            for (int k1 = 0; k1 < E; ++k1) Z[zidx<N>(k1 + E * bitrev5(lane), c)] = v[k1];
+        } else {
+#pragma unroll
+            for (int k1 = 0; k1 < E; ++k1) {
+                const int row = k1 + E * bitrev5(lane);
+                Z[zidx<N>(row, 0)] = make_double2(v[k1].x, 0.0);
+                Z[zidx<N>(row, N / 2)] = make_double2(v[k1].y, 0.0);
+            }
+        }
+    }
+    __syncthreads();
+    for (int r = warp; r < N / 2; r += kFusedWarps) {
+        double2 v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int k = lane + 32 * m;
+            double2 a, b;
+            if (k <= N / 2) {
+                a = Z[zidx<N>(2 * r, k)];
+                b = Z[zidx<N>(2 * r + 1, k)];
+                if (k == 0 || k == N / 2) a.y = b.y = 0.0;
+            } else {
+                a = Z[zidx<N>(2 * r, N - k)];
+                b = Z[zidx<N>(2 * r + 1, N - k)];
+                a.y = -a.y;
+                b.y = -b.y;
+            }
+            v[m] = make_double2(a.x - b.y, a.y + b.x);  // a + i b
+        }
+        warp_fft<E, true>(v, lane, tw);
+        __syncwarp();
+        double* ra = (double*)(Z + (2 * r) * LD);
+        double* rb = (double*)(Z + (2 * r + 1) * LD);
+#pragma unroll
+        for (int k1 = 0; k1 < E; ++k1) {
+            const int x = k1 + E * bitrev5(lane);
+            ra[x] = v[k1].x;
+            rb[x] = v[k1].y;
+        }
+    }
+    __syncthreads();
+}
+
+// window of the centred, normalised spectrum in Z to [fine][fine/2+1]
+template <int E>
+__device__ __forceinline__ void fused_window(const double2* Z, int fine, double* __restrict__ re, double* __restrict__ im) {
+    constexpr int N = 32 * E;
+    const int fF = fine / 2 + 1, per = fine * fF;
+    const double nn = (double)N * N;
+    for (int q = threadIdx.x; q < per; q += blockDim.x) {
+        const int i = q / fF, j = q - (q / fF) * fF;
+        const int ip = i < fF ? i : i - fine;
+        const int si = ip < 0 ? ip + N : ip;
+        const double2 v = Z[zidx<N>(si, j)];
+        const double sg = ((si + j) & 1) ? -1.0 : 1.0;
+        re[q] = sg * __ddiv_rn(v.x, nn);
+        im[q] = sg * __ddiv_rn(v.y, nn);
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void load_twiddles(double2* tw, const double2* __restrict__ gtw) {
+    for (int q = threadIdx.x; q < 32 * E; q += blockDim.x) tw[q] = gtw[q];
+}
+
+// Fimages_nomask: translate, centre, transform, window, one image per CTA iteration
+template <int E, typename T>
+__global__ void __launch_bounds__(kFusedWarps * 32) fused_nomask_kernel(int chunk, int fine, const T* __restrict__ raw,
+                                                                        const double* __restrict__ part, int do_norm,
+                                                                        double avg, const double2* __restrict__ gtw,
+                                                                        double* __restrict__ out_re,
+                                                                        double* __restrict__ out_im) {
+    using L = FusedSmem<E>;
+    constexpr int N = 32 * E;
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* Z = (double2*)sm;
+    double2* scr = (double2*)(sm + L::Z);
+    double2* tw = (double2*)(sm + L::Z + L::SCR);
+    load_twiddles<E>(tw, gtw);
+    __syncthreads();
+    const int Ff = fine * (fine / 2 + 1);
+    for (int p = blockIdx.x; p < chunk; p += gridDim.x) {
+        const double* pp = part + (size_t)p * PP_COUNT;
+        const int dx = (int)pp[PP_DX], dy = (int)pp[PP_DY];
+        const double norm = pp[PP_NORM];
+        const T* img = raw + (size_t)p * N * N;
+        fused_forward<E>(Z, scr, tw, [&](int a, int b) { return translated_at(img, N, a, b, dx, dy, do_norm, avg, norm); });
+        fused_window<E>(Z, fine, out_re + (size_t)p * Ff, out_im + (size_t)p * Ff);
+        __syncthreads();
+    }
+}
+
+// Fimages_mask: noise image (backward transform of the chunk's noise spectra
+// [chunk][n][n/2+1]) or background average, soft mask, transform, window,
+// power spectrum and highres_Xi2
+template <int E, typename T>
+__global__ void __launch_bounds__(kFusedWarps * 32) fused_masked_kernel(
+    int chunk, int fine, const T* __restrict__ raw, const double* __restrict__ part, int do_norm, double avg,
+    const double2* __restrict__ gtw, const double* __restrict__ mw, const double2* __restrict__ noise,
+    const int* __restrict__ shell_start, const int* __restrict__ shell_pix, double* __restrict__ out_re,
+    double* __restrict__ out_im, double* __restrict__ power, double* __restrict__ xi2) {
+    using L = FusedSmem<E>;
+    constexpr int N = 32 * E, LD = N / 2 + 1;
+    extern __shared__ __align__(16) unsigned char sm[];
+    double2* Z = (double2*)sm;
+    double2* scr = (double2*)(sm + L::Z);
+    double2* tw = (double2*)(sm + L::Z + L::SCR);
+    double* spec = (double*)(sm + L::Z + L::SCR + L::TW);
+    double* red = (double*)(sm + L::Z + L::SCR + L::TW + L::SPEC);
+    load_twiddles<E>(tw, gtw);
+    __syncthreads();
+    const int Ff = fine * (fine / 2 + 1), fF = fine / 2 + 1;
+    const double nn = (double)N * N;
+    for (int p = blockIdx.x; p < chunk; p += gridDim.x) {
+        const double* pp = part + (size_t)p * PP_COUNT;
+        const int dx = (int)pp[PP_DX], dy = (int)pp[PP_DY];
+        const double norm = pp[PP_NORM];
+        const T* img = raw + (size_t)p * N * N;
+        double bg = 0.0;
+        if (noise) {
+            const double2* ns = noise + (size_t)p * N * LD;
+            for (int q = threadIdx.x; q < N * LD; q += blockDim.x) Z[zidx<N>(q / LD, q % LD)] = ns[q];
+            __syncthreads();
+            fused_backward<E>(Z, tw);
+        } else {
+            // softMaskOutsideMap's weighted background average
+            double s = 0.0, sw = 0.0;
+            for (int q = threadIdx.x; q < N * N; q += blockDim.x) {
+                const double w0 = mw[q];
+                if (w0 < 0.0) continue;
+                const double w = w0 > 1.0 ? 1.0 : w0;
+                s += w * translated_at(img, N, q / N, q % N, dx, dy, do_norm, avg, norm);
+                sw += w;
+            }
+            red[threadIdx.x] = s;
+            red[blockDim.x + threadIdx.x] = sw;
+            __syncthreads();
+            for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+                if (threadIdx.x < k) {
+                    red[threadIdx.x] += red[threadIdx.x + k];
+                    red[blockDim.x + threadIdx.x] += red[blockDim.x + threadIdx.x + k];
+                }
+                __syncthreads();
+            }
+            bg = red[0] / red[blockDim.x];
+            __syncthreads();
+        }
+        // soft mask into the real rows of Z (uncentred); 4 pixels per thread per step, loads first
+        for (int q0 = threadIdx.x; q0 < N * N; q0 += 4 * blockDim.x) {
+            double v[4], w[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + u * blockDim.x;
+                v[u] = 0.0;
+                w[u] = -1.0;
+                if (q < N * N) {
+                    v[u] = translated_at(img, N, q / N, q % N, dx, dy, do_norm, avg, norm);
+                    w[u] = mw[q];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int q = q0 + u * blockDim.x;
+                if (q >= N * N) continue;
+                double* row = (double*)(Z + (q / N) * LD);
+                double x = v[u];
+                if (w[u] >= 0.0) {
+                    const double add = noise ? row[q % N] : bg;
+                    x = w[u] > 1.0 ? add : (1 - w[u]) * x + w[u] * add;
+                }
+                row[q % N] = x;
+            }
+        }
+        __syncthreads();
+        fused_forward<E>(Z, scr, tw, [&](int a, int b) { return ((const double*)(Z + a * LD))[b]; });
+        fused_window<E>(Z, fine, out_re + (size_t)p * Ff, out_im + (size_t)p * Ff);
+        if (fine < N) {
+            for (int sh = threadIdx.x; sh < LD; sh += blockDim.x) {
+                double acc = 0.0;
+                for (int k = shell_start[sh]; k < shell_start[sh + 1]; ++k) {
+                    const int q = shell_pix[k];  // pixel i * (n/2+1) + j
+                    const double2 v = Z[zidx<N>(q / LD, q % LD)];
+                    const double re = __ddiv_rn(v.x, nn), im = __ddiv_rn(v.y, nn);
+                    acc += re * re + im * im;
+                }
+                spec[sh] = acc;
+                power[(size_t)p * LD + sh] = acc;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double x = 0.0;
+                for (int sh = fF; sh < LD; ++sh) x += spec[sh];
+                xi2[p] = x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 namespace {
@@ -491,7 +875,7 @@ struct PrepTables {
     bool valid = false;
     std::vector<double> key;  // sizes, mask radius and width, sigma2_fudge, sigma2_noise
     size_t o_ires = 0, o_sig = 0, o_pog = 0, o_dst = 0, o_dcn = 0, o_dpx = 0, o_zst = 0, o_zcn = 0, o_zpx = 0, o_ss = 0,
-           o_sp = 0, o_mw = 0;
+           o_sp = 0, o_mw = 0, o_tw = 0;
 };
 
 struct PrepState {
@@ -604,6 +988,7 @@ void build_tables(RomeGpuCtx* ctx, PrepTables& tb, int n, int fine, int G, bool 
     tb.o_ss = carve(shell_start.size() * 4);
     tb.o_sp = carve(shell_pix.size() * 4);
     tb.o_mw = carve(nn * 8);
+    tb.o_tw = carve((size_t)n * 16);
     char* tab = (char*)ctx->ws[S_PREP_TAB].get(bytes);
     auto up = [&](size_t off, const auto& v) {
         if (!v.empty()) {
@@ -622,9 +1007,53 @@ void build_tables(RomeGpuCtx* ctx, PrepTables& tb, int n, int fine, int G, bool 
     up(tb.o_ss, shell_start);
     up(tb.o_sp, shell_pix);
     up(tb.o_mw, mw);
+    // exp(-2 pi i q / n), q < n, for the fused kernels' transforms (host libm)
+    std::vector<double2> tw(n);
+    for (int q = 0; q < n; ++q)
+        tw[q] = make_double2(std::cos(2.0 * kPi * q / n), -std::sin(2.0 * kPi * q / n));
+    up(tb.o_tw, tw);
     // the host vectors are pageable: the copies are complete when they return, but wait anyway
     // so that nothing of this call's tables is in flight when the vectors go
     ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// one of the fused kernels (masked: the second) for n = 32, 64 or 128, on as
+// many CTAs as are resident (each loops over the chunk's images)
+template <int E, typename T>
+void launch_fused_e(int pc, int fine, const T* raw, const double* pp, int norm_on, double avg, const double2* gtw,
+                    double* re, double* im, const double* mw, const double2* noise, const int* ss, const int* sp,
+                    double* pow, double* xi2, cudaStream_t st, bool masked) {
+    const size_t smem = FusedSmem<E>::TOTAL;
+    int per_sm = 0, sms = 0, dev = 0;
+    ROME_CUDA(cudaGetDevice(&dev));
+    ROME_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (masked) {
+        auto k = fused_masked_kernel<E, T>;
+        ROME_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ROME_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kFusedWarps * 32, smem));
+        const int grid = std::max(1, std::min(pc, std::max(1, per_sm) * sms));
+        k<<<grid, kFusedWarps * 32, smem, st>>>(pc, fine, raw, pp, norm_on, avg, gtw, mw, noise, ss, sp, re, im, pow,
+                                                 xi2);
+    } else {
+        auto k = fused_nomask_kernel<E, T>;
+        ROME_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ROME_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kFusedWarps * 32, smem));
+        const int grid = std::max(1, std::min(pc, std::max(1, per_sm) * sms));
+        k<<<grid, kFusedWarps * 32, smem, st>>>(pc, fine, raw, pp, norm_on, avg, gtw, re, im);
+    }
+    ROME_CHECK_LAUNCH();
+}
+
+template <typename T>
+void launch_fused(int n, int pc, int fine, const T* raw, const double* pp, int norm_on, double avg,
+                  const double2* gtw, double* re, double* im, const double* mw, const double2* noise, const int* ss,
+                  const int* sp, double* pow, double* xi2, void*, cudaStream_t st, bool masked) {
+    if (n == 32)
+        launch_fused_e<1, T>(pc, fine, raw, pp, norm_on, avg, gtw, re, im, mw, noise, ss, sp, pow, xi2, st, masked);
+    else if (n == 64)
+        launch_fused_e<2, T>(pc, fine, raw, pp, norm_on, avg, gtw, re, im, mw, noise, ss, sp, pow, xi2, st, masked);
+    else
+        launch_fused_e<4, T>(pc, fine, raw, pp, norm_on, avg, gtw, re, im, mw, noise, ss, sp, pow, xi2, st, masked);
 }
 
 template <typename T>
@@ -725,15 +1154,19 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
 
     prof.begin(ROME_PHASE_IMAGES);
     // chunks of equal size bounded by the work buffers' footprint
-    const size_t per_img = nn * 8 + npix * 16 + (noise ? npix * 16 + nn * 8 : 0) + (in.images_on_device ? 0 : nn * sizeof(T));
+    // power-of-two sizes up to 128 run the fused shared-memory kernels; the
+    // others go through cuFFT with FP64 intermediates in HBM
+    const bool fused = n == 32 || n == 64 || n == 128;
+    const size_t per_img = (fused ? 0 : nn * 8 + npix * 16 + (noise ? nn * 8 : 0)) + (noise ? npix * 16 : 0) +
+                           (in.images_on_device ? 0 : nn * sizeof(T)) + 16;
     const size_t budget = ctx->workspace_limit ? ctx->workspace_limit : (size_t)1536 << 20;
     // (cuFFT's 32-bit plans: a chunk holds fewer than 2^31 elements)
     const int cmax = (int)std::max<size_t>(1, std::min<size_t>({(size_t)P, budget / per_img, (size_t)2147483647 / nn}));
     const int nchunk = (P + cmax - 1) / cmax, chunk = (P + nchunk - 1) / nchunk;
-    double* d_R = ctx->ws[S_PREP_R].as<double>((size_t)chunk * nn);
-    double2* d_C = ctx->ws[S_PREP_C].as<double2>((size_t)chunk * npix);
+    double* d_R = fused ? nullptr : ctx->ws[S_PREP_R].as<double>((size_t)chunk * nn);
+    double2* d_C = fused ? nullptr : ctx->ws[S_PREP_C].as<double2>((size_t)chunk * npix);
     double2* d_NC = noise ? ctx->ws[S_PREP_NC].as<double2>((size_t)chunk * npix) : nullptr;
-    double* d_NR = noise ? ctx->ws[S_PREP_NR].as<double>((size_t)chunk * nn) : nullptr;
+    double* d_NR = noise && !fused ? ctx->ws[S_PREP_NR].as<double>((size_t)chunk * nn) : nullptr;
     const T* d_raw_all = in.images_on_device ? (const T*)in.images : nullptr;
     T* d_raw_chunk = in.images_on_device ? nullptr : ctx->ws[S_PREP_RAW].as<T>((size_t)chunk * nn);
     const int norm_on = in.do_norm_correction ? 1 : 0;
@@ -768,7 +1201,8 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
             noise_spectra_kernel<<<(pc + kNoiseWarps - 1) / kNoiseWarps, kNoiseWarps * 32, 0, side>>>(
                 pc, (int)npix, oF, seed0 + (uint32_t)c0, pp, (const int*)at(tb.o_pog), (const int*)at(tb.o_dst),
                 (const int*)at(tb.o_dcn), (const int*)at(tb.o_dpx), (const int*)at(tb.o_zst), (const int*)at(tb.o_zcn),
-                (const int*)at(tb.o_zpx), d_ires, d_sig, d_NC);
+                (const int*)at(tb.o_zpx), d_ires, d_sig, fused ? (long)oF : (long)pc * oF, fused ? (long)npix : (long)oF,
+                d_NC);
             ROME_CHECK_LAUNCH();
             ROME_CUDA(cudaEventRecord(state->ev_noise, side));
             prof.launched(ROME_PHASE_IMAGES);
@@ -780,6 +1214,18 @@ void run_prepare(RomeGpuCtx* ctx, const RomePrepIn& in, RomePrepOut& out) {
             ROME_CUDA(cudaMemcpyAsync(d_raw_chunk, (const T*)in.images + (size_t)c0 * nn, (size_t)pc * nn * sizeof(T),
                                       cudaMemcpyHostToDevice, st));
             raw = d_raw_chunk;
+        }
+        if (fused) {
+            const auto* gtw = (const double2*)at(tb.o_tw);
+            launch_fused<T>(n, pc, fine, raw, pp, norm_on, avg, gtw, o_nre + (size_t)c0 * Ff, o_nim + (size_t)c0 * Ff,
+                            nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, st, false);
+            if (noise) ROME_CUDA(cudaStreamWaitEvent(st, state->ev_noise, 0));
+            launch_fused<T>(n, pc, fine, raw, pp, norm_on, avg, gtw, o_re + (size_t)c0 * Ff, o_im + (size_t)c0 * Ff,
+                            d_mw, noise ? d_NC : nullptr, d_ss, d_sp, d_pow + (size_t)c0 * oF, d_xi2 + c0, nullptr, st,
+                            true);
+            if (noise) ROME_CUDA(cudaEventRecord(state->ev_nc_free, st));
+            prof.launched(ROME_PHASE_IMAGES, 2);
+            continue;
         }
         PrepPlan& plan = get_plan(ctx, &state->plans, n, pc);
         // unmasked image

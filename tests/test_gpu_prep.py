@@ -206,3 +206,16 @@ def test_raw_images_to_estep_matches_reference(ctx, golden, case):
     assert frac >= 0.9
     for k in ["wsum_sigma2_noise", "wsum_pdf_class", "wsum_sigma2_offset", "wsum_sumw_group"]:
         assert relerr(out[k], g["pool0_after_update_" + k]) < SUM_TOL, k
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_size_128_against_oracle(ctx, dtype):
+    """128^2 (the benchmark size, shared-memory transforms) with current_size
+    < ori_size (power spectra, highres_Xi2), norm correction and offsets."""
+    P, ori, cur, G = 3, 128, 100, 2
+    raw, meta, group, sig2 = synthetic(P, ori, G, 12, dtype)
+    o = oracle_opts(particle_diameter=150.0, pixel_size=1.5)
+    ref = po.prepare_pool(raw, meta, group, sig2, cur, 40, o)
+    out = prepare_particles(ctx, images_from(raw, meta, group, 40), opts_from(o), sig2, cur)
+    compare(out, ref)
+    assert np.abs(ref["highres_Xi2"]).max() > 0
