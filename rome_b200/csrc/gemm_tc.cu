@@ -195,8 +195,11 @@ void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const v
 }
 
 void tc_bias_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
-                  const float* bias, int group, int* derr) {
-    launch<128, 2, 3>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
+                  const float* bias, int group, int* derr, bool split) {
+    if (split)
+        launch<128, 2, 3>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
+    else
+        launch<256, 1, 4>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
 }
 
 // hi/lo bf16 planes of a [rows][K] fp32 matrix, zero padded to Kpad columns
@@ -209,12 +212,12 @@ __global__ void split_bf16_kernel(const float* __restrict__ in, long rows, int K
     float v = k < K ? in[r * ldin + k] : 0.f;
     __nv_bfloat16 h = __float2bfloat16_rn(v);
     hi[q] = h;
-    lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
+    if (lo) lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
 }
 
-void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, int Kpad, void* out) {
+void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, int Kpad, void* out, bool with_lo) {
     __nv_bfloat16* hi = (__nv_bfloat16*)out;
-    __nv_bfloat16* lo = hi + rows * Kpad;
+    __nv_bfloat16* lo = with_lo ? hi + rows * Kpad : nullptr;
     long n = rows * Kpad;
     split_bf16_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, rows, K, ldin, Kpad, hi, lo);
     ROME_CHECK_LAUNCH();

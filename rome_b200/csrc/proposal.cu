@@ -658,15 +658,18 @@ void conv_forward(int Ci, int R, int A, int Co, int n, const float* x, const flo
     ROME_CHECK_LAUNCH();
 }
 
-void net_forward(RomeProposalNet* net, int n, cudaStream_t st) {
+// split: the head contraction in split BF16 (training: gradients checked
+// against the FP64 oracle); otherwise one BF16 product (the proposals rank
+// the outputs, the training loss does not see them)
+void net_forward(RomeProposalNet* net, int n, cudaStream_t st, bool split = true) {
     const int R = net->R, A = net->A;
     const float* P = net->params;
     conv_forward(2, R, A, net->c0, n, net->x, P + net->off[0], P + net->off[1], net->h0, st);
     conv_forward(net->c0, R, A, net->c1, n, net->h0, P + net->off[2], P + net->off[3], net->h1, st);
     net_expand_head(net, st);
-    split_bf16(st, net->h1, n, net->CRA, net->CRA, net->CRAp, net->hs);
+    split_bf16(st, net->h1, n, net->CRA, net->CRA, net->CRAp, net->hs, split);
     tc_bias_gemm(st, n, net->KA, net->CRAp, net->hs, net->wt, net->z, net->KA, net->params + net->off[5], A,
-                 net->ctx->d_err);
+                 net->ctx->d_err, split);
     net->ctx->total_launches += 4;
 }
 
@@ -914,7 +917,7 @@ void proposal_predict_device(RomeProposalNet* net, int n, const float* dfeat, in
         const int m = std::min(chunk, n - done);
         ROME_CUDA(cudaMemcpyAsync(net->x, dfeat + (long)done * row_x, sizeof(float) * row_x * m,
                                   cudaMemcpyDeviceToDevice, st));
-        net_forward(net, m, st);
+        net_forward(net, m, st, false);
         topk_warp_kernel<<<(m + PT / 32 - 1) / (PT / 32), PT, 0, st>>>(m, O, k, net->z, didx + (long)done * k,
                                                                        dprob ? dprob + (long)done * k : nullptr);
         ROME_CHECK_LAUNCH();
