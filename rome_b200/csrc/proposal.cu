@@ -125,9 +125,12 @@ __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A
                                                              const float* __restrict__ x,
                                                              const float* __restrict__ w,
                                                              const float* __restrict__ b, float* __restrict__ y) {
+    // one sample per block, its input and the weights in shared memory; a
+    // thread computes 4 output channels at 4 consecutive angles of one
+    // radius, so each input value it loads feeds 12 multiply-adds
     extern __shared__ float4 sm4[];
     float* xs = (float*)sm4;
-    const int RA = R * A, G = Co / 4;
+    const int RA = R * A, G = Co / 4, AB = (A + 3) / 4;
     float* ws = xs + ((long)Ci * RA + 3) / 4 * 4;
     const int n = blockIdx.x;
     const float* xn = x + (long)n * Ci * RA;
@@ -137,16 +140,23 @@ __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A
         ws[rest * Co + co] = w[q];
     }
     __syncthreads();
-    for (int item = threadIdx.x; item < G * RA; item += PT) {
-        const int g = item / RA, pos = item - g * RA;
-        const int r = pos / A, a = pos - r * A;
-        const int am = a == 0 ? A - 1 : a - 1, ap = a == A - 1 ? 0 : a + 1;
-        float acc[4] = {0.f, 0.f, 0.f, 0.f};
-        if (b) {
-            acc[0] = b[4 * g];
-            acc[1] = b[4 * g + 1];
-            acc[2] = b[4 * g + 2];
-            acc[3] = b[4 * g + 3];
+    for (int item = threadIdx.x; item < G * R * AB; item += PT) {
+        const int g = item / (R * AB), rem = item - g * (R * AB);
+        const int r = rem / AB, a0 = (rem - r * AB) * 4;
+        // the 6 angles a0-1 .. a0+4, circular
+        int ai[6];
+#pragma unroll
+        for (int u = 0; u < 6; u++) {
+            int aa = a0 + u - 1;
+            aa = aa < 0 ? aa + A : (aa >= A ? aa - A : aa);
+            ai[u] = aa;
+        }
+        float acc[4][4];
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            const float bias = b ? b[4 * g + c] : 0.f;
+#pragma unroll
+            for (int p = 0; p < 4; p++) acc[c][p] = bias;
         }
         for (int ci = 0; ci < Ci; ci++) {
             const float* xc = xs + ci * RA;
@@ -156,19 +166,28 @@ __global__ void __launch_bounds__(PT) pconv_fwd_smem_kernel(int Ci, int R, int A
                 const int rr = r + kh - 1;
                 if (rr < 0 || rr >= R) continue;
                 const float* row = xc + rr * A;
-                const float v[3] = {row[am], row[a], row[ap]};
+                float v[6];
+#pragma unroll
+                for (int u = 0; u < 6; u++) v[u] = row[ai[u]];
 #pragma unroll
                 for (int kw = 0; kw < 3; kw++) {
                     const float4 wv = wc[(kh * 3 + kw) * G];
-                    acc[0] = fmaf(wv.x, v[kw], acc[0]);
-                    acc[1] = fmaf(wv.y, v[kw], acc[1]);
-                    acc[2] = fmaf(wv.z, v[kw], acc[2]);
-                    acc[3] = fmaf(wv.w, v[kw], acc[3]);
+#pragma unroll
+                    for (int p = 0; p < 4; p++) {
+                        acc[0][p] = fmaf(wv.x, v[p + kw], acc[0][p]);
+                        acc[1][p] = fmaf(wv.y, v[p + kw], acc[1][p]);
+                        acc[2][p] = fmaf(wv.z, v[p + kw], acc[2][p]);
+                        acc[3][p] = fmaf(wv.w, v[p + kw], acc[3][p]);
+                    }
                 }
             }
         }
 #pragma unroll
-        for (int c = 0; c < 4; c++) y[(((long)n * Co + 4 * g + c) * R + r) * A + a] = RELU ? fmaxf(acc[c], 0.f) : acc[c];
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+            for (int p = 0; p < 4; p++)
+                if (a0 + p < A)
+                    y[(((long)n * Co + 4 * g + c) * R + r) * A + a0 + p] = RELU ? fmaxf(acc[c][p], 0.f) : acc[c][p];
     }
 }
 
