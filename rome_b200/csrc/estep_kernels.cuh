@@ -539,7 +539,7 @@ __global__ void scatter_by_j_kernel(int n, int T, const SigEntry* __restrict__ l
 
 // updateOtherParams over the particle's list segment (see wsum_kernel)
 template <int NT, int PIX>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
     wsum_list_kernel(int T, int nrot, int K, int F, int csF, int cs, int oriF, const SigEntry* __restrict__ list,
                      const int* __restrict__ seg, const double2* __restrict__ Fimg, const double* __restrict__ lctf,
                      int apply_ctf, const double2* __restrict__ proj, const int* __restrict__ actidx, int Kact,
@@ -618,7 +618,7 @@ __global__ void __launch_bounds__(NT)
 
 // backProjection over the orientation's list segment (see bp_kernel)
 template <int NT, int PIX>
-__global__ void __launch_bounds__(NT)
+__global__ void __launch_bounds__(NT, 4)
     bp_list_kernel(int T, int nrot, int F, int csF, int cs, const SigEntry* __restrict__ sorted,
                    const int* __restrict__ off, const double2* __restrict__ Fnm, const double* __restrict__ Mctf2,
                    const double2* __restrict__ shifts, const double2* __restrict__ ph,

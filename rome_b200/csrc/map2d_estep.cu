@@ -521,7 +521,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         const int cap = listcap;
         prof.begin(ROME_PHASE_WSUM);
         {
-            const int NT = 256, PIX = 8;
+            const int NT = 256, PIX = 4;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
             wsum_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
                 g.T, g.nrot, K, g.F, g.csF, cur, oriF, dList, dSeg, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
@@ -557,7 +557,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 scatter_by_j_kernel<<<(nsigtot + 255) / 256, 256, 0, st>>>(nsigtot, g.T, dList, dOff, dFill, dSorted);
                 prof.launched(ROME_PHASE_BACKPROJECT);
             }
-            const int NT = 256, PIX = 8;
+            const int NT = 256, PIX = 4;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
             bp_list_kernel<NT, PIX><<<dim3(nsplit, g.J), NT, 0, st>>>(
                 g.T, g.nrot, g.F, g.csF, cur, dSorted, dOff, dFnm, dMctf2, dShift, dPh, dRot, ctx->r_max,
