@@ -184,26 +184,66 @@ __device__ __forceinline__ double hyp_weight(float d, double mn, double pdir, do
 // pass size (windowFourierTransform / windowTransform, src/image.h:419-568)
 // and build Minvsigma2 = 1/(sigma2_fudge * sigma2_noise[ires]), 0 at ires <= 0.
 // rows: optional input row of each particle (a subset of a staged pool).
+// The restricted tensor-core search's per-particle operands come out of the
+// same pass when xw is given (the restricted_prep_kernel arithmetic, in its
+// order): xw[i][a] = Minvsigma2 * ctf * X and w2[i][a] = Minvsigma2 * ctf^2 at
+// the active pixels a = actidx[n] (zero up to Kh), S[i] = sum_n Minvsigma2 |X|^2.
+struct RestrictedOut {
+    float2* xw = nullptr;
+    float* w2 = nullptr;
+    float* S = nullptr;
+    const int* actidx = nullptr;
+    int Kact = 0, Kh = 0, apply_ctf = 0;
+};
+
 __global__ void prep_particles_kernel(int P, int cur, int cs, const double* __restrict__ Fr,
                                       const double* __restrict__ Fi, const double* __restrict__ ctf_fine,
                                       const int* __restrict__ Mresol, const double* __restrict__ sigma2,
                                       const int* __restrict__ group, int oriF, double fudge, double2* __restrict__ Fimg,
                                       double* __restrict__ lctf, double* __restrict__ Minv,
-                                      const int* __restrict__ rows = nullptr) {
+                                      const int* __restrict__ rows = nullptr, RestrictedOut ro = RestrictedOut{}) {
+    __shared__ double red[32];
     const int i = blockIdx.x;
     const long ri = rows ? rows[i] : i;
     const int curF = cur / 2 + 1, curF2 = cur * curF, csF = cs / 2 + 1, F = cs * csF;
     const double* s2 = sigma2 + (long)group[i] * oriF;
+    double s = 0.0;
     for (int n = threadIdx.x; n < F; n += blockDim.x) {
         int oi = n / csF, j = n - oi * csF;
         int ip = oi < csF ? oi : oi - cs;
         int in_i = ip < 0 ? ip + cur : ip;
         long src = ri * curF2 + (long)in_i * curF + j;
         long dst = (long)i * F + n;
-        Fimg[dst] = make_double2(Fr[src], Fi[src]);
-        lctf[dst] = ctf_fine[src];
+        const double2 X = make_double2(Fr[src], Fi[src]);
+        const double c = ctf_fine[src];
+        Fimg[dst] = X;
+        lctf[dst] = c;
         int ires = Mresol[n];
-        Minv[dst] = ires > 0 ? 1. / (fudge * s2[ires]) : 0.;
+        const double m = ires > 0 ? 1. / (fudge * s2[ires]) : 0.;
+        Minv[dst] = m;
+        if (ro.xw) {
+            s += m * (X.x * X.x + X.y * X.y);
+            const int a = ro.actidx[n];
+            if (a >= 0) {
+                const double cc = ro.apply_ctf ? c : 1.0;
+                const double wd = ro.apply_ctf ? m * c : m;
+                ro.xw[(long)i * ro.Kh + a] = make_float2((float)(wd * X.x), (float)(wd * X.y));
+                ro.w2[(long)i * ro.Kh + a] = (float)(m * cc * cc);
+            }
+        }
+    }
+    if (!ro.xw) return;
+    for (int a = ro.Kact + threadIdx.x; a < ro.Kh; a += blockDim.x) {
+        ro.xw[(long)i * ro.Kh + a] = make_float2(0.f, 0.f);
+        ro.w2[(long)i * ro.Kh + a] = 0.f;
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); q++) t += red[q];
+        ro.S[i] = (float)t;
     }
 }
 

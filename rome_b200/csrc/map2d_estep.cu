@@ -261,9 +261,23 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             dFimg = ctx->ws[S_FIMG].as<double2>((size_t)P * g.F);
             dLctf = ctx->ws[S_CTF].as<double>((size_t)P * g.F);
             dMinv = ctx->ws[S_MINV].as<double>((size_t)P * g.F);
+            // the restricted tensor-core search takes its per-particle operands from the same pass
+            const bool rtc_pass = restricted && ctx->precision != ROME_PREC_FP32 && g.T <= 256;
+            RestrictedOut ro;
+            if (rtc_pass) {
+                const int Kh = g.Kp / 2;
+                char* buf = (char*)ctx->ws[S_A].get((size_t)P * Kh * (sizeof(float2) + sizeof(float)));
+                ro.xw = (float2*)buf;
+                ro.w2 = (float*)(buf + (size_t)P * Kh * sizeof(float2));
+                ro.S = ctx->ws[S_S].as<float>((size_t)P * g.T);
+                ro.actidx = dActIdx;
+                ro.Kact = g.Kact;
+                ro.Kh = Kh;
+                ro.apply_ctf = apply_ctf ? 1 : 0;
+            }
             prof.begin(ROME_PHASE_PREP);
             prep_particles_kernel<<<P, 256, 0, st>>>(P, cur, cs, dFr, dFi, dCtf, dMres, dSig2, dGroup, oriF,
-                                                      in->sigma2_fudge, dFimg, dLctf, dMinv, dRows);
+                                                      in->sigma2_fudge, dFimg, dLctf, dMinv, dRows, ro);
             prof.launched(ROME_PHASE_PREP);
             prof.end(ROME_PHASE_PREP);
 
@@ -319,12 +333,10 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                 g.T, g.Kact, g.csF, cs, dAct, dShift, ctx->shift_sampling, dPidx);
             prof.launched(ROME_PHASE_SHIFT);
             if (rtc) {
-                char* buf = (char*)ctx->ws[S_A].get((size_t)P * Kh * (sizeof(float2) + sizeof(float)));
-                dXw = (float2*)buf;
-                dW2h = (float*)(buf + (size_t)P * Kh * sizeof(float2));
+                // xw, w2 and S were written by prep_particles_kernel (ro)
+                dXw = ro.xw;
+                dW2h = ro.w2;
                 dSh = ctx->ws[S_NORM].get((size_t)2 * restricted_tile_tn(g.T) * g.Kp * 2);
-                restricted_prep(st, P, g.F, g.Kact, Kh, dFimg, dLctf, dMinv, apply_ctf ? 1 : 0, dAct, dXw, dW2h, dS);
-                prof.launched(ROME_PHASE_SHIFT);
                 restricted_shift_operand(st, g.T, g.Kact, g.Kp, dPidx, ctx->d_shift_tab, ctx->precision, dSh);
                 prof.launched(ROME_PHASE_SHIFT);
             } else {
