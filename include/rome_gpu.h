@@ -123,6 +123,27 @@ int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, 
  * (src/map_model.cpp:209-231). */
 int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int clear_src);
 
+/* Back-projection of n particle images at known poses into class iclass's
+ * 3D back-projector: the per-image loop of the reference's rome_reconstruct
+ * (apps/rome_reconstruct.cpp:160-330).  Fimg_real/imag: [n][size][size/2+1]
+ * FFTW half-plane transforms of the centred images (what the image
+ * preparation returns as the unmasked transform, with zero old offsets, at
+ * current size = size).  Fctf: [n][size][size/2+1] CTF images, or NULL for
+ * no CTF.  poses: [n][5] = rot, tilt, psi (degrees), xoff, yoff (pixels),
+ * host memory.  Each image is shifted by (xoff, yoff) with the tabulated
+ * phases of shiftImageInFourierTransform (src/image.h:1478-1575),
+ * multiplied by its CTF and scattered with weight CTF^2 by
+ * MyBackProjector::backproject (src/reconstruct.cpp:977-1164); the volume
+ * accumulates (+=) until rome_gpu_set_projectors or
+ * rome_gpu_set_backprojector replaces it.  A zero
+ * offset leaves the spectrum unshifted.  inputs_on_device: Fimg_* and Fctf
+ * are device pointers.  size must equal the back-projector's ori_size;
+ * follow with rome_gpu_reconstruct (do_map 0, normalise 1) for the
+ * reference's reconstruction. */
+int rome_gpu_backproject_images(RomeGpuCtx* ctx, int iclass, int n, int size, const double* Fimg_real,
+                                const double* Fimg_imag, const double* Fctf, const double* poses,
+                                int inputs_on_device);
+
 /* ---------------------------------------------------------------------
  * Particle image preparation for one pool.  Replaces
  * ParticleModel::setFourierTransforms (src/exp_model.h:397-640), called by

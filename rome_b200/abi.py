@@ -173,7 +173,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_proposal_loss_grad", "rome_gpu_proposal_train", "rome_gpu_proposal_predict",
     "rome_gpu_proposal_propose",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
-    "rome_gpu_add_backprojectors", "rome_gpu_prepare_particles",
+    "rome_gpu_add_backprojectors", "rome_gpu_prepare_particles", "rome_gpu_backproject_images",
 ]
 
 _LIB = None
@@ -226,6 +226,8 @@ def load_library():
     lib.rome_gpu_select_significant.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP, _DP]
     lib.rome_gpu_copy_from_host.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]
     lib.rome_gpu_add_backprojectors.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.rome_gpu_backproject_images.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, _DP, C.c_int]
     lib.rome_gpu_select_significant_static.argtypes = [C.c_void_p, C.c_int, C.c_long, _DP, _DP, C.c_double, _DP,
                                                        _DP]
     lib.rome_gpu_reconstruct.argtypes = [C.c_void_p, C.POINTER(RomeReconIn), C.POINTER(RomeReconOut)]

@@ -335,6 +335,50 @@ __global__ void __launch_bounds__(NT)
     if (threadIdx.x == 0 && sumwd != 0.0) atomicAdd(&normcorr[i], sumwd);
 }
 
+// Trilinear scatter of one slice coefficient (x, y) with value (vr, vi) and
+// weight mw into a class volume: MyBackProjector::backproject
+// (src/reconstruct.cpp:977-1164) for one pixel, with the reference's
+// operation order.  A is Ainv = A^T * padding; points with xp < 0 go to
+// their Friedel mate (negated coordinates, conjugated value).
+__device__ __forceinline__ void bp3d_scatter(const Rot3& A, double x, double y, double vr, double vi, double mw,
+                                             int pad, int padF, double2* __restrict__ D, double* __restrict__ W) {
+    const int shift = -(int)((float)pad / 2.0f);
+    const long py = padF, pz = (long)pad * padF;
+    double xp = dadd(dmul(A.a00, x), dmul(A.a01, y));
+    double yp = dadd(dmul(A.a10, x), dmul(A.a11, y));
+    double zp = dadd(dmul(A.a20, x), dmul(A.a21, y));
+    if (xp < 0) {
+        xp = -xp;
+        yp = -yp;
+        zp = -zp;
+        vi = -vi;
+    }
+    const int x0 = (int)floor(xp);
+    const double fx = dsub(xp, (double)x0);
+    int y0 = (int)floor(yp);
+    const double fy = dsub(yp, (double)y0);
+    y0 -= shift;
+    int z0 = (int)floor(zp);
+    const double fz = dsub(zp, (double)z0);
+    z0 -= shift;
+    const double mfx = dsub(1., fx), mfy = dsub(1., fy), mfz = dsub(1., fz);
+    const double dd[8] = {dmul(dmul(mfz, mfy), mfx), dmul(dmul(mfz, mfy), fx), dmul(dmul(mfz, fy), mfx),
+                          dmul(dmul(mfz, fy), fx),   dmul(dmul(fz, mfy), mfx), dmul(dmul(fz, mfy), fx),
+                          dmul(dmul(fz, fy), mfx),   dmul(dmul(fz, fy), fx)};
+    const long b000 = z0 * pz + y0 * py + x0;
+    const long base[4] = {b000, b000 + py, b000 + pz, b000 + pz + py};  // (z0,y0) (z0,y1) (z1,y0) (z1,y1)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        double* td = (double*)(D + base[c]);
+        atomicAdd(td + 0, dmul(dd[2 * c], vr));
+        atomicAdd(td + 1, dmul(dd[2 * c], vi));
+        atomicAdd(td + 2, dmul(dd[2 * c + 1], vr));
+        atomicAdd(td + 3, dmul(dd[2 * c + 1], vi));
+        atomicAdd(W + base[c], dmul(dd[2 * c], mw));
+        atomicAdd(W + base[c] + 1, dmul(dd[2 * c + 1], mw));
+    }
+}
+
 // backProjection (src/map3d_optimizer.cpp:2360-2479): per fine orientation,
 // the weighted sum of the significant shifted nomask images (times ctf *
 // Minvsigma2) and of ctf^2 * Minvsigma2, then MyBackProjector::backproject
@@ -396,50 +440,61 @@ __global__ void __launch_bounds__(NT)
         }
     }
     const Rot3 A = rot[j];
-    const int shift = -(int)((float)pad / 2.0f);
     double2* D = bp_data + (long)jclass[j] * vox;
     double* W = bp_weight + (long)jclass[j] * vox;
-    const long py = padF, pz = (long)pad * padF;
 #pragma unroll
     for (int p = 0; p < PIX; p++) {
         if (!on[p]) continue;
         const double mw = sw[p];
         if (!(mw > 0.)) continue;
-        const double x = (double)xs[p], y = (double)ys[p];
-        double vr = sr[p], vi = si[p];
-        double xp = dadd(dmul(A.a00, x), dmul(A.a01, y));
-        double yp = dadd(dmul(A.a10, x), dmul(A.a11, y));
-        double zp = dadd(dmul(A.a20, x), dmul(A.a21, y));
-        if (xp < 0) {
-            xp = -xp;
-            yp = -yp;
-            zp = -zp;
-            vi = -vi;
-        }
-        const int x0 = (int)floor(xp);
-        const double fx = dsub(xp, (double)x0);
-        int y0 = (int)floor(yp);
-        const double fy = dsub(yp, (double)y0);
-        y0 -= shift;
-        int z0 = (int)floor(zp);
-        const double fz = dsub(zp, (double)z0);
-        z0 -= shift;
-        const double mfx = dsub(1., fx), mfy = dsub(1., fy), mfz = dsub(1., fz);
-        const double dd[8] = {dmul(dmul(mfz, mfy), mfx), dmul(dmul(mfz, mfy), fx), dmul(dmul(mfz, fy), mfx),
-                              dmul(dmul(mfz, fy), fx),   dmul(dmul(fz, mfy), mfx), dmul(dmul(fz, mfy), fx),
-                              dmul(dmul(fz, fy), mfx),   dmul(dmul(fz, fy), fx)};
-        const long b000 = z0 * pz + y0 * py + x0;
-        const long base[4] = {b000, b000 + py, b000 + pz, b000 + pz + py};  // (z0,y0) (z0,y1) (z1,y0) (z1,y1)
+        bp3d_scatter(A, (double)xs[p], (double)ys[p], sr[p], si[p], mw, pad, padF, D, W);
+    }
+}
+
+// Back-projection of whole particle images at known poses: the per-image
+// loop of rome_reconstruct (apps/rome_reconstruct.cpp:160-330).  Image i's
+// spectrum is shifted by its own offset with the tabulated phases of
+// shiftImageInFourierTransform (src/image.h:1478-1575: dotp, index
+// (int)(|dotp| / sampling) % 5000, sign of dotp on the sine), multiplied by
+// its CTF, and scattered with weight CTF^2 (unit value and weight without
+// CTF) through MyBackProjector::backproject (src/reconstruct.cpp:977-1164).
+// One block row per image (blockIdx.y), PIX pixels per thread.
+template <int NT, int PIX>
+__global__ void __launch_bounds__(NT)
+    bp_images_kernel(int F, int csF, int cs, const double* __restrict__ Fre, const double* __restrict__ Fim,
+                     const double* __restrict__ Fctf, const double2* __restrict__ shifts,
+                     const double2* __restrict__ tab, double sampling, const Rot3* __restrict__ rot, int r_max,
+                     int pad, int padF, double2* __restrict__ D, double* __restrict__ W) {
+    const long i = blockIdx.y;
+    const double2 sh = shifts[i];
+    const Rot3 A = rot[i];
+    const int max_r2 = r_max * r_max;
+    const double two_pi = 2 * kPi;
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            double* td = (double*)(D + base[c]);
-            atomicAdd(td + 0, dmul(dd[2 * c], vr));
-            atomicAdd(td + 1, dmul(dd[2 * c], vi));
-            atomicAdd(td + 2, dmul(dd[2 * c + 1], vr));
-            atomicAdd(td + 3, dmul(dd[2 * c + 1], vi));
-            atomicAdd(W + base[c], dmul(dd[2 * c], mw));
-            atomicAdd(W + base[c] + 1, dmul(dd[2 * c + 1], mw));
-        }
+    for (int p = 0; p < PIX; p++) {
+        const int n = blockIdx.x * NT * PIX + threadIdx.x + p * NT;
+        if (n >= F) continue;
+        const int row = n / csF, x = n - row * csF;
+        int y;
+        if (row <= r_max) {
+            y = row;
+            if (x > r_max) continue;
+        } else if (row >= cs - r_max) {
+            y = row - cs;
+            if (x < 1 || x > r_max) continue;  // x == 0 column stored twice in FFTW order: only once here
+        } else
+            continue;
+        if (x * x + y * y > max_r2) continue;
+        const double c = Fctf ? Fctf[i * F + n] : 1.0;
+        const double mw = Fctf ? dmul(c, c) : 1.0;
+        if (!(mw > 0.)) continue;
+        const double2 v = make_double2(Fre[i * F + n], Fim[i * F + n]);
+        const double dotp = dmul(two_pi, dadd(dmul((double)x, sh.x), dmul((double)y, sh.y)));
+        const int idx = ((int)__ddiv_rn(fabs(dotp), sampling)) % 5000;
+        const double2 cs2 = tab[idx];
+        const double2 s = apply_phase(sh, make_double2(cs2.x, dotp < 0 ? -cs2.y : cs2.y), v);
+        const double vr = Fctf ? dmul(s.x, c) : s.x, vi = Fctf ? dmul(s.y, c) : s.y;
+        bp3d_scatter(A, (double)x, (double)y, vr, vi, mw, pad, padF, D, W);
     }
 }
 

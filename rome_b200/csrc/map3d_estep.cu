@@ -713,3 +713,59 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             if (h_sum[i] == 0) fail(ROME_ERR_NUMERIC, "exp_sum_weight[%d] == 0", i);
     });
 }
+
+extern "C" int rome_gpu_backproject_images(RomeGpuCtx* ctx, int iclass, int n, int size, const double* Fimg_real,
+                                           const double* Fimg_imag, const double* Fctf, const double* poses,
+                                           int inputs_on_device) {
+    if (!ctx) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->bp_data || ctx->ref_dim != 3) fail(ROME_ERR_STATE, "3D back-projectors not set (rome_gpu_set_projectors)");
+        ROME_REQUIRE(iclass >= 0 && iclass < ctx->nr_classes, "iclass %d out of range", iclass);
+        ROME_REQUIRE(n >= 0 && Fimg_real && Fimg_imag && poses, "bad back-projection args");
+        ROME_REQUIRE(size == ctx->ori_size, "image size %d differs from the back-projector's %d", size,
+                     ctx->ori_size);
+        if (n == 0) return;
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        arena_reset(ctx);
+        cudaStream_t st = ctx->stream;
+        const int csF = size / 2 + 1, F = size * csF;
+        const int r_max = std::min(ctx->r_max, size / 2);
+        std::vector<Rot3> hrot(n);
+        std::vector<double2> hsh(n);
+        for (int i = 0; i < n; i++) {
+            const double* a = poses + 5 * (size_t)i;
+            for (int q = 0; q < 5; q++)
+                ROME_REQUIRE(std::isfinite(a[q]), "pose %d field %d is not finite", i, q);
+            hrot[i] = rot3_inv(a[0], a[1], a[2], ctx->padding);
+            hsh[i] = make_double2(a[3] / (-size), a[4] / (-size));
+        }
+        Rot3* dRot = upload3(ctx, S_ROTM, hrot.data(), hrot.size());
+        double2* dSh = upload3(ctx, S_SHIFT, hsh.data(), hsh.size());
+        const double *dRe = Fimg_real, *dIm = Fimg_imag, *dCtf = Fctf;
+        if (!inputs_on_device) {
+            double* buf = ctx->ws[S_FNOMASK].as<double>((size_t)2 * n * F);
+            ROME_CUDA(cudaMemcpyAsync(buf, Fimg_real, sizeof(double) * n * F, cudaMemcpyHostToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(buf + (size_t)n * F, Fimg_imag, sizeof(double) * n * F, cudaMemcpyHostToDevice,
+                                      st));
+            dRe = buf;
+            dIm = buf + (size_t)n * F;
+            if (Fctf) {
+                double* c = ctx->ws[S_CTF].as<double>((size_t)n * F);
+                ROME_CUDA(cudaMemcpyAsync(c, Fctf, sizeof(double) * n * F, cudaMemcpyHostToDevice, st));
+                dCtf = c;
+            }
+        }
+        const int NT = 256, PIX = 4;
+        const int nsplit = (F + NT * PIX - 1) / (NT * PIX);
+        for (int i0 = 0; i0 < n; i0 += 65535) {  // grid y limit
+            const int m = std::min(n - i0, 65535);
+            const size_t o = (size_t)i0 * F;
+            bp_images_kernel<NT, PIX><<<dim3(nsplit, m), NT, 0, st>>>(
+                F, csF, size, dRe + o, dIm + o, dCtf ? dCtf + o : nullptr, dSh + i0, ctx->d_shift_tab,
+                ctx->shift_sampling, dRot + i0, r_max, ctx->pad_size, ctx->pad_size / 2 + 1,
+                ctx->bp_data + (long)iclass * ctx->vox, ctx->bp_weight + (long)iclass * ctx->vox);
+            ROME_CHECK_LAUNCH();
+        }
+        ROME_CUDA(cudaStreamSynchronize(st));
+    });
+}

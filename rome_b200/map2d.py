@@ -356,6 +356,34 @@ class GpuContext:
         """This context's back-projectors += src's (same device), src zeroed when clear."""
         self._check(self.lib.rome_gpu_add_backprojectors(self.h, src.h, int(clear)))
 
+    def backproject_images(self, iclass: int, Fimg_real, Fimg_imag, Fctf, poses: np.ndarray):
+        """rome_gpu_backproject_images: images [n][F] at poses [n][5] (rot,
+        tilt, psi, xoff, yoff) into class iclass's 3D back-projector.  The
+        spectra (and Fctf, or None) are numpy arrays or torch CUDA tensors
+        (float64, contiguous) on this context's device."""
+        poses = _f64(poses).reshape(-1, 5)
+        n = poses.shape[0]
+        on_dev = not isinstance(Fimg_real, np.ndarray)
+        if on_dev:
+            arrs = [Fimg_real, Fimg_imag] + ([Fctf] if Fctf is not None else [])
+            for a in arrs:
+                if not (a.is_cuda and a.is_contiguous() and str(a.dtype) == "torch.float64"
+                        and a.device.index == self.device and a.shape[0] == n):
+                    raise ValueError("device spectra must be contiguous float64 CUDA tensors of n rows on this device")
+            ptr = [a.data_ptr() for a in arrs] + ([None] if Fctf is None else [])
+        else:
+            arrs = [_f64(Fimg_real), _f64(Fimg_imag)] + ([_f64(Fctf)] if Fctf is not None else [])
+            for a in arrs:
+                if a.shape[0] != n:
+                    raise ValueError("spectra and poses disagree on the number of images")
+            ptr = [a.ctypes.data for a in arrs] + ([None] if Fctf is None else [])
+        F = int(arrs[0].shape[1])
+        size = int(round((1 + 2 * F) ** 0.5)) - 1       # F = size * (size / 2 + 1)
+        if size * (size // 2 + 1) != F or any(int(a.shape[1]) != F for a in arrs):
+            raise ValueError(f"{F} coefficients per image is not a half-plane transform of a square image")
+        self._check(self.lib.rome_gpu_backproject_images(self.h, iclass, n, size, ptr[0], ptr[1], ptr[2],
+                                                         abi.dptr(poses), int(on_dev)))
+
     def set_backprojector(self, iclass: int, data: np.ndarray, weight: np.ndarray):
         self._check(self.lib.rome_gpu_set_backprojector(self.h, iclass, abi.dptr(_f64(data)), abi.dptr(_f64(weight))))
 

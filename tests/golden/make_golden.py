@@ -54,6 +54,14 @@ CASES3D = {
                 dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1, pool=4,
                      offset_range=2, offset_step=1, ctf=1, uniform_directions=1)),
 }
+# reconstruction at known poses: (dataset spec, rome_reconstruct options) for oracle/_ref/rome_reconstruct_ref
+CASESRECON = {
+    # 32^2 particles of one blob volume, CTF on, poses and origins from the generator, 10 gridding iterations
+    "recon3d_a": (Map3dSpec(n_particles=300, size=32, n_classes=1, n_blobs=15, blob_sigma=(1.5, 3.0), max_shift=2.0,
+                            snr=1.0, pixel=3.0, seed=11),
+                  dict(angpix=3.0, ctf=1, iter=10)),
+}
+
 SKIP3D = ("Fimg_shifted_real", "Fimg_shifted_imag", "local_Fctf", "Minvsigma2", "local_sqrtXi2")
 
 # arrays copied from the dump into the fixture (the per-translation shifted
@@ -64,7 +72,7 @@ SKIP_SUFFIXES = ("Fimg_shifted_real", "Fimg_shifted_imag", "Fref_real", "Fref_im
 
 def build_reference():
     subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "_ref/map2d_dump", "_ref/map3d_dump",
-                           "_ref/librome_oracle.so"], stdout=subprocess.DEVNULL)
+                           "_ref/librome_oracle.so", "_ref/rome_reconstruct_ref"], stdout=subprocess.DEVNULL)
 
 
 def make_case3d(name: str):
@@ -84,6 +92,59 @@ def make_case3d(name: str):
         out = os.path.join(HERE, name + ".npz")
         np.savez_compressed(out, **keep)
         print(f"{name}: {len(keep)} arrays, {os.path.getsize(out) / 1e6:.2f} MB")
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def write_posed_star(path: str, mrcs: str, meta: dict, spec) -> None:
+    """A particle STAR with the generating poses: rlnAngleRot/Tilt/Psi and
+    rlnOriginX/Y = minus the generating shift (the offset that recentres the
+    particle), plus the CTF columns."""
+    labels = ["rlnImageName", "rlnMicrographName", "rlnDefocusU", "rlnDefocusV", "rlnDefocusAngle", "rlnVoltage",
+              "rlnSphericalAberration", "rlnAmplitudeContrast", "rlnAngleRot", "rlnAngleTilt", "rlnAnglePsi",
+              "rlnOriginX", "rlnOriginY"]
+    with open(path, "w") as f:
+        f.write("\ndata_\n\nloop_\n")
+        for i, lab in enumerate(labels):
+            f.write(f"_{lab} #{i + 1}\n")
+        for p in range(len(meta["du"])):
+            f.write(f"{p + 1:06d}@{mrcs} mic{p % 5:03d}.mrc {meta['du'][p]:.6f} {meta['dv'][p]:.6f} "
+                    f"{meta['dang'][p]:.6f} {spec.voltage:.6f} {spec.cs:.6f} {spec.q0:.6f} {meta['rot'][p]:.6f} "
+                    f"{meta['tilt'][p]:.6f} {meta['psi'][p]:.6f} {-meta['shx'][p]:.6f} {-meta['shy'][p]:.6f}\n")
+
+
+def recon_dataset(name: str, out_dir: str) -> str:
+    """Write the seeded dataset of a reconstruction case; returns the STAR path."""
+    from rome_b200.synthetic import make_particles_3d, write_mrcs
+    spec, _ = CASESRECON[name]
+    os.makedirs(out_dir, exist_ok=True)
+    imgs, meta, _ = make_particles_3d(spec)
+    mrcs = os.path.abspath(os.path.join(out_dir, name + ".mrcs"))
+    write_mrcs(mrcs, imgs, spec.pixel)
+    star = os.path.join(out_dir, name + ".star")
+    write_posed_star(star, mrcs, meta, spec)
+    return star
+
+
+def make_recon_case(name: str):
+    """Run the reference's rome_reconstruct on the case's dataset and keep
+    the reconstructed volume (float32, as the reference writes it)."""
+    from rome_b200.star_mrcs import read_mrcs_header
+    _, opt = CASESRECON[name]
+    tmp = tempfile.mkdtemp(prefix="rome_golden_")
+    try:
+        star = recon_dataset(name, os.path.join(tmp, "data"))
+        out = os.path.join(tmp, "recon")
+        cmd = [os.path.join(ROOT, "oracle", "_ref", "rome_reconstruct_ref"), "-i", star, "-o", out]
+        for k, v in opt.items():
+            cmd += [f"-{k}", str(v)]
+        env = dict(os.environ, OMP_NUM_THREADS="1")
+        subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=tmp)
+        h = read_mrcs_header(out + ".mrc")
+        vol = np.fromfile(out + ".mrc", "<f4", offset=1024).reshape(h.ns, h.nr, h.nc)
+        dst = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(dst, vol=vol, meta_options=np.array([str(opt)]))
+        print(f"{name}: volume {vol.shape}, {os.path.getsize(dst) / 1e6:.2f} MB")
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 
@@ -117,9 +178,11 @@ def make_case(name: str):
 
 if __name__ == "__main__":
     build_reference()
-    names = sys.argv[1:] or list(CASES) + list(CASES3D)
+    names = sys.argv[1:] or list(CASES) + list(CASES3D) + list(CASESRECON)
     for n in names:
-        if n in CASES3D:
+        if n in CASESRECON:
+            make_recon_case(n)
+        elif n in CASES3D:
             make_case3d(n)
         else:
             make_case(n)
