@@ -32,6 +32,16 @@ METRIC = "E-step particles/s: learned-proposal+BF16 vs plain FP32 GPU at >=99% p
 UNIT = "particles/s"
 
 
+
+def tuned_shapes():
+    """The tensor-core autotuner's choices: kind/planes N x Kp (128-row tiles) -> tile, with candidate times."""
+    from rome_b200 import abi
+    out = {}
+    for r in abi.tuning_report():
+        key = f"{r['kind']}/{r['planes']}p N={r['N']} Kp={r['Kp']} mtiles={r['mtiles']}"
+        out[key] = {"choice": r["choice"], "ms": {k: float(v[:-2]) for k, v in r.items() if v.endswith("ms")}}
+    return out
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -380,6 +390,7 @@ def run_ours(args):
         "exhaustive_%s" % args.precision: {"value": round(N / (ex_ms / 1e3), 2), "unit": UNIT},
         "clocks": clk.summary(),
     }
+    line["autotune"] = tuned_shapes()
     if fp32_line is not None:
         line["plain_fp32"] = fp32_line
     if train_info is not None:

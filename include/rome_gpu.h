@@ -91,6 +91,17 @@ typedef struct {
 } RomeGpuTimings;
 
 int rome_gpu_get_timings(RomeGpuCtx* ctx, RomeGpuTimings* out);
+
+/* The tensor-core contractions' tile-shape autotuner (no reference
+ * counterpart): the first call of a contraction with a new key (kind,
+ * operand planes, device, N, Kp, 128-row tiles rounded up to a power of
+ * two) times every candidate tile shape on its own operands and keeps the
+ * fastest; all candidates give identical outputs.  ROME_TC_TUNE=0 in the
+ * environment disables it (default shapes); ROME_TC_SHAPE=<i> pins
+ * candidate i of every list.  Writes one line per key with
+ * the choice and every candidate's time (process-wide, all contexts) into
+ * buf (NUL-terminated, truncated to len) and returns the full length. */
+size_t rome_gpu_tuning_report(char* buf, size_t len);
 int rome_gpu_reset_timings(RomeGpuCtx* ctx);
 
 /* Context lifetime.  Replaces nothing in the reference (it owns no device). */

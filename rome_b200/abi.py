@@ -174,9 +174,27 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_proposal_propose",
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
     "rome_gpu_add_backprojectors", "rome_gpu_prepare_particles", "rome_gpu_backproject_images",
+    "rome_gpu_tuning_report",
 ]
 
 _LIB = None
+
+
+def tuning_report() -> list:
+    """The tensor-core autotuner's choices, one dict per key."""
+    lib = load_library()
+    n = lib.rome_gpu_tuning_report(None, 0)
+    buf = C.create_string_buffer(n + 1)
+    lib.rome_gpu_tuning_report(buf, n + 1)
+    out = []
+    for line in buf.value.decode().splitlines():
+        f = line.split()
+        d = {"kind": f[0]}
+        for kv in f[1:]:
+            k, v = kv.split("=", 1) if "=" in kv else kv.split(":", 1)
+            d[k] = v
+        out.append(d)
+    return out
 
 
 def library_path() -> str:
@@ -234,5 +252,7 @@ def load_library():
     lib.rome_gpu_prepare_particles.argtypes = [C.c_void_p, C.POINTER(RomePrepIn), C.POINTER(RomePrepOut)]
     lib.rome_gpu_get_timings.argtypes = [C.c_void_p, C.POINTER(RomeGpuTimings)]
     lib.rome_gpu_reset_timings.argtypes = [C.c_void_p]
+    lib.rome_gpu_tuning_report.argtypes = [C.c_char_p, C.c_size_t]
+    lib.rome_gpu_tuning_report.restype = C.c_size_t
     _LIB = lib
     return lib

@@ -20,6 +20,13 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+
 #include "common.cuh"
 #include "gemm_tc.cuh"
 #include "tc_ptx.cuh"
@@ -177,29 +184,153 @@ void launch(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B,
     ROME_CHECK_LAUNCH();
 }
 
+// ---- tile-shape autotuner -------------------------------------------------
+// The tile width BN and the ring depth STAGES trade the number of CTAs (and
+// so the balance of the last wave over 148 SMs) against the reuse of each
+// A tile and the latency the ring hides; which wins depends on M, N and Kp.
+// The first call with a given key -- epilogue kind, operand planes, device,
+// N, Kp and the number of 128-row tiles rounded up to a power of two -- runs
+// every candidate shape on that call's own operands, timed with CUDA events
+// on the call's stream (one untimed run, then one timed run each), and keeps
+// the fastest; later calls with the key launch it directly.  All candidates
+// write identical outputs (each output element accumulates the same K blocks
+// in the same order whatever the tile width, and the epilogues only store
+// values and fold row minima), so the results do not depend on which
+// candidate ran last.  With ROME_TC_TUNE=0 in the environment the first
+// candidate of each list (the untuned default) is used; ROME_TC_SHAPE=<i>
+// pins candidate i of each list (clamped to the list), e.g. to reproduce a
+// choice.
+template <typename Epi>
+struct Cand {
+    const char* name;
+    void (*fn)(cudaStream_t, int, int, int, const void*, const void*, const Epi&, int*);
+};
+
+struct TuneKey {
+    int kind, nplane, dev, N, Kp, mb;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(kind, nplane, dev, N, Kp, mb) < std::tie(o.kind, o.nplane, o.dev, o.N, o.Kp, o.mb);
+    }
+};
+struct TuneEntry {
+    int choice = 0, ncand = 0;
+    const char* names[4] = {};
+    float ms[4] = {};
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneEntry> g_tune;
+
+bool tuning_enabled() {
+    const char* e = getenv("ROME_TC_TUNE");
+    return !(e && e[0] == '0');
+}
+
+// ROME_TC_SHAPE=<i>: the pinned candidate index, or -1
+int pinned_shape() {
+    const char* e = getenv("ROME_TC_SHAPE");
+    if (!e || e[0] < '0' || e[0] > '9') return -1;
+    return atoi(e);
+}
+
+template <typename Epi, int NC>
+void tuned(int kind, int nplane, const Cand<Epi> (&c)[NC], cudaStream_t st, int M, int N, int Kp, const void* A,
+           const void* B, const Epi& epi, int* derr) {
+    static_assert(NC >= 1 && NC <= 4, "1-4 candidates");
+    const int pin = pinned_shape();
+    if (pin >= 0) {
+        c[pin < NC ? pin : NC - 1].fn(st, M, N, Kp, A, B, epi, derr);
+        return;
+    }
+    if (!tuning_enabled() || NC == 1) {
+        c[0].fn(st, M, N, Kp, A, B, epi, derr);
+        return;
+    }
+    int dev = 0;
+    ROME_CUDA(cudaGetDevice(&dev));
+    int mb = 1;
+    while (mb < (M + BM - 1) / BM) mb <<= 1;
+    const TuneKey key{kind, nplane, dev, N, Kp, mb};
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+        c[it->second.choice].fn(st, M, N, Kp, A, B, epi, derr);
+        return;
+    }
+    TuneEntry e;
+    e.ncand = NC;
+    cudaEvent_t ev[2];
+    ROME_CUDA(cudaEventCreate(&ev[0]));
+    ROME_CUDA(cudaEventCreate(&ev[1]));
+    float best = 0.f;
+    for (int q = 0; q < NC; q++) {
+        e.names[q] = c[q].name;
+        c[q].fn(st, M, N, Kp, A, B, epi, derr);
+        ROME_CUDA(cudaEventRecord(ev[0], st));
+        c[q].fn(st, M, N, Kp, A, B, epi, derr);
+        ROME_CUDA(cudaEventRecord(ev[1], st));
+        ROME_CUDA(cudaEventSynchronize(ev[1]));
+        ROME_CUDA(cudaEventElapsedTime(&e.ms[q], ev[0], ev[1]));
+        if (q == 0 || e.ms[q] < best) {
+            best = e.ms[q];
+            e.choice = q;
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    g_tune[key] = e;
+}
+
+enum { KIND_DIFF2 = 0, KIND_STORE = 1, KIND_BIAS = 2 };
+
+template <typename Epi>
+struct Shapes {
+    static constexpr Cand<Epi> one[2] = {{"256x4", launch<256, 1, 4, Epi>}, {"128x6", launch<128, 1, 6, Epi>}};
+    static constexpr Cand<Epi> two[2] = {{"128x3", launch<128, 2, 3, Epi>}, {"64x4", launch<64, 2, 4, Epi>}};
+};
+
 }  // namespace
 
 void tc_diff2_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, int precision,
                    const Diff2Epi& epi, int* derr) {
     if (precision == ROME_PREC_BF16)
-        launch<256, 1, 4>(st, M, N, Kp, A, B, epi, derr);
+        tuned(KIND_DIFF2, 1, Shapes<Diff2Epi>::one, st, M, N, Kp, A, B, epi, derr);
     else if (precision == ROME_PREC_BF16X3)
-        launch<128, 2, 3>(st, M, N, Kp, A, B, epi, derr);
+        tuned(KIND_DIFF2, 2, Shapes<Diff2Epi>::two, st, M, N, Kp, A, B, epi, derr);
     else
         fail(ROME_ERR_UNSUPPORTED, "precision %d has no tensor-core path", precision);
 }
 
 void tc_store_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
                    int* derr) {
-    launch<128, 2, 3>(st, M, N, Kp, A, B, StoreEpi{out, ld}, derr);
+    tuned(KIND_STORE, 2, Shapes<StoreEpi>::two, st, M, N, Kp, A, B, StoreEpi{out, ld}, derr);
 }
 
 void tc_bias_gemm(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B, float* out, int ld,
                   const float* bias, int group, int* derr, bool split) {
+    const BiasStoreEpi epi{out, ld, bias, group};
     if (split)
-        launch<128, 2, 3>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
+        tuned(KIND_BIAS, 2, Shapes<BiasStoreEpi>::two, st, M, N, Kp, A, B, epi, derr);
     else
-        launch<256, 1, 4>(st, M, N, Kp, A, B, BiasStoreEpi{out, ld, bias, group}, derr);
+        tuned(KIND_BIAS, 1, Shapes<BiasStoreEpi>::one, st, M, N, Kp, A, B, epi, derr);
+}
+
+std::string tc_tuning_report() {
+    static const char* kinds[] = {"diff2", "store", "bias"};
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    std::string out;
+    char line[256];
+    for (const auto& kv : g_tune) {
+        const TuneKey& k = kv.first;
+        const TuneEntry& e = kv.second;
+        int n = snprintf(line, sizeof line, "%s planes=%d dev=%d N=%d Kp=%d mtiles=%d choice=%s", kinds[k.kind],
+                         k.nplane, k.dev, k.N, k.Kp, k.mb, e.names[e.choice]);
+        for (int q = 0; q < e.ncand && n < (int)sizeof line; q++)
+            n += snprintf(line + n, sizeof line - n, " %s:%.4fms", e.names[q], e.ms[q]);
+        out += line;
+        out += "\n";
+    }
+    return out;
 }
 
 // hi/lo bf16 planes of a [rows][K] fp32 matrix, zero padded to Kpad columns
@@ -264,3 +395,13 @@ void tc_check_error(cudaStream_t st, int* derr) {
 }
 
 }  // namespace rome
+
+extern "C" size_t rome_gpu_tuning_report(char* buf, size_t len) {
+    const std::string r = rome::tc_tuning_report();
+    if (buf && len) {
+        const size_t n = std::min(len - 1, r.size());
+        memcpy(buf, r.data(), n);
+        buf[n] = '\0';
+    }
+    return r.size();
+}

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "epilogues.cuh"
 
 namespace rome {
@@ -22,6 +24,8 @@ void split_bf16(cudaStream_t st, const float* in, long rows, int K, int ldin, in
                 bool with_lo = true);
 // the same planes of the transpose: [cols][rows_pad] from a [rows][ldin] matrix (rows beyond `rows` zero)
 void split_bf16_t(cudaStream_t st, const float* in, int rows, int cols, int ldin, int rows_pad, void* out);
+// the autotuner's choices: one line per key with every candidate's time
+std::string tc_tuning_report();
 // raises ROME_ERR_TIMEOUT if a tensor-core kernel's bounded wait expired
 void tc_check_error(cudaStream_t st, int* derr);
 }  // namespace rome
