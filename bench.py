@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--pool", type=int, default=2000)
     ap.add_argument("--particles", type=int, default=0, help="override the particle count (debug)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive", "prep"],
+    ap.add_argument("--mode", default="learned", choices=["learned", "exhaustive", "prep", "reconstruct"],
                     help="prep: the image preparation (setFourierTransforms) alone, from float32 images")
     ap.add_argument("--topk", type=int, default=16, help="network outputs proposed per particle (x2 orientations)")
     ap.add_argument("--train-particles", type=int, default=20000)
@@ -691,10 +691,114 @@ def run_prep(args):
     print(json.dumps(line), flush=True)
 
 
+def run_reconstruct(args):
+    """Secondary mode: reconstruction at known poses (the reference's
+    rome_reconstruct) of 10,000 particles of 128^2 into the padded 259^3
+    grid of the 3D configuration's M-step.  value: back-projection of the
+    prepared spectra resident in HBM (particles/s); reconstruct_ms: the
+    gridding-corrected reconstruction of the volume (10 iterations); e2e:
+    STAR + MRCS on disk -> loader -> device preparation -> back-projection ->
+    reconstruction -> volume in host memory.  Images are seeded noise with
+    random poses and CTFs (the work does not depend on their content).  One
+    JSON line."""
+    import tempfile
+
+    import torch
+
+    from rome_b200.map2d import GpuContext
+    from rome_b200.particles import PrepOptions, prepare_particles
+    from rome_b200.reconstruct_poses import POSE_LABELS, reconstruct_from_star
+    from rome_b200.star_mrcs import ParticleStack
+    from rome_b200.synthetic import write_mrcs
+    N = args.particles or 10000
+    S, angpix = 128, 1.5
+    rng = np.random.default_rng(5)
+    tmp = tempfile.mkdtemp(prefix="rome_recon_bench_")
+    mrcs = os.path.join(tmp, "p.mrcs")
+    write_mrcs(mrcs, rng.standard_normal((N, S, S), dtype=np.float32), angpix)
+    star = os.path.join(tmp, "p.star")
+    rot, psi = rng.uniform(0, 360, N), rng.uniform(0, 360, N)
+    tilt = np.rad2deg(np.arccos(rng.uniform(-1, 1, N)))
+    ox, oy = rng.uniform(-4, 4, N), rng.uniform(-4, 4, N)
+    du, dv, da = rng.uniform(1e4, 3e4, N), rng.uniform(1e4, 3e4, N), rng.uniform(0, 180, N)
+    labels = ["rlnImageName", "rlnMicrographName", "rlnDefocusU", "rlnDefocusV", "rlnDefocusAngle", "rlnVoltage",
+              "rlnSphericalAberration", "rlnAmplitudeContrast", *POSE_LABELS]
+    with open(star, "w") as f:
+        f.write("data_\nloop_\n" + "".join(f"_{lab} #{i + 1}\n" for i, lab in enumerate(labels)))
+        for i in range(N):
+            f.write(f"{i + 1:06d}@{mrcs} mic{i % 50:03d} {du[i]:.3f} {dv[i]:.3f} {da[i]:.3f} 300 2.7 0.1 "
+                    f"{rot[i]:.4f} {tilt[i]:.4f} {psi[i]:.4f} {ox[i]:.4f} {oy[i]:.4f}\n")
+    poses = np.stack([rot, tilt, psi, ox, oy], axis=1)
+    st = ParticleStack(star)
+    order = np.argsort(np.asarray([int(x.split("@")[0]) for x in st.columns["rlnImageName"]]))  # file order
+    r_max, F = S // 2, S * (S // 2 + 1)
+    pad = 2 * (2 * r_max + 1) + 1
+    ctx = GpuContext(0, "fp32", profile=True)
+    ctx.set_projectors(np.zeros((1, pad, pad, pad // 2 + 1, 2)), S, r_max)
+    opts = PrepOptions(pixel_size=angpix, particle_diameter=S * angpix, do_ctf_correction=True)
+    sig = np.ones((st.nr_groups, S // 2 + 1))
+    spectra = []
+    for imgs in st.device_pools(0, args.pool, order=order):
+        imgs.xoff[:] = 0.0
+        imgs.yoff[:] = 0.0
+        o = prepare_particles(ctx, imgs, opts, sig, S, on_device=True, power=False)
+        spectra.append((o["Fimg_nomask_real"], o["Fimg_nomask_imag"], o["Fctf"],
+                        poses[imgs.first_image:imgs.first_image + imgs.nr_images]))
+
+    def step():
+        for re, im, c, ps in spectra:
+            ctx.backproject_images(0, re, im, c, ps)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.reset_timings()
+    with ClockSampler(0) as clk:
+        ms, _ = _timed(torch, step, args.steps)
+    t = ctx.get_timings()
+    rec = lambda: ctx.reconstruct(0, S, 3, np.zeros(S // 2 + 1), 1.0, 1.0, 10, False)  # noqa: E731
+    rec()  # warm-up: cuFFT plans and work buffers
+    rec_ms, _ = _timed(torch, rec, 1)
+    del spectra
+    ctx.close()
+    reconstruct_from_star(star, angpix, 10, True, pool=args.pool)  # warm-up (page cache, allocations)
+    e_ms, _ = _timed(torch, lambda: reconstruct_from_star(star, angpix, 10, True, pool=args.pool), 1)
+    hbm, _, peak_kind = load_peaks()
+    bp = t["backproject"]
+    achieved = bp["bytes"] / (bp["ms"] / 1e3) / 1e9
+    line = {
+        "metric": "reconstruction at known poses: back-projection particles/s (rome_reconstruct)",
+        "value": round(N / (ms / args.steps / 1e3), 2), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded noise images, random poses and CTFs; the work does not depend on content)",
+        "config": {"workload": "map3d_cfg3 M-step shapes: reconstruction at known poses", "particles": N, "image": S,
+                   "pad": pad, "gridding_iterations": 10, "pool": args.pool, "ctf": True,
+                   "inputs": "larger than L2 (no flush)"},
+        "reconstruct_ms": round(rec_ms, 3),
+        "e2e": {"value": round(N / (e_ms / 1e3), 2), "unit": UNIT,
+                "from": "STAR + MRCS on disk (page cache): loader, copy, device preparation, back-projection, "
+                        "reconstruction, volume back",
+                "ms": round(e_ms, 2), "h2d_bytes_per_step": int(N * S * S * 4),
+                "d2h_bytes_per_step": int(S ** 3 * 8)},
+        "gpu_launches": int(t["total_launches"]),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                     "frac": round(achieved / hbm, 4), "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "bp_images_kernel: algorithmic bytes = spectra and CTF read once (24 B per "
+                               "coefficient); the 12 FP64 atomics per active pixel land in L2",
+                     "launches": int(bp["launches"])},
+        "cpu_baseline": None,
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.mode == "prep" and a.impl != "reference":
         run_prep(a)
+        sys.exit(0)
+    if a.mode == "reconstruct" and a.impl != "reference":
+        run_reconstruct(a)
         sys.exit(0)
     if a.config.startswith("map3d") and a.impl != "reference":
         run_ours_3d(a)

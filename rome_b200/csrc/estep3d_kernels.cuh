@@ -458,14 +458,17 @@ __global__ void __launch_bounds__(NT)
 // (int)(|dotp| / sampling) % 5000, sign of dotp on the sine), multiplied by
 // its CTF, and scattered with weight CTF^2 (unit value and weight without
 // CTF) through MyBackProjector::backproject (src/reconstruct.cpp:977-1164).
-// One block row per image (blockIdx.y), PIX pixels per thread.
+// One block row per image, PIX pixels per thread; block row y works on
+// image order[y], so that images whose slices share voxels run at the same
+// time and their atomics meet in L2.
 template <int NT, int PIX>
 __global__ void __launch_bounds__(NT)
-    bp_images_kernel(int F, int csF, int cs, const double* __restrict__ Fre, const double* __restrict__ Fim,
-                     const double* __restrict__ Fctf, const double2* __restrict__ shifts,
-                     const double2* __restrict__ tab, double sampling, const Rot3* __restrict__ rot, int r_max,
-                     int pad, int padF, double2* __restrict__ D, double* __restrict__ W) {
-    const long i = blockIdx.y;
+    bp_images_kernel(int F, int csF, int cs, const int* __restrict__ order, const double* __restrict__ Fre,
+                     const double* __restrict__ Fim, const double* __restrict__ Fctf,
+                     const double2* __restrict__ shifts, const double2* __restrict__ tab, double sampling,
+                     const Rot3* __restrict__ rot, int r_max, int pad, int padF, double2* __restrict__ D,
+                     double* __restrict__ W) {
+    const long i = order[blockIdx.y];
     const double2 sh = shifts[i];
     const Rot3 A = rot[i];
     const int max_r2 = r_max * r_max;

@@ -732,15 +732,35 @@ extern "C" int rome_gpu_backproject_images(RomeGpuCtx* ctx, int iclass, int n, i
         const int r_max = std::min(ctx->r_max, size / 2);
         std::vector<Rot3> hrot(n);
         std::vector<double2> hsh(n);
+        std::vector<double> key(n);
+        const double d2r = 3.14159265358979323846 / 180.;
         for (int i = 0; i < n; i++) {
             const double* a = poses + 5 * (size_t)i;
             for (int q = 0; q < 5; q++)
                 ROME_REQUIRE(std::isfinite(a[q]), "pose %d field %d is not finite", i, q);
             hrot[i] = rot3_inv(a[0], a[1], a[2], ctx->padding);
             hsh[i] = make_double2(a[3] / (-size), a[4] / (-size));
+            // the slice's plane is set by its normal, the projection direction
+            // (sin tilt cos rot, sin tilt sin rot, cos tilt), up to sign
+            // (Friedel); order images along serpentine bands of the polar angle
+            // of the upper-hemisphere normal so concurrent blocks share voxels
+            double nx = sin(a[1] * d2r) * cos(a[0] * d2r), ny = sin(a[1] * d2r) * sin(a[0] * d2r);
+            double nz = cos(a[1] * d2r);
+            if (nz < 0) {
+                nx = -nx;
+                ny = -ny;
+                nz = -nz;
+            }
+            const double theta = acos(std::min(1.0, nz)) / d2r, phi = atan2(ny, nx);
+            const int band = std::min(29, (int)(theta / 3.0));
+            key[i] = band * 16.0 + ((band & 1) ? -phi : phi);
         }
+        std::vector<int> ord(n);
+        for (int i = 0; i < n; i++) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return key[x] < key[y]; });
         Rot3* dRot = upload3(ctx, S_ROTM, hrot.data(), hrot.size());
         double2* dSh = upload3(ctx, S_SHIFT, hsh.data(), hsh.size());
+        int* dOrd = upload3(ctx, S_PARTI, ord.data(), ord.size());
         const double *dRe = Fimg_real, *dIm = Fimg_imag, *dCtf = Fctf;
         if (!inputs_on_device) {
             double* buf = ctx->ws[S_FNOMASK].as<double>((size_t)2 * n * F);
@@ -757,15 +777,20 @@ extern "C" int rome_gpu_backproject_images(RomeGpuCtx* ctx, int iclass, int n, i
         }
         const int NT = 256, PIX = 4;
         const int nsplit = (F + NT * PIX - 1) / (NT * PIX);
+        Profiler prof(ctx);
+        prof.begin(ROME_PHASE_BACKPROJECT);
         for (int i0 = 0; i0 < n; i0 += 65535) {  // grid y limit
             const int m = std::min(n - i0, 65535);
-            const size_t o = (size_t)i0 * F;
             bp_images_kernel<NT, PIX><<<dim3(nsplit, m), NT, 0, st>>>(
-                F, csF, size, dRe + o, dIm + o, dCtf ? dCtf + o : nullptr, dSh + i0, ctx->d_shift_tab,
-                ctx->shift_sampling, dRot + i0, r_max, ctx->pad_size, ctx->pad_size / 2 + 1,
-                ctx->bp_data + (long)iclass * ctx->vox, ctx->bp_weight + (long)iclass * ctx->vox);
+                F, csF, size, dOrd + i0, dRe, dIm, dCtf, dSh, ctx->d_shift_tab, ctx->shift_sampling, dRot, r_max,
+                ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data + (long)iclass * ctx->vox,
+                ctx->bp_weight + (long)iclass * ctx->vox);
             ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_BACKPROJECT);
         }
+        prof.end(ROME_PHASE_BACKPROJECT);
+        prof.add_bytes(ROME_PHASE_BACKPROJECT, (double)n * F * (Fctf ? 24.0 : 16.0));  // spectra (+ CTF) read once
         ROME_CUDA(cudaStreamSynchronize(st));
+        prof.collect();
     });
 }
