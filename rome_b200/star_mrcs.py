@@ -291,16 +291,19 @@ class ParticleStack:
 
         th = threading.Thread(target=load, args=(0,))
         th.start()
-        for q, (lo, hi) in enumerate(ranges):
-            th.join()
-            imgs = result[q]
-            result[q] = None
-            if isinstance(imgs, BaseException):
-                raise imgs
-            if q + 1 < len(ranges):
-                th = threading.Thread(target=load, args=(q + 1,))
-                th.start()
-            yield self.particles(order[lo:hi], imgs, lo)
+        try:
+            for q, (lo, hi) in enumerate(ranges):
+                th.join()
+                imgs = result[q]
+                result[q] = None
+                if isinstance(imgs, BaseException):
+                    raise imgs
+                if q + 1 < len(ranges):
+                    th = threading.Thread(target=load, args=(q + 1,))
+                    th.start()
+                yield self.particles(order[lo:hi], imgs, lo)
+        finally:
+            th.join()   # a consumer that stops early leaves no reader behind
 
     def device_pools(self, device: int, pool: int, first: int = 0, last: Optional[int] = None,
                      order: Optional[np.ndarray] = None) -> Iterator[ParticleImages]:
@@ -313,12 +316,17 @@ class ParticleStack:
         import torch
         dev = torch.device("cuda", device)
         side = torch.cuda.Stream(device=dev)
+        consumer = torch.cuda.current_stream(dev)
         prev = None
         for host in self.pools(pool, first, last, order, pinned=True, nbuf=2):
             with torch.cuda.stream(side):
                 t = torch.from_numpy(host.images).to(dev, non_blocking=True)
                 ev = torch.cuda.Event()
                 ev.record(side)
+            # allocated on the side stream, used on the caller's: the allocator
+            # must not hand the block back to the side stream before the
+            # caller's work on it is done
+            t.record_stream(consumer)
             if prev is not None:
                 yield prev
             ev.synchronize()

@@ -158,3 +158,15 @@ def test_device_pools_feed_the_preparation(datasets, golden):
                 assert np.array_equal(a[k], b[k]), k
             n += pool.nr_images
     assert n == st.nr_images
+
+
+def test_early_stop_leaves_no_reader(datasets):
+    import threading
+    st = ParticleStack(datasets["map2d_a"])
+    before = threading.active_count()
+    for pool in st.pools(4):
+        break
+    gen = st.pools(4)
+    next(gen)
+    gen.close()
+    assert threading.active_count() == before
