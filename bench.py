@@ -760,6 +760,15 @@ def run_reconstruct(args):
     rec_ms, _ = _timed(torch, rec, 1)
     del spectra
     ctx.close()
+    # the pool loader alone: STAR/MRCS (page cache) -> page-locked buffers -> device, one pool ahead
+    def load_all():
+        n = 0
+        for q in st.device_pools(0, args.pool, order=order):
+            n += q.nr_images
+        return n
+
+    load_all()
+    load_ms, _ = _timed(torch, load_all, 1)
     reconstruct_from_star(star, angpix, 10, True, pool=args.pool)  # warm-up (page cache, allocations)
     e_ms, _ = _timed(torch, lambda: reconstruct_from_star(star, angpix, 10, True, pool=args.pool), 1)
     hbm, _, peak_kind = load_peaks()
@@ -775,6 +784,10 @@ def run_reconstruct(args):
                    "pad": pad, "gridding_iterations": 10, "pool": args.pool, "ctf": True,
                    "inputs": "larger than L2 (no flush)"},
         "reconstruct_ms": round(rec_ms, 3),
+        "loader": {"value": round(N / (load_ms / 1e3), 2), "unit": UNIT, "ms": round(load_ms, 2),
+                   "GB_per_s": round(N * S * S * 4 / (load_ms / 1e3) / 1e9, 2),
+                   "what": "STAR/MRCS pool loader: memory-mapped stack (page cache) -> page-locked buffer -> "
+                           "device, next pool read while the current one is copied"},
         "e2e": {"value": round(N / (e_ms / 1e3), 2), "unit": UNIT,
                 "from": "STAR + MRCS on disk (page cache): loader, copy, device preparation, back-projection, "
                         "reconstruction, volume back",

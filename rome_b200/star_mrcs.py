@@ -128,6 +128,21 @@ def read_star(path: str) -> Dict[str, List[str]]:
     return out
 
 
+#: threads that copy one request's images out of the memory-mapped stacks
+READ_THREADS = 4
+_POOL = None
+_POOL_LOCK = threading.Lock()
+
+
+def _reader_pool():
+    global _POOL
+    with _POOL_LOCK:
+        if _POOL is None:
+            from concurrent.futures import ThreadPoolExecutor
+            _POOL = ThreadPoolExecutor(max_workers=READ_THREADS, thread_name_prefix="mrcs-read")
+        return _POOL
+
+
 def _atoi(s: str) -> int:
     """C atoi: optional sign and leading digits, 0 if none."""
     s = s.strip()
@@ -236,11 +251,33 @@ class ParticleStack:
 
     def read_images(self, rows: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Images of the given particle rows, float32 [len(rows)][S][S];
-        runs of consecutive images of one stack are read as one slice."""
+        runs of consecutive images of one stack are read as one slice.  Large
+        requests are split over `READ_THREADS` threads (the copies out of the
+        memory-mapped stacks release the GIL), since one thread's copy from
+        the page cache runs well below the host-to-device link."""
         rows = np.asarray(rows, np.int64)
         S = self._size
         if out is None:
             out = np.empty((rows.size, S, S), np.float32)
+        nt = min(READ_THREADS, max(1, rows.size * S * S * 4 // (8 << 20)))
+        if nt > 1:
+            cuts = np.linspace(0, rows.size, nt + 1).astype(int)
+            futs = [_reader_pool().submit(self._read_into, rows[a:b], out[a:b]) for a, b in zip(cuts[:-1], cuts[1:])]
+            for f in futs:
+                f.result()
+            return out
+        return self._read_into(rows, out)
+
+    def _read_into(self, rows: np.ndarray, out: np.ndarray) -> np.ndarray:
+        if rows.size and np.all(self.stack[rows] == self.stack[rows[0]]):
+            # one stack (the usual case): one slice copy for consecutive images,
+            # else a single gather in C, whatever the order
+            mm, idx = self._map(int(self.stack[rows[0]])), self.index[rows] - 1
+            if np.all(np.diff(idx) == 1):
+                out[:] = mm[idx[0]:idx[0] + idx.size]
+            else:
+                np.take(mm, idx, axis=0, out=out)
+            return out
         i = 0
         while i < rows.size:
             s, first = int(self.stack[rows[i]]), int(self.index[rows[i]])
