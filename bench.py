@@ -488,22 +488,33 @@ def oracle_rate(w, target_seconds: float = 15.0, cores: int = 0):
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "map2d_bench")
 
 
+# one CPU-baseline sample for both the GPU arm's cpu_baseline and the reference arm: pools of 16 particles,
+# the first REF_WARM_POOLS run and not counted
+REF_POOL, REF_WARM_POOLS, REF_TIMED_POOLS = 16, 2, 8
+
+
 def reference_rate(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str):
     """Particles/s of the reference's own MAP2D E-step (oracle/_ref/map2d_bench:
     the reference sources compiled unchanged, every OpenMP thread of the host)
-    on a dataset of the same workload: iteration 1 through the reference's
-    driver, then iteration 2's expectationSomeParticles() timed per pool at
-    full image size with all classes searched.  The first `warm_pools` pools
-    are not counted."""
-    from rome_b200.synthetic import Map2dSpec, write_dataset_2d
+    on a dataset of the same workload, searched against the templates the
+    particles were made from (as the GPU benchmark does) at the full image
+    size with every class: expectationSomeParticles() timed per pool, the
+    first `warm_pools` pools not counted.  Returns (baseline dict, seconds per
+    timed pool)."""
+    from rome_b200.synthetic import Map2dSpec, _render_blobs_2d, make_templates_2d, write_dataset_2d
     npools = warm_pools + timed_pools
     spec = Map2dSpec(n_particles=pool * npools, size=w.ori_size, n_classes=w.n_classes, n_blobs=w.n_blobs,
                      blob_sigma=w.blob_sigma, max_shift=w.max_shift, defocus=w.defocus, pixel=w.pixel, snr=w.snr,
                      seed=w.seed + 101)
     star = write_dataset_2d(os.path.join(tmpdir, "data"), spec)
+    tmpl = make_templates_2d(np.random.default_rng(spec.seed), spec)  # the generator's own first draws
+    raw = os.path.join(tmpdir, "refs.f64")
+    np.stack([_render_blobs_2d(spec.size, t["centers"], t["sigmas"], t["amps"]) for t in tmpl]).astype(
+        np.float64).tofile(raw)
     cmd = [REF_BENCH, "-i", star, "-K", str(w.n_classes), "-angpix", str(w.pixel), "-psi_step",
            str(int(round(w.psi_step))), "-offset_range", str(w.offset_range), "-offset_step", str(w.offset_step),
-           "-oversampling", "0", "-ctf", "1", "-pool", str(pool), "-time_pools", str(npools)]
+           "-oversampling", "0", "-ctf", "1", "-pool", str(pool), "-warm_pools", str(warm_pools),
+           "-time_pools", str(timed_pools), "-refs_raw", raw]
     out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, cwd=tmpdir)
     if out.returncode != 0:
         raise RuntimeError(f"map2d_bench exited {out.returncode}: {out.stderr[-300:]}")
@@ -514,14 +525,64 @@ def reference_rate(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str)
             pools.append((int(kv["particles"]), float(kv["estep_s"])))
         elif ln.startswith("map2d_bench "):
             threads, cur = int(kv["threads"]), int(kv["current_size"])
-    timed = pools[warm_pools:]
-    n = sum(p for p, _ in timed)
-    t = sum(x for _, x in timed)
+    n = sum(p for p, _ in pools)
+    t = sum(x for _, x in pools)
+    per = sorted(x / p for p, x in pools)
     return {"value": round(n / t, 4), "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"{n} particles ({len(timed)} pools of {pool}) of {w.ori_size}x{w.ori_size}, K={w.n_classes}, "
+            "sample": f"{n} particles ({len(pools)} pools of {pool}) of {w.ori_size}x{w.ori_size}, K={w.n_classes}, "
                       f"{int(round(360 / w.psi_step))} psi x translations +-{w.offset_range} step {w.offset_step}, "
-                      f"current_size {cur}, reference expectationSomeParticles() timed with dtime(), "
-                      f"{t:.1f} s; {warm_pools} warm-up pools not counted"}, t / max(len(timed), 1)
+                      f"current_size {cur}, searched against the generating templates; reference "
+                      f"expectationSomeParticles() timed with dtime(), {t:.1f} s; {warm_pools} warm-up pools "
+                      f"not counted",
+            "s_per_particle": {"min": round(per[0], 4), "median": round(per[len(per) // 2], 4),
+                               "max": round(per[-1], 4)}}, t / max(len(pools), 1)
+
+
+REF_BENCH3D = os.path.join(ROOT, "oracle", "_ref", "map3d_bench")
+
+
+def reference_rate_3d(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str):
+    """Particles/s of the reference's own MAP3D E-step (oracle/_ref/map3d_bench:
+    the reference sources compiled unchanged, every OpenMP thread of the host)
+    on a dataset of the same workload (128^2 particles projected from K
+    random-blob volumes, CTF, white noise at the workload's SNR), searched
+    against those K volumes at the full image size with every class: one
+    pool after another as expectation() runs them, the first `warm_pools`
+    not counted.  Returns (baseline dict, seconds per timed pool)."""
+    from rome_b200.synthetic import Map3dSpec, make_volumes_3d, render_volume, write_dataset_3d
+    npools = warm_pools + timed_pools
+    spec = Map3dSpec(n_particles=pool * npools, size=w.ori_size, n_classes=w.n_classes, n_blobs=w.n_blobs,
+                     blob_sigma=w.blob_sigma, max_shift=w.max_shift, defocus=w.defocus, pixel=w.pixel, snr=w.snr,
+                     seed=w.seed + 101)
+    star, ref = write_dataset_3d(os.path.join(tmpdir, "data"), spec)
+    vols = make_volumes_3d(np.random.default_rng(spec.seed), spec)  # the generator's own first draws
+    raw = os.path.join(tmpdir, "refs.f64")
+    np.stack([render_volume(spec.size, v) for v in vols]).astype(np.float64).tofile(raw)
+    cmd = [REF_BENCH3D, "-i", star, "-ref", ref, "-refs_raw", raw, "-K", str(w.n_classes), "-angpix", str(w.pixel),
+           "-healpix_order", str(w.healpix_order), "-oversampling", "1", "-offset_range", str(w.offset_range),
+           "-offset_step", str(w.offset_step), "-ctf", "1", "-pool", str(pool), "-warm_pools", str(warm_pools),
+           "-time_pools", str(timed_pools)]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=1800, cwd=tmpdir)
+    if out.returncode != 0:
+        raise RuntimeError(f"map3d_bench exited {out.returncode}: {out.stderr[-300:]}")
+    pools, threads, cur, coarse = [], 0, 0, 0
+    for ln in out.stdout.splitlines():
+        kv = dict(x.split("=") for x in ln.split()[1:] if "=" in x)
+        if ln.startswith("map3d_bench_pool"):
+            pools.append((int(kv["particles"]), float(kv["estep_s"])))
+        elif ln.startswith("map3d_bench "):
+            threads, cur, coarse = int(kv["threads"]), int(kv["current_size"]), int(kv["coarse_size"])
+    n = sum(p for p, _ in pools)
+    t = sum(x for _, x in pools)
+    per = sorted(x / p for p, x in pools)
+    return {"value": round(n / t, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n} particles ({len(pools)} pools of {pool}) of {w.ori_size}x{w.ori_size}, K={w.n_classes}, "
+                      f"HEALPix order {w.healpix_order}, oversampling 1, translations +-{w.offset_range} step "
+                      f"{w.offset_step}, coarse size {coarse}, current size {cur}, searched against the generating "
+                      f"volumes; reference expectationSomeParticles() timed with dtime(), {t:.1f} s; "
+                      f"{warm_pools} warm-up pools not counted",
+            "s_per_particle": {"min": round(per[0], 4), "median": round(per[len(per) // 2], 4),
+                               "max": round(per[-1], 4)}}, t / max(len(pools), 1)
 
 
 def cpu_baseline(args, w):
@@ -529,9 +590,10 @@ def cpu_baseline(args, w):
     built, else the oracle port."""
     import tempfile
     try:
-        if os.path.exists(REF_BENCH):
+        rate = reference_rate_3d if args.config.startswith("map3d") else reference_rate
+        if os.path.exists(REF_BENCH3D if args.config.startswith("map3d") else REF_BENCH):
             with tempfile.TemporaryDirectory(prefix="rome_refbench_") as tmp:
-                return reference_rate(w, pool=16, warm_pools=1, timed_pools=4, tmpdir=tmp)[0]
+                return rate(w, pool=REF_POOL, warm_pools=REF_WARM_POOLS, timed_pools=REF_TIMED_POOLS, tmpdir=tmp)[0]
         return oracle_rate(w, target_seconds=15.0)
     except Exception as e:  # the baseline is reported, never required
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
@@ -547,38 +609,49 @@ def run_reference(args):
         return
     from rome_b200.workload import CONFIGS
     w = CONFIGS[args.config]
-    if os.path.exists(REF_BENCH):
-        # one pool of 16 particles per step; warm-up pools are run and dropped
-        steps = max(1, min(args.steps, 16))
-        warm = max(0, min(args.warmup, 4))
+    is3d = args.config.startswith("map3d")
+    if os.path.exists(REF_BENCH3D if is3d else REF_BENCH):
+        # the cpu_baseline sample (one pool of 16 particles per step), so that both arms report one number
         with tempfile.TemporaryDirectory(prefix="rome_refbench_") as tmp:
-            best, s_per_step = reference_rate(w, pool=16, warm_pools=warm, timed_pools=steps, tmpdir=tmp)
+            best, s_per_step = (reference_rate_3d if is3d else reference_rate)(
+                w, pool=REF_POOL, warm_pools=REF_WARM_POOLS, timed_pools=REF_TIMED_POOLS, tmpdir=tmp)
+    elif is3d:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/map3d_bench was not built (the "
+                          "reference tree was absent at build time); the 3D oracle port is not a timing harness"}))
+        return
     else:
         best = oracle_rate(w, target_seconds=20.0)
         s_per_step = None
-    line = {"metric": METRIC, "value": best["value"], "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+    line = {"value": best["value"], "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(s_per_step * 1e3, 3) if s_per_step else None, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "metric": "MAP3D E-step particles/s (exhaustive search)" if is3d else METRIC,
             "config": {"workload": args.config, "image": w.ori_size, "classes": w.n_classes,
-                       "step": "one pool of 16 particles"},
+                       "step": f"one pool of {REF_POOL} particles ({REF_TIMED_POOLS} timed, {REF_WARM_POOLS} "
+                               f"warm-up)"},
             "cpu_baseline": best,
             "e2e": {"value": best["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 def run_ours_3d(args):
-    """Secondary measurement (not the headline metric): the exhaustive MAP3D
-    E-step (coarse pass on the tensor cores, fine pass over the
-    coarse-significant points, wsums, back-projection) on the cfg3-shaped
-    synthetic workload, images staged in HBM; one JSON line."""
+    """The MAP3D E-step (coarse pass over every class x direction x psi x
+    translation on the tensor cores, fine pass over the coarse-significant
+    points, posterior and significance in FP64, wsums, back-projection) on
+    the 3D configuration's synthetic workload, one JSON line.  value: images
+    prepared once and resident in HBM; e2e: float32 images and metadata in
+    page-locked host memory, copied in (pool k + 1 while pool k computes),
+    prepared on the device (setFourierTransforms), E-step, results back."""
     import dataclasses
 
     import torch
 
-    from rome_b200.map2d import DEVICE_FIELDS, GpuContext
+    from rome_b200.map2d import GpuContext
     from rome_b200.map3d import map3d_estep_pool
-    from rome_b200.workload import CONFIGS, build_map3d, subset3d
+    from rome_b200.particles import h2d_bytes as prep_h2d_bytes
+    from rome_b200.particles import pin_particles, prepared_pool, prepared_stream
+    from rome_b200.workload import CONFIGS, build_map3d, prep_options, raw_particles, slice_particles, subset3d
     w = CONFIGS[args.config]
     if args.particles:
         w = dataclasses.replace(w, n_particles=args.particles)
@@ -586,14 +659,25 @@ def run_ours_3d(args):
     pool, proj, r_max, truth = build_map3d(w)
     t_build = time.perf_counter() - t0
     N = pool.nr_images
-    pools = [subset3d(pool, lo, min(N, lo + args.pool)) for lo in range(0, N, args.pool)]
+    raw = raw_particles(pool, truth)
+    bounds = [(lo, min(N, lo + args.pool)) for lo in range(0, N, args.pool)]
+    tmpls = [subset3d(pool, lo, hi) for lo, hi in bounds]
+    opts = prep_options(w)
     ctx = GpuContext(0, args.precision, profile=True)
     ctx.set_projectors(proj, pool.ori_size, r_max)
-    dev = [{name: torch.from_numpy(np.ascontiguousarray(getattr(q, name), np.float64)).cuda()
-            for name in DEVICE_FIELDS} for q in pools]
+    prep_ctx = GpuContext(0, "fp32", profile=True)
+    d_raw = torch.from_numpy(raw.images).cuda()
+    dr = dataclasses.replace(raw, images=d_raw)
+    staged = [prepared_pool(prep_ctx, t, slice_particles(dr, lo, hi), opts) for t, (lo, hi) in zip(tmpls, bounds)]
+    del d_raw, dr
+    host_raw = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
 
     def step():
-        return [map3d_estep_pool(ctx, q, dev=d) for q, d in zip(pools, dev)]
+        return [map3d_estep_pool(ctx, sp.pool, dev=sp.dev) for sp in staged]
+
+    def step_e2e():
+        return [map3d_estep_pool(ctx, sp.pool, dev=sp.dev)
+                for sp in prepared_stream(prep_ctx, list(zip(tmpls, host_raw)), opts)]
 
     for _ in range(args.warmup):
         step()
@@ -601,21 +685,67 @@ def run_ours_3d(args):
     with ClockSampler(0) as clk:
         ms, last = _timed(torch, step, args.steps)
     timings = ctx.get_timings()
+    step_e2e()
+    e_ms, _ = _timed(torch, step_e2e, max(1, args.steps))
     cls = np.concatenate([r["cls"] for r in last]) - 1
+    # the plain FP32 E-step on the same prepared particles: the comparison arm and the pose judge
+    judge = {}
+    if args.precision != "fp32":
+        with GpuContext(0, "fp32") as c32:
+            c32.set_projectors(proj, pool.ori_size, r_max)
+            map3d_estep_pool(c32, staged[0].pool, dev=staged[0].dev)
+            f_ms, f_res = _timed(torch, lambda: [map3d_estep_pool(c32, sp.pool, dev=sp.dev) for sp in staged], 1)
+        cat = lambda rs, k: np.concatenate([r[k] for r in rs])  # noqa: E731
+        same = np.ones(N, bool)
+        for k in ("cls", "rot", "tilt", "psi", "xoff", "yoff"):
+            same &= cat(last, k) == cat(f_res, k)
+        judge = {"pose_agreement_vs_plain_fp32": round(float(same.mean()), 5),
+                 "plain_fp32": {"value": round(N / (f_ms / 1e3), 2), "unit": UNIT}}
+    hbm, bf16, peak_kind = load_peaks()
+    phases = {k: round(v["ms"] / args.steps, 3) for k, v in timings.items() if isinstance(v, dict)}
+    # the phase with the most device time names the roofline: the posterior (HBM: diff2 read once, 4 B per
+    # hypothesis) or the contraction (tensor: 4 * active pixels flops per hypothesis, coarse and fine)
+    post, gem = timings["posterior"], timings["cross_gemm"]
+    if post["ms"] >= gem["ms"]:
+        ach = post["bytes"] / (post["ms"] / 1e3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": hbm, "unit": "GB/s", "frac": round(ach / hbm, 4),
+                "traffic": None, "peak_kind": peak_kind, "launches": int(post["launches"]),
+                "ms_per_step": round(post["ms"] / args.steps, 3),
+                "kernel": "posterior + significance (post_select2_kernel and fallbacks): algorithmic bytes = the "
+                          "diff2 rows read once, 4 B per hypothesis"}
+    else:
+        ach = gem["flops"] / (gem["ms"] / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": round(ach, 2), "peak": bf16, "unit": "TFLOP/s",
+                "frac": round(ach / bf16, 4), "traffic": None, "peak_kind": peak_kind,
+                "launches": int(gem["launches"]), "ms_per_step": round(gem["ms"] / args.steps, 3),
+                "kernel": "cross-term contraction (coarse tc_gemm_kernel + fine pass): 4 * active pixels flops "
+                          "per hypothesis"}
     line = {
-        "metric": "MAP3D E-step particles/s (exhaustive, secondary)", "value": round(N / (ms / args.steps / 1e3), 2),
+        "metric": "MAP3D E-step particles/s (exhaustive search)", "value": round(N / (ms / args.steps / 1e3), 2),
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "dtype": args.precision,
+        "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "bf16": "bf16", "bf16x3": "bf16x3"}[args.precision],
         "data": "synthetic (seeded random-blob volumes, Fourier-slice particles, CTF, white noise)",
         "config": {"workload": args.config, "particles": N, "image": w.ori_size, "coarse_size": pool.coarse_size,
                    "classes": w.n_classes, "directions": pool.nr_dir, "psi": pool.nr_psi,
-                   "translations": pool.nr_trans, "pool": args.pool, "build_s": round(t_build, 1)},
+                   "translations": pool.nr_trans, "oversampling": 1, "pool": args.pool, "precision": args.precision,
+                   "inputs": "larger than L2 (no flush)", "build_s": round(t_build, 1)},
+        "e2e": {"value": round(N / (e_ms / max(1, args.steps) / 1e3), 2), "unit": UNIT,
+                "from": "float32 images + metadata in page-locked host memory: copy, image preparation "
+                        "(setFourierTransforms), E-step, results back",
+                "h2d_bytes_per_step": int(sum(prep_h2d_bytes(r) for r in host_raw)),
+                "d2h_bytes_per_step": int(N * (11 * 8 + 4))},
         "class_agreement_vs_truth": round(float(np.mean(cls == truth["cls"])), 4),
         "nr_sign_mean": round(float(np.mean(np.concatenate([r["nr_sign"] for r in last]))), 1),
-        "phases_ms_per_step": {k: round(v["ms"] / args.steps, 3) for k, v in timings.items() if isinstance(v, dict)},
+        "judge": judge,
+        "phases_ms_per_step": phases,
         "gpu_launches": int(timings["total_launches"]),
+        "roofline": roof,
         "clocks": clk.summary(),
     }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, w)
+    prep_ctx.close()
     ctx.close()
     print(json.dumps(line), flush=True)
 
@@ -768,7 +898,8 @@ def run_reconstruct(args):
         return n
 
     load_all()
-    load_ms, _ = _timed(torch, load_all, 1)
+    load_runs = sorted(_timed(torch, load_all, 1)[0] for _ in range(5))
+    load_ms = load_runs[len(load_runs) // 2]
     reconstruct_from_star(star, angpix, 10, True, pool=args.pool)  # warm-up (page cache, allocations)
     e_ms, _ = _timed(torch, lambda: reconstruct_from_star(star, angpix, 10, True, pool=args.pool), 1)
     hbm, _, peak_kind = load_peaks()
@@ -785,9 +916,12 @@ def run_reconstruct(args):
                    "inputs": "larger than L2 (no flush)"},
         "reconstruct_ms": round(rec_ms, 3),
         "loader": {"value": round(N / (load_ms / 1e3), 2), "unit": UNIT, "ms": round(load_ms, 2),
+                   "ms_runs": [round(x, 2) for x in load_runs],
                    "GB_per_s": round(N * S * S * 4 / (load_ms / 1e3) / 1e9, 2),
                    "what": "STAR/MRCS pool loader: memory-mapped stack (page cache) -> page-locked buffer -> "
-                           "device, next pool read while the current one is copied"},
+                           "device, next pool read while the current one is copied; median of 5 runs after "
+                           "one warm-up, each run's page-locked buffers and side stream created inside its "
+                           "timed region"},
         "e2e": {"value": round(N / (e_ms / 1e3), 2), "unit": UNIT,
                 "from": "STAR + MRCS on disk (page cache): loader, copy, device preparation, back-projection, "
                         "reconstruction, volume back",

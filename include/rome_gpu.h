@@ -464,9 +464,14 @@ int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, const double* 
  * Limits: n <= ROME_SELECT_STATIC_MAX_IMAGES, n * len <=
  * ROME_SELECT_STATIC_MAX_WEIGHTS; beyond them it returns ROME_ERR_ARG.
  * The first call on a device looks the array up (cudaGetSymbolAddress) and
- * should come before any stream capture on that device.  Calls on one
- * device share the array, so overlapping calls would race: the function
- * takes a process-wide lock and returns after its stream work is done. */
+ * should come before any stream capture on that device.  With lazy module
+ * loading (CUDA's default) that first call may also load the library's
+ * device code on the device, which is when the driver reserves the array
+ * and the code: treat it as a warm-up; from the second call on, nothing is
+ * allocated.  The call is synchronous: it returns once the results are in
+ * the caller's host arrays.  Calls on one device share the array, so
+ * overlapping calls would race: the function takes a process-wide lock and
+ * returns after its stream work is done. */
 #define ROME_SELECT_STATIC_MAX_IMAGES 4096
 #define ROME_SELECT_STATIC_MAX_WEIGHTS (1 << 20)
 int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const double* weights,

@@ -7,11 +7,18 @@
 // current resolution is set to Nyquist first so that the E-step runs at the
 // full image size (current_size = ori_size, the size the GPU benchmark
 // uses) and every class has a positive prior (all K classes are searched).
-// The first -time_pools pools of iteration 2 are then processed as
-// expectation() does (src/map2d_optimizer.cpp:760-799) and
-// expectationSomeParticles() (:802-854) is timed with the reference's own
-// dtime(); every OpenMP thread of the host is used.  Prints one line per
-// timed pool and a total:
+// With -refs_raw (K float64 images [K][ori][ori]) iteration 1 is skipped and
+// those images are the class references of iteration 2 (the templates the
+// particles were made from, which is what the GPU benchmark searches): the
+// work per particle then no longer depends on how well a short iteration 1
+// on the timing sample seeded the classes (it seeds each class from 1/K of
+// the sample, src/map2d_optimizer.cpp:731-760, so a small sample gives
+// noisier references, broader posteriors and more significant hypotheses).
+// The first -warm_pools + -time_pools pools of iteration 2 are then
+// processed as expectation() does (src/map2d_optimizer.cpp:760-799) and
+// expectationSomeParticles() (:802-854) of the last -time_pools is timed
+// with the reference's own dtime(); every OpenMP thread of the host is
+// used.  Prints one line per timed pool and a total:
 //   map2d_bench_pool index=<i> particles=<n> estep_s=<t>
 //   map2d_bench particles=<n> estep_s=<t> prep_s=<t> current_size=<s> threads=<n>
 #include "map2d_optimizer.h"
@@ -39,6 +46,8 @@ int main(int argc, char* argv[]) {
     option.addOption("-psi_step", "Psi step (degrees)", "10");
     option.addOption("-ctf", "CTF correction", "0");
     option.addOption("-time_pools", "Pools of iteration 2 to time", "1");
+    option.addOption("-warm_pools", "Pools of iteration 2 run before timing", "0");
+    option.addOption("-refs_raw", "K class references, float64 [K][ori][ori] raw (skips iteration 1)", "NULL");
     option.readCommandLine(argc, argv);
 
     star_fn = pathRemoveSuffix(option.getStrOption("-i")) + ".star";
@@ -70,11 +79,29 @@ int main(int argc, char* argv[]) {
     ref_fn = "NULL";
     const int time_pools = option.getIntOption("-time_pools");
 
+    const int warm_pools = option.getIntOption("-warm_pools");
+    const std::string refs_raw = option.getStrOption("-refs_raw");
+
     setupMap2dOptimizer();
     readImages();
     Map2dOptimizer_old::prepare();
-    nr_iter = 1;
-    Map2dOptimizer_old::iterate();
+    if (refs_raw == "NULL") {
+        nr_iter = 1;
+        Map2dOptimizer_old::iterate();
+    } else {
+        const size_t n2 = (size_t)ori_size * ori_size;
+        std::vector<double> buf(n2 * nr_classes);
+        FILE* f = std::fopen(refs_raw.c_str(), "rb");
+        if (!f || std::fread(buf.data(), sizeof(double), buf.size(), f) != buf.size()) {
+            std::fprintf(stderr, "map2d_bench: cannot read %zu doubles from -refs_raw\n", buf.size());
+            return 2;
+        }
+        std::fclose(f);
+        for (int k = 0; k < nr_classes; k++) {
+            auto r = mapModel.Irefs[k].wptr();
+            for (size_t i = 0; i < n2; i++) r[i] = buf[k * n2 + i];
+        }
+    }
     nr_iter = 2;
     iter = 2;
 
@@ -92,7 +119,7 @@ int main(int argc, char* argv[]) {
 
     double t_estep = 0, t_prep = 0;
     int nr_done = 0, pool_index = 0, timed = 0;
-    while (nr_done < nr_local_images && pool_index < time_pools) {
+    while (nr_done < nr_local_images && pool_index < warm_pools + time_pools) {
         int first = first_local_image + nr_done;
         int last = std::min(first_local_image + nr_local_images - 1, first + nr_pool - 1);
         exp_first_image = first;
@@ -113,11 +140,13 @@ int main(int argc, char* argv[]) {
         const double t1 = dtime();
         expectationSomeParticles();
         const double t2 = dtime();
-        std::printf("map2d_bench_pool index=%d particles=%d estep_s=%.6f\n", pool_index, exp_nr_images, t2 - t1);
-        std::fflush(stdout);
-        t_prep += t1 - t0;
-        t_estep += t2 - t1;
-        timed += exp_nr_images;
+        if (pool_index >= warm_pools) {
+            std::printf("map2d_bench_pool index=%d particles=%d estep_s=%.6f\n", pool_index, exp_nr_images, t2 - t1);
+            std::fflush(stdout);
+            t_prep += t1 - t0;
+            t_estep += t2 - t1;
+            timed += exp_nr_images;
+        }
         for (int i = 0; i < exp_nr_images; i++) metadata[i + first] = exp_metadata[i];
         nr_done += last - first + 1;
         pool_index++;

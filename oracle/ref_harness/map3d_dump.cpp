@@ -81,6 +81,8 @@ void dump_backprojectors(Dumper& d, const std::string& pre) {
 }
 
 // the sampling tables of the current pass and its per-particle inputs
+bool g_light = false;
+
 void dump_pass_inputs(Dumper& d, const std::string& pre) {
     int nd = exp_nr_dir, npsi = exp_nr_psi, nor = exp_nr_over_rot, ntr = exp_nr_trans, notr = exp_nr_over_trans;
     std::vector<double> ang((size_t)nd * npsi * nor * 3);
@@ -121,8 +123,10 @@ void dump_pass_inputs(Dumper& d, const std::string& pre) {
                 si[((size_t)i * ntr * notr + t) * F + n] = pi[n];
             }
         }
-    d.f64(pre + "Fimg_shifted_real", sr.data(), {exp_nr_images, ntr * notr, F});
-    d.f64(pre + "Fimg_shifted_imag", si.data(), {exp_nr_images, ntr * notr, F});
+    if (!g_light) {
+        d.f64(pre + "Fimg_shifted_real", sr.data(), {exp_nr_images, ntr * notr, F});
+        d.f64(pre + "Fimg_shifted_imag", si.data(), {exp_nr_images, ntr * notr, F});
+    }
 }
 
 // Exp_Mweight_old as flat lists: count[P][K][ndir][npsi], then (ihidden, value)
@@ -199,6 +203,9 @@ int main(int argc, char* argv[]) {
     option.addOption("-always_cc", "CC in every iteration", "0");
     option.addOption("-dump_pools", "Number of pools dumped step by step", "1");
     option.addOption("-uniform_directions", "Reset pdf_direction to uniform before the dumped iteration", "0");
+    option.addOption("-full_size", "Run the dumped iteration at the full image size (current resolution = Nyquist)", "0");
+    option.addOption("-light", "Skip the per-translation shifted images and the input maps (large at 128^2)", "0");
+    option.addOption("-skip_mstep", "Stop after dumping the M-step inputs (no maximization)", "0");
     option.readCommandLine(argc, argv);
 
     std::string dump_dir = option.getStrOption("-dump_dir");
@@ -241,6 +248,7 @@ int main(int argc, char* argv[]) {
     guidance_fn = "NULL";
     iter = 0;
     int dump_pools = option.getIntOption("-dump_pools");
+    g_light = option.getBoolOption("-light");
     if (dump_iter < 2 || adaptive_oversampling < 1) {
         std::cerr << "-iter must be >= 2 and -oversampling >= 1" << std::endl;
         return 2;
@@ -263,6 +271,11 @@ int main(int argc, char* argv[]) {
         for (int k = 0; k < nr_classes; k++)
             for (int j = 0; j < sampler3d.NrDir(); j++)
                 mlModel.pdf_direction[k][j] = 1. / ((double)nr_classes * sampler3d.NrDir());
+
+    // Optionally run the dumped iteration at the full image size, the size
+    // a converged refinement reaches (current_size = ori_size, projectors
+    // padded to 2*(2*ori/2+1)+1), whatever resolution the short run reached.
+    if (option.getBoolOption("-full_size")) mapModel.current_resolution = 1. / (2. * pixel_size);
 
     // ---- iteration dump_iter, step by step (iterate() body) ----
     double ang = sampler3d.getAngularSampling();
@@ -335,7 +348,7 @@ int main(int argc, char* argv[]) {
         d.iscalar("projector_r_max", mapModel.projector[0].r_max);
         d.iscalar("projector_pad_size", pad);
         d.iscalar("projector_padding_factor", mapModel.projector[0].padding_factor);
-        d.f64("Irefs_before", irefs.data(), {K, ori_size, ori_size, ori_size});
+        if (!g_light) d.f64("Irefs_before", irefs.data(), {K, ori_size, ori_size, ori_size});
         std::vector<double> tau2((size_t)K * oF), dvp((size_t)K * oF);
         for (int k = 0; k < K; k++)
             for (int n = 0; n < oF; n++) {
@@ -459,6 +472,10 @@ int main(int argc, char* argv[]) {
     // ---- M-step inputs and outputs ----
     dump_model_sums(d, "iter_");
     dump_backprojectors(d, "iter_");
+    if (option.getBoolOption("-skip_mstep")) {
+        std::cout << "map3d_dump: done (M-step skipped)" << std::endl;
+        return 0;
+    }
     maximization();
     {
         size_t ov = (size_t)ori_size * ori_size * ori_size;

@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <map>
@@ -191,8 +192,11 @@ void launch(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B,
 // The first call with a given key -- epilogue kind, operand planes, device,
 // N, Kp and the number of 128-row tiles rounded up to a power of two -- runs
 // every candidate shape on that call's own operands, timed with CUDA events
-// on the call's stream (one untimed run, then one timed run each), and keeps
-// the fastest; later calls with the key launch it directly.  All candidates
+// on the call's stream (one untimed run, then the median of three timed
+// runs each), and keeps the fastest; later calls with the key launch it
+// directly.  Only the table is locked: tuning runs outside the lock, and
+// other host threads that meet a key while it is being tuned launch the
+// default shape.  All candidates
 // write identical outputs (each output element accumulates the same K blocks
 // in the same order whatever the tile width, and the epilogues only store
 // values and fold row minima), so the results do not depend on which
@@ -214,6 +218,7 @@ struct TuneKey {
 };
 struct TuneEntry {
     int choice = 0, ncand = 0;
+    bool done = false;
     const char* names[4] = {};
     float ms[4] = {};
 };
@@ -251,33 +256,45 @@ void tuned(int kind, int nplane, const Cand<Epi> (&c)[NC], cudaStream_t st, int 
     int mb = 1;
     while (mb < (M + BM - 1) / BM) mb <<= 1;
     const TuneKey key{kind, nplane, dev, N, Kp, mb};
-    std::lock_guard<std::mutex> lock(g_tune_mu);
-    auto it = g_tune.find(key);
-    if (it != g_tune.end()) {
-        c[it->second.choice].fn(st, M, N, Kp, A, B, epi, derr);
-        return;
+    {
+        // the lock covers the table only: a key being tuned by another host
+        // thread runs the default shape meanwhile instead of waiting
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+            const int q = it->second.done ? it->second.choice : 0;
+            c[q].fn(st, M, N, Kp, A, B, epi, derr);
+            return;
+        }
+        g_tune[key] = TuneEntry{};  // in progress
     }
     TuneEntry e;
     e.ncand = NC;
-    cudaEvent_t ev[2];
-    ROME_CUDA(cudaEventCreate(&ev[0]));
-    ROME_CUDA(cudaEventCreate(&ev[1]));
+    constexpr int kReps = 3;
+    cudaEvent_t ev[kReps + 1];
+    for (auto& x : ev) ROME_CUDA(cudaEventCreate(&x));
     float best = 0.f;
     for (int q = 0; q < NC; q++) {
         e.names[q] = c[q].name;
         c[q].fn(st, M, N, Kp, A, B, epi, derr);
         ROME_CUDA(cudaEventRecord(ev[0], st));
-        c[q].fn(st, M, N, Kp, A, B, epi, derr);
-        ROME_CUDA(cudaEventRecord(ev[1], st));
-        ROME_CUDA(cudaEventSynchronize(ev[1]));
-        ROME_CUDA(cudaEventElapsedTime(&e.ms[q], ev[0], ev[1]));
+        for (int r = 0; r < kReps; r++) {
+            c[q].fn(st, M, N, Kp, A, B, epi, derr);
+            ROME_CUDA(cudaEventRecord(ev[r + 1], st));
+        }
+        ROME_CUDA(cudaEventSynchronize(ev[kReps]));
+        float t[kReps];
+        for (int r = 0; r < kReps; r++) ROME_CUDA(cudaEventElapsedTime(&t[r], ev[r], ev[r + 1]));
+        std::sort(t, t + kReps);
+        e.ms[q] = t[kReps / 2];  // median of the timed runs
         if (q == 0 || e.ms[q] < best) {
             best = e.ms[q];
             e.choice = q;
         }
     }
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
+    for (auto& x : ev) cudaEventDestroy(x);
+    e.done = true;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
     g_tune[key] = e;
 }
 
@@ -323,6 +340,7 @@ std::string tc_tuning_report() {
     for (const auto& kv : g_tune) {
         const TuneKey& k = kv.first;
         const TuneEntry& e = kv.second;
+        if (!e.done) continue;
         int n = snprintf(line, sizeof line, "%s planes=%d dev=%d N=%d Kp=%d mtiles=%d choice=%s", kinds[k.kind],
                          k.nplane, k.dev, k.N, k.Kp, k.mb, e.names[e.choice]);
         for (int q = 0; q < e.ncand && n < (int)sizeof line; q++)

@@ -654,7 +654,11 @@ extern "C" int rome_gpu_select_significant(RomeGpuCtx* ctx, int n, long len, con
 //
 // The first call on each device looks the array's device address up
 // (cudaGetSymbolAddress, which may load the module on that device); make
-// that first call before any stream capture on the device.  All calls on one
+// that first call before any stream capture on the device.  Under lazy
+// module loading that first call is where the driver reserves the array and
+// the module's code, so it is a warm-up: later calls allocate nothing.  The
+// call is synchronous (results are in the caller's host arrays when it
+// returns).  All calls on one
 // device share the array, so two calls overlapping in time would race on it:
 // the entry point holds a process-wide lock and returns only after its
 // stream work has finished, which serialises calls from different host

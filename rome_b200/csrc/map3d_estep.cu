@@ -324,6 +324,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                 ROME_CHECK_LAUNCH();
                 prof.launched(ROME_PHASE_CROSS_GEMM);
                 prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * J * g.Kact);
+                prof.add_bytes(ROME_PHASE_CROSS_GEMM, 4.0 * (double)M * J);  // diff2 written once
                 prof.end(ROME_PHASE_CROSS_GEMM);
             } else {
                 // ---- restricted coarse search: only the proposed orientations ----
@@ -367,6 +368,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             int listcap = std::max(1024, P * 64), nsig = 0;
             SigEntry* dList = nullptr;
             prof.begin(ROME_PHASE_POSTERIOR);
+            prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)P * Xrow);  // diff2 read once
             for (;;) {
                 dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap);
                 SelectResult sr = run_select(ctx, st, 0, P, Xrow, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
@@ -572,6 +574,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         int listcap = std::max(1024, P * 64), nsig = 0;
         SigEntry* dList = nullptr;
         prof.begin(ROME_PHASE_POSTERIOR);
+        prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)P * Xf);  // diff2 rows read once
         for (;;) {
             dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
             SelectResult sr = run_select(ctx, st, 0, P, Xf, Lf, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,

@@ -138,12 +138,16 @@ def prepared_pool(ctx: GpuContext, template: Map2dPool, imgs: ParticleImages, op
                   power: bool = False) -> StagedPool:
     """The E-step input of a pool prepared on the device: `template`'s model
     and sampling with this pool's particles, the images left on the device
-    (a StagedPool for GpuContext.map2d_estep_pool and the learned E-step)."""
+    (a StagedPool for GpuContext.map2d_estep_pool and the learned E-step, or,
+    with a Map3dPool template, for map3d.map3d_estep_pool(ctx, sp.pool,
+    dev=sp.dev))."""
     o = prepare_particles(ctx, imgs, opts, template.sigma2_noise, template.current_size, on_device=True, power=power)
     P = imgs.nr_images
     rep = {name: np.empty((P, 0)) for name in DEVICE_FIELDS}
     rep.update(highres_Xi2=o["highres_Xi2"], old_offsetx=o["old_offsetx"], old_offsety=o["old_offsety"],
-               group=_i32(imgs.group), proposals=None, particle_rows=None)
+               group=_i32(imgs.group), proposals=None)
+    if hasattr(template, "particle_rows"):  # MAP2D pools only
+        rep["particle_rows"] = None
     pool = dataclasses.replace(template, **rep)
     sp = StagedPool(pool, {name: o[name] for name in DEVICE_FIELDS})
     if power:

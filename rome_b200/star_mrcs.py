@@ -220,6 +220,7 @@ class ParticleStack:
             raise ValueError(f"{star_path}: image {self.index[i]} of {paths[self.stack[i]]} is outside its stack "
                              f"of {headers[self.stack[i]].ns}")
         self._maps: Dict[int, np.memmap] = {}
+        self._maps_lock = threading.Lock()
 
     @staticmethod
     def _groups(group_names: Sequence[str], mics: Sequence[str]):
@@ -241,13 +242,15 @@ class ParticleStack:
         return self._size
 
     def _map(self, s: int) -> np.memmap:
-        m = self._maps.get(s)
-        if m is None:
-            S = self._size
-            m = np.memmap(self.stack_paths[s], dtype="<f4", mode="r", offset=MRC_HEADER_BYTES,
-                          shape=(self.headers[s].ns, S, S))
-            self._maps[s] = m
-        return m
+        # reader threads share the maps: one mapping per stack
+        with self._maps_lock:
+            m = self._maps.get(s)
+            if m is None:
+                S = self._size
+                m = np.memmap(self.stack_paths[s], dtype="<f4", mode="r", offset=MRC_HEADER_BYTES,
+                              shape=(self.headers[s].ns, S, S))
+                self._maps[s] = m
+            return m
 
     def read_images(self, rows: np.ndarray, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Images of the given particle rows, float32 [len(rows)][S][S];
@@ -276,7 +279,10 @@ class ParticleStack:
             if np.all(np.diff(idx) == 1):
                 out[:] = mm[idx[0]:idx[0] + idx.size]
             else:
-                np.take(mm, idx, axis=0, out=out)
+                # indices were range-checked when the STAR file was read; with
+                # mode="clip" numpy gathers straight into `out` (the default
+                # mode="raise" buffers the whole gather and copies it again)
+                np.take(mm, idx, axis=0, out=out, mode="clip")
             return out
         i = 0
         while i < rows.size:

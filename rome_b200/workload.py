@@ -453,7 +453,7 @@ def build_map3d(w: Map3dWorkload):
         pdf_class=np.full(K, 1.0 / K), pdf_direction=np.full((K, ndir), 1.0 / ndir),
         prior_offsetx_class=np.zeros(K), prior_offsety_class=np.zeros(K),
         sigma2_offset=float(w.offset_range) ** 2 / 4.0, adaptive_oversampling=1)
-    truth = dict(cls=cls, rot=rot, tilt=tilt, psi=psi, sx=sx, sy=sy)
+    truth = dict(cls=cls, rot=rot, tilt=tilt, psi=psi, sx=sx, sy=sy, defocus_u=du, defocus_v=dv, defocus_angle=da)
     return pool, proj, r_max, truth
 
 

@@ -9,6 +9,8 @@ use into tests/golden/<case>.npz.
 
     python tests/golden/make_golden.py            # all cases
     python tests/golden/make_golden.py map2d_a    # one case
+
+ROME_REFERENCE (or REF) names the reference tree oracle/Makefile compiles.
 """
 from __future__ import annotations
 
@@ -54,6 +56,78 @@ CASES3D = {
                 dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1, pool=4,
                      offset_range=2, offset_step=1, ctf=1, uniform_directions=1)),
 }
+# 128^2 cases of the MAP3D configuration's shape (HEALPix order 2: 192 directions x 24 psi, 13
+# translations, oversampling 1, fine pass at the full size, M-step into the pad-259 grid).  The
+# whole dump (~1.2 GB: projectors and back-projectors at pad 259) is too large to commit: the
+# fixture keeps every per-particle result, the model sums, checksums of the large arrays and the
+# M-step outputs (class 0's map as float32), and the GPU tests regenerate the full dump from the
+# same seeded dataset with oracle/_ref/map3d_dump (run_map3d_dump, M-step skipped) and check it
+# against the fixture before comparing.
+CASES3D_FULL = {
+    # 24 particles in pools of 8 (every pool recorded), K=2, SNR 0.05, iteration 2 at full size
+    "map3d_b": (Map3dSpec(n_particles=24, size=128, n_classes=2, n_blobs=60, blob_sigma=(2.0, 8.0), max_shift=4.0,
+                          snr=0.05, pixel=1.5, seed=13),
+                dict(K=2, iter=2, angpix=1.5, ini_high=30, tau2_fudge=2, oversampling=1, healpix_order=2, pool=8,
+                     offset_range=4, offset_step=2, ctf=1, uniform_directions=1, full_size=1, light=1, dump_pools=3)),
+}
+# per-particle results and model sums copied whole from a CASES3D_FULL dump (name suffixes)
+FULL_KEEP = ("min_diff2", "sum_weight", "significant_weight", "nr_sign", "pmax", "class", "rot", "tilt", "psi",
+             "xoff", "yoff", "dLL", "norm_out", "wsum_norm_correction", "wsum_sigma2_noise", "wsum_pdf_class",
+             "wsum_pdf_direction", "wsum_sigma2_offset", "wsum_sumw_group", "wsum_LL", "wsum_ave_Pmax",
+             "current_size", "coarse_size", "nr_dir", "nr_psi", "nr_trans", "nr_images", "gridding_nr_iter",
+             "minres_map", "do_map", "tau2_fudge_factor", "_count", "_after", "_before", "pdf_class",
+             "projector_r_max", "projector_pad_size")
+# large arrays represented by checksums (sum, sum of squares, element count)
+FULL_CHECKSUM = ("projector_data", "iter_bp_data", "iter_bp_weight", "pass0_diff2_value", "pass1_diff2_value",
+                 "pass0_weight_value", "pass1_weight_value", "Fimg_real", "Fimg_nomask_real", "Fctf",
+                 "pass0_Mcoarse_significant")
+
+
+def run_map3d_dump(name: str, out_dir: str, skip_mstep: bool = True, threads: int = 0) -> dict:
+    """Write the seeded dataset of a CASES3D_FULL case under out_dir and run
+    oracle/_ref/map3d_dump on it (the reference's own MAP3D path); returns
+    the dump's arrays.  Used by make_case3d_full and by the GPU tests, which
+    run it on the test machine (the binary is built from the reference here
+    and travels with the repository; the reference tree itself is not read)."""
+    from rome_b200.map2d import load_dump as _load
+    spec, opt = CASES3D_FULL[name]
+    os.makedirs(out_dir, exist_ok=True)
+    star, ref = write_dataset_3d(os.path.join(out_dir, "data"), spec)
+    dump = os.path.join(out_dir, "dump")
+    cmd = [os.path.join(ROOT, "oracle", "_ref", "map3d_dump"), "-i", star, "-ref", ref, "-dump_dir", dump]
+    for k, v in opt.items():
+        cmd += [f"-{k}", str(v)]
+    if skip_mstep:
+        cmd += ["-skip_mstep", "1"]
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=out_dir)
+    return _load(dump)
+
+
+def checksum(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a, np.float64).ravel()
+    return np.array([a.sum(), np.dot(a, a), a.size])
+
+
+def make_case3d_full(name: str):
+    tmp = tempfile.mkdtemp(prefix="rome_golden_")
+    try:
+        d = run_map3d_dump(name, tmp, skip_mstep=False)
+        keep = {k: v for k, v in d.items() if k.endswith(FULL_KEEP) and v.nbytes <= (1 << 20)}
+        for k, v in d.items():
+            if k.endswith(FULL_CHECKSUM):
+                keep["checksum_" + k] = checksum(v)
+        keep["Irefs_after0_f32"] = d["Irefs_after"][0].astype(np.float32)
+        keep["meta_options"] = np.array([str(CASES3D_FULL[name][1])])
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(out, **keep)
+        print(f"{name}: {len(keep)} arrays, {os.path.getsize(out) / 1e6:.2f} MB")
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
 # reconstruction at known poses: (dataset spec, rome_reconstruct options) for oracle/_ref/rome_reconstruct_ref
 CASESRECON = {
     # 32^2 particles of one blob volume, CTF on, poses and origins from the generator, 10 gridding iterations
@@ -71,7 +145,9 @@ SKIP_SUFFIXES = ("Fimg_shifted_real", "Fimg_shifted_imag", "Fref_real", "Fref_im
 
 
 def build_reference():
-    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", "_ref/map2d_dump", "_ref/map3d_dump",
+    ref = os.environ.get("ROME_REFERENCE") or os.environ.get("REF", "")
+    subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", f"REF={ref}", "_ref/map2d_dump",
+                           "_ref/map3d_dump",
                            "_ref/librome_oracle.so", "_ref/rome_reconstruct_ref"], stdout=subprocess.DEVNULL)
 
 
@@ -178,9 +254,11 @@ def make_case(name: str):
 
 if __name__ == "__main__":
     build_reference()
-    names = sys.argv[1:] or list(CASES) + list(CASES3D) + list(CASESRECON)
+    names = sys.argv[1:] or list(CASES) + list(CASES3D) + list(CASESRECON) + list(CASES3D_FULL)
     for n in names:
-        if n in CASESRECON:
+        if n in CASES3D_FULL:
+            make_case3d_full(n)
+        elif n in CASESRECON:
             make_recon_case(n)
         elif n in CASES3D:
             make_case3d(n)

@@ -1,0 +1,233 @@
+"""GPU MAP3D E-step and M-step parity at the 3D configuration's shape:
+particles of 128^2, HEALPix order 2 (192 directions x 24 psi in the coarse
+pass at coarse size 20, 8 over-rotations x 4 over-translations per
+coarse-significant point in the fine pass at the full size 128, F = 8,320),
+13 translations (+-4 px step 2), K = 2, CTF on, and the M-step into the
+pad-259 grid (2 * (2 * 64 + 1) + 1), 10 gridding iterations.
+
+The reference side is the reference's own MAP3D path (oracle/_ref/map3d_dump,
+compiled from the reference sources) run on the seeded 24-particle dataset
+of the `map3d_b` case in tests/golden/make_golden.py, iteration 2 at the
+full image size, three pools of 8, every pool recorded.  Its dump is about
+1.2 GB (projectors and back-projectors at pad 259), too large to commit, so
+the test regenerates it on this machine (M-step skipped) and first checks
+it against tests/golden/map3d_b.npz, which holds every per-particle result,
+the model sums, checksums of the large arrays and the M-step outputs
+recorded when the fixture was made.  The per-particle selection of this
+dataset is heavy-tailed (from 5 to ~37,000 coarse-significant hypotheses
+per particle), so both the short and the long fine lists are exercised.
+
+Tolerances of the plain FP32 mode are those of test_gpu_map3d: diff2 <= 1e-5
+relative per hypothesis in both passes, the reference's exact hypothesis
+lists, FP64 sums / weights / model sums / back-projectors within 1e-3
+relative, identical best poses except at a near tie of the reference's top
+two weights; M-step FSC >= 0.999 at every shell and <= 1e-6 relative RMS
+against the reference's maximization() map (stored as float32, whose
+rounding is ~6e-8 relative), sigma2 / data_vs_prior spectra to 1e-9.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from rome_b200.map2d import GpuContext
+from rome_b200.map3d import fine_lists_from_dump, map3d_estep_pool, pool3d_from_dump
+from tests.test_gpu_reconstruct import fsc
+from tests.util import relerr
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "map3d_dump")
+DIFF2_TOL = 1e-5
+SUM_TOL = 1e-3
+NPOOLS = 3
+WSUMS = ["wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_sigma2_offset", "wsum_sumw_group"]
+
+
+@pytest.fixture(scope="module")
+def full3d(golden, tmp_path_factory):
+    if not os.path.exists(REF_BIN):
+        pytest.skip("oracle/_ref/map3d_dump is not built (it is compiled where the reference tree is present)")
+    from tests.golden.make_golden import run_map3d_dump
+    d = run_map3d_dump("map3d_b", str(tmp_path_factory.mktemp("map3d_b")), skip_mstep=True)
+    return d, golden["map3d_b"]
+
+
+@pytest.fixture(scope="module")
+def gpu_fp32(full3d):
+    d, _ = full3d
+    out = []
+    with GpuContext(0, "fp32") as ctx:
+        ctx.set_projectors(d["projector_data"], int(d["ori_size"][0]), int(d["projector_r_max"][0]))
+        for k in range(NPOOLS):
+            p = pool3d_from_dump(d, k)
+            o = map3d_estep_pool(ctx, p, checkpoints=True)
+            if k == 0:
+                bp = [ctx.get_backprojector(c) for c in range(p.nr_classes)]
+                o["bp_data"] = np.stack([b[0] for b in bp])
+                o["bp_weight"] = np.stack([b[1] for b in bp])
+            out.append((p, o))
+    return out
+
+
+def test_regenerated_dump_matches_fixture(full3d):
+    """The reference run here reproduces the one the fixture was recorded from."""
+    from tests.golden.make_golden import checksum
+    d, g = full3d
+    checked = 0
+    for k, v in g.items():
+        if k.startswith("checksum_"):
+            name = k[len("checksum_"):]
+            assert name in d, name
+            c = checksum(d[name])
+            assert c[2] == v[2] and abs(c[0] - v[0]) <= 1e-9 * max(abs(v[0]), 1e-300) + 1e-12 * np.sqrt(v[1]), name
+            assert abs(c[1] - v[1]) <= 1e-9 * v[1], name
+        elif k in d:
+            a, b = np.asarray(d[k]), np.asarray(v)
+            assert a.shape == b.shape, k
+            if np.issubdtype(b.dtype, np.integer):
+                assert np.array_equal(a, b), k
+            else:
+                assert relerr(a, b) <= 1e-9, k
+        else:
+            continue
+        checked += 1
+    assert checked > 100, checked
+
+
+def coarse_ref(d, p, pool):
+    out = np.full((p.nr_images, p.ncoarse), float(np.iinfo(np.int32).min))
+    for i, (idx, v) in enumerate(fine_lists_from_dump(d, f"pool{pool}_pass0_diff2_", p.nr_trans, nh=1)):
+        out[i, idx] = v
+    return out
+
+
+def test_coarse_pass_matches_reference(full3d, gpu_fp32):
+    d, _ = full3d
+    for k, (p, o) in enumerate(gpu_fp32):
+        pre = f"pool{k}_pass0_"
+        ref = coarse_ref(d, p, k)
+        ok = ref > -1e9
+        assert np.array_equal(ok, o["coarse_diff2"] > -1e9), f"pool {k}: different coarse hypotheses computed"
+        rel = np.abs(o["coarse_diff2"][ok] - ref[ok]) / np.abs(ref[ok])
+        assert rel.max() <= DIFF2_TOL, (k, rel.max())
+        assert relerr(o["pass_min_diff20"], d[pre + "min_diff2"]) < DIFF2_TOL
+        assert relerr(o["pass_sum_weight0"], d[pre + "sum_weight"]) < SUM_TOL
+        assert relerr(o["pass_significant_weight0"], d[pre + "significant_weight"]) < SUM_TOL
+        agree = (o["Mcoarse_significant"] == d[pre + "Mcoarse_significant"]).mean()
+        assert agree >= 0.999, (k, agree)
+        nr = np.abs(o["nr_sign"] - d[pre + "nr_sign"]) / d[pre + "nr_sign"]
+        assert nr.max() <= 0.01, (k, nr.max())
+
+
+def test_fine_pass_lists_match_reference(full3d, gpu_fp32):
+    d, _ = full3d
+    checked = total = 0
+    for k, (p, o) in enumerate(gpu_fp32):
+        d2 = fine_lists_from_dump(d, f"pool{k}_pass1_diff2_", p.nr_trans)
+        wt = fine_lists_from_dump(d, f"pool{k}_pass1_weight_", p.nr_trans)
+        mc_same = (o["Mcoarse_significant"] == d[f"pool{k}_pass0_Mcoarse_significant"]).all(axis=1)
+        q = 0
+        for i in range(p.nr_images):
+            n = int(o["fine_count"][i])
+            idx, dv, w = o["fine_index"][q:q + n], o["fine_diff2"][q:q + n], o["fine_weight"][q:q + n]
+            q += n
+            total += 1
+            if not mc_same[i]:
+                continue
+            ridx, rd = d2[i]
+            assert np.array_equal(idx, ridx), f"pool {k} particle {i}: fine list differs"
+            rel = np.abs(dv - rd) / np.abs(rd)
+            assert rel.max() <= DIFF2_TOL, (k, i, rel.max())
+            assert relerr(w, wt[i][1]) < SUM_TOL, (k, i)
+            checked += 1
+    assert checked >= total - 1, (checked, total)
+
+
+def _same_pose(o, d, pre):
+    return ((o["cls"] == d[pre + "class"]) & (o["rot"] == d[pre + "rot"]) & (o["tilt"] == d[pre + "tilt"])
+            & (o["psi"] == d[pre + "psi"]) & (o["xoff"] == d[pre + "xoff"]) & (o["yoff"] == d[pre + "yoff"]))
+
+
+def _near_tie(wt, i, rel):
+    top = np.sort(wt[i][1])[::-1][:2]
+    return top.size == 2 and top[1] >= top[0] * (1 - rel)
+
+
+def test_fine_pass_results_match_reference(full3d, gpu_fp32):
+    d, _ = full3d
+    for k, (p, o) in enumerate(gpu_fp32):
+        pre = f"pool{k}_pass1_"
+        assert relerr(o["min_diff2"], d[pre + "min_diff2"]) < DIFF2_TOL
+        assert relerr(o["sum_weight"], d[pre + "sum_weight"]) < SUM_TOL
+        assert relerr(o["significant_weight"], d[pre + "significant_weight"]) < SUM_TOL
+        assert relerr(o["pmax"], d[pre + "pmax"]) < SUM_TOL
+        wt = fine_lists_from_dump(d, pre + "weight_", p.nr_trans)
+        for i in np.nonzero(~_same_pose(o, d, pre))[0]:
+            assert _near_tie(wt, i, 1e-3), f"pool {k} particle {i}: pose differs without a near tie"
+
+
+def test_wsums_and_backprojection_match_reference(full3d, gpu_fp32):
+    d, _ = full3d
+    for k, (p, o) in enumerate(gpu_fp32):
+        assert relerr(o["wsum_norm_correction"], d[f"pool{k}_wsum_norm_correction"]) < SUM_TOL
+        for name in WSUMS:
+            # the reference's sums accumulate over pools: this pool's share is the difference
+            ref = d[f"pool{k}_after_update_{name}"] - (d[f"pool{k - 1}_after_store_{name}"] if k else 0.0)
+            assert relerr(o[name], ref) < SUM_TOL, (k, name)
+    o = gpu_fp32[0][1]
+    assert relerr(o["bp_data"], d["pool0_after_bp_bp_data"]) < SUM_TOL
+    assert relerr(o["bp_weight"], d["pool0_after_bp_bp_weight"]) < SUM_TOL
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "bf16"])
+def test_tensor_core_coarse_pass_poses(full3d, prec):
+    """Tensor-core coarse pass (split BF16 / BF16): the final poses are the
+    reference's except where its top two weights are within the precision's
+    diff2 error of each other (1e-3 relative weight for split BF16, which is
+    as accurate as FP32; exp(-0.05) for BF16, whose cross term carries
+    ~1e-4 relative error)."""
+    d, _ = full3d
+    same_all, n = 0, 0
+    tie = 1e-3 if prec == "bf16x3" else 1 - np.exp(-0.05)
+    with GpuContext(0, prec) as ctx:
+        ctx.set_projectors(d["projector_data"], int(d["ori_size"][0]), int(d["projector_r_max"][0]))
+        for k in range(NPOOLS):
+            p = pool3d_from_dump(d, k)
+            o = map3d_estep_pool(ctx, p)
+            pre = f"pool{k}_pass1_"
+            same = _same_pose(o, d, pre)
+            wt = fine_lists_from_dump(d, pre + "weight_", p.nr_trans)
+            for i in np.nonzero(~same)[0]:
+                assert _near_tie(wt, i, tie), f"{prec} pool {k} particle {i}: pose differs without a near tie"
+            assert relerr(o["sum_weight"], d[pre + "sum_weight"]) < (SUM_TOL if prec == "bf16x3" else 0.05)
+            same_all += int(same.sum())
+            n += same.size
+    print(f"{prec}: {same_all}/{n} poses identical")
+
+
+def test_reconstruct_pad259_matches_reference(full3d):
+    """maximization() of both classes from the reference's own back-projectors
+    (pad 259): the map of class 0 against the recorded map, and the sigma2 /
+    data_vs_prior spectra of both classes."""
+    d, g = full3d
+    ori = int(d["ori_size"][0])
+    K = int(d["nr_classes"][0])
+    assert d["iter_bp_data"].shape[1] == 259
+    with GpuContext(0) as ctx:
+        ctx.set_projectors(d["projector_data"], ori, int(d["projector_r_max"][0]))
+        for k in range(K):
+            ctx.set_backprojector(k, d["iter_bp_data"][k], d["iter_bp_weight"][k])
+            o = ctx.reconstruct(k, ori, 3, d["tau2_class_before"][k], float(d["tau2_fudge_factor"][0]),
+                                float(d["iter_wsum_pdf_class"][k]), int(d["gridding_nr_iter"][0]),
+                                bool(d["do_map"][0]), int(d["minres_map"][0]))
+            assert relerr(o["sigma2"], g["sigma2_class_after"][k]) <= 1e-9, k
+            assert relerr(o["data_vs_prior"], g["data_vs_prior_after"][k]) <= 1e-9, k
+            if k == 0:
+                ref = g["Irefs_after0_f32"].astype(np.float64)
+                rms = np.sqrt(np.mean((o["vol"] - ref) ** 2)) / np.sqrt(np.mean(ref ** 2))
+                f = fsc(o["vol"], ref)
+                print(f"map3d_b class 0 at pad 259: rel rms {rms:.2e}, min FSC {f.min():.6f}")
+                assert f.min() >= 0.999
+                assert rms <= 1e-6
