@@ -2,20 +2,29 @@
 //   C[m][n] = sum_k A[m][k] * B[n][k]      A, B bf16, K-major; C fp32 in TMEM
 // with the diff2 epilogue applied straight out of TMEM.
 //
-// One CTA computes a BM x BN = 128 x BN tile (cta_group::1, UMMA M = 128):
+// Persistent, warp-specialised kernel: one CTA per SM walks BM x BN = 128 x
+// BN output tiles (cta_group::1, UMMA M = 128) in a grouped order (GROUP_M
+// row tiles side by side, so the CTAs in flight share B tiles and a few A
+// stripes in L2):
 //   warp 0 / lane 0 : TMA producer (cp.async.bulk.tensor, 128B swizzle,
-//                     STAGES-deep shared-memory ring, mbarrier complete_tx)
+//                     STAGES-deep shared-memory ring over the k blocks of
+//                     every tile, mbarrier complete_tx)
 //   warp 1 / lane 0 : MMA issuer (tcgen05.mma kind::f16, 4 x K16 per 64-wide
-//                     K block; tcgen05.commit frees a stage / signals the
-//                     accumulator)
-//   warps 0-3       : epilogue, tcgen05.ld 32x32b (warp w owns TMEM lanes
-//                     32w..32w+31 = rows of the tile)
+//                     K block) into one of two TMEM accumulators (2 x BN
+//                     columns); tcgen05.commit frees a ring stage and, after
+//                     a tile's last k block, hands the accumulator over
+//   warps 2-9       : epilogue, tcgen05.ld 32x32b (warp w reads TMEM lanes
+//                     32(w%4)..+31 = rows of the tile; warps 2-5 the first
+//                     half of the columns, 6-9 the second), then frees the
+//                     accumulator, so tile i's epilogue runs while tile
+//                     i+1's MMAs fill the other accumulator.
 // Split precision (ROME_PREC_BF16X3) loads hi and lo planes of both operands
 // and issues hi*hi + hi*lo + lo*hi into the same accumulator.
 //
 // Every mbarrier wait is bounded; on expiry the kernel records a timeout in a
-// device flag, drains the copies it issued (again bounded), frees its TMEM
-// and returns, and the host reports ROME_ERR_TIMEOUT.
+// shared flag that every role polls, drains the copies and MMAs it issued
+// (again bounded), frees its TMEM and returns, and the host reports
+// ROME_ERR_TIMEOUT.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -43,9 +52,25 @@ struct TcSmem {
     static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 };
 
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 64 + 32 * kEpiWarps;
+constexpr int GROUP_M = 8;
+
+// tile t of the grouped order -> (row tile, column tile)
+__device__ __forceinline__ void tile_coords(int t, int ntm, int ntn, int& tm, int& tn) {
+    const int per_group = GROUP_M * ntn;
+    const int g = t / per_group, first = g * GROUP_M;
+    const int gm = min(ntm - first, GROUP_M);
+    const int r = t - g * per_group;
+    tm = first + r % gm;
+    tn = r / gm;
+}
+
+__device__ __forceinline__ bool flag_set(const int* f) { return *(volatile const int*)f != 0; }
+
 // NPLANE = 1: bf16; NPLANE = 2: split precision (hi and lo planes)
 template <int BN, int NPLANE, int STAGES, typename Epi>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     tc_gemm_kernel(const __grid_constant__ CUtensorMap mapA0, const __grid_constant__ CUtensorMap mapA1,
                    const __grid_constant__ CUtensorMap mapB0, const __grid_constant__ CUtensorMap mapB1, int M, int N,
                    int Kp, Epi epi, int* err) {
@@ -54,14 +79,15 @@ __global__ void __launch_bounds__(128, 1)
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint64_t* full = (uint64_t*)(smem + STAGES * S::STAGE_BYTES);
     uint64_t* empty = full + STAGES;
-    uint64_t* accum = empty + STAGES;
-    uint32_t* tmem_slot = (uint32_t*)(accum + 1);
+    uint64_t* tfull = empty + STAGES;  // [2] accumulator ready for the epilogue
+    uint64_t* tempty = tfull + 2;      // [2] accumulator drained by the epilogue
+    uint32_t* tmem_slot = (uint32_t*)(tempty + 2);
     __shared__ int timed_out;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int ntm = (M + BM - 1) / BM, ntn = (N + BN - 1) / BN, ntiles = ntm * ntn;
     const int nk = Kp / BK;
-    constexpr uint32_t TMEM_COLS = BN;  // power of two >= 32
+    constexpr uint32_t TMEM_COLS = 2 * BN;  // two accumulators; a power of two >= 32
 
     if (threadIdx.x == 0) {
         timed_out = 0;
@@ -69,7 +95,10 @@ __global__ void __launch_bounds__(128, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        mbar_init(accum, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], kEpiWarps);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -82,91 +111,139 @@ __global__ void __launch_bounds__(128, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
 
-    int issued = 0;  // stages the producer armed (for draining after a timeout)
-    if (warp == 0 && lane == 0) {
-        // ---------------- TMA producer ----------------
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % STAGES;
-            if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) + 1) & 1)) {
-                atomicExch(&timed_out, 1);
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            long it = 0, issued = 0;
+            for (int t = blockIdx.x; t < ntiles && !flag_set(&timed_out); t += gridDim.x) {
+                int tm, tn;
+                tile_coords(t, ntm, ntn, tm, tn);
+                const int m0 = tm * BM, n0 = tn * BN;
+                for (int kb = 0; kb < nk; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (it >= STAGES && !mbar_wait(&empty[s], (uint32_t)(((it / STAGES) + 1) & 1))) {
+                        atomicExch(&timed_out, 1);
+                        break;
+                    }
+                    if (flag_set(&timed_out)) break;
+                    uint8_t* st = smem + s * S::STAGE_BYTES;
+                    mbar_expect_tx(&full[s], S::STAGE_BYTES);
+                    tma_load_2d(st, &mapA0, &full[s], kb * BK, m0);
+                    tma_load_2d(st + S::A_BYTES, &mapB0, &full[s], kb * BK, n0);
+                    if (NPLANE == 2) {
+                        tma_load_2d(st + S::A_BYTES + S::B_BYTES, &mapA1, &full[s], kb * BK, m0);
+                        tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, &mapB1, &full[s], kb * BK, n0);
+                    }
+                    issued = it + 1;
+                }
             }
-            if (timed_out) break;
-            uint8_t* st = smem + s * S::STAGE_BYTES;
-            mbar_expect_tx(&full[s], S::STAGE_BYTES);
-            tma_load_2d(st, &mapA0, &full[s], kb * BK, m0);
-            tma_load_2d(st + S::A_BYTES, &mapB0, &full[s], kb * BK, n0);
-            if (NPLANE == 2) {
-                tma_load_2d(st + S::A_BYTES + S::B_BYTES, &mapA1, &full[s], kb * BK, m0);
-                tma_load_2d(st + 2 * S::A_BYTES + S::B_BYTES, &mapB1, &full[s], kb * BK, n0);
+            if (flag_set(&timed_out)) {
+                // drain the copies still in flight (bounded) before the CTA leaves
+                for (long q = (issued > STAGES ? issued - STAGES : 0); q < issued; q++)
+                    mbar_wait(&full[q % STAGES], (uint32_t)((q / STAGES) & 1));
             }
-            issued = kb + 1;
         }
-    } else if (warp == 1 && lane == 0) {
-        // ---------------- MMA issuer ----------------
-        const uint32_t idesc = idesc_bf16<BN>();
-        for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % STAGES;
-            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            const uint32_t idesc = idesc_bf16<BN>();
+            long it = 0;
+            int lt = 0, committed = -1;
+            for (int t = blockIdx.x; t < ntiles && !flag_set(&timed_out); t += gridDim.x, lt++) {
+                const int b = lt & 1;
+                if (lt >= 2 && !mbar_wait(&tempty[b], (uint32_t)(((lt >> 1) + 1) & 1))) {
+                    atomicExch(&timed_out, 1);
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_base = tmem_base + (uint32_t)(b * BN);
+                bool ok = true;
+                for (int kb = 0; kb < nk; kb++, it++) {
+                    const int s = (int)(it % STAGES);
+                    if (!mbar_wait(&full[s], (uint32_t)((it / STAGES) & 1))) {
+                        atomicExch(&timed_out, 1);
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    uint8_t* st = smem + s * S::STAGE_BYTES;
+                    const uint32_t a0 = smem_u32(st), b0 = smem_u32(st + S::A_BYTES);
+                    const uint32_t a1 = smem_u32(st + S::A_BYTES + S::B_BYTES);
+                    const uint32_t b1 = smem_u32(st + 2 * S::A_BYTES + S::B_BYTES);
+#pragma unroll
+                    for (int j = 0; j < BK / 16; j++) {
+                        // advance 16 bf16 (32 bytes) along K inside the swizzle atom
+                        const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
+                        umma_bf16(acc_base, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, acc);
+                        if (NPLANE == 2) {
+                            umma_bf16(acc_base, sw128_desc(a0 + 32 * j), sw128_desc(b1 + 32 * j), idesc, 1u);
+                            umma_bf16(acc_base, sw128_desc(a1 + 32 * j), sw128_desc(b0 + 32 * j), idesc, 1u);
+                        }
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&tfull[b]);
+                committed = lt;
+            }
+            if (flag_set(&timed_out) && committed >= 0) {
+                // the last accumulator hand-over covers every MMA issued before it (bounded wait)
+                mbar_wait(&tfull[committed & 1], (uint32_t)((committed >> 1) & 1));
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- epilogue ----------------
+        const int q = warp & 3;                  // TMEM lane quarter this warp may read
+        const int half = (warp - 2) >> 2;        // column half
+        const int c_lo = half * (BN / 2), c_hi = c_lo + BN / 2;
+        int lt = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
+            const int b = lt & 1;
+            if (flag_set(&timed_out)) break;
+            if (!mbar_wait(&tfull[b], (uint32_t)((lt >> 1) & 1))) {
                 atomicExch(&timed_out, 1);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint8_t* st = smem + s * S::STAGE_BYTES;
-            const uint32_t a0 = smem_u32(st), b0 = smem_u32(st + S::A_BYTES);
-            const uint32_t a1 = smem_u32(st + S::A_BYTES + S::B_BYTES), b1 = smem_u32(st + 2 * S::A_BYTES + S::B_BYTES);
-#pragma unroll
-            for (int j = 0; j < BK / 16; j++) {
-                // advance 16 bf16 (32 bytes) along K inside the swizzle atom
-                const uint32_t acc = (kb > 0 || j > 0) ? 1u : 0u;
-                umma_bf16(tmem_base, sw128_desc(a0 + 32 * j), sw128_desc(b0 + 32 * j), idesc, acc);
-                if (NPLANE == 2) {
-                    umma_bf16(tmem_base, sw128_desc(a0 + 32 * j), sw128_desc(b1 + 32 * j), idesc, 1u);
-                    umma_bf16(tmem_base, sw128_desc(a1 + 32 * j), sw128_desc(b0 + 32 * j), idesc, 1u);
-                }
-            }
-            umma_commit(&empty[s]);
-        }
-        umma_commit(accum);
-    }
-    __syncwarp();
-    // ---------------- epilogue ----------------
-    bool ok = mbar_wait(accum, 0);
-    if (!ok) atomicExch(&timed_out, 1);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!timed_out) {
-        const int row = m0 + warp * 32 + lane;
-        const uint32_t lane_base = tmem_base + ((uint32_t)(warp * 32) << 16);
-        float rmin = INFINITY;
+            int tm, tn;
+            tile_coords(t, ntm, ntn, tm, tn);
+            const int row = tm * BM + q * 32 + lane, n0 = tn * BN;
+            const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
+            float rmin = INFINITY;
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            float v[16];
-            tmem_ld16(lane_base + c, v);
-            if (row < M) {
+            for (int c = c_lo; c < c_hi; c += 16) {
+                float v[16];
+                tmem_ld16(lane_base + c, v);
+                if (row < M) {
 #pragma unroll
-                for (int q = 0; q < 16; q++) {
-                    int n = n0 + c + q;
-                    if (n < N) rmin = fminf(rmin, epi(row, n, v[q]));
+                    for (int k = 0; k < 16; k++) {
+                        const int n = n0 + c + k;
+                        if (n < N) rmin = fminf(rmin, epi(row, n, v[k]));
+                    }
                 }
             }
+            if (row < M) epi.finish_row(row, rmin);
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        if (row < M) epi.finish_row(row, rmin);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (timed_out) {
-        // drain the copies this CTA issued before leaving (bounded)
-        if (warp == 0 && lane == 0) {
-            for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; kb++)
-                mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1);
-            atomicExch(err, 1);
-        }
-        __syncthreads();
-    }
+    if (threadIdx.x == 0 && timed_out) atomicExch(err, 1);
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(TMEM_COLS));
     }
+}
+
+int sm_count() {
+    int dev = 0, n = 0;
+    ROME_CUDA(cudaGetDevice(&dev));
+    ROME_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n > 0 ? n : 1;
 }
 
 template <int BN, int NPLANE, int STAGES, typename Epi>
@@ -180,8 +257,9 @@ void launch(cudaStream_t st, int M, int N, int Kp, const void* A, const void* B,
     CUtensorMap b1 = NPLANE == 2 ? make_map(Bh + (size_t)N * Kp, N, Kp, BN) : b0;
     auto kern = tc_gemm_kernel<BN, NPLANE, STAGES, Epi>;
     ROME_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, S::TOTAL));
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    kern<<<grid, 128, S::TOTAL, st>>>(a0, a1, b0, b1, M, N, Kp, epi, derr);
+    const long ntiles = (long)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    const int grid = (int)std::min<long>(ntiles, sm_count());
+    kern<<<grid, kThreads, S::TOTAL, st>>>(a0, a1, b0, b1, M, N, Kp, epi, derr);
     ROME_CHECK_LAUNCH();
 }
 

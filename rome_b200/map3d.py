@@ -194,7 +194,8 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
 def pool3d_from_dump(d: Dict[str, np.ndarray], pool: int = 0) -> Map3dPool:
     """The E-step inputs of one pool recorded by oracle/ref_harness/map3d_dump."""
     pp = f"pool{pool}_"
-    g = lambda k: d[k]  # noqa: E731
+    # the sampling tables of an iteration are recorded with its first pool only
+    g = lambda k: d[k] if k in d or not k.startswith(pp) else d["pool0_" + k[len(pp):]]  # noqa: E731
     sc = lambda k: float(np.asarray(d[k]).ravel()[0])  # noqa: E731
     ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
     return Map3dPool(
