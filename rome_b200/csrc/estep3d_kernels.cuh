@@ -112,14 +112,33 @@ __global__ void project3d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
 // exp_Mcoarse_significant in exactly this order).
 
 // number of significant coarse points per particle
+// Significant coarse points per particle (Mcoarse_significant holds 0 or 1
+// per byte): 16 bytes per load when the rows are 16-byte aligned.
 __global__ void mcoarse_count_kernel(long ncoarse, const char* __restrict__ mcoarse, int* __restrict__ cnt) {
     __shared__ int red[32];
     const int i = blockIdx.x;
     const char* m = mcoarse + (long)i * ncoarse;
     int c = 0;
-    for (long e = threadIdx.x; e < ncoarse; e += blockDim.x) c += m[e] != 0;
+    if ((ncoarse & 15) == 0) {
+        const uint4* m4 = (const uint4*)m;
+        for (long q = threadIdx.x; q < ncoarse / 16; q += blockDim.x) {
+            const uint4 v = m4[q];
+            c += __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+        }
+    } else {
+        for (long e = threadIdx.x; e < ncoarse; e += blockDim.x) c += m[e] != 0;
+    }
     c = block_reduce_sum(c, red);
     if (threadIdx.x == 0) cnt[i] = c;
+}
+
+// Orientations some particle needs (exp_Rot_significant,
+// isSignificantAnyParticleAnyTranslation, src/map3d_optimizer.cpp:956-985,
+// :2801-2814) from the list of coarse-significant points (coarse index e =
+// jc * ntr + itr): the same set the dense Mcoarse_significant marks.
+__global__ void rotsig_from_list_kernel(int n, int ntr, const SigEntry* __restrict__ list, char* __restrict__ rotsig) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) rotsig[list[q].e / ntr] = 1;
 }
 
 // Ordered compaction of particle i's significant coarse points e = jc * ntr
@@ -127,64 +146,161 @@ __global__ void mcoarse_count_kernel(long ncoarse, const char* __restrict__ mcoa
 // the compact index of orientation jc among the orientations some particle
 // needs, and (b) the row-layout prior index ent[i * stride + r] =
 // (jc / npsi, itr), the pdf_direction index (class * ndir + dir) and the
-// coarse translation.  Padding of ent stays (-1, 0).
-__global__ void __launch_bounds__(1024)
+// coarse translation.  Padding of ent stays (-1, 0).  Each thread scans 16
+// bytes per step (one block-wide scan of the counts per 8 KB of the row).
+constexpr int FE_THREADS = 512;
+__global__ void __launch_bounds__(FE_THREADS)
     fine_entries_kernel(long ncoarse, int ntr, int npsi, const char* __restrict__ mcoarse, const int* __restrict__ off,
                         const int* __restrict__ ucompact, int stride, int4* __restrict__ fe, int2* __restrict__ ent) {
-    __shared__ int wsum[32];
-    __shared__ int base;
+    __shared__ int wsum[FE_THREADS / 32 + 1];
     const int i = blockIdx.x;
     const char* m = mcoarse + (long)i * ncoarse;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    if (threadIdx.x == 0) base = 0;
-    __syncthreads();
-    for (long c0 = 0; c0 < ncoarse; c0 += blockDim.x) {
-        const long e = c0 + threadIdx.x;
-        const bool f = e < ncoarse && m[e] != 0;
-        const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) wsum[warp] = __popc(bal);
-        __syncthreads();
-        int before = 0, total = 0;
-        for (int w = 0; w < nwarp; w++) {
-            const int v = wsum[w];
-            if (w < warp) before += v;
-            total += v;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool vec = (ncoarse & 15) == 0;
+    const int per = vec ? 16 : 1;  // bytes per thread per step
+    int base = 0;
+    for (long c0 = 0; c0 < ncoarse; c0 += (long)FE_THREADS * per) {
+        const long e0 = c0 + (long)threadIdx.x * per;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        int cnt = 0;
+        if (e0 < ncoarse) {
+            if (vec) {
+                v = *(const uint4*)(m + e0);
+                cnt = __popc(v.x) + __popc(v.y) + __popc(v.z) + __popc(v.w);
+            } else {
+                v.x = m[e0] != 0;
+                cnt = (int)v.x;
+            }
         }
-        if (f) {
-            const int r = base + before + __popc(bal & ((1u << lane) - 1u));
-            const int jc = (int)(e / ntr), itr = (int)(e - (long)jc * ntr);
-            fe[off[i] + r] = make_int4(i, r, ucompact[jc], itr);
-            ent[(long)i * stride + r] = make_int2(jc / npsi, itr);
+        // block-wide exclusive scan of the counts
+        int incl = cnt;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < FE_THREADS / 32 ? wsum[lane] : 0;
+            int x = w;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            if (lane < FE_THREADS / 32) wsum[lane] = x - w;  // exclusive warp offsets
+            if (lane == FE_THREADS / 32 - 1) wsum[FE_THREADS / 32] = x;  // block total
         }
         __syncthreads();
-        if (threadIdx.x == 0) base += total;
+        if (cnt) {
+            int r = base + wsum[warp] + incl - cnt;
+            const unsigned words[4] = {v.x, v.y, v.z, v.w};
+            for (int b = 0; b < per; b++) {
+                if (!((words[b >> 2] >> (8 * (b & 3))) & 0xFF)) continue;
+                const long e = e0 + b;
+                const int jc = (int)(e / ntr), itr = (int)(e - (long)jc * ntr);
+                fe[off[i] + r] = make_int4(i, r, ucompact[jc], itr);
+                ent[(long)i * stride + r] = make_int2(jc / npsi, itr);
+                r++;
+            }
+        }
+        base += wsum[FE_THREADS / 32];
         __syncthreads();
     }
+}
+
+// The (particle, coarse translation) pairs the fine pass needs: flag[i *
+// ntr + itr] for every coarse-significant point.
+__global__ void fine_pair_flag_kernel(int E, int ntr, const int4* __restrict__ fe, int* __restrict__ flag) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < E) flag[fe[q].x * ntr + fe[q].w] = 1;
+}
+
+// pair index -> particle * ntr + coarse translation (pid = exclusive scan of the flags)
+__global__ void fine_pair_list_kernel(int n, const int* __restrict__ flag, const int* __restrict__ pid,
+                                      int* __restrict__ pair_of) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n && flag[q]) pair_of[pid[q]] = q;
+}
+
+// Fine-pass A operand of the needed (particle, coarse translation) pairs
+// only: rows pair * notr + t for the notr over-translations of the pair's
+// coarse translation (the rows shift_operand2_kernel would write at i * Tf +
+// itr * notr + t, same arithmetic, FP32), and S of each row.  One CTA per
+// pair slot; slots beyond the number of pairs (npairs[0]) return.
+template <int NT>
+__global__ void __launch_bounds__(NT)
+    fine_pair_operand_kernel(const int* __restrict__ npairs, const int* __restrict__ pair_of, int ntr, int notr, int F,
+                             int Kact, int Kp, const double2* __restrict__ Fimg, const double* __restrict__ lctf,
+                             const double* __restrict__ Minv, int apply_ctf, const int* __restrict__ act,
+                             const unsigned short* __restrict__ pidx, const double2* __restrict__ tab,
+                             float* __restrict__ A, float* __restrict__ S) {
+    const int p = blockIdx.x;
+    if (p >= npairs[0]) return;
+    __shared__ float2 stab[5000];
+    __shared__ double red[32];
+    const int q = pair_of[p], i = q / ntr, itr = q - i * ntr;
+    for (int k = threadIdx.x; k < 5000; k += NT) stab[k] = make_float2((float)tab[k].x, (float)tab[k].y);
+    const double2* X = Fimg + (long)i * F;
+    const double* M = Minv + (long)i * F;
+    const double* C = lctf + (long)i * F;
+    double s = 0.0;
+    for (int n = threadIdx.x; n < F; n += NT) {
+        const double2 v = X[n];
+        s += M[n] * (v.x * v.x + v.y * v.y);
+    }
+    s = block_reduce_sum(s, red);
+    for (int a = threadIdx.x; a < Kp / 2; a += NT) {
+        float2 xw = make_float2(0.f, 0.f);
+        if (a < Kact) {
+            const int n = act[a];
+            const double w = apply_ctf ? M[n] * C[n] : M[n];
+            xw = make_float2((float)(w * X[n].x), (float)(w * X[n].y));
+        }
+        for (int t = 0; t < notr; t++) {
+            float fr = 0.f, fi = 0.f;
+            if (a < Kact) {
+                const unsigned short pi = pidx[(long)(itr * notr + t) * Kact + a];
+                if (pi == 0xFFFF) {
+                    fr = xw.x;
+                    fi = xw.y;
+                } else {
+                    const float2 cs = stab[pi & 0x7FFF];
+                    const float sn = (pi & 0x8000) ? -cs.y : cs.y;
+                    fr = cs.x * xw.x - sn * xw.y;
+                    fi = cs.x * xw.y + sn * xw.x;
+                }
+            }
+            *(float2*)(A + ((long)p * notr + t) * Kp + 2 * a) = make_float2(fr, fi);
+        }
+    }
+    if (threadIdx.x < notr) S[(long)p * notr + threadIdx.x] = (float)s;
 }
 
 // Fine-pass squared differences of one coarse-significant point: nor fine
 // orientations (u * nor + o) x notr fine translations (itr * notr + t),
 // written at [i][r * nor * notr + o * notr + t] (the ihidden order
 // itrans -> over_rot -> over_trans of the reference's lists,
-// src/map3d_optimizer.cpp:1340-1358).  diff2 = (N - 2 C + S + Xi2) / 2 with
+// src/map3d_optimizer.cpp:1340-1358).  A holds the shifted images of the
+// needed (particle, coarse translation) pairs only, pair pid[i * ntr + itr].  diff2 = (N - 2 C + S + Xi2) / 2 with
 // the cross term C = <A_(i,t), B_(u,o)>, the norm term N = <W2_i, Q_(u,o)>
 // (FP32 products, FP64 block sums) and the per-particle minimum folded in.
 template <int NT, int NOR, int NOTR>
 __global__ void __launch_bounds__(NT)
-    fine_diff2_kernel(int Tf, int Kp, int Kq, const int4* __restrict__ fe, const float* __restrict__ A,
-                      const float* __restrict__ B, const float* __restrict__ W2, const float* __restrict__ Q,
-                      const float* __restrict__ S, const double* __restrict__ xi2, long Xf, float* __restrict__ diff2,
-                      unsigned* __restrict__ rowmin) {
+    fine_diff2_kernel(int ntr, int Kp, int Kq, const int4* __restrict__ fe, const int* __restrict__ pid,
+                      const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ W2,
+                      const float* __restrict__ Q, const float* __restrict__ S, const double* __restrict__ xi2, long Xf,
+                      float* __restrict__ diff2, unsigned* __restrict__ rowmin) {
     constexpr int NH = NOR * NOTR;
     static_assert(NH == 32, "one warp holds the 32 sub-hypotheses of a point");
     __shared__ double red[NT / 32][NH + NOR];
     const int4 en = fe[blockIdx.x];
     const int i = en.x, r = en.y, u = en.z, itr = en.w;
+    const long arow = (long)pid[i * ntr + itr] * NOTR;  // the pair's rows of the compacted A operand
     const float2* Ar[NOTR];
     const float2* Br[NOR];
     const float* Qr[NOR];
 #pragma unroll
-    for (int t = 0; t < NOTR; t++) Ar[t] = (const float2*)(A + ((long)i * Tf + itr * NOTR + t) * Kp);
+    for (int t = 0; t < NOTR; t++) Ar[t] = (const float2*)(A + (arow + t) * Kp);
 #pragma unroll
     for (int o = 0; o < NOR; o++) {
         Br[o] = (const float2*)(B + ((long)u * NOR + o) * Kp);
@@ -227,7 +343,7 @@ __global__ void __launch_bounds__(NT)
             cs += red[w][h];
             ns += red[w][NH + o];
         }
-        const float v = (float)(0.5 * (ns - 2.0 * cs + (double)S[(long)i * Tf + itr * NOTR + t] + xi2[i]));
+        const float v = (float)(0.5 * (ns - 2.0 * cs + (double)S[arow + t] + xi2[i]));
         diff2[(long)i * Xf + (long)r * NH + h] = v;
         float m = v;
         for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));

@@ -487,6 +487,24 @@ __device__ __forceinline__ bool hyp_prior(long e, int i, const PostLayout& L, co
 }
 
 template <typename TVal>
+__device__ TVal block_reduce_max(TVal v, TVal* sh) {
+    for (int off = 16; off > 0; off >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, off));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    TVal r = v;
+    if (threadIdx.x < 32) {
+        r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : sh[0];
+        for (int off = 16; off > 0; off >>= 1) r = max(r, __shfl_down_sync(0xffffffffu, r, off));
+        if (threadIdx.x == 0) sh[0] = r;
+    }
+    __syncthreads();
+    r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+template <typename TVal>
 __device__ TVal block_reduce_sum(TVal v, TVal* sh) {
     for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
     __syncthreads();

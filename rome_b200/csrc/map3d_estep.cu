@@ -215,6 +215,10 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         std::vector<double> hpart((size_t)P * 8);
         std::vector<int> hparti((size_t)P * 8);
 
+        // the coarse pass's significant list (coarse index per entry) outlives the pass
+        int nsig0 = 0;
+        const SigEntry* dList0 = nullptr;
+
         // ================= pass 0: coarse, dense =================
         {
             std::vector<int> act, actidx;
@@ -393,6 +397,8 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                 ROME_CUDA(cudaMemcpyAsync(out->post_coarse, dMarg, sizeof(double) * P * J, cudaMemcpyDeviceToHost,
                                           st));
             }
+            nsig0 = nsig;
+            dList0 = dList;
             ROME_CUDA(cudaMemsetAsync(dMcoarse, 0, (size_t)P * ncoarse, st));
             if (nsig > 0) {
                 mcoarse_from_list_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, X, dList, dMcoarse);
@@ -437,9 +443,12 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
 
         // orientations some particle needs (getReferenceAllOrientations, :956-985)
         char* dRotSig = ctx->ws[S_ROTSIG].as<char>((size_t)Jc);
-        rot_sig_kernel<<<(Jc + 255) / 256, 256, 0, st>>>(Jc, P, ntr, ncoarse, dMcoarse, dRotSig);
-        ROME_CHECK_LAUNCH();
-        prof.launched(ROME_PHASE_PROJECT);
+        ROME_CUDA(cudaMemsetAsync(dRotSig, 0, (size_t)Jc, st));
+        if (nsig0 > 0) {
+            rotsig_from_list_kernel<<<(nsig0 + 255) / 256, 256, 0, st>>>(nsig0, ntr, dList0, dRotSig);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_PROJECT);
+        }
         std::vector<char> hrs(Jc);
         ROME_CUDA(cudaMemcpyAsync(hrs.data(), dRotSig, Jc, cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
@@ -503,22 +512,15 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         prof.launched(ROME_PHASE_PROJECT);
         prof.end(ROME_PHASE_PROJECT);
 
-        const long Mf = (long)P * Tf;
-        float* dA = ctx->ws[S_A].as<float>((size_t)Mf * g.Kp);
-        float* dS = ctx->ws[S_S].as<float>((size_t)Mf);
         float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
         unsigned short* dPidx = ctx->ws[S_PIDX].as<unsigned short>((size_t)Tf * g.Kact);
         prof.begin(ROME_PHASE_SHIFT);
         phase_index_kernel<<<(unsigned)(((long)Tf * g.Kact + 255) / 256), 256, 0, st>>>(
             Tf, g.Kact, g.csF, cur, dAct, dShift, ctx->shift_sampling, dPidx);
         ROME_CHECK_LAUNCH();
-        shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, Tf, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
-                                                       apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA, dS,
-                                                       ROME_PREC_FP32);
-        ROME_CHECK_LAUNCH();
         w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
         ROME_CHECK_LAUNCH();
-        prof.launched(ROME_PHASE_SHIFT, 3);
+        prof.launched(ROME_PHASE_SHIFT, 2);
         prof.end(ROME_PHASE_SHIFT);
 
         // compaction of the coarse-significant points
@@ -540,9 +542,35 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         int4* dFe = ctx->ws[S_FE].as<int4>((size_t)std::max(E, 1));
         int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)P * stride);
         ROME_CUDA(cudaMemsetAsync(dEnt, 0xFF, sizeof(int2) * (size_t)P * stride, st));
-        fine_entries_kernel<<<P, 1024, 0, st>>>(ncoarse, ntr, npsi, dMcoarse, dOffP, dUcomp, stride, dFe, dEnt);
+        fine_entries_kernel<<<P, FE_THREADS, 0, st>>>(ncoarse, ntr, npsi, dMcoarse, dOffP, dUcomp, stride, dFe, dEnt);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_PROJECT, 2);
+
+        // shifted images of the (particle, coarse translation) pairs the points need, NOTR rows each
+        const int NPT = P * ntr;
+        int* dPairFlag = ctx->ws[S_PAIRS].as<int>((size_t)3 * NPT + 2);
+        int* dPairId = dPairFlag + NPT;       // exclusive scan of the flags, [NPT + 1] (last: the count)
+        int* dPairOf = dPairId + NPT + 1;     // pair -> particle * ntr + coarse translation
+        const int pair_cap = std::max(1, std::min(E, NPT));
+        float* dA = ctx->ws[S_A].as<float>((size_t)pair_cap * NOTR * g.Kp);
+        float* dS = ctx->ws[S_S].as<float>((size_t)pair_cap * NOTR);
+        prof.begin(ROME_PHASE_SHIFT);
+        ROME_CUDA(cudaMemsetAsync(dPairFlag, 0, sizeof(int) * NPT, st));
+        if (E > 0) {
+            fine_pair_flag_kernel<<<(E + 255) / 256, 256, 0, st>>>(E, ntr, dFe, dPairFlag);
+            ROME_CHECK_LAUNCH();
+        }
+        exclusive_scan_kernel<<<1, 1024, 0, st>>>(NPT, dPairFlag, dPairId);
+        ROME_CHECK_LAUNCH();
+        fine_pair_list_kernel<<<(NPT + 255) / 256, 256, 0, st>>>(NPT, dPairFlag, dPairId, dPairOf);
+        ROME_CHECK_LAUNCH();
+        fine_pair_operand_kernel<256><<<pair_cap, 256, 0, st>>>(dPairId + NPT, dPairOf, ntr, NOTR, g.F, g.Kact, g.Kp,
+                                                                dFimg, dLctf, dMinv, apply_ctf ? 1 : 0, dAct, dPidx,
+                                                                ctx->d_shift_tab, dA, dS);
+        ROME_CHECK_LAUNCH();
+        prof.launched(ROME_PHASE_SHIFT, 4);
+        prof.add_bytes(ROME_PHASE_SHIFT, 4.0 * pair_cap * NOTR * g.Kp);
+        prof.end(ROME_PHASE_SHIFT);
 
         // fine squared differences, ragged rows [P][stride * 32] padded with +inf
         const long Xf = (long)stride * NH;
@@ -553,8 +581,8 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         ROME_CHECK_LAUNCH();
         ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
         if (E > 0) {
-            fine_diff2_kernel<128, 8, 4><<<E, 128, 0, st>>>(Tf, g.Kp, g.Kq, dFe, dA, dB, dW2, dQ, dS, dXi2, Xf, dDiff2,
-                                                          dRowMin);
+            fine_diff2_kernel<128, 8, 4><<<E, 128, 0, st>>>(ntr, g.Kp, g.Kq, dFe, dPairId, dA, dB, dW2, dQ, dS, dXi2,
+                                                          Xf, dDiff2, dRowMin);
             ROME_CHECK_LAUNCH();
         }
         prof.launched(ROME_PHASE_CROSS_GEMM, 2);

@@ -116,32 +116,110 @@ __global__ void __launch_bounds__(SEL2_THREADS)
             }
         }
     } else if (mode == 0) {
-        // orientation-major sweep: one division per orientation, the loop-order
-        // index only on ties (argmax of the reference's loop, :1140-1146)
+        // dense rows [J][T]: the warp packs G = 32 / T whole orientations when T < 32 (lanes over the
+        // G * T contiguous entries), else one orientation with lanes over its translations; the
+        // orientation's class / direction indices advance incrementally (no division per entry).
+        // Weights below 2^-60 of the smallest possible maximum weight are not summed (see skip_cut).
         const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
-        const int J = (int)(X / L.T), nrot = L.npsi * L.nor;
-        const int tsh = L.notr == 1 ? 0 : (L.notr == 4 ? 2 : 31);
-        for (int j = warp; j < J; j += nwarp) {
-            const int k = j / nrot;
-            const double pdk = pdir[k];
-            const double* pok = po + (k / L.ndir) * L.ntr;
-            for (int t = lane; t < L.T; t += 32) {
-                const long e = (long)j * L.T + t;
-                const int itr = tsh < 31 ? (t >> tsh) : t / L.notr;
-                float dv = d[e];
-                if (dv < INFINITY) maxpd = fmax(maxpd, pdk * pok[itr]);
-                double w = hyp_weight(dv, mn, pdk, pok[itr]);
-                if (wout) wout[(long)i * X + e] = w;
-                sum += w;
-                if (w >= maxw && w > DBL_MIN) {
-                    int kk, it2;
-                    long lo;
-                    decode_e(e, L, kk, it2, lo);
-                    if (w > maxw || lo < best_lo) {
-                        maxw = w;
-                        best_lo = lo;
-                        best_e = e;
+        const int J = (int)(X / L.T), nrot = L.npsi * L.nor, Kd = J / nrot;
+        const int G = L.T < 32 ? 32 / L.T : 1;
+        const bool active = L.T < 32 ? lane < G * L.T : true;
+        const int jj = L.T < 32 ? lane / L.T : 0;
+        const int t0 = L.T < 32 ? lane - jj * L.T : lane;
+        const int tstep = L.T < 32 ? L.T : 32;
+        // per-particle bounds of the prior pdf_orientation * pdf_offset
+        double pmax = 0.0, pmin = INFINITY, omax = 0.0, omin = INFINITY;
+        for (int q = threadIdx.x; q < Kd; q += blockDim.x) {
+            const double v = pdir[q];
+            pmax = fmax(pmax, v);
+            if (v > 0.0) pmin = fmin(pmin, v);
+        }
+        for (int q = threadIdx.x; q < L.K * L.ntr; q += blockDim.x) {
+            const double v = po[q];
+            omax = fmax(omax, v);
+            if (v > 0.0) omin = fmin(omin, v);
+        }
+        pmax = block_reduce_max(pmax, red);
+        omax = block_reduce_max(omax, red);
+        pmin = -block_reduce_max(-pmin, red);
+        omin = -block_reduce_max(-omin, red);
+        const double minpos = pmin * omin;
+        // A weight pd * po * exp(-(d - mn)) with d - mn > skip_cut is below minpos * 2^-60; the entry
+        // at the minimum has weight pd * po >= minpos whenever its prior is positive, so the skipped
+        // weights (at most X of them) change the sum by less than X * 2^-60 of itself (~2e-13 at X =
+        // 2.4e5).  The sum is checked against minpos below and recomputed in full if that premise fails.
+        double skip_cut = (minpos > 0.0 && minpos < INFINITY) ? 41.6 + log(pmax * omax / minpos) : INFINITY;
+        for (int pass = 0; pass < 2; pass++) {
+            sum = 0.0;
+            maxw = DBL_MIN;
+            maxpd = 0.0;
+            best_lo = LONG_MAX;
+            best_e = 0;
+            if (active) {
+                // lane state: orientation j, its k = j / nrot (remainder rk), class c = k / ndir (remainder rc)
+                int j = warp * G + jj;
+                int k = j / nrot, rk = j - k * nrot;
+                int c = k / L.ndir, rc = k - c * L.ndir;
+                const int S = nwarp * G;
+                for (; j < J; j += S) {
+                    const double pdk = pdir[k];
+                    const double* pok = po + c * L.ntr;
+                    for (int t = t0; t < L.T; t += tstep) {
+                        const long e = (long)j * L.T + t;
+                        const float dv = d[e];
+                        if (!(dv < INFINITY)) {
+                            if (wout) wout[(long)i * X + e] = 0.0;
+                            continue;
+                        }
+                        const int itr = L.notr == 1 ? t : t / L.notr;
+                        const double pp = pdk * pok[itr];
+                        maxpd = fmax(maxpd, pp);
+                        const double diff = (double)dv - mn;
+                        if (diff > skip_cut) continue;  // written after the sweep when wout is wanted
+                        if (diff > 700.) {
+                            if (wout) wout[(long)i * X + e] = 0.0;
+                            continue;
+                        }
+                        const double w = pp * exp(-diff);
+                        if (wout) wout[(long)i * X + e] = w;
+                        sum += w;
+                        if (w >= maxw && w > DBL_MIN) {
+                            int kk, it2;
+                            long lo;
+                            decode_e(e, L, kk, it2, lo);
+                            if (w > maxw || lo < best_lo) {
+                                maxw = w;
+                                best_lo = lo;
+                                best_e = e;
+                            }
+                        }
                     }
+                    rk += S;
+                    while (rk >= nrot) {
+                        rk -= nrot;
+                        k++;
+                        if (++rc == L.ndir) {
+                            rc = 0;
+                            c++;
+                        }
+                    }
+                }
+            }
+            if (skip_cut == INFINITY) break;
+            // premise of the skip: the sum is at least the smallest positive prior
+            const double tot = block_reduce_sum(sum, red);
+            if (tot >= minpos * (1.0 - 1e-12)) break;
+            skip_cut = INFINITY;
+        }
+        if (wout && skip_cut < INFINITY) {
+            // skipped entries still get their (zero or negligible) weights written for the caller
+            for (long e = threadIdx.x; e < X; e += blockDim.x) {
+                const float dv = d[e];
+                if (dv < INFINITY && (double)dv - mn > skip_cut) {
+                    double pd, pof;
+                    long lo;
+                    hyp_prior(e, i, L, pdir, po, pd, pof, lo);
+                    wout[(long)i * X + e] = hyp_weight(dv, mn, pd, pof);
                 }
             }
         }
