@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 
 namespace rome {
 
@@ -17,6 +18,10 @@ __device__ __forceinline__ float key_float(unsigned k) {
     return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
 }
 
+// Epilogues are called per element (operator()) by the CUDA-core contraction
+// and per 16 consecutive columns of one row (row() once per row and tile,
+// then chunk16()) by the tensor-core one, which reads 16 columns at a time
+// out of TMEM; chunk16 returns the minimum of the values it stored.
 struct StoreEpi {
     float* out;
     int ld;
@@ -25,6 +30,17 @@ struct StoreEpi {
         return v;
     }
     __device__ __forceinline__ void finish_row(int, float) const {}
+    struct Row {
+        int m;
+    };
+    __device__ __forceinline__ Row row(int m) const { return Row{m}; }
+    __device__ __forceinline__ float chunk16(const Row& r, int n, const float (&v)[16], int nvalid) const {
+        float mn = INFINITY;
+#pragma unroll
+        for (int q = 0; q < 16; q++)
+            if (q < nvalid) mn = fminf(mn, (*this)(r.m, n + q, v[q]));
+        return mn;
+    }
 };
 
 // out[m][n] = v + bias[n / group] (a per-class bias over `group` columns)
@@ -39,6 +55,17 @@ struct BiasStoreEpi {
         return v;
     }
     __device__ __forceinline__ void finish_row(int, float) const {}
+    struct Row {
+        int m;
+    };
+    __device__ __forceinline__ Row row(int m) const { return Row{m}; }
+    __device__ __forceinline__ float chunk16(const Row& r, int n, const float (&v)[16], int nvalid) const {
+        float mn = INFINITY;
+#pragma unroll
+        for (int q = 0; q < 16; q++)
+            if (q < nvalid) mn = fminf(mn, (*this)(r.m, n + q, v[q]));
+        return mn;
+    }
 };
 
 // diff2 epilogue of the cross-term GEMM (rows m = particle*T + translation,
@@ -71,6 +98,51 @@ struct Diff2Epi {
     }
     __device__ __forceinline__ void finish_row(int m, float v) const {
         if (rowmin && v < INFINITY) atomicMin(&rowmin[m / T], float_key(v));
+    }
+    // per-row constants of a tile row: output base, S[m] + Xi2[i], the
+    // particle's norm row and Mcoarse row
+    struct Row {
+        long out;
+        double rc;
+        const float* nrm;
+        const char* mc;
+    };
+    __device__ __forceinline__ Row row(int m) const {
+        const int i = m / T, t = m - i * T;
+        return Row{(long)i * X + t, (double)S[m] + xi2[i], norm + (long)i * J,
+                   mcoarse ? mcoarse + (long)i * ncoarse + t / notr : nullptr};
+    }
+    __device__ __forceinline__ float chunk16(const Row& r, int n, const float (&v)[16], int nvalid) const {
+        float nv[16];
+        int jv[16];
+        if (nvalid == 16 && (((uintptr_t)(r.nrm + n) | (uintptr_t)(jvalid + n)) & 15) == 0) {
+            // 16-byte loads (when both addresses are 16-byte aligned): the row's norm terms and the
+            // column validity
+#pragma unroll
+            for (int q = 0; q < 16; q += 4) {
+                const float4 a = *(const float4*)(r.nrm + n + q);
+                const int4 b = *(const int4*)(jvalid + n + q);
+                nv[q] = a.x, nv[q + 1] = a.y, nv[q + 2] = a.z, nv[q + 3] = a.w;
+                jv[q] = b.x, jv[q + 1] = b.y, jv[q + 2] = b.z, jv[q + 3] = b.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                nv[q] = q < nvalid ? r.nrm[n + q] : 0.f;
+                jv[q] = q < nvalid ? jvalid[n + q] : 0;
+            }
+        }
+        float mn = INFINITY;
+#pragma unroll
+        for (int q = 0; q < 16; q++) {
+            if (q >= nvalid) break;
+            bool ok = jv[q] != 0;
+            if (ok && r.mc) ok = r.mc[(long)((n + q) / nor) * ntr] != 0;
+            const float val = ok ? (float)(0.5 * ((double)nv[q] - 2.0 * (double)v[q] + r.rc)) : INFINITY;
+            diff2[r.out + (long)(n + q) * T] = val;
+            mn = fminf(mn, val);
+        }
+        return mn;
     }
 };
 

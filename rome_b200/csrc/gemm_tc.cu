@@ -13,11 +13,11 @@
 //                     K block) into one of two TMEM accumulators (2 x BN
 //                     columns); tcgen05.commit frees a ring stage and, after
 //                     a tile's last k block, hands the accumulator over
-//   warps 2-9       : epilogue, tcgen05.ld 32x32b (warp w reads TMEM lanes
-//                     32(w%4)..+31 = rows of the tile; warps 2-5 the first
-//                     half of the columns, 6-9 the second), then frees the
-//                     accumulator, so tile i's epilogue runs while tile
-//                     i+1's MMAs fill the other accumulator.
+//   warps 2-17      : epilogue, tcgen05.ld 32x32b (warp w reads TMEM lanes
+//                     32(w%4)..+31 = rows of the tile; the four warps of a
+//                     lane quarter take a quarter of the columns each), then
+//                     free the accumulator, so tile i's epilogue runs while
+//                     tile i+1's MMAs fill the other accumulator.
 // Split precision (ROME_PREC_BF16X3) loads hi and lo planes of both operands
 // and issues hi*hi + hi*lo + lo*hi into the same accumulator.
 //
@@ -52,7 +52,7 @@ struct TcSmem {
     static constexpr int TOTAL = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
 };
 
-constexpr int kEpiWarps = 8;
+constexpr int kEpiWarps = 16;
 constexpr int kThreads = 64 + 32 * kEpiWarps;
 constexpr int GROUP_M = 8;
 
@@ -196,8 +196,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else {
         // ---------------- epilogue ----------------
         const int q = warp & 3;                  // TMEM lane quarter this warp may read
-        const int half = (warp - 2) >> 2;        // column half
-        const int c_lo = half * (BN / 2), c_hi = c_lo + BN / 2;
+        constexpr int kParts = kEpiWarps / 4;    // warps per lane quarter, each with 1/kParts of the columns
+        constexpr int kCols = BN / kParts;       // a multiple of 16
+        static_assert(kCols % 16 == 0, "column share of an epilogue warp");
+        const int part = (warp - 2) >> 2;
+        const int c_lo = part * kCols, c_hi = c_lo + kCols;
         int lt = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, lt++) {
             const int b = lt & 1;
@@ -212,17 +215,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int row = tm * BM + q * 32 + lane, n0 = tn * BN;
             const uint32_t lane_base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN);
             float rmin = INFINITY;
+            const typename Epi::Row R = epi.row(row < M ? row : M - 1);
 #pragma unroll 1
             for (int c = c_lo; c < c_hi; c += 16) {
                 float v[16];
                 tmem_ld16(lane_base + c, v);
-                if (row < M) {
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        const int n = n0 + c + k;
-                        if (n < N) rmin = fminf(rmin, epi(row, n, v[k]));
-                    }
-                }
+                if (row < M && n0 + c < N) rmin = fminf(rmin, epi.chunk16(R, n0 + c, v, min(16, N - (n0 + c))));
             }
             if (row < M) epi.finish_row(row, rmin);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

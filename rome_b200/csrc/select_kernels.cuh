@@ -20,6 +20,8 @@
 // updateOtherParams and backProjection.
 #pragma once
 
+#include <cstdint>
+
 #include "estep_kernels.cuh"
 
 namespace rome {
@@ -161,39 +163,37 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                 int k = j / nrot, rk = j - k * nrot;
                 int c = k / L.ndir, rc = k - c * L.ndir;
                 const int S = nwarp * G;
-                for (; j < J; j += S) {
-                    const double pdk = pdir[k];
-                    const double* pok = po + c * L.ntr;
-                    for (int t = t0; t < L.T; t += tstep) {
-                        const long e = (long)j * L.T + t;
-                        const float dv = d[e];
-                        if (!(dv < INFINITY)) {
-                            if (wout) wout[(long)i * X + e] = 0.0;
-                            continue;
-                        }
-                        const int itr = L.notr == 1 ? t : t / L.notr;
-                        const double pp = pdk * pok[itr];
-                        maxpd = fmax(maxpd, pp);
-                        const double diff = (double)dv - mn;
-                        if (diff > skip_cut) continue;  // written after the sweep when wout is wanted
-                        if (diff > 700.) {
-                            if (wout) wout[(long)i * X + e] = 0.0;
-                            continue;
-                        }
-                        const double w = pp * exp(-diff);
-                        if (wout) wout[(long)i * X + e] = w;
-                        sum += w;
-                        if (w >= maxw && w > DBL_MIN) {
-                            int kk, it2;
-                            long lo;
-                            decode_e(e, L, kk, it2, lo);
-                            if (w > maxw || lo < best_lo) {
-                                maxw = w;
-                                best_lo = lo;
-                                best_e = e;
-                            }
+                // one entry (orientation jq of class index kq / class cq, translation t, value dv)
+                auto visit = [&](int jq, int kq, int cq, int t, float dv) {
+                    const long e = (long)jq * L.T + t;
+                    if (!(dv < INFINITY)) {
+                        if (wout) wout[(long)i * X + e] = 0.0;
+                        return;
+                    }
+                    const int itr = L.notr == 1 ? t : t / L.notr;
+                    const double pp = pdir[kq] * po[cq * L.ntr + itr];
+                    maxpd = fmax(maxpd, pp);
+                    const double diff = (double)dv - mn;
+                    if (diff > skip_cut) return;  // written after the sweep when wout is wanted
+                    if (diff > 700.) {
+                        if (wout) wout[(long)i * X + e] = 0.0;
+                        return;
+                    }
+                    const double w = pp * exp(-diff);
+                    if (wout) wout[(long)i * X + e] = w;
+                    sum += w;
+                    if (w >= maxw && w > DBL_MIN) {
+                        int kk, it2;
+                        long lo;
+                        decode_e(e, L, kk, it2, lo);
+                        if (w > maxw || lo < best_lo) {
+                            maxw = w;
+                            best_lo = lo;
+                            best_e = e;
                         }
                     }
+                };
+                auto advance = [&]() {
                     rk += S;
                     while (rk >= nrot) {
                         rk -= nrot;
@@ -202,6 +202,28 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                             rc = 0;
                             c++;
                         }
+                    }
+                };
+                if (L.T < 32) {
+                    // U loads in flight per lane before any of them is used
+                    constexpr int U = 4;
+                    for (; j < J; j += S * U) {
+                        float dvs[U];
+#pragma unroll
+                        for (int u = 0; u < U; u++) {
+                            const int ju = j + u * S;
+                            dvs[u] = ju < J ? d[(long)ju * L.T + t0] : INFINITY;
+                        }
+#pragma unroll
+                        for (int u = 0; u < U; u++) {
+                            if (j + u * S < J) visit(j + u * S, k, c, t0, dvs[u]);
+                            advance();
+                        }
+                    }
+                } else {
+                    for (; j < J; j += S) {
+                        for (int t = t0; t < L.T; t += tstep) visit(j, k, c, t, d[(long)j * L.T + t]);
+                        advance();
                     }
                 }
             }
@@ -280,24 +302,43 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                                                                 : INFINITY;
     __syncthreads();
     // ---- candidates w >= t0 ----
-    for (long e = threadIdx.x; e < X; e += blockDim.x) {
-        double w;
-        if (mode == 0) {
-            float dv = d[e];
-            if (!(dv < INFINITY) || (double)dv > dlim0) continue;
-            double pd, pof;
-            long lo;
-            if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) continue;
-            w = hyp_weight(dv, mn, pd, pof);
-        } else {
-            w = wg[e];
-        }
+    auto candidate = [&](long e, double w) {
         if (w > 0.0 && w >= t0) {
             int q = atomicAdd(&ncand, 1);
             if (q < SEL2_CAP) {
                 key[q] = w;
                 idx[q] = (int)e;
             }
+        }
+    };
+    auto diff2_candidate = [&](long e, float dv) {
+        if (!(dv < INFINITY) || (double)dv > dlim0) return;
+        double pd, pof;
+        long lo;
+        if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) return;
+        candidate(e, hyp_weight(dv, mn, pd, pof));
+    };
+    if (mode == 0 && (X & 3) == 0 && ((uintptr_t)d & 15) == 0) {
+        // 16-byte loads, two in flight per thread
+        const float4* d4 = (const float4*)d;
+        const long X4 = X / 4;
+        for (long q = threadIdx.x; q < X4; q += 2 * (long)blockDim.x) {
+            const long q2 = q + blockDim.x;
+            const float4 v0 = d4[q];
+            const float4 v1 = q2 < X4 ? d4[q2] : make_float4(INFINITY, INFINITY, INFINITY, INFINITY);
+            diff2_candidate(4 * q, v0.x);
+            diff2_candidate(4 * q + 1, v0.y);
+            diff2_candidate(4 * q + 2, v0.z);
+            diff2_candidate(4 * q + 3, v0.w);
+            diff2_candidate(4 * q2, v1.x);
+            diff2_candidate(4 * q2 + 1, v1.y);
+            diff2_candidate(4 * q2 + 2, v1.z);
+            diff2_candidate(4 * q2 + 3, v1.w);
+        }
+    } else {
+        for (long e = threadIdx.x; e < X; e += blockDim.x) {
+            if (mode == 0) diff2_candidate(e, d[e]);
+            else candidate(e, wg[e]);
         }
     }
     __syncthreads();
