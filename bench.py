@@ -202,6 +202,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
+    from rome_b200.distributed import MODEL_SUM_KEYS, allreduce_backprojectors, allreduce_model_sums
     from rome_b200.map2d import GpuContext
     from rome_b200.particles import h2d_bytes as prep_h2d_bytes
     from rome_b200.particles import pin_particles, prepared_pool, prepared_stream
@@ -259,18 +260,41 @@ def run_ours(args):
     host_raw = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
     items = list(zip(tmpls, host_raw))
 
+    exchange_bytes = [0]
+
+    def exchange(res):
+        """The iteration's one exchange step over ranks (MLModel::reduceData and
+        MAPModel::reduceData): the pools' weighted sums and every class's
+        back-projector summed over all ranks, the latter device-resident (NCCL)."""
+        if world == 1:
+            return
+        sums = {}
+        for r in res:
+            o = r[0] if isinstance(r, tuple) else r
+            for k in MODEL_SUM_KEYS:
+                if k in o:
+                    sums[k] = sums.get(k, 0) + np.asarray(o[k], np.float64)
+        red = allreduce_model_sums(sums, device=f"cuda:{local}")
+        exchange_bytes[0] = allreduce_backprojectors(ctx) + sum(int(np.asarray(v).nbytes) for v in red.values())
+
     def step_dev():
         if learned:
-            return learned_estep_pools(ctx, net, dev, args.topk, args.min_mass, workers=workers)
-        return [(ctx.map2d_estep_pool(q), None, None, None) for q in dev]
+            res = learned_estep_pools(ctx, net, dev, args.topk, args.min_mass, workers=workers)
+        else:
+            res = [(ctx.map2d_estep_pool(q), None, None, None) for q in dev]
+        exchange(res)
+        return res
 
     def step_e2e():
         # host (pinned) raw images copied in and prepared on the device (pool k + 1 while pool k computes),
         # E-step, results copied out
         stream = prepared_stream(prep_ctx, items, opts)
         if learned:
-            return learned_estep_pools(ctx, net, stream, args.topk, args.min_mass, workers=workers)
-        return [ctx.map2d_estep_pool(q) for q in stream]
+            res = learned_estep_pools(ctx, net, stream, args.topk, args.min_mass, workers=workers)
+        else:
+            res = [ctx.map2d_estep_pool(q) for q in stream]
+        exchange(res)
+        return res
 
     for _ in range(args.warmup):
         step_dev()
@@ -365,7 +389,10 @@ def run_ours(args):
                    "search": (f"learned proposals, top-{args.topk} network outputs -> {2 * args.topk} orientations; "
                               f"exhaustive where their probability mass < {args.min_mass}" if learned else "exhaustive"),
                    "inputs": "larger than L2 (no flush)",
-                   "host_threads": args.workers if learned else 1},
+                   "host_threads": args.workers if learned else 1,
+                   "exchange": ("per step: wsums and every class's back-projector all-reduced over the ranks on "
+                                f"the device (NCCL), {exchange_bytes[0]} bytes per rank" if world > 1 else
+                                "none (one rank)")},
         "e2e": {"value": round(e2e_value, 2), "unit": UNIT,
                 "from": "float32 images + metadata in page-locked host memory: copy, image preparation "
                         "(setFourierTransforms), E-step, results back",
@@ -665,6 +692,15 @@ def run_ours_3d(args):
     opts = prep_options(w)
     ctx = GpuContext(0, args.precision, profile=True)
     ctx.set_projectors(proj, pool.ori_size, r_max)
+    # one context per host thread: pools are dealt round-robin, so one context's host-side work (list sizes,
+    # result copies) overlaps the other's kernels; their back-projectors are added into ctx's after each step
+    lanes = [ctx]
+    for _ in range(max(0, args.workers - 1)):
+        c = GpuContext(0, args.precision, profile=True)
+        c.set_projectors(proj, pool.ori_size, r_max)
+        lanes.append(c)
+    from concurrent.futures import ThreadPoolExecutor
+    execs = [ThreadPoolExecutor(max_workers=1) for _ in lanes]
     prep_ctx = GpuContext(0, "fp32", profile=True)
     d_raw = torch.from_numpy(raw.images).cuda()
     dr = dataclasses.replace(raw, images=d_raw)
@@ -672,19 +708,27 @@ def run_ours_3d(args):
     del d_raw, dr
     host_raw = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
 
+    def run_lanes(pools):
+        futs = [execs[q % len(lanes)].submit(map3d_estep_pool, lanes[q % len(lanes)], sp.pool, dev=sp.dev)
+                for q, sp in enumerate(pools)]
+        res = [f.result() for f in futs]
+        for c in lanes[1:]:
+            ctx.add_backprojectors(c, clear=True)
+        return res
+
     def step():
-        return [map3d_estep_pool(ctx, sp.pool, dev=sp.dev) for sp in staged]
+        return run_lanes(staged)
 
     def step_e2e():
-        return [map3d_estep_pool(ctx, sp.pool, dev=sp.dev)
-                for sp in prepared_stream(prep_ctx, list(zip(tmpls, host_raw)), opts)]
+        return run_lanes(prepared_stream(prep_ctx, list(zip(tmpls, host_raw)), opts))
 
     for _ in range(args.warmup):
         step()
-    ctx.reset_timings()
+    for c in lanes:
+        c.reset_timings()
     with ClockSampler(0) as clk:
         ms, last = _timed(torch, step, args.steps)
-    timings = ctx.get_timings()
+    timings = merge_timings([c.get_timings() for c in lanes])
     step_e2e()
     e_ms, _ = _timed(torch, step_e2e, max(1, args.steps))
     cls = np.concatenate([r["cls"] for r in last]) - 1
@@ -729,7 +773,8 @@ def run_ours_3d(args):
         "config": {"workload": args.config, "particles": N, "image": w.ori_size, "coarse_size": pool.coarse_size,
                    "classes": w.n_classes, "directions": pool.nr_dir, "psi": pool.nr_psi,
                    "translations": pool.nr_trans, "oversampling": 1, "pool": args.pool, "precision": args.precision,
-                   "inputs": "larger than L2 (no flush)", "build_s": round(t_build, 1)},
+                   "inputs": "larger than L2 (no flush)", "host_threads": len(lanes),
+                   "build_s": round(t_build, 1)},
         "e2e": {"value": round(N / (e_ms / max(1, args.steps) / 1e3), 2), "unit": UNIT,
                 "from": "float32 images + metadata in page-locked host memory: copy, image preparation "
                         "(setFourierTransforms), E-step, results back",
@@ -745,8 +790,11 @@ def run_ours_3d(args):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w)
+    for e in execs:
+        e.shutdown(wait=True)
     prep_ctx.close()
-    ctx.close()
+    for c in lanes:
+        c.close()
     print(json.dumps(line), flush=True)
 
 

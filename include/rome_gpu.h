@@ -134,6 +134,20 @@ int rome_gpu_set_backprojector(RomeGpuCtx* ctx, int iclass, const double* data, 
  * (src/map_model.cpp:209-231). */
 int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int clear_src);
 
+/* Device-resident exchange of the back-projectors across ranks (the
+ * reference's MAPModel::reduceData, src/map_model.cpp:604-666, all-reduces
+ * or reduces them over MPI).  rome_gpu_backprojector_size gives the number
+ * of doubles of all classes' back-projectors, 3 * voxels * K: data as
+ * interleaved complex [K][voxels][2], then weight [K][voxels].
+ * rome_gpu_backprojector_device_copy copies them between the library and a
+ * caller's device buffer of that size on the context's device (to_library
+ * 0: library -> dev_buf, 1: dev_buf -> library), device to device, on
+ * `stream` (NULL: the context's stream) after the context's pending work;
+ * it returns when the copy is done.  A collective (NCCL all-reduce or
+ * per-class reduce) then runs on the buffer without any host copy. */
+int rome_gpu_backprojector_size(RomeGpuCtx* ctx, size_t* doubles);
+int rome_gpu_backprojector_device_copy(RomeGpuCtx* ctx, int to_library, void* dev_buf, void* stream);
+
 /* Back-projection of n particle images at known poses into class iclass's
  * 3D back-projector: the per-image loop of the reference's rome_reconstruct
  * (apps/rome_reconstruct.cpp:160-330).  Fimg_real/imag: [n][size][size/2+1]
@@ -489,6 +503,18 @@ int rome_gpu_select_significant_static(RomeGpuCtx* ctx, int n, long len, const d
  * ROME_ERR_ARG for pageable or unaligned buffers.  Asynchronous.
  * ------------------------------------------------------------------- */
 int rome_gpu_copy_from_host(RomeGpuCtx* ctx, void* dst, const void* host, size_t bytes, void* stream);
+
+/* ---------------------------------------------------------------------
+ * Failure-handling check of the bounded device waits.  No reference
+ * counterpart (the reference has no device code): every tensor-core kernel
+ * waits on mbarriers with a bound (2 s) after which it records a timeout in
+ * the context's error flag, drains and returns, and the entry point reports
+ * ROME_ERR_TIMEOUT with the context still usable.  This launches one wait
+ * on an mbarrier that nothing arrives on, bounded by limit_seconds (1e-4 to
+ * 2), so that callers and tests can see that path run out: it returns
+ * ROME_ERR_TIMEOUT and the measured wait in *waited_seconds (may be null).
+ * ------------------------------------------------------------------- */
+int rome_gpu_wait_selftest(RomeGpuCtx* ctx, double limit_seconds, double* waited_seconds);
 
 /* ---------------------------------------------------------------------
  * M-step reconstruction of one class from its accumulated backprojector.

@@ -192,6 +192,39 @@ extern "C" int rome_gpu_add_backprojectors(RomeGpuCtx* dst, RomeGpuCtx* src, int
     });
 }
 
+extern "C" int rome_gpu_backprojector_size(RomeGpuCtx* ctx, size_t* doubles) {
+    if (!ctx || !doubles) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->bp_data) fail(ROME_ERR_STATE, "no projectors/backprojectors set");
+        *doubles = (size_t)3 * ctx->vox * ctx->nr_classes;
+    });
+}
+
+extern "C" int rome_gpu_backprojector_device_copy(RomeGpuCtx* ctx, int to_library, void* dev_buf, void* stream) {
+    if (!ctx || !dev_buf) return ROME_ERR_ARG;
+    return guarded(ctx, [&] {
+        if (!ctx->bp_data) fail(ROME_ERR_STATE, "no projectors/backprojectors set");
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        cudaPointerAttributes at;
+        ROME_CUDA(cudaPointerGetAttributes(&at, dev_buf));
+        ROME_REQUIRE(at.type == cudaMemoryTypeDevice && at.device == ctx->device,
+                     "dev_buf is not device memory of device %d", ctx->device);
+        cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+        if (st != ctx->stream) ROME_CUDA(cudaStreamSynchronize(ctx->stream));  // the E-step's writes first
+        const size_t n = (size_t)ctx->vox * ctx->nr_classes;
+        double* data = (double*)dev_buf;
+        double* weight = data + 2 * n;
+        if (to_library) {
+            ROME_CUDA(cudaMemcpyAsync(ctx->bp_data, data, sizeof(double2) * n, cudaMemcpyDeviceToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(ctx->bp_weight, weight, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        } else {
+            ROME_CUDA(cudaMemcpyAsync(data, ctx->bp_data, sizeof(double2) * n, cudaMemcpyDeviceToDevice, st));
+            ROME_CUDA(cudaMemcpyAsync(weight, ctx->bp_weight, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+        }
+        ROME_CUDA(cudaStreamSynchronize(st));
+    });
+}
+
 extern "C" int rome_gpu_get_timings(RomeGpuCtx* ctx, RomeGpuTimings* out) {
     if (!ctx || !out) return ROME_ERR_ARG;
     for (int q = 0; q < ROME_PHASE_COUNT; q++) {

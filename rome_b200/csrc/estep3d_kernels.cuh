@@ -59,6 +59,30 @@ __device__ __forceinline__ double2 project3d_point(const double2* __restrict__ d
     return v;
 }
 
+// one projected coefficient into the requested outputs of project3d_kernel
+__device__ __forceinline__ void project3d_store(int j, int a, double2 v, int J, int Kact, int Kp, int Kq,
+                                                double2* __restrict__ P_out, float* __restrict__ Q,
+                                                void* __restrict__ Bop, int precision) {
+    if (P_out && a < Kact) P_out[(long)j * Kact + a] = v;
+    if (Q && a < Kq) Q[(long)j * Kq + a] = (float)(v.x * v.x + v.y * v.y);
+    if (!Bop) return;
+    const long o = (long)j * Kp + 2 * a;
+    if (precision == ROME_PREC_FP32) {
+        *(float2*)((float*)Bop + o) = make_float2((float)v.x, (float)v.y);
+    } else {
+        __nv_bfloat16* Bh = (__nv_bfloat16*)Bop;
+        __nv_bfloat16* Bl = Bh + (long)J * Kp;
+        const float fr = (float)v.x, fi = (float)v.y;
+        const __nv_bfloat16 hr = __float2bfloat16_rn(fr), hi = __float2bfloat16_rn(fi);
+        Bh[o] = hr;
+        Bh[o + 1] = hi;
+        if (precision == ROME_PREC_BF16X3) {
+            Bl[o] = __float2bfloat16_rn(fr - __bfloat162float(hr));
+            Bl[o + 1] = __float2bfloat16_rn(fi - __bfloat162float(hi));
+        }
+    }
+}
+
 // Projections of J orientations on the active pixels (r^2 <= my_r_max^2;
 // every other coefficient of the slice is zero).  jclass[j] selects the
 // class volume.  Writes, each optional: the FP64 projection [J][Kact], |P|^2
@@ -73,7 +97,7 @@ __global__ void project3d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
     const bool ok = jvalid == nullptr || jvalid[j] != 0;
     const Rot3 A = rot[j];
     const double2* data = proj_data + (long)jclass[j] * vox;
-    for (int a = threadIdx.x; a < Kp / 2; a += blockDim.x) {
+    auto point = [&](int a) {
         double2 v = make_double2(0.0, 0.0);
         if (ok && a < Kact) {
             const int n = act[a];
@@ -82,23 +106,18 @@ __global__ void project3d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
             const int y = row <= my_r_max ? row : row - cs;
             v = project3d_point(data, pad, padF, A, x, y);
         }
-        if (P_out && a < Kact) P_out[(long)j * Kact + a] = v;
-        if (Q && a < Kq) Q[(long)j * Kq + a] = (float)(v.x * v.x + v.y * v.y);
-        if (!Bop) continue;
-        const long o = (long)j * Kp + 2 * a;
-        if (precision == ROME_PREC_FP32) {
-            *(float2*)((float*)Bop + o) = make_float2((float)v.x, (float)v.y);
-        } else {
-            __nv_bfloat16* Bh = (__nv_bfloat16*)Bop;
-            __nv_bfloat16* Bl = Bh + (long)J * Kp;
-            const float fr = (float)v.x, fi = (float)v.y;
-            const __nv_bfloat16 hr = __float2bfloat16_rn(fr), hi = __float2bfloat16_rn(fi);
-            Bh[o] = hr;
-            Bh[o + 1] = hi;
-            if (precision == ROME_PREC_BF16X3) {
-                Bl[o] = __float2bfloat16_rn(fr - __bfloat162float(hr));
-                Bl[o + 1] = __float2bfloat16_rn(fi - __bfloat162float(hi));
-            }
+        return v;
+    };
+    // two pixels per thread per step: both pixels' 8 voxel loads are in flight before either is interpolated
+    for (int a0 = threadIdx.x; a0 < Kp / 2; a0 += 2 * blockDim.x) {
+        const int a1 = a0 + blockDim.x;
+        const double2 v0 = point(a0);
+        const double2 v1 = a1 < Kp / 2 ? point(a1) : make_double2(0.0, 0.0);
+        for (int h = 0; h < 2; h++) {
+            const int a = h ? a1 : a0;
+            if (a >= Kp / 2) break;
+            const double2 v = h ? v1 : v0;
+            project3d_store(j, a, v, J, Kact, Kp, Kq, P_out, Q, Bop, precision);
         }
     }
     if (Q)
@@ -111,7 +130,6 @@ __global__ void project3d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
 // getAllSquaredDifferencesFine, src/map3d_optimizer.cpp:1261-1372, visits
 // exp_Mcoarse_significant in exactly this order).
 
-// number of significant coarse points per particle
 // Significant coarse points per particle (Mcoarse_significant holds 0 or 1
 // per byte): 16 bytes per load when the rows are 16-byte aligned.
 __global__ void mcoarse_count_kernel(long ncoarse, const char* __restrict__ mcoarse, int* __restrict__ cnt) {

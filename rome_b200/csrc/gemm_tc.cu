@@ -488,7 +488,39 @@ void tc_check_error(cudaStream_t st, int* derr) {
     }
 }
 
+// A wait that runs out: one thread initialises an mbarrier that nothing
+// arrives on and waits for its first phase with the same bounded wait the
+// tensor-core kernels use, for limit_ns of wall time; the expiry is recorded
+// in the context's error flag exactly as a kernel's would be.
+__global__ void wait_selftest_kernel(uint64_t limit_ns, int* err, unsigned long long* waited_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    const uint64_t t0 = global_ns();
+    const bool ok = mbar_wait_ns(&bar, 0, limit_ns);
+    *waited_ns = global_ns() - t0;
+    if (!ok) atomicExch(err, 1);
+}
+
 }  // namespace rome
+
+extern "C" int rome_gpu_wait_selftest(RomeGpuCtx* ctx, double limit_seconds, double* waited_seconds) {
+    if (!ctx) return ROME_ERR_ARG;
+    return rome::guarded(ctx, [&] {
+        ROME_REQUIRE(limit_seconds >= 1e-4 && limit_seconds <= 2.0, "limit %g s outside [1e-4, 2]", limit_seconds);
+        ROME_CUDA(cudaSetDevice(ctx->device));
+        unsigned long long* dw = ctx->ws[rome::S_TMP2].as<unsigned long long>(1);
+        rome::wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>((uint64_t)(limit_seconds * 1e9), ctx->d_err, dw);
+        ROME_CHECK_LAUNCH();
+        unsigned long long h = 0;
+        ROME_CUDA(cudaMemcpyAsync(&h, dw, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        ROME_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (waited_seconds) *waited_seconds = (double)h * 1e-9;
+        ctx->total_launches += 1;
+        rome::tc_check_error(ctx->stream, ctx->d_err);
+    });
+}
 
 extern "C" size_t rome_gpu_tuning_report(char* buf, size_t len) {
     const std::string r = rome::tc_tuning_report();

@@ -38,9 +38,9 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// bounded wait on an mbarrier phase (iteration count and 2 s of wall time);
-// returns false on expiry
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// bounded wait on an mbarrier phase (iteration count and limit_ns of wall
+// time); returns false on expiry
+__device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uint64_t limit_ns) {
     uint32_t addr = smem_u32(bar);
     uint64_t t0 = 0;
     for (long it = 0; it < WAIT_LIMIT; it++) {
@@ -56,10 +56,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         if ((it & 1023) == 0) {
             uint64_t t = global_ns();
             if (it == 0) t0 = t;
-            else if (t - t0 > 2000000000ull) return false;
+            else if (t - t0 > limit_ns) return false;
         }
     }
     return false;
+}
+
+// the kernels' waits: 2 s of wall time
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    return mbar_wait_ns(bar, parity, 2000000000ull);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {

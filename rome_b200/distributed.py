@@ -9,7 +9,13 @@ Reference counterparts:
   (src/map_optimizer_base.h:373-409);
 * per-iteration reduction of the model sums: ``MLModel::reduceData``
   (src/ml_model.cpp:587-637) and of the back-projectors
-  ``MAPModel::reduceData`` (src/map_model.cpp:604-620).
+  ``MAPModel::reduceData`` (src/map_model.cpp:604-620, all-reduce; :621-666,
+  each class reduced onto the node that reconstructs it, then the new
+  references broadcast).
+
+The back-projectors never leave the device: the context copies them device
+to device into one flat FP64 buffer (``rome_gpu_backprojector_device_copy``),
+the collective runs on that buffer, and the result is copied back.
 """
 from __future__ import annotations
 
@@ -19,7 +25,7 @@ from typing import Dict, Tuple
 import numpy as np
 
 __all__ = ["divide_equally", "divide_equally_pool", "allreduce_model_sums", "allreduce_backprojectors",
-           "max_over_ranks"]
+           "reduce_backprojectors_by_class", "broadcast_class_maps", "owner_of_class", "max_over_ranks"]
 
 # the pool sums of one E-step call (rome_b200.map2d.alloc_outputs), added over ranks
 MODEL_SUM_KEYS = ("wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_prior_offsetx_class",
@@ -73,15 +79,66 @@ def allreduce_model_sums(sums: Dict[str, np.ndarray], device="cpu") -> Dict[str,
     return out
 
 
-def allreduce_backprojectors(ctx, nr_classes: int, device=None):
-    """Sum every class's back-projector (data and weight, FP64) over all
-    ranks in place in each rank's context: get_backprojector -> all-reduce
-    on the rank's GPU (NCCL) -> set_backprojector."""
-    dev = device if device is not None else f"cuda:{ctx.device}"
+def _bp_buffer(ctx):
+    """One flat FP64 tensor holding every class's back-projector, filled
+    device to device from the context (data [K][vox][2], then weight [K][vox])."""
+    import torch
+    buf = torch.empty(ctx.backprojector_doubles(), dtype=torch.float64, device=ctx.torch_device)
+    ctx.copy_backprojectors_to(buf)
+    return buf
+
+
+def allreduce_backprojectors(ctx, group=None) -> int:
+    """Every class's back-projector (data and weight, FP64) summed over all
+    ranks, in place in each rank's context (MAPModel::reduceData with the
+    all-reduce, src/map_model.cpp:604-620): one device-to-device copy into a
+    flat buffer, one all-reduce on it (NCCL on the rank's GPU), one copy
+    back; nothing crosses to the host.  Returns the bytes each rank
+    contributes."""
+    import torch.distributed as dist
+    buf = _bp_buffer(ctx)
+    dist.all_reduce(buf, op=dist.ReduceOp.SUM, group=group)
+    ctx.copy_backprojectors_from(buf)
+    return int(buf.numel()) * 8
+
+
+def owner_of_class(iclass: int, world: int) -> int:
+    """The rank that reconstructs class iclass when the back-projectors are
+    reduced by class: round-robin, as the reference deals classes to nodes
+    (src/map_model.cpp:621-666)."""
+    return iclass % world
+
+
+def reduce_backprojectors_by_class(ctx, nr_classes: int, group=None) -> list:
+    """Class-partitioned exchange (the reference's MAPModel::reduceData
+    without the all-reduce, src/map_model.cpp:621-666): class k's
+    back-projector is summed onto rank owner_of_class(k) only, on the
+    device, so that each rank reconstructs its own classes; the other ranks'
+    copies of class k are left as they were.  Returns the classes this rank
+    owns."""
+    import torch.distributed as dist
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    buf = _bp_buffer(ctx)
+    vox = buf.numel() // (3 * nr_classes)
+    data, weight = buf[:2 * vox * nr_classes], buf[2 * vox * nr_classes:]
     for k in range(nr_classes):
-        data, weight = ctx.get_backprojector(k)
-        red = _allreduce_np({"data": data, "weight": weight}, dev)
-        ctx.set_backprojector(k, red["data"], red["weight"])
+        dst = owner_of_class(k, world)
+        dist.reduce(data[2 * vox * k:2 * vox * (k + 1)], dst=dst, op=dist.ReduceOp.SUM, group=group)
+        dist.reduce(weight[vox * k:vox * (k + 1)], dst=dst, op=dist.ReduceOp.SUM, group=group)
+    ctx.copy_backprojectors_from(buf)
+    return [k for k in range(nr_classes) if owner_of_class(k, world) == rank]
+
+
+def broadcast_class_maps(maps, group=None):
+    """After a class-partitioned reconstruction: every rank receives every
+    class's map from its owner (the reference's broadcast of the new
+    references).  maps: one tensor per class, on the rank's device, the
+    owner's holding its reconstruction; all of them are overwritten in place."""
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    for k, m in enumerate(maps):
+        dist.broadcast(m, src=owner_of_class(k, world), group=group)
+    return maps
 
 
 def max_over_ranks(value: float, device="cpu") -> float:

@@ -327,6 +327,43 @@ class GpuContext:
             self.lib.rome_gpu_destroy(self.h)
             self.h = None
 
+    @property
+    def torch_device(self) -> str:
+        return f"cuda:{self.device}"
+
+    def backprojector_doubles(self) -> int:
+        """Doubles of all classes' back-projectors (data [K][vox][2], then weight [K][vox])."""
+        n = C.c_size_t()
+        self._check(self.lib.rome_gpu_backprojector_size(self.h, C.byref(n)))
+        return int(n.value)
+
+    def copy_backprojectors_to(self, buf) -> None:
+        """Library back-projectors -> a flat FP64 torch tensor on this device (device to device)."""
+        self._bp_copy(0, buf)
+
+    def copy_backprojectors_from(self, buf) -> None:
+        """A flat FP64 torch tensor on this device -> the library's back-projectors."""
+        self._bp_copy(1, buf)
+
+    def _bp_copy(self, to_library: int, buf) -> None:
+        import torch
+        assert buf.dtype == torch.float64 and buf.is_contiguous() and buf.numel() == self.backprojector_doubles()
+        assert buf.is_cuda and buf.device.index == self.device
+        stream = torch.cuda.current_stream(self.device)
+        self._check(self.lib.rome_gpu_backprojector_device_copy(self.h, to_library, C.c_void_p(buf.data_ptr()),
+                                                                C.c_void_p(stream.cuda_stream)))
+
+    def wait_selftest(self, limit_seconds: float) -> float:
+        """rome_gpu_wait_selftest: a bounded device wait that nothing ends;
+        raises RomeError(ROME_ERR_TIMEOUT) after about limit_seconds and
+        records the measured wait in self.last_wait_seconds."""
+        w = np.zeros(1)
+        self.last_wait_seconds = None
+        rc = self.lib.rome_gpu_wait_selftest(self.h, float(limit_seconds), abi.dptr(w))
+        self.last_wait_seconds = float(w[0])
+        self._check(rc)
+        return self.last_wait_seconds
+
     def __enter__(self):
         return self
 

@@ -226,3 +226,51 @@ def test_learned_pools_with_two_worker_threads_match_one():
             assert not c1.get_backprojector(k)[1].any()  # cleared after the merge
         for n in nets:
             n.close()
+
+
+def test_learned_bf16_with_fallback_agrees_with_plain_fp32():
+    """The metric's comparison at test size: learned proposals (top 16 of the
+    network's 108 (class, psi mod 180) outputs, i.e. 32 of 216 orientations)
+    + the restricted E-step on the tensor cores, with the exhaustive E-step as
+    the fallback for particles whose proposals carry less than 0.999 of the
+    network's probability, on held-out particles.  Gates on identical best
+    (class, psi, offset):
+    - learned + split BF16 (as accurate as FP32) against the plain FP32
+      exhaustive E-step: >= 99% (what the proposals lose);
+    - learned + BF16 against plain FP32 no worse than the exhaustive BF16
+      E-step itself (at 64^2 and SNR 0.1 BF16 rounding alone moves ~2% of
+      the poses, where the FP32 posterior's top hypotheses are nearly tied;
+      the restricted and the dense BF16 contractions round differently, so
+      they also differ from each other at those ties);
+    and the network, not the fallback, decides most particles."""
+    from rome_b200.proposal import learned_estep_pools
+    w = Map2dWorkload(n_particles=4400, ori_size=64, n_classes=6, n_blobs=20, psi_step=10, offset_range=3,
+                      offset_step=1, max_shift=2, pixel=2.0, snr=0.1, seed=29)
+    p, proj, r_max, _ = build_map2d(w)
+    K, npsi = p.nr_classes, p.nr_psi
+    train, test = subset(p, 0, 4000), subset(p, 4000, 4400)
+    with GpuContext(0, "fp32") as c32:
+        c32.set_projectors(proj, p.ori_size, r_max)
+        ref = c32.map2d_estep_pool(test)
+    with GpuContext(0, "bf16") as cb, GpuContext(0, "bf16x3") as cx:
+        cb.set_projectors(proj, p.ori_size, r_max)
+        cx.set_projectors(proj, p.ori_size, r_max)
+        tr = cb.map2d_estep_pool(train, marginals=True)
+        with ProposalNet(cb, K, npsi // 2, 16, r_lo=2.0, r_hi=24.0, seed=7) as net:
+            net.train(net.features(train), posterior_targets(tr["post_class_psi"], K, npsi), epochs=15, batch=128,
+                      lr=3e-3)
+            lb, props, mass, low = learned_estep_pools(cb, net, [test], 16, min_mass=0.999)[0]
+            lx = learned_estep_pools(cx, net, [test], 16, min_mass=0.999)[0][0]
+        ex = cb.map2d_estep_pool(test)
+
+    def agree(o, r):
+        return float(np.mean((o["cls"] == r["cls"]) & (o["psi"] == r["psi"]) & (o["xoff"] == r["xoff"])
+                             & (o["yoff"] == r["yoff"])))
+
+    print(f"{props.shape[1]} of {K * npsi} orientations searched, fallback {len(low) / test.nr_images:.3f}; pose "
+          f"agreement: learned BF16 vs exhaustive BF16 {agree(lb, ex):.4f}, learned split BF16 vs plain FP32 "
+          f"{agree(lx, ref):.4f}, learned BF16 vs plain FP32 {agree(lb, ref):.4f}, exhaustive BF16 vs plain FP32 "
+          f"{agree(ex, ref):.4f}")
+    assert agree(lx, ref) >= 0.99
+    assert agree(lb, ref) >= agree(ex, ref) - 0.005
+    assert len(low) <= 0.5 * test.nr_images
