@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=15)
     ap.add_argument("--workers", type=int, default=2,
                     help="host threads, each with its own context, working on alternate pools (learned mode)")
+    ap.add_argument("--snr-scale", type=float, default=1.0,
+                    help="3D workloads: multiply the configured signal-to-noise ratios (calibration runs)")
     ap.add_argument("--min-mass", type=float, default=0.995,
                     help="particles whose top-k proposals hold less network probability are searched exhaustively")
     return ap.parse_args()
@@ -682,6 +684,9 @@ def run_ours_3d(args):
     w = CONFIGS[args.config]
     if args.particles:
         w = dataclasses.replace(w, n_particles=args.particles)
+    if args.snr_scale != 1.0:
+        w = dataclasses.replace(w, snr=w.snr * args.snr_scale, snr_range=None if w.snr_range is None else
+                                tuple(v * args.snr_scale for v in w.snr_range))
     t0 = time.perf_counter()
     pool, proj, r_max, truth = build_map3d(w)
     t_build = time.perf_counter() - t0
@@ -774,6 +779,7 @@ def run_ours_3d(args):
                    "classes": w.n_classes, "directions": pool.nr_dir, "psi": pool.nr_psi,
                    "translations": pool.nr_trans, "oversampling": 1, "pool": args.pool, "precision": args.precision,
                    "inputs": "larger than L2 (no flush)", "host_threads": len(lanes),
+                   "snr": w.snr, "snr_range": w.snr_range, "noisy_fraction": w.noisy_fraction,
                    "build_s": round(t_build, 1)},
         "e2e": {"value": round(N / (e_ms / max(1, args.steps) / 1e3), 2), "unit": UNIT,
                 "from": "float32 images + metadata in page-locked host memory: copy, image preparation "
@@ -782,6 +788,12 @@ def run_ours_3d(args):
                 "d2h_bytes_per_step": int(N * (11 * 8 + 4))},
         "class_agreement_vs_truth": round(float(np.mean(cls == truth["cls"])), 4),
         "nr_sign_mean": round(float(np.mean(np.concatenate([r["nr_sign"] for r in last]))), 1),
+        # the per-particle spread of the coarse significance (what the reference's
+        # Exp_Mweight_old::analysis records per pool, src/exp_mweight.cpp:95-160): coarse-significant
+        # points per particle, each refined by 32 fine hypotheses
+        "coarse_significant_per_particle": dict(zip(
+            ("min", "p10", "p50", "p90", "p99", "max"),
+            (float(v) for v in np.percentile(np.concatenate([r["nr_sign"] for r in last]), [0, 10, 50, 90, 99, 100])))),
         "judge": judge,
         "phases_ms_per_step": phases,
         "gpu_launches": int(timings["total_launches"]),

@@ -525,8 +525,8 @@ __global__ void __launch_bounds__(NT)
                      const int* __restrict__ jclass, const double2* __restrict__ Fnm, const double* __restrict__ Mctf2,
                      const double2* __restrict__ shifts, const double2* __restrict__ ph, const Rot3* __restrict__ rot,
                      int r_max, int pad, int padF, double2* __restrict__ bp_data, double* __restrict__ bp_weight,
-                     long vox) {
-    const int j = blockIdx.y;
+                     long vox, int j0) {
+    const int j = j0 + blockIdx.y;  // launched in chunks of at most 65,535 orientations (grid y limit)
     const int s0 = off[j], ns = off[j + 1] - s0;
     if (ns == 0) return;
     const int n0 = blockIdx.x * NT * PIX;

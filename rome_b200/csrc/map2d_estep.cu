@@ -535,6 +535,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         {
             const int NT = 256, PIX = 4;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
+            ROME_REQUIRE(P <= 65535, "pool of %d particles: at most 65,535", P);
             wsum_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
                 g.T, g.nrot, K, g.F, g.csF, cur, oriF, dList, dSeg, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
                 g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dCls + K,
@@ -571,9 +572,10 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
             }
             const int NT = 256, PIX = 4;
             int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
-            bp_list_kernel<NT, PIX><<<dim3(nsplit, g.J), NT, 0, st>>>(
-                g.T, g.nrot, g.F, g.csF, cur, dSorted, dOff, dFnm, dMctf2, dShift, dPh, dRot, ctx->r_max,
-                ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
+            for (int j0 = 0; j0 < g.J; j0 += 65535)  // grid y limit
+                bp_list_kernel<NT, PIX><<<dim3(nsplit, std::min(g.J - j0, 65535)), NT, 0, st>>>(
+                    g.T, g.nrot, g.F, g.csF, cur, dSorted, dOff, dFnm, dMctf2, dShift, dPh, dRot, ctx->r_max,
+                    ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox, j0);
             prof.launched(ROME_PHASE_BACKPROJECT);
             prof.end(ROME_PHASE_BACKPROJECT);
         }

@@ -460,6 +460,18 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             }
         const int nU = (int)uj.size(), Jf = nU * NOR;
         ROME_REQUIRE(nU > 0, "no significant coarse orientation");
+        {
+            // the fine projections of the pool live on the device together (FP64 slice, |P|^2 and operand
+            // rows per fine orientation): refuse pools whose union of significant orientations would not fit
+            std::vector<int> a2, ai2;
+            const Pass gf = active_pixels(cur, ctx->r_max, a2, ai2);
+            const double need = (double)nU * NOR * ((double)gf.Kact * 16 + (double)gf.Kq * 4 + (double)gf.Kp * 4);
+            size_t free_b = 0, total_b = 0;
+            ROME_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            if (need > 0.8 * (double)free_b)
+                fail(ROME_ERR_OOM, "fine pass: %d significant coarse orientations need %.1f GB of projections "
+                     "(%.1f GB free); use smaller pools", nU, need / 1e9, free_b / 1e9);
+        }
         int* dUcomp = upload3(ctx, S_TMP2, ucompact.data(), ucompact.size());
         std::vector<int> hjf((size_t)2 * Jf);  // jclass, jcd
         std::vector<Rot3> hrotf(Jf);
@@ -683,6 +695,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         const int NT = 256, PIX = 8;
         const int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
         prof.begin(ROME_PHASE_WSUM);
+        ROME_REQUIRE(P <= 65535, "pool of %d particles: at most 65,535", P);
         wsum3d_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
             Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
             g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk);
@@ -714,10 +727,12 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                 scatter_by_j_kernel<<<(nsig + 255) / 256, 256, 0, st>>>(nsig, Tf, dList, dJoff, dFill, dSorted);
                 ROME_CHECK_LAUNCH();
             }
-            bp3d_list_kernel<NT, PIX><<<dim3(nsplit, Jf), NT, 0, st>>>(
-                Tf, g.F, g.csF, cur, dSorted, dJoff, dJf, dFnm, dMctf2, dShift, dPh, dRotF, ctx->r_max, ctx->pad_size,
-                ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox);
-            ROME_CHECK_LAUNCH();
+            for (int j0 = 0; j0 < Jf; j0 += 65535) {  // grid y limit
+                bp3d_list_kernel<NT, PIX><<<dim3(nsplit, std::min(Jf - j0, 65535)), NT, 0, st>>>(
+                    Tf, g.F, g.csF, cur, dSorted, dJoff, dJf, dFnm, dMctf2, dShift, dPh, dRotF, ctx->r_max,
+                    ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox, j0);
+                ROME_CHECK_LAUNCH();
+            }
             prof.launched(ROME_PHASE_BACKPROJECT, 5);
             prof.end(ROME_PHASE_BACKPROJECT);
         }

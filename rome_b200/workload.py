@@ -291,6 +291,13 @@ class Map3dWorkload:
     seed: int = 1
     random_perturbation: float = 0.0
     particle_seed: Optional[int] = None
+    # uneven noise: per-particle SNR log-uniform in snr_range (when set), and noisy_fraction of the
+    # particles with noisy_factor (range) times the noise amplitude on top
+    snr_range: Optional[tuple] = None
+    noisy_fraction: float = 0.0
+    noisy_factor: tuple = (2.0, 4.0)
+    # distinct particles generated; the rest repeat them in order (0: all distinct)
+    unique_particles: int = 0
 
 
 def blob_volumes(rng, ori, K, n_blobs, sig):
@@ -399,7 +406,8 @@ def build_map3d(w: Map3dWorkload):
     proj = np.stack(proj)
     if w.particle_seed is not None:
         rng = np.random.default_rng(w.particle_seed)
-    N = w.n_particles
+    N_all = w.n_particles
+    N = min(N_all, w.unique_particles) if w.unique_particles else N_all
     Fs = cur // 2 + 1
     cls = rng.integers(0, K, N)
     rot = rng.uniform(0.0, 360.0, N)
@@ -433,11 +441,35 @@ def build_map3d(w: Map3dWorkload):
                 ctf[i] = c.reshape(-1)
                 sig_all.append(np.mean(np.abs(s.reshape(-1)[mres > 0]) ** 2))
     sig_pow = float(np.mean(sig_all))
-    sigma2 = sig_pow / (2.0 * w.snr)
-    Fr += rng.normal(0, math.sqrt(sigma2), Fr.shape)
-    Fi += rng.normal(0, math.sqrt(sigma2), Fi.shape)
+    sigma2 = sig_pow / (2.0 * w.snr)  # the model's noise power at the configured SNR
+    amp = np.ones(N)
+    if w.snr_range is not None:
+        lo, hi = np.log(w.snr_range[0]), np.log(w.snr_range[1])
+        amp *= np.sqrt(w.snr / np.exp(rng.uniform(lo, hi, N)))
+    if w.noisy_fraction > 0:
+        noisy = rng.uniform(0, 1, N) < w.noisy_fraction
+        amp *= np.where(noisy, rng.uniform(w.noisy_factor[0], w.noisy_factor[1], N), 1.0)
+    Fr += rng.normal(0, math.sqrt(sigma2), Fr.shape) * amp[:, None]
+    Fi += rng.normal(0, math.sqrt(sigma2), Fi.shape) * amp[:, None]
     Fr[:, 0] = 0.0
     Fi[:, 0] = 0.0
+    # uneven noise: the particles are grouped by noise level (8 log-spaced bins of the amplitude), each
+    # group with its own noise power in the model, as the reference estimates sigma2_noise per group
+    if w.snr_range is not None or w.noisy_fraction > 0:
+        edges = np.exp(np.linspace(np.log(amp.min()), np.log(amp.max()) + 1e-9, 9))
+        group = np.clip(np.searchsorted(edges, amp, side="right") - 1, 0, 7).astype(np.int32)
+        gamp = np.array([np.exp(np.mean(np.log(amp[group == g]))) if np.any(group == g) else 1.0 for g in range(8)])
+        sigma2_groups = sigma2 * gamp ** 2
+    else:
+        group = np.zeros(N, np.int32)
+        sigma2_groups = np.array([sigma2])
+    if N < N_all:
+        # the remaining particles repeat the distinct ones in order (the E-step's work per particle
+        # does not depend on which particle it is)
+        rep = np.arange(N_all) % N
+        Fr, Fi, ctf, group = Fr[rep], Fi[rep], ctf[rep], group[rep]
+        cls, rot, tilt, psi, sx, sy, du, dv, da = (a[rep] for a in (cls, rot, tilt, psi, sx, sy, du, dv, da))
+        N = N_all
     oriF = ori // 2 + 1
     tx, ty = translations(w.offset_range, w.offset_step)
     rp = w.random_perturbation
@@ -445,11 +477,11 @@ def build_map3d(w: Map3dWorkload):
     otr = [oversampled_translations(tx, ty, float(w.offset_step), o, rp) for o in (0, 1)]
     ndir = angles[0].shape[0]
     pool = Map3dPool(
-        ori_size=ori, current_size=cur, coarse_size=cs, nr_classes=K, nr_groups=1, nr_dir=ndir, angles=angles,
-        over_trans_x=[otr[0][0], otr[1][0]], over_trans_y=[otr[0][1], otr[1][1]], trans_x=tx, trans_y=ty,
-        Fimg_real=Fr, Fimg_imag=Fi, Fimg_nomask_real=Fr.copy(), Fimg_nomask_imag=Fi.copy(), Fctf=ctf,
-        highres_Xi2=np.zeros(N), old_offsetx=np.zeros(N), old_offsety=np.zeros(N), group=np.zeros(N, np.int32),
-        sigma2_noise=np.full((1, oriF), sigma2), Mresol_fine=mres, Mresol_coarse=mresol(cs),
+        ori_size=ori, current_size=cur, coarse_size=cs, nr_classes=K, nr_groups=len(sigma2_groups), nr_dir=ndir,
+        angles=angles, over_trans_x=[otr[0][0], otr[1][0]], over_trans_y=[otr[0][1], otr[1][1]], trans_x=tx,
+        trans_y=ty, Fimg_real=Fr, Fimg_imag=Fi, Fimg_nomask_real=Fr.copy(), Fimg_nomask_imag=Fi.copy(), Fctf=ctf,
+        highres_Xi2=np.zeros(N), old_offsetx=np.zeros(N), old_offsety=np.zeros(N), group=group,
+        sigma2_noise=np.repeat(sigma2_groups[:, None], oriF, axis=1), Mresol_fine=mres, Mresol_coarse=mresol(cs),
         pdf_class=np.full(K, 1.0 / K), pdf_direction=np.full((K, ndir), 1.0 / ndir),
         prior_offsetx_class=np.zeros(K), prior_offsety_class=np.zeros(K),
         sigma2_offset=float(w.offset_range) ** 2 / 4.0, adaptive_oversampling=1)
@@ -488,6 +520,14 @@ CONFIGS = {
     # MAP3D: 10,000 particles of 128^2 from K=4 blob volumes (60 blobs, sigma 2-8 voxels), HEALPix order 2
     # (192 directions x 24 coarse psi), +-4 px step 2 (13 translations), adaptive oversampling 1; coarse
     # size 20 as the reference's formula gives for these images (map_model.cpp:505-520)
+    # Batched uneven MAP3D: 50,000 particles of 128^2 (10,000 distinct, repeated) from K=8 blob volumes,
+    # HEALPix order 3 (768 directions x 48 coarse psi, coarse size 40), +-4 px step 2, oversampling 1;
+    # per-particle SNR log-uniform over a decade and 30% of the particles with 2-4x the noise amplitude,
+    # noise power per noise-level group, so the number of coarse-significant points varies widely
+    "map3d_cfg4": Map3dWorkload(n_particles=50000, ori_size=128, coarse_size=40, n_classes=8, n_blobs=60,
+                                blob_sigma=(2.0, 8.0), healpix_order=3, offset_range=4, offset_step=2, max_shift=4.0,
+                                pixel=1.5, snr=0.0316, seed=4, snr_range=(0.01, 0.1), noisy_fraction=0.3,
+                                noisy_factor=(2.0, 4.0), unique_particles=10000),
     "map3d_cfg3": Map3dWorkload(n_particles=10000, ori_size=128, coarse_size=20, n_classes=4, n_blobs=60,
                                 blob_sigma=(2.0, 8.0), healpix_order=2, offset_range=4, offset_step=2, max_shift=4.0,
                                 pixel=1.5, snr=0.05, seed=3),
