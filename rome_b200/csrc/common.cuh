@@ -109,6 +109,7 @@ enum Slot {
     S_LIST,       // particle list of the selection fallback
     S_ROTSIG,     // Rot_significant [K*npsi] char
     S_PAIRS,      // 3D fine pass: (particle, coarse translation) pair flags, ids and list
+    S_SELEXACT,   // particles whose significance walk needs the exact sort
     S_ACTIDX,     // pixel -> active index [F] int
     S_TRANS,      // translations of the last pass [T] double2
     S_LISTCNT,    // list counter + per-orientation counts

@@ -162,14 +162,14 @@ __global__ void rotsig_from_list_kernel(int n, int ntr, const SigEntry* __restri
 // Ordered compaction of particle i's significant coarse points e = jc * ntr
 // + itr into (a) the fine-pass entries fe[off[i] + r] = (i, r, u, itr), u
 // the compact index of orientation jc among the orientations some particle
-// needs, and (b) the row-layout prior index ent[i * stride + r] =
+// needs, and (b) the row-layout prior index ent[off[i] + r] =
 // (jc / npsi, itr), the pdf_direction index (class * ndir + dir) and the
-// coarse translation.  Padding of ent stays (-1, 0).  Each thread scans 16
+// coarse translation.  Each thread scans 16
 // bytes per step (one block-wide scan of the counts per 8 KB of the row).
 constexpr int FE_THREADS = 512;
 __global__ void __launch_bounds__(FE_THREADS)
     fine_entries_kernel(long ncoarse, int ntr, int npsi, const char* __restrict__ mcoarse, const int* __restrict__ off,
-                        const int* __restrict__ ucompact, int stride, int4* __restrict__ fe, int2* __restrict__ ent) {
+                        const int* __restrict__ ucompact, int4* __restrict__ fe, int2* __restrict__ ent) {
     __shared__ int wsum[FE_THREADS / 32 + 1];
     const int i = blockIdx.x;
     const char* m = mcoarse + (long)i * ncoarse;
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(FE_THREADS)
                 const long e = e0 + b;
                 const int jc = (int)(e / ntr), itr = (int)(e - (long)jc * ntr);
                 fe[off[i] + r] = make_int4(i, r, ucompact[jc], itr);
-                ent[(long)i * stride + r] = make_int2(jc / npsi, itr);
+                ent[off[i] + r] = make_int2(jc / npsi, itr);
                 r++;
             }
         }
@@ -296,7 +296,7 @@ __global__ void __launch_bounds__(NT)
 
 // Fine-pass squared differences of one coarse-significant point: nor fine
 // orientations (u * nor + o) x notr fine translations (itr * notr + t),
-// written at [i][r * nor * notr + o * notr + t] (the ihidden order
+// written at [off[i] + r][o * notr + t] of the unpadded ragged rows (the ihidden order
 // itrans -> over_rot -> over_trans of the reference's lists,
 // src/map3d_optimizer.cpp:1340-1358).  A holds the shifted images of the
 // needed (particle, coarse translation) pairs only, pair pid[i * ntr + itr].  diff2 = (N - 2 C + S + Xi2) / 2 with
@@ -306,13 +306,13 @@ template <int NT, int NOR, int NOTR>
 __global__ void __launch_bounds__(NT)
     fine_diff2_kernel(int ntr, int Kp, int Kq, const int4* __restrict__ fe, const int* __restrict__ pid,
                       const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ W2,
-                      const float* __restrict__ Q, const float* __restrict__ S, const double* __restrict__ xi2, long Xf,
+                      const float* __restrict__ Q, const float* __restrict__ S, const double* __restrict__ xi2,
                       float* __restrict__ diff2, unsigned* __restrict__ rowmin) {
     constexpr int NH = NOR * NOTR;
     static_assert(NH == 32, "one warp holds the 32 sub-hypotheses of a point");
     __shared__ double red[NT / 32][NH + NOR];
     const int4 en = fe[blockIdx.x];
-    const int i = en.x, r = en.y, u = en.z, itr = en.w;
+    const int i = en.x, u = en.z, itr = en.w;
     const long arow = (long)pid[i * ntr + itr] * NOTR;  // the pair's rows of the compacted A operand
     const float2* Ar[NOTR];
     const float2* Br[NOR];
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(NT)
             ns += red[w][NH + o];
         }
         const float v = (float)(0.5 * (ns - 2.0 * cs + (double)S[arow + t] + xi2[i]));
-        diff2[(long)i * Xf + (long)r * NH + h] = v;
+        diff2[(long)blockIdx.x * NH + h] = v;  // point blockIdx.x = off[i] + r of the ragged rows
         float m = v;
         for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
         if (h == 0) atomicMin(&rowmin[i], float_key(m));
@@ -402,10 +402,14 @@ __global__ void __launch_bounds__(NT)
                        const double2* __restrict__ ph, const int* __restrict__ Mresol, const int* __restrict__ group,
                        const double2* __restrict__ oldoff, const double2* __restrict__ trans,
                        const double* __restrict__ priorx, const double* __restrict__ priory,
-                       double* __restrict__ wsn, double* __restrict__ normcorr, double* __restrict__ wk) {
+                       double* __restrict__ wsn, double* __restrict__ normcorr, double* __restrict__ wk, int chunk) {
     const int i = blockIdx.y;
     const int n0 = blockIdx.x * NT * PIX;
-    const int s0 = seg[2 * i], ns = seg[2 * i + 1];
+    // blockIdx.z takes entries [z * chunk, (z + 1) * chunk) of the particle's segment, so that a particle
+    // with many significant hypotheses is spread over many CTAs (all sums below are atomic)
+    const int z0 = blockIdx.z * chunk;
+    if (z0 >= seg[2 * i + 1]) return;
+    const int s0 = seg[2 * i] + z0, ns = min(chunk, seg[2 * i + 1] - z0);
     __shared__ double spec[1024];
     __shared__ double red[32];
     for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) spec[q] = 0.0;

@@ -450,6 +450,9 @@ struct PostLayout {
     int ndir = 1;
     const int2* ent = nullptr;
     int ent_stride = 0;
+    // ragged rows without padding: particle i's entries are roff[i] .. roff[i + 1] - 1 (each epr
+    // hypotheses), so its row starts at roff[i] * epr and ent[roff[i] + r] describes entry r
+    const int* roff = nullptr;
     int epr = 0;
     int list_zeros = 0;  // 3D: computed zero weights take part in the sorted walk
 };
@@ -472,7 +475,7 @@ __device__ __forceinline__ bool hyp_prior(long e, int i, const PostLayout& L, co
                                           const double* __restrict__ po, double& pd, double& pof, long& lo) {
     int k, itr;
     if (L.ent) {
-        const int2 en = L.ent[(long)i * L.ent_stride + e / L.epr];
+        const int2 en = L.ent[(L.roff ? (long)L.roff[i] : (long)i * L.ent_stride) + e / L.epr];
         if (en.x < 0) return false;
         k = en.x;
         // y < 0: the entry's hypotheses are its translations (restricted 2D search)

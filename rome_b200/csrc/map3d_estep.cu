@@ -60,11 +60,6 @@ Rot3 rot3_inv(double rot, double tilt, double psi, int padding) {
     return Rot3{A00 * p, A10 * p, A01 * p, A11 * p, A02 * p, A12 * p};
 }
 
-__global__ void fill_float_kernel(long n, float v, float* __restrict__ out) {
-    long q = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < n) out[q] = v;
-}
-
 struct Pass {
     int cs, csF, F, Kact, Kp, Kq, my_r_max;
 };
@@ -552,9 +547,8 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         const int E = hoffp[P];
         stage_copy(ctx, dOffP, hoffp.data(), (size_t)P + 1);
         int4* dFe = ctx->ws[S_FE].as<int4>((size_t)std::max(E, 1));
-        int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)P * stride);
-        ROME_CUDA(cudaMemsetAsync(dEnt, 0xFF, sizeof(int2) * (size_t)P * stride, st));
-        fine_entries_kernel<<<P, FE_THREADS, 0, st>>>(ncoarse, ntr, npsi, dMcoarse, dOffP, dUcomp, stride, dFe, dEnt);
+        int2* dEnt = ctx->ws[S_FENT].as<int2>((size_t)std::max(E, 1));
+        fine_entries_kernel<<<P, FE_THREADS, 0, st>>>(ncoarse, ntr, npsi, dMcoarse, dOffP, dUcomp, dFe, dEnt);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_PROJECT, 2);
 
@@ -584,20 +578,20 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         prof.add_bytes(ROME_PHASE_SHIFT, 4.0 * pair_cap * NOTR * g.Kp);
         prof.end(ROME_PHASE_SHIFT);
 
-        // fine squared differences, ragged rows [P][stride * 32] padded with +inf
+        // fine squared differences in ragged rows without padding: particle i's row is points
+        // off[i] .. off[i + 1] - 1, NH sub-hypotheses each (every entry is written by the kernel);
+        // Xf, the longest row, sizes the selection's scratch
         const long Xf = (long)stride * NH;
-        float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)P * Xf);
+        float* dDiff2 = ctx->ws[S_DIFF2].as<float>((size_t)std::max(E, 1) * NH);
         unsigned* dRowMin = ctx->ws[S_ROWMIN].as<unsigned>((size_t)P);
         prof.begin(ROME_PHASE_CROSS_GEMM);
-        fill_float_kernel<<<(unsigned)((P * Xf + 255) / 256), 256, 0, st>>>(P * Xf, INFINITY, dDiff2);
-        ROME_CHECK_LAUNCH();
         ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
         if (E > 0) {
             fine_diff2_kernel<128, 8, 4><<<E, 128, 0, st>>>(ntr, g.Kp, g.Kq, dFe, dPairId, dA, dB, dW2, dQ, dS, dXi2,
-                                                          Xf, dDiff2, dRowMin);
+                                                          dDiff2, dRowMin);
             ROME_CHECK_LAUNCH();
         }
-        prof.launched(ROME_PHASE_CROSS_GEMM, 2);
+        if (E > 0) prof.launched(ROME_PHASE_CROSS_GEMM);
         prof.add_flops(ROME_PHASE_CROSS_GEMM, 4.0 * (double)E * NH * g.Kact);
         prof.end(ROME_PHASE_CROSS_GEMM);
 
@@ -606,15 +600,16 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         Lf.ndir = ndir;
         Lf.ent = dEnt;
         Lf.ent_stride = stride;
+        Lf.roff = dOffP;
         Lf.epr = NH;
         Lf.list_zeros = 1;
         double* dW = nullptr;
-        if (out->fine_weight) dW = ctx->ws[S_WCHK].as<double>((size_t)P * Xf);
+        if (out->fine_weight) dW = ctx->ws[S_WCHK].as<double>((size_t)std::max(E, 1) * NH);
         int* dCounter = ctx->ws[S_LISTCNT].as<int>((size_t)Jf + 4);
         int listcap = std::max(1024, P * 64), nsig = 0;
         SigEntry* dList = nullptr;
         prof.begin(ROME_PHASE_POSTERIOR);
-        prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)P * Xf);  // diff2 rows read once
+        prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)E * NH);  // diff2 rows read once
         for (;;) {
             dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
             SelectResult sr = run_select(ctx, st, 0, P, Xf, Lf, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,
@@ -638,10 +633,10 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         std::vector<float> hd;
         std::vector<double> hw;
         if (out->fine_count || out->fine_index || out->fine_diff2 || out->fine_weight) {
-            hd.resize((size_t)P * Xf);
+            hd.resize((size_t)std::max(E, 1) * NH);
             ROME_CUDA(cudaMemcpyAsync(hd.data(), dDiff2, sizeof(float) * hd.size(), cudaMemcpyDeviceToHost, st));
             if (dW) {
-                hw.resize((size_t)P * Xf);
+                hw.resize((size_t)std::max(E, 1) * NH);
                 ROME_CUDA(cudaMemcpyAsync(hw.data(), dW, sizeof(double) * hw.size(), cudaMemcpyDeviceToHost, st));
             }
         }
@@ -656,8 +651,9 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                     const int4 en = hfe[hoffp[i] + e / NH];
                     const long jc = uj[en.z];
                     if (out->fine_index) out->fine_index[q] = ((jc * ntr + en.w) * NH) + e % NH;
-                    if (out->fine_diff2) out->fine_diff2[q] = (double)hd[(size_t)i * Xf + e];
-                    if (out->fine_weight) out->fine_weight[q] = hw.empty() ? 0.0 : hw[(size_t)i * Xf + e];
+                    const size_t at = (size_t)hoffp[i] * NH + e;
+                    if (out->fine_diff2) out->fine_diff2[q] = (double)hd[at];
+                    if (out->fine_weight) out->fine_weight[q] = hw.empty() ? 0.0 : hw[at];
                 }
             }
         }
@@ -696,9 +692,18 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         const int nsplit = (g.F + NT * PIX - 1) / (NT * PIX);
         prof.begin(ROME_PHASE_WSUM);
         ROME_REQUIRE(P <= 65535, "pool of %d particles: at most 65,535", P);
-        wsum3d_list_kernel<NT, PIX><<<dim3(nsplit, P), NT, 0, st>>>(
+        // the longest list segment sets the number of entry chunks (grid z) of the wsum kernel
+        std::vector<int> hseg((size_t)2 * P);
+        ROME_CUDA(cudaMemcpyAsync(hseg.data(), dSeg, sizeof(int) * 2 * P, cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        int maxseg = 1;
+        for (int i = 0; i < P; i++) maxseg = std::max(maxseg, hseg[(size_t)2 * i + 1]);
+        const int WCH = 256;
+        const int nzch = std::min(65535, (maxseg + WCH - 1) / WCH);
+        const int wchunk = (maxseg + nzch - 1) / nzch;
+        wsum3d_list_kernel<NT, PIX><<<dim3(nsplit, P, nzch), NT, 0, st>>>(
             Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
-            g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk);
+            g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk, wchunk);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_WSUM);
         prof.end(ROME_PHASE_WSUM);

@@ -57,7 +57,7 @@ __device__ __forceinline__ void bitonic_desc_kv(double* key, int* val, int n) {
 }
 
 __global__ void __launch_bounds__(SEL2_THREADS)
-    post_select2_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2,
+    post_select2_kernel(int mode, long Xrow, PostLayout L, const float* __restrict__ diff2,
                         const double* __restrict__ pdir, const double* __restrict__ poff, double frac,
                         double* __restrict__ part, int* __restrict__ parti, const double* __restrict__ wgiven,
                         double* __restrict__ wout, SigEntry* __restrict__ list, int* __restrict__ counter, int cap,
@@ -72,8 +72,11 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     __shared__ int ncand, s_nsig, s_over, s_m, s_base;
     __shared__ double s_sig;
     const int i = blockIdx.x;
-    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
-    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
+    // the particle's row: fixed length Xrow at i * Xrow, or (ragged rows, L.roff) its own span
+    const long X = L.roff ? (long)(L.roff[i + 1] - L.roff[i]) * L.epr : Xrow;
+    const long rb = L.roff ? (long)L.roff[i] * L.epr : (long)i * Xrow;
+    const float* d = diff2 ? diff2 + rb : nullptr;
+    const double* wg = wgiven ? wgiven + rb : nullptr;
     const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
 
     // ---- min over computed diff2 ----
@@ -109,7 +112,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
             float dv = d[e];
             if (dv < INFINITY) maxpd = fmax(maxpd, pd * pof);
             double w = hyp_weight(dv, mn, pd, pof);
-            if (wout) wout[(long)i * X + e] = w;
+            if (wout) wout[rb + e] = w;
             sum += w;
             if (w > maxw || (w == maxw && w > DBL_MIN && lo < best_lo)) {
                 maxw = w;
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                 auto visit = [&](int jq, int kq, int cq, int t, float dv) {
                     const long e = (long)jq * L.T + t;
                     if (!(dv < INFINITY)) {
-                        if (wout) wout[(long)i * X + e] = 0.0;
+                        if (wout) wout[rb + e] = 0.0;
                         return;
                     }
                     const int itr = L.notr == 1 ? t : t / L.notr;
@@ -176,11 +179,11 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                     const double diff = (double)dv - mn;
                     if (diff > skip_cut) return;  // written after the sweep when wout is wanted
                     if (diff > 700.) {
-                        if (wout) wout[(long)i * X + e] = 0.0;
+                        if (wout) wout[rb + e] = 0.0;
                         return;
                     }
                     const double w = pp * exp(-diff);
-                    if (wout) wout[(long)i * X + e] = w;
+                    if (wout) wout[rb + e] = w;
                     sum += w;
                     if (w >= maxw && w > DBL_MIN) {
                         int kk, it2;
@@ -241,7 +244,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                     double pd, pof;
                     long lo;
                     hyp_prior(e, i, L, pdir, po, pd, pof, lo);
-                    wout[(long)i * X + e] = hyp_weight(dv, mn, pd, pof);
+                    wout[rb + e] = hyp_weight(dv, mn, pd, pof);
                 }
             }
         }
@@ -416,18 +419,21 @@ __global__ void __launch_bounds__(SEL2_THREADS)
 // ran out), sorts them (bitonic, descending) and walks them.  One CTA per
 // listed particle, each with its own scratch slot.
 __global__ void __launch_bounds__(SEL2_THREADS)
-    select_fallback2_kernel(int mode, long X, PostLayout L, const float* __restrict__ diff2,
+    select_fallback2_kernel(int mode, long Xrow, PostLayout L, const float* __restrict__ diff2,
                             const double* __restrict__ pdir, const double* __restrict__ poff,
                             const double* __restrict__ wgiven, const int* __restrict__ plist, long slot_len,
                             double* __restrict__ scratch, double* __restrict__ part, int* __restrict__ parti) {
     const int i = plist[blockIdx.x];
+    // the particle's row: fixed length Xrow at i * Xrow, or (ragged rows, L.roff) its own span
+    const long X = L.roff ? (long)(L.roff[i + 1] - L.roff[i]) * L.epr : Xrow;
+    const long rb = L.roff ? (long)L.roff[i] * L.epr : (long)i * Xrow;
     double* buf = scratch + (long)blockIdx.x * slot_len;
     __shared__ int ncand, nzero;
     __shared__ double red[32];
     double* pp = part + (long)i * 8;
     const double mn = pp[0], thr = pp[3];
-    const float* d = diff2 ? diff2 + (long)i * X : nullptr;
-    const double* wg = wgiven ? wgiven + (long)i * X : nullptr;
+    const float* d = diff2 ? diff2 + rb : nullptr;
+    const double* wg = wgiven ? wgiven + rb : nullptr;
     const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
     if (threadIdx.x == 0) ncand = nzero = 0;
     __syncthreads();
@@ -499,16 +505,246 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     }
 }
 
+// Completes the selection of listed particles without sorting every weight:
+// an MSB-first radix select on the FP64 bit patterns of the positive weights
+// (positive doubles order like their bits) finds the weight at which the
+// descending running sum crosses f * sum, 11 bits per level: a histogram of
+// counts and sums per digit, the crossing digit kept, until the crossing
+// bucket holds at most SR_LEAF weights, which are sorted in shared memory and
+// walked from the sum of everything above them.  The reference adds the
+// weights one by one in descending order; the sums here are added in another
+// order, so every comparison of the walk is checked against the rounding
+// both orders can make (4 (n + 1) DBL_EPSILON S after n additions): if any
+// comparison at the crossing lies within that margin the particle is marked
+// in `redo` and finished by the exact sort (select_fallback2_kernel).  One
+// CTA per listed particle; `scratch` holds its positive weights.
+constexpr int SR_THREADS = 1024;
+constexpr int SR_DIGITS = 2048;
+constexpr int SR_LEAF = 2048;  // (histograms 24 KB + leaf 16 KB of static shared memory)
+
+__global__ void __launch_bounds__(SR_THREADS)
+    select_radix_kernel(int mode, long Xrow, PostLayout L, const float* __restrict__ diff2,
+                        const double* __restrict__ pdir, const double* __restrict__ poff,
+                        const double* __restrict__ wgiven, const int* __restrict__ plist, long slot_len,
+                        double* __restrict__ scratch, double* __restrict__ part, int* __restrict__ parti,
+                        int* __restrict__ redo) {
+    const int i = plist[blockIdx.x];
+    // the particle's row: fixed length Xrow at i * Xrow, or (ragged rows, L.roff) its own span
+    const long X = L.roff ? (long)(L.roff[i + 1] - L.roff[i]) * L.epr : Xrow;
+    const long rb = L.roff ? (long)L.roff[i] * L.epr : (long)i * Xrow;
+    double* buf = scratch + (long)blockIdx.x * slot_len;
+    __shared__ unsigned hcnt[SR_DIGITS];
+    __shared__ double hsum[SR_DIGITS];
+    __shared__ double leaf[SR_LEAF];
+    __shared__ double red[32];
+    __shared__ int ncand, nzero, nleaf;
+    __shared__ int s_digit, s_stop;
+    __shared__ double s_above;
+    __shared__ long long s_above_n;
+    double* pp = part + (long)i * 8;
+    const double mn = pp[0], thr = pp[3];
+    // only weights >= t0 = (1 - f) sum / X can be walked (post_select2_kernel's bound, diff2 cut dlim0)
+    const double t0 = pp[6], dlim0 = pp[7];
+    const float* d = diff2 ? diff2 + rb : nullptr;
+    const double* wg = wgiven ? wgiven + rb : nullptr;
+    const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
+    if (threadIdx.x == 0) {
+        ncand = nzero = nleaf = 0;
+        s_above = 0.0;
+        s_above_n = 0;
+    }
+    __syncthreads();
+    // ---- the particle's positive weights (and, in 3D, the count of computed zeros) ----
+    double maxpd = 0.0;
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        double w;
+        if (mode == 0) {
+            double pd, pof;
+            long lo;
+            if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) continue;
+            const float dv = d[e];
+            if (!(dv < INFINITY)) continue;
+            maxpd = fmax(maxpd, pd * pof);
+            if (t0 > 0.0 && (double)dv > dlim0) continue;  // below t0: never walked
+            w = hyp_weight(dv, mn, pd, pof);
+            if (w == 0.0 && L.list_zeros) atomicAdd(&nzero, 1);
+        } else {
+            w = wg[e];
+        }
+        if (w > 0.0 && (w >= t0 || t0 <= 0.0)) buf[atomicAdd(&ncand, 1)] = w;
+    }
+    maxpd = block_reduce_max(maxpd, red);
+    const int cnt = ncand;
+    // ---- radix levels: digits of 11 bits from the top (exponent), the last one 8 bits ----
+    unsigned long long prefix = 0;  // the digits fixed so far (bits above `shift + width`)
+    int shift = 52, width = 11;
+    bool stopped = false, leaf_ready = false;
+    for (;;) {
+        for (int q = threadIdx.x; q < SR_DIGITS; q += blockDim.x) {
+            hcnt[q] = 0u;
+            hsum[q] = 0.0;
+        }
+        __syncthreads();
+        const unsigned long long mask = (1ull << width) - 1ull;
+        // each thread adds runs of equal digits before touching shared memory: the weights of a broad
+        // posterior share a few exponents, and one shared counter per digit would serialise them
+        int cur = -1;
+        unsigned cc = 0u;
+        double cs = 0.0;
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+            const double w = buf[q];
+            const unsigned long long k = (unsigned long long)__double_as_longlong(w);
+            if ((k >> (shift + width)) != prefix) continue;
+            const int dg = (int)((k >> shift) & mask);
+            if (dg != cur) {
+                if (cur >= 0) {
+                    atomicAdd(&hcnt[cur], cc);
+                    atomicAdd(&hsum[cur], cs);
+                }
+                cur = dg;
+                cc = 0u;
+                cs = 0.0;
+            }
+            cc++;
+            cs += w;
+        }
+        if (cur >= 0) {
+            atomicAdd(&hcnt[cur], cc);
+            atomicAdd(&hsum[cur], cs);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            // descending digits until the running sum crosses the threshold
+            double above = s_above;
+            long long an = s_above_n;
+            int dg = -1;
+            for (int q = (int)mask; q >= 0; q--) {
+                if (hcnt[q] == 0u) continue;
+                if (above + hsum[q] > thr) {
+                    dg = q;
+                    break;
+                }
+                above += hsum[q];
+                an += hcnt[q];
+            }
+            s_digit = dg;
+            s_above = above;
+            s_above_n = an;
+        }
+        __syncthreads();
+        const int dg = s_digit;
+        if (dg < 0) break;  // the positive weights never exceed the threshold
+        prefix = (prefix << width) | (unsigned long long)dg;
+        if (hcnt[dg] <= (unsigned)SR_LEAF || shift == 0) {
+            leaf_ready = true;
+            break;
+        }
+        shift -= 11;
+        if (shift < 0) {
+            width = 11 + shift;  // the remaining low bits
+            shift = 0;
+        }
+    }
+    if (leaf_ready) {
+        // the crossing bucket: every weight whose bits above `shift` match the prefix
+        for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+            const double w = buf[q];
+            const unsigned long long k = (unsigned long long)__double_as_longlong(w);
+            if ((k >> shift) == prefix) {
+                const int r = atomicAdd(&nleaf, 1);
+                if (r < SR_LEAF) leaf[r] = w;
+            }
+        }
+        __syncthreads();
+        const int m = min(nleaf, SR_LEAF);  // more only when they are all equal (shift 0)
+        int n2 = 1;
+        while (n2 < m) n2 <<= 1;
+        for (int q = m + threadIdx.x; q < n2; q += blockDim.x) leaf[q] = -1.0;
+        __syncthreads();
+        for (int k = 2; k <= n2; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+                    const int o = q ^ j;
+                    if (o > q) {
+                        const bool desc = (q & k) == 0;
+                        const double x = leaf[q], y = leaf[o];
+                        if (desc ? (x < y) : (x > y)) {
+                            leaf[q] = y;
+                            leaf[o] = x;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        if (threadIdx.x == 0) {
+            double sacc = s_above, sig = 0.0;
+            long long ns = s_above_n;
+            bool ambiguous = false;
+            const int nl = nleaf;
+            // the comparison before the leaf (the sum of everything above it stays <= thr)
+            if (fabs(sacc - thr) <= 4.0 * (double)(ns + 1) * DBL_EPSILON * fmax(sacc, thr)) ambiguous = true;
+            for (int q = 0; q < nl; q++) {
+                const double w = q < m ? leaf[q] : leaf[0];  // beyond SR_LEAF: equal weights
+                sacc += w;
+                ns++;
+                sig = w;
+                if (fabs(sacc - thr) <= 4.0 * (double)(ns + 1) * DBL_EPSILON * fmax(sacc, thr)) ambiguous = true;
+                if (sacc > thr) {
+                    stopped = true;
+                    break;
+                }
+            }
+            if (!stopped) ambiguous = true;  // cannot happen when the bucket crossed; leave it to the exact sort
+            s_stop = ambiguous ? -1 : 1;
+            if (!ambiguous) {
+                pp[2] = sig;
+                parti[(long)i * 8 + 1] = (int)ns;
+                pp[5] = (sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
+            }
+        }
+    } else if (threadIdx.x == 0 && t0 > 0.0) {
+        // with the t0 bound the walk must stop among the gathered weights: leave the rest to the exact sort
+        s_stop = -1;
+    } else if (threadIdx.x == 0) {
+        // every positive weight walked without passing the threshold: the 3D walk continues through the
+        // computed zeros (src/map3d_optimizer.cpp:1840-1864), which is exact whatever the order of the sum
+        // only if it is clearly below the threshold
+        const double sacc = s_above;
+        const bool ambiguous = fabs(sacc - thr) <= 4.0 * (double)(cnt + 1) * DBL_EPSILON * fmax(sacc, thr);
+        s_stop = ambiguous ? -1 : 0;
+        if (!ambiguous) {
+            double sig = 0.0;
+            // the smallest positive weight is the last one walked
+            sig = INFINITY;
+            for (int q = 0; q < cnt; q++) sig = fmin(sig, buf[q]);
+            if (cnt == 0) sig = 0.0;
+            int ns = cnt;
+            if (nzero > 0) {
+                ns += nzero;
+                sig = 0.0;
+            }
+            pp[2] = sig;
+            parti[(long)i * 8 + 1] = ns;
+            pp[5] = (sig > 0.0 && maxpd > 0.0) ? mn + log(maxpd / sig) + 1e-6 * (1.0 + fabs(mn)) : INFINITY;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) redo[blockIdx.x] = s_stop < 0 ? 1 : 0;
+}
+
 // list segments of listed particles (the ones the fallback finished)
-__global__ void __launch_bounds__(256)
-    sig_list_some_kernel(const int* __restrict__ plist, long X, PostLayout L, const float* __restrict__ diff2,
+__global__ void __launch_bounds__(1024)
+    sig_list_some_kernel(const int* __restrict__ plist, long Xrow, PostLayout L, const float* __restrict__ diff2,
                          const double* __restrict__ pdir, const double* __restrict__ poff,
                          const double* __restrict__ part, int* __restrict__ counter, int cap,
                          SigEntry* __restrict__ list, int* __restrict__ seg) {
     const int i = plist[blockIdx.x];
+    // the particle's row: fixed length Xrow at i * Xrow, or (ragged rows, L.roff) its own span
+    const long X = L.roff ? (long)(L.roff[i + 1] - L.roff[i]) * L.epr : Xrow;
+    const long rb = L.roff ? (long)L.roff[i] * L.epr : (long)i * Xrow;
     const double mn = part[(long)i * 8 + 0], sumw = part[(long)i * 8 + 1], sig = part[(long)i * 8 + 2];
     const double dcut = part[(long)i * 8 + 5];
-    const float* d = diff2 + (long)i * X;
+    const float* d = diff2 + rb;
     const double* po = poff + (long)i * L.K * L.ntr;
     __shared__ int cnt, base;
     if (threadIdx.x == 0) cnt = 0;
@@ -578,21 +814,44 @@ inline SelectResult run_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P
     for (int i = 0; i < P; i++)
         if (hpi[(size_t)i * 8 + 2]) over.push_back(i);
     if (!over.empty()) {
-        long n2 = 1;
-        while (n2 < X) n2 <<= 1;
+        // radix select first (work proportional to the weights, not to sorting them all); the particles
+        // it cannot settle exactly (a comparison within rounding of the threshold) take the exact sort
         const int slots = (int)std::min<size_t>(over.size(), 64);
-        double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)slots * n2);
-        int* dli = ctx->ws[S_LIST].as<int>(over.size());
+        int* dli = ctx->ws[S_LIST].as<int>(2 * over.size());
+        int* dredo = dli + over.size();
         stage_copy(ctx, dli, over.data(), over.size());
-        for (size_t b = 0; b < over.size(); b += slots) {
-            int nb = (int)std::min<size_t>(slots, over.size() - b);
-            select_fallback2_kernel<<<nb, SEL2_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dli + b, n2,
-                                                                scratch, part, parti);
-            ROME_CHECK_LAUNCH();
-            res.launches++;
+        {
+            double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)slots * X);
+            for (size_t b = 0; b < over.size(); b += slots) {
+                const int nb = (int)std::min<size_t>(slots, over.size() - b);
+                select_radix_kernel<<<nb, SR_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dli + b, X,
+                                                              scratch, part, parti, dredo + b);
+                ROME_CHECK_LAUNCH();
+                res.launches++;
+            }
+        }
+        std::vector<int> hredo(over.size()), exact;
+        ROME_CUDA(cudaMemcpyAsync(hredo.data(), dredo, sizeof(int) * over.size(), cudaMemcpyDeviceToHost, st));
+        ROME_CUDA(cudaStreamSynchronize(st));
+        for (size_t q = 0; q < over.size(); q++)
+            if (hredo[q]) exact.push_back(over[q]);
+        if (!exact.empty()) {
+            long n2 = 1;
+            while (n2 < X) n2 <<= 1;
+            const int eslots = (int)std::min<size_t>(exact.size(), 64);
+            double* scratch = ctx->ws[S_SCRATCH].as<double>((size_t)eslots * n2);
+            int* dex = ctx->ws[S_SELEXACT].as<int>(exact.size());
+            stage_copy(ctx, dex, exact.data(), exact.size());
+            for (size_t b = 0; b < exact.size(); b += eslots) {
+                const int nb = (int)std::min<size_t>(eslots, exact.size() - b);
+                select_fallback2_kernel<<<nb, SEL2_THREADS, 0, st>>>(mode, X, L, diff2, pdir, poff, wgiven, dex + b,
+                                                                    n2, scratch, part, parti);
+                ROME_CHECK_LAUNCH();
+                res.launches++;
+            }
         }
         if (counter && mode == 0) {
-            sig_list_some_kernel<<<(int)over.size(), 256, 0, st>>>(dli, X, L, diff2, pdir, poff, part, counter, cap,
+            sig_list_some_kernel<<<(int)over.size(), 1024, 0, st>>>(dli, X, L, diff2, pdir, poff, part, counter, cap,
                                                                   list, seg);
             ROME_CHECK_LAUNCH();
             res.launches++;

@@ -523,10 +523,13 @@ CONFIGS = {
     # Batched uneven MAP3D: 50,000 particles of 128^2 (10,000 distinct, repeated) from K=8 blob volumes,
     # HEALPix order 3 (768 directions x 48 coarse psi, coarse size 40), +-4 px step 2, oversampling 1;
     # per-particle SNR log-uniform over a decade and 30% of the particles with 2-4x the noise amplitude,
-    # noise power per noise-level group, so the number of coarse-significant points varies widely
+    # noise power per noise-level group, so the number of coarse-significant points varies widely.  The
+    # SNR here is per Fourier component of the CTF-modulated projection; the decade [0.01, 0.1] on that
+    # scale leaves the noisiest particles nearly uninformative (significant over most of the 3.8 M coarse
+    # hypotheses), so the decade is [0.05, 0.5], which puts the tail of the counts in the thousands
     "map3d_cfg4": Map3dWorkload(n_particles=50000, ori_size=128, coarse_size=40, n_classes=8, n_blobs=60,
                                 blob_sigma=(2.0, 8.0), healpix_order=3, offset_range=4, offset_step=2, max_shift=4.0,
-                                pixel=1.5, snr=0.0316, seed=4, snr_range=(0.01, 0.1), noisy_fraction=0.3,
+                                pixel=1.5, snr=0.158, seed=4, snr_range=(0.05, 0.5), noisy_fraction=0.3,
                                 noisy_factor=(2.0, 4.0), unique_particles=10000),
     "map3d_cfg3": Map3dWorkload(n_particles=10000, ori_size=128, coarse_size=20, n_classes=4, n_blobs=60,
                                 blob_sigma=(2.0, 8.0), healpix_order=2, offset_range=4, offset_step=2, max_shift=4.0,
