@@ -280,6 +280,9 @@ def run_ours(args):
         exchange_bytes[0] = allreduce_backprojectors(ctx) + sum(int(np.asarray(v).nbytes) for v in red.values())
 
     def step_dev():
+        # one EM iteration: the model's projections are computed once per step, not carried over
+        for c in lane_ctxs:
+            c.invalidate_projections()
         if learned:
             res = learned_estep_pools(ctx, net, dev, args.topk, args.min_mass, workers=workers)
         else:
@@ -290,6 +293,8 @@ def run_ours(args):
     def step_e2e():
         # host (pinned) raw images copied in and prepared on the device (pool k + 1 while pool k computes),
         # E-step, results copied out
+        for c in lane_ctxs:
+            c.invalidate_projections()
         stream = prepared_stream(prep_ctx, items, opts)
         if learned:
             res = learned_estep_pools(ctx, net, stream, args.topk, args.min_mass, workers=workers)

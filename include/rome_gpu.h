@@ -120,6 +120,16 @@ int rome_gpu_abi_version(void);
 int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_classes, int ori_size, int pad_size, int r_max,
                             int padding_factor, const double* data);
 
+/* The pools of one EM iteration share the coarse-pass projections of every
+ * class and orientation: a 2D pool whose model, sampling tables and
+ * precision equal the previous call's reuses them (the reference recomputes
+ * them per pool, getReferenceAllOrientations, src/map2d_optimizer.cpp:
+ * 857-905).  rome_gpu_set_projectors starts a new model; this marks the
+ * cached projections stale without uploading anything, so that the next
+ * pool recomputes them (one projection per iteration when the model changed
+ * on the device, or to time an iteration as a whole). */
+int rome_gpu_invalidate_projections(RomeGpuCtx* ctx);
+
 /* Download (and optionally reset) the accumulated backprojector of one
  * class: MyBackProjector::data (interleaved complex) and ::weight, same
  * shape as the projector.  Used for the reduction across ranks

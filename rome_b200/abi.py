@@ -175,7 +175,7 @@ EXPORTED_SYMBOLS = [
     "rome_gpu_reconstruct", "rome_gpu_get_timings", "rome_gpu_reset_timings", "rome_gpu_copy_from_host",
     "rome_gpu_add_backprojectors", "rome_gpu_prepare_particles", "rome_gpu_backproject_images",
     "rome_gpu_tuning_report", "rome_gpu_wait_selftest", "rome_gpu_backprojector_size",
-    "rome_gpu_backprojector_device_copy",
+    "rome_gpu_backprojector_device_copy", "rome_gpu_invalidate_projections",
 ]
 
 _LIB = None
@@ -254,6 +254,7 @@ def load_library():
     lib.rome_gpu_get_timings.argtypes = [C.c_void_p, C.POINTER(RomeGpuTimings)]
     lib.rome_gpu_reset_timings.argtypes = [C.c_void_p]
     lib.rome_gpu_wait_selftest.argtypes = [C.c_void_p, C.c_double, _DP]
+    lib.rome_gpu_invalidate_projections.argtypes = [C.c_void_p]
     lib.rome_gpu_backprojector_size.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
     lib.rome_gpu_backprojector_device_copy.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     lib.rome_gpu_tuning_report.argtypes = [C.c_char_p, C.c_size_t]

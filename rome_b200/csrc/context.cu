@@ -91,6 +91,13 @@ extern "C" int rome_gpu_set_precision(RomeGpuCtx* ctx, int precision) {
     });
 }
 
+extern "C" int rome_gpu_invalidate_projections(RomeGpuCtx* ctx) {
+    if (!ctx) return ROME_ERR_ARG;
+    ctx->proj_version++;
+    ctx->proj_key.clear();
+    return ROME_OK;
+}
+
 extern "C" int rome_gpu_set_projectors(RomeGpuCtx* ctx, int ref_dim, int nr_classes, int ori_size, int pad_size,
                                        int r_max, int padding_factor, const double* data) {
     if (!ctx) return ROME_ERR_ARG;

@@ -327,6 +327,10 @@ class GpuContext:
             self.lib.rome_gpu_destroy(self.h)
             self.h = None
 
+    def invalidate_projections(self) -> None:
+        """rome_gpu_invalidate_projections: the next pool recomputes the orientation projections."""
+        self._check(self.lib.rome_gpu_invalidate_projections(self.h))
+
     @property
     def torch_device(self) -> str:
         return f"cuda:{self.device}"
