@@ -682,7 +682,7 @@ def run_ours_3d(args):
     import torch
 
     from rome_b200.map2d import GpuContext
-    from rome_b200.map3d import map3d_estep_pool
+    from rome_b200.map3d import map3d_estep_pools_adaptive
     from rome_b200.particles import h2d_bytes as prep_h2d_bytes
     from rome_b200.particles import pin_particles, prepared_pool, prepared_stream
     from rome_b200.workload import CONFIGS, build_map3d, prep_options, raw_particles, slice_particles, subset3d
@@ -719,7 +719,7 @@ def run_ours_3d(args):
     host_raw = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
 
     def run_lanes(pools):
-        futs = [execs[q % len(lanes)].submit(map3d_estep_pool, lanes[q % len(lanes)], sp.pool, dev=sp.dev)
+        futs = [execs[q % len(lanes)].submit(map3d_estep_pools_adaptive, lanes[q % len(lanes)], sp.pool, sp.dev)
                 for q, sp in enumerate(pools)]
         res = [f.result() for f in futs]
         for c in lanes[1:]:
@@ -747,8 +747,8 @@ def run_ours_3d(args):
     if args.precision != "fp32":
         with GpuContext(0, "fp32") as c32:
             c32.set_projectors(proj, pool.ori_size, r_max)
-            map3d_estep_pool(c32, staged[0].pool, dev=staged[0].dev)
-            f_ms, f_res = _timed(torch, lambda: [map3d_estep_pool(c32, sp.pool, dev=sp.dev) for sp in staged], 1)
+            map3d_estep_pools_adaptive(c32, staged[0].pool, staged[0].dev)
+            f_ms, f_res = _timed(torch, lambda: [map3d_estep_pools_adaptive(c32, sp.pool, sp.dev) for sp in staged], 1)
         cat = lambda rs, k: np.concatenate([r[k] for r in rs])  # noqa: E731
         same = np.ones(N, bool)
         for k in ("cls", "rot", "tilt", "psi", "xoff", "yoff"):

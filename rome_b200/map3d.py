@@ -191,6 +191,45 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
     return o
 
 
+# per-particle outputs of map3d_estep_pool (the rest are the pool's model sums)
+_PER_PARTICLE = ("min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "rot", "tilt",
+                 "psi", "xoff", "yoff", "nr_sign", "cls")
+
+
+def map3d_estep_pools_adaptive(ctx: GpuContext, p: Map3dPool, dev: Optional[dict] = None,
+                               min_pool: int = 1) -> Dict[str, np.ndarray]:
+    """map3d_estep_pool for a pool whose fine pass may not fit: when the
+    union of the pool's coarse-significant orientations needs more device
+    memory for its fine projections than is free (the library refuses such a
+    pool with ROME_ERR_OOM before any output is written or back-projected),
+    the pool is split in halves, recursively, and the halves' results joined:
+    per-particle outputs concatenated, model sums added.  Broad posteriors
+    (noisy particles searched at HEALPix order 3) are what make this happen;
+    the reference runs such particles in the same pools, one at a time."""
+    from .map2d import RomeError
+    try:
+        return map3d_estep_pool(ctx, p, dev=dev)
+    except RomeError as e:
+        if e.code != abi.ROME_ERR_OOM or "fine pass" not in str(e) or p.nr_images <= max(1, min_pool):
+            raise
+    h = p.nr_images // 2
+    parts = []
+    for lo, hi in ((0, h), (h, p.nr_images)):
+        q = dataclasses.replace(p)
+        for name in ("Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf", "highres_Xi2",
+                     "old_offsetx", "old_offsety", "group"):
+            setattr(q, name, np.ascontiguousarray(getattr(p, name)[lo:hi]))
+        d = None if dev is None else {k: v[lo:hi] for k, v in dev.items()}
+        parts.append(map3d_estep_pools_adaptive(ctx, q, d, min_pool))
+    out = {}
+    for k in parts[0]:
+        if k in _PER_PARTICLE:
+            out[k] = np.concatenate([r[k] for r in parts])
+        else:
+            out[k] = sum(r[k] for r in parts)
+    return out
+
+
 def pool3d_from_dump(d: Dict[str, np.ndarray], pool: int = 0) -> Map3dPool:
     """The E-step inputs of one pool recorded by oracle/ref_harness/map3d_dump."""
     pp = f"pool{pool}_"
