@@ -526,10 +526,11 @@ CONFIGS = {
     # noise power per noise-level group, so the number of coarse-significant points varies widely.  The
     # SNR here is per Fourier component of the CTF-modulated projection; the decade [0.01, 0.1] on that
     # scale leaves the noisiest particles nearly uninformative (significant over most of the 3.8 M coarse
-    # hypotheses), so the decade is [0.05, 0.5], which puts the tail of the counts in the thousands
+    # hypotheses, tens of thousands of coarse orientations for one particle), so the decade is
+    # [0.06, 0.6], which puts the largest counts at a few thousand
     "map3d_cfg4": Map3dWorkload(n_particles=50000, ori_size=128, coarse_size=40, n_classes=8, n_blobs=60,
                                 blob_sigma=(2.0, 8.0), healpix_order=3, offset_range=4, offset_step=2, max_shift=4.0,
-                                pixel=1.5, snr=0.158, seed=4, snr_range=(0.05, 0.5), noisy_fraction=0.3,
+                                pixel=1.5, snr=0.19, seed=4, snr_range=(0.06, 0.6), noisy_fraction=0.3,
                                 noisy_factor=(2.0, 4.0), unique_particles=10000),
     "map3d_cfg3": Map3dWorkload(n_particles=10000, ori_size=128, coarse_size=20, n_classes=4, n_blobs=60,
                                 blob_sigma=(2.0, 8.0), healpix_order=2, offset_range=4, offset_step=2, max_shift=4.0,
