@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(SR_THREADS)
     __shared__ double leaf[SR_LEAF];
     __shared__ double red[32];
     __shared__ int ncand, nzero, nleaf;
-    __shared__ int s_digit, s_stop;
+    __shared__ int s_digit, s_leaf, s_stop;
     __shared__ double s_above;
     __shared__ long long s_above_n;
     double* pp = part + (long)i * 8;
@@ -628,14 +628,19 @@ __global__ void __launch_bounds__(SR_THREADS)
                 an += hcnt[q];
             }
             s_digit = dg;
+            // the decision every thread takes, made once here: reading hcnt after the barrier would race
+            // with the threads that already clear it for the next level
+            s_leaf = dg >= 0 && (hcnt[dg] <= (unsigned)SR_LEAF || shift == 0);
             s_above = above;
             s_above_n = an;
         }
         __syncthreads();
         const int dg = s_digit;
+        const bool to_leaf = s_leaf != 0;
+        __syncthreads();  // s_digit / s_leaf are rewritten by the next level
         if (dg < 0) break;  // the positive weights never exceed the threshold
         prefix = (prefix << width) | (unsigned long long)dg;
-        if (hcnt[dg] <= (unsigned)SR_LEAF || shift == 0) {
+        if (to_leaf) {
             leaf_ready = true;
             break;
         }
