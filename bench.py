@@ -742,6 +742,11 @@ def run_ours_3d(args):
     step_e2e()
     e_ms, _ = _timed(torch, step_e2e, max(1, args.steps))
     cls = np.concatenate([r["cls"] for r in last]) - 1
+    # the timed contexts' device memory is released before the comparison arm runs
+    for e in execs:
+        e.shutdown(wait=True)
+    for c in lanes:
+        c.close()
     # the plain FP32 E-step on the same prepared particles: the comparison arm and the pose judge
     judge = {}
     if args.precision != "fp32":
@@ -807,11 +812,7 @@ def run_ours_3d(args):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w)
-    for e in execs:
-        e.shutdown(wait=True)
     prep_ctx.close()
-    for c in lanes:
-        c.close()
     print(json.dumps(line), flush=True)
 
 
