@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define ROME_GPU_ABI_VERSION 3
+#define ROME_GPU_ABI_VERSION 4
 
 enum RomeStatus {
     ROME_OK = 0,
@@ -371,10 +371,18 @@ int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* in, RomeMap2
  * (:1610-1810), findAllSignificantPoints (:1812-1931), updateOtherParams
  * (:2059-2236, CoarseAndFineSearch::updateModel :1484-1602) and
  * backProjection (:2242-2506, MyBackProjector::backproject
- * src/reconstruct.cpp:977-1164).  Maximum-likelihood mode with
- * adaptive_oversampling 1 (the reference's 3D path always has the fine
- * pass); cross-correlation mode and scale correction return
- * ROME_ERR_UNSUPPORTED.  Projectors must be set with ref_dim 3.
+ * src/reconstruct.cpp:977-1164), with adaptive_oversampling 1 (the
+ * reference's 3D path always has the fine pass).  Maximum-likelihood mode,
+ * or cross-correlation mode (do_cross_correlation: the reference's
+ * (iter == 1 && do_firstiter_cc) || do_always_cc, :907): every hypothesis
+ * scored by -sum(Frefctf . X) / (|Frefctf| |X|) (get_diff, :1086-1102) and
+ * only the best one kept with weight 1 (:1626-1671).  Intensity-scale
+ * correction (do_scale_correction): each group's scale multiplies the
+ * references and the CTF of the back-projection (applyCtfToClass
+ * :1054-1066, :2274-2282) and the per-particle XA/AA spectra of
+ * updateModel (:1426-1502, :2090-2112) are returned.  Either mode with
+ * proposals returns ROME_ERR_UNSUPPORTED.  Projectors must be set with
+ * ref_dim 3.
  * ------------------------------------------------------------------- */
 typedef struct {
     int nr_images;
@@ -415,8 +423,8 @@ typedef struct {
     int do_ctf_correction;
     int refs_are_ctf_corrected;
     int do_map;
-    int do_scale_correction;         /* must be 0 */
-    int do_cross_correlation;        /* must be 0 */
+    int do_scale_correction;
+    int do_cross_correlation;
     int inputs_on_device;
     /* optional coarse-pass search restriction (no reference counterpart): per
      * particle nr_proposals coarse orientations j = (class * nr_dir + dir) *
@@ -426,6 +434,13 @@ typedef struct {
      * NULL: the exhaustive coarse pass of the reference. */
     const int* proposals;
     int nr_proposals;
+    /* with do_scale_correction: mlModel.scale_correction [nr_groups] and
+     * mlModel.data_vs_prior_class [nr_classes][ori_size/2+1] (the shells
+     * whose data_vs_prior exceeds 3 enter the XA/AA spectra); a scale is
+     * checked like check_scale (:1000-1018): NaN, Inf or > 10000 is
+     * ROME_ERR_NUMERIC, below 0.001 it is raised to 0.001 */
+    const double* scale_correction;
+    const double* data_vs_prior_class;
 } RomeMap3dPool;
 
 typedef struct {
@@ -466,6 +481,13 @@ typedef struct {
      * normalised weights summed per coarse orientation, [P][K * nr_dir * nr_psi]
      * (training targets of the proposal network) */
     double* post_coarse;
+    /* with do_scale_correction: exp_wsum_scale_correction_XA / _AA as
+     * updateOtherParams leaves them, [nr_images][ori_size/2+1] per resolution
+     * shell (overwritten, not accumulated; storeWeightedSums divides them by
+     * the scale and its square and adds them to the group spectra); NULL to
+     * skip */
+    double* wsum_scale_correction_XA;
+    double* wsum_scale_correction_AA;
 } RomeMap3dPoolOut;
 
 int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* in, RomeMap3dPoolOut* out);

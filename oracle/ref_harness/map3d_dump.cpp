@@ -63,6 +63,19 @@ void dump_model_sums(Dumper& d, const std::string& pre) {
     d.scalar(pre + "wsum_LL", mlModel.wsum_LL);
     d.scalar(pre + "wsum_ave_Pmax", mlModel.wsum_ave_Pmax);
     d.scalar(pre + "wsum_avg_norm_correction", mlModel.wsum_avg_norm_correction);
+    if (do_scale_correction) {
+        std::vector<double> xa((size_t)G * oF), aa((size_t)G * oF);
+        for (int g = 0; g < G; g++) {
+            auto px = mlModel.wsum_signal_product_spectra[g].wptr(oF);
+            auto pa = mlModel.wsum_reference_power_spectra[g].wptr(oF);
+            for (int n = 0; n < oF; n++) {
+                xa[(size_t)g * oF + n] = px[n];
+                aa[(size_t)g * oF + n] = pa[n];
+            }
+        }
+        d.f64(pre + "wsum_signal_product_spectra", xa.data(), {G, oF});
+        d.f64(pre + "wsum_reference_power_spectra", aa.data(), {G, oF});
+    }
 }
 
 void dump_backprojectors(Dumper& d, const std::string& pre) {
@@ -299,6 +312,7 @@ int main(int argc, char* argv[]) {
     d.iscalar("do_scale_correction", do_scale_correction);
     d.iscalar("do_norm_correction", do_norm_correction);
     d.iscalar("do_map", do_map);
+    d.iscalar("do_cross_correlation", (iter == 1 && do_firstiter_cc) || do_always_cc);
     d.scalar("sigma2_fudge", sigma2_fudge);
     d.scalar("adaptive_fraction", adaptive_fraction);
     d.scalar("pixel_size", pixel_size);
@@ -448,6 +462,13 @@ int main(int argc, char* argv[]) {
             }
             updateOtherParams();
             d.f64(pp + "wsum_norm_correction", exp_wsum_norm_correction.wptrAll(), {P});
+            if (do_scale_correction) {
+                // per-particle scale-correction spectra of updateOtherParams (before storeWeightedSums divides them)
+                auto xa = flat2(exp_wsum_scale_correction_XA, P, oF);
+                d.f64(pp + "wsum_scale_correction_XA", xa.data(), {P, oF});
+                auto aa = flat2(exp_wsum_scale_correction_AA, P, oF);
+                d.f64(pp + "wsum_scale_correction_AA", aa.data(), {P, oF});
+            }
             dump_model_sums(d, pp + "after_update_");
             backProjection();
             if (pool_index == 0) dump_backprojectors(d, pp + "after_bp_");

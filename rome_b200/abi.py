@@ -37,7 +37,7 @@ class RomeGpuConfig(C.Structure):
                 ("profile", C.c_int)]
 
 
-ABI_VERSION = 3  # ROME_GPU_ABI_VERSION of include/rome_gpu.h
+ABI_VERSION = 4  # ROME_GPU_ABI_VERSION of include/rome_gpu.h
 
 PHASES = ["prep", "project", "shift", "norm_gemm", "cross_gemm", "posterior", "wsum", "backproject", "reconstruct",
           "restricted", "propose", "images"]
@@ -92,6 +92,7 @@ class RomeMap3dPool(C.Structure):
         ("do_ctf_correction", C.c_int), ("refs_are_ctf_corrected", C.c_int), ("do_map", C.c_int),
         ("do_scale_correction", C.c_int), ("do_cross_correlation", C.c_int), ("inputs_on_device", C.c_int),
         ("proposals", _IP), ("nr_proposals", C.c_int),
+        ("scale_correction", _DP), ("data_vs_prior_class", _DP),
     ]
 
 
@@ -106,6 +107,7 @@ class RomeMap3dPoolOut(C.Structure):
         ("coarse_diff2", _DP), ("Mcoarse_significant", _CP),
         ("fine_capacity", C.c_long), ("fine_count", _IP), ("fine_index", C.POINTER(C.c_long)),
         ("fine_diff2", _DP), ("fine_weight", _DP), ("post_coarse", _DP),
+        ("wsum_scale_correction_XA", _DP), ("wsum_scale_correction_AA", _DP),
     ]
 
 

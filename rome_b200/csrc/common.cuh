@@ -110,6 +110,8 @@ enum Slot {
     S_ROTSIG,     // Rot_significant [K*npsi] char
     S_PAIRS,      // 3D fine pass: (particle, coarse translation) pair flags, ids and list
     S_SELEXACT,   // particles whose significance walk needs the exact sort
+    S_CCX,        // 3D cross-correlation mode: image norms of the pass [P] double
+    S_PSCALE,     // 3D intensity-scale correction: per-particle scale and its spectra [P] + [P][2][oriF] double
     S_ACTIDX,     // pixel -> active index [F] int
     S_TRANS,      // translations of the last pass [T] double2
     S_LISTCNT,    // list counter + per-orientation counts

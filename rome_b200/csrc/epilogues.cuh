@@ -74,7 +74,11 @@ struct BiasStoreEpi {
 // Hypotheses the reference skips (class/orientation not significant, or
 // coarse translation not significant in the fine pass) become +inf.  The
 // per-particle minimum (exp_min_diff2, src/map2d_optimizer.cpp:1043-1062)
-// is folded in with one atomicMin per row and tile.
+// is folded in with one atomicMin per row and tile.  With ccx (per particle
+// image norm |X|, exp_local_sqrtXi2) the epilogue writes the cross-correlation
+// mode's value -C / (sqrt(N) |X|) instead (get_diff,
+// src/map3d_optimizer.cpp:1086-1102; the operands then carry no
+// Minvsigma2, so C is the signal product and N the reference power).
 struct Diff2Epi {
     float* diff2;
     const float* norm;
@@ -87,20 +91,22 @@ struct Diff2Epi {
     long ncoarse;
     const char* mcoarse;
     unsigned* rowmin;  // per particle, float_key order; may be null
+    const double* ccx = nullptr;
     __device__ __forceinline__ float operator()(int m, int n, float c) const {
         int i = m / T, t = m - i * T;
         bool ok = jvalid[n] != 0;
         if (ok && mcoarse) ok = mcoarse[(long)i * ncoarse + (long)(n / nor) * ntr + t / notr] != 0;
         float v = INFINITY;
-        if (ok) v = (float)(0.5 * ((double)norm[(long)i * J + n] - 2.0 * (double)c + (double)S[m] + xi2[i]));
+        if (ok && ccx) v = (float)(-(double)c / (sqrt((double)norm[(long)i * J + n]) * ccx[i]));
+        else if (ok) v = (float)(0.5 * ((double)norm[(long)i * J + n] - 2.0 * (double)c + (double)S[m] + xi2[i]));
         diff2[(long)i * X + (long)n * T + t] = v;
         return v;
     }
     __device__ __forceinline__ void finish_row(int m, float v) const {
         if (rowmin && v < INFINITY) atomicMin(&rowmin[m / T], float_key(v));
     }
-    // per-row constants of a tile row: output base, S[m] + Xi2[i], the
-    // particle's norm row and Mcoarse row
+    // per-row constants of a tile row: output base, S[m] + Xi2[i] (cross-correlation
+    // mode: the image norm), the particle's norm row and Mcoarse row
     struct Row {
         long out;
         double rc;
@@ -109,7 +115,7 @@ struct Diff2Epi {
     };
     __device__ __forceinline__ Row row(int m) const {
         const int i = m / T, t = m - i * T;
-        return Row{(long)i * X + t, (double)S[m] + xi2[i], norm + (long)i * J,
+        return Row{(long)i * X + t, ccx ? ccx[i] : (double)S[m] + xi2[i], norm + (long)i * J,
                    mcoarse ? mcoarse + (long)i * ncoarse + t / notr : nullptr};
     }
     __device__ __forceinline__ float chunk16(const Row& r, int n, const float (&v)[16], int nvalid) const {
@@ -138,7 +144,9 @@ struct Diff2Epi {
             if (q >= nvalid) break;
             bool ok = jv[q] != 0;
             if (ok && r.mc) ok = r.mc[(long)((n + q) / nor) * ntr] != 0;
-            const float val = ok ? (float)(0.5 * ((double)nv[q] - 2.0 * (double)v[q] + r.rc)) : INFINITY;
+            const float val = !ok  ? INFINITY
+                              : ccx ? (float)(-(double)v[q] / (sqrt((double)nv[q]) * r.rc))
+                                    : (float)(0.5 * ((double)nv[q] - 2.0 * (double)v[q] + r.rc));
             diff2[r.out + (long)(n + q) * T] = val;
             mn = fminf(mn, val);
         }

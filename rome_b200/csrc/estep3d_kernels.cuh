@@ -125,6 +125,20 @@ __global__ void project3d_kernel(int J, int Kact, int Kp, int Kq, int cs, int cs
 }
 
 // ---------------------------------------------------------------------------
+// Cross-correlation mode: the norm of each particle's masked image at the
+// pass size, sqrt(sum_n |X_n|^2) over every coefficient of the window
+// (exp_local_sqrtXi2, src/exp_model.cpp:1037-1045).  One CTA per particle.
+__global__ void sqrt_xi2_kernel(int F, const double2* __restrict__ Fimg, double* __restrict__ out) {
+    __shared__ double red[32];
+    const int i = blockIdx.x;
+    const double2* X = Fimg + (long)i * F;
+    double s = 0.0;
+    for (int n = threadIdx.x; n < F; n += blockDim.x) s += X[n].x * X[n].x + X[n].y * X[n].y;
+    s = block_reduce_sum(s, red);
+    if (threadIdx.x == 0) out[i] = sqrt(s);
+}
+
+// ---------------------------------------------------------------------------
 // Fine pass: the coarse-significant points of every particle, in the
 // reference's list order (class, dir, psi, coarse translation ascending:
 // getAllSquaredDifferencesFine, src/map3d_optimizer.cpp:1261-1372, visits
@@ -251,7 +265,7 @@ __global__ void __launch_bounds__(NT)
                              int Kact, int Kp, const double2* __restrict__ Fimg, const double* __restrict__ lctf,
                              const double* __restrict__ Minv, int apply_ctf, const int* __restrict__ act,
                              const unsigned short* __restrict__ pidx, const double2* __restrict__ tab,
-                             float* __restrict__ A, float* __restrict__ S) {
+                             float* __restrict__ A, float* __restrict__ S, const double* __restrict__ pscale) {
     const int p = blockIdx.x;
     if (p >= npairs[0]) return;
     __shared__ float2 stab[5000];
@@ -259,19 +273,21 @@ __global__ void __launch_bounds__(NT)
     const int q = pair_of[p], i = q / ntr, itr = q - i * ntr;
     for (int k = threadIdx.x; k < 5000; k += NT) stab[k] = make_float2((float)tab[k].x, (float)tab[k].y);
     const double2* X = Fimg + (long)i * F;
-    const double* M = Minv + (long)i * F;
+    const double* M = Minv ? Minv + (long)i * F : nullptr;  // null: cross-correlation mode, no weighting
     const double* C = lctf + (long)i * F;
+    const double sc = pscale ? pscale[i] : 1.0;  // the group's intensity scale on the reference
     double s = 0.0;
     for (int n = threadIdx.x; n < F; n += NT) {
         const double2 v = X[n];
-        s += M[n] * (v.x * v.x + v.y * v.y);
+        s += (M ? M[n] : 1.0) * (v.x * v.x + v.y * v.y);
     }
     s = block_reduce_sum(s, red);
     for (int a = threadIdx.x; a < Kp / 2; a += NT) {
         float2 xw = make_float2(0.f, 0.f);
         if (a < Kact) {
             const int n = act[a];
-            const double w = apply_ctf ? M[n] * C[n] : M[n];
+            const double m = M ? M[n] : 1.0;
+            const double w = (apply_ctf ? m * C[n] : m) * sc;
             xw = make_float2((float)(w * X[n].x), (float)(w * X[n].y));
         }
         for (int t = 0; t < notr; t++) {
@@ -307,7 +323,7 @@ __global__ void __launch_bounds__(NT)
     fine_diff2_kernel(int ntr, int Kp, int Kq, const int4* __restrict__ fe, const int* __restrict__ pid,
                       const float* __restrict__ A, const float* __restrict__ B, const float* __restrict__ W2,
                       const float* __restrict__ Q, const float* __restrict__ S, const double* __restrict__ xi2,
-                      float* __restrict__ diff2, unsigned* __restrict__ rowmin) {
+                      float* __restrict__ diff2, unsigned* __restrict__ rowmin, const double* __restrict__ ccx) {
     constexpr int NH = NOR * NOTR;
     static_assert(NH == 32, "one warp holds the 32 sub-hypotheses of a point");
     __shared__ double red[NT / 32][NH + NOR];
@@ -361,7 +377,10 @@ __global__ void __launch_bounds__(NT)
             cs += red[w][h];
             ns += red[w][NH + o];
         }
-        const float v = (float)(0.5 * (ns - 2.0 * cs + (double)S[arow + t] + xi2[i]));
+        // cross-correlation mode (ccx = the particle's image norms): -C / (sqrt(N) * |X|), get_diff,
+        // src/map3d_optimizer.cpp:1086-1102
+        const float v = ccx ? (float)(-cs / (sqrt(ns) * ccx[i]))
+                            : (float)(0.5 * (ns - 2.0 * cs + (double)S[arow + t] + xi2[i]));
         diff2[(long)blockIdx.x * NH + h] = v;  // point blockIdx.x = off[i] + r of the ragged rows
         float m = v;
         for (int off = 16; off > 0; off >>= 1) m = fminf(m, __shfl_down_sync(0xffffffffu, m, off));
@@ -393,7 +412,18 @@ __global__ void fine_list_dense_kernel(int n, int nor, int notr, int Tf, int str
 // wsum_pdf_class, wsum_pdf_direction[class][dir] and wsum_sigma2_offset.
 // jcd[j] = class * ndir + dir of fine orientation j.  wk: [0,K) pdf_class,
 // [K, K + K*ndir) pdf_direction, then sigma2_offset, then [G] sumw_group.
-template <int NT, int PIX>
+// SCALE (intensity-scale correction): the reference is Frefctf times the
+// particle's scale sc.pscale[i], and the pixels of the shells whose
+// data_vs_prior of the hypothesis' class exceeds 3 also add
+// w * Re(Frefctf conj(X)) and w * |Frefctf|^2 to the particle's XA and AA
+// spectra (get_wdiff2 'S' pixels, src/map3d_optimizer.cpp:1488-1502).
+struct ScaleSums {
+    const double* pscale = nullptr;  // [P]
+    const double* dvp = nullptr;     // data_vs_prior_class [K][oriF]
+    double* xa = nullptr;            // [P][oriF]
+    double* aa = nullptr;            // [P][oriF]
+};
+template <int NT, int PIX, bool SCALE>
 __global__ void __launch_bounds__(NT)
     wsum3d_list_kernel(int T, int K, int ndir, int F, int csF, int cs, int oriF, const SigEntry* __restrict__ list,
                        const int* __restrict__ seg, const int* __restrict__ jcd, const double2* __restrict__ Fimg,
@@ -402,7 +432,8 @@ __global__ void __launch_bounds__(NT)
                        const double2* __restrict__ ph, const int* __restrict__ Mresol, const int* __restrict__ group,
                        const double2* __restrict__ oldoff, const double2* __restrict__ trans,
                        const double* __restrict__ priorx, const double* __restrict__ priory,
-                       double* __restrict__ wsn, double* __restrict__ normcorr, double* __restrict__ wk, int chunk) {
+                       double* __restrict__ wsn, double* __restrict__ normcorr, double* __restrict__ wk, int chunk,
+                       ScaleSums sc) {
     const int i = blockIdx.y;
     const int n0 = blockIdx.x * NT * PIX;
     // blockIdx.z takes entries [z * chunk, (z + 1) * chunk) of the particle's segment, so that a particle
@@ -412,16 +443,22 @@ __global__ void __launch_bounds__(NT)
     const int s0 = seg[2 * i] + z0, ns = min(chunk, seg[2 * i + 1] - z0);
     __shared__ double spec[1024];
     __shared__ double red[32];
-    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) spec[q] = 0.0;
+    __shared__ double sxa[SCALE ? 1024 : 1], saa[SCALE ? 1024 : 1];
+    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) {
+        spec[q] = 0.0;
+        if (SCALE) sxa[q] = saa[q] = 0.0;
+    }
     __syncthreads();
-    double acc[PIX];
+    double acc[PIX], axa[SCALE ? PIX : 1], aaa[SCALE ? PIX : 1];
     int ires_p[PIX];
     double2 Xp[PIX];
     double cp[PIX];
     int ap[PIX];
+    const double psc = SCALE ? sc.pscale[i] : 1.0;
 #pragma unroll
     for (int p = 0; p < PIX; p++) {
         acc[p] = 0.0;
+        if (SCALE) axa[p] = aaa[p] = 0.0;
         const int n = n0 + threadIdx.x + p * NT;
         ires_p[p] = n < F ? Mresol[n] : -1;
         if (ires_p[p] > -1) {
@@ -440,17 +477,26 @@ __global__ void __launch_bounds__(NT)
         const double w = s.w;
         const double2 sh = shifts[t];
         const double2* Pj = proj + (long)j * Kact;
+        const double* dv = SCALE ? sc.dvp + (long)(jcd[j] / ndir) * oriF : nullptr;
 #pragma unroll
         for (int p = 0; p < PIX; p++) {
             if (ires_p[p] > -1) {
                 const double2 v = apply_phase(sh, ph[(long)t * F + n0 + threadIdx.x + p * NT], Xp[p]);
                 const double2 pv = ap[p] >= 0 ? Pj[ap[p]] : make_double2(0.0, 0.0);
-                const double pr = apply_ctf ? dmul(pv.x, cp[p]) : pv.x;
-                const double pim = apply_ctf ? dmul(pv.y, cp[p]) : pv.y;
+                double pr = apply_ctf ? dmul(pv.x, cp[p]) : pv.x;
+                double pim = apply_ctf ? dmul(pv.y, cp[p]) : pv.y;
+                if (SCALE) {
+                    pr = dmul(pr, psc);
+                    pim = dmul(pim, psc);
+                }
                 const double dr = dsub(pr, v.x), di = dsub(pim, v.y);
                 const double wd = dmul(w, dadd(dmul(dr, dr), dmul(di, di)));
                 acc[p] += wd;
                 sumwd += wd;
+                if (SCALE && dv[ires_p[p]] > 3.) {
+                    axa[p] += dmul(w, dadd(dmul(pr, v.x), dmul(pim, v.y)));
+                    aaa[p] += dmul(w, dadd(dmul(pr, pr), dmul(pim, pim)));
+                }
             }
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -464,12 +510,20 @@ __global__ void __launch_bounds__(NT)
         }
     }
 #pragma unroll
-    for (int p = 0; p < PIX; p++)
+    for (int p = 0; p < PIX; p++) {
         if (ires_p[p] > -1 && ires_p[p] < 1024 && acc[p] != 0.0) atomicAdd(&spec[ires_p[p]], acc[p]);
+        if (SCALE && ires_p[p] > -1 && ires_p[p] < 1024 && (axa[p] != 0.0 || aaa[p] != 0.0)) {
+            atomicAdd(&sxa[ires_p[p]], axa[p]);
+            atomicAdd(&saa[ires_p[p]], aaa[p]);
+        }
+    }
     sumwd = block_reduce_sum(sumwd, red);
     __syncthreads();
-    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT)
+    for (int q = threadIdx.x; q < oriF && q < 1024; q += NT) {
         if (spec[q] != 0.0) atomicAdd(&wsn[(long)g * oriF + q], spec[q]);
+        if (SCALE && sxa[q] != 0.0) atomicAdd(&sc.xa[(long)i * oriF + q], sxa[q]);
+        if (SCALE && saa[q] != 0.0) atomicAdd(&sc.aa[(long)i * oriF + q], saa[q]);
+    }
     if (threadIdx.x == 0 && sumwd != 0.0) atomicAdd(&normcorr[i], sumwd);
 }
 

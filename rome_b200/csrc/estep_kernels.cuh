@@ -98,25 +98,30 @@ __global__ void phase_index_kernel(int T, int Kact, int csF, int cs, const int* 
 // its own rounding), and S = sum_n Minvsigma2 |X|^2 over all pixels in FP64
 // (a phase shift leaves |X|^2 unchanged up to rounding, so S is the same
 // for every translation).  One CTA per particle; the 5000-entry table is
-// staged in shared memory as float2.
+// staged in shared memory as float2.  Minv null: no Minvsigma2 weighting
+// (the cross-correlation mode's signal product).  pscale (per particle,
+// may be null): the group's intensity scale, which multiplies the
+// reference (applyCtfToClass, src/map3d_optimizer.cpp:1054-1066) and so
+// the cross term once.
 template <int NT>
 __global__ void __launch_bounds__(NT)
     shift_operand2_kernel(int P, int T, int F, int Kact, int Kp, const double2* __restrict__ Fimg,
                           const double* __restrict__ lctf, const double* __restrict__ Minv, int apply_ctf,
                           const int* __restrict__ act, const unsigned short* __restrict__ pidx,
                           const double2* __restrict__ tab, void* __restrict__ Aop, float* __restrict__ S,
-                          int precision) {
+                          int precision, const double* __restrict__ pscale = nullptr) {
     __shared__ float2 stab[5000];
     __shared__ double red[32];
     const int i = blockIdx.x;
     for (int q = threadIdx.x; q < 5000; q += NT) stab[q] = make_float2((float)tab[q].x, (float)tab[q].y);
     const double2* X = Fimg + (long)i * F;
-    const double* M = Minv + (long)i * F;
+    const double* M = Minv ? Minv + (long)i * F : nullptr;
     const double* C = lctf + (long)i * F;
+    const double sc = pscale ? pscale[i] : 1.0;
     double s = 0.0;
     for (int n = threadIdx.x; n < F; n += NT) {
         double2 v = X[n];
-        s += M[n] * (v.x * v.x + v.y * v.y);
+        s += (M ? M[n] : 1.0) * (v.x * v.x + v.y * v.y);
     }
     s = block_reduce_sum(s, red);  // includes a __syncthreads after the table fill
     const long M2 = (long)P * T;
@@ -126,7 +131,8 @@ __global__ void __launch_bounds__(NT)
         float2 xw = make_float2(0.f, 0.f);
         if (a < Kact) {
             int n = act[a];
-            double w = apply_ctf ? M[n] * C[n] : M[n];
+            const double m = M ? M[n] : 1.0;
+            double w = (apply_ctf ? m * C[n] : m) * sc;
             xw = make_float2((float)(w * X[n].x), (float)(w * X[n].y));
         }
         for (int t = 0; t < T; t++) {
@@ -421,16 +427,20 @@ __global__ void shift_operand_kernel(int P, int T, int F, int csF, int cs, int K
     }
 }
 
-// norm-term operand Minvsigma2 * ctf^2 on the active pixels
+// norm-term operand Minvsigma2 * ctf^2 on the active pixels (Minv null:
+// ctf^2 alone, the reference power of the cross-correlation mode); times
+// the square of the particle's intensity scale when pscale is given
 __global__ void w2_kernel(int P, int Kact, int Kq, const int* __restrict__ act, const double* __restrict__ lctf,
-                          const double* __restrict__ Minv, int F, int apply_ctf, float* __restrict__ W2) {
+                          const double* __restrict__ Minv, int F, int apply_ctf, float* __restrict__ W2,
+                          const double* __restrict__ pscale = nullptr) {
     const int i = blockIdx.x;
+    const double sc = pscale ? pscale[i] : 1.0;
     for (int a = threadIdx.x; a < Kq; a += blockDim.x) {
         float v = 0.f;
         if (a < Kact) {
             long n = (long)i * F + act[a];
-            double c = apply_ctf ? lctf[n] : 1.0;
-            v = (float)(Minv[n] * c * c);
+            double c = (apply_ctf ? lctf[n] : 1.0) * sc;
+            v = (float)((Minv ? Minv[n] : 1.0) * c * c);
         }
         W2[(long)i * Kq + a] = v;
     }
@@ -527,12 +537,14 @@ __device__ TVal block_reduce_sum(TVal v, TVal* sh) {
 
 // backProjection preparation (src/map2d_optimizer.cpp:1670-1737): origin of
 // Minvsigma2 restored, Minvsigma2 -> 1 without MAP, CTF -> 1 without CTF
-// correction; nomask image times ctf*Minvsigma2 and Mctf2 = ctf^2*Minvsigma2.
+// correction, then CTF times the group's intensity scale with scale
+// correction (pscale, src/map3d_optimizer.cpp:2274-2282); nomask image times
+// ctf*Minvsigma2 and Mctf2 = ctf^2*Minvsigma2.
 __global__ void bp_prep_kernel(int P, int F, const double* __restrict__ Fnr, const double* __restrict__ Fni,
                                const double* __restrict__ lctf, double* __restrict__ Minv,
                                const double* __restrict__ sigma2, const int* __restrict__ group, int oriF, double fudge,
                                int do_map, int do_ctf, double2* __restrict__ Fnm, double* __restrict__ Mctf2,
-                               const int* __restrict__ rows = nullptr) {
+                               const int* __restrict__ rows = nullptr, const double* __restrict__ pscale = nullptr) {
     const int i = blockIdx.x;
     const long ri = rows ? rows[i] : i;
     for (int n = threadIdx.x; n < F; n += blockDim.x) {
@@ -541,6 +553,7 @@ __global__ void bp_prep_kernel(int P, int F, const double* __restrict__ Fnr, con
         if (n == 0) m = 1. / (fudge * sigma2[(long)group[i] * oriF + 0]);
         if (!do_map) m = 1.0;
         double c = do_ctf ? lctf[q] : 1.0;
+        if (pscale) c = dmul(c, pscale[i]);
         double mc = dmul(c, m);
         Fnm[q] = make_double2(dmul(Fnr[qi], mc), dmul(Fni[qi], mc));
         Mctf2[q] = dmul(c, mc);

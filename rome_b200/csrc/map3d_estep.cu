@@ -17,6 +17,12 @@
 // differences of their 32 sub-hypotheses (fine_diff2_kernel), the posterior
 // over the ragged rows, then updateOtherParams and backProjection over the
 // significant fine hypotheses.
+//
+// Cross-correlation mode replaces the squared difference by the negative
+// normalised correlation and the posterior by the single best hypothesis;
+// intensity-scale correction multiplies the references (and the
+// back-projection's CTF) by each particle's group scale and adds the XA/AA
+// spectra to updateOtherParams.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -109,8 +115,6 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                      in->coarse_size);
         if (in->adaptive_oversampling != 1)
             fail(ROME_ERR_UNSUPPORTED, "3D E-step needs adaptive_oversampling 1 (got %d)", in->adaptive_oversampling);
-        if (in->do_scale_correction) fail(ROME_ERR_UNSUPPORTED, "scale correction is not supported");
-        if (in->do_cross_correlation) fail(ROME_ERR_UNSUPPORTED, "cross-correlation mode is not supported");
         ROME_REQUIRE(in->iclass_min >= 0 && in->iclass_max < K && in->iclass_min <= in->iclass_max, "bad class range");
         ROME_REQUIRE(ctx->r_max == std::min(cur / 2, ori / 2), "projector r_max %d does not match current_size %d",
                      ctx->r_max, cur);
@@ -134,6 +138,27 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         // optional coarse-pass restriction (learned proposals): validated on the host
         const bool restricted = in->proposals != nullptr;
         const int nprop = restricted ? in->nr_proposals : 0;
+        // cross-correlation mode (-firstiter_cc in iteration 1, -always_cc): normalised signal products
+        // instead of squared differences, and the best hypothesis alone instead of the posterior
+        const bool ccm = in->do_cross_correlation != 0;
+        if (ccm && restricted) fail(ROME_ERR_UNSUPPORTED, "cross-correlation mode with proposals");
+        // intensity-scale correction: per-particle scale of its group (check_scale, map3d_optimizer.cpp:1000-1018)
+        const bool scl = in->do_scale_correction != 0;
+        if (scl && restricted) fail(ROME_ERR_UNSUPPORTED, "scale correction with proposals");
+        std::vector<double> hscale;
+        if (scl) {
+            ROME_REQUIRE(in->scale_correction && in->data_vs_prior_class,
+                         "scale correction needs scale_correction and data_vs_prior_class");
+            hscale.resize(P);
+            for (int i = 0; i < P; i++) {
+                const int gi = in->group[i];
+                ROME_REQUIRE(gi >= 0 && gi < G, "group %d of particle %d out of range", gi, i);
+                double sc = in->scale_correction[gi];
+                if (std::isnan(sc) || std::isinf(sc)) fail(ROME_ERR_NUMERIC, "Scale is Nan or Inf (group %d)", gi + 1);
+                if (sc > 10000.) fail(ROME_ERR_NUMERIC, "scale correction %g of group %d is very high", sc, gi + 1);
+                hscale[i] = sc < 0.001 ? 0.001 : sc;
+            }
+        }
         int* dProp = nullptr;
         if (restricted) {
             ROME_REQUIRE(nprop > 0 && nprop <= Jc, "nr_proposals %d (1..%d)", nprop, Jc);
@@ -172,6 +197,16 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         double* dSig2 = upload3(ctx, S_SIG2, in->sigma2_noise, (size_t)G * oriF);
         int* dGroup = upload3(ctx, S_GROUP, in->group, (size_t)P);
         double* dXi2 = upload3(ctx, S_XI2, in->highres_Xi2, (size_t)P);
+        double* dScale = nullptr;  // [P] scales, then XA [P][oriF], AA [P][oriF]
+        ScaleSums ssum;
+        if (scl) {
+            dScale = ctx->ws[S_PSCALE].as<double>((size_t)P * (1 + 2 * oriF) + (size_t)K * oriF);
+            stage_copy(ctx, dScale, hscale.data(), (size_t)P);
+            double* dDvp = dScale + (size_t)P * (1 + 2 * oriF);
+            stage_copy(ctx, dDvp, in->data_vs_prior_class, (size_t)K * oriF);
+            ROME_CUDA(cudaMemsetAsync(dScale + P, 0, sizeof(double) * 2 * P * oriF, st));
+            ssum = ScaleSums{dScale, dDvp, dScale + P, dScale + P + (size_t)P * oriF};
+        }
         // model values: pdf_direction [K*ndir], prior offsets [K] x 2
         std::vector<double> hcls((size_t)KD + 2 * K);
         for (int q = 0; q < KD; q++) hcls[q] = in->pdf_direction[q];
@@ -246,6 +281,13 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                                                       in->sigma2_fudge, dFimg, dLctf, dMinv);
             ROME_CHECK_LAUNCH();
             prof.launched(ROME_PHASE_PREP);
+            double* dSx = nullptr;
+            if (ccm) {
+                dSx = ctx->ws[S_CCX].as<double>((size_t)P);
+                sqrt_xi2_kernel<<<P, 256, 0, st>>>(g.F, dFimg, dSx);
+                ROME_CHECK_LAUNCH();
+                prof.launched(ROME_PHASE_PREP);
+            }
             prof.end(ROME_PHASE_PREP);
 
             float* dQ = ctx->ws[S_Q].as<float>((size_t)J * g.Kq);
@@ -283,11 +325,13 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             } else {
                 dA = ctx->ws[S_A].get((size_t)M * g.Kp * 4);
                 dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
-                shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMinv,
+                // cross-correlation mode: no Minvsigma2 in either operand
+                const double* dMw = ccm ? nullptr : dMinv;
+                shift_operand2_kernel<256><<<P, 256, 0, st>>>(P, T, g.F, g.Kact, g.Kp, dFimg, dLctf, dMw,
                                                                apply_ctf ? 1 : 0, dAct, dPidx, ctx->d_shift_tab, dA,
-                                                               dS, ctx->precision);
+                                                               dS, ctx->precision, dScale);
                 ROME_CHECK_LAUNCH();
-                w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+                w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMw, g.F, apply_ctf ? 1 : 0, dW2, dScale);
                 ROME_CHECK_LAUNCH();
             }
             prof.launched(ROME_PHASE_SHIFT, 3);
@@ -316,7 +360,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                 prof.add_flops(ROME_PHASE_NORM_GEMM, 2.0 * P * J * g.Kact);
                 prof.end(ROME_PHASE_NORM_GEMM);
 
-                Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJ, T, J, X, 1, 1, ntr, ncoarse, nullptr, dRowMin};
+                Diff2Epi epi{dDiff2, dNorm, dS, dXi2, dJ, T, J, X, 1, 1, ntr, ncoarse, nullptr, dRowMin, dSx};
                 prof.begin(ROME_PHASE_CROSS_GEMM);
                 if (!tc) sgemm_tn(st, (int)M, J, g.Kp, (const float*)dA, g.Kp, (const float*)dB, g.Kp, epi);
                 else tc_diff2_gemm(st, (int)M, J, g.Kp, dA, dB, ctx->precision, epi, ctx->d_err);
@@ -370,8 +414,11 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)P * Xrow);  // diff2 read once
             for (;;) {
                 dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap);
-                SelectResult sr = run_select(ctx, st, 0, P, Xrow, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
-                                             dPart, dPartI, nullptr, nullptr, dList, dCounter, listcap, dSeg, dRowMin);
+                SelectResult sr = ccm ? run_select_cc(st, P, Xrow, Lp, dDiff2, dPart, dPartI, nullptr, dList,
+                                                      dCounter, listcap, dSeg)
+                                      : run_select(ctx, st, 0, P, Xrow, Lp, dDiff2, dPdir, dPoff, in->adaptive_fraction,
+                                                   dPart, dPartI, nullptr, nullptr, dList, dCounter, listcap, dSeg,
+                                                   dRowMin);
                 prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
                 nsig = sr.nlist;
                 if (sr.nlist <= listcap) break;
@@ -505,6 +552,14 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                                                   in->sigma2_fudge, dFimg, dLctf, dMinv);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_PREP);
+        double* dSx = nullptr;
+        if (ccm) {
+            dSx = ctx->ws[S_CCX].as<double>((size_t)P);
+            sqrt_xi2_kernel<<<P, 256, 0, st>>>(g.F, dFimg, dSx);
+            ROME_CHECK_LAUNCH();
+            prof.launched(ROME_PHASE_PREP);
+        }
+        const double* dMw = ccm ? nullptr : dMinv;  // operands without Minvsigma2 in cross-correlation mode
         prof.end(ROME_PHASE_PREP);
 
         // fine projections: FP64 for wsum/backprojection, FP32 operands for diff2
@@ -525,7 +580,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         phase_index_kernel<<<(unsigned)(((long)Tf * g.Kact + 255) / 256), 256, 0, st>>>(
             Tf, g.Kact, g.csF, cur, dAct, dShift, ctx->shift_sampling, dPidx);
         ROME_CHECK_LAUNCH();
-        w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMinv, g.F, apply_ctf ? 1 : 0, dW2);
+        w2_kernel<<<P, 256, 0, st>>>(P, g.Kact, g.Kq, dAct, dLctf, dMw, g.F, apply_ctf ? 1 : 0, dW2, dScale);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_SHIFT, 2);
         prof.end(ROME_PHASE_SHIFT);
@@ -571,8 +626,8 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         fine_pair_list_kernel<<<(NPT + 255) / 256, 256, 0, st>>>(NPT, dPairFlag, dPairId, dPairOf);
         ROME_CHECK_LAUNCH();
         fine_pair_operand_kernel<256><<<pair_cap, 256, 0, st>>>(dPairId + NPT, dPairOf, ntr, NOTR, g.F, g.Kact, g.Kp,
-                                                                dFimg, dLctf, dMinv, apply_ctf ? 1 : 0, dAct, dPidx,
-                                                                ctx->d_shift_tab, dA, dS);
+                                                                dFimg, dLctf, dMw, apply_ctf ? 1 : 0, dAct, dPidx,
+                                                                ctx->d_shift_tab, dA, dS, dScale);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_SHIFT, 4);
         prof.add_bytes(ROME_PHASE_SHIFT, 4.0 * pair_cap * NOTR * g.Kp);
@@ -588,7 +643,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         ROME_CUDA(cudaMemsetAsync(dRowMin, 0xFF, sizeof(unsigned) * P, st));
         if (E > 0) {
             fine_diff2_kernel<128, 8, 4><<<E, 128, 0, st>>>(ntr, g.Kp, g.Kq, dFe, dPairId, dA, dB, dW2, dQ, dS, dXi2,
-                                                          dDiff2, dRowMin);
+                                                          dDiff2, dRowMin, dSx);
             ROME_CHECK_LAUNCH();
         }
         if (E > 0) prof.launched(ROME_PHASE_CROSS_GEMM);
@@ -612,8 +667,10 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         prof.add_bytes(ROME_PHASE_POSTERIOR, 4.0 * (double)E * NH);  // diff2 rows read once
         for (;;) {
             dList = ctx->ws[S_SIGLIST].as<SigEntry>((size_t)listcap * 2);
-            SelectResult sr = run_select(ctx, st, 0, P, Xf, Lf, dDiff2, dPdir, dPoff, in->adaptive_fraction, dPart,
-                                         dPartI, nullptr, dW, dList, dCounter, listcap, dSeg, dRowMin);
+            SelectResult sr = ccm ? run_select_cc(st, P, Xf, Lf, dDiff2, dPart, dPartI, dW, dList, dCounter, listcap,
+                                                  dSeg)
+                                  : run_select(ctx, st, 0, P, Xf, Lf, dDiff2, dPdir, dPoff, in->adaptive_fraction,
+                                               dPart, dPartI, nullptr, dW, dList, dCounter, listcap, dSeg, dRowMin);
             prof.launched(ROME_PHASE_POSTERIOR, sr.launches);
             nsig = sr.nlist;
             if (sr.nlist <= listcap) break;
@@ -701,9 +758,16 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         const int WCH = 256;
         const int nzch = std::min(65535, (maxseg + WCH - 1) / WCH);
         const int wchunk = (maxseg + nzch - 1) / nzch;
-        wsum3d_list_kernel<NT, PIX><<<dim3(nsplit, P, nzch), NT, 0, st>>>(
-            Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj, dActIdx,
-            g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk, wchunk);
+        if (scl)
+            wsum3d_list_kernel<NT, PIX, true><<<dim3(nsplit, P, nzch), NT, 0, st>>>(
+                Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj,
+                dActIdx, g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk, wchunk,
+                ssum);
+        else
+            wsum3d_list_kernel<NT, PIX, false><<<dim3(nsplit, P, nzch), NT, 0, st>>>(
+                Tf, K, ndir, g.F, g.csF, cur, oriF, dList, dSeg, dJf + Jf, dFimg, dLctf, apply_ctf ? 1 : 0, dProj,
+                dActIdx, g.Kact, dShift, dPh, dMresF, dGroup, dOld, dTr, dPriorX, dPriorY, dWsn, dNormCorr, dWk, wchunk,
+                ssum);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_WSUM);
         prof.end(ROME_PHASE_WSUM);
@@ -714,7 +778,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             double* dMctf2 = dMinv;  // becomes ctf^2 * Minvsigma2 in place
             prof.begin(ROME_PHASE_BACKPROJECT);
             bp_prep_kernel<<<P, 256, 0, st>>>(P, g.F, dFnr, dFni, dLctf, dMinv, dSig2, dGroup, oriF, in->sigma2_fudge,
-                                              in->do_map, in->do_ctf_correction, dFnm, dMctf2);
+                                              in->do_map, in->do_ctf_correction, dFnm, dMctf2, nullptr, dScale);
             ROME_CHECK_LAUNCH();
             int* dJcnt = dCounter + 2;
             int* dJoff = ctx->ws[S_REC_SMALL].as<int>((size_t)2 * Jf + 2);
@@ -746,6 +810,12 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         std::vector<double> hwsn((size_t)G * oriF + P), hwk(nwk);
         ROME_CUDA(cudaMemcpyAsync(hwsn.data(), dWsn, sizeof(double) * hwsn.size(), cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaMemcpyAsync(hwk.data(), dWk, sizeof(double) * hwk.size(), cudaMemcpyDeviceToHost, st));
+        if (scl && out->wsum_scale_correction_XA)
+            ROME_CUDA(cudaMemcpyAsync(out->wsum_scale_correction_XA, ssum.xa, sizeof(double) * P * oriF,
+                                      cudaMemcpyDeviceToHost, st));
+        if (scl && out->wsum_scale_correction_AA)
+            ROME_CUDA(cudaMemcpyAsync(out->wsum_scale_correction_AA, ssum.aa, sizeof(double) * P * oriF,
+                                      cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
         prof.collect();
         for (size_t q = 0; q < (size_t)G * oriF; q++) out->wsum_sigma2_noise[q] += hwsn[q];

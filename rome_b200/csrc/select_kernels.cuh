@@ -790,6 +790,83 @@ __global__ void mcoarse_from_list_kernel(int n, long X, const SigEntry* __restri
     if (q < n) mcoarse[(long)list[q].i * X + list[q].e] = 1;
 }
 
+// Cross-correlation mode (convertSquaredDifferencesToWeights with
+// do_cross_correlation, src/map3d_optimizer.cpp:1626-1671): no
+// marginalisation.  The computed hypothesis with the smallest diff2 (the
+// largest normalised correlation; the first one in the reference's loop
+// order, which is the row order, at a tie) gets weight 1 and every other
+// weight is 0, so exp_sum_weight = 1, PMAX = 1, and the significance walk
+// over that single listed weight (findAllSignificantPoints,
+// :1812-1931) gives significant_weight = 1 and NR_SIGN = 1.  One CTA per
+// particle; the part/parti layout and the list segment are those of
+// post_select2_kernel.  A row with no computed hypothesis reports
+// sum_weight 0 and no significant point.
+__global__ void __launch_bounds__(SEL2_THREADS)
+    cc_select_kernel(long Xrow, PostLayout L, const float* __restrict__ diff2, double* __restrict__ part,
+                     int* __restrict__ parti, double* __restrict__ wout, SigEntry* __restrict__ list,
+                     int* __restrict__ counter, int cap, int* __restrict__ seg) {
+    __shared__ float sv[32];
+    __shared__ long se[32];
+    const int i = blockIdx.x;
+    const long X = L.roff ? (long)(L.roff[i + 1] - L.roff[i]) * L.epr : Xrow;
+    const long rb = L.roff ? (long)L.roff[i] * L.epr : (long)i * Xrow;
+    const float* d = diff2 + rb;
+    float best = INFINITY;
+    long be = LONG_MAX;
+    for (long e = threadIdx.x; e < X; e += blockDim.x) {
+        const float v = d[e];
+        if (v < best) {  // e rises within a thread: its first minimum is kept
+            best = v;
+            be = e;
+        }
+        if (wout) wout[rb + e] = 0.0;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_down_sync(0xffffffffu, best, off);
+        const long oe = __shfl_down_sync(0xffffffffu, be, off);
+        if (ov < best || (ov == best && oe < be)) {
+            best = ov;
+            be = oe;
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        sv[threadIdx.x >> 5] = best;
+        se[threadIdx.x >> 5] = be;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+            if (sv[w] < best || (sv[w] == best && se[w] < be)) {
+                best = sv[w];
+                be = se[w];
+            }
+        const bool found = best < INFINITY;
+        double* pp = part + (long)i * 8;
+        int* pi = parti + (long)i * 8;
+        pp[0] = found ? (double)best : (double)INFINITY;
+        pp[1] = found ? 1.0 : 0.0;
+        pp[2] = found ? 1.0 : 0.0;
+        pp[3] = 0.0;
+        pp[4] = found ? 1.0 : 0.0;
+        pp[5] = found ? (double)best : (double)INFINITY;
+        pp[6] = 0.0;
+        pp[7] = 0.0;
+        int base = 0;
+        if (list) {
+            base = found ? atomicAdd(counter, 1) : 0;
+            seg[2 * i] = base;
+            seg[2 * i + 1] = found ? 1 : 0;
+            if (found && base < cap) list[base] = SigEntry{i, (int)be, 1.0};
+        }
+        if (wout && found) wout[rb + be] = 1.0;
+        pi[0] = found ? (int)be : 0;
+        pi[1] = found ? 1 : 0;
+        pi[2] = 0;
+        pi[3] = found ? 1 : 0;
+        pi[4] = base;
+    }
+}
+
 struct SelectResult {
     int nlist;     // total significant entries
     int launches;  // kernels launched
@@ -864,6 +941,21 @@ inline SelectResult run_select(RomeGpuCtx* ctx, cudaStream_t st, int mode, int P
             ROME_CUDA(cudaStreamSynchronize(st));
         }
     }
+    res.nlist = hcount;
+    return res;
+}
+
+// Cross-correlation mode selection for P particles (cc_select_kernel);
+// returns the list size (one entry per particle with a computed hypothesis).
+inline SelectResult run_select_cc(cudaStream_t st, int P, long X, PostLayout L, const float* diff2, double* part,
+                                  int* parti, double* wout, SigEntry* list, int* counter, int cap, int* seg) {
+    SelectResult res{0, 1};
+    if (counter) ROME_CUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
+    cc_select_kernel<<<P, SEL2_THREADS, 0, st>>>(X, L, diff2, part, parti, wout, list, counter, cap, seg);
+    ROME_CHECK_LAUNCH();
+    int hcount = 0;
+    if (counter) ROME_CUDA(cudaMemcpyAsync(&hcount, counter, sizeof(int), cudaMemcpyDeviceToHost, st));
+    ROME_CUDA(cudaStreamSynchronize(st));
     res.nlist = hcount;
     return res;
 }

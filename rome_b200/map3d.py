@@ -58,6 +58,12 @@ class Map3dPool:
     iclass_min: int = 0
     iclass_max: int = -1
     adaptive_oversampling: int = 1
+    # cross-correlation mode ((iter == 1 && do_firstiter_cc) || do_always_cc, src/map3d_optimizer.cpp:907)
+    do_cross_correlation: bool = False
+    # intensity-scale correction: mlModel.scale_correction [G] and data_vs_prior_class [K][ori/2+1]
+    do_scale_correction: bool = False
+    scale_correction: Optional[np.ndarray] = None
+    data_vs_prior_class: Optional[np.ndarray] = None
     # optional restricted coarse search: [P][nr_proposals] coarse orientations (class * nr_dir + dir) * nr_psi + psi
     proposals: Optional[np.ndarray] = None
 
@@ -113,8 +119,10 @@ def _pack(p: Map3dPool):
     s.sigma2_offset, s.sigma2_fudge, s.adaptive_fraction = p.sigma2_offset, p.sigma2_fudge, p.adaptive_fraction
     s.do_ctf_correction, s.refs_are_ctf_corrected = int(p.do_ctf_correction), int(p.refs_are_ctf_corrected)
     s.do_map = int(p.do_map)
-    s.do_scale_correction = 0
-    s.do_cross_correlation = 0
+    s.do_scale_correction = int(p.do_scale_correction)
+    if p.do_scale_correction:
+        s.scale_correction, s.data_vs_prior_class = d(p.scale_correction), d(p.data_vs_prior_class)
+    s.do_cross_correlation = int(p.do_cross_correlation)
     s.inputs_on_device = 0
     if p.proposals is not None:
         pr = _i32(p.proposals)
@@ -182,6 +190,10 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
     if marginals:
         o["post_coarse"] = np.zeros((P, K * p.nr_dir * p.nr_psi))
         so.post_coarse = abi.dptr(o["post_coarse"])
+    if p.do_scale_correction:
+        for name in ("wsum_scale_correction_XA", "wsum_scale_correction_AA"):
+            o[name] = np.zeros((P, oF))
+            setattr(so, name, abi.dptr(o[name]))
     ctx._check(ctx.lib.rome_gpu_map3d_estep_pool(ctx.h, C.byref(s), C.byref(so)))
     del keep
     if checkpoints:
@@ -193,7 +205,7 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
 
 # per-particle outputs of map3d_estep_pool (the rest are the pool's model sums)
 _PER_PARTICLE = ("min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "rot", "tilt",
-                 "psi", "xoff", "yoff", "nr_sign", "cls")
+                 "psi", "xoff", "yoff", "nr_sign", "cls", "wsum_scale_correction_XA", "wsum_scale_correction_AA")
 
 
 def map3d_estep_pools_adaptive(ctx: GpuContext, p: Map3dPool, dev: Optional[dict] = None,
@@ -254,7 +266,10 @@ def pool3d_from_dump(d: Dict[str, np.ndarray], pool: int = 0) -> Map3dPool:
         sigma2_offset=sc("sigma2_offset"), sigma2_fudge=sc("sigma2_fudge"),
         adaptive_fraction=sc("adaptive_fraction"), do_ctf_correction=bool(ic("do_ctf_correction")),
         refs_are_ctf_corrected=bool(ic("refs_are_ctf_corrected")), do_map=bool(ic("do_map")),
-        adaptive_oversampling=ic("adaptive_oversampling"))
+        adaptive_oversampling=ic("adaptive_oversampling"),
+        do_cross_correlation=bool(ic("do_cross_correlation")) if "do_cross_correlation" in d else False,
+        do_scale_correction=bool(ic("do_scale_correction")), scale_correction=g("scale_correction"),
+        data_vs_prior_class=g("data_vs_prior_before"))
 
 
 def fine_lists_from_dump(d: Dict[str, np.ndarray], prefix: str, nr_trans: int, nh: int = 32):

@@ -55,6 +55,16 @@ CASES3D = {
                           snr=2.0, pixel=4.0, seed=7),
                 dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1, pool=4,
                      offset_range=2, offset_step=1, ctf=1, uniform_directions=1)),
+    # the same shapes in cross-correlation mode (-always_cc: CC in the dumped iteration too)
+    "map3d_cc": (Map3dSpec(n_particles=96, size=24, n_classes=2, n_blobs=10, blob_sigma=(1.2, 2.5), max_shift=2.0,
+                           snr=2.0, pixel=4.0, seed=8),
+                 dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1, pool=4,
+                      offset_range=2, offset_step=1, ctf=1, uniform_directions=1, always_cc=1, dump_pools=6)),
+    # intensity-scale correction (seven micrograph groups, per-group scales after iteration 1)
+    "map3d_scale": (Map3dSpec(n_particles=96, size=24, n_classes=2, n_blobs=10, blob_sigma=(1.2, 2.5), max_shift=2.0,
+                              snr=2.0, pixel=4.0, seed=9),
+                    dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1,
+                         pool=4, offset_range=2, offset_step=1, ctf=1, uniform_directions=1, scale=1)),
 }
 # 128^2 cases of the MAP3D configuration's shape (HEALPix order 2: 192 directions x 24 psi, 13
 # translations, oversampling 1, fine pass at the full size, M-step into the pad-259 grid).  The
@@ -163,7 +173,9 @@ def make_case3d(name: str):
         env = dict(os.environ, OMP_NUM_THREADS="1")
         subprocess.check_call(cmd, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL, env=env, cwd=tmp)
         d = load_dump(dump)
-        keep = {k: v for k, v in d.items() if not k.endswith(SKIP3D)}
+        # the image norms of the CC denominator are kept where the dumped iteration runs in CC mode
+        skip = tuple(x for x in SKIP3D if not (opt.get("always_cc") and x == "local_sqrtXi2"))
+        keep = {k: v for k, v in d.items() if not k.endswith(skip)}
         keep["meta_options"] = np.array([str(opt)])
         out = os.path.join(HERE, name + ".npz")
         np.savez_compressed(out, **keep)

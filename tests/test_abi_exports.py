@@ -28,7 +28,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version_callable_without_gpu():
     lib = abi.load_library()
     lib.rome_gpu_abi_version.restype = ctypes.c_int
-    assert lib.rome_gpu_abi_version() == abi.ABI_VERSION == 3
+    assert lib.rome_gpu_abi_version() == abi.ABI_VERSION == 4
 
 
 def test_create_fails_cleanly_without_device():
