@@ -1,0 +1,51 @@
+"""The reference's own MAP3D driver calling the library through
+include/rome_gpu.h from C++ (oracle/_ref/map3d_dropin, built from
+oracle/ref_harness/map3d_dropin.cpp against the reference's objects and
+rome_b200/librome_b200.so): it fills RomeMap3dPool from
+Map3dOptimizer_old's own state as a patched expectationSomeParticles()
+would, calls rome_gpu_map3d_estep_pool, runs the reference's E-step
+functions on the same pool, and compares (diff2 1e-5 relative, FP64 sums
+and back-projectors 1e-3 relative, poses identical but for near ties).
+Maximum-likelihood, cross-correlation and scale-correction modes, on the
+seeded 24^2 datasets of the golden cases."""
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from rome_b200.synthetic import write_dataset_3d
+from tests.golden.make_golden import CASES3D
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(ROOT, "oracle", "_ref", "map3d_dropin")
+KEYS = ("K", "iter", "angpix", "ini_high", "tau2_fudge", "oversampling", "healpix_order", "pool", "offset_range",
+        "offset_step", "ctf", "uniform_directions", "always_cc", "scale")
+
+
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_cc", "map3d_scale"])
+def test_reference_driver_calls_the_library(case):
+    assert os.path.exists(BIN), "oracle/_ref/map3d_dropin is built by __graft_entry__.build()"
+    spec, opt = CASES3D[case]
+    with tempfile.TemporaryDirectory(prefix="rome_dropin_") as tmp:
+        star, ref = write_dataset_3d(os.path.join(tmp, "data"), spec)
+        cmd = [BIN, "-i", star, "-ref", ref]
+        for k in KEYS:
+            if k in opt:
+                cmd += [f"-{k}", str(opt[k])]
+        env = dict(os.environ, OMP_NUM_THREADS="8")
+        r = subprocess.run(cmd, cwd=tmp, env=env, capture_output=True, text=True, timeout=900)
+    line = [x for x in r.stdout.splitlines() if x.startswith("DROPIN")]
+    assert line, (r.returncode, r.stdout[-2000:], r.stderr[-2000:])
+    print(case, line[-1])
+    vals = dict(kv.split("=") for kv in line[-1].split()[1:])
+    assert r.returncode == 0, line[-1]
+    assert int(vals["cc"]) == int(opt.get("always_cc", 0)) and int(vals["scale"]) == int(opt.get("scale", 0))
+    assert int(vals["same_pose"]) >= int(vals["particles"]) - 1
+    assert float(vals["min_diff2"]) <= 1e-5
+    for k in ("sum_weight", "wsum_sigma2_noise", "bp_data", "bp_weight"):
+        assert float(vals[k]) <= 1e-3, k
+    assert re.match(r"^\d+$", vals["same_nr_sign"])
