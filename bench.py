@@ -573,6 +573,7 @@ def reference_rate(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str)
 
 
 REF_BENCH3D = os.path.join(ROOT, "oracle", "_ref", "map3d_bench")
+REF_RECON = os.path.join(ROOT, "oracle", "_ref", "recon_bench")
 
 
 def reference_rate_3d(w, pool: int, warm_pools: int, timed_pools: int, tmpdir: str):
@@ -633,6 +634,32 @@ def cpu_baseline(args, w):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
 
 
+def reference_rate_recon(n: int = 60000):
+    """The reference's per-image reconstruction work (rome_reconstruct's
+    image loop on transformed spectra: shift, CTF image and products,
+    MyBackProjector::backproject into the padded grid) timed by
+    oracle/_ref/recon_bench on every host core, one back-projector per
+    thread as one per MPI rank."""
+    import subprocess
+    cores = os.cpu_count() or 1
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores))
+    r = subprocess.run([REF_RECON, "-n", str(n), "-size", "128", "-angpix", "1.5"], env=env, capture_output=True,
+                       text=True, timeout=1800)
+    line = [x for x in r.stdout.splitlines() if x.startswith("RECON_BENCH")]
+    if r.returncode != 0 or not line:
+        raise RuntimeError(f"recon_bench failed ({r.returncode}): {r.stderr[-500:]}")
+    v = dict(kv.split("=") for kv in line[-1].split()[1:])
+    secs = float(v["seconds"])
+    return {"value": round(n / secs, 2), "unit": "particles/s", "cores": int(v["threads"]), "kind": "reference",
+            "sample": f"{n} images of 128x128 back-projected at known poses into the pad-2 grid (259^3) by the "
+                      f"reference's own shiftImageInFourierTransform, CTF::getFftwImage and "
+                      f"MyBackProjector::backproject (rome_reconstruct's image loop without reading and "
+                      f"transforming the images), one back-projector per thread as one per MPI rank, "
+                      f"{secs:.1f} s",
+            "s_per_image_per_thread": {"min": float(v["per_image_min"]), "median": float(v["per_image_median"]),
+                                       "max": float(v["per_image_max"])}}
+
+
 def run_reference(args):
     """The reference arm: the reference's own CPU E-step (oracle/_ref, or the
     oracle port where the reference could not be built) on every host core,
@@ -640,6 +667,22 @@ def run_reference(args):
     import tempfile
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return
+    if args.mode == "reconstruct":
+        if not os.path.exists(REF_RECON):
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/recon_bench was not built (the "
+                              "reference tree was absent at build time)"}))
+            return
+        best = reference_rate_recon()
+        print(json.dumps({"metric": "reconstruction at known poses: back-projection particles/s (rome_reconstruct)",
+                          "value": best["value"], "unit": UNIT, "n_gpus": int(os.environ.get("WORLD_SIZE", 1)),
+                          "steps": args.steps, "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                          "impl": "reference", "config": {"workload": "map3d_cfg3 M-step shapes: reconstruction at "
+                                                                      "known poses", "image": 128, "pad": 259},
+                          "cpu_baseline": best,
+                          "e2e": {"value": best["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
         return
     from rome_b200.workload import CONFIGS
     w = CONFIGS[args.config]
@@ -999,7 +1042,8 @@ def run_reconstruct(args):
                      "kernel": "bp_images_kernel: algorithmic bytes = spectra and CTF read once (24 B per "
                                "coefficient); the 12 FP64 atomics per active pixel land in L2",
                      "launches": int(bp["launches"])},
-        "cpu_baseline": None,
+        "cpu_baseline": (reference_rate_recon() if not args.no_cpu_baseline and os.path.exists(REF_RECON)
+                         else None),
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
