@@ -69,7 +69,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     __shared__ float redf[32];
     __shared__ double smax[32];
     __shared__ long slo[32], se[32];
-    __shared__ int ncand, s_nsig, s_over, s_m, s_base;
+    __shared__ int ncand, s_nsig, s_over, s_m, s_base, s_cached;
     __shared__ double s_sig;
     const int i = blockIdx.x;
     // the particle's row: fixed length Xrow at i * Xrow, or (ragged rows, L.roff) its own span
@@ -78,6 +78,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     const float* d = diff2 ? diff2 + rb : nullptr;
     const double* wg = wgiven ? wgiven + rb : nullptr;
     const double* po = poff ? poff + (long)i * L.K * L.ntr : nullptr;
+    if (threadIdx.x == 0) s_cached = -1;  // set by the dense sweep when it kept the candidates
 
     // ---- min over computed diff2 ----
     double mn = 0.0;
@@ -154,12 +155,23 @@ __global__ void __launch_bounds__(SEL2_THREADS)
         // weights (at most X of them) change the sum by less than X * 2^-60 of itself (~2e-13 at X =
         // 2.4e5).  The sum is checked against minpos below and recomputed in full if that premise fails.
         double skip_cut = (minpos > 0.0 && minpos < INFINITY) ? 41.6 + log(pmax * omax / minpos) : INFINITY;
+        // Under the same premise (sum >= minpos) every candidate of the walk, w >= t0 = (1 - frac) * sum /
+        // X (1 - 1e-6), has w >= tlow; the sweep keeps those weights with their index in the candidate
+        // buffer, so that the candidate pass needs no second read of the row when they fit.  The cut of
+        // the skip bound is far above (log(X / (1 - frac)) < 41.6), so no candidate is skipped.
+        const double tlow0 = (skip_cut < INFINITY && frac < 1.0)
+                                 ? (1.0 - frac) * minpos / (double)X * (1.0 - 1e-6) * (1.0 - 1e-9)
+                                 : 0.0;
         for (int pass = 0; pass < 2; pass++) {
             sum = 0.0;
             maxw = DBL_MIN;
             maxpd = 0.0;
             best_lo = LONG_MAX;
             best_e = 0;
+            const double tlow = pass == 0 ? tlow0 : 0.0;
+            __syncthreads();
+            if (threadIdx.x == 0) ncand = 0;
+            __syncthreads();
             if (active) {
                 // lane state: orientation j, its k = j / nrot (remainder rk), class c = k / ndir (remainder rc)
                 int j = warp * G + jj;
@@ -185,6 +197,13 @@ __global__ void __launch_bounds__(SEL2_THREADS)
                     const double w = pp * exp(-diff);
                     if (wout) wout[rb + e] = w;
                     sum += w;
+                    if (w > 0.0 && w >= tlow) {
+                        const int q = atomicAdd(&ncand, 1);
+                        if (q < SEL2_CAP) {
+                            key[q] = w;
+                            idx[q] = (int)e;
+                        }
+                    }
                     if (w >= maxw && w > DBL_MIN) {
                         int kk, it2;
                         long lo;
@@ -236,6 +255,9 @@ __global__ void __launch_bounds__(SEL2_THREADS)
             if (tot >= minpos * (1.0 - 1e-12)) break;
             skip_cut = INFINITY;
         }
+        __syncthreads();
+        // the kept weights are the candidate set's superset when they all fit and the cut held
+        if (threadIdx.x == 0) s_cached = (tlow0 > 0.0 && skip_cut < INFINITY && ncand <= SEL2_CAP) ? ncand : -1;
         if (wout && skip_cut < INFINITY) {
             // skipped entries still get their (zero or negligible) weights written for the caller
             for (long e = threadIdx.x; e < X; e += blockDim.x) {
@@ -304,6 +326,7 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     const double dlim0 = (mode == 0 && t0 > 0.0 && maxpd > 0.0) ? mn + log(maxpd / t0) + 1e-6 * (1.0 + fabs(mn))
                                                                 : INFINITY;
     __syncthreads();
+    const int cached = s_cached;
     // ---- candidates w >= t0 ----
     auto candidate = [&](long e, double w) {
         if (w > 0.0 && w >= t0) {
@@ -321,7 +344,21 @@ __global__ void __launch_bounds__(SEL2_THREADS)
         if (!hyp_prior(e, i, L, pdir, po, pd, pof, lo)) return;
         candidate(e, hyp_weight(dv, mn, pd, pof));
     };
-    if (mode == 0 && (X & 3) == 0 && ((uintptr_t)d & 15) == 0) {
+    int sort_n = -1;  // with kept weights: the buffer's length, non-candidates marked -1
+    if (cached >= 0) {
+        int nc = 0;
+        for (int q = threadIdx.x; q < cached; q += blockDim.x) {
+            if (key[q] > 0.0 && key[q] >= t0) {
+                nc++;
+            } else {
+                key[q] = -1.0;
+                idx[q] = -1;
+            }
+        }
+        nc = block_reduce_sum(nc, (int*)red);
+        if (threadIdx.x == 0) ncand = nc;
+        sort_n = cached;
+    } else if (mode == 0 && (X & 3) == 0 && ((uintptr_t)d & 15) == 0) {
         // 16-byte loads, two in flight per thread
         const float4* d4 = (const float4*)d;
         const long X4 = X / 4;
@@ -346,12 +383,13 @@ __global__ void __launch_bounds__(SEL2_THREADS)
     }
     __syncthreads();
     const int cnt = ncand;
+    if (sort_n < 0) sort_n = cnt;
     if (cnt > SEL2_CAP) {
         if (threadIdx.x == 0) s_over = 1;
     } else {
         int n2 = 1;
-        while (n2 < cnt) n2 <<= 1;
-        for (int q = cnt + threadIdx.x; q < n2; q += blockDim.x) {
+        while (n2 < sort_n) n2 <<= 1;
+        for (int q = sort_n + threadIdx.x; q < n2; q += blockDim.x) {
             key[q] = -1.0;
             idx[q] = -1;
         }
