@@ -545,6 +545,7 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         prof.end(ROME_PHASE_WSUM);
 
         // ---- backProjection ----
+        std::vector<int> hoff_bp;  // list offsets per orientation (profiling: slices back-projected)
         {
             double2* dFnm = ctx->ws[S_FNOMASK].as<double2>((size_t)P * g.F);
             double* dMctf2 = dMinv;  // reused in place: becomes ctf^2 * Minvsigma2
@@ -578,6 +579,10 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
                     ctx->pad_size, ctx->pad_size / 2 + 1, ctx->bp_data, ctx->bp_weight, ctx->vox, j0);
             prof.launched(ROME_PHASE_BACKPROJECT);
             prof.end(ROME_PHASE_BACKPROJECT);
+            if (ctx->profile) {
+                hoff_bp.resize((size_t)g.J + 1);
+                ROME_CUDA(cudaMemcpyAsync(hoff_bp.data(), dOff, sizeof(int) * (g.J + 1), cudaMemcpyDeviceToHost, st));
+            }
         }
 
         // ---- outputs ----
@@ -586,6 +591,14 @@ extern "C" int rome_gpu_map2d_estep_pool(RomeGpuCtx* ctx, const RomeMap2dPool* i
         ROME_CUDA(cudaMemcpyAsync(hwk.data(), dWk, sizeof(double) * hwk.size(), cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
         prof.collect();
+        if (!hoff_bp.empty()) {
+            // algorithmic bytes of the back-projection: the prepared image and ctf^2 Minvsigma2 of every
+            // significant hypothesis (24 B per active pixel) and 12 FP64 updates (96 B) per active pixel of
+            // every back-projected slice (orientation with significant hypotheses)
+            long nslice = 0;
+            for (int j = 0; j + 1 < (int)hoff_bp.size(); j++) nslice += hoff_bp[j + 1] > hoff_bp[j];
+            prof.add_bytes(ROME_PHASE_BACKPROJECT, (double)g.Kact * (24.0 * nsigtot + 96.0 * nslice));
+        }
         for (size_t q = 0; q < (size_t)G * oriF; q++) out->wsum_sigma2_noise[q] += hwsn[q];
         for (int i = 0; i < P; i++) {
             if (out->wsum_norm_correction) out->wsum_norm_correction[i] = hwsn[(size_t)G * oriF + i];

@@ -298,6 +298,9 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                                                  nullptr, dQ, dB, ctx->precision);
             ROME_CHECK_LAUNCH();
             prof.launched(ROME_PHASE_PROJECT);
+            // algorithmic bytes: the class volumes read once, |P|^2 and the cross-term operand written
+            prof.add_bytes(ROME_PHASE_PROJECT, (double)K * ctx->vox * 16 + (double)J * g.Kq * 4 +
+                                                   (double)J * g.Kp * (ctx->precision == ROME_PREC_BF16 ? 2 : 4));
             prof.end(ROME_PHASE_PROJECT);
 
             const long M = (long)P * T;
@@ -572,6 +575,9 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                                               dProj, dQ, dB, ROME_PREC_FP32);
         ROME_CHECK_LAUNCH();
         prof.launched(ROME_PHASE_PROJECT);
+        // algorithmic bytes: the class volumes read once, FP64 projections, |P|^2 and FP32 operand written
+        prof.add_bytes(ROME_PHASE_PROJECT, (double)K * ctx->vox * 16 +
+                                               (double)Jf * ((double)g.Kact * 16 + (double)g.Kq * 4 + (double)g.Kp * 4));
         prof.end(ROME_PHASE_PROJECT);
 
         float* dW2 = ctx->ws[S_W2].as<float>((size_t)P * g.Kq);
@@ -773,6 +779,7 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
         prof.end(ROME_PHASE_WSUM);
 
         // ---- backProjection ----
+        std::vector<int> hoff_bp;  // list offsets per fine orientation (profiling: slices back-projected)
         {
             double2* dFnm = ctx->ws[S_FNOMASK].as<double2>((size_t)P * g.F);
             double* dMctf2 = dMinv;  // becomes ctf^2 * Minvsigma2 in place
@@ -804,6 +811,10 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             }
             prof.launched(ROME_PHASE_BACKPROJECT, 5);
             prof.end(ROME_PHASE_BACKPROJECT);
+            if (ctx->profile) {
+                hoff_bp.resize((size_t)Jf + 1);
+                ROME_CUDA(cudaMemcpyAsync(hoff_bp.data(), dJoff, sizeof(int) * (Jf + 1), cudaMemcpyDeviceToHost, st));
+            }
         }
 
         // ---- outputs ----
@@ -818,6 +829,14 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
                                       cudaMemcpyDeviceToHost, st));
         ROME_CUDA(cudaStreamSynchronize(st));
         prof.collect();
+        if (!hoff_bp.empty()) {
+            // algorithmic bytes of the back-projection: the prepared image and ctf^2 Minvsigma2 of every
+            // significant hypothesis (24 B per active pixel) and 24 FP64 updates (192 B) per active pixel of
+            // every back-projected slice (fine orientation with significant hypotheses)
+            long nslice = 0;
+            for (int j = 0; j + 1 < (int)hoff_bp.size(); j++) nslice += hoff_bp[j + 1] > hoff_bp[j];
+            prof.add_bytes(ROME_PHASE_BACKPROJECT, (double)g.Kact * (24.0 * nsig + 192.0 * nslice));
+        }
         for (size_t q = 0; q < (size_t)G * oriF; q++) out->wsum_sigma2_noise[q] += hwsn[q];
         for (int i = 0; i < P; i++) {
             if (out->wsum_norm_correction) out->wsum_norm_correction[i] = hwsn[(size_t)G * oriF + i];
