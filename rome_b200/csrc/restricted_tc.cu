@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
     if (tid == 0) {
         timed_out = 0;
         for (int s = 0; s < L::STAGES; s++) {
-            mbar_init(&full[s], RT_PRODUCERS);
+            mbar_init(&full[s], RT_PRODUCERS / 32);  // one arrival per producer warp
             mbar_init(&bfull[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -140,11 +140,12 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
         }
         for (int kb = 0; kb < nk; kb++) {
             const int s = kb % L::STAGES;
-            if (kb >= L::STAGES && !mbar_wait(&empty[s], ((kb / L::STAGES) + 1) & 1)) {
+            // the warp leaves the loop together (one lane arrives for it below)
+            const bool failed = kb >= L::STAGES && !mbar_wait(&empty[s], ((kb / L::STAGES) + 1) & 1);
+            if (__any_sync(0xffffffffu, failed || *vto)) {
                 *vto = 1;
                 break;
             }
-            if (*vto) break;
             uint8_t* st = smem + s * L::STAGE_BYTES;
             const int px = kb * 32 + cc * 4;  // first of the chunk's 4 complex pixels
             // all loads of the step first (rows' P chunks, then the particles' image and weights)
@@ -197,8 +198,11 @@ __global__ void __launch_bounds__(RT_THREADS, NPLANE == 1 && TN <= 64 ? 2 : 1)
                 *(uint4*)(st + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
                 if (NPLANE == 2) *(uint4*)(st + L::A_BYTES + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
             }
+            // every thread's tile writes are made visible to the tensor core's proxy, then the warp's
+            // lanes are joined and one lane arrives for the warp
             fence_async_smem();
-            mbar_arrive(&full[s]);
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&full[s]);
         }
         // each row's norm term: the sum over its eight chunk threads (consecutive lanes)
 #pragma unroll
