@@ -510,12 +510,23 @@ extern "C" int rome_gpu_map3d_estep_pool(RomeGpuCtx* ctx, const RomeMap3dPool* i
             // rows per fine orientation): refuse pools whose union of significant orientations would not fit
             std::vector<int> a2, ai2;
             const Pass gf = active_pixels(cur, ctx->r_max, a2, ai2);
-            const double need = (double)nU * NOR * ((double)gf.Kact * 16 + (double)gf.Kq * 4 + (double)gf.Kp * 4);
-            size_t free_b = 0, total_b = 0;
-            ROME_CUDA(cudaMemGetInfo(&free_b, &total_b));
-            if (need > 0.8 * (double)free_b)
-                fail(ROME_ERR_OOM, "fine pass: %d significant coarse orientations need %.1f GB of projections "
-                     "(%.1f GB free); use smaller pools", nU, need / 1e9, free_b / 1e9);
+            const double nb[3] = {(double)nU * NOR * gf.Kact * 16, (double)nU * NOR * gf.Kq * 4,
+                                  (double)nU * NOR * gf.Kp * 4};
+            const Slot sl[3] = {S_PROJ, S_Q, S_B};
+            double need = 0.0, held = 0.0;
+            bool grows = false;
+            for (int q = 0; q < 3; q++) {
+                need += nb[q];
+                held += (double)ctx->ws[sl[q]].bytes;
+                grows |= nb[q] > (double)ctx->ws[sl[q]].bytes;
+            }
+            if (grows) {  // only a pool that enlarges the buffers can run out (they are freed, then reallocated)
+                size_t free_b = 0, total_b = 0;
+                ROME_CUDA(cudaMemGetInfo(&free_b, &total_b));
+                if (need > 0.8 * ((double)free_b + held))
+                    fail(ROME_ERR_OOM, "fine pass: %d significant coarse orientations need %.1f GB of projections "
+                         "(%.1f GB free); use smaller pools", nU, need / 1e9, ((double)free_b + held) / 1e9);
+            }
         }
         int* dUcomp = upload3(ctx, S_TMP2, ucompact.data(), ucompact.size());
         std::vector<int> hjf((size_t)2 * Jf);  // jclass, jcd
