@@ -445,6 +445,15 @@ def run_ours(args):
     if fp32_line is not None:
         line["plain_fp32"] = fp32_line
     if train_info is not None:
+        # the one-time cost of the learned path (staging, labels from the exhaustive E-step, training),
+        # spread over EM iterations of this many particles, against the exhaustive BF16 E-step
+        once = train_info["stage_s"] + train_info["label_s"] + train_info["train_s"]
+        step_s, ex_s = ms_step / 1e3, ex_ms / 1e3
+        train_info["one_time_s"] = round(once, 2)
+        train_info["amortised"] = {
+            f"{n}_iterations": round(n * N * world / (n * step_s + once), 2) for n in (10, 25, 100)}
+        train_info["break_even_iterations_vs_exhaustive_%s" % args.precision] = (
+            round(once / (ex_s - step_s), 1) if ex_s > step_s else None)
         line["learned"] = train_info
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w)
