@@ -111,7 +111,7 @@ enum Slot {
     S_PAIRS,      // 3D fine pass: (particle, coarse translation) pair flags, ids and list
     S_SELEXACT,   // particles whose significance walk needs the exact sort
     S_CCX,        // 3D cross-correlation mode: image norms of the pass [P] double
-    S_PSCALE,     // 3D intensity-scale correction: per-particle scale and its spectra [P] + [P][2][oriF] double
+    S_PSCALE,     // 3D intensity-scale correction: scales [P], XA/AA spectra [P][2][oriF], data_vs_prior [K][oriF]
     S_ACTIDX,     // pixel -> active index [F] int
     S_TRANS,      // translations of the last pass [T] double2
     S_LISTCNT,    // list counter + per-orientation counts

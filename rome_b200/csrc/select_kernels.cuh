@@ -17,7 +17,11 @@
 //
 // The same kernel emits the significant hypotheses (w >= significant
 // weight) as the particle's contiguous segment of the SigEntry list used by
-// updateOtherParams and backProjection.
+// updateOtherParams and backProjection.  Rows with more candidates than the
+// shared-memory buffer holds take the exact radix select
+// (select_radix_kernel) and, where a decision falls within rounding, the
+// exact sort (select_fallback2_kernel); the 3D cross-correlation mode keeps
+// the best hypothesis alone (cc_select_kernel).
 #pragma once
 
 #include <cstdint>
