@@ -11,7 +11,9 @@ records: count[P][K][ndir][npsi], then (ihidden, value) in that loop order):
   (src/map3d_optimizer.cpp:1610-1810), maximum-likelihood and
   cross-correlation branches;
 * Map3dOptimizer_old::findAllSignificantPoints (:1812-1931): the ascending
-  sort of every listed weight (zeros included) and the walk from the largest.
+  sort of every listed weight (zeros included) and the walk from the largest;
+* the metadata of the largest weight (class, rot, tilt, psi, offsets,
+  :1787-1804).
 
 decodeOverRotTrans: ihidden = (itrans * nr_over_rot + iover_rot) *
 nr_over_trans + iover_trans (src/map3d_optimizer.cpp:1247-1249).
@@ -104,3 +106,23 @@ def significance(weights: np.ndarray, sum_weight: float, adaptive_fraction: floa
         if frac > adaptive_fraction * sum_weight:
             break
     return sig, n
+
+
+def best_pose(pl: ParticleList, weights: np.ndarray, nr_dir: int, nr_psi: int, nr_over_rot: int,
+              nr_over_trans: int, angles: np.ndarray, over_trans_x: np.ndarray, over_trans_y: np.ndarray,
+              old_offx: float, old_offy: float):
+    """The metadata convertSquaredDifferencesToWeights writes for the largest
+    weight (:1787-1804): class (1-based), rot, tilt, psi of the over-rotation
+    (SamplingGrid::setOrientation, `angles` [ndir][npsi][nor][3]) and the
+    offsets old_offset + exp_over_trans (over_trans_x/y [ntr][notr]).  The
+    first largest weight in loop order wins."""
+    q = int(np.argmax(weights))
+    kd, ipsi = divmod(int(pl.kdp[q]), nr_psi)
+    cls, idir = divmod(kd, nr_dir)
+    h = int(pl.ihidden[q])
+    itrans, rest = divmod(h, nr_over_rot * nr_over_trans)
+    iover_rot, iover_trans = divmod(rest, nr_over_trans)
+    rot, tilt, psi = (float(x) for x in angles[idir, ipsi, iover_rot])
+    return {"class": cls + 1, "rot": rot, "tilt": tilt, "psi": psi,
+            "xoff": old_offx + float(over_trans_x[itrans, iover_trans]),
+            "yoff": old_offy + float(over_trans_y[itrans, iover_trans])}

@@ -36,6 +36,11 @@ def test_ml_weights_and_significance_match_reference(golden, case, ipass):
         np.testing.assert_allclose(w, rw.value, rtol=1e-13, atol=0)
         assert s == pytest.approx(float(g[pre + "sum_weight"][i]), rel=1e-12)
         assert mx / s == pytest.approx(float(g[pre + "pmax"][i]), rel=1e-12)
+        pose = so.best_pose(pl, w, nd, npsi, nor, notr, g[f"pool0_pass{ipass}_angles"],
+                            g[f"pool0_pass{ipass}_over_trans_x"], g[f"pool0_pass{ipass}_over_trans_y"],
+                            float(g["pool0_old_offsetx"][i]), float(g["pool0_old_offsety"][i]))
+        for k in ("class", "rot", "tilt", "psi", "xoff", "yoff"):
+            assert pose[k] == g[pre + k][i], (i, k)
         sig, n = so.significance(rw.value, float(g[pre + "sum_weight"][i]), frac)
         assert sig == float(g[pre + "significant_weight"][i])
         if ipass == 0:
