@@ -242,16 +242,35 @@ def test_learned_bf16_with_fallback_agrees_with_plain_fp32():
       the poses, where the FP32 posterior's top hypotheses are nearly tied;
       the restricted and the dense BF16 contractions round differently, so
       they also differ from each other at those ties);
-    and the network, not the fallback, decides most particles."""
+    and the network, not the fallback, decides most particles.  Then the
+    reconstructions (gridding-corrected, no MAP term) of every class from the
+    learned split-BF16 pass's back-projectors and from the plain FP32 pass's
+    are compared shell by shell: measured min FSC 0.9949 over the 6 classes
+    and 31 shells of these 400 held-out particles (about 67 per class, so
+    one particle whose pose or posterior tail differs moves a class by ~1.5 %);
+    gated at 0.99."""
     from rome_b200.proposal import learned_estep_pools
+    from tests.test_gpu_reconstruct import fsc
     w = Map2dWorkload(n_particles=4400, ori_size=64, n_classes=6, n_blobs=20, psi_step=10, offset_range=3,
                       offset_step=1, max_shift=2, pixel=2.0, snr=0.1, seed=29)
     p, proj, r_max, _ = build_map2d(w)
     K, npsi = p.nr_classes, p.nr_psi
     train, test = subset(p, 0, 4000), subset(p, 4000, 4400)
+
+    def volumes(c, o):
+        vols = []
+        for k in range(K):
+            if o["wsum_pdf_class"][k] > 0:
+                vols.append(c.reconstruct(k, p.ori_size, 2, np.ones(p.ori_size // 2 + 1), 1.0,
+                                          float(o["wsum_pdf_class"][k]), 10, False, 0)["vol"])
+            else:
+                vols.append(None)
+        return vols
+
     with GpuContext(0, "fp32") as c32:
         c32.set_projectors(proj, p.ori_size, r_max)
         ref = c32.map2d_estep_pool(test)
+        ref_vols = volumes(c32, ref)
     with GpuContext(0, "bf16") as cb, GpuContext(0, "bf16x3") as cx:
         cb.set_projectors(proj, p.ori_size, r_max)
         cx.set_projectors(proj, p.ori_size, r_max)
@@ -261,7 +280,11 @@ def test_learned_bf16_with_fallback_agrees_with_plain_fp32():
                       lr=3e-3)
             lb, props, mass, low = learned_estep_pools(cb, net, [test], 16, min_mass=0.999)[0]
             lx = learned_estep_pools(cx, net, [test], 16, min_mass=0.999)[0][0]
+        lx_vols = volumes(cx, lx)
         ex = cb.map2d_estep_pool(test)
+    fmin = min(float(fsc(a, b).min()) for a, b in zip(lx_vols, ref_vols) if a is not None and b is not None)
+    print(f"learned split BF16 vs plain FP32 reconstructions: min FSC over classes and shells {fmin:.6f}")
+    assert fmin >= 0.99
 
     def agree(o, r):
         return float(np.mean((o["cls"] == r["cls"]) & (o["psi"] == r["psi"]) & (o["xoff"] == r["xoff"])
