@@ -1,0 +1,157 @@
+"""CPU restatement of the MAP3D coarse pass (numpy; the translation phases
+through the C oracle's restatement of the 5000-entry table).
+
+Test infrastructure only: imported by tests/, never by the product package.
+
+For one pool at the coarse size it restates
+* the windowing of the fine-size masked image and CTF to the pass size
+  (windowFourierTransform / windowTransform, ParticleModel::
+  preShiftedImagesCtfsAndInvSigma2s, src/exp_model.cpp:1015-1049) and
+  Minvsigma2 = 1 / (sigma2_fudge * sigma2_noise[group][ires]), 0 at
+  ires <= 0 (:1078-1092);
+* the image norm of the cross-correlation mode (exp_local_sqrtXi2, :1037-1045);
+* the translated images (shiftImageInFourierTransform, src/image.h:1478-1575,
+  via oracle/estep_oracle.c);
+* MyProjector::project, trilinear branch (src/reconstruct.cpp:226-410);
+* applyCtfToClass (src/map3d_optimizer.cpp:1040-1067, CTF and the group's
+  intensity scale) and get_diff (:1079-1123), maximum-likelihood and
+  cross-correlation forms, over every (class, direction) the coarse pass
+  visits (pdf_class > 0 and pdf_direction > 0, :1205-1206).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import oracle_py
+
+
+def window_half(F: np.ndarray, cur: int, cs: int) -> np.ndarray:
+    """[cur][cur/2+1] half-plane -> [cs][cs/2+1] (rows wrap negative)."""
+    csF = cs // 2 + 1
+    out = np.zeros((cs, csF), F.dtype)
+    F = F.reshape(cur, cur // 2 + 1)
+    for i in range(cs):
+        ip = i if i < csF else i - cs
+        out[i] = F[ip if ip >= 0 else ip + cur, :csF]
+    return out
+
+
+def euler_matrix(rot: float, tilt: float, psi: float) -> np.ndarray:
+    return np.asarray(oracle_py.euler_matrix(rot, tilt, psi)).reshape(3, 3)
+
+
+def _lin(a, lo, hi):
+    return lo + (hi - lo) * a
+
+
+def project3d(data: np.ndarray, r_max: int, padding: int, A: np.ndarray, cs: int) -> np.ndarray:
+    """MyProjector::project (trilinear): the [cs][cs/2+1] slice of the
+    [pad][pad][pad/2+1] complex volume `data` at orientation A."""
+    pad = data.shape[0]
+    csF = cs // 2 + 1
+    my_r_max = min(r_max, cs // 2)
+    shift = -int(np.float32(pad) / np.float32(2.0))
+    Ainv = A.T * float(padding)
+    out = np.zeros((cs, csF), np.complex128)
+    rows, xs = [], []
+    for i in range(cs):
+        if i <= my_r_max:
+            y = i
+        elif i >= cs - my_r_max:
+            y = i - cs
+        else:
+            continue
+        for x in range(my_r_max + 1):
+            if x * x + y * y <= my_r_max * my_r_max:
+                rows.append((i, x, y))
+    i_, x_, y_ = (np.array(v) for v in zip(*rows))
+    xd, yd = x_.astype(np.float64), y_.astype(np.float64)
+    xp = Ainv[0, 0] * xd + Ainv[0, 1] * yd
+    yp = Ainv[1, 0] * xd + Ainv[1, 1] * yd
+    zp = Ainv[2, 0] * xd + Ainv[2, 1] * yd
+    neg = xp < 0
+    xp, yp, zp = np.where(neg, -xp, xp), np.where(neg, -yp, yp), np.where(neg, -zp, zp)
+    x0 = np.floor(xp).astype(np.int64)
+    fx = xp - x0
+    y0f = np.floor(yp).astype(np.int64)
+    fy = yp - y0f
+    y0 = y0f - shift
+    z0f = np.floor(zp).astype(np.int64)
+    fz = zp - z0f
+    z0 = z0f - shift
+    d = lambda z, y, x: data[z, y, x]  # noqa: E731
+    d000, d001 = d(z0, y0, x0), d(z0, y0, x0 + 1)
+    d010, d011 = d(z0, y0 + 1, x0), d(z0, y0 + 1, x0 + 1)
+    d100, d101 = d(z0 + 1, y0, x0), d(z0 + 1, y0, x0 + 1)
+    d110, d111 = d(z0 + 1, y0 + 1, x0), d(z0 + 1, y0 + 1, x0 + 1)
+    vals = []
+    for part in (np.real, np.imag):
+        dx00, dx01 = _lin(fx, part(d000), part(d001)), _lin(fx, part(d100), part(d101))
+        dx10, dx11 = _lin(fx, part(d010), part(d011)), _lin(fx, part(d110), part(d111))
+        dxy0, dxy1 = _lin(fy, dx00, dx10), _lin(fy, dx01, dx11)
+        vals.append(_lin(fz, dxy0, dxy1))
+    re, im = vals
+    im = np.where(neg, -1.0 * im, im)
+    out[i_, x_] = re + 1j * im
+    return out
+
+
+def coarse_diff2(d: dict, pool: int = 0, cc: bool = False):
+    """The coarse pass of pool `pool` of a MAP3D dump (the arrays
+    oracle/ref_harness/map3d_dump records): diff2 [P][K][ndir][npsi][ntr]
+    (NaN where the reference computes nothing), and in cross-correlation
+    mode the image norms [P].  The shifted images are the coarse
+    translations around each particle's rounded old offset."""
+    pp = f"pool{pool}_"
+    g = lambda k: d[k] if k in d or not k.startswith(pp) else d["pool0_" + k[len(pp):]]  # noqa: E731
+    ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    ori, cur, cs = ic("ori_size"), ic("current_size"), ic("coarse_size")
+    K, ndir, npsi, ntr = ic("nr_classes"), ic("nr_dir"), ic("nr_psi"), ic("nr_trans")
+    r_max, padding = ic("projector_r_max"), ic("projector_padding_factor")
+    apply_ctf = ic("do_ctf_correction") and ic("refs_are_ctf_corrected")
+    scale = ic("do_scale_correction")
+    fudge = float(np.asarray(d["sigma2_fudge"]).ravel()[0])
+    P = int(np.asarray(d[pp + "nr_images"]).ravel()[0])
+    csF = cs // 2 + 1
+    angles = g(pp + "pass0_angles")            # [ndir][npsi][1][3]
+    otx, oty = g(pp + "pass0_over_trans_x"), g(pp + "pass0_over_trans_y")  # [ntr][1]
+    vol = d["projector_data"][..., 0] + 1j * d["projector_data"][..., 1]
+    mres = np.asarray(d["Mresol_coarse"]).reshape(cs, csF)
+    s2 = np.asarray(d["sigma2_noise"])
+    group = np.asarray(g(pp + "group")).astype(int)
+    xi2 = np.asarray(g(pp + "highres_Xi2"))
+    pdir, pcls = np.asarray(d["pdf_direction"]).reshape(K, ndir), np.asarray(d["pdf_class"])
+    sc = np.asarray(d["scale_correction"]) if scale else None
+    # projections of every visited (class, direction, psi)
+    proj = {}
+    for k in range(K):
+        for j in range(ndir):
+            if not (pcls[k] > 0 and pdir[k, j] > 0):
+                continue
+            for p in range(npsi):
+                proj[(k, j, p)] = project3d(vol[k], r_max, padding, euler_matrix(*angles[j, p, 0]), cs)
+    out = np.full((P, K, ndir, npsi, ntr), np.nan)
+    norms = np.zeros(P)
+    for i in range(P):
+        X = window_half(g(pp + "Fimg_real")[i] + 1j * g(pp + "Fimg_imag")[i], cur, cs)
+        ctf = window_half(np.asarray(g(pp + "Fctf")[i]), cur, cs)
+        minv = np.where(mres > 0, 1.0 / (fudge * s2[group[i]][np.maximum(mres, 0)]), 0.0)
+        norms[i] = np.sqrt(np.sum(X.real * X.real + X.imag * X.imag))
+        shifted = []
+        for t in range(ntr):
+            sr, si = oracle_py.shift_image(X.real.ravel(), X.imag.ravel(), cs, float(otx[t, 0]), float(oty[t, 0]),
+                                           ori)
+            shifted.append((sr + 1j * si).reshape(cs, csF))
+        for (k, j, p), P3 in proj.items():
+            Pc = P3 * ctf if apply_ctf else P3.copy()
+            if scale:  # check_scale raises a scale below 0.001 to 0.001 (:1000-1018)
+                Pc = Pc * max(float(sc[group[i]]), 0.001)
+            for t in range(ntr):
+                Xt = shifted[t]
+                if cc:
+                    num = -np.sum(Pc.real * Xt.real + Pc.imag * Xt.imag)
+                    out[i, k, j, p, t] = num / (np.sqrt(np.sum(Pc.real ** 2 + Pc.imag ** 2)) * norms[i])
+                else:
+                    dr, di = Pc.real - Xt.real, Pc.imag - Xt.imag
+                    out[i, k, j, p, t] = (np.sum((dr * dr + di * di) * minv) + xi2[i]) / 2
+    return out, norms
