@@ -1,9 +1,10 @@
-"""CPU restatement of the MAP3D coarse pass (numpy; the translation phases
-through the C oracle's restatement of the 5000-entry table).
+"""CPU restatement of the MAP3D squared differences, coarse and fine pass
+(numpy; the translation phases through the C oracle's restatement of the
+5000-entry table).
 
 Test infrastructure only: imported by tests/, never by the product package.
 
-For one pool at the coarse size it restates
+For one pool it restates
 * the windowing of the fine-size masked image and CTF to the pass size
   (windowFourierTransform / windowTransform, ParticleModel::
   preShiftedImagesCtfsAndInvSigma2s, src/exp_model.cpp:1015-1049) and
@@ -16,7 +17,9 @@ For one pool at the coarse size it restates
 * applyCtfToClass (src/map3d_optimizer.cpp:1040-1067, CTF and the group's
   intensity scale) and get_diff (:1079-1123), maximum-likelihood and
   cross-correlation forms, over every (class, direction) the coarse pass
-  visits (pdf_class > 0 and pdf_direction > 0, :1205-1206).
+  visits (pdf_class > 0 and pdf_direction > 0, :1205-1206), and over the
+  over-sampled neighbours of the coarse-significant points in the fine pass
+  (:1261-1372).
 """
 from __future__ import annotations
 
@@ -155,3 +158,74 @@ def coarse_diff2(d: dict, pool: int = 0, cc: bool = False):
                     dr, di = Pc.real - Xt.real, Pc.imag - Xt.imag
                     out[i, k, j, p, t] = (np.sum((dr * dr + di * di) * minv) + xi2[i]) / 2
     return out, norms
+
+
+def fine_diff2(d: dict, pool: int = 0, cc: bool = False):
+    """The fine pass of pool `pool` of a MAP3D dump at the current size: for
+    every coarse point the reference recorded as significant
+    (exp_Mcoarse_significant, coarse index ((class * ndir + dir) * npsi +
+    psi) * ntr + itrans), the 8 over-rotations x 4 over-translations in the
+    reference's list order (getAllSquaredDifferencesFine,
+    src/map3d_optimizer.cpp:1261-1372: class, dir, psi, then ihidden =
+    (itrans * nor + iover_rot) * notr + iover_trans).  Returns per particle
+    (kdp [n], ihidden [n], diff2 [n])."""
+    pp = f"pool{pool}_"
+    g = lambda k: d[k] if k in d or not k.startswith(pp) else d["pool0_" + k[len(pp):]]  # noqa: E731
+    ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    ori, cur = ic("ori_size"), ic("current_size")
+    K, ndir, npsi, ntr = ic("nr_classes"), ic("nr_dir"), ic("nr_psi"), ic("nr_trans")
+    r_max, padding = ic("projector_r_max"), ic("projector_padding_factor")
+    apply_ctf = ic("do_ctf_correction") and ic("refs_are_ctf_corrected")
+    scale = ic("do_scale_correction")
+    fudge = float(np.asarray(d["sigma2_fudge"]).ravel()[0])
+    P = int(np.asarray(d[pp + "nr_images"]).ravel()[0])
+    curF = cur // 2 + 1
+    angles = g(pp + "pass1_angles")                                        # [ndir][npsi][nor][3]
+    otx, oty = g(pp + "pass1_over_trans_x"), g(pp + "pass1_over_trans_y")  # [ntr][notr]
+    nor, notr = angles.shape[2], otx.shape[1]
+    vol = d["projector_data"][..., 0] + 1j * d["projector_data"][..., 1]
+    mres = np.asarray(d["Mresol_fine"]).reshape(cur, curF)
+    s2 = np.asarray(d["sigma2_noise"])
+    group = np.asarray(g(pp + "group")).astype(int)
+    xi2 = np.asarray(g(pp + "highres_Xi2"))
+    mc = np.asarray(d[pp + "pass0_Mcoarse_significant"])
+    sc = np.asarray(d["scale_correction"]) if scale else None
+    cache = {}
+    out = []
+    for i in range(P):
+        X = (g(pp + "Fimg_real")[i] + 1j * g(pp + "Fimg_imag")[i]).reshape(cur, curF)
+        ctf = np.asarray(g(pp + "Fctf")[i]).reshape(cur, curF)
+        minv = np.where(mres > 0, 1.0 / (fudge * s2[group[i]][np.maximum(mres, 0)]), 0.0)
+        norm = np.sqrt(np.sum(X.real * X.real + X.imag * X.imag))
+        shifted = {}
+        kdp, ih, val = [], [], []
+        for q in np.flatnonzero(mc[i]):
+            kd_p, itr = divmod(int(q), ntr)
+            kd, p = divmod(kd_p, npsi)
+            k, j = divmod(kd, ndir)
+            for o in range(nor):
+                key = (k, j, p, o)
+                if key not in cache:
+                    cache[key] = project3d(vol[k], r_max, padding, euler_matrix(*angles[j, p, o]), cur)
+                Pc = cache[key] * ctf if apply_ctf else cache[key].copy()
+                if scale:  # check_scale raises a scale below 0.001 to 0.001 (:1000-1018)
+                    Pc = Pc * max(float(sc[group[i]]), 0.001)
+                for t in range(notr):
+                    if (itr, t) not in shifted:
+                        sr, si = oracle_py.shift_image(X.real.ravel(), X.imag.ravel(), cur, float(otx[itr, t]),
+                                                       float(oty[itr, t]), ori)
+                        shifted[(itr, t)] = (sr + 1j * si).reshape(cur, curF)
+                    Xt = shifted[(itr, t)]
+                    if cc:
+                        v = -np.sum(Pc.real * Xt.real + Pc.imag * Xt.imag) / (
+                            np.sqrt(np.sum(Pc.real ** 2 + Pc.imag ** 2)) * norm)
+                    else:
+                        dr, di = Pc.real - Xt.real, Pc.imag - Xt.imag
+                        v = (np.sum((dr * dr + di * di) * minv) + xi2[i]) / 2
+                    kdp.append(kd_p)
+                    ih.append((itr * nor + o) * notr + t)
+                    val.append(v)
+        # the reference's order: by (class, dir, psi), then ihidden ascending within it
+        order = np.lexsort((np.array(ih), np.array(kdp))) if kdp else np.zeros(0, int)
+        out.append((np.array(kdp)[order], np.array(ih)[order], np.array(val)[order]))
+    return out

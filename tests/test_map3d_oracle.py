@@ -34,3 +34,21 @@ def test_coarse_pass_matches_reference(golden, case):
     assert rel.max() <= 1e-10
     if cc:
         np.testing.assert_allclose(norms, g["pool0_pass0_local_sqrtXi2"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+def test_fine_pass_matches_reference(golden, case):
+    """The fine pass over the coarse points the reference recorded as
+    significant: the same list (order and ihidden) and every value within
+    1e-10 relative."""
+    g = golden[case]
+    cc = bool(int(g["do_cross_correlation"][0])) if "do_cross_correlation" in g else False
+    mine = mo.fine_diff2(g, 0, cc=cc)
+    ref = so.lists_from_dump(g, "pool0_pass1_diff2_")
+    worst, n = 0.0, 0
+    for (kdp, ih, v), rl in zip(mine, ref):
+        assert np.array_equal(kdp, rl.kdp) and np.array_equal(ih, rl.ihidden)
+        worst = max(worst, float(np.max(np.abs(v - rl.value) / np.abs(rl.value))) if v.size else 0.0)
+        n += v.size
+    print(f"{case}: {n} fine hypotheses, max rel diff {worst:.2e}")
+    assert worst <= 1e-10
