@@ -229,3 +229,80 @@ def fine_diff2(d: dict, pool: int = 0, cc: bool = False):
         order = np.lexsort((np.array(ih), np.array(kdp))) if kdp else np.zeros(0, int)
         out.append((np.array(kdp)[order], np.array(ih)[order], np.array(val)[order]))
     return out
+
+
+def update_other_params(d: dict, pool: int = 0):
+    """updateOtherParams of one pool (src/map3d_optimizer.cpp:2059-2236 and
+    CoarseAndFineSearch::updateModel :1484-1602) from the fine-pass weights,
+    exp_significant_weight and exp_sum_weight the reference recorded: every
+    fine hypothesis with w >= significant_weight, normalised by the sum,
+    adds w |Frefctf - X_t|^2 per pixel of resolution shell ires > -1 to
+    wsum_sigma2_noise[group][ires] and to the particle's norm-correction sum,
+    w to wsum_pdf_class, wsum_pdf_direction and wsum_sumw_group, and
+    w |prior - old offset - translation|^2 to wsum_sigma2_offset; with scale
+    correction, at the shells whose data_vs_prior exceeds 3 for the class,
+    w Re(Frefctf conj X_t) and w |Frefctf|^2 to the particle's XA/AA spectra
+    (get_wdiff2 :1426-1482, binned :2090-2112)."""
+    from oracle.select3d_oracle import lists_from_dump
+    pp = f"pool{pool}_"
+    g = lambda k: d[k] if k in d or not k.startswith(pp) else d["pool0_" + k[len(pp):]]  # noqa: E731
+    ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    ori, cur = ic("ori_size"), ic("current_size")
+    K, ndir, npsi, G = ic("nr_classes"), ic("nr_dir"), ic("nr_psi"), ic("nr_groups")
+    r_max, padding = ic("projector_r_max"), ic("projector_padding_factor")
+    apply_ctf = ic("do_ctf_correction") and ic("refs_are_ctf_corrected")
+    scale = ic("do_scale_correction")
+    oF, curF = ori // 2 + 1, cur // 2 + 1
+    angles = g(pp + "pass1_angles")
+    otx, oty = g(pp + "pass1_over_trans_x"), g(pp + "pass1_over_trans_y")
+    nor, notr = angles.shape[2], otx.shape[1]
+    vol = d["projector_data"][..., 0] + 1j * d["projector_data"][..., 1]
+    mres = np.asarray(d["Mresol_fine"]).reshape(cur, curF)
+    group = np.asarray(g(pp + "group")).astype(int)
+    sc = np.asarray(d["scale_correction"]) if scale else None
+    dvp = np.asarray(d["data_vs_prior_before"]).reshape(K, oF)
+    prx, pry = np.asarray(d["prior_offsetx_class"]), np.asarray(d["prior_offsety_class"])
+    sig, sumw = g(pp + "pass1_significant_weight"), g(pp + "pass1_sum_weight")
+    lists = lists_from_dump(d, pp + "pass1_weight_")
+    P = len(lists)
+    out = {"wsum_sigma2_noise": np.zeros((G, oF)), "wsum_pdf_class": np.zeros(K),
+           "wsum_pdf_direction": np.zeros((K, ndir)), "wsum_sigma2_offset": 0.0, "wsum_sumw_group": np.zeros(G),
+           "wsum_norm_correction": np.zeros(P), "XA": np.zeros((P, oF)), "AA": np.zeros((P, oF))}
+    sel = mres > -1
+    ires_sel = mres[sel]
+    for i, pl in enumerate(lists):
+        X = (g(pp + "Fimg_real")[i] + 1j * g(pp + "Fimg_imag")[i]).reshape(cur, curF)
+        ctf = np.asarray(g(pp + "Fctf")[i]).reshape(cur, curF)
+        gi = group[i]
+        for kdp, h, w in zip(pl.kdp, pl.ihidden, pl.value):
+            if w < sig[i]:
+                continue
+            w = w / sumw[i]
+            kd, p = divmod(int(kdp), npsi)
+            k, j = divmod(kd, ndir)
+            itr, rest = divmod(int(h), nor * notr)
+            o, t = divmod(rest, notr)
+            Pc = project3d(vol[k], r_max, padding, euler_matrix(*angles[j, p, o]), cur)
+            if apply_ctf:
+                Pc = Pc * ctf
+            if scale:
+                Pc = Pc * max(float(sc[gi]), 0.001)
+            sr, si = oracle_py.shift_image(X.real.ravel(), X.imag.ravel(), cur, float(otx[itr, t]), float(oty[itr, t]),
+                                           ori)
+            Xt = (sr + 1j * si).reshape(cur, curF)
+            dr, di = Pc.real - Xt.real, Pc.imag - Xt.imag
+            wd = (w * (dr * dr + di * di))[sel]
+            np.add.at(out["wsum_sigma2_noise"][gi], ires_sel, wd)
+            out["wsum_norm_correction"][i] += wd.sum()
+            out["wsum_pdf_class"][k] += w
+            out["wsum_pdf_direction"][k, j] += w
+            out["wsum_sumw_group"][gi] += w
+            ox = prx[k] - float(g(pp + "old_offsetx")[i]) - float(otx[itr, t])
+            oy = pry[k] - float(g(pp + "old_offsety")[i]) - float(oty[itr, t])
+            out["wsum_sigma2_offset"] += w * (ox * ox + oy * oy)
+            if scale:
+                s_pix = sel & (dvp[k][np.maximum(mres, 0)] > 3.0)
+                ir = mres[s_pix]
+                np.add.at(out["XA"][i], ir, (w * (Pc.real * Xt.real + Pc.imag * Xt.imag))[s_pix])
+                np.add.at(out["AA"][i], ir, (w * (Pc.real * Pc.real + Pc.imag * Pc.imag))[s_pix])
+    return out

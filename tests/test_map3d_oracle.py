@@ -52,3 +52,23 @@ def test_fine_pass_matches_reference(golden, case):
         n += v.size
     print(f"{case}: {n} fine hypotheses, max rel diff {worst:.2e}")
     assert worst <= 1e-10
+
+
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+def test_update_other_params_matches_reference(golden, case):
+    """updateOtherParams restated on the recorded fine-pass weights: the
+    model sums of the pool, the norm-correction sums and (scale correction)
+    the XA/AA spectra, within 1e-11 of each array's largest value."""
+    g = golden[case]
+    o = mo.update_other_params(g, 0)
+    pre = "pool0_after_update_"
+    for k in ("wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_sigma2_offset", "wsum_sumw_group"):
+        ref = np.asarray(g[pre + k], np.float64).reshape(np.shape(o[k]))
+        err = np.max(np.abs(o[k] - ref)) / max(np.max(np.abs(ref)), 1e-300)
+        assert err <= 1e-11, (k, err)
+    ref = g["pool0_wsum_norm_correction"]
+    assert np.max(np.abs(o["wsum_norm_correction"] - ref)) <= 1e-11 * np.max(np.abs(ref))
+    if case == "map3d_scale":
+        for k in ("XA", "AA"):
+            ref = g["pool0_wsum_scale_correction_" + k]
+            assert np.max(np.abs(o[k] - ref)) <= 1e-11 * np.max(np.abs(ref)), k
