@@ -19,7 +19,12 @@ For one pool it restates
   cross-correlation forms, over every (class, direction) the coarse pass
   visits (pdf_class > 0 and pdf_direction > 0, :1205-1206), and over the
   over-sampled neighbours of the coarse-significant points in the fine pass
-  (:1261-1372).
+  (:1261-1372);
+* from the recorded fine-pass weights, updateOtherParams with get_wdiff2
+  (:1426-1602, :2059-2236): the model sums, the norm-correction sums and the
+  scale-correction spectra;
+* backProjection (:2242-2466) with MyBackProjector::backproject
+  (src/reconstruct.cpp:977-1164): the pool's class back-projectors.
 """
 from __future__ import annotations
 
@@ -306,3 +311,119 @@ def update_other_params(d: dict, pool: int = 0):
                 np.add.at(out["XA"][i], ir, (w * (Pc.real * Xt.real + Pc.imag * Xt.imag))[s_pix])
                 np.add.at(out["AA"][i], ir, (w * (Pc.real * Pc.real + Pc.imag * Pc.imag))[s_pix])
     return out
+
+
+def backproject3d(data: np.ndarray, weight: np.ndarray, f2d: np.ndarray, fw: np.ndarray, r_max: int, padding: int,
+                  A: np.ndarray) -> None:
+    """MyBackProjector::backproject, trilinear branch, A not inverted
+    (src/reconstruct.cpp:977-1164): adds the [f][f/2+1] slice `f2d` and its
+    weights `fw` (only where fw > 0) into the [pad][pad][pad/2+1] complex
+    `data` and real `weight` at orientation A, in place.  Rows past r_max
+    from the top and the x = 0 column of negative rows are skipped (the
+    FFTW layout stores that column twice)."""
+    pad = data.shape[0]
+    f = f2d.shape[0]
+    shift = -int(float(pad) / 2.0)
+    Ainv = A.T * float(padding)
+    rows = []
+    for i in range(f):
+        if i <= r_max:
+            y, first_x = i, 0
+        elif i >= f - r_max:
+            y, first_x = i - f, 1
+        else:
+            continue
+        for x in range(first_x, r_max + 1):
+            if x * x + y * y <= r_max * r_max and fw[i, x] > 0.0:
+                rows.append((i, x, y))
+    if not rows:
+        return
+    i_, x_, y_ = (np.array(v) for v in zip(*rows))
+    val, wgt = f2d[i_, x_], fw[i_, x_]
+    xd, yd = x_.astype(np.float64), y_.astype(np.float64)
+    xp = Ainv[0, 0] * xd + Ainv[0, 1] * yd
+    yp = Ainv[1, 0] * xd + Ainv[1, 1] * yd
+    zp = Ainv[2, 0] * xd + Ainv[2, 1] * yd
+    neg = xp < 0
+    xp, yp, zp = np.where(neg, -xp, xp), np.where(neg, -yp, yp), np.where(neg, -zp, zp)
+    val = np.where(neg, np.conj(val), val)
+    x0 = np.floor(xp).astype(np.int64)
+    fx = xp - x0
+    y0f = np.floor(yp).astype(np.int64)
+    fy = yp - y0f
+    z0f = np.floor(zp).astype(np.int64)
+    fz = zp - z0f
+    y0, z0 = y0f - shift, z0f - shift
+    mfx, mfy, mfz = 1.0 - fx, 1.0 - fy, 1.0 - fz
+    for dz, dy, dx, c in ((0, 0, 0, mfz * mfy * mfx), (0, 0, 1, mfz * mfy * fx), (0, 1, 0, mfz * fy * mfx),
+                          (0, 1, 1, mfz * fy * fx), (1, 0, 0, fz * mfy * mfx), (1, 0, 1, fz * mfy * fx),
+                          (1, 1, 0, fz * fy * mfx), (1, 1, 1, fz * fy * fx)):
+        idx = (z0 + dz, y0 + dy, x0 + dx)
+        np.add.at(data, idx, c * val)
+        np.add.at(weight, idx, c * wgt)
+
+
+def back_projection(d: dict, pool: int = 0):
+    """backProjection of one pool (doBackProjectionNew and
+    prepareNomaskImageAndMinvsigma2s, src/map3d_optimizer.cpp:2242-2466):
+    the unmasked image times Minvsigma2 * CTF (the fine pass's Minvsigma2,
+    its origin put back to 1 / (sigma2_fudge * sigma2_noise[group][0]); 1
+    without MAP, CTF 1 without CTF correction, CTF times the group's clamped
+    scale with scale correction), translated by each significant fine
+    hypothesis (w >= significant_weight) and summed with weight w / sum per
+    (class, direction, psi, over-rotation), the weights summing
+    Minvsigma2 * CTF^2 * w / sum; each sum then back-projected into its
+    class at the over-rotation's orientation.  Returns (data [K][pad][pad]
+    [pad/2+1] complex, weight [K][pad][pad][pad/2+1])."""
+    from oracle.select3d_oracle import lists_from_dump
+    pp = f"pool{pool}_"
+    g = lambda k: d[k] if k in d or not k.startswith(pp) else d["pool0_" + k[len(pp):]]  # noqa: E731
+    ic = lambda k: int(np.asarray(d[k]).ravel()[0])  # noqa: E731
+    ori, cur = ic("ori_size"), ic("current_size")
+    K, ndir, npsi = ic("nr_classes"), ic("nr_dir"), ic("nr_psi")
+    r_max, padding = ic("projector_r_max"), ic("projector_padding_factor")
+    do_map, do_ctf, scale = ic("do_map"), ic("do_ctf_correction"), ic("do_scale_correction")
+    fudge = float(np.asarray(d["sigma2_fudge"]).ravel()[0])
+    curF = cur // 2 + 1
+    angles = g(pp + "pass1_angles")
+    otx, oty = g(pp + "pass1_over_trans_x"), g(pp + "pass1_over_trans_y")
+    nor, notr = angles.shape[2], otx.shape[1]
+    mres = np.asarray(d["Mresol_fine"]).reshape(cur, curF)
+    s2 = np.asarray(d["sigma2_noise"])
+    group = np.asarray(g(pp + "group")).astype(int)
+    sc = np.asarray(d["scale_correction"])
+    sig, sumw = g(pp + "pass1_significant_weight"), g(pp + "pass1_sum_weight")
+    pad = d["projector_data"].shape[1]
+    data = np.zeros((K, pad, pad, pad // 2 + 1), np.complex128)
+    weight = np.zeros((K, pad, pad, pad // 2 + 1))
+    for i, pl in enumerate(lists_from_dump(d, pp + "pass1_weight_")):
+        gi = group[i]
+        if do_map:
+            minv = np.where(mres > 0, 1.0 / (fudge * s2[gi][np.maximum(mres, 0)]), 0.0)
+            minv[0, 0] = 1.0 / (fudge * s2[gi][0])
+        else:
+            minv = np.ones((cur, curF))
+        ctf = np.asarray(g(pp + "Fctf")[i]).reshape(cur, curF) if do_ctf else np.ones((cur, curF))
+        if scale:
+            ctf = ctf * max(float(sc[gi]), 0.001)
+        mc = minv * ctf
+        Xn = (g(pp + "Fimg_nomask_real")[i] * mc.ravel()) + 1j * (g(pp + "Fimg_nomask_imag")[i] * mc.ravel())
+        w2 = mc * ctf
+        sums = {}
+        for kdp, h, w in zip(pl.kdp, pl.ihidden, pl.value):
+            if w < sig[i]:
+                continue
+            w = w / sumw[i]
+            itr, rest = divmod(int(h), nor * notr)
+            o, t = divmod(rest, notr)
+            sr, si = oracle_py.shift_image(Xn.real, Xn.imag, cur, float(otx[itr, t]), float(oty[itr, t]), ori)
+            key = (int(kdp), o)
+            if key not in sums:
+                sums[key] = [np.zeros((cur, curF), np.complex128), np.zeros((cur, curF))]
+            sums[key][0] += (sr + 1j * si).reshape(cur, curF) * w
+            sums[key][1] += w2 * w
+        for (kdp, o), (fr, fw) in sums.items():
+            kd, p = divmod(kdp, npsi)
+            k, j = divmod(kd, ndir)
+            backproject3d(data[k], weight[k], fr, fw, r_max, padding, euler_matrix(*angles[j, p, o]))
+    return data, weight
