@@ -15,9 +15,9 @@ from typing import Dict, Optional
 import numpy as np
 
 from . import abi
-from .map2d import GpuContext, _f64, _i32
+from .map2d import GpuContext, RomeError, _f64, _i32
 
-__all__ = ["Map3dPool", "map3d_estep_pool", "pool3d_from_dump", "fine_lists_from_dump"]
+__all__ = ["Map3dPool", "map3d_estep_pool", "store_weighted_sums", "pool3d_from_dump", "fine_lists_from_dump"]
 
 
 @dataclasses.dataclass
@@ -201,6 +201,60 @@ def map3d_estep_pool(ctx: GpuContext, p: Map3dPool, checkpoints: bool = False,
         for name in ("fine_index", "fine_diff2", "fine_weight"):
             o[name] = o[name][:n]
     return o
+
+
+def store_weighted_sums(p: Map3dPool, est: Dict[str, np.ndarray], power_imgs: np.ndarray, norm_in: np.ndarray,
+                        avg_norm_correction: float, do_norm_correction: bool, wsum: Dict[str, np.ndarray]):
+    """storeWeightedSums (src/map3d_optimizer.cpp:1933-2045), host side, FP64,
+    on the outputs of map3d_estep_pool (``est``: sum_weight, min_diff2, pmax,
+    wsum_norm_correction and, with scale correction, the
+    wsum_scale_correction_XA/AA spectra).
+
+    Per particle, in order: the power spectrum beyond the current size is
+    added to the group's wsum_sigma2_noise and to the norm-correction sum;
+    with norm correction NORM = NORM / avg_norm_correction * sqrt(2 sum)
+    and that value is added to wsum_avg_norm_correction; with scale
+    correction XA / scale and AA / scale^2 (the scale as stored, without the
+    clamp the E-step applies) are added to the group's
+    wsum_signal_product_spectra / wsum_reference_power_spectra; dLL is
+    -min_diff2 in cross-correlation mode, else log(sum_weight) - min_diff2 -
+    the sum over the current-size pixels with ires > 0 of log(2 pi sigma2).
+    Returns per-particle (dLL, NORM) and accumulates into ``wsum`` (keys
+    wsum_sigma2_noise, wsum_avg_norm_correction, wsum_LL, wsum_ave_Pmax and,
+    with scale correction, wsum_signal_product_spectra and
+    wsum_reference_power_spectra [G][ori/2+1])."""
+    cur_F = p.current_size // 2 + 1
+    ori_F = p.ori_size // 2 + 1
+    P = p.nr_images
+    dll = np.zeros(P)
+    norm = np.array(norm_in, np.float64).copy()
+    wnc = np.array(est["wsum_norm_correction"], np.float64).copy()
+    ires = np.asarray(p.Mresol_fine).ravel()
+    ires = ires[ires > 0]
+    # the sum over the pixels of log(2 pi sigma2), one per group
+    logsigma2 = np.log(2. * np.pi * np.asarray(p.sigma2_noise)[:, ires]).sum(axis=1)
+    for i in range(P):
+        g = int(p.group[i])
+        for r in range(cur_F, ori_F):
+            wsum["wsum_sigma2_noise"][g, r] += power_imgs[i, r]
+            wnc[i] += power_imgs[i, r]
+        if do_norm_correction:
+            old = norm[i] / avg_norm_correction
+            norm[i] = old * np.sqrt(wnc[i] * 2.)
+            wsum["wsum_avg_norm_correction"] += old * np.sqrt(wnc[i] * 2.)
+        if p.do_scale_correction:
+            s = float(p.scale_correction[g])
+            wsum["wsum_signal_product_spectra"][g] += est["wsum_scale_correction_XA"][i] / s
+            wsum["wsum_reference_power_spectra"][g] += est["wsum_scale_correction_AA"][i] / (s * s)
+        if est["sum_weight"][i] == 0:
+            raise RomeError(abi.ROME_ERR_NUMERIC, "exp_sum_weight[ipart]==0")
+        if p.do_cross_correlation:
+            dll[i] = -est["min_diff2"][i]
+        else:
+            dll[i] = np.log(est["sum_weight"][i]) - est["min_diff2"][i] - logsigma2[g]
+        wsum["wsum_LL"] += dll[i]
+        wsum["wsum_ave_Pmax"] += est["pmax"][i]
+    return dll, norm
 
 
 # per-particle outputs of map3d_estep_pool (the rest are the pool's model sums)

@@ -65,6 +65,12 @@ CASES3D = {
                               snr=2.0, pixel=4.0, seed=9),
                     dict(K=2, iter=2, angpix=4.0, ini_high=16, tau2_fudge=2, oversampling=1, healpix_order=1,
                          pool=4, offset_range=2, offset_step=1, ctf=1, uniform_directions=1, scale=1)),
+    # norm correction at 32^2 with the current size below the image size (30 of 32, coarse 12): the
+    # windowing of the fine pass, the power-spectrum fill of storeWeightedSums and the new NORM
+    "map3d_norm": (Map3dSpec(n_particles=96, size=32, n_classes=2, n_blobs=10, blob_sigma=(1.2, 2.5), max_shift=2.0,
+                             snr=0.5, pixel=4.0, seed=13),
+                   dict(K=2, iter=2, angpix=4.0, ini_high=24, tau2_fudge=2, oversampling=1, healpix_order=1,
+                        pool=4, offset_range=2, offset_step=1, ctf=1, uniform_directions=1, norm=1)),
 }
 # 128^2 cases of the MAP3D configuration's shape (HEALPix order 2: 192 directions x 24 psi, 13
 # translations, oversampling 1, fine pass at the full size, M-step into the pad-259 grid).  The
@@ -147,6 +153,10 @@ CASESRECON = {
 }
 
 SKIP3D = ("Fimg_shifted_real", "Fimg_shifted_imag", "local_Fctf", "Minvsigma2", "local_sqrtXi2")
+# cases whose fixture keeps the E-step records only: the whole-iteration back-projectors and the maps
+# before and after the M-step are left out (no test of these cases reconstructs)
+ESTEP_ONLY3D = ("map3d_norm",)
+MSTEP3D = ("iter_bp_data", "iter_bp_weight", "Irefs_before", "Irefs_after")
 
 # arrays copied from the dump into the fixture (the per-translation shifted
 # images and per-orientation projections are large and are checked through
@@ -175,6 +185,8 @@ def make_case3d(name: str):
         d = load_dump(dump)
         # the image norms of the CC denominator are kept where the dumped iteration runs in CC mode
         skip = tuple(x for x in SKIP3D if not (opt.get("always_cc") and x == "local_sqrtXi2"))
+        if name in ESTEP_ONLY3D:
+            skip += MSTEP3D
         keep = {k: v for k, v in d.items() if not k.endswith(skip)}
         keep["meta_options"] = np.array([str(opt)])
         out = os.path.join(HERE, name + ".npz")

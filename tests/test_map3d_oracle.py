@@ -1,10 +1,13 @@
-"""The CPU restatement of the MAP3D coarse pass (oracle/map3d_oracle.py:
-windowing, Minvsigma2, translated images, MyProjector::project, CTF and
-intensity scale on the references, get_diff) pinned against the coarse
-squared differences the reference itself recorded (tests/golden/map3d_a,
-map3d_scale, map3d_cc): the same hypotheses computed and every value within
-1e-10 relative (both FP64; only the summation order differs), and in
-cross-correlation mode the recorded image norms.  No GPU."""
+"""The CPU restatement of the MAP3D E-step (oracle/map3d_oracle.py)
+pinned stage by stage against what the reference itself recorded
+(tests/golden/map3d_a, map3d_scale, map3d_cc and map3d_norm, the last at a
+current size of 30 below the 32-pixel images): the coarse pass (windowing,
+Minvsigma2, translated images, MyProjector::project, CTF and intensity scale
+on the references, get_diff; the same hypotheses computed, every value
+within 1e-10 relative, and in cross-correlation mode the recorded image
+norms), the fine pass over the recorded coarse-significant points, the model
+sums of updateOtherParams and the class back-projectors, each from the
+reference's recorded input of that stage.  No GPU."""
 import numpy as np
 import pytest
 
@@ -21,7 +24,7 @@ def recorded_coarse(g, shape):
     return out
 
 
-@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc", "map3d_norm"])
 def test_coarse_pass_matches_reference(golden, case):
     g = golden[case]
     cc = bool(int(g["do_cross_correlation"][0])) if "do_cross_correlation" in g else False
@@ -36,7 +39,7 @@ def test_coarse_pass_matches_reference(golden, case):
         np.testing.assert_allclose(norms, g["pool0_pass0_local_sqrtXi2"], rtol=1e-12)
 
 
-@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc", "map3d_norm"])
 def test_fine_pass_matches_reference(golden, case):
     """The fine pass over the coarse points the reference recorded as
     significant: the same list (order and ihidden) and every value within
@@ -54,7 +57,7 @@ def test_fine_pass_matches_reference(golden, case):
     assert worst <= 1e-10
 
 
-@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc", "map3d_norm"])
 def test_update_other_params_matches_reference(golden, case):
     """updateOtherParams restated on the recorded fine-pass weights: the
     model sums of the pool, the norm-correction sums and (scale correction)
@@ -74,7 +77,7 @@ def test_update_other_params_matches_reference(golden, case):
             assert np.max(np.abs(o[k] - ref)) <= 1e-11 * np.max(np.abs(ref)), k
 
 
-@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc"])
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_cc", "map3d_norm"])
 def test_back_projection_matches_reference(golden, case):
     """backProjection restated on the recorded fine-pass weights: the
     pool's class back-projectors (data and weight) within 1e-13 of their

@@ -1,6 +1,6 @@
 """The CPU restatement of the MAP3D posterior and significance steps
 (oracle/select3d_oracle.py) pinned against the reference's own recorded
-lists (tests/golden/map3d_a, map3d_scale, map3d_cc: oracle/_ref/map3d_dump):
+lists (tests/golden/map3d_a, map3d_scale, map3d_cc, map3d_norm: oracle/_ref/map3d_dump):
 from the recorded diff2 lists it reproduces the recorded weights (1e-13
 relative), exp_sum_weight (1e-12), significant_weight and NR_SIGN, the
 coarse significance mask, and in cross-correlation mode the single weight-1
@@ -17,7 +17,7 @@ def _pass_shape(g, p):
     return int(ang.shape[2]), int(otx.shape[1])
 
 
-@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale"])
+@pytest.mark.parametrize("case", ["map3d_a", "map3d_scale", "map3d_norm"])
 @pytest.mark.parametrize("ipass", [0, 1])
 def test_ml_weights_and_significance_match_reference(golden, case, ipass):
     g = golden[case]
