@@ -444,6 +444,18 @@ int main(int argc, char* argv[]) {
         d.f64("sigma2_class_after", sig.data(), {K, oF});
         d.f64("data_vs_prior_after", dvp.data(), {K, oF});
         d.f64("pdf_class_after", mlModel.pdf_class.wptrAll(), {K});
+        // the rest of the model as maximizationOtherParameters (map2d_optimizer.cpp:1984-2045) left it
+        d.f64("sigma2_noise_after", flat2(mlModel.sigma2_noise, G, oF).data(), {G, oF});
+        std::vector<double> pdir(K);
+        for (int k = 0; k < K; k++) pdir[k] = mlModel.pdf_direction[k][0];
+        d.f64("pdf_direction_after", pdir.data(), {K});
+        d.f64("prior_offsetx_class_after", mlModel.prior_offsetx_class.wptrAll(), {K});
+        d.f64("prior_offsety_class_after", mlModel.prior_offsety_class.wptrAll(), {K});
+        d.scalar("sigma2_offset_after", mlModel.sigma2_offset);
+        d.scalar("avg_norm_correction_after", mlModel.avg_norm_correction);
+        d.scalar("LL_after", mlModel.LL);
+        d.scalar("ave_Pmax_after", mlModel.ave_Pmax);
+        d.iscalar("refs_are_ctf_corrected_after", refs_are_ctf_corrected);
     }
     std::cout << "map2d_dump: done" << std::endl;
     return 0;

@@ -515,6 +515,17 @@ int main(int argc, char* argv[]) {
         d.f64("sigma2_class_after", sig.data(), {K, oF});
         d.f64("data_vs_prior_after", dvp.data(), {K, oF});
         d.f64("pdf_class_after", mlModel.pdf_class.wptrAll(), {K});
+        // the rest of the model as maximizationOtherParameters (map3d_optimizer.cpp:2620-2798) left it
+        const int nd = mlModel.nr_directions;
+        d.f64("sigma2_noise_after", flat2(mlModel.sigma2_noise, G, oF).data(), {G, oF});
+        d.f64("pdf_direction_after", flat2(mlModel.pdf_direction, K, nd).data(), {K, nd});
+        d.scalar("sigma2_offset_after", mlModel.sigma2_offset);
+        d.scalar("avg_norm_correction_after", mlModel.avg_norm_correction);
+        d.f64("scale_correction_after", mlModel.scale_correction.wptrAll(), {G});
+        d.scalar("LL_after", mlModel.LL);
+        d.scalar("ave_Pmax_after", mlModel.ave_Pmax);
+        d.i32("nr_particles_group", mlModel.nr_particles_group.wptrAll(), {G});
+        d.iscalar("refs_are_ctf_corrected_after", refs_are_ctf_corrected);
     }
     std::cout << "map3d_dump: done" << std::endl;
     return 0;

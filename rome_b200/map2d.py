@@ -574,6 +574,62 @@ def store_weighted_sums(p: Map2dPool, est: Dict[str, np.ndarray], power_imgs: np
     return dll, norm
 
 
+
+def _scalar(v) -> float:
+    """A model scalar given as a number or a one-element array."""
+    return float(np.asarray(v, np.float64).ravel()[0])
+
+
+def _running_sum(v) -> float:
+    """Sum in index order (the reference's sequential FP64 loops)."""
+    t = 0.0
+    for x in np.asarray(v, np.float64).ravel():
+        t += float(x)
+    return t
+
+
+def maximization_other_parameters(model: Dict, wsum: Dict, Npix_per_shell: np.ndarray, do_norm_correction: bool,
+                                  do_ctf_correction: bool) -> Dict:
+    """maximizationOtherParameters of MAP2D (src/map2d_optimizer.cpp:1984-2045),
+    host side, FP64: the model parameters other than the class maps, from the
+    iteration's summed weights.  ``model`` (updated in place and returned):
+    pdf_class [K], pdf_direction [K], prior_offsetx_class / prior_offsety_class
+    [K], sigma2_offset, sigma2_noise [G][ori/2+1], avg_norm_correction, LL,
+    ave_Pmax, refs_are_ctf_corrected.  ``wsum``: the wsum_* sums of every pool
+    of the iteration (wsum_pdf_class, wsum_pdf_direction,
+    wsum_prior_offsetx_class / y, wsum_sigma2_offset, wsum_sigma2_noise,
+    wsum_sumw_group, wsum_avg_norm_correction, wsum_LL, wsum_ave_Pmax).
+
+    With W the sum of wsum_pdf_class: pdf_class and pdf_direction are their
+    sums over W, a class's prior offset is its weighted offset sum over its
+    weight (0 for a class without weight), sigma2_offset = wsum_sigma2_offset
+    / 2W, sigma2_noise[g][n] = wsum_sigma2_noise[g][n] / (2 wsum_sumw_group[g]
+    Npix_per_shell[n]), avg_norm_correction (with norm correction) =
+    wsum_avg_norm_correction / W, LL = wsum_LL, ave_Pmax = wsum_ave_Pmax / W;
+    with CTF correction the references count as CTF-corrected from now on."""
+    wpc = np.asarray(wsum["wsum_pdf_class"], np.float64).ravel()
+    K = wpc.size
+    W = _running_sum(wpc)
+    if do_norm_correction:
+        model["avg_norm_correction"] = _scalar(wsum["wsum_avg_norm_correction"]) / W
+    model["pdf_class"] = wpc / W
+    px = np.asarray(wsum["wsum_prior_offsetx_class"], np.float64).ravel()
+    py = np.asarray(wsum["wsum_prior_offsety_class"], np.float64).ravel()
+    model["prior_offsetx_class"] = np.array([px[k] / wpc[k] if wpc[k] > 0. else 0. for k in range(K)])
+    model["prior_offsety_class"] = np.array([py[k] / wpc[k] if wpc[k] > 0. else 0. for k in range(K)])
+    model["pdf_direction"] = np.asarray(wsum["wsum_pdf_direction"], np.float64).reshape(K) / W
+    model["sigma2_offset"] = _scalar(wsum["wsum_sigma2_offset"]) / (2. * W)
+    sumw = np.asarray(wsum["wsum_sumw_group"], np.float64).ravel()
+    npix = np.asarray(Npix_per_shell, np.float64).ravel()
+    with np.errstate(divide="ignore", invalid="ignore"):  # an empty group or shell divides by 0, as in C
+        model["sigma2_noise"] = np.asarray(wsum["wsum_sigma2_noise"], np.float64) / (2. * sumw[:, None] * npix[None, :])
+    if do_ctf_correction:
+        model["refs_are_ctf_corrected"] = True
+    model["LL"] = _scalar(wsum["wsum_LL"])
+    model["ave_Pmax"] = _scalar(wsum["wsum_ave_Pmax"]) / W
+    return model
+
+
 def load_dump(path: str) -> Dict[str, np.ndarray]:
     """Read a reference-harness dump directory (manifest.txt + *.bin)."""
     import os

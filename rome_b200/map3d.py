@@ -15,9 +15,9 @@ from typing import Dict, Optional
 import numpy as np
 
 from . import abi
-from .map2d import GpuContext, RomeError, _f64, _i32
+from .map2d import GpuContext, RomeError, _f64, _i32, _running_sum, _scalar
 
-__all__ = ["Map3dPool", "map3d_estep_pool", "store_weighted_sums", "pool3d_from_dump", "fine_lists_from_dump"]
+__all__ = ["Map3dPool", "map3d_estep_pool", "store_weighted_sums", "maximization_other_parameters", "pool3d_from_dump", "fine_lists_from_dump"]
 
 
 @dataclasses.dataclass
@@ -255,6 +255,74 @@ def store_weighted_sums(p: Map3dPool, est: Dict[str, np.ndarray], power_imgs: np
         wsum["wsum_LL"] += dll[i]
         wsum["wsum_ave_Pmax"] += est["pmax"][i]
     return dll, norm
+
+
+
+def maximization_other_parameters(model: Dict, wsum: Dict, Npix_per_shell: np.ndarray,
+                                  nr_particles_group: np.ndarray, do_norm_correction: bool,
+                                  do_scale_correction: bool, do_ctf_correction: bool,
+                                  cross_correlation: bool = False, first_iteration_cc: bool = False) -> Dict:
+    """maximizationOtherParameters of MAP3D (src/map3d_optimizer.cpp:2620-2798),
+    host side, FP64: the model parameters other than the class maps, from the
+    iteration's summed weights.  ``model`` (updated in place and returned):
+    pdf_class [K], pdf_direction [K][ndir], sigma2_offset, sigma2_noise
+    [G][ori/2+1], scale_correction [G], avg_norm_correction, LL, ave_Pmax,
+    refs_are_ctf_corrected.  ``wsum``: the wsum_* sums of every pool of the
+    iteration (with scale correction also wsum_signal_product_spectra and
+    wsum_reference_power_spectra [G][ori/2+1]).
+
+    With W the sum of wsum_pdf_class: avg_norm_correction (with norm
+    correction) = wsum_avg_norm_correction / W; with scale correction each
+    group's scale is sum(XA) / sum(AA) (1 without reference power), held
+    within [median / 5, 5 median] of the groups (the median is element G / 2
+    of the sorted scales), then divided by the particle-weighted mean scale;
+    pdf_class and pdf_direction are their sums over W, sigma2_offset =
+    wsum_sigma2_offset / 2W, sigma2_noise[g][n] = wsum_sigma2_noise[g][n] /
+    (2 wsum_sumw_group[g] Npix_per_shell[n]); LL = wsum_LL (over W in
+    cross-correlation mode: the mean correlation), ave_Pmax = wsum_ave_Pmax /
+    W; with CTF correction the references count as CTF-corrected from now
+    on.  The first iteration of -firstiter_cc also low-pass filters the
+    class maps and seeds every class from the first; that step stays with
+    the caller (ROME_ERR_UNSUPPORTED here)."""
+    if first_iteration_cc:
+        raise RomeError(abi.ROME_ERR_UNSUPPORTED,
+                        "the first -firstiter_cc iteration filters the class maps: the caller's own step")
+    wpc = np.asarray(wsum["wsum_pdf_class"], np.float64).ravel()
+    K = wpc.size
+    W = _running_sum(wpc)
+    if do_norm_correction:
+        model["avg_norm_correction"] = _scalar(wsum["wsum_avg_norm_correction"]) / W
+    if do_scale_correction:
+        xa = np.asarray(wsum["wsum_signal_product_spectra"], np.float64)
+        aa = np.asarray(wsum["wsum_reference_power_spectra"], np.float64)
+        G = xa.shape[0]
+        sc = np.empty(G)
+        for g in range(G):
+            sxa, saa = _running_sum(xa[g]), _running_sum(aa[g])
+            sc[g] = sxa / saa if saa > 0. else 1.
+        median = float(np.sort(sc)[G // 2])
+        avg, nr = 0.0, 0.0
+        npg = np.asarray(nr_particles_group).ravel()
+        for g in range(G):
+            if sc[g] > 5. * median:
+                sc[g] = 5. * median
+            elif sc[g] < median / 5.:
+                sc[g] = median / 5.
+            avg += float(npg[g]) * sc[g]
+            nr += float(npg[g])
+        model["scale_correction"] = sc / (avg / nr)
+    model["pdf_class"] = wpc / W
+    model["pdf_direction"] = np.asarray(wsum["wsum_pdf_direction"], np.float64).reshape(K, -1) / W
+    model["sigma2_offset"] = _scalar(wsum["wsum_sigma2_offset"]) / (2. * W)
+    sumw = np.asarray(wsum["wsum_sumw_group"], np.float64).ravel()
+    npix = np.asarray(Npix_per_shell, np.float64).ravel()
+    with np.errstate(divide="ignore", invalid="ignore"):  # an empty group or shell divides by 0, as in C
+        model["sigma2_noise"] = np.asarray(wsum["wsum_sigma2_noise"], np.float64) / (2. * sumw[:, None] * npix[None, :])
+    if do_ctf_correction:
+        model["refs_are_ctf_corrected"] = True
+    model["LL"] = _scalar(wsum["wsum_LL"]) / W if cross_correlation else _scalar(wsum["wsum_LL"])
+    model["ave_Pmax"] = _scalar(wsum["wsum_ave_Pmax"]) / W
+    return model
 
 
 # per-particle outputs of map3d_estep_pool (the rest are the pool's model sums)

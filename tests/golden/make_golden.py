@@ -48,7 +48,10 @@ CASES = {
                      offset_step=1, ctf=1)),
 }
 
-# 3D cases: (dataset spec, reference options) for oracle/_ref/map3d_dump
+# 3D cases: (dataset spec, reference options) for oracle/_ref/map3d_dump.  The reference fills a
+# particle's power spectrum only when the current size is below the image size
+# (setFourierTransforms, src/exp_model.h:568-571); at full size pool*_power_imgs holds whatever its
+# buffer held, which nothing reads, so those bytes alone differ from one generation to the next.
 CASES3D = {
     # HEALPix order 1 (48 directions, 12 psi), oversampling 1, +-2 px step 1, iteration 2
     "map3d_a": (Map3dSpec(n_particles=96, size=24, n_classes=2, n_blobs=10, blob_sigma=(1.2, 2.5), max_shift=2.0,
