@@ -46,6 +46,12 @@ CASES = {
                           snr=0.05, pixel=2.0, seed=1),
                 dict(K=3, iter=2, angpix=2.0, tau2_fudge=2, oversampling=0, pool=6, psi_step=10, offset_range=5,
                      offset_step=1, ctf=1)),
+    # norm correction (per-particle NORM and avg_norm_correction after iteration 1) and the zero mask
+    # (zeros outside the particle instead of seeded noise), single pass
+    "map2d_norm": (Map2dSpec(n_particles=40, size=32, n_classes=2, n_blobs=8, blob_sigma=(1.5, 3.0), max_shift=2.0,
+                             snr=0.2, pixel=4.0, seed=4),
+                   dict(K=2, iter=2, angpix=4.0, tau2_fudge=2, oversampling=0, pool=10, psi_step=30, offset_range=2,
+                        offset_step=1, ctf=1, norm=1, zero_mask=1)),
 }
 
 # 3D cases: (dataset spec, reference options) for oracle/_ref/map3d_dump.  The reference fills a

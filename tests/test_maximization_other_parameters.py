@@ -38,7 +38,7 @@ def _check(m, g, names):
     assert bool(m["refs_are_ctf_corrected"]) == bool(int(g["refs_are_ctf_corrected_after"][0]))
 
 
-@pytest.mark.parametrize("case", ["map2d_a", "map2d_b", "map2d_c"])
+@pytest.mark.parametrize("case", ["map2d_a", "map2d_b", "map2d_c", "map2d_norm"])
 def test_maximization_other_parameters_2d(golden, case):
     g = golden[case]
     wsum = {k: g["iter_" + k] for k in WSUM + ("wsum_prior_offsetx_class", "wsum_prior_offsety_class")}

@@ -13,7 +13,7 @@ import pytest
 from oracle import oracle_py
 from tests.util import golden_pool, relerr
 
-CASES = ["map2d_a", "map2d_b", "map2d_c"]
+CASES = ["map2d_a", "map2d_b", "map2d_c", "map2d_norm"]
 
 
 @pytest.fixture(scope="module")

@@ -1,6 +1,7 @@
 """Pin the particle-preparation oracle (oracle/prep_oracle.py) against the
 reference's own ParticleModel::setFourierTransforms outputs
-(src/exp_model.h:397-640) recorded in tests/golden/map2d_*.npz: the
+(src/exp_model.h:397-640) recorded in tests/golden/map2d_*.npz (map2d_norm
+with norm correction and the zero mask): the
 unmasked and masked transforms at current_size, the CTF images, the power
 spectra, highres_Xi2 and the rounded old offsets of the first pool, from
 the raw images and metadata recorded beside them."""
@@ -10,7 +11,7 @@ import pytest
 from oracle import prep_oracle as po
 from tests.util import relerr
 
-CASES = ["map2d_a", "map2d_b", "map2d_c"]
+CASES = ["map2d_a", "map2d_b", "map2d_c", "map2d_norm"]
 
 
 def run_case(g, n=None):
@@ -36,15 +37,16 @@ def test_unmasked_transform(prepared, golden, case):
 
 
 @pytest.mark.parametrize("case", CASES)
-def test_masked_transform_with_seeded_noise(prepared, golden, case):
-    """The noise outside the mask comes from the reference's seeded
-    generator: a wrong draw order or seed moves the masked transform by tens
-    of percent, the restatement agrees to FP64 round-off."""
+def test_masked_transform(prepared, golden, case):
+    """The masked transform, outside the mask either the reference's seeded
+    noise (a wrong draw order or seed moves it by tens of percent) or, with
+    the zero mask (map2d_norm), the background average: the restatement
+    agrees to FP64 round-off."""
     g, out = golden[case], prepared[case]
-    assert not po.options_from_golden(g)["do_zero_mask"]
     gm = g["pool0_Fimg_real"] + 1j * g["pool0_Fimg_imag"]
     assert np.abs(out["Fimg"] - gm).max() / np.abs(gm).max() < 1e-13
     assert np.abs(gm - (g["pool0_Fimg_nomask_real"] + 1j * g["pool0_Fimg_nomask_imag"])).max() > 1e-3 * np.abs(gm).max()
+    assert po.options_from_golden(g)["do_zero_mask"] == (case == "map2d_norm")
 
 
 @pytest.mark.parametrize("case", CASES)

@@ -13,7 +13,7 @@ from rome_b200.map2d import pool_from_dump, store_weighted_sums
 from tests.util import relerr
 
 
-@pytest.mark.parametrize("case", ["map2d_a", "map2d_b", "map2d_c"])
+@pytest.mark.parametrize("case", ["map2d_a", "map2d_b", "map2d_c", "map2d_norm"])
 def test_store_weighted_sums_matches_reference(golden, case):
     g = golden[case]
     p = pool_from_dump(g, 0)
