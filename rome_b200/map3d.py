@@ -17,7 +17,8 @@ import numpy as np
 from . import abi
 from .map2d import GpuContext, RomeError, _f64, _i32, _running_sum, _scalar
 
-__all__ = ["Map3dPool", "map3d_estep_pool", "store_weighted_sums", "maximization_other_parameters", "pool3d_from_dump", "fine_lists_from_dump"]
+__all__ = ["Map3dPool", "map3d_estep_pool", "take_pool3d", "merge_results3d", "store_weighted_sums",
+           "maximization_other_parameters", "pool3d_from_dump", "fine_lists_from_dump"]
 
 
 @dataclasses.dataclass
@@ -327,7 +328,38 @@ def maximization_other_parameters(model: Dict, wsum: Dict, Npix_per_shell: np.nd
 
 # per-particle outputs of map3d_estep_pool (the rest are the pool's model sums)
 _PER_PARTICLE = ("min_diff2", "sum_weight", "significant_weight", "wsum_norm_correction", "pmax", "rot", "tilt",
-                 "psi", "xoff", "yoff", "nr_sign", "cls", "wsum_scale_correction_XA", "wsum_scale_correction_AA")
+                 "psi", "xoff", "yoff", "nr_sign", "cls", "wsum_scale_correction_XA", "wsum_scale_correction_AA",
+                 "post_coarse")
+# the per-particle inputs of a Map3dPool
+_PARTICLE_FIELDS = ("Fimg_real", "Fimg_imag", "Fimg_nomask_real", "Fimg_nomask_imag", "Fctf", "highres_Xi2",
+                    "old_offsetx", "old_offsety", "group")
+
+
+def take_pool3d(p: Map3dPool, idx) -> Map3dPool:
+    """The particles `idx` of a 3D pool, in that order (same model and sampling)."""
+    idx = np.asarray(idx, np.int64)
+    q = dataclasses.replace(p)
+    for name in _PARTICLE_FIELDS:
+        setattr(q, name, np.ascontiguousarray(np.asarray(getattr(p, name))[idx]))
+    if p.proposals is not None:
+        q.proposals = np.ascontiguousarray(p.proposals[idx])
+    return q
+
+
+def merge_results3d(parts, n: int) -> Dict[str, np.ndarray]:
+    """Outputs of 3D E-steps over disjoint particle subsets [(idx, result)] of
+    one pool of n particles: per-particle outputs scattered back to pool
+    order, the pool's model sums added."""
+    out: Dict[str, np.ndarray] = {}
+    for idx, r in parts:
+        for name, a in r.items():
+            if name in _PER_PARTICLE:
+                if name not in out:
+                    out[name] = np.zeros((n,) + a.shape[1:], a.dtype)
+                out[name][idx] = a
+            else:
+                out[name] = out[name] + a if name in out else np.array(a, copy=True)
+    return out
 
 
 def map3d_estep_pools_adaptive(ctx: GpuContext, p: Map3dPool, dev: Optional[dict] = None,

@@ -268,6 +268,36 @@ def learned_estep_pools(ctx: GpuContext, net: ProposalNet, pools, k: int, min_ma
             ctx.add_backprojectors(c, clear=True)
 
 
+def learned_estep3d(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: float = 0.0,
+                    marginals: bool = False):
+    """MAP3D E-step of one pool (Map3dPool) with learned proposals: the
+    network (one output per (class, direction), psi mod 180) proposes the 2k
+    coarse orientations (class * nr_dir + dir) * nr_psi + psi of each
+    particle's top-k outputs and the coarse pass searches only those, with
+    every translation (the fine pass refines the coarse-significant points
+    among them as usual); particles whose top-k outputs hold less than
+    `min_mass` of the network's probability are searched exhaustively
+    (map3d_estep_pools_adaptive, which splits a pool whose fine pass would
+    not fit).  Both calls back-project into the context's back-projectors.
+    Returns (the E-step outputs in pool order, proposals [P][2k], mass [P],
+    the indices of the exhaustively searched particles)."""
+    from .map3d import map3d_estep_pool, map3d_estep_pools_adaptive, merge_results3d, take_pool3d
+    props, mass = net.propose(pool, k)
+    n = pool.nr_images
+    low = np.flatnonzero(mass < min_mass)
+    high = np.flatnonzero(mass >= min_mass)
+    parts = []
+    if high.size:
+        sub = pool if low.size == 0 else take_pool3d(pool, high)
+        parts.append((high, map3d_estep_pool(ctx, sub, marginals=marginals, proposals=props[high])))
+    if low.size:
+        if marginals:
+            parts.append((low, map3d_estep_pool(ctx, take_pool3d(pool, low), marginals=True)))
+        else:
+            parts.append((low, map3d_estep_pools_adaptive(ctx, take_pool3d(pool, low))))
+    return merge_results3d(parts, n), props, mass, low
+
+
 def _pool_part(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: float, marginals: bool):
     """propose + restricted E-step of one pool's confident particles; the rest
     are returned as a view for the exhaustive fallback."""

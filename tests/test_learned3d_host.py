@@ -1,0 +1,70 @@
+"""Host logic of the 3D learned E-step (rome_b200.proposal.learned_estep3d),
+with the network's proposals and the library's E-step replaced by fakes:
+the particles whose top-k outputs hold at least min_mass are searched over
+their own proposals, the others exhaustively, and the two calls' outputs
+come back in pool order with the pool sums added.  CPU only."""
+import numpy as np
+
+from rome_b200 import map3d, proposal
+from rome_b200.map3d import merge_results3d, pool3d_from_dump, take_pool3d
+
+
+class FakeNet:
+    def __init__(self, props, mass):
+        self.props, self.mass = props, mass
+
+    def propose(self, pool, k):
+        assert pool.nr_images == len(self.mass)
+        return self.props, self.mass
+
+
+def fake_estep(calls, tag):
+    """An E-step that names each particle by its highres_Xi2 and records the call."""
+    def run(ctx, p, marginals=False, proposals=None, **kw):
+        calls.append((tag, p.highres_Xi2.copy(), None if proposals is None else proposals.copy()))
+        n = p.nr_images
+        return {"min_diff2": p.highres_Xi2 * 2.0, "cls": np.arange(n, dtype=np.int32) + (100 if tag == "r" else 200),
+                "wsum_pdf_class": np.full(2, float(n)), "wsum_sigma2_offset": np.ones(1)}
+    return run
+
+
+def test_split_and_merge(golden, monkeypatch):
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    p.highres_Xi2 = np.arange(p.nr_images, dtype=np.float64) + 1.0  # particle i is named i + 1
+    calls = []
+    monkeypatch.setattr(map3d, "map3d_estep_pool", fake_estep(calls, "r"))
+    monkeypatch.setattr(map3d, "map3d_estep_pools_adaptive", fake_estep(calls, "x"))
+    props = np.arange(4 * 6, dtype=np.int32).reshape(4, 6)
+    mass = np.array([0.99, 0.5, 0.999, 0.1], np.float32)
+    out, pr, ms, low = proposal.learned_estep3d(None, FakeNet(props, mass), p, 3, min_mass=0.95)
+    assert low.tolist() == [1, 3]
+    (t0, ids0, pr0), (t1, ids1, pr1) = calls
+    assert t0 == "r" and ids0.tolist() == [1.0, 3.0] and np.array_equal(pr0, props[[0, 2]])
+    assert t1 == "x" and ids1.tolist() == [2.0, 4.0] and pr1 is None
+    assert out["min_diff2"].tolist() == [2.0, 4.0, 6.0, 8.0]
+    assert out["cls"].tolist() == [100, 200, 101, 201]
+    assert out["wsum_pdf_class"].tolist() == [4.0, 4.0] and out["wsum_sigma2_offset"].tolist() == [2.0]
+
+
+def test_all_confident_is_one_restricted_call(golden, monkeypatch):
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    calls = []
+    monkeypatch.setattr(map3d, "map3d_estep_pool", fake_estep(calls, "r"))
+    monkeypatch.setattr(map3d, "map3d_estep_pools_adaptive", fake_estep(calls, "x"))
+    props = np.zeros((4, 2), np.int32)
+    out, _, _, low = proposal.learned_estep3d(None, FakeNet(props, np.ones(4, np.float32)), p, 1, min_mass=0.5)
+    assert low.size == 0 and [c[0] for c in calls] == ["r"]
+    assert np.array_equal(calls[0][1], p.highres_Xi2)
+
+
+def test_take_and_merge_round_trip(golden):
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    q = take_pool3d(p, [2, 0])
+    assert q.nr_images == 2 and np.array_equal(q.Fimg_real, p.Fimg_real[[2, 0]])
+    assert np.array_equal(q.group, np.asarray(p.group)[[2, 0]]) and q.angles is p.angles
+    m = merge_results3d([(np.array([2, 0]), {"pmax": np.array([0.5, 0.25]), "wsum_sumw_group": np.ones(3)}),
+                         (np.array([1]), {"pmax": np.array([0.75]), "wsum_sumw_group": np.ones(3)})], 3)
+    assert m["pmax"].tolist() == [0.25, 0.75, 0.5] and m["wsum_sumw_group"].tolist() == [2.0, 2.0, 2.0]
