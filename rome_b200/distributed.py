@@ -27,9 +27,14 @@ import numpy as np
 __all__ = ["divide_equally", "divide_equally_pool", "allreduce_model_sums", "allreduce_backprojectors",
            "reduce_backprojectors_by_class", "broadcast_class_maps", "owner_of_class", "max_over_ranks"]
 
-# the pool sums of one E-step call (rome_b200.map2d.alloc_outputs), added over ranks
+# the model sums added over ranks (MLModel::reduceData, src/ml_model.cpp:587-637): the pool sums of the
+# E-step calls (rome_b200.map2d.alloc_outputs, rome_b200.map3d.map3d_estep_pool), then those the host-side
+# storeWeightedSums adds (the scale-correction group spectra, wsum_avg_norm_correction, wsum_LL,
+# wsum_ave_Pmax; scalars may be plain floats)
 MODEL_SUM_KEYS = ("wsum_sigma2_noise", "wsum_pdf_class", "wsum_pdf_direction", "wsum_prior_offsetx_class",
-                  "wsum_prior_offsety_class", "wsum_sigma2_offset", "wsum_sumw_group")
+                  "wsum_prior_offsety_class", "wsum_sigma2_offset", "wsum_sumw_group",
+                  "wsum_signal_product_spectra", "wsum_reference_power_spectra", "wsum_avg_norm_correction",
+                  "wsum_LL", "wsum_ave_Pmax")
 
 
 def divide_equally(n: int, size: int, rank: int) -> Tuple[int, int]:
@@ -64,8 +69,9 @@ def _allreduce_np(arrays: Dict[str, np.ndarray], device) -> Dict[str, np.ndarray
     flat = t.cpu().numpy()
     for k in keys:
         a = arrays[k]
-        out[k] = flat[off:off + a.size].reshape(a.shape).copy()
-        off += a.size
+        n = int(np.size(a))
+        out[k] = float(flat[off]) if np.ndim(a) == 0 else flat[off:off + n].reshape(np.shape(a)).copy()
+        off += n
     return out
 
 

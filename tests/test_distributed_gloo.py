@@ -55,9 +55,10 @@ def _worker(rank, world, port, q):
         rng = np.random.default_rng(rank)
         sums = {k: rng.normal(size=(3, 4) if k == "wsum_sigma2_noise" else (5,)) for k in MODEL_SUM_KEYS}
         sums["min_diff2"] = np.full(4, float(rank))  # per particle: not reduced
+        sums["wsum_LL"] = float(rank) + 0.25             # a host-side scalar as a plain float
         out = allreduce_model_sums(sums)
         m = max_over_ranks(10.0 + rank)
-        q.put((rank, {k: v.tolist() for k, v in out.items()}, m))
+        q.put((rank, {k: (v.tolist() if isinstance(v, np.ndarray) else v) for k, v in out.items()}, m))
     finally:
         dist.destroy_process_group()
 
@@ -82,11 +83,13 @@ def test_allreduce_model_sums_world2():
         for k in MODEL_SUM_KEYS:
             v = rng.normal(size=(3, 4) if k == "wsum_sigma2_noise" else (5,))
             want[k] = want.get(k, 0) + v
+    want["wsum_LL"] = 0.25 + 1.25
     for rank in range(2):
         out, m = res[rank]
         assert m == 11.0
         for k in MODEL_SUM_KEYS:
             np.testing.assert_allclose(np.array(out[k]), want[k], rtol=1e-15, atol=1e-15)
+        assert isinstance(out["wsum_LL"], float)
         assert out["min_diff2"] == [float(rank)] * 4
 
 
