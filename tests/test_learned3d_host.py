@@ -1,8 +1,11 @@
-"""Host logic of the 3D learned E-step (rome_b200.proposal.learned_estep3d),
-with the network's proposals and the library's E-step replaced by fakes:
-the particles whose top-k outputs hold at least min_mass are searched over
-their own proposals, the others exhaustively, and the two calls' outputs
-come back in pool order with the pool sums added.  CPU only."""
+"""Host logic of the 3D proposal-restricted E-steps (rome_b200.proposal:
+learned_estep3d, lowres_proposals3d, lowres_estep3d), with the network's
+proposals and the library's E-step replaced by fakes: the particles whose
+proposals hold at least min_mass are searched over them, the others
+exhaustively, and the two calls' outputs come back in pool order with the
+pool sums added; the low-resolution proposals are the top k of one
+exhaustive call at the small coarse size on the auxiliary context.  CPU
+only."""
 import numpy as np
 
 from rome_b200 import map3d, proposal
@@ -68,3 +71,47 @@ def test_take_and_merge_round_trip(golden):
     m = merge_results3d([(np.array([2, 0]), {"pmax": np.array([0.5, 0.25]), "wsum_sumw_group": np.ones(3)}),
                          (np.array([1]), {"pmax": np.array([0.75]), "wsum_sumw_group": np.ones(3)})], 3)
     assert m["pmax"].tolist() == [0.25, 0.75, 0.5] and m["wsum_sumw_group"].tolist() == [2.0, 2.0, 2.0]
+
+
+def test_lowres_proposals_from_the_small_coarse_pass(golden, monkeypatch):
+    """lowres_proposals3d: one exhaustive E-step call on the auxiliary
+    context at the small coarse size (its resolution table, a significance
+    fraction that keeps one coarse point), and the k most probable coarse
+    orientations of its posterior, ascending, with the mass they hold."""
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    Jc = p.nr_classes * p.nr_dir * p.nr_psi
+    rng = np.random.default_rng(1)
+    post = rng.random((p.nr_images, Jc))
+    post /= post.sum(1, keepdims=True)
+    seen = []
+
+    def fake(ctx, q, marginals=False, proposals=None, **kw):
+        seen.append((ctx, q.coarse_size, q.adaptive_fraction, marginals, proposals, q.Mresol_coarse))
+        return {"post_coarse": post}
+    monkeypatch.setattr(map3d, "map3d_estep_pool", fake)
+    props, mass = proposal.lowres_proposals3d("aux", p, 5, coarse_size=8)
+    (ctx, cs, frac, marg, pr, mres), = seen
+    assert ctx == "aux" and cs == 8 and frac < 1e-9 and marg and pr is None
+    from rome_b200.workload import mresol
+    assert np.array_equal(mres, mresol(8))
+    want = np.sort(np.argsort(-post, axis=1)[:, :5], axis=1)
+    assert np.array_equal(props, want) and props.dtype == np.int32
+    np.testing.assert_allclose(mass, np.take_along_axis(post, want, 1).sum(1), rtol=1e-12)
+
+
+def test_lowres_estep_splits_on_the_low_resolution_mass(golden, monkeypatch):
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    p.highres_Xi2 = np.arange(p.nr_images, dtype=np.float64) + 1.0
+    props = np.tile(np.arange(3, dtype=np.int32), (4, 1))
+    monkeypatch.setattr(proposal, "lowres_proposals3d",
+                        lambda aux, pool, k, cs=12: (props, np.array([0.2, 0.999, 0.9995, 0.5])))
+    calls = []
+    monkeypatch.setattr(map3d, "map3d_estep_pool", fake_estep(calls, "r"))
+    monkeypatch.setattr(map3d, "map3d_estep_pools_adaptive", fake_estep(calls, "x"))
+    out, pr, ms, low = proposal.lowres_estep3d("ctx", "aux", p, 3, min_mass=0.99)
+    assert low.tolist() == [0, 3]
+    assert [c[0] for c in calls] == ["r", "x"]
+    assert calls[0][1].tolist() == [2.0, 3.0] and calls[1][1].tolist() == [1.0, 4.0]
+    assert out["cls"].tolist() == [200, 100, 101, 201]
