@@ -64,6 +64,10 @@ def parse():
                     help="3D workloads: multiply the configured signal-to-noise ratios (calibration runs)")
     ap.add_argument("--min-mass", type=float, default=0.995,
                     help="particles whose top-k proposals hold less network probability are searched exhaustively")
+    ap.add_argument("--proposals3d", default="none", choices=["none", "lowres"],
+                    help="3D workloads: lowres restricts each particle's coarse pass to the --topk orientations "
+                         "of a low-resolution exhaustive coarse pass at --lowres-size (fallback below --min-mass)")
+    ap.add_argument("--lowres-size", type=int, default=12, help="coarse size of the low-resolution pass")
     return ap.parse_args()
 
 
@@ -780,6 +784,15 @@ def run_ours_3d(args):
         lanes.append(c)
     from concurrent.futures import ThreadPoolExecutor
     execs = [ThreadPoolExecutor(max_workers=1) for _ in lanes]
+    # low-resolution proposals: one auxiliary context per lane runs the small exhaustive coarse pass (its
+    # sums and back-projectors are discarded); its device time is counted with the lanes'
+    lowres = args.proposals3d == "lowres"
+    auxes = []
+    for _ in (lanes if lowres else []):
+        a = GpuContext(0, args.precision, profile=True)
+        a.set_projectors(proj, pool.ori_size, r_max)
+        auxes.append(a)
+    fallback = []
     prep_ctx = GpuContext(0, "fp32", profile=True)
     d_raw = torch.from_numpy(raw.images).cuda()
     dr = dataclasses.replace(raw, images=d_raw)
@@ -787,9 +800,19 @@ def run_ours_3d(args):
     del d_raw, dr
     host_raw = [pin_particles(slice_particles(raw, lo, hi)) for lo, hi in bounds]
 
+    def lowres_pool(c, a, sp):
+        from rome_b200.proposal import lowres_estep3d
+        out, _, _, low = lowres_estep3d(c, a, sp.pool, args.topk, args.lowres_size, args.min_mass, dev=sp.dev)
+        fallback.append((int(low.size), sp.pool.nr_images))
+        return out
+
     def run_lanes(pools):
-        futs = [execs[q % len(lanes)].submit(map3d_estep_pools_adaptive, lanes[q % len(lanes)], sp.pool, sp.dev)
-                for q, sp in enumerate(pools)]
+        if lowres:
+            futs = [execs[q % len(lanes)].submit(lowres_pool, lanes[q % len(lanes)], auxes[q % len(lanes)], sp)
+                    for q, sp in enumerate(pools)]
+        else:
+            futs = [execs[q % len(lanes)].submit(map3d_estep_pools_adaptive, lanes[q % len(lanes)], sp.pool, sp.dev)
+                    for q, sp in enumerate(pools)]
         res = [f.result() for f in futs]
         for c in lanes[1:]:
             ctx.add_backprojectors(c, clear=True)
@@ -803,18 +826,20 @@ def run_ours_3d(args):
 
     for _ in range(args.warmup):
         step()
-    for c in lanes:
+    for c in lanes + auxes:
         c.reset_timings()
+    fallback.clear()
     with ClockSampler(0) as clk:
         ms, last = _timed(torch, step, args.steps)
-    timings = merge_timings([c.get_timings() for c in lanes])
+    timings = merge_timings([c.get_timings() for c in lanes + auxes])
+    timed_fallback = list(fallback)
     step_e2e()
     e_ms, _ = _timed(torch, step_e2e, max(1, args.steps))
     cls = np.concatenate([r["cls"] for r in last]) - 1
     # the timed contexts' device memory is released before the comparison arm runs
     for e in execs:
         e.shutdown(wait=True)
-    for c in lanes:
+    for c in lanes + auxes:
         c.close()
     # the plain FP32 E-step on the same prepared particles: the comparison arm and the pose judge
     judge = {}
@@ -858,7 +883,9 @@ def run_ours_3d(args):
                 "kernel": "cross-term contraction (coarse tc_gemm_kernel + fine pass): 4 * active pixels flops "
                           "per hypothesis"}
     line = {
-        "metric": "MAP3D E-step particles/s (exhaustive search)", "value": round(N / (ms / args.steps / 1e3), 2),
+        "metric": "MAP3D E-step particles/s (" + ("coarse pass restricted to low-resolution proposals" if lowres
+                                                  else "exhaustive search") + ")",
+        "value": round(N / (ms / args.steps / 1e3), 2),
         "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms / args.steps, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": {"fp32": "f32", "bf16": "bf16", "bf16x3": "bf16x3"}[args.precision],
@@ -888,6 +915,11 @@ def run_ours_3d(args):
         "roofline": roof,
         "clocks": clk.summary(),
     }
+    if lowres:
+        line["proposals3d"] = {"kind": "lowres", "k": args.topk, "coarse_size": args.lowres_size,
+                               "min_mass": args.min_mass,
+                               "fallback_fraction": round(sum(a for a, _ in timed_fallback)
+                                                          / max(1, sum(b for _, b in timed_fallback)), 5)}
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, w)
     prep_ctx.close()

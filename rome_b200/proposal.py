@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
-from typing import Dict, List, Tuple
+from typing import Dict, List, Optional, Tuple
 
 import numpy as np
 
@@ -287,28 +287,29 @@ def learned_estep3d(ctx: GpuContext, net: ProposalNet, pool, k: int, min_mass: f
     return out, props, mass, low
 
 
-def lowres_proposals3d(aux: GpuContext, pool, k: int, coarse_size: int = 12):
+def lowres_proposals3d(aux: GpuContext, pool, k: int, coarse_size: int = 12, dev: Optional[dict] = None):
     """Coarse-pass proposals for a MAP3D pool from an exhaustive coarse pass
     at a small coarse size: every orientation and translation compared over
     the shells below coarse_size / 2 only, with the pool's priors.  The
     library's 3D E-step runs on `aux`, a second context with the same
     projectors, whose weighted sums and back-projectors are not used; its
     significance fraction is set so small that the fine pass refines one
-    coarse point per particle.  Returns (the k most probable coarse
-    orientations of each particle, ascending [P][k], and the low-resolution
-    posterior mass they hold [P])."""
+    coarse point per particle.  `dev`: the pool's images already on the
+    device (as for map3d_estep_pool).  Returns (the k most probable coarse
+    orientations of each particle, ascending [P][k], and the
+    low-resolution posterior mass they hold [P])."""
     from .map3d import map3d_estep_pool
     from .workload import mresol
     q = dataclasses.replace(pool, coarse_size=coarse_size, Mresol_coarse=mresol(coarse_size),
                             adaptive_fraction=1e-12, proposals=None)
-    post = map3d_estep_pool(aux, q, marginals=True)["post_coarse"]
+    post = map3d_estep_pool(aux, q, marginals=True, dev=dev)["post_coarse"]
     top = np.argpartition(-post, k - 1, axis=1)[:, :k]
     mass = np.take_along_axis(post, top, axis=1).sum(axis=1)
     return np.sort(top, axis=1).astype(np.int32), mass
 
 
 def lowres_estep3d(ctx: GpuContext, aux: GpuContext, pool, k: int, coarse_size: int = 12, min_mass: float = 0.0,
-                   marginals: bool = False):
+                   marginals: bool = False, dev: Optional[dict] = None):
     """MAP3D E-step of one pool with proposals from a low-resolution
     exhaustive coarse pass (lowres_proposals3d on `aux`): each particle's
     coarse pass at the pool's own coarse size searches only its k proposed
@@ -316,29 +317,41 @@ def lowres_estep3d(ctx: GpuContext, aux: GpuContext, pool, k: int, coarse_size: 
     less than `min_mass` of the low-resolution posterior are searched
     exhaustively.  Returns (outputs in pool order, proposals [P][k], mass
     [P], the indices of the exhaustively searched particles)."""
-    props, mass = lowres_proposals3d(aux, pool, k, coarse_size)
-    out, low = _restricted_or_exhaustive3d(ctx, pool, props, mass, min_mass, marginals)
+    props, mass = lowres_proposals3d(aux, pool, k, coarse_size, dev=dev)
+    out, low = _restricted_or_exhaustive3d(ctx, pool, props, mass, min_mass, marginals, dev=dev)
     return out, props, mass, low
 
 
+def _rows3d(pool, dev: Optional[dict], idx: np.ndarray):
+    """The particles idx of a pool and of its device images (None: host images only)."""
+    from .map3d import take_pool3d
+    if dev is None:
+        return take_pool3d(pool, idx), None
+    import torch
+    t = next(iter(dev.values()))
+    ix = torch.as_tensor(np.asarray(idx, np.int64), device=t.device)
+    return take_pool3d(pool, idx), {name: v.index_select(0, ix) for name, v in dev.items()}
+
+
 def _restricted_or_exhaustive3d(ctx: GpuContext, pool, props: np.ndarray, mass: np.ndarray, min_mass: float,
-                                marginals: bool):
+                                marginals: bool, dev: Optional[dict] = None):
     """The restricted coarse pass for the particles whose proposals hold at
     least min_mass, the exhaustive one for the rest; outputs merged back to
     pool order, sums added.  Returns (outputs, the exhaustive particles)."""
-    from .map3d import map3d_estep_pool, map3d_estep_pools_adaptive, merge_results3d, take_pool3d
+    from .map3d import map3d_estep_pool, map3d_estep_pools_adaptive, merge_results3d
     n = pool.nr_images
     low = np.flatnonzero(mass < min_mass)
     high = np.flatnonzero(mass >= min_mass)
     parts = []
     if high.size:
-        sub = pool if low.size == 0 else take_pool3d(pool, high)
-        parts.append((high, map3d_estep_pool(ctx, sub, marginals=marginals, proposals=props[high])))
+        sub, sdev = (pool, dev) if low.size == 0 else _rows3d(pool, dev, high)
+        parts.append((high, map3d_estep_pool(ctx, sub, marginals=marginals, proposals=props[high], dev=sdev)))
     if low.size:
+        sub, sdev = _rows3d(pool, dev, low)
         if marginals:
-            parts.append((low, map3d_estep_pool(ctx, take_pool3d(pool, low), marginals=True)))
+            parts.append((low, map3d_estep_pool(ctx, sub, marginals=True, dev=sdev)))
         else:
-            parts.append((low, map3d_estep_pools_adaptive(ctx, take_pool3d(pool, low))))
+            parts.append((low, map3d_estep_pools_adaptive(ctx, sub, dev=sdev)))
     return merge_results3d(parts, n), low
 
 

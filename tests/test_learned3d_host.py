@@ -106,7 +106,7 @@ def test_lowres_estep_splits_on_the_low_resolution_mass(golden, monkeypatch):
     p.highres_Xi2 = np.arange(p.nr_images, dtype=np.float64) + 1.0
     props = np.tile(np.arange(3, dtype=np.int32), (4, 1))
     monkeypatch.setattr(proposal, "lowres_proposals3d",
-                        lambda aux, pool, k, cs=12: (props, np.array([0.2, 0.999, 0.9995, 0.5])))
+                        lambda aux, pool, k, cs=12, **kw: (props, np.array([0.2, 0.999, 0.9995, 0.5])))
     calls = []
     monkeypatch.setattr(map3d, "map3d_estep_pool", fake_estep(calls, "r"))
     monkeypatch.setattr(map3d, "map3d_estep_pools_adaptive", fake_estep(calls, "x"))
@@ -115,3 +115,30 @@ def test_lowres_estep_splits_on_the_low_resolution_mass(golden, monkeypatch):
     assert [c[0] for c in calls] == ["r", "x"]
     assert calls[0][1].tolist() == [2.0, 3.0] and calls[1][1].tolist() == [1.0, 4.0]
     assert out["cls"].tolist() == [200, 100, 101, 201]
+
+
+def test_device_images_follow_the_split(golden, monkeypatch):
+    """With the images on the device (here CPU tensors standing in), each
+    call gets its own particles' rows of every image tensor."""
+    import torch
+    g = golden["map3d_a"]
+    p = pool3d_from_dump(g, 0)
+    p.highres_Xi2 = np.arange(p.nr_images, dtype=np.float64) + 1.0
+    dev = {"Fimg_real": torch.arange(4, dtype=torch.float64)[:, None].repeat(1, 3),
+           "Fctf": 10.0 + torch.arange(4, dtype=torch.float64)[:, None]}
+    seen = []
+
+    def fake(tag):
+        def run(ctx, q, marginals=False, proposals=None, dev=None, **kw):
+            seen.append((tag, q.highres_Xi2.tolist(), None if dev is None else dev["Fimg_real"][:, 0].tolist(),
+                         None if dev is None else dev["Fctf"][:, 0].tolist()))
+            return {"pmax": q.highres_Xi2.copy()}
+        return run
+    monkeypatch.setattr(map3d, "map3d_estep_pool", fake("r"))
+    monkeypatch.setattr(map3d, "map3d_estep_pools_adaptive", fake("x"))
+    props = np.zeros((4, 2), np.int32)
+    out, low = proposal._restricted_or_exhaustive3d("ctx", p, props, np.array([1.0, 0.0, 0.0, 1.0]), 0.5, False,
+                                                    dev=dev)
+    assert low.tolist() == [1, 2]
+    assert seen == [("r", [1.0, 4.0], [0.0, 3.0], [10.0, 13.0]), ("x", [2.0, 3.0], [1.0, 2.0], [11.0, 12.0])]
+    assert out["pmax"].tolist() == [1.0, 2.0, 3.0, 4.0]
