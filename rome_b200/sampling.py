@@ -8,6 +8,10 @@ The library itself never derives these tables -- it consumes the caller's
 that do not come from the reference, with the reference's arithmetic
 (scalar libm calls through `math`, the reference's operation order), and is
 checked against the reference's tables recorded in tests/golden/map3d_a.npz.
+It also restates the per-iteration choice of image sizes (the resolution
+reached, the current and coarse sizes, the shell counts and resolution
+tables: MAPModel::updateCurrentResolution and
+updateImageSizeAndResolutionPointers), checked against every golden case.
 """
 from __future__ import annotations
 
@@ -17,7 +21,8 @@ from typing import Tuple
 import numpy as np
 
 __all__ = ["healpix_directions", "psi_step_3d", "psi_angles_3d", "oversampled_orientations_3d",
-           "oversampled_translations", "euler_matrix", "euler_matrix2angles", "check_direction"]
+           "oversampled_translations", "euler_matrix", "euler_matrix2angles", "check_direction", "angular_sampling",
+           "resolution_indices", "npix_per_shell", "current_resolution", "image_sizes"]
 
 ROME_PI = 3.14159265358979323846      # rome_pi, src/math.h:38
 HALFPI = 1.570796326794896619231321691639751442099  # Healpix_2.15a/lsconstants.h:43
@@ -230,3 +235,88 @@ def oversampled_translations(tx: np.ndarray, ty: np.ndarray, offset_step: float,
                 ox[t, iy * n + ix] = x
                 oy[t, iy * n + ix] = y
     return ox, oy
+
+
+# ---- image sizes of an iteration (MAPModel::updateCurrentResolution, updateImageSizeAndResolutionPointers) ----
+
+def angular_sampling(healpix_order: int = -1, psi_step: float = 0.0, adaptive_oversampling: int = 0) -> float:
+    """HealpixSampler::getAngularSampling (src/sampling.cpp:287-295): 360 /
+    (6 * 2^(order + oversampling)) in 3D (healpix_order >= 0), else the psi
+    step / 2^oversampling."""
+    if healpix_order >= 0:
+        return 360.0 / (6 * round(2.0 ** (healpix_order + adaptive_oversampling)))
+    return psi_step / 2.0 ** adaptive_oversampling
+
+
+def resolution_indices(size: int) -> np.ndarray:
+    """Mresol_fine / Mresol_coarse of an image of `size` (src/map_model.cpp:540-575):
+    the rounded radius of every coefficient of the FFTW half-plane, -1 beyond
+    size / 2 and on the negative half of the x = 0 column."""
+    Fs = size // 2 + 1
+    i = np.arange(size)
+    ip = np.where(i < Fs, i, i - size)
+    jp = np.arange(Fs)
+    ires = np.round(np.sqrt(ip[:, None] ** 2 + jp[None, :] ** 2)).astype(np.int32)
+    bad = (ires >= Fs) | ((jp[None, :] == 0) & (ip[:, None] < 0))
+    return np.where(bad, -1, ires).astype(np.int32).reshape(-1)
+
+
+def npix_per_shell(ori_size: int) -> np.ndarray:
+    """Npix_per_shell (src/map_model.cpp:523-537): coefficients of the
+    ori_size half-plane per rounded radius, the negative half of the x = 0
+    column left out."""
+    r = resolution_indices(ori_size)
+    return np.bincount(r[r >= 0], minlength=ori_size // 2 + 1).astype(np.int32)
+
+
+def current_resolution(data_vs_prior: np.ndarray, ori_size: int, pixel_size: float, minres_map: int,
+                       do_map: bool = True, ini_high: float = 0.0, set_by_ini_high: bool = False) -> float:
+    """MAPModel::updateCurrentResolution (src/map_model.cpp:375-424), the
+    resolution (1/A) the next iteration works to: with MAP, from ini_high
+    when set_by_ini_high, else the shell before the first one (from 1) at
+    which any class's data_vs_prior drops below 1, the largest over classes
+    and at least minres_map; Nyquist without MAP."""
+    if do_map:
+        if set_by_ini_high:
+            maxres = int(round(ori_size * pixel_size / ini_high))
+        else:
+            maxres = 0
+            for row in np.asarray(data_vs_prior, np.float64):
+                ires = 1
+                while ires < ori_size // 2 and not row[ires] < 1.0:
+                    ires += 1
+                maxres = max(maxres, ires - 1)
+            maxres = max(maxres, minres_map)
+    else:
+        maxres = ori_size // 2
+    return maxres / (pixel_size * ori_size)
+
+
+def image_sizes(current_res: float, ori_size: int, pixel_size: float, adaptive_oversampling: int,
+                angular_sampling_deg: float, particle_diameter: float, ref_dim: int, incr_size: int = 10,
+                ave_pmax: float = 0.0, has_high_fsc_at_limit: bool = False, do_use_all_data: bool = False) -> dict:
+    """MAPModel::updateImageSizeAndResolutionPointers (src/map_model.cpp:463-576):
+    current_size = 2 * (the resolution's pixel + incr_size) (+ a quarter of
+    the image instead with a high FSC at the limit and Pmax > 0.1), at most
+    ori_size; with adaptive oversampling coarse_size = 2 * ceil(pixel_size *
+    ori_size / coarse_resolution), coarse_resolution the arc the angular
+    step sweeps on the particle's diameter divided by 1.2 (3D) or 1.5 (2D),
+    at most current_size; the shell counts and resolution tables of those
+    sizes."""
+    maxres = int(current_res * pixel_size * ori_size + 0.0001)  # getPixelFromResolution, src/map_model.h:102
+    if ave_pmax > 0.1 and has_high_fsc_at_limit:
+        maxres += int(round(0.25 * ori_size / 2))
+    else:
+        maxres += incr_size
+    cur = ori_size if do_use_all_data else maxres * 2
+    cur = min(cur, ori_size)
+    if adaptive_oversampling > 0:
+        rotated_distance = (angular_sampling_deg / 360.0) * ROME_PI * particle_diameter
+        keepsafe = 1.2 if ref_dim == 3 else 1.5
+        coarse = 2 * int(math.ceil(pixel_size * ori_size / (rotated_distance / keepsafe)))
+        coarse = min(ori_size, coarse)
+    else:
+        coarse = cur
+    coarse = min(cur, coarse)
+    return {"current_size": cur, "coarse_size": coarse, "Npix_per_shell": npix_per_shell(ori_size),
+            "Mresol_fine": resolution_indices(cur), "Mresol_coarse": resolution_indices(coarse)}

@@ -127,13 +127,8 @@ def rotate2d_np(data: np.ndarray, r_max: int, psi_deg: np.ndarray, size: int, pa
 
 def mresol(size: int) -> np.ndarray:
     """Mresol_fine / Mresol_coarse (src/map_model.cpp:540-575)."""
-    Fs = size // 2 + 1
-    i = np.arange(size)
-    ip = np.where(i < Fs, i, i - size)
-    jp = np.arange(Fs)
-    ires = np.round(np.sqrt(ip[:, None] ** 2 + jp[None, :] ** 2)).astype(np.int32)
-    bad = (ires >= Fs) | ((jp[None, :] == 0) & (ip[:, None] < 0))
-    return np.where(bad, -1, ires).astype(np.int32).reshape(-1)
+    from .sampling import resolution_indices
+    return resolution_indices(size)
 
 
 def translations(offset_range: int, offset_step: int):
