@@ -303,6 +303,7 @@ def lowres_proposals3d(aux: GpuContext, pool, k: int, coarse_size: int = 12, dev
     q = dataclasses.replace(pool, coarse_size=coarse_size, Mresol_coarse=mresol(coarse_size),
                             adaptive_fraction=1e-12, proposals=None)
     post = map3d_estep_pool(aux, q, marginals=True, dev=dev)["post_coarse"]
+    k = min(k, post.shape[1])  # k at or above the orientation count proposes them all
     top = np.argpartition(-post, k - 1, axis=1)[:, :k]
     mass = np.take_along_axis(post, top, axis=1).sum(axis=1)
     return np.sort(top, axis=1).astype(np.int32), mass

@@ -98,6 +98,10 @@ def test_lowres_proposals_from_the_small_coarse_pass(golden, monkeypatch):
     want = np.sort(np.argsort(-post, axis=1)[:, :5], axis=1)
     assert np.array_equal(props, want) and props.dtype == np.int32
     np.testing.assert_allclose(mass, np.take_along_axis(post, want, 1).sum(1), rtol=1e-12)
+    # more proposals than coarse orientations: all of them
+    props, mass = proposal.lowres_proposals3d("aux", p, Jc + 7, coarse_size=8)
+    assert np.array_equal(props, np.tile(np.arange(Jc, dtype=np.int32), (p.nr_images, 1)))
+    np.testing.assert_allclose(mass, 1.0, rtol=1e-12)
 
 
 def test_lowres_estep_splits_on_the_low_resolution_mass(golden, monkeypatch):
