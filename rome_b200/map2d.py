@@ -351,8 +351,10 @@ class GpuContext:
 
     def _bp_copy(self, to_library: int, buf) -> None:
         import torch
-        assert buf.dtype == torch.float64 and buf.is_contiguous() and buf.numel() == self.backprojector_doubles()
-        assert buf.is_cuda and buf.device.index == self.device
+        if not (buf.dtype == torch.float64 and buf.is_contiguous() and buf.numel() == self.backprojector_doubles()):
+            raise ValueError("back-projector buffer: a contiguous float64 tensor of backprojector_doubles() elements")
+        if not (buf.is_cuda and buf.device.index == self.device):
+            raise ValueError(f"back-projector buffer must live on cuda:{self.device}")
         stream = torch.cuda.current_stream(self.device)
         self._check(self.lib.rome_gpu_backprojector_device_copy(self.h, to_library, C.c_void_p(buf.data_ptr()),
                                                                 C.c_void_p(stream.cuda_stream)))
