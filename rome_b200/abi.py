@@ -143,24 +143,32 @@ class RomePrepOut(C.Structure):
                 ("old_offsety", _DP), ("power_imgs", _DP)]
 
 
+def _need(a: np.ndarray, dtype) -> None:
+    """An array handed to the library as a raw pointer: the element type and
+    C-contiguous layout the C side reads."""
+    if a.dtype != dtype or not a.flags.c_contiguous:
+        raise TypeError(f"expected a C-contiguous {np.dtype(dtype).name} array, got {a.dtype} "
+                        f"(C-contiguous: {a.flags.c_contiguous})")
+
+
 def dptr(a: Optional[np.ndarray]):
     if a is None:
         return _DP()
-    assert a.dtype == np.float64 and a.flags.c_contiguous, (a.dtype, a.flags)
+    _need(a, np.float64)
     return a.ctypes.data_as(_DP)
 
 
 def iptr(a: Optional[np.ndarray]):
     if a is None:
         return _IP()
-    assert a.dtype == np.int32 and a.flags.c_contiguous
+    _need(a, np.int32)
     return a.ctypes.data_as(_IP)
 
 
 def cptr(a: Optional[np.ndarray]):
     if a is None:
         return _CP()
-    assert a.dtype == np.int8 and a.flags.c_contiguous
+    _need(a, np.int8)
     return a.ctypes.data_as(_CP)
 
 

@@ -86,13 +86,15 @@ def prepare_particles(ctx: GpuContext, imgs: ParticleImages, opts: PrepOptions, 
     im = imgs.images
     if hasattr(im, "data_ptr"):  # torch tensor
         import torch
-        assert im.is_cuda and im.is_contiguous() and im.dtype in (torch.float32, torch.float64)
+        if not (im.is_cuda and im.is_contiguous() and im.dtype in (torch.float32, torch.float64)):
+            raise TypeError("device images: a contiguous float32 or float64 CUDA tensor")
         s.images, s.images_on_device = C.c_void_p(im.data_ptr()), 1
         s.image_type = 1 if im.dtype == torch.float32 else 0
         torch.cuda.current_stream(im.device).synchronize()
     else:
         im = np.ascontiguousarray(im)
-        assert im.dtype in (np.float32, np.float64)
+        if im.dtype not in (np.float32, np.float64):
+            raise TypeError(f"images: float32 or float64, got {im.dtype}")
         keep.append(im)
         s.images, s.images_on_device = C.c_void_p(im.ctypes.data), 0
         s.image_type = 1 if im.dtype == np.float32 else 0

@@ -26,7 +26,7 @@ _FP = C.POINTER(C.c_float)
 
 
 def _fptr(a: np.ndarray):
-    assert a.dtype == np.float32 and a.flags.c_contiguous
+    abi._need(a, np.float32)
     return a.ctypes.data_as(_FP)
 
 
@@ -114,7 +114,8 @@ class ProposalNet:
 
     def set_params(self, flat: np.ndarray):
         flat = np.ascontiguousarray(flat, np.float32)
-        assert flat.size == self.nparam
+        if flat.size != self.nparam:
+            raise ValueError(f"{flat.size} parameters given, the network has {self.nparam}")
         self.ctx._check(self.lib.rome_gpu_proposal_set_params(self.h, _fptr(flat)))
 
     def features(self, p) -> np.ndarray:
