@@ -81,3 +81,18 @@ def test_offsets_and_sizes_match_the_c_compiler():
         assert got[(name, "sizeof")] == ctypes.sizeof(st), name
         for field in st._fields_:
             assert got[(name, field[0])] == getattr(st, field[0]).offset, (name, field[0])
+
+
+def test_pointer_helpers_reject_the_wrong_arrays():
+    """Arrays passed to the library as raw pointers must have the element
+    type and C-contiguous layout the C side reads; anything else is refused
+    before the call (also under python -O)."""
+    import numpy as np
+    assert abi.dptr(None) is not None and not abi.dptr(None)
+    abi.dptr(np.zeros(3))
+    abi.iptr(np.zeros(3, np.int32))
+    abi.cptr(np.zeros(3, np.int8))
+    for bad, fn in ((np.zeros(3, np.float32), abi.dptr), (np.zeros((4, 4))[:, ::2], abi.dptr),
+                    (np.zeros(3, np.int64), abi.iptr), (np.zeros(3, np.uint8), abi.cptr)):
+        with pytest.raises(TypeError):
+            fn(bad)
